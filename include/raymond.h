@@ -1,0 +1,321 @@
+/*
+ * raymond.h — C ABI of the B200 wavefront path tracer.
+ *
+ * This is the drop-in boundary for the rendering path of iRath96/raymond
+ * (Swift host + Metal device library).  Every entry point below names the
+ * reference interface it replaces (paths are relative to the reference
+ * project).  The header is plain C99 so that a Swift host can import it
+ * through a module map, and so that Python reaches it through ctypes.
+ *
+ * Ownership: callers own every host array they pass; the library copies
+ * what it needs during the call (the reference copied into shared
+ * MTLBuffers, raymond/host/scene/ShapeBuilder.swift:259-268).  Device memory
+ * is owned by the library behind opaque handles and released by the
+ * matching *_destroy call.
+ *
+ * Errors: every function returns an rmd_status.  rmd_last_error() returns a
+ * thread-local description of the last failure on the calling thread
+ * (the reference threw CodegenError / MeshLoaderError, or returned nil,
+ * raymond/host/scene/MaterialBuilder.swift:45-51, Renderer.swift:319-330).
+ *
+ * Threading: calls on one handle must be serialised by the caller (the
+ * reference kept one frame in flight, Renderer.swift:285); distinct
+ * renderers are independent.
+ */
+#ifndef RAYMOND_H
+#define RAYMOND_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* ------------------------------------------------------------------ status */
+
+typedef int32_t rmd_status;
+#define RMD_OK                         0
+#define RMD_ERROR_INVALID_ARGUMENT     1
+#define RMD_ERROR_CUDA                 2
+#define RMD_ERROR_NVRTC                3
+/* Codegen errors, MaterialBuilder.swift:45-51 */
+#define RMD_ERROR_CODEGEN_CYCLE        4
+#define RMD_ERROR_CODEGEN_MULTI_INPUT  5
+#define RMD_ERROR_CODEGEN_UNSUPPORTED  6
+#define RMD_ERROR_OUT_OF_MEMORY        7
+/* a device queue was too small for the work pushed into it */
+#define RMD_ERROR_QUEUE_OVERFLOW       8
+/* a bounded device-side wait ran out */
+#define RMD_ERROR_WATCHDOG             9
+#define RMD_ERROR_NO_DEVICE           10
+
+/* Thread-local message for the last failing call on this thread. */
+const char *rmd_last_error(void);
+/* Library version string. */
+const char *rmd_version(void);
+
+/* --------------------------------------------------------------- constants */
+
+/* RayFlags, raymond/bridge/Ray.hpp:6-15 (entity visibility uses the same bits) */
+#define RMD_RAY_CAMERA        (1u << 0)
+#define RMD_RAY_REFLECTION    (1u << 1)
+#define RMD_RAY_TRANSMISSION  (1u << 2)
+#define RMD_RAY_SHADOW        (1u << 3)
+#define RMD_RAY_VOLUME        (1u << 4)
+#define RMD_RAY_DIFFUSE       (1u << 5)
+#define RMD_RAY_GLOSSY        (1u << 6)
+#define RMD_RAY_SINGULAR      (1u << 7)
+
+/* SamplingMode, raymond/bridge/Uniforms.hpp:5-9 */
+#define RMD_SAMPLING_BSDF  0
+#define RMD_SAMPLING_NEE   1
+#define RMD_SAMPLING_MIS   2
+
+/* Tonemapping, raymond/bridge/Uniforms.hpp:11-15 */
+#define RMD_TONEMAP_LINEAR 0
+#define RMD_TONEMAP_HABLE  1
+#define RMD_TONEMAP_ACES   2
+
+/* Random number generators.  RMD_RNG_TEA is the reference's PrngState
+ * (raymond/device/PrngState.metal:20-93) seeded per frame exactly as
+ * generateRays does (kernels/shading/generate.metal:88-94).  RMD_RNG_PCG32
+ * keeps the PrngState interface with a PCG32 body: one stream per path,
+ * sequence = sampleIndex * width * height + y * width + x. */
+#define RMD_RNG_PCG32 0
+#define RMD_RNG_TEA   1
+
+/* ---------------------------------------------------------- shader graphs */
+/*
+ * A material is the node graph the reference's Blender exporter writes
+ * (scripts/blender_exporter/raymond_blender/materials.py:273-547) and the
+ * Rayjay package parsed into Material/Node/Kernel types before
+ * MaterialBuilder.swift turned it into Metal (Codegen.add(material:),
+ * MaterialBuilder.swift:676-711).  Here the host passes it as plain structs.
+ */
+
+#define RMD_PARAM_STRING  0
+#define RMD_PARAM_NUMBER  1
+#define RMD_PARAM_BOOL    2
+#define RMD_PARAM_NUMBERS 3   /* flat float list, e.g. ColorRamp elements as
+                                 [pos, r, g, b, a, pos, r, g, b, a, ...] */
+
+typedef struct rmd_node_param {
+    const char *key;           /* e.g. "noise_dimensions", "blend_type" */
+    int32_t kind;              /* RMD_PARAM_* */
+    const char *string_value;  /* RMD_PARAM_STRING */
+    double number_value;       /* RMD_PARAM_NUMBER / RMD_PARAM_BOOL */
+    const float *numbers;      /* RMD_PARAM_NUMBERS */
+    int32_t num_numbers;
+} rmd_node_param;
+
+typedef struct rmd_node_input {
+    const char *name;          /* Blender socket identifier, e.g. "Base Color" */
+    const char *type;          /* "VALUE", "RGBA", "VECTOR", "SHADER", ... */
+    int32_t num_values;        /* 0: no literal; 1: scalar; 2..4: vector */
+    float values[4];
+    const char *link_node;     /* NULL when unlinked */
+    const char *link_socket;   /* output socket identifier of link_node */
+    int32_t num_links;         /* >1 reproduces CodegenError.multiInputDetected */
+} rmd_node_input;
+
+typedef struct rmd_node {
+    const char *name;          /* unique within the material */
+    const char *type;          /* Blender node type, e.g. "BSDF_PRINCIPLED" */
+    int32_t num_inputs;
+    const rmd_node_input *inputs;
+    int32_t num_params;
+    const rmd_node_param *params;
+} rmd_node;
+
+typedef struct rmd_material {
+    const char *name;
+    int32_t num_nodes;
+    const rmd_node *nodes;
+} rmd_material;
+
+/* ---------------------------------------------------------------- geometry */
+
+/* One shape = one PLY mesh of the reference (ShapeBuilder.swift:259-298). */
+typedef struct rmd_shape {
+    uint32_t num_vertices;
+    uint32_t num_faces;
+    const float *vertices;     /* 3 floats per vertex (packed float3, bridge/common.hpp:56) */
+    const float *normals;      /* 3 floats per vertex */
+    const float *texcoords;    /* 2 floats per vertex */
+    const uint32_t *indices;   /* 3 per face (IndexTriplet, bridge/common.hpp:66-75) */
+    const uint16_t *materials; /* per face: index into rmd_scene_desc.surface_materials */
+} rmd_shape;
+
+/* One entity = one instance of a shape (EntityBuilder.swift:66-77). */
+typedef struct rmd_entity {
+    uint32_t shape;
+    uint32_t visibility;       /* RMD_RAY_* mask (EntityBuilder.swift:55-64) */
+    float matrix[16];          /* column-major float4x4 point transform */
+} rmd_entity;
+
+/* --------------------------------------------------------------- lights */
+/* Field-for-field the device records of raymond/bridge/lights/ *.hpp, as
+ * LightBuilder.build fills them (LightBuilder.swift:187-223): colours
+ * already multiplied by power, spot angles already as cosines. */
+
+typedef struct rmd_light_info {             /* bridge/lights/LightInfo.hpp:5-9 */
+    uint16_t shader_index;                  /* index into light_materials */
+    uint8_t casts_shadows;
+    uint8_t uses_mis;                       /* the reference forces 0 (LightBuilder.swift:45) */
+} rmd_light_info;
+
+typedef struct rmd_area_light {             /* bridge/lights/AreaLight.hpp:6-16 */
+    rmd_light_info info;
+    float transform[12];                    /* float3x4: three float4 columns =
+                                               the first three rows of the world matrix */
+    float color[3];
+    uint32_t is_circular;
+} rmd_area_light;
+
+typedef struct rmd_point_light {            /* bridge/lights/PointLight.hpp:6-16 */
+    rmd_light_info info;
+    float location[3];
+    float radius;
+    float color[3];
+} rmd_point_light;
+
+typedef struct rmd_sun_light {              /* bridge/lights/SunLight.hpp:6-16 */
+    rmd_light_info info;
+    float direction[3];
+    float cos_angle;
+    float color[3];
+} rmd_sun_light;
+
+typedef struct rmd_spot_light {             /* bridge/lights/SpotLight.hpp:6-19 */
+    rmd_light_info info;
+    float location[3];
+    float direction[3];
+    float radius;
+    float color[3];
+    float spot_size;                        /* cos(size / 2) */
+    float spot_blend;                       /* (1 - spot_size) * blend */
+} rmd_spot_light;
+
+/* ---------------------------------------------------------------- camera */
+
+typedef struct rmd_camera {                 /* bridge/Camera.hpp:5-11 */
+    float transform[16];                    /* column-major camera-to-world */
+    float near_clip;
+    float far_clip;
+    float focal_length;                     /* lens_mm / (sensor_width / 2), SceneLoader.swift:135-136 */
+    float shift[2];
+} rmd_camera;
+
+/* ----------------------------------------------------------------- scene */
+
+typedef struct rmd_scene_desc {
+    int32_t num_surface_materials;          /* shadeSurface table */
+    const rmd_material *surface_materials;
+    int32_t num_light_materials;            /* shadeLight table */
+    const rmd_material *light_materials;
+
+    int32_t num_shapes;
+    const rmd_shape *shapes;
+    int32_t num_entities;
+    const rmd_entity *entities;
+
+    uint16_t world_shader;                  /* light material of the world (LightBuilder.swift:247-248) */
+    int32_t envmap_exponent;                /* envmap resolution 2^e; the reference uses 11 */
+
+    int32_t num_area_lights;
+    const rmd_area_light *area_lights;
+    int32_t num_point_lights;
+    const rmd_point_light *point_lights;
+    int32_t num_sun_lights;
+    const rmd_sun_light *sun_lights;
+    int32_t num_spot_lights;
+    const rmd_spot_light *spot_lights;
+
+    rmd_camera camera;
+} rmd_scene_desc;
+
+/* -------------------------------------------------------------- renderer */
+
+typedef struct rmd_render_settings {
+    uint32_t spp;              /* samples per pixel added by this call (one
+                                  reference frame per sample) */
+    uint32_t max_depth;        /* shade passes per path (Renderer.swift:290) */
+    uint32_t sampling_mode;    /* RMD_SAMPLING_* (Uniforms.samplingMode) */
+    uint32_t rng;              /* RMD_RNG_* */
+    uint64_t seed;             /* PCG32 initstate */
+    int64_t first_sample;      /* <0: continue after the samples already in
+                                  the film; >=0: start at this sample index */
+    uint32_t film_fp64;        /* accumulate the film in double precision */
+    uint32_t reserved;
+} rmd_render_settings;
+
+typedef struct rmd_stats {
+    uint64_t paths;            /* camera samples traced to termination */
+    uint64_t segments;         /* closest-hit rays traced and shaded */
+    uint64_t shadow_rays;      /* shadow rays traced */
+    uint64_t iterations;       /* wavefront iterations of the last render */
+    double   ms_total;         /* device time of the last render */
+    double   ms_trace;         /* closest-hit traversal */
+    double   ms_shade;         /* shading, NEE and BSDF sampling */
+    double   ms_shadow;        /* any-hit traversal + shadow resolve */
+    double   ms_film;          /* film accumulation and path regeneration */
+    uint32_t pool_size;        /* path slots in flight */
+    uint32_t errors;           /* device error flags (queue overflow, watchdog) */
+} rmd_stats;
+
+typedef struct rmd_context rmd_context;
+typedef struct rmd_scene rmd_scene;
+typedef struct rmd_renderer rmd_renderer;
+
+/* Device selection and stream.  Replaces MTLCreateSystemDefaultDevice and
+ * the command queue of Renderer.init (Renderer.swift:319-325). */
+rmd_status rmd_context_create(int32_t device, rmd_context **out);
+void rmd_context_destroy(rmd_context *ctx);
+
+/* Upload geometry, build the BVH, JIT-compile every material through NVRTC,
+ * build shape lights and the environment importance map.  Replaces
+ * SceneLoader.loadScene (SceneLoader.swift:46-143) with its
+ * MaterialBuilder / ShapeBuilder / EntityBuilder / LightBuilder stages. */
+rmd_status rmd_scene_create(rmd_context *ctx, const rmd_scene_desc *desc, rmd_scene **out);
+void rmd_scene_destroy(rmd_scene *scene);
+/* Number of triangles after instancing, and BVH nodes. */
+rmd_status rmd_scene_info(const rmd_scene *scene, uint64_t *triangles, uint64_t *bvh_nodes,
+                          int32_t *num_lights_total);
+
+/* Renderer.init (Renderer.swift:319-390). pool_size 0 = autotuned. */
+rmd_status rmd_renderer_create(rmd_scene *scene, uint32_t width, uint32_t height,
+                               uint32_t pool_size, rmd_renderer **out);
+void rmd_renderer_destroy(rmd_renderer *r);
+/* Renderer.setSize (Renderer.swift:757-798); clears the film. */
+rmd_status rmd_renderer_set_size(rmd_renderer *r, uint32_t width, uint32_t height);
+/* Renderer.reset (Renderer.swift:729-732). */
+rmd_status rmd_renderer_reset(rmd_renderer *r);
+/* Renderer.updateProjection / scene.camera (Renderer.swift:749-755); resets. */
+rmd_status rmd_renderer_set_camera(rmd_renderer *r, const rmd_camera *camera);
+
+/* Renderer.execute(in:) (Renderer.swift:480-696), settings->spp times:
+ * raygen, maxDepth shade passes with NEE shadow rays, film accumulation.
+ * Runs on the renderer's stream; returns when the work is enqueued and
+ * finished (blocking), with device error flags checked. */
+rmd_status rmd_render(rmd_renderer *r, const rmd_render_settings *settings);
+
+/* Copy the film to host memory: W*H*3 floats, row-major from the top-left
+ * pixel.  With normalize != 0 the normalizeImage kernel math is applied
+ * (exposure * L / samples, then the tonemap; normalizeImage.metal:39-59). */
+rmd_status rmd_film_read(rmd_renderer *r, float *rgb, int32_t normalize, uint32_t tonemapping,
+                         float exposure);
+/* The double-precision film (settings.film_fp64), raw sums. */
+rmd_status rmd_film_read_f64(rmd_renderer *r, double *rgb);
+/* Samples accumulated in the film (frameIndex of Renderer.swift:288). */
+rmd_status rmd_film_samples(const rmd_renderer *r, uint64_t *samples);
+
+/* Per-stage device timings and counters of the last rmd_render
+ * (RendererCounters, Renderer.swift:13-268). */
+rmd_status rmd_renderer_stats(const rmd_renderer *r, rmd_stats *out);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* RAYMOND_H */

@@ -1,0 +1,65 @@
+/*
+ * oracle.h — CPU restatement of the reference's rendering path.
+ *
+ * TEST INFRASTRUCTURE ONLY.  This library is the checker the parity tests,
+ * smoke() and the bench's CPU-baseline leg compare the CUDA path against; the
+ * product never links, loads or calls it.
+ *
+ * It restates iRath96/raymond's Metal device library (raymond/device/ **) and
+ * the host logic around it (Renderer.execute, LightBuilder, EntityBuilder,
+ * MaterialBuilder) as host C++ with OpenMP, each function citing the
+ * reference file:line it follows.  Apple's closed ray-tracing intersector is
+ * replaced by a CPU BVH with a watertight triangle test.
+ *
+ * Parity of this oracle against the reference itself is pinned by
+ * oracle/ref/ (the reference's own Metal sources compiled for the host
+ * through a shim) where that build is available; see the oracle tests.
+ */
+#ifndef RAYMOND_ORACLE_H
+#define RAYMOND_ORACLE_H
+
+#include <stdint.h>
+#include "../include/raymond.h"
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+typedef struct oracle_scene oracle_scene;
+
+typedef struct oracle_settings {
+    uint32_t width, height;
+    uint32_t spp;
+    uint32_t max_depth;
+    uint32_t sampling_mode; /* RMD_SAMPLING_* */
+    uint32_t rng;           /* RMD_RNG_* */
+    uint64_t seed;
+    int64_t first_sample;   /* sample index of the first frame */
+    int32_t threads;        /* 0 = all */
+    int32_t film_fp64;      /* accumulate in double */
+} oracle_settings;
+
+/* returns 0 or an RMD_ERROR_* code; err receives a message */
+int oracle_scene_create(const rmd_scene_desc *desc, oracle_scene **out, char *err, int errlen);
+void oracle_scene_destroy(oracle_scene *s);
+int oracle_scene_info(const oracle_scene *s, uint64_t *triangles, int32_t *num_lights_total, int32_t *num_shape_lights);
+
+/* Film sums (W*H*3, row-major from the top-left pixel) of `spp` frames;
+ * stats[0..2] = paths, segments (closest-hit rays shaded), shadow rays. */
+int oracle_render(oracle_scene *s, const oracle_settings *st, double *film_rgb, uint64_t *stats);
+
+/* Unit hooks. */
+/* n values of PrngState.sample() for the stream (a, b): TEA(a, b) or PCG32(seed=a, seq=b). */
+void oracle_prng(int32_t mode, uint64_t a, uint64_t b, int32_t n, float *out);
+/* rays: n x 8 floats (origin, tmin, direction, tmax); out: n x 4 (t, b0, b1, as-float prim)
+ * plus n instance ids; any != 0 runs the occlusion query (t = 1 occluded, -1 not). */
+int oracle_trace(const oracle_scene *s, const float *rays, int32_t n, int32_t any, float *out, uint32_t *instances);
+/* Perlin/fractal noise of utils/noise.hpp at n points (x,y,z): out[i] = fractal_noise(p, detail, roughness). */
+void oracle_fractal_noise3(const float *p, int32_t n, float detail, float roughness, float *out);
+/* Evaluate a surface material and its BSDF: see tests for the record layout. */
+int oracle_material_eval(const oracle_scene *s, int32_t material, const float *records, int32_t n, float *out);
+
+#ifdef __cplusplus
+}
+#endif
+#endif

@@ -1,0 +1,140 @@
+"""ctypes binding of the oracle library (oracle/oracle.h).
+
+TEST INFRASTRUCTURE ONLY: imported by tests/, by __graft_entry__.smoke() and
+by bench.py's CPU-baseline leg, as the checker.  The product never imports it.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+import subprocess
+from pathlib import Path
+
+import numpy as np
+
+HERE = Path(__file__).resolve().parent
+LIB = HERE / "_build" / "liboracle.so"
+
+
+class OracleSettings(C.Structure):
+    _fields_ = [("width", C.c_uint32), ("height", C.c_uint32), ("spp", C.c_uint32), ("max_depth", C.c_uint32),
+                ("sampling_mode", C.c_uint32), ("rng", C.c_uint32), ("seed", C.c_uint64),
+                ("first_sample", C.c_int64), ("threads", C.c_int32), ("film_fp64", C.c_int32)]
+
+
+def build() -> Path:
+    """Compile the oracle with its Makefile (gcc + OpenMP)."""
+    subprocess.run(["make", "-s", "-C", str(HERE)], check=True)
+    return LIB
+
+
+_lib = None
+
+
+def lib():
+    global _lib
+    if _lib is None:
+        if not LIB.exists():
+            build()
+        L = C.CDLL(str(LIB))
+        L.oracle_scene_create.argtypes = [C.c_void_p, C.POINTER(C.c_void_p), C.c_char_p, C.c_int]
+        L.oracle_scene_destroy.argtypes = [C.c_void_p]
+        L.oracle_scene_info.argtypes = [C.c_void_p, C.POINTER(C.c_uint64), C.POINTER(C.c_int32),
+                                        C.POINTER(C.c_int32)]
+        L.oracle_render.argtypes = [C.c_void_p, C.POINTER(OracleSettings), C.POINTER(C.c_double),
+                                    C.POINTER(C.c_uint64)]
+        L.oracle_prng.argtypes = [C.c_int32, C.c_uint64, C.c_uint64, C.c_int32, C.POINTER(C.c_float)]
+        L.oracle_trace.argtypes = [C.c_void_p, C.POINTER(C.c_float), C.c_int32, C.c_int32, C.POINTER(C.c_float),
+                                   C.POINTER(C.c_uint32)]
+        L.oracle_fractal_noise3.argtypes = [C.POINTER(C.c_float), C.c_int32, C.c_float, C.c_float,
+                                            C.POINTER(C.c_float)]
+        L.oracle_material_eval.argtypes = [C.c_void_p, C.c_int32, C.POINTER(C.c_float), C.c_int32,
+                                           C.POINTER(C.c_float)]
+        _lib = L
+    return _lib
+
+
+def _f32(a):
+    return np.ascontiguousarray(a, np.float32)
+
+
+class OracleScene:
+    def __init__(self, desc):
+        """desc: raymond_b200._abi.SceneDesc"""
+        self.desc = desc
+        self.h = C.c_void_p()
+        err = C.create_string_buffer(512)
+        st = lib().oracle_scene_create(C.byref(desc.c), C.byref(self.h), err, 512)
+        if st != 0:
+            raise RuntimeError(f"oracle_scene_create failed ({st}): {err.value.decode()}")
+
+    def __del__(self):
+        if getattr(self, "h", None) and self.h.value:
+            lib().oracle_scene_destroy(self.h)
+            self.h = C.c_void_p()
+
+    def info(self):
+        t = C.c_uint64()
+        n = C.c_int32()
+        s = C.c_int32()
+        lib().oracle_scene_info(self.h, C.byref(t), C.byref(n), C.byref(s))
+        return {"triangles": t.value, "lights": n.value, "shape_lights": s.value}
+
+    def render(self, width, height, spp, max_depth, sampling_mode=2, rng=0, seed=1, first_sample=0, threads=0,
+               film_fp64=False):
+        """Film sums (H, W, 3) float64 and stats (paths, segments, shadow rays)."""
+        st = OracleSettings(width, height, spp, max_depth, sampling_mode, rng, seed, first_sample, threads,
+                            int(film_fp64))
+        film = np.zeros((height, width, 3), np.float64)
+        stats = (C.c_uint64 * 3)()
+        r = lib().oracle_render(self.h, C.byref(st), film.ctypes.data_as(C.POINTER(C.c_double)), stats)
+        if r != 0:
+            raise RuntimeError(f"oracle_render failed ({r})")
+        return film, {"paths": stats[0], "segments": stats[1], "shadow_rays": stats[2]}
+
+    def trace(self, rays: np.ndarray, any_hit=False):
+        rays = _f32(rays)
+        n = len(rays)
+        out = np.zeros((n, 4), np.float32)
+        inst = np.zeros(n, np.uint32)
+        lib().oracle_trace(self.h, rays.ctypes.data_as(C.POINTER(C.c_float)), n, int(any_hit),
+                           out.ctypes.data_as(C.POINTER(C.c_float)), inst.ctypes.data_as(C.POINTER(C.c_uint32)))
+        return out, inst
+
+    def material_eval(self, material: int, records: np.ndarray):
+        records = _f32(records)
+        n = len(records)
+        out = np.zeros((n, 16), np.float32)
+        r = lib().oracle_material_eval(self.h, material, records.ctypes.data_as(C.POINTER(C.c_float)), n,
+                                       out.ctypes.data_as(C.POINTER(C.c_float)))
+        if r != 0:
+            raise RuntimeError(f"oracle_material_eval failed ({r})")
+        return out
+
+
+def prng(mode: int, a: int, b: int, n: int) -> np.ndarray:
+    out = np.zeros(n, np.float32)
+    lib().oracle_prng(mode, a, b, n, out.ctypes.data_as(C.POINTER(C.c_float)))
+    return out
+
+
+def fractal_noise3(p: np.ndarray, detail: float, roughness: float) -> np.ndarray:
+    p = _f32(p)
+    out = np.zeros(len(p), np.float32)
+    lib().oracle_fractal_noise3(p.ctypes.data_as(C.POINTER(C.c_float)), len(p), detail, roughness,
+                                out.ctypes.data_as(C.POINTER(C.c_float)))
+    return out
+
+
+def cpu_model() -> str:
+    try:
+        for line in open("/proc/cpuinfo"):
+            if line.startswith("model name"):
+                return line.split(":", 1)[1].strip()
+    except OSError:
+        pass
+    return "unknown"
+
+
+def cores() -> int:
+    return len(os.sched_getaffinity(0)) if hasattr(os, "sched_getaffinity") else os.cpu_count() or 1

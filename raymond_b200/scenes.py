@@ -1,0 +1,294 @@
+"""Seeded procedural scenes for the benchmark configurations.
+
+The reference ships no scenes (its author's scenes are not in the
+repository), so every input is generated here from a seed with numpy's
+PCG64 generator.  Each generator returns the scene dictionary consumed by
+`raymond_b200._abi.SceneDesc` (and by the C ABI through it).
+
+  cornell()        36-triangle Cornell box, emissive ceiling quad (radiance 15)
+  spheres_terrain() 64 icospheres + fBm terrain, sun + 16 point lights, noise graph
+  glossy_room()    10x10x4 closed room with furniture boxes, lit through a window
+"""
+from __future__ import annotations
+
+import math
+from typing import Any
+
+import numpy as np
+
+from . import materials as M
+from ._abi import VISIBLE_ALL
+
+
+# ----------------------------------------------------------------- helpers
+
+def look_at(eye, target, up=(0.0, 1.0, 0.0)) -> np.ndarray:
+    """Camera-to-world matrix (row-major); the camera looks down its -Z, +Y up."""
+    eye = np.asarray(eye, np.float64)
+    f = np.asarray(target, np.float64) - eye
+    f /= np.linalg.norm(f)
+    r = np.cross(f, np.asarray(up, np.float64))
+    r /= np.linalg.norm(r)
+    u = np.cross(r, f)
+    m = np.eye(4)
+    m[:3, 0], m[:3, 1], m[:3, 2], m[:3, 3] = r, u, -f, eye
+    return m
+
+
+def translate_scale_rotate_y(t=(0, 0, 0), s=(1, 1, 1), angle=0.0) -> np.ndarray:
+    c, sn = math.cos(angle), math.sin(angle)
+    rot = np.array([[c, 0, sn, 0], [0, 1, 0, 0], [-sn, 0, c, 0], [0, 0, 0, 1]])
+    sc = np.diag([s[0], s[1], s[2], 1.0])
+    tr = np.eye(4)
+    tr[:3, 3] = t
+    return tr @ rot @ sc
+
+
+def _orient(v: np.ndarray, idx: np.ndarray, want: np.ndarray) -> np.ndarray:
+    """Flip faces whose geometric normal cross(v1-v0, v2-v0) disagrees with `want`."""
+    n = np.cross(v[idx[:, 1]] - v[idx[:, 0]], v[idx[:, 2]] - v[idx[:, 0]])
+    flip = np.einsum("ij,ij->i", n, want) < 0
+    idx = idx.copy()
+    idx[flip, 1], idx[flip, 2] = idx[flip, 2], idx[flip, 1].copy()
+    return idx
+
+
+def quad_mesh(corners: np.ndarray, normal, material: int) -> dict[str, Any]:
+    """Two triangles over 4 corners (in order around the quad), flat normal."""
+    v = np.asarray(corners, np.float32)
+    n = np.tile(np.asarray(normal, np.float32), (4, 1))
+    t = np.array([[0, 0], [1, 0], [1, 1], [0, 1]], np.float32)
+    idx = np.array([[0, 1, 2], [0, 2, 3]], np.uint32)
+    idx = _orient(v, idx, n[:2]).astype(np.uint32)
+    return {"vertices": v, "normals": n, "texcoords": t, "indices": idx,
+            "materials": np.full(2, material, np.uint16)}
+
+
+def box_mesh(lo, hi, material: int) -> dict[str, Any]:
+    """Axis-aligned box, 6 faces x 2 triangles, outward normals."""
+    lo, hi = np.asarray(lo, np.float32), np.asarray(hi, np.float32)
+    faces = []
+    for axis in range(3):
+        for side, val in ((-1, lo[axis]), (1, hi[axis])):
+            a, b = [k for k in range(3) if k != axis]
+            c = np.zeros((4, 3), np.float32)
+            c[:, axis] = val
+            for i, (ua, ub) in enumerate(((0, 0), (1, 0), (1, 1), (0, 1))):
+                c[i, a] = lo[a] if ua == 0 else hi[a]
+                c[i, b] = lo[b] if ub == 0 else hi[b]
+            nrm = np.zeros(3, np.float32)
+            nrm[axis] = side
+            faces.append(quad_mesh(c, nrm, material))
+    return merge_meshes(faces)
+
+
+def merge_meshes(meshes: list[dict[str, Any]]) -> dict[str, Any]:
+    out: dict[str, list] = {k: [] for k in ("vertices", "normals", "texcoords", "indices", "materials")}
+    base = 0
+    for m in meshes:
+        out["vertices"].append(m["vertices"])
+        out["normals"].append(m["normals"])
+        out["texcoords"].append(m["texcoords"])
+        out["indices"].append(m["indices"] + base)
+        out["materials"].append(m["materials"])
+        base += len(m["vertices"])
+    return {"vertices": np.concatenate(out["vertices"]).astype(np.float32),
+            "normals": np.concatenate(out["normals"]).astype(np.float32),
+            "texcoords": np.concatenate(out["texcoords"]).astype(np.float32),
+            "indices": np.concatenate(out["indices"]).astype(np.uint32),
+            "materials": np.concatenate(out["materials"]).astype(np.uint16)}
+
+
+def icosphere(subdivisions: int) -> tuple[np.ndarray, np.ndarray]:
+    """Unit icosphere with Blender's subdivision count (1 = icosahedron, 20 faces;
+    every further level splits each face in four: subdivisions=5 -> 5120 faces)."""
+    p = (1 + 5 ** 0.5) / 2
+    v = [(-1, p, 0), (1, p, 0), (-1, -p, 0), (1, -p, 0), (0, -1, p), (0, 1, p), (0, -1, -p), (0, 1, -p),
+         (p, 0, -1), (p, 0, 1), (-p, 0, -1), (-p, 0, 1)]
+    f = [(0, 11, 5), (0, 5, 1), (0, 1, 7), (0, 7, 10), (0, 10, 11), (1, 5, 9), (5, 11, 4), (11, 10, 2),
+         (10, 7, 6), (7, 1, 8), (3, 9, 4), (3, 4, 2), (3, 2, 6), (3, 6, 8), (3, 8, 9), (4, 9, 5), (2, 4, 11),
+         (6, 2, 10), (8, 6, 7), (9, 8, 1)]
+    verts = [np.asarray(x, np.float64) / np.linalg.norm(x) for x in v]
+    faces = list(f)
+    for _ in range(max(0, subdivisions - 1)):
+        cache: dict[tuple[int, int], int] = {}
+
+        def mid(a: int, b: int) -> int:
+            key = (a, b) if a < b else (b, a)
+            if key not in cache:
+                m = verts[a] + verts[b]
+                verts.append(m / np.linalg.norm(m))
+                cache[key] = len(verts) - 1
+            return cache[key]
+
+        nf = []
+        for a, b, c in faces:
+            ab, bc, ca = mid(a, b), mid(b, c), mid(c, a)
+            nf += [(a, ab, ca), (b, bc, ab), (c, ca, bc), (ab, bc, ca)]
+        faces = nf
+    V = np.asarray(verts, np.float32)
+    F = np.asarray(faces, np.uint32)
+    F = _orient(V.astype(np.float64), F, V[F].mean(axis=1).astype(np.float64))
+    return V, F.astype(np.uint32)
+
+
+def sphere_mesh(V: np.ndarray, F: np.ndarray, material: int) -> dict[str, Any]:
+    u = (np.arctan2(V[:, 2], V[:, 0]) / (2 * np.pi) + 0.5).astype(np.float32)
+    w = (np.arccos(np.clip(V[:, 1], -1, 1)) / np.pi).astype(np.float32)
+    return {"vertices": V, "normals": V.copy(), "texcoords": np.stack([u, w], 1),
+            "indices": F, "materials": np.full(len(F), material, np.uint16)}
+
+
+def fbm_heightfield(n: int, octaves: int, seed: int) -> np.ndarray:
+    """(n+1)x(n+1) fractal sum of bilinearly interpolated value noise in [-1, 1]."""
+    rng = np.random.default_rng(seed)
+    h = np.zeros((n + 1, n + 1), np.float64)
+    amp, total = 1.0, 0.0
+    x = np.linspace(0, 1, n + 1)
+    for o in range(octaves):
+        res = 4 * 2 ** o
+        lattice = rng.uniform(-1, 1, (res + 2, res + 2))
+        gx = x * res
+        i0 = np.floor(gx).astype(int)
+        fx = gx - i0
+        fx = fx * fx * (3 - 2 * fx)
+        a = lattice[np.ix_(i0, i0)]
+        b = lattice[np.ix_(i0 + 1, i0)]
+        c = lattice[np.ix_(i0, i0 + 1)]
+        d = lattice[np.ix_(i0 + 1, i0 + 1)]
+        fxr = fx[:, None]
+        fzr = fx[None, :]
+        h += amp * ((a * (1 - fxr) + b * fxr) * (1 - fzr) + (c * (1 - fxr) + d * fxr) * fzr)
+        total += amp
+        amp *= 0.5
+    return h / total
+
+
+def terrain_mesh(cells: int, size: float, amplitude: float, octaves: int, seed: int, material: int):
+    h = fbm_heightfield(cells, octaves, seed) * amplitude
+    xs = np.linspace(0, size, cells + 1)
+    X, Z = np.meshgrid(xs, xs, indexing="ij")
+    V = np.stack([X, h, Z], -1).reshape(-1, 3).astype(np.float32)
+    dx = np.gradient(h, xs, axis=0)
+    dz = np.gradient(h, xs, axis=1)
+    N = np.stack([-dx, np.ones_like(h), -dz], -1)
+    N /= np.linalg.norm(N, axis=-1, keepdims=True)
+    T = np.stack([X / size, Z / size], -1).reshape(-1, 2).astype(np.float32)
+    i, j = np.meshgrid(np.arange(cells), np.arange(cells), indexing="ij")
+    a = (i * (cells + 1) + j).reshape(-1)
+    b = a + (cells + 1)
+    c = b + 1
+    d = a + 1
+    F = np.concatenate([np.stack([a, b, c], 1), np.stack([a, c, d], 1)]).astype(np.int64)
+    F = _orient(V.astype(np.float64), F, np.tile([0.0, 1.0, 0.0], (len(F), 1)))
+    return {"vertices": V, "normals": N.reshape(-1, 3).astype(np.float32), "texcoords": T,
+            "indices": F.astype(np.uint32), "materials": np.full(len(F), material, np.uint16)}
+
+
+def _identity():
+    return np.eye(4)
+
+
+# ----------------------------------------------------------------- configurations
+
+def cornell(seed: int = 1, envmap_exponent: int = 11) -> dict[str, Any]:
+    """Unit room (floor, ceiling, back, left, right walls), two boxes and a
+    0.25 x 0.25 emissive ceiling quad of radiance 15: 36 triangles.  Every
+    surface is Principled with base colour U[0.2, 0.8]^3, roughness 0.5,
+    metallic 0; the world is black."""
+    rng = np.random.default_rng(seed)
+    mats = []
+    shapes = []
+    entities = []
+
+    def add_material(name, graph):
+        mats.append((name, graph))
+        return len(mats) - 1
+
+    walls = {
+        "floor": ([[0, 0, 0], [1, 0, 0], [1, 0, 1], [0, 0, 1]], [0, 1, 0]),
+        "ceiling": ([[0, 1, 0], [1, 1, 0], [1, 1, 1], [0, 1, 1]], [0, -1, 0]),
+        "back": ([[0, 0, 0], [1, 0, 0], [1, 1, 0], [0, 1, 0]], [0, 0, 1]),
+        "left": ([[0, 0, 0], [0, 1, 0], [0, 1, 1], [0, 0, 1]], [1, 0, 0]),
+        "right": ([[1, 0, 0], [1, 1, 0], [1, 1, 1], [1, 0, 1]], [-1, 0, 0]),
+    }
+    for name, (corners, normal) in walls.items():
+        m = add_material(name, M.principled(base_color=tuple(rng.uniform(0.2, 0.8, 3)), roughness=0.5, metallic=0.0))
+        shapes.append(quad_mesh(np.asarray(corners, np.float32), normal, m))
+        entities.append({"shape": len(shapes) - 1, "matrix": _identity(), "visibility": VISIBLE_ALL})
+    for name, (size, pos, ang) in {"short_box": ((0.3, 0.3, 0.3), (0.33, 0.0, 0.62), 0.3),
+                                   "tall_box": ((0.3, 0.6, 0.3), (0.66, 0.0, 0.33), -0.3)}.items():
+        m = add_material(name, M.principled(base_color=tuple(rng.uniform(0.2, 0.8, 3)), roughness=0.5, metallic=0.0))
+        sx, sy, sz = size
+        shapes.append(box_mesh((-sx / 2, 0, -sz / 2), (sx / 2, sy, sz / 2), m))
+        entities.append({"shape": len(shapes) - 1, "matrix": translate_scale_rotate_y(pos, (1, 1, 1), ang),
+                         "visibility": VISIBLE_ALL})
+    m = add_material("light", M.emission((1, 1, 1, 1), 15.0))
+    y = 0.999
+    shapes.append(quad_mesh(np.asarray([[0.375, y, 0.375], [0.625, y, 0.375], [0.625, y, 0.625],
+                                        [0.375, y, 0.625]], np.float32), [0, -1, 0], m))
+    entities.append({"shape": len(shapes) - 1, "matrix": _identity(), "visibility": VISIBLE_ALL})
+    return {
+        "name": "cornell",
+        "materials": mats,
+        "light_materials": [("world", M.world((0, 0, 0, 1), 1.0))],
+        "world_shader": 0,
+        "envmap_exponent": envmap_exponent,
+        "shapes": shapes,
+        "entities": entities,
+        "camera": {"transform": look_at((0.5, 0.5, 2.3), (0.5, 0.5, 0.0)), "near_clip": 0.1, "far_clip": 100.0,
+                   "focal_length": 2.5},
+    }
+
+
+def spheres_terrain(seed: int = 1, num_spheres: int = 64, subdivisions: int = 5, terrain_cells: int = 512,
+                    num_point_lights: int = 16, envmap_exponent: int = 11) -> dict[str, Any]:
+    """64 icospheres (Blender subdivisions=5: 5120 faces each) with centres
+    U[0, 20]^3 and radius U[0.3, 1.5] on a 512 x 512-cell fBm terrain (4 octaves,
+    amplitude 2) spanning 20 x 20: 327,680 + 524,288 = 851,968 triangles.
+    Per object a Principled BSDF with roughness U[0.05, 1], metallic
+    Bernoulli(0.3), base colour U[0, 1]^3, whose base colour is
+    Noise(scale 5, detail 2) -> ColorRamp -> Mix(A = base colour).  One sun and
+    16 point lights; black world."""
+    rng = np.random.default_rng(seed)
+    V, F = icosphere(subdivisions)
+    mats, shapes, entities = [], [], []
+
+    def material(i):
+        return M.principled_noise_ramp(base_color=tuple(rng.uniform(0, 1, 3)), roughness=float(rng.uniform(0.05, 1.0)),
+                                       metallic=float(rng.uniform() < 0.3))
+
+    for i in range(num_spheres):
+        mats.append((f"sphere{i}", material(i)))
+        shapes.append(sphere_mesh(V, F, len(mats) - 1))
+        c = rng.uniform(0, 20, 3)
+        r = float(rng.uniform(0.3, 1.5))
+        entities.append({"shape": len(shapes) - 1, "matrix": translate_scale_rotate_y(c, (r, r, r), 0.0),
+                         "visibility": VISIBLE_ALL})
+    mats.append(("terrain", material(num_spheres)))
+    shapes.append(terrain_mesh(terrain_cells, 20.0, 2.0, 4, seed + 1000, len(mats) - 1))
+    entities.append({"shape": len(shapes) - 1, "matrix": _identity(), "visibility": VISIBLE_ALL})
+    lmats = [("world", M.world((0, 0, 0, 1), 1.0)), ("lamp", M.light((1, 1, 1, 1), 1.0))]
+    points = []
+    for i in range(num_point_lights):
+        col = rng.uniform(0.5, 1.0, 3)
+        points.append({"shader": 1, "location": tuple(rng.uniform([0, 4, 0], [20, 14, 20])), "radius": 0.0,
+                       "color": tuple(col * 400.0)})
+    suns = [{"shader": 1, "direction": (-0.4, 1.0, 0.3), "angle": 0.05, "color": (3.0, 2.9, 2.7)}]
+    return {
+        "name": "spheres_terrain",
+        "materials": mats,
+        "light_materials": lmats,
+        "world_shader": 0,
+        "envmap_exponent": envmap_exponent,
+        "shapes": shapes,
+        "entities": entities,
+        "point_lights": points,
+        "sun_lights": suns,
+        "camera": {"transform": look_at((10.0, 16.0, 40.0), (10.0, 3.0, 9.0)), "near_clip": 0.1, "far_clip": 100.0,
+                   "focal_length": 2.0},
+    }
+
+
+def triangle_count(scene: dict[str, Any]) -> int:
+    return int(sum(len(scene["shapes"][e["shape"]]["indices"]) for e in scene["entities"]))
