@@ -1,0 +1,262 @@
+"""Benchmark: the plain tracer at scale (config 2), whole-job Mpaths/s.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+
+Workload: 64 icospheres (Blender subdivisions 5) on a 512x512-cell fBm
+terrain, 851,968 triangles, noise->ramp->mix Principled material per object,
+1 sun + 16 point lights, 1920x1080, 64 spp, max depth 12, PCG32 seed 1.
+A step renders one full 64-spp frame (132.7 M paths).  With N ranks every
+rank renders its own 64 samples of the same image (sample ranges disjoint):
+weak scaling, no collective on the data path.
+
+`value`  : paths of all ranks / max-over-ranks device time (CUDA events of
+           the library's stream, reported by rmd_renderer_stats), scene and
+           path pool resident.
+`e2e`    : the same metric through the public C ABI with host buffers: each
+           step uploads the camera (rmd_renderer_set_camera), renders and
+           reads the film back to host memory (rmd_film_read).
+--impl reference times the CPU restatement of the reference's integrator
+(oracle/, all host cores) on a bounded sample of the same workload.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import threading
+import time
+from pathlib import Path
+
+import numpy as np
+
+ROOT = Path(__file__).resolve().parent
+sys.path.insert(0, str(ROOT))
+
+W, H, SPP, DEPTH, SEED = 1920, 1080, 64, 12, 1
+WORKLOAD = "spheres_terrain_1080p_64spp_depth12"
+METRIC = "Mpaths/s (plain tracer, config 2)"
+# algorithmic HBM bytes of the path state each stage must move (per unit)
+BYTES_TRACE_PER_RAY = 32 + 20      # ray in, hit out
+BYTES_SHADE_PER_SEGMENT = 20 + 64 + 32 + 110 + 48  # hit in, path state r/w, next ray, triangle attributes, shadow ray
+BYTES_SHADOW_PER_RAY = 32 + 8 + 16  # shadow ray in, occlusion flag, resolve read
+BYTES_FILM_PER_PATH = 24
+
+
+def rank_info():
+    return int(os.environ.get("RANK", "0")), int(os.environ.get("WORLD_SIZE", "1")), \
+        int(os.environ.get("LOCAL_RANK", "0"))
+
+
+class ClockSampler:
+    """nvidia-smi clocks and throttle reasons sampled every 200 ms."""
+
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, gpu_index: int):
+        self.gpu = gpu_index
+        self.rows: list[list[str]] = []
+        self.proc = None
+
+    def start(self):
+        try:
+            self.proc = subprocess.Popen(["nvidia-smi", f"--id={self.gpu}", f"--query-gpu={self.FIELDS}",
+                                          "--format=csv,noheader,nounits", "-lms", "200"],
+                                         stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.thread = threading.Thread(target=self._read, daemon=True)
+            self.thread.start()
+        except OSError:
+            self.proc = None
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.rows.append([x.strip() for x in line.split(",")])
+
+    def stop(self) -> dict:
+        if self.proc is None:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except subprocess.TimeoutExpired:
+            self.proc.kill()
+        sm = [float(r[1]) for r in self.rows if len(r) >= 9 and r[1].replace(".", "").isdigit()]
+        mx = [float(r[2]) for r in self.rows if len(r) >= 9 and r[2].replace(".", "").isdigit()]
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = sorted({names[k] for r in self.rows if len(r) >= 9 for k in range(4) if r[5 + k] == "Active"})
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": max(mx) if mx else None,
+                "reasons": reasons, "samples": len(self.rows)}
+
+
+def make_scene():
+    from raymond_b200 import scenes
+
+    return scenes.spheres_terrain(seed=SEED)
+
+
+def cpu_baseline_sample(desc, threads: int = 0):
+    """Oracle (CPU restatement, all host cores) on 1 spp of the full frame."""
+    sys.path.insert(0, str(ROOT / "oracle"))
+    import oracle_ctypes as O
+
+    orc = O.OracleScene(desc)
+    t0 = time.perf_counter()
+    film, st = orc.render(W, H, 1, DEPTH, first_sample=0, seed=SEED, threads=threads)
+    dt = time.perf_counter() - t0
+    return {"value": st["paths"] / dt / 1e6, "unit": "Mpaths/s", "cores": O.cores(), "kind": "port",
+            "sample": f"1 spp of the 1920x1080 frame ({st['paths']} paths, depth {DEPTH}) on {O.cpu_model()}",
+            "segments_per_s": st["segments"] / dt, "seconds": dt}
+
+
+def run_reference(args):
+    rank, world, _ = rank_info()
+    if rank != 0:
+        return
+    from raymond_b200._abi import SceneDesc
+
+    desc = SceneDesc(make_scene())
+    sys.path.insert(0, str(ROOT / "oracle"))
+    import oracle_ctypes as O
+
+    orc = O.OracleScene(desc)
+    # one step = 1 spp of the full frame (a bounded sample of the 64-spp step)
+    for _ in range(args.warmup):
+        orc.render(W, H, 1, DEPTH, first_sample=0, seed=SEED)
+    paths, secs = 0, 0.0
+    for k in range(args.steps):
+        t0 = time.perf_counter()
+        _, st = orc.render(W, H, 1, DEPTH, first_sample=k, seed=SEED)
+        secs += time.perf_counter() - t0
+        paths += st["paths"]
+    v = paths / secs / 1e6
+    line = {"impl": "reference", "metric": METRIC, "value": v, "unit": "Mpaths/s", "n_gpus": world,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 * secs / args.steps,
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+            "config": {"workload": WORKLOAD, "width": W, "height": H, "spp": SPP, "max_depth": DEPTH,
+                       "step": "1 spp of the frame per step (bounded CPU sample)"},
+            "cpu_baseline": {"value": v, "unit": "Mpaths/s", "cores": O.cores(), "kind": "port",
+                             "sample": f"1 spp of the 1920x1080 frame per step on {O.cpu_model()}"},
+            "e2e": {"value": v, "unit": "Mpaths/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(line), flush=True)
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=5)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--pool", type=int, default=0)
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    args = ap.parse_args()
+    if args.impl == "reference":
+        return run_reference(args)
+
+    rank, world, local = rank_info()
+    dist = None
+    if world > 1:
+        import torch.distributed as dist  # noqa: F811
+
+        dist.init_process_group("gloo", timeout=__import__("datetime").timedelta(seconds=600))
+
+    from raymond_b200 import api
+    from raymond_b200._abi import SceneDesc, make_camera
+
+    desc = SceneDesc(make_scene())
+    ctx = api.Context(local)
+    t0 = time.perf_counter()
+    scene = api.Scene(ctx, desc)
+    build_s = time.perf_counter() - t0
+    r = api.Renderer(scene, W, H, pool_size=args.pool)
+    cam = desc.scene["camera"]
+    film_host = np.zeros((H, W, 3), np.float32)
+
+    def step(k, e2e=False):
+        first = (rank + world * k) * SPP
+        if e2e:
+            r.set_camera(cam)  # host -> device: camera
+        else:
+            r.reset()
+        r.render(spp=SPP, max_depth=DEPTH, seed=SEED, first_sample=first)
+        if e2e:
+            film_host[:] = r.film()  # device -> host: the frame
+        return r.stats()
+
+    for k in range(args.warmup):
+        step(k)
+    if dist:
+        dist.barrier()
+    sampler = ClockSampler(local)
+    sampler.start()
+    tot_ms, tot = 0.0, {"paths": 0, "segments": 0, "shadow_rays": 0, "iterations": 0, "ms_trace": 0.0,
+                        "ms_shade": 0.0, "ms_shadow": 0.0, "ms_film": 0.0}
+    for k in range(args.steps):
+        s = step(k)
+        tot_ms += s["ms_total"]
+        for key in tot:
+            tot[key] += s[key]
+    clocks = sampler.stop()
+    # end to end through the C ABI with host buffers
+    t0 = time.perf_counter()
+    for k in range(args.steps):
+        step(k, e2e=True)
+    e2e_s = time.perf_counter() - t0
+    if dist:
+        import torch
+
+        t = torch.tensor([tot_ms, e2e_s], dtype=torch.float64)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        tot_ms, e2e_s = float(t[0]), float(t[1])
+        dist.barrier()
+    if rank != 0:
+        if dist:
+            dist.destroy_process_group()
+        return
+    paths_all = tot["paths"] * world
+    value = paths_all / (tot_ms / 1e3) / 1e6
+    seg_rate = tot["segments"] * world / (tot_ms / 1e3)
+    e2e_value = paths_all / e2e_s / 1e6
+    stage_ms = {"film_regen": tot["ms_film"], "trace": tot["ms_trace"], "shade": tot["ms_shade"],
+                "shadow": tot["ms_shadow"]}
+    dominant = max(stage_ms, key=stage_ms.get)
+    units = {"trace": (tot["segments"] + 0.0, BYTES_TRACE_PER_RAY),
+             "shade": (tot["segments"] + 0.0, BYTES_SHADE_PER_SEGMENT),
+             "shadow": (tot["shadow_rays"] + 0.0, BYTES_SHADOW_PER_RAY),
+             "film_regen": (tot["paths"] + 0.0, BYTES_FILM_PER_PATH)}
+    n_units, bpu = units[dominant]
+    achieved = n_units * bpu / (stage_ms[dominant] / 1e3) / 1e9
+    peaks = json.loads((ROOT / "MEASURED_PEAKS.json").read_text()) if (ROOT / "MEASURED_PEAKS.json").exists() else {}
+    peak = peaks.get("hbm_gbs", 6650.0)
+    line = {
+        "metric": METRIC, "value": value, "unit": "Mpaths/s", "n_gpus": world, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": tot_ms / args.steps, "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "f32", "data": "synthetic (seeded procedural scene)",
+        "config": {"workload": WORKLOAD, "width": W, "height": H, "spp_per_rank_step": SPP, "max_depth": DEPTH,
+                   "rng": "PCG32 seed 1", "triangles": scene.info()["triangles"],
+                   "l2": "inputs larger than L2 (path pool + BVH + film)", "pool_size": r.stats()["pool_size"],
+                   "parallelism": f"{world} ranks x disjoint sample ranges"},
+        "segments_per_s": seg_rate, "msegments_per_s": seg_rate / 1e6,
+        "stage_ms_per_step": {k: v / args.steps for k, v in stage_ms.items()},
+        "iterations_per_step": tot["iterations"] / args.steps,
+        "roofline": {"bound": "hbm", "kernel": dominant, "achieved": achieved, "peak": peak, "unit": "GB/s",
+                     "frac": achieved / peak, "peak_source": "measured" if peaks else "fallback",
+                     "bytes_per_unit": bpu, "traffic": None},
+        "e2e": {"value": e2e_value, "unit": "Mpaths/s", "h2d_bytes_per_step": 64 + 40,
+                "d2h_bytes_per_step": W * H * 3 * 4},
+        "gpu_launches": int(tot["iterations"] * 4 + args.steps),
+        "clocks": clocks,
+        "scene_build_s": build_s,
+    }
+    if not args.no_cpu_baseline:
+        line["cpu_baseline"] = cpu_baseline_sample(desc)
+    print(json.dumps(line), flush=True)
+    if dist:
+        dist.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

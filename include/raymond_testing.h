@@ -1,0 +1,54 @@
+/*
+ * raymond_testing.h — test hooks of the B200 path tracer.
+ *
+ * These entry points have no counterpart in the reference: they expose single
+ * device-side building blocks (random numbers, BVH queries, one material's
+ * BSDF) so that the parity tests can compare them with the CPU oracle on the
+ * same inputs.  They allocate and free scratch memory per call and are not
+ * meant for rendering.
+ */
+#ifndef RAYMOND_TESTING_H
+#define RAYMOND_TESTING_H
+
+#include "raymond.h"
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* n values of PrngState.sample() for one stream: TEA(a, b) (mode 1) or
+ * PCG32 with initstate a and sequence b (mode 0). */
+rmd_status rmd_test_prng(uint32_t mode, uint64_t a, uint64_t b, int32_t n, float *out);
+
+/* rays: n x 8 floats (origin.xyz, tmin, direction.xyz, tmax).  Closest hit:
+ * out n x 4 = (t or -1, weight of v0, weight of v1, primitive index bits),
+ * instances[n].  any != 0: occlusion query, out[4i] = 1 occluded / -1 not. */
+rmd_status rmd_test_trace(const rmd_scene *scene, const float *rays, int32_t n, int32_t any, float *out,
+                          uint32_t *instances);
+
+/* Shade n records with surface material `material` and evaluate / sample its
+ * BSDF as handleIntersections does.  Record: position, normal, trueNormal,
+ * generated, uv, wo, wi, rnd (float3 each), rayFlags, 3 pad (28 floats).
+ * Output: emission(3), eval(3), eval pdf, sampled wi(3), sampled weight(3),
+ * sampled pdf, sampled flags, alpha (16 floats). */
+rmd_status rmd_test_material_eval(const rmd_scene *scene, int32_t material, const float *records, int32_t n,
+                                  float *out);
+
+/* The CUDA source the material JIT generates for a scene description
+ * (hoist != 0: literals hoisted into per-material parameter blocks).  Writes
+ * at most buflen bytes (NUL-terminated) and the full size to *needed.  Needs
+ * no GPU. */
+rmd_status rmd_test_generate_source(const rmd_scene_desc *desc, int32_t hoist, char *buf, int64_t buflen,
+                                    int64_t *needed);
+
+/* Generate and NVRTC-compile the material module of a scene description for
+ * sm_100a without loading it (no GPU needed).  The compile log (or the error)
+ * goes to `log`, the cubin size to *cubin_bytes. */
+rmd_status rmd_test_jit_compile(const rmd_scene_desc *desc, int32_t hoist, char *log, int64_t loglen,
+                                int64_t *cubin_bytes);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif

@@ -876,6 +876,15 @@ static Kind coercedKind(const std::string &type) {
     throw CodegenError{RMD_ERROR_CODEGEN_UNSUPPORTED, "unsupported socket type '" + type + "'"};
 }
 
+// `field = TYPE(x)` compiles when the coerced type is the field's, or a scalar
+// widened to a vector (Metal's implicit scalar-to-vector conversion).
+static void checkAssignable(const std::string &type, Kind fieldKind, const std::string &field) {
+    const Kind k = coercedKind(type);
+    if (k == fieldKind) return;
+    if (k == K_F1 && (fieldKind == K_F3 || fieldKind == K_F4)) return;
+    throw CodegenError{RMD_ERROR_CODEGEN_UNSUPPORTED, "cannot assign " + type + " to field '" + field + "'"};
+}
+
 static void coerce(const std::string &type, Kind k, const void *src, Kind dstKind, void *dst) {
     float f[4] = {0, 0, 0, 0};
     const UberShader *sh = nullptr;
@@ -988,11 +997,13 @@ MaterialProgram::MaterialProgram(const rmd_material &m) {
                 bool isDefault = (!defaultInput.empty() && defaultInput == in->name);
                 if (isDefault || in->num_values <= 0) continue;  // value cleared by provideDefaults / no value
                 auto fd = step.proto->field(fieldName);
-                if (!fd) continue;  // field not consumed by the kernel struct: literal is dropped
+                if (!fd)  // the generated Metal would not compile: the struct has no such field
+                    throw CodegenError{RMD_ERROR_CODEGEN_UNSUPPORTED,
+                                       "node '" + key + "' has no input field '" + fieldName + "'"};
                 // MaterialBuilder.swift:110-121: TYPE(literal)
                 std::string ty = in->type ? in->type : "VALUE";
-                Kind litKind = in->num_values == 1 ? K_F1 : (Kind)in->num_values;
-                coercedKind(ty);
+                Kind litKind = in->num_values == 1 ? K_F1 : (Kind)std::min(4, in->num_values);
+                checkAssignable(ty, fd->kind, fieldName);
                 coerce(ty, litKind, in->values, fd->kind, (char *)base + fd->offset);
                 inputs.erase(fd->name);
             } else {
@@ -1013,7 +1024,9 @@ MaterialProgram::MaterialProgram(const rmd_material &m) {
                 b.dst_offset = fd->offset;
                 b.dst_kind = fd->kind;
                 b.in_type = in->type ? in->type : "VALUE";
-                coercedKind(b.in_type);
+                checkAssignable(b.in_type, fd->kind, fieldName);
+                if (b.in_type == "VALUE" && sfd->kind == K_F2)
+                    throw CodegenError{RMD_ERROR_CODEGEN_UNSUPPORTED, "VALUE() of a float2 output"};
                 b.src_node = si;
                 b.src_offset = sfd->offset;
                 b.src_kind = sfd->kind;

@@ -1,0 +1,235 @@
+"""Python host API over the C ABI of librmd.so.
+
+Mirrors the reference's host objects: `Scene` is SceneLoader.loadScene's
+result (SceneLoader.swift:46-143), `Renderer` is Renderer
+(Renderer.swift:270-808) with render() = execute(in:) repeated `spp` times,
+set_size / reset / set_camera, film read-out with normalizeImage's
+arithmetic, and per-stage statistics (RendererCounters).
+
+Every call goes through librmd.so; there is no Python or CPU fallback: when
+the library or a GPU is missing the calls raise.
+"""
+from __future__ import annotations
+
+import ctypes as C
+from pathlib import Path
+from typing import Any
+
+import numpy as np
+
+from . import _abi
+from ._abi import RenderSettings, SceneDesc, Stats
+
+LIB_PATH = Path(__file__).resolve().parent / "librmd.so"
+
+# every function the C headers declare (include/raymond.h, include/raymond_testing.h)
+EXPORTS = [
+    "rmd_last_error", "rmd_version", "rmd_context_create", "rmd_context_destroy", "rmd_scene_create",
+    "rmd_scene_destroy", "rmd_scene_info", "rmd_renderer_create", "rmd_renderer_destroy", "rmd_renderer_set_size",
+    "rmd_renderer_reset", "rmd_renderer_set_camera", "rmd_render", "rmd_film_read", "rmd_film_read_f64",
+    "rmd_film_samples", "rmd_renderer_stats",
+    "rmd_test_prng", "rmd_test_trace", "rmd_test_material_eval", "rmd_test_generate_source", "rmd_test_jit_compile",
+]
+
+
+class RmdError(RuntimeError):
+    def __init__(self, status: int, message: str):
+        super().__init__(f"{_abi.STATUS_NAMES.get(status, status)}: {message}")
+        self.status = status
+
+
+_lib = None
+
+
+def lib() -> C.CDLL:
+    """Load librmd.so (build it first with raymond_b200.build)."""
+    global _lib
+    if _lib is not None:
+        return _lib
+    if not LIB_PATH.exists():
+        raise RuntimeError(f"{LIB_PATH} is missing: run `python -m raymond_b200.build`")
+    L = C.CDLL(str(LIB_PATH))
+    vp = C.c_void_p
+    P = C.POINTER
+    sig = {
+        "rmd_last_error": ([], C.c_char_p),
+        "rmd_version": ([], C.c_char_p),
+        "rmd_context_create": ([C.c_int32, P(vp)], C.c_int32),
+        "rmd_context_destroy": ([vp], None),
+        "rmd_scene_create": ([vp, P(_abi.SceneDescC), P(vp)], C.c_int32),
+        "rmd_scene_destroy": ([vp], None),
+        "rmd_scene_info": ([vp, P(C.c_uint64), P(C.c_uint64), P(C.c_int32)], C.c_int32),
+        "rmd_renderer_create": ([vp, C.c_uint32, C.c_uint32, C.c_uint32, P(vp)], C.c_int32),
+        "rmd_renderer_destroy": ([vp], None),
+        "rmd_renderer_set_size": ([vp, C.c_uint32, C.c_uint32], C.c_int32),
+        "rmd_renderer_reset": ([vp], C.c_int32),
+        "rmd_renderer_set_camera": ([vp, P(_abi.Camera)], C.c_int32),
+        "rmd_render": ([vp, P(RenderSettings)], C.c_int32),
+        "rmd_film_read": ([vp, P(C.c_float), C.c_int32, C.c_uint32, C.c_float], C.c_int32),
+        "rmd_film_read_f64": ([vp, P(C.c_double)], C.c_int32),
+        "rmd_film_samples": ([vp, P(C.c_uint64)], C.c_int32),
+        "rmd_renderer_stats": ([vp, P(Stats)], C.c_int32),
+        "rmd_test_prng": ([C.c_uint32, C.c_uint64, C.c_uint64, C.c_int32, P(C.c_float)], C.c_int32),
+        "rmd_test_trace": ([vp, P(C.c_float), C.c_int32, C.c_int32, P(C.c_float), P(C.c_uint32)], C.c_int32),
+        "rmd_test_material_eval": ([vp, C.c_int32, P(C.c_float), C.c_int32, P(C.c_float)], C.c_int32),
+        "rmd_test_generate_source": ([P(_abi.SceneDescC), C.c_int32, C.c_char_p, C.c_int64, P(C.c_int64)], C.c_int32),
+        "rmd_test_jit_compile": ([P(_abi.SceneDescC), C.c_int32, C.c_char_p, C.c_int64, P(C.c_int64)], C.c_int32),
+    }
+    for name, (args, res) in sig.items():
+        f = getattr(L, name)
+        f.argtypes = args
+        f.restype = res
+    _lib = L
+    return L
+
+
+def check(status: int) -> None:
+    if status != 0:
+        raise RmdError(status, lib().rmd_last_error().decode(errors="replace"))
+
+
+def _f32p(a: np.ndarray):
+    return a.ctypes.data_as(C.POINTER(C.c_float))
+
+
+class Context:
+    """A CUDA device and stream (rmd_context)."""
+
+    def __init__(self, device: int = 0):
+        self.h = C.c_void_p()
+        check(lib().rmd_context_create(device, C.byref(self.h)))
+
+    def close(self):
+        if self.h.value:
+            lib().rmd_context_destroy(self.h)
+            self.h = C.c_void_p()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+class Scene:
+    """Geometry, BVH, JIT-compiled materials and lights on one device."""
+
+    def __init__(self, ctx: Context, scene: dict[str, Any] | SceneDesc):
+        self.ctx = ctx
+        self.desc = scene if isinstance(scene, SceneDesc) else SceneDesc(scene)
+        self.h = C.c_void_p()
+        check(lib().rmd_scene_create(ctx.h, C.byref(self.desc.c), C.byref(self.h)))
+
+    def info(self) -> dict[str, int]:
+        t, n = C.c_uint64(), C.c_uint64()
+        lights = C.c_int32()
+        check(lib().rmd_scene_info(self.h, C.byref(t), C.byref(n), C.byref(lights)))
+        return {"triangles": t.value, "bvh_nodes": n.value, "lights": lights.value}
+
+    def trace(self, rays: np.ndarray, any_hit: bool = False):
+        rays = np.ascontiguousarray(rays, np.float32)
+        n = len(rays)
+        out = np.zeros((n, 4), np.float32)
+        inst = np.zeros(n, np.uint32)
+        check(lib().rmd_test_trace(self.h, _f32p(rays), n, int(any_hit), _f32p(out),
+                                   inst.ctypes.data_as(C.POINTER(C.c_uint32))))
+        return out, inst
+
+    def material_eval(self, material: int, records: np.ndarray) -> np.ndarray:
+        records = np.ascontiguousarray(records, np.float32)
+        out = np.zeros((len(records), 16), np.float32)
+        check(lib().rmd_test_material_eval(self.h, material, _f32p(records), len(records), _f32p(out)))
+        return out
+
+    def close(self):
+        if self.h.value:
+            lib().rmd_scene_destroy(self.h)
+            self.h = C.c_void_p()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+class Renderer:
+    """Wavefront renderer for one film (rmd_renderer)."""
+
+    def __init__(self, scene: Scene, width: int, height: int, pool_size: int = 0):
+        self.scene = scene
+        self.width, self.height = width, height
+        self.h = C.c_void_p()
+        check(lib().rmd_renderer_create(scene.h, width, height, pool_size, C.byref(self.h)))
+
+    def render(self, spp: int, max_depth: int = 8, sampling_mode: int = _abi.SAMPLING_MIS, rng: int = _abi.RNG_PCG32,
+               seed: int = 1, first_sample: int = -1, film_fp64: bool = False) -> None:
+        s = RenderSettings(spp, max_depth, sampling_mode, rng, seed, first_sample, int(film_fp64), 0)
+        check(lib().rmd_render(self.h, C.byref(s)))
+
+    def film(self, normalize: bool = False, tonemapping: int = _abi.TONEMAP_LINEAR, exposure: float = 1.0) -> np.ndarray:
+        out = np.zeros((self.height, self.width, 3), np.float32)
+        check(lib().rmd_film_read(self.h, _f32p(out), int(normalize), tonemapping, exposure))
+        return out
+
+    def film64(self) -> np.ndarray:
+        out = np.zeros((self.height, self.width, 3), np.float64)
+        check(lib().rmd_film_read_f64(self.h, out.ctypes.data_as(C.POINTER(C.c_double))))
+        return out
+
+    def samples(self) -> int:
+        v = C.c_uint64()
+        check(lib().rmd_film_samples(self.h, C.byref(v)))
+        return v.value
+
+    def reset(self) -> None:
+        check(lib().rmd_renderer_reset(self.h))
+
+    def set_size(self, width: int, height: int) -> None:
+        check(lib().rmd_renderer_set_size(self.h, width, height))
+        self.width, self.height = width, height
+
+    def set_camera(self, camera: dict[str, Any]) -> None:
+        cam = _abi.make_camera(camera)
+        check(lib().rmd_renderer_set_camera(self.h, C.byref(cam)))
+
+    def stats(self) -> dict[str, float]:
+        s = Stats()
+        check(lib().rmd_renderer_stats(self.h, C.byref(s)))
+        return {k: getattr(s, k) for k, _ in Stats._fields_}
+
+    def close(self):
+        if self.h.value:
+            lib().rmd_renderer_destroy(self.h)
+            self.h = C.c_void_p()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+def generate_source(scene: dict[str, Any] | SceneDesc, hoist: bool = True) -> str:
+    """The CUDA source the material JIT emits for a scene (no GPU needed)."""
+    desc = scene if isinstance(scene, SceneDesc) else SceneDesc(scene)
+    need = C.c_int64()
+    check(lib().rmd_test_generate_source(C.byref(desc.c), int(hoist), None, 0, C.byref(need)))
+    buf = C.create_string_buffer(need.value)
+    check(lib().rmd_test_generate_source(C.byref(desc.c), int(hoist), buf, need.value, C.byref(need)))
+    return buf.value.decode()
+
+
+def jit_compile(scene: dict[str, Any] | SceneDesc, hoist: bool = True) -> tuple[int, str]:
+    """NVRTC-compile a scene's material module for sm_100a (no GPU needed): (cubin bytes, log)."""
+    desc = scene if isinstance(scene, SceneDesc) else SceneDesc(scene)
+    log = C.create_string_buffer(1 << 16)
+    nbytes = C.c_int64()
+    check(lib().rmd_test_jit_compile(C.byref(desc.c), int(hoist), log, 1 << 16, C.byref(nbytes)))
+    return nbytes.value, log.value.decode(errors="replace")
+
+
+def test_prng(mode: int, a: int, b: int, n: int) -> np.ndarray:
+    out = np.zeros(n, np.float32)
+    check(lib().rmd_test_prng(mode, a, b, n, _f32p(out)))
+    return out

@@ -1,0 +1,38 @@
+// Node graph -> CUDA source for the NVRTC material module.
+#pragma once
+#include <cstdint>
+#include <string>
+#include <vector>
+
+#include "../../include/raymond.h"
+
+namespace rmdhost {
+
+struct CodegenError {
+    int status;
+    std::string message;
+};
+
+// Swift `camelCase` + non-word replacement of MaterialBuilder.swift:19-30,41-43.
+std::string makeIdentifier(const std::string &name);
+
+struct MaterialTable {
+    // per material: (function group, offset into params)
+    std::vector<uint32_t> group, offset;
+};
+
+struct GeneratedModule {
+    std::string source;                  // CUDA source (includes device/integrator.cuh)
+    std::vector<float> params;           // hoisted literals of all materials
+    MaterialTable surface, light;
+    std::vector<bool> surfaceEmissive;   // Material.hasSurfaceEmission per surface material
+    int surfaceGroups = 0, lightGroups = 0;
+};
+
+// Emits one function per distinct graph structure; literal inputs become
+// loads from a per-material parameter block when `hoist` is set, or inline
+// constants (the reference's code shape) otherwise.  Throws CodegenError.
+GeneratedModule generateModule(const rmd_material *surface, int numSurface, const rmd_material *light, int numLight,
+                               bool hoist);
+
+}  // namespace rmdhost

@@ -1,0 +1,219 @@
+// The shading megakernel (handleIntersections, raymond/device/kernels/shading/
+// intersection.metal:22-211) and the environment-map build kernel
+// (kernels/envmap/build.metal:4-51) over the wavefront path pool.  Compiled
+// by NVRTC together with the generated material functions, so shadeSurface /
+// shadeLight resolve to the scene's node graphs.
+#pragma once
+#include "nodes.cuh"
+#include "wavefront.cuh"
+
+namespace rmd {
+
+// intersection.metal:14-20
+RMD_HD float computeMisWeight(float pdf, float other) {
+    pdf *= pdf;
+    if (is_inf(pdf)) return 1.0f;
+    other *= other;
+    return pdf / (pdf + other);
+}
+
+// One path vertex: intersection.metal:43-208 for the path in `slot`.
+__device__ __forceinline__ void shadePath(const ShadeParams &p, uint32_t slot) {
+    const Context &ctx = p.ctx;
+    const PathPool &pool = p.pool;
+    const FrameParams &fp = p.fp;
+    Counters *cnt = p.counters;
+
+    const float4 d4 = pool.rayD[slot];
+    const float4 tp4 = pool.tp[slot];
+    const float4 h4 = pool.hit[slot];
+    const uint32_t meta = pool.meta[slot];
+    const uint32_t pixel = pool.pixel[slot];
+    const uint32_t sample = pool.sample[slot];
+    float3 L = xyz(pool.L[slot]);
+    const float3 rayDir = xyz(d4);
+    const float3 rayWeight = xyz(tp4);
+    const float rayBsdfPdf = tp4.w;
+    const uint32_t depth = meta & 0xffffu;
+    const uint32_t rayFlags = (meta >> 16) & 0xffu;
+    const bool lastDepth = depth + 1u >= fp.maxDepth;
+    PrngState prng = PrngState::unpack(fp.rngMode, pool.rng[slot], pathSequence(sample, pixel, fp.numPixels));
+
+    const bool needsToCollectEmission = is_inf(rayBsdfPdf) || fp.samplingMode != 1u;
+    ShadingContext shading;
+    shading.rayFlags = rayFlags;
+    shading.rnd = prng.sample3d();
+    shading.wo = -rayDir;
+
+    bool alive = false;
+    if (h4.x <= 0.0f) {  // miss, intersection.metal:75-91
+        if (needsToCollectEmission) {
+            const float misWeight = (fp.samplingMode == 0u) || is_inf(rayBsdfPdf)
+                                        ? 1.0f
+                                        : computeMisWeight(rayBsdfPdf, lightsEnvmapPdf(ctx, rayDir));
+            evaluateEnvironment(ctx, shading);
+            L += misWeight * rayWeight * shading.material.emission;
+        }
+    } else {
+        warpAdd64(&cnt->segments, 1u);
+        const PerInstanceData &inst = ctx.instances[pool.hitInst[slot]];
+        uint32_t shaderIndex;
+        buildShading(shading, ctx, inst, __float_as_uint(h4.w), make_float2(h4.y, h4.z), h4.x, shaderIndex);
+        if (inst.visibility & rayFlags) shadeSurface(shaderIndex, ctx, shading);
+        else shading.material.alpha = 0.0f;
+
+        if (needsToCollectEmission && mean(shading.material.emission) != 0.0f) {
+            const float misWeight = (fp.samplingMode == 0u) || is_inf(rayBsdfPdf)
+                                        ? 1.0f
+                                        : computeMisWeight(rayBsdfPdf, lightsShapePdf(ctx, inst, shading));
+            L += misWeight * rayWeight * shading.material.emission;
+        }
+
+        float3 shNormal;
+        if (all_zero(shading.material.normal)) {
+            shNormal = shading.trueNormal;
+        } else {
+            float3 geoNormal = shading.trueNormal;
+            if (dot(geoNormal, shading.wo) < 0.0f) geoNormal *= -1.0f;
+            shNormal = ensure_valid_reflection(geoNormal, shading.wo, shading.material.normal);
+        }
+
+        if (fp.samplingMode != 0u) {  // NEE, intersection.metal:149-181
+            LightSample nee = lightsSample(ctx, shading, prng);
+            float bsdfPdf;
+            const float3 bsdf = shading.material.evaluate(shading.wo, nee.direction, shNormal, shading.trueNormal, bsdfPdf);
+            const float3 contribution = nee.weight * bsdf * rayWeight;
+            if (nee.castsShadows) {
+                const float misWeight =
+                    fp.samplingMode == 1u || !nee.canBeHit ? 1.0f : computeMisWeight(nee.pdf, bsdfPdf);
+                const float3 neeWeight = misWeight * contribution;
+                // shadow rays of the last shade pass are never traced (Renderer.swift:623-625)
+                if (isfinite3(neeWeight) && any_nonzero(neeWeight) && !lastDepth) {
+                    const uint32_t k = warpAppend(&cnt->nShadow);
+                    if (k < pool.capacity) {
+                        pool.shO[k] = f4(shading.position, nee.distance - SHADOW_EPS);
+                        pool.shD[k] = f4(nee.direction, __uint_as_float(slot));
+                        pool.shW[k] = f4(neeWeight, 0.0f);
+                    } else {
+                        atomicOr(&cnt->errors, ERR_QUEUE_OVERFLOW);
+                    }
+                }
+            } else {
+                L += rayWeight * contribution;  // intersection.metal:172-179 (weight applied twice, as there)
+            }
+        }
+
+        // BSDF sampling and Russian roulette, intersection.metal:185-208
+        const BsdfSample bs = shading.material.sample(shading.rnd, -rayDir, shNormal, shading.trueNormal, (uint8_t)rayFlags);
+        const float3 weight = rayWeight * bs.weight;
+        const float meanWeight = mean(weight);
+        if (is_finite(meanWeight)) {
+            const float survivalProb = fminf(meanWeight, 1.0f);
+            if (prng.sample() < survivalProb && !lastDepth) {
+                alive = true;
+                pool.rayO[slot] = f4(shading.position, SHADOW_EPS);
+                pool.rayD[slot] = f4(bs.wi, inf_f());
+                pool.tp[slot] = f4(weight * (1.0f / survivalProb), bs.pdf);
+                pool.meta[slot] = (depth + 1u) | ((uint32_t)bs.flags << 16);
+                pool.rng[slot] = prng.pack();
+            }
+        }
+    }
+    pool.L[slot] = f4(L, 0.0f);
+    if (alive) {
+        const uint32_t k = warpAppend(&cnt->nQ[p.cur ^ 1u]);
+        if (k < pool.capacity) pool.q[p.cur ^ 1u][k] = slot;
+        else atomicOr(&cnt->errors, ERR_QUEUE_OVERFLOW);
+    } else {
+        const uint32_t k = warpAppend(&cnt->nDone);
+        if (k < pool.capacity) pool.qDone[k] = slot;
+        else atomicOr(&cnt->errors, ERR_QUEUE_OVERFLOW);
+    }
+}
+
+}  // namespace rmd
+
+extern "C" __global__ void __launch_bounds__(128) rmd_shade(const __grid_constant__ rmd::ShadeParams p) {
+    const unsigned n = p.counters->nQ[p.cur];
+    const unsigned *q = p.pool.q[p.cur];
+    for (unsigned i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x)
+        rmd::shadePath(p, q[i]);
+}
+
+// kernels/envmap/build.metal:4-51 — the finest level of the importance map:
+// mean of 64 world-shader evaluations per texel (+1e-8), written both as a
+// pdf and into the quad-ordered mip level.
+extern "C" __global__ void rmd_envmap_build(const __grid_constant__ rmd::Context ctx, float *mipmap, float *pdfs,
+                                            int resolution) {
+    using namespace rmd;
+    const int tx = blockIdx.x * blockDim.x + threadIdx.x;
+    const int ty = blockIdx.y * blockDim.y + threadIdx.y;
+    if (tx >= resolution || ty >= resolution) return;
+    const int rayIndex = ty * resolution + tx;
+    float value = 0.0f;
+    const int numSamples = 64;
+    for (int sampleIndex = 0; sampleIndex < numSamples; sampleIndex++) {
+        PrngState prng = PrngState::tea((uint32_t)sampleIndex, (uint32_t)rayIndex);
+        const float2 projected = (make_float2((float)tx, (float)ty) + prng.sample2d()) /
+                                 make_float2((float)resolution, (float)resolution);
+        const float3 wo = warp::uniformSquareToSphere(projected);
+        ShadingContext sh;
+        sh.uv = sh.position = sh.generated = sh.object = sh.normal = sh.trueNormal = sh.tu = sh.tv = f3(0.0f);
+        sh.distance = 0.0f;
+        sh.rayFlags = 0;
+        sh.rnd = prng.sample3d();
+        sh.wo = -wo;
+        evaluateEnvironment(ctx, sh);
+        value += mean(sh.material.emission);
+    }
+    value /= (float)numSamples;
+    value += 1e-8f;
+    const unsigned qx = tx / 2, qy = ty / 2, qw = resolution / 2;
+    const unsigned outputIndex = resolution == 1 ? 0u : 4u * (qy * qw + qx) + (tx & 1) + 2u * (ty & 1);
+    mipmap[outputIndex] = value;
+    pdfs[rayIndex] = value;
+}
+
+// Test hook: shade records with one material and evaluate / sample its BSDF the
+// way handleIntersections does (intersection.metal:93-185).  Record layout:
+// position, normal, trueNormal, generated, uv, wo, wi, rnd (float3 each),
+// rayFlags, 3 pad; output: emission, eval value, eval pdf, sampled wi,
+// sampled weight, sampled pdf, sampled flags, alpha.
+extern "C" __global__ void rmd_material_eval(const __grid_constant__ rmd::Context ctx, unsigned material,
+                                             const float *records, float *out, int n) {
+    using namespace rmd;
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    const float *r = records + 28 * (size_t)i;
+    ShadingContext sh;
+    sh.position = make_float3(r[0], r[1], r[2]);
+    sh.normal = make_float3(r[3], r[4], r[5]);
+    sh.trueNormal = make_float3(r[6], r[7], r[8]);
+    sh.generated = make_float3(r[9], r[10], r[11]);
+    sh.uv = make_float3(r[12], r[13], r[14]);
+    sh.wo = make_float3(r[15], r[16], r[17]);
+    const float3 wi = make_float3(r[18], r[19], r[20]);
+    sh.rnd = make_float3(r[21], r[22], r[23]);
+    sh.rayFlags = (unsigned)r[24];
+    sh.object = sh.generated;
+    sh.tu = sh.tv = f3(0.0f);
+    sh.distance = 0.0f;
+    shadeSurface(material, ctx, sh);
+    float3 shNormal;
+    if (all_zero(sh.material.normal)) {
+        shNormal = sh.trueNormal;
+    } else {
+        float3 g = sh.trueNormal;
+        if (dot(g, sh.wo) < 0.0f) g *= -1.0f;
+        shNormal = ensure_valid_reflection(g, sh.wo, sh.material.normal);
+    }
+    float pdf;
+    const float3 f = sh.material.evaluate(sh.wo, wi, shNormal, sh.trueNormal, pdf);
+    const BsdfSample bs = sh.material.sample(sh.rnd, sh.wo, shNormal, sh.trueNormal, (uint8_t)sh.rayFlags);
+    float *o = out + 16 * (size_t)i;
+    o[0] = sh.material.emission.x; o[1] = sh.material.emission.y; o[2] = sh.material.emission.z;
+    o[3] = f.x; o[4] = f.y; o[5] = f.z; o[6] = pdf;
+    o[7] = bs.wi.x; o[8] = bs.wi.y; o[9] = bs.wi.z;
+    o[10] = bs.weight.x; o[11] = bs.weight.y; o[12] = bs.weight.z;
+    o[13] = bs.pdf; o[14] = (float)bs.flags; o[15] = sh.material.alpha;
+}

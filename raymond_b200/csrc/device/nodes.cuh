@@ -1,0 +1,622 @@
+// Cycles node library of the reference (raymond/device/nodes/nodes.hpp) for the
+// NVRTC material module: the same struct names, template parameters, field
+// names and `compute(ctx, shading)` contract, so that generated material code
+// has the shape MaterialBuilder.swift emits (`Kernel<params> n_x{}; n_x.field =
+// TYPE(...); n_x.compute(ctx, shading);`).
+#pragma once
+#include "noise.cuh"
+#include "scene.cuh"
+
+namespace rmd {
+
+RMD_HD float luminance(float3 c) { return dot(make_float3(0.2126f, 0.7152f, 0.0722f), c); }  // color.hpp:3-6
+
+// color.hpp:9-72
+RMD_HD float3 rgb2hsv(float3 rgb) {
+    const float cmax = fmaxf(rgb.x, fmaxf(rgb.y, rgb.z));
+    const float cmin = fminf(rgb.x, fminf(rgb.y, rgb.z));
+    const float cdelta = cmax - cmin;
+    float h = 0.0f, s = 0.0f, v = cmax;
+    if (cmax != 0.0f) s = cdelta / cmax;
+    if (s != 0.0f) {
+        const float3 c = (f3(cmax) - rgb) / cdelta;
+        if (rgb.x == cmax) h = 0.0f + c.z - c.y;
+        else if (rgb.y == cmax) h = 2.0f + c.x - c.z;
+        else h = 4.0f + c.y - c.x;
+        h /= 6.0f;
+        if (h < 0.0f) h += 1.0f;
+    }
+    return make_float3(h, s, v);
+}
+RMD_HD float3 hsv2rgb(float3 hsv) {
+    float h = hsv.x;
+    const float s = hsv.y, v = hsv.z;
+    if (s == 0.0f) return make_float3(v, v, v);
+    if (h == 1.0f) h = 0.0f;
+    h *= 6.0f;
+    const float i = floorf(h);
+    const float f = h - i;
+    const float p = v * (1.0f - s);
+    const float q = v * (1.0f - (s * f));
+    const float t = v * (1.0f - (s * (1.0f - f)));
+    switch ((int)i) {
+        case 0: return make_float3(v, t, p);
+        case 1: return make_float3(q, v, p);
+        case 2: return make_float3(p, v, t);
+        case 3: return make_float3(p, q, v);
+        case 4: return make_float3(t, p, v);
+        default: return make_float3(v, p, q);
+    }
+}
+
+// ---------------------------------------------------------------- coercions (nodes.hpp:2007-2031)
+RMD_HD float3 VECTOR(float v) { return f3(v); }
+RMD_HD float3 VECTOR(float2 v) { return f3(v, 0.0f); }
+RMD_HD float3 VECTOR(float3 v) { return v; }
+RMD_HD float3 VECTOR(float4 v) { return xyz(v); }
+RMD_HD float3 VECTOR(const UberShader &) { return f3(0.0f); }
+RMD_HD float4 RGBA(float v) { return make_float4(v, v, v, 1.0f); }
+RMD_HD float4 RGBA(float2 v) { return make_float4(v.x, v.y, 0.0f, 1.0f); }
+RMD_HD float4 RGBA(float3 v) { return f4(v, 1.0f); }
+RMD_HD float4 RGBA(float4 v) { return v; }
+RMD_HD float4 RGBA(const UberShader &v) { return f4(v.emission, 1.0f); }
+RMD_HD float VALUE(float v) { return v; }
+RMD_HD float VALUE(float3 v) { return (v.x + v.y + v.z) / 3.0f; }
+RMD_HD float VALUE(float4 v) { return v.w * (v.x + v.y + v.z) / 3.0f; }
+RMD_HD UberShader SHADER(const UberShader &v) { return v; }
+RMD_HD UberShader SHADER(float3 v) {
+    UberShader m;
+    m.emission = v;
+    return m;
+}
+RMD_HD UberShader SHADER(float v) { return SHADER(f3(v)); }
+RMD_HD UberShader SHADER(float2 v) { return SHADER(f3(v, 0.0f)); }
+RMD_HD UberShader SHADER(float4 v) { return SHADER(xyz(v)); }
+
+// ---------------------------------------------------------------- input nodes
+struct LightPath {  // nodes.hpp:15-43
+    bool isCameraRay, isReflectionRay, isTransmissionRay, isShadowRay, isDiffuseRay, isGlossyRay, isSingularRay;
+    float rayLength;
+    RMD_HD void compute(const Context &, const ShadingContext &sh) {
+        const uint32_t f = sh.rayFlags;
+        isCameraRay = (f & RayFlagsCamera) != 0;
+        isReflectionRay = (f & RayFlagsReflection) != 0;
+        isTransmissionRay = (f & RayFlagsTransmission) != 0;
+        isShadowRay = (f & RayFlagsShadow) != 0;
+        isDiffuseRay = (f & RayFlagsDiffuse) != 0;
+        isGlossyRay = (f & RayFlagsGlossy) != 0;
+        isSingularRay = (f & RayFlagsSingular) != 0;
+        rayLength = sh.distance;
+        if (isSingularRay) isGlossyRay = true;
+    }
+};
+struct NewGeometry {  // nodes.hpp:201-221
+    float3 normal, trueNormal, tangent, position, parametric, incoming, randomPerIsland;
+    bool backfacing;
+    RMD_HD void compute(const Context &, const ShadingContext &sh) {
+        normal = sh.normal;
+        trueNormal = sh.trueNormal;
+        tangent = sh.tu;
+        position = sh.position;
+        parametric = sh.uv;
+        incoming = sh.wo;
+        randomPerIsland = f3(0.0f);
+        backfacing = dot(sh.wo, sh.normal) < 0.0f;
+    }
+};
+struct TextureCoordinate {  // nodes.hpp:223-237
+    float3 generated, uv, object, normal, reflection;
+    RMD_HD void compute(const Context &, const ShadingContext &sh) {
+        uv = sh.uv;
+        generated = sh.generated;
+        object = sh.object;
+        normal = sh.normal;
+        reflection = sh.normal;
+    }
+};
+struct UVMapCoordinate {  // nodes.hpp:239-245
+    float3 uv;
+    RMD_HD void compute(const Context &, const ShadingContext &sh) { uv = sh.uv; }
+};
+struct Value {  // nodes.hpp:1716-1719
+    float value;
+    RMD_HD void compute(const Context &, const ShadingContext &) {}
+};
+struct RGB {  // nodes.hpp:1721-1724
+    float4 color;
+    RMD_HD void compute(const Context &, const ShadingContext &) {}
+};
+
+// ---------------------------------------------------------------- textures
+struct TexChecker {  // nodes.hpp:247-264
+    float scale;
+    float4 color1, color2;
+    float3 vector;
+    float fac;
+    float4 color;
+    RMD_HD void compute(const Context &, const ShadingContext &) {
+        float3 p = (vector * scale + 0.000001f) * 0.999999f;
+        const int ix = (int)floorf(p.x), iy = (int)floorf(p.y), iz = (int)floorf(p.z);
+        const bool which = ((ix ^ iy ^ iz) & 1) != 0;
+        color = which ? color1 : color2;
+        fac = which ? 1.0f : 0.0f;
+    }
+};
+
+struct kTexNoise {
+    enum Dimension { DIMENSION_1D, DIMENSION_2D, DIMENSION_3D, DIMENSION_4D };
+};
+template <int Dimension>
+struct TexNoise {  // nodes.hpp:872-1011
+    float detail, distortion, roughness, scale, w;
+    float3 vector;
+    float fac;
+    float4 color;
+
+    RMD_HD static float off1(float seed) { return 100.0f + noise::hash_float_to_float(seed) * 100.0f; }
+    RMD_HD static float off2(float seed, float k) {
+        return 100.0f + noise::hash_float2_to_float(make_float2(seed, k)) * 100.0f;
+    }
+    RMD_HD static float2 off2v(float s) { return make_float2(off2(s, 0.0f), off2(s, 1.0f)); }
+    RMD_HD static float3 off3v(float s) { return make_float3(off2(s, 0.0f), off2(s, 1.0f), off2(s, 2.0f)); }
+    RMD_HD static float4 off4v(float s) {
+        return make_float4(off2(s, 0.0f), off2(s, 1.0f), off2(s, 2.0f), off2(s, 3.0f));
+    }
+    RMD_HD void compute(const Context &, const ShadingContext &) {
+        const float3 p3 = this->vector * scale;
+        const float ww = this->w * scale;
+        if (Dimension == kTexNoise::DIMENSION_1D) {
+            float p = ww;
+            if (distortion != 0.0f) p += noise::snoise(p + off1(0.0f)) * distortion;
+            color = make_float4(noise::fractal_noise(p, detail, roughness),
+                                noise::fractal_noise(p + off1(1.0f), detail, roughness),
+                                noise::fractal_noise(p + off1(2.0f), detail, roughness), 1.0f);
+        } else if (Dimension == kTexNoise::DIMENSION_2D) {
+            float2 p = make_float2(p3.x, p3.y);
+            if (distortion != 0.0f)
+                p = p + distortion * make_float2(noise::snoise(p + off2v(0.0f)), noise::snoise(p + off2v(1.0f)));
+            color = make_float4(noise::fractal_noise(p, detail, roughness),
+                                noise::fractal_noise(p + off2v(2.0f), detail, roughness),
+                                noise::fractal_noise(p + off2v(3.0f), detail, roughness), 1.0f);
+        } else if (Dimension == kTexNoise::DIMENSION_3D) {
+            float3 p = p3;
+            if (distortion != 0.0f)
+                p += distortion * make_float3(noise::snoise(p + off3v(0.0f)), noise::snoise(p + off3v(1.0f)),
+                                              noise::snoise(p + off3v(2.0f)));
+            color = make_float4(noise::fractal_noise(p, detail, roughness),
+                                noise::fractal_noise(p + off3v(3.0f), detail, roughness),
+                                noise::fractal_noise(p + off3v(4.0f), detail, roughness), 1.0f);
+        } else {
+            float4 p = f4(p3, ww);
+            if (distortion != 0.0f)
+                p = p + distortion * make_float4(noise::snoise(p + off4v(0.0f)), noise::snoise(p + off4v(1.0f)),
+                                                 noise::snoise(p + off4v(2.0f)), noise::snoise(p + off4v(3.0f)));
+            color = make_float4(noise::fractal_noise(p, detail, roughness),
+                                noise::fractal_noise(p + off4v(4.0f), detail, roughness),
+                                noise::fractal_noise(p + off4v(5.0f), detail, roughness), 1.0f);
+        }
+        fac = color.x;
+    }
+};
+
+struct ColorRampElement {
+    float position;
+    float4 color;
+};
+template <int NumElements>
+struct ColorRamp {  // nodes.hpp:1013-1046
+    float fac;
+    float4 color;
+    ColorRampElement elements[NumElements];
+    RMD_HD void compute(const Context &, const ShadingContext &) {
+        if (fac < elements[0].position) {
+            color = elements[0].color;
+            return;
+        }
+        if (fac > elements[NumElements - 1].position) {
+            color = elements[NumElements - 1].color;
+            return;
+        }
+        for (int i = 1; i < NumElements; ++i) {
+            if (elements[i].position >= fac) {
+                const ColorRampElement a = elements[i - 1], b = elements[i];
+                float v = (fac - a.position) / (b.position - a.position);
+                color = (1.0f - v) * a.color + v * b.color;
+                return;
+            }
+        }
+    }
+};
+
+// ---------------------------------------------------------------- converters
+struct kColorMix {
+    enum BlendType {
+        BLEND_TYPE_MIX, BLEND_TYPE_ADD, BLEND_TYPE_MULTIPLY, BLEND_TYPE_SCREEN, BLEND_TYPE_OVERLAY,
+        BLEND_TYPE_SUB, BLEND_TYPE_COLOR, BLEND_TYPE_LIGHTEN, BLEND_TYPE_DARKEN, BLEND_TYPE_VALUE
+    };
+};
+template <int BlendType, bool Clamp>
+struct ColorMix {  // nodes.hpp:1319-1385
+    float4 color1, color2;
+    float fac;
+    float4 color;
+    RMD_HD void compute(const Context &, const ShadingContext &) {
+        switch (BlendType) {
+            case kColorMix::BLEND_TYPE_MIX: color = lerp(color1, color2, fac); break;
+            case kColorMix::BLEND_TYPE_ADD: color = color1 + fac * color2; break;
+            case kColorMix::BLEND_TYPE_SUB: color = color1 - fac * color2; break;
+            case kColorMix::BLEND_TYPE_MULTIPLY: color = color1 * lerp(f4(1.0f), color2, fac); break;
+            case kColorMix::BLEND_TYPE_SCREEN: color = f4(1.0f) - (f4(1.0f) - fac * color1) * (f4(1.0f) - color1); break;
+            case kColorMix::BLEND_TYPE_OVERLAY: {
+                color = color1;
+                float *c = &color.x;
+                const float *c2 = &color2.x;
+                for (int d = 0; d < 3; d++) {
+                    if (c[d] < 0.5f) c[d] *= 1.0f - fac + 2.0f * fac * c2[d];
+                    else c[d] = 1.0f - (1.0f - fac + 2.0f * fac * (1.0f - c2[d])) * (1.0f - c[d]);
+                }
+                break;
+            }
+            case kColorMix::BLEND_TYPE_COLOR: {
+                color = color1;
+                const float3 hsv2 = rgb2hsv(xyz(color2));
+                if (hsv2.y == 0.0f) {
+                    color = color1;
+                } else {
+                    float3 hsv = rgb2hsv(xyz(color1));
+                    hsv.x = hsv2.x;
+                    hsv.y = hsv2.y;
+                    color = lerp(color1, f4(hsv2rgb(hsv), color2.w), fac);
+                }
+                break;
+            }
+            case kColorMix::BLEND_TYPE_LIGHTEN: color = lerp(color1, vmax(color1, color2), fac); break;
+            case kColorMix::BLEND_TYPE_DARKEN: color = lerp(color1, vmin(color1, color2), fac); break;
+            case kColorMix::BLEND_TYPE_VALUE: {
+                float3 hsv = rgb2hsv(xyz(color1));
+                hsv.z = rgb2hsv(xyz(color2)).z;
+                color = lerp(color1, f4(hsv2rgb(hsv), color2.w), fac);
+                break;
+            }
+        }
+        if (Clamp) color = saturate(color);
+    }
+};
+struct kMix {
+    enum FactorMode { FACTOR_MODE_UNIFORM, FACTOR_MODE_NON_UNIFORM };
+};
+template <bool ClampFactor, bool ClampResult, int FactorMode>
+struct Mix {  // nodes.hpp:1940-1974
+    float4 a_Color, b_Color, result_Color;
+    float a_Float, b_Float, result_Float;
+    float3 a_Vector, b_Vector, result_Vector;
+    float factor_Float;
+    float3 factor_Vector;
+    RMD_HD void compute(const Context &, const ShadingContext &) {
+        if (ClampFactor) {
+            factor_Float = saturate(factor_Float);
+            factor_Vector = saturate(factor_Vector);
+        }
+        if (FactorMode == kMix::FACTOR_MODE_UNIFORM) result_Vector = lerp(a_Vector, b_Vector, factor_Float);
+        else result_Vector = a_Vector + (b_Vector - a_Vector) * factor_Vector;
+        result_Float = lerp(a_Float, b_Float, factor_Float);
+        result_Color = lerp(a_Color, b_Color, factor_Float);
+        if (ClampResult) result_Color = saturate(result_Color);
+    }
+};
+struct kMath {
+    enum Operation {
+        OPERATION_ADD, OPERATION_SUBTRACT, OPERATION_MULTIPLY, OPERATION_DIVIDE, OPERATION_MULTIPLY_ADD,
+        OPERATION_POWER, OPERATION_MINIMUM, OPERATION_MAXIMUM, OPERATION_TANGENT, OPERATION_LESS_THAN,
+        OPERATION_GREATER_THAN, OPERATION_MODULO
+    };
+};
+template <int Operation, bool Clamp>
+struct Math {  // nodes.hpp:1145-1193
+    float value, value_001, value_002;
+    RMD_HD void compute(const Context &, const ShadingContext &) {
+        switch (Operation) {
+            case kMath::OPERATION_ADD: value = value + value_001; break;
+            case kMath::OPERATION_SUBTRACT: value = value - value_001; break;
+            case kMath::OPERATION_MULTIPLY: value = value * value_001; break;
+            case kMath::OPERATION_DIVIDE: value = value_001 == 0.0f ? 0.0f : value / value_001; break;
+            case kMath::OPERATION_MULTIPLY_ADD: value = value * value_001 + value_002; break;
+            case kMath::OPERATION_POWER: value = powf(value, value_001); break;
+            case kMath::OPERATION_MINIMUM: value = fminf(value, value_001); break;
+            case kMath::OPERATION_MAXIMUM: value = fmaxf(value, value_001); break;
+            case kMath::OPERATION_TANGENT: value = tanf(value); break;
+            case kMath::OPERATION_LESS_THAN: value = value < value_001 ? 1.0f : 0.0f; break;
+            case kMath::OPERATION_GREATER_THAN: value = value > value_001 ? 1.0f : 0.0f; break;
+            case kMath::OPERATION_MODULO: value = fmodf(value, value_001); break;
+        }
+        if (Clamp) value = saturate(value);
+    }
+};
+struct kVectorMath {
+    enum Operation {
+        OPERATION_ADD, OPERATION_SUBTRACT, OPERATION_MULTIPLY, OPERATION_MULTIPLY_ADD, OPERATION_NORMALIZE,
+        OPERATION_SCALE, OPERATION_MINIMUM, OPERATION_LENGTH, OPERATION_DOT_PRODUCT
+    };
+};
+template <int Operation>
+struct VectorMath {  // nodes.hpp:165-199
+    float scale, value;
+    float3 vector, vector_001, vector_002;
+    RMD_HD void compute(const Context &, const ShadingContext &) {
+        switch (Operation) {
+            case kVectorMath::OPERATION_ADD: vector = vector + vector_001; break;
+            case kVectorMath::OPERATION_SUBTRACT: vector = vector - vector_001; break;
+            case kVectorMath::OPERATION_MULTIPLY: vector = vector * vector_001; break;
+            case kVectorMath::OPERATION_MULTIPLY_ADD: vector = vector * vector_001 + vector_002; break;
+            case kVectorMath::OPERATION_NORMALIZE: vector = normalize(vector); break;
+            case kVectorMath::OPERATION_SCALE: vector = vector * scale; break;
+            case kVectorMath::OPERATION_MINIMUM: vector = vmin(vector, vector_001); break;
+            case kVectorMath::OPERATION_LENGTH: value = length(vector); break;
+            case kVectorMath::OPERATION_DOT_PRODUCT: vector = f3(dot(vector, vector_001)); break;
+        }
+    }
+};
+struct SeparateVector {  // nodes.hpp:266-275
+    float3 vector;
+    float x, y, z;
+    RMD_HD void compute(const Context &, const ShadingContext &) {
+        x = vector.x;
+        y = vector.y;
+        z = vector.z;
+    }
+};
+struct CombineVector {  // nodes.hpp:277-284
+    float x, y, z;
+    float3 vector;
+    RMD_HD void compute(const Context &, const ShadingContext &) { vector = make_float3(x, y, z); }
+};
+struct kMapRange {
+    enum DataType { DATA_TYPE_FLOAT };
+    enum InterpolationType { INTERPOLATION_TYPE_LINEAR };
+};
+template <bool Clamp, int DataType, int InterpolationType>
+struct MapRange {  // nodes.hpp:314-344
+    float fromMin, fromMax, toMin, toMax, steps;
+    float3 steps_Float3, from_Min_Float3, from_Max_Float3, to_Min_Float3, to_Max_Float3;
+    float value;
+    float3 vector;
+    float result;
+    RMD_HD void compute(const Context &, const ShadingContext &) {
+        float v = (value - fromMin) / (fromMax - fromMin);
+        if (Clamp) v = saturate(v);
+        result = lerp(toMin, toMax, v);
+    }
+};
+struct RGBToBW {  // nodes.hpp:1726-1734
+    float4 color;
+    float val;
+    RMD_HD void compute(const Context &, const ShadingContext &) { val = luminance(xyz(color)); }
+};
+struct ColorInvert {  // nodes.hpp:1387-1394
+    float4 color;
+    float fac;
+    RMD_HD void compute(const Context &, const ShadingContext &) {
+        const float3 c = xyz(color) - fac * (2.0f * xyz(color) - f3(1.0f));
+        color = f4(c, color.w);
+    }
+};
+struct Gamma {  // nodes.hpp:1292-1302
+    float4 color;
+    float gamma;
+    RMD_HD void compute(const Context &, const ShadingContext &) {
+        if (gamma == 0.0f) {
+            color.x = color.y = color.z = 1.0f;
+        } else {
+            if (color.x > 0.0f) color.x = powf(color.x, gamma);
+            if (color.y > 0.0f) color.y = powf(color.y, gamma);
+            if (color.z > 0.0f) color.z = powf(color.z, gamma);
+        }
+    }
+};
+struct Fresnel {  // nodes.hpp:1112-1126
+    float ior;
+    float3 normal;
+    float fac;
+    RMD_HD void compute(const Context &, const ShadingContext &sh) {
+        const float cosI = dot(sh.wo, normal);
+        const bool backfacing = cosI < 0.0f;
+        float eta = fmaxf(ior, 1e-5f);
+        eta = backfacing ? 1.0f / eta : eta;
+        fac = fresnelDielectricCos(cosI, eta);
+    }
+};
+struct LayerWeight {  // nodes.hpp:1689-1714
+    float blend;
+    float3 normal;
+    float fresnel, facing;
+    RMD_HD void compute(const Context &, const ShadingContext &sh) {
+        const bool backfacing = dot(sh.wo, normal) < 0.0f;
+        const float cosI = dot(sh.wo, normal);
+        float eta = fmaxf(1.0f - blend, 1e-5f);
+        eta = backfacing ? eta : 1.0f / eta;
+        fresnel = fresnelDielectricCos(cosI, eta);
+        facing = fabsf(cosI);
+        if (blend != 0.5f) {
+            float b = clampf(blend, 0.0f, 1.0f - 1e-5f);
+            b = (b < 0.5f) ? 2.0f * b : 0.5f / (1.0f - b);
+            facing = powf(facing, b);
+        }
+        facing = 1.0f - facing;
+    }
+};
+
+// ---------------------------------------------------------------- shaders
+struct Emission {  // nodes.hpp:1396-1407
+    float4 color;
+    float strength, weight;
+    UberShader emission;
+    RMD_HD void compute(const Context &, const ShadingContext &) {
+        emission.lobeProbabilities[0] = 1.0f;
+        emission.emission = xyz(color) * strength;
+    }
+};
+struct Background {  // nodes.hpp:1409-1419
+    float4 color;
+    float strength, weight;
+    UberShader background;
+    RMD_HD void compute(const Context &, const ShadingContext &) { background.emission = xyz(color) * strength; }
+};
+struct kBsdfPrincipled {
+    enum Distribution { DISTRIBUTION_GGX };
+    enum SubsurfaceMethod { SUBSURFACE_METHOD_BURLEY, SUBSURFACE_METHOD_RANDOM_WALK, SUBSURFACE_METHOD_RANDOM_WALK_FIXED_RADIUS };
+};
+template <int Distribution, int SubsurfaceMethod>
+struct BsdfPrincipled {  // nodes.hpp:1581-1687
+    float weight;
+    float4 emission;
+    float sheenTint, emissionStrength, transmission;
+    float3 clearcoatNormal;
+    float alpha, specularTint;
+    float3 tangent;
+    float roughness, subsurfaceIor, anisotropic, sheen;
+    float3 subsurfaceRadius, normal;
+    float subsurfaceAnisotropy;
+    float4 baseColor;
+    float transmissionRoughness, metallic, specular, clearcoatRoughness;
+    float4 subsurfaceColor;
+    float subsurface, ior, anisotropicRotation, clearcoat;
+    UberShader bsdf;
+
+    RMD_HD void compute(const Context &, const ShadingContext &) {
+        clearcoatRoughness = fmaxf(clearcoatRoughness, 1e-4f);
+        roughness = fmaxf(roughness, 1e-4f);
+        const float diffuseWeight = (1.0f - saturate(transmission)) * (1.0f - saturate(metallic));
+        const float transmissionWeight = saturate(transmission) * (1.0f - saturate(metallic));
+        const float specularWeight = 1.0f - transmissionWeight;
+        const float3 base = xyz(baseColor);
+        const float lum = luminance(base);
+        const float3 tintColor = lum > 0.0f ? base * (1.0f / lum) : f3(1.0f);
+        const float3 sheenColor = lerp(f3(1.0f), tintColor, sheenTint);
+        const float3 specularColor = lerp(f3(1.0f), tintColor, specularTint);
+        const float3 Cspec0 = lerp(specular * 0.08f * specularColor, base, metallic);
+        const float aspect = sqrtf(1.0f - 0.9f * anisotropic);
+        const float r2 = square(roughness);
+        bsdf.diffuse = Diffuse{diffuseWeight * base, diffuseWeight * sheen * sheenColor, roughness, false};
+        bsdf.specular = Specular{r2 / aspect, r2 * aspect, Cspec0, (2.0f / (1.0f - sqrtf(0.08f * specular))) - 1.0f,
+                                 specularWeight};
+        bsdf.transmission = Transmission{r2,
+                                         square(1.0f - (1.0f - roughness) * (1.0f - transmissionRoughness)),
+                                         base,
+                                         lerp(f3(1.0f), base, specularTint),
+                                         ior,
+                                         transmissionWeight,
+                                         false};
+        bsdf.clearcoat = Clearcoat{square(clearcoatRoughness), clearcoat};
+        bsdf.lobeProbabilities[0] = diffuseWeight;
+        bsdf.lobeProbabilities[1] = specularWeight;
+        bsdf.lobeProbabilities[2] = transmissionWeight;
+        bsdf.lobeProbabilities[3] = clearcoat * 0.25f;
+        float weightsSum = 0.0f;
+        for (int i = 0; i < 4; i++) weightsSum += bsdf.lobeProbabilities[i];
+        for (int i = 0; i < 4; i++) bsdf.lobeProbabilities[i] /= weightsSum;
+        bsdf.alpha = alpha;
+        bsdf.normal = normal;
+        bsdf.emission = alpha * xyz(emission) * emissionStrength;
+    }
+};
+struct BsdfDiffuse {  // nodes.hpp:1809-1827
+    float4 color;
+    float3 normal;
+    float roughness, weight;
+    UberShader bsdf;
+    RMD_HD void compute(const Context &, const ShadingContext &) {
+        bsdf.diffuse = Diffuse{xyz(color), f3(0.0f), roughness, false};
+        bsdf.normal = normal;
+        bsdf.lobeProbabilities[0] = 1.0f;
+    }
+};
+struct kBsdfGlossy {
+    enum Distribution { DISTRIBUTION_GGX };
+};
+template <int Distribution>
+struct BsdfGlossy {  // nodes.hpp:1534-1567
+    float4 color;
+    float3 normal;
+    float roughness, weight;
+    UberShader bsdf;
+    RMD_HD void compute(const Context &, const ShadingContext &) {
+        const float a = square(fmaxf(roughness, 1e-4f));
+        bsdf.specular = Specular{a, a, xyz(color), 1.45f, 1.0f};
+        bsdf.lobeProbabilities[1] = 1.0f;
+        bsdf.normal = normal;
+    }
+};
+struct kBsdfGlass {
+    enum Distribution { DISTRIBUTION_GGX };
+};
+template <int Distribution>
+struct BsdfGlass {  // nodes.hpp:1497-1532
+    float4 color;
+    float ior;
+    float3 normal;
+    float roughness, weight;
+    UberShader bsdf;
+    RMD_HD void compute(const Context &, const ShadingContext &) {
+        const float a = square(fmaxf(roughness, 1e-4f));
+        bsdf.transmission = Transmission{a, a, xyz(color), xyz(color), ior, 1.0f, false};
+        bsdf.lobeProbabilities[2] = 1.0f;
+        bsdf.normal = normal;
+    }
+};
+struct BsdfTransparent {  // nodes.hpp:1797-1807
+    float4 color;
+    float weight;
+    UberShader bsdf;
+    RMD_HD void compute(const Context &, const ShadingContext &) {
+        bsdf.alpha = 0.0f;
+        bsdf.alphaWeight = xyz(color);
+    }
+};
+struct AddShader {  // nodes.hpp:1895-1911
+    UberShader shader, shader_001;
+    RMD_HD void compute(const Context &, ShadingContext &sh) {
+        const float3 em = shader_001.emission + shader.emission;
+        if (sh.rnd.x < 0.5f) {
+            sh.rnd.x /= 0.5f;
+            shader = shader_001;
+        } else {
+            sh.rnd.x = 2.0f * (sh.rnd.x - 0.5f);
+        }
+        shader.emission = em;
+        shader.weight *= 2.0f;
+    }
+};
+struct MixShader {  // nodes.hpp:1916-1931
+    float fac;
+    UberShader shader, shader_001;
+    RMD_HD void compute(const Context &, ShadingContext &sh) {
+        const float3 em = fac * shader_001.emission + (1.0f - fac) * shader.emission;
+        if (sh.rnd.x < fac) {
+            sh.rnd.x /= fac;
+            shader = shader_001;
+        } else {
+            sh.rnd.x = (sh.rnd.x - fac) / (1.0f - fac);
+        }
+        shader.emission = em;
+    }
+};
+struct OutputMaterial {  // nodes.hpp:1976-1986
+    float3 displacement;
+    float thickness;
+    UberShader surface, volume;
+    RMD_HD void compute(const Context &, ShadingContext &sh) { sh.material = surface; }
+};
+struct OutputWorld {  // nodes.hpp:1988-1995
+    float thickness;
+    UberShader surface;
+    RMD_HD void compute(const Context &, ShadingContext &sh) { sh.material = surface; }
+};
+struct OutputLight {  // nodes.hpp:1997-2005
+    UberShader surface;
+    RMD_HD void compute(const Context &, ShadingContext &sh) {
+        sh.material.alpha = 0.0f;
+        sh.material.emission = surface.emission;
+    }
+};
+
+}  // namespace rmd

@@ -1,0 +1,132 @@
+// Path pool, queues and counters of the persistent wavefront, shared by the
+// static kernels (film / regeneration, traversal) and the NVRTC shading
+// module.  Paths live in fixed slots (structure of arrays, 16-byte fields);
+// queues hold slot indices.  One iteration is
+//     film+regen -> closest-hit trace -> shade (NEE, BSDF sample) -> shadow trace
+// and replaces one depth step of Renderer.execute (Renderer.swift:545-673)
+// for every path in flight; finished paths are replaced by new camera
+// samples, so the pool stays full until the last samples drain.
+#pragma once
+#include "scene.cuh"
+
+namespace rmd {
+
+constexpr uint32_t INVALID_PIXEL = 0xffffffffu;
+constexpr float SHADOW_EPS = 0.001f;  // device/constants.hpp:3
+
+// error flags
+constexpr uint32_t ERR_QUEUE_OVERFLOW = 1u;
+constexpr uint32_t ERR_STACK_OVERFLOW = 2u;
+
+struct Counters {
+    uint32_t nQ[2];       // active-path queue sizes (ping-pong)
+    uint32_t nDone;       // finished / free slots waiting for the film kernel
+    uint32_t nShadow;     // shadow rays of this iteration
+    uint32_t traceWork;   // persistent closest-hit work counter
+    uint32_t shadowWork;  // persistent any-hit work counter
+    uint32_t errors;
+    uint32_t pad;
+    unsigned long long nextPath;    // next path id handed out by the film kernel
+    unsigned long long endPath;     // one past the last path id of this render
+    unsigned long long pathsDone;   // paths whose radiance reached the film
+    unsigned long long segments;    // closest-hit rays shaded
+    unsigned long long shadowRays;  // shadow rays traced
+    unsigned long long pad2;
+};
+
+struct PathPool {
+    float4 *rayO;      // origin.xyz, tmin
+    float4 *rayD;      // direction.xyz, tmax
+    float4 *tp;        // throughput.xyz, bsdfPdf
+    float4 *L;         // radiance gathered so far
+    uint2 *rng;        // PrngState
+    uint32_t *pixel;   // y * width + x, or INVALID_PIXEL
+    uint32_t *sample;  // sample index of the path
+    uint32_t *meta;    // depth (bits 0-15) | ray flags (bits 16-23)
+    float4 *hit;       // t (<= 0: miss), b0, b1, primitive (bits)
+    uint32_t *hitInst; // instance index
+    uint32_t *q[2];    // active queues
+    uint32_t *qDone;   // finished slots
+    float4 *shO;       // shadow: origin.xyz, tmax
+    float4 *shD;       // shadow: direction.xyz, slot (bits)
+    float4 *shW;       // shadow: weight.xyz
+    uint32_t capacity;
+};
+
+struct FrameParams {
+    uint32_t width, height, numPixels;
+    uint32_t maxDepth, samplingMode, rngMode;
+    uint64_t seed;
+    int filmFp64;
+    float4 *film;      // rgb sums (w unused)
+    double *film64;    // rgb sums, 3 per pixel
+};
+
+// kernel parameters of the shading megakernel (device/integrator.cuh)
+struct ShadeParams {
+    Context ctx;
+    PathPool pool;
+    FrameParams fp;
+    Counters *counters;
+    uint32_t cur;
+};
+
+// Appends the calling lane to a queue with one atomic per warp
+// (ballot / popc / shfl), returning its position.
+__device__ __forceinline__ uint32_t warpAppend(uint32_t *counter) {
+    const unsigned mask = __activemask();
+    const int leader = __ffs(mask) - 1;
+    const int lane = threadIdx.x & 31;
+    uint32_t base = 0;
+    if (lane == leader) base = atomicAdd(counter, (uint32_t)__popc(mask));
+    base = __shfl_sync(mask, base, leader);
+    return base + (uint32_t)__popc(mask & ((1u << lane) - 1u));
+}
+__device__ __forceinline__ void warpAdd64(unsigned long long *counter, uint32_t v) {
+    const unsigned mask = __activemask();
+    const int leader = __ffs(mask) - 1;
+    const uint32_t total = __reduce_add_sync(mask, v);
+    if ((int)(threadIdx.x & 31) == leader && total) atomicAdd(counter, (unsigned long long)total);
+}
+
+// generate.metal:88-91 with 8x8 threadgroups: block-linear ray index and its inverse
+RMD_HD uint32_t blockLinearIndex(uint32_t x, uint32_t y, uint32_t W, uint32_t H) {
+    const uint32_t gx = x / 8, gy = y / 8, tx = x % 8, ty = y % 8;
+    const uint32_t awx = min(8u, W - gx * 8), awy = min(8u, H - gy * 8);
+    return tx + ty * awx + gx * 8 * awy + gy * 8 * W;
+}
+RMD_HD void blockLinearToPixel(uint32_t r, uint32_t W, uint32_t H, uint32_t &x, uint32_t &y) {
+    const uint32_t gy = r / (8 * W);
+    uint32_t rr = r - gy * 8 * W;
+    const uint32_t awy = min(8u, H - gy * 8);
+    const uint32_t gx = rr / (8 * awy);
+    rr -= gx * 8 * awy;
+    const uint32_t awx = min(8u, W - gx * 8);
+    const uint32_t ty = rr / awx, tx = rr - ty * awx;
+    x = gx * 8 + tx;
+    y = gy * 8 + ty;
+}
+
+RMD_HD uint64_t pathSequence(uint32_t sample, uint32_t pixel, uint32_t numPixels) {
+    return (uint64_t)sample * (uint64_t)numPixels + (uint64_t)pixel;
+}
+
+// generate.metal:72-121 (pinhole branch): a camera ray for (x, y, sample)
+RMD_HD void cameraRay(const Context &ctx, const FrameParams &fp, uint32_t x, uint32_t y, uint32_t sample,
+                      PrngState &prng, float3 &org, float3 &dir) {
+    const uint32_t W = fp.width, H = fp.height;
+    if (fp.rngMode == RNG_TEA) {
+        prng = PrngState::tea(sample + 1u, blockLinearIndex(x, y, W, H));
+    } else {
+        prng = PrngState::pcg(fp.seed, pathSequence(sample, y * W + x, fp.numPixels));
+    }
+    const float2 jittered = make_float2((float)x, (float)y) + prng.sample2d();
+    const float2 uv = make_float2(1.0f, -1.0f) * ((jittered / make_float2((float)W, (float)H) + ctx.shift) * 2.0f - 1.0f);
+    const float aspect = (float)H / (float)W;
+    org = xyz(ctx.cameraTransform[3]);  // (T * float4(0, 0, 0, 1)).xyz
+    const float4 dd = ctx.cameraTransform[0] * uv.x + ctx.cameraTransform[1] * (uv.y * aspect) +
+                      ctx.cameraTransform[2] * (-ctx.focalLength) + ctx.cameraTransform[3] * 0.0f;
+    dir = normalize(xyz(dd));
+}
+
+}  // namespace rmd

@@ -1,0 +1,284 @@
+// Static sm_100a kernels of the wavefront: closest-hit and shadow traversal,
+// film accumulation + path regeneration, frame set-up, the environment-map
+// pyramid reductions, film read-out, and small test hooks.  The shading
+// megakernel lives in the NVRTC module (device/integrator.cuh).
+#include <cuda_runtime.h>
+
+#include "device/traverse.cuh"
+#include "device/wavefront.cuh"
+#include "kernels.h"
+
+namespace rmd {
+
+// ------------------------------------------------------------- frame set-up
+// Every slot starts on the done queue with no pixel, so the first film pass
+// hands each one a camera sample.
+__global__ void k_frame_init(PathPool pool, Counters *cnt, uint64_t firstPath, uint64_t endPath) {
+    const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i == 0) {
+        cnt->nQ[0] = cnt->nQ[1] = 0;
+        cnt->nDone = pool.capacity;
+        cnt->nShadow = 0;
+        cnt->traceWork = cnt->shadowWork = 0;
+        cnt->errors = 0;
+        cnt->nextPath = firstPath;
+        cnt->endPath = endPath;
+        cnt->pathsDone = 0;
+        cnt->segments = 0;
+        cnt->shadowRays = 0;
+    }
+    if (i < pool.capacity) {
+        pool.qDone[i] = i;
+        pool.pixel[i] = INVALID_PIXEL;
+    }
+}
+
+// ------------------------------------------------------------- film + regeneration
+// Adds the radiance of every finished path to the film (the film writes of
+// intersection.metal:84-87,111-116,174-178 and shadow.metal:24-27, gathered
+// per path) and replaces the path with the next camera sample
+// (generate.metal:72-121) while samples remain.
+__global__ void __launch_bounds__(256) k_film_regen(Context ctx, PathPool pool, FrameParams fp, Counters *cnt,
+                                                    uint32_t cur) {
+    if (blockIdx.x == 0 && threadIdx.x == 0) cnt->traceWork = 0;
+    const uint32_t n = cnt->nDone;
+    for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+        const uint32_t slot = pool.qDone[i];
+        const uint32_t px = pool.pixel[slot];
+        if (px != INVALID_PIXEL) {
+            const float4 L = pool.L[slot];
+            if (fp.filmFp64) {
+                atomicAdd(&fp.film64[3 * (size_t)px + 0], (double)L.x);
+                atomicAdd(&fp.film64[3 * (size_t)px + 1], (double)L.y);
+                atomicAdd(&fp.film64[3 * (size_t)px + 2], (double)L.z);
+            } else {
+                atomicAdd(&fp.film[px], make_float4(L.x, L.y, L.z, 1.0f));
+            }
+            warpAdd64(&cnt->pathsDone, 1u);
+        }
+        // one 64-bit atomic per warp for the new path ids
+        const unsigned mask = __activemask();
+        const int leader = __ffs(mask) - 1;
+        const int lane = threadIdx.x & 31;
+        unsigned long long base = 0;
+        if (lane == leader) base = atomicAdd(&cnt->nextPath, (unsigned long long)__popc(mask));
+        base = __shfl_sync(mask, base, leader);
+        const uint64_t id = base + (uint64_t)__popc(mask & ((1u << lane) - 1u));
+        if (id < cnt->endPath) {
+            const uint32_t sample = (uint32_t)(id / fp.numPixels);
+            const uint32_t r = (uint32_t)(id - (uint64_t)sample * fp.numPixels);
+            uint32_t x, y;
+            blockLinearToPixel(r, fp.width, fp.height, x, y);
+            PrngState prng;
+            float3 org, dir;
+            cameraRay(ctx, fp, x, y, sample, prng, org, dir);
+            pool.rayO[slot] = f4(org, ctx.nearClip);
+            pool.rayD[slot] = f4(dir, ctx.farClip);
+            pool.tp[slot] = make_float4(1.0f, 1.0f, 1.0f, inf_f());
+            pool.L[slot] = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
+            pool.rng[slot] = prng.pack();
+            pool.pixel[slot] = y * fp.width + x;
+            pool.sample[slot] = sample;
+            pool.meta[slot] = (uint32_t)RayFlagsCamera << 16;
+            const uint32_t k = warpAppend(&cnt->nQ[cur]);
+            if (k < pool.capacity) pool.q[cur][k] = slot;
+            else atomicOr(&cnt->errors, ERR_QUEUE_OVERFLOW);
+        } else {
+            pool.pixel[slot] = INVALID_PIXEL;
+        }
+    }
+}
+
+// ------------------------------------------------------------- traversal
+// Persistent warps pull 32 queue entries at a time (Aila & Laine 2009).
+__global__ void __launch_bounds__(128) k_trace_closest(const BvhNode *__restrict__ nodes,
+                                                       const float4 *__restrict__ tris, PathPool pool,
+                                                       Counters *cnt, uint32_t cur) {
+    if (blockIdx.x == 0 && threadIdx.x == 0) {
+        cnt->nQ[cur ^ 1u] = 0;
+        cnt->nDone = 0;
+        cnt->nShadow = 0;
+        cnt->shadowWork = 0;
+    }
+    const uint32_t n = cnt->nQ[cur];
+    const uint32_t *q = pool.q[cur];
+    const int lane = threadIdx.x & 31;
+    while (true) {
+        uint32_t base = 0;
+        if (lane == 0) base = atomicAdd(&cnt->traceWork, 32u);
+        base = __shfl_sync(0xffffffffu, base, 0);
+        if (base >= n) break;
+        const uint32_t i = base + lane;
+        if (i < n) {
+            const uint32_t slot = q[i];
+            const float4 o = pool.rayO[slot];
+            const float4 d = pool.rayD[slot];
+            float4 hit;
+            uint32_t inst;
+            traceClosest(nodes, tris, xyz(o), xyz(d), o.w, d.w, hit, inst, &cnt->errors);
+            pool.hit[slot] = hit;
+            pool.hitInst[slot] = inst;
+        }
+    }
+}
+
+// raytraceAny fused with handleShadowRays (shadow.metal:6-29): an unoccluded
+// shadow ray adds its weight to its path's radiance.
+__global__ void __launch_bounds__(128) k_trace_shadow(const BvhNode *__restrict__ nodes,
+                                                      const float4 *__restrict__ tris, PathPool pool,
+                                                      Counters *cnt) {
+    const uint32_t n = cnt->nShadow;
+    const int lane = threadIdx.x & 31;
+    while (true) {
+        uint32_t base = 0;
+        if (lane == 0) base = atomicAdd(&cnt->shadowWork, 32u);
+        base = __shfl_sync(0xffffffffu, base, 0);
+        if (base >= n) break;
+        const uint32_t i = base + lane;
+        if (i < n) {
+            const float4 o = pool.shO[i];
+            const float4 d = pool.shD[i];
+            const bool occluded = traceAny(nodes, tris, xyz(o), xyz(d), SHADOW_EPS, o.w, &cnt->errors);
+            if (!occluded) {
+                const uint32_t slot = __float_as_uint(d.w);
+                const float4 w = pool.shW[i];
+                float4 L = pool.L[slot];
+                L.x += w.x;
+                L.y += w.y;
+                L.z += w.z;
+                pool.L[slot] = L;
+            }
+        }
+        if (lane == 0) {
+            const uint32_t done = min(32u, n - base);
+            atomicAdd((unsigned long long *)&cnt->shadowRays, (unsigned long long)done);
+        }
+    }
+}
+
+// ------------------------------------------------------------- environment map
+// kernels/envmap/reduce.metal:3-24 over one level of `cur x cur` quads.
+__global__ void k_envmap_reduce(float *mip, int cur) {
+    const int tx = blockIdx.x * blockDim.x + threadIdx.x;
+    const int ty = blockIdx.y * blockDim.y + threadIdx.y;
+    if (tx >= cur || ty >= cur) return;
+    const int inputIndex = ty * cur + tx;
+    const int gridLength = cur * cur;
+    float sum = 0.0f;
+    for (int i = 0; i < 4; ++i) sum += mip[gridLength + 4 * inputIndex + i];
+    for (int i = 0; i < 4; ++i) mip[gridLength + 4 * inputIndex + i] /= sum;
+    const unsigned qx = tx / 2, qy = ty / 2, qw = cur / 2;
+    const unsigned outputIndex = cur == 1 ? 0u : 4u * (qy * qw + qx) + (tx & 1) + 2u * (ty & 1);
+    mip[outputIndex] = sum;
+}
+// kernels/envmap/normalize.metal:4-11
+__global__ void k_envmap_normalize(const float *sum, float *pdfs, uint32_t gridSize) {
+    const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= gridSize) return;
+    const float scale = (float)gridSize * warp::uniformSquareToSpherePdf() / *sum;
+    pdfs[i] *= scale;
+}
+
+// ------------------------------------------------------------- film read-out
+// kernels/utils/normalizeImage.metal:11-59
+__device__ float3 tonemapHablePartial(float3 x) {
+    const float hA = 0.15f, hB = 0.50f, hC = 0.10f, hD = 0.20f, hE = 0.02f, hF = 0.30f;
+    return ((x * (hA * x + hC * hB) + hD * hE) / (x * (hA * x + hB) + hD * hF)) - hE / hF;
+}
+__global__ void k_film_resolve(const float4 *film, const double *film64, int fp64, float *out, uint32_t numPixels,
+                               float scale, uint32_t tonemapping) {
+    const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= numPixels) return;
+    float3 c;
+    if (fp64) c = make_float3((float)film64[3 * (size_t)i], (float)film64[3 * (size_t)i + 1], (float)film64[3 * (size_t)i + 2]);
+    else c = xyz(film[i]);
+    c = c * scale;
+    if (tonemapping == 1u) {
+        const float3 curr = tonemapHablePartial(c * 2.0f);
+        const float3 whiteScale = 1.0f / tonemapHablePartial(f3(11.2f));
+        c = curr * whiteScale;
+    } else if (tonemapping == 2u) {
+        const float tA = 2.51f, tB = 0.03f, tC = 2.43f, tD = 0.59f, tE = 0.14f;
+        c = saturate((c * (tA * c + tB)) / (c * (tC * c + tD) + tE));
+    }
+    out[3 * (size_t)i + 0] = c.x;
+    out[3 * (size_t)i + 1] = c.y;
+    out[3 * (size_t)i + 2] = c.z;
+}
+
+// ------------------------------------------------------------- test hooks
+__global__ void k_debug_prng(uint32_t mode, uint64_t a, uint64_t b, int n, float *out) {
+    if (blockIdx.x != 0 || threadIdx.x != 0) return;
+    PrngState p = mode == RNG_TEA ? PrngState::tea((uint32_t)a, (uint32_t)b) : PrngState::pcg(a, b);
+    for (int i = 0; i < n; i++) out[i] = p.sample();
+}
+__global__ void k_debug_trace(const BvhNode *nodes, const float4 *tris, const float *rays, int n, int any, float *out,
+                              uint32_t *inst, uint32_t *errors) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    const float *r = rays + 8 * (size_t)i;
+    const float3 o = make_float3(r[0], r[1], r[2]), d = make_float3(r[4], r[5], r[6]);
+    float4 h = make_float4(-1.0f, 0.0f, 0.0f, 0.0f);
+    uint32_t id = 0;
+    if (any) {
+        h.x = traceAny(nodes, tris, o, d, r[3], r[7], errors) ? 1.0f : -1.0f;
+    } else {
+        traceClosest(nodes, tris, o, d, r[3], r[7], h, id, errors);
+    }
+    out[4 * (size_t)i + 0] = h.x;
+    out[4 * (size_t)i + 1] = h.y;
+    out[4 * (size_t)i + 2] = h.z;
+    out[4 * (size_t)i + 3] = h.w;
+    inst[i] = id;
+}
+
+}  // namespace rmd
+
+// ------------------------------------------------------------- launch wrappers
+using namespace rmd;
+
+cudaError_t rmdLaunchFrameInit(const PathPool &pool, Counters *cnt, uint64_t firstPath, uint64_t endPath,
+                               cudaStream_t s) {
+    const uint32_t threads = 256;
+    const uint32_t blocks = (pool.capacity + threads - 1) / threads;
+    k_frame_init<<<blocks, threads, 0, s>>>(pool, cnt, firstPath, endPath);
+    return cudaGetLastError();
+}
+cudaError_t rmdLaunchFilmRegen(const Context &ctx, const PathPool &pool, const FrameParams &fp, Counters *cnt,
+                               uint32_t cur, int blocks, cudaStream_t s) {
+    k_film_regen<<<blocks, 256, 0, s>>>(ctx, pool, fp, cnt, cur);
+    return cudaGetLastError();
+}
+cudaError_t rmdLaunchTraceClosest(const BvhNode *nodes, const float4 *tris, const PathPool &pool, Counters *cnt,
+                                  uint32_t cur, int blocks, cudaStream_t s) {
+    k_trace_closest<<<blocks, 128, 0, s>>>(nodes, tris, pool, cnt, cur);
+    return cudaGetLastError();
+}
+cudaError_t rmdLaunchTraceShadow(const BvhNode *nodes, const float4 *tris, const PathPool &pool, Counters *cnt,
+                                 int blocks, cudaStream_t s) {
+    k_trace_shadow<<<blocks, 128, 0, s>>>(nodes, tris, pool, cnt);
+    return cudaGetLastError();
+}
+cudaError_t rmdLaunchEnvmapReduce(float *mip, int cur, cudaStream_t s) {
+    dim3 b(8, 8), g((cur + 7) / 8, (cur + 7) / 8);
+    k_envmap_reduce<<<g, b, 0, s>>>(mip, cur);
+    return cudaGetLastError();
+}
+cudaError_t rmdLaunchEnvmapNormalize(const float *sum, float *pdfs, uint32_t gridSize, cudaStream_t s) {
+    k_envmap_normalize<<<(gridSize + 255) / 256, 256, 0, s>>>(sum, pdfs, gridSize);
+    return cudaGetLastError();
+}
+cudaError_t rmdLaunchFilmResolve(const float4 *film, const double *film64, int fp64, float *out, uint32_t numPixels,
+                                 float scale, uint32_t tonemapping, cudaStream_t s) {
+    k_film_resolve<<<(numPixels + 255) / 256, 256, 0, s>>>(film, film64, fp64, out, numPixels, scale, tonemapping);
+    return cudaGetLastError();
+}
+cudaError_t rmdLaunchDebugPrng(uint32_t mode, uint64_t a, uint64_t b, int n, float *out, cudaStream_t s) {
+    k_debug_prng<<<1, 1, 0, s>>>(mode, a, b, n, out);
+    return cudaGetLastError();
+}
+cudaError_t rmdLaunchDebugTrace(const BvhNode *nodes, const float4 *tris, const float *rays, int n, int any, float *out,
+                                uint32_t *inst, uint32_t *errors, cudaStream_t s) {
+    k_debug_trace<<<(n + 127) / 128, 128, 0, s>>>(nodes, tris, rays, n, any, out, inst, errors);
+    return cudaGetLastError();
+}

@@ -1,0 +1,874 @@
+// C ABI of include/raymond.h: scene building (SceneLoader / ShapeBuilder /
+// EntityBuilder / LightBuilder / MaterialBuilder of the reference) and the
+// persistent wavefront render loop that replaces Renderer.execute.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <chrono>
+#include <cmath>
+#include <cstring>
+#include <memory>
+#include <string>
+#include <vector>
+
+#include "../../include/raymond.h"
+#include "../../include/raymond_testing.h"
+#include "bvh_build.h"
+#include "codegen.h"
+#include "device/wavefront.cuh"
+#include "jit.h"
+#include "kernels.h"
+
+using namespace rmd;
+
+namespace {
+
+thread_local std::string g_lastError;
+
+rmd_status fail(rmd_status s, const std::string &msg) {
+    g_lastError = msg;
+    return s;
+}
+
+#define RMD_CUDA(expr)                                                                                      \
+    do {                                                                                                    \
+        cudaError_t e_ = (expr);                                                                            \
+        if (e_ != cudaSuccess)                                                                              \
+            return fail(e_ == cudaErrorMemoryAllocation ? RMD_ERROR_OUT_OF_MEMORY : RMD_ERROR_CUDA,         \
+                        std::string(#expr) + ": " + cudaGetErrorString(e_));                               \
+    } while (0)
+
+// Device buffer owned by a scene or renderer.
+struct DevBuf {
+    void *ptr = nullptr;
+    size_t bytes = 0;
+    DevBuf() = default;
+    DevBuf(const DevBuf &) = delete;
+    DevBuf &operator=(const DevBuf &) = delete;
+    ~DevBuf() { release(); }
+    void release() {
+        if (ptr) cudaFree(ptr);
+        ptr = nullptr;
+        bytes = 0;
+    }
+    cudaError_t alloc(size_t n) {
+        release();
+        bytes = n;
+        if (n == 0) return cudaSuccess;
+        return cudaMalloc(&ptr, n);
+    }
+    cudaError_t upload(const void *src, size_t n, cudaStream_t s) {
+        cudaError_t e = alloc(n);
+        if (e != cudaSuccess || n == 0) return e;
+        e = cudaMemcpyAsync(ptr, src, n, cudaMemcpyHostToDevice, s);
+        if (e != cudaSuccess) return e;
+        return cudaStreamSynchronize(s);
+    }
+    template <class T>
+    T *as() const {
+        return static_cast<T *>(ptr);
+    }
+};
+
+struct HostMat4 {
+    float c[4][4];  // columns
+};
+
+}  // namespace
+
+struct rmd_context {
+    int device = 0;
+    int smCount = 148;
+    cudaStream_t stream = nullptr;
+};
+
+struct rmd_scene {
+    rmd_context *ctx = nullptr;
+    Context dctx{};  // device view
+    DevBuf vertices, normals, texcoords, faces, instances, lightFaces, envPdfs, envMipmap;
+    DevBuf areaLights, pointLights, sunLights, spotLights, shapeLights;
+    DevBuf surfaceTable, lightTable, materialParams;
+    DevBuf bvhNodes, bvhTris;
+    rmdhost::JitModule jit;
+    uint64_t triangles = 0, bvhNodeCount = 0;
+    int numSurface = 0, numLight = 0;
+    int shadeBlocks = 0, traceBlocks = 0, regenBlocks = 0;
+    ~rmd_scene() { rmdhost::unloadModule(jit); }
+};
+
+struct rmd_renderer {
+    rmd_scene *scene = nullptr;
+    uint32_t width = 0, height = 0, capacity = 0;
+    DevBuf rayO, rayD, tp, L, rng, pixel, sample, meta, hit, hitInst, q0, q1, qDone, shO, shD, shW;
+    DevBuf counters, film, film64, resolve;
+    Counters *hostCounters = nullptr;  // pinned
+    Context dctx{};
+    uint64_t samples = 0;
+    rmd_stats stats{};
+    cudaEvent_t ev[4] = {};
+    std::vector<cudaEvent_t> stageEvents;  // 4 per iteration + 1, recorded between the stage kernels
+    ~rmd_renderer() {
+        if (hostCounters) cudaFreeHost(hostCounters);
+        for (auto &e : ev)
+            if (e) cudaEventDestroy(e);
+        for (auto &e : stageEvents) cudaEventDestroy(e);
+    }
+    cudaError_t stageEvent(size_t i, cudaEvent_t &out) {
+        while (stageEvents.size() <= i) {
+            cudaEvent_t e;
+            cudaError_t err = cudaEventCreate(&e);
+            if (err != cudaSuccess) return err;
+            stageEvents.push_back(e);
+        }
+        out = stageEvents[i];
+        return cudaSuccess;
+    }
+};
+
+// --------------------------------------------------------------------- helpers
+namespace {
+
+// column-major 4x4 from the C ABI
+HostMat4 toMat(const float *m) {
+    HostMat4 r;
+    for (int c = 0; c < 4; c++)
+        for (int k = 0; k < 4; k++) r.c[c][k] = m[4 * c + k];
+    return r;
+}
+
+// (M * float4(p, 1)).xyz in the same association order as the device code
+void transformPoint(const HostMat4 &M, const float *p, float *out) {
+    for (int k = 0; k < 3; k++) {
+        float a = M.c[0][k] * p[0];
+        float b = M.c[1][k] * p[1];
+        float c = M.c[2][k] * p[2];
+        float d = M.c[3][k] * 1.0f;
+        out[k] = ((a + b) + c) + d;
+    }
+}
+
+// inverse-transpose of the upper 3x3 (EntityBuilder.swift:98), columns
+void inverseTranspose3(const HostMat4 &M, float out[3][3]) {
+    const float *a = M.c[0], *b = M.c[1], *c = M.c[2];
+    auto cross = [](const float *u, const float *v, float *r) {
+        r[0] = u[1] * v[2] - u[2] * v[1];
+        r[1] = u[2] * v[0] - u[0] * v[2];
+        r[2] = u[0] * v[1] - u[1] * v[0];
+    };
+    float r0[3], r1[3], r2[3];
+    cross(b, c, r0);
+    cross(c, a, r1);
+    cross(a, b, r2);
+    const float det = a[0] * r0[0] + a[1] * r0[1] + a[2] * r0[2];
+    for (int k = 0; k < 3; k++) {
+        out[0][k] = r0[k] / det;
+        out[1][k] = r1[k] / det;
+        out[2][k] = r2[k] / det;
+    }
+}
+
+// host/lights/distribution.m:7-39 (area CDF over all faces of the shape, accumulated in double)
+float buildLightDistribution(const HostMat4 &M, const uint32_t *idx, const float *verts, uint32_t faceCount,
+                             float *output) {
+    double acc = 0;
+    auto mul = [&](const float *v, float *r) {  // inner3x3 * v
+        for (int k = 0; k < 3; k++) r[k] = M.c[0][k] * v[0] + M.c[1][k] * v[1] + M.c[2][k] * v[2];
+    };
+    for (uint32_t i = 0; i < faceCount; i++) {
+        const float *v0 = verts + 3 * idx[3 * i], *v1 = verts + 3 * idx[3 * i + 1], *v2 = verts + 3 * idx[3 * i + 2];
+        float e0[3], e1[3], a[3], b[3];
+        for (int k = 0; k < 3; k++) {
+            e0[k] = v2[k] - v0[k];
+            e1[k] = v2[k] - v1[k];
+        }
+        mul(e0, a);
+        mul(e1, b);
+        const float tn[3] = {a[1] * b[2] - a[2] * b[1], a[2] * b[0] - a[0] * b[2], a[0] * b[1] - a[1] * b[0]};
+        const float area = std::sqrt(tn[0] * tn[0] + tn[1] * tn[1] + tn[2] * tn[2]) / 2;
+        output[i] = (float)(acc += area);
+    }
+    for (uint32_t i = 0; i < faceCount; i++) output[i] = (float)(output[i] / acc);
+    return (float)acc;
+}
+
+rmd_status buildEnvironmentMap(rmd_scene *s, int exponent) {
+    cudaStream_t st = s->ctx->stream;
+    const int res = 1 << exponent;
+    size_t mipSize = 0;
+    for (int e = 0; e <= exponent; e++) mipSize += (size_t)1 << (2 * e);
+    RMD_CUDA(s->envMipmap.alloc(mipSize * sizeof(float)));
+    RMD_CUDA(s->envPdfs.alloc((size_t)res * res * sizeof(float)));
+    s->dctx.envResolution = res;
+    s->dctx.envMipmap = s->envMipmap.as<float>();
+    s->dctx.envPdfs = s->envPdfs.as<float>();
+    const size_t lastLevel = mipSize - (size_t)res * res;
+    float *finest = s->envMipmap.as<float>() + lastLevel;
+    float *pdfs = s->envPdfs.as<float>();
+    void *args[] = {&s->dctx, &finest, &pdfs, (void *)&res};
+    dim3 b(8, 8), g((res + 7) / 8, (res + 7) / 8);
+    RMD_CUDA(cudaLaunchKernel((const void *)s->jit.envmapBuild, g, b, args, 0, st));
+    size_t off = lastLevel;
+    for (int e = exponent - 1; e >= 0; e--) {
+        const int cur = 1 << e;
+        off -= (size_t)cur * cur;
+        RMD_CUDA(rmdLaunchEnvmapReduce(s->envMipmap.as<float>() + off, cur, st));
+    }
+    RMD_CUDA(rmdLaunchEnvmapNormalize(s->envMipmap.as<float>(), pdfs, (uint32_t)res * (uint32_t)res, st));
+    RMD_CUDA(cudaStreamSynchronize(st));
+    return RMD_OK;
+}
+
+int occupancyBlocks(const void *fn, int threads, int smCount) {
+    int perSm = 0;
+    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&perSm, fn, threads, 0) != cudaSuccess || perSm <= 0) perSm = 4;
+    return perSm * smCount;
+}
+
+}  // namespace
+
+// --------------------------------------------------------------------- C ABI
+extern "C" {
+
+const char *rmd_last_error(void) { return g_lastError.c_str(); }
+const char *rmd_version(void) { return "raymond_b200 0.1 (sm_100a)"; }
+
+rmd_status rmd_context_create(int32_t device, rmd_context **out) {
+    if (!out) return fail(RMD_ERROR_INVALID_ARGUMENT, "out is NULL");
+    int count = 0;
+    if (cudaGetDeviceCount(&count) != cudaSuccess || count == 0) return fail(RMD_ERROR_NO_DEVICE, "no CUDA device");
+    if (device < 0 || device >= count) return fail(RMD_ERROR_INVALID_ARGUMENT, "device index out of range");
+    auto c = std::make_unique<rmd_context>();
+    c->device = device;
+    RMD_CUDA(cudaSetDevice(device));
+    RMD_CUDA(cudaDeviceGetAttribute(&c->smCount, cudaDevAttrMultiProcessorCount, device));
+    RMD_CUDA(cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking));
+    *out = c.release();
+    return RMD_OK;
+}
+
+void rmd_context_destroy(rmd_context *c) {
+    if (!c) return;
+    if (c->stream) cudaStreamDestroy(c->stream);
+    delete c;
+}
+
+rmd_status rmd_scene_create(rmd_context *ctx, const rmd_scene_desc *d, rmd_scene **out) {
+    if (!ctx || !d || !out) return fail(RMD_ERROR_INVALID_ARGUMENT, "NULL argument");
+    if (d->num_surface_materials < 0 || d->num_light_materials <= 0 || d->num_shapes < 0 || d->num_entities < 0)
+        return fail(RMD_ERROR_INVALID_ARGUMENT, "invalid counts (at least the world material is required)");
+    if (d->world_shader >= d->num_light_materials) return fail(RMD_ERROR_INVALID_ARGUMENT, "world_shader out of range");
+    if (d->envmap_exponent < 0 || d->envmap_exponent > 12)
+        return fail(RMD_ERROR_INVALID_ARGUMENT, "envmap_exponent out of range (0..12)");
+    RMD_CUDA(cudaSetDevice(ctx->device));
+    auto s = std::make_unique<rmd_scene>();
+    s->ctx = ctx;
+    cudaStream_t st = ctx->stream;
+
+    // MaterialBuilder.build: generate and JIT-compile the material module
+    rmdhost::GeneratedModule mod;
+    try {
+        const bool hoist = std::getenv("RMD_NO_HOIST") == nullptr;
+        mod = rmdhost::generateModule(d->surface_materials, d->num_surface_materials, d->light_materials,
+                                      d->num_light_materials, hoist);
+    } catch (const rmdhost::CodegenError &e) {
+        return fail(e.status, e.message);
+    }
+    s->numSurface = d->num_surface_materials;
+    s->numLight = d->num_light_materials;
+
+    // ShapeBuilder.build (ShapeBuilder.swift:251-298)
+    struct ShapeInfo {
+        uint32_t vertexOffset, faceOffset, faceCount;
+        float boundsMin[3], boundsMax[3];
+        bool hasEmission;
+    };
+    std::vector<ShapeInfo> shapes;
+    std::vector<float4> verts, norms;
+    std::vector<float2> uvs;
+    std::vector<uint4> faces;
+    std::vector<float> vertsPacked;  // for the light CDF
+    std::vector<uint32_t> idxPacked;
+    for (int si = 0; si < d->num_shapes; si++) {
+        const rmd_shape &sh = d->shapes[si];
+        if ((sh.num_vertices && (!sh.vertices || !sh.normals || !sh.texcoords)) ||
+            (sh.num_faces && (!sh.indices || !sh.materials)))
+            return fail(RMD_ERROR_INVALID_ARGUMENT, "shape " + std::to_string(si) + " has NULL arrays");
+        ShapeInfo info{};
+        info.vertexOffset = (uint32_t)verts.size();
+        info.faceOffset = (uint32_t)faces.size();
+        info.faceCount = sh.num_faces;
+        for (int k = 0; k < 3; k++) {
+            info.boundsMin[k] = INFINITY;
+            info.boundsMax[k] = -INFINITY;
+        }
+        for (uint32_t v = 0; v < sh.num_vertices; v++) {
+            const float *p = sh.vertices + 3 * v;
+            for (int k = 0; k < 3; k++) {  // PLYReader.m:119-122 (else-if: the first vertex never raises the max)
+                if (p[k] < info.boundsMin[k]) info.boundsMin[k] = p[k];
+                else if (p[k] > info.boundsMax[k]) info.boundsMax[k] = p[k];
+            }
+            verts.push_back(make_float4(p[0], p[1], p[2], 0.0f));
+            vertsPacked.insert(vertsPacked.end(), p, p + 3);
+            const float *n = sh.normals + 3 * v;
+            norms.push_back(make_float4(n[0], n[1], n[2], 0.0f));
+            uvs.push_back(make_float2(sh.texcoords[2 * v], sh.texcoords[2 * v + 1]));
+        }
+        info.hasEmission = false;
+        for (uint32_t f = 0; f < sh.num_faces; f++) {
+            const uint32_t *ix = sh.indices + 3 * f;
+            if (ix[0] >= sh.num_vertices || ix[1] >= sh.num_vertices || ix[2] >= sh.num_vertices)
+                return fail(RMD_ERROR_INVALID_ARGUMENT, "vertex index out of range in shape " + std::to_string(si));
+            const uint16_t m = sh.materials[f];
+            if (m >= d->num_surface_materials)
+                return fail(RMD_ERROR_INVALID_ARGUMENT, "face material out of range in shape " + std::to_string(si));
+            faces.push_back(make_uint4(ix[0], ix[1], ix[2], m));
+            idxPacked.insert(idxPacked.end(), ix, ix + 3);
+            if (mod.surfaceEmissive[m]) info.hasEmission = true;
+        }
+        shapes.push_back(info);
+    }
+
+    // EntityBuilder.build (EntityBuilder.swift:79-141), flattened into one BVH
+    std::vector<PerInstanceData> insts;
+    std::vector<float> t0, t1, t2;
+    std::vector<uint32_t> triInst, triPrim;
+    struct PendingLight {
+        uint32_t instance, shape;
+        HostMat4 M;
+        uint32_t lightFaceOffset;
+    };
+    std::vector<PendingLight> pending;
+    uint32_t lightFaceOffset = 0;
+    for (int ei = 0; ei < d->num_entities; ei++) {
+        const rmd_entity &e = d->entities[ei];
+        if (e.shape >= (uint32_t)d->num_shapes) return fail(RMD_ERROR_INVALID_ARGUMENT, "entity shape out of range");
+        const ShapeInfo &si = shapes[e.shape];
+        const HostMat4 M = toMat(e.matrix);
+        PerInstanceData inst{};
+        inst.vertexOffset = si.vertexOffset;
+        inst.faceOffset = si.faceOffset;
+        inst.visibility = e.visibility;
+        inst.lightIndex = 0xffffffffu;
+        inst.triOffset = (uint32_t)triInst.size();
+        inst.boundsMin = make_float4(si.boundsMin[0], si.boundsMin[1], si.boundsMin[2], 0.0f);
+        inst.boundsSize = make_float4(si.boundsMax[0] - si.boundsMin[0], si.boundsMax[1] - si.boundsMin[1],
+                                      si.boundsMax[2] - si.boundsMin[2], 0.0f);
+        for (int c = 0; c < 4; c++) inst.pointTransform[c] = make_float4(M.c[c][0], M.c[c][1], M.c[c][2], M.c[c][3]);
+        float nt[3][3];
+        inverseTranspose3(M, nt);
+        for (int c = 0; c < 3; c++) inst.normalTransform[c] = make_float4(nt[c][0], nt[c][1], nt[c][2], 0.0f);
+        if (si.hasEmission) {
+            inst.lightIndex = (uint32_t)pending.size();
+            inst.lightFaceOffset = lightFaceOffset;
+            inst.lightFaceCount = si.faceCount;
+            pending.push_back({(uint32_t)ei, e.shape, M, lightFaceOffset});
+            lightFaceOffset += si.faceCount;
+        }
+        insts.push_back(inst);
+        for (uint32_t f = 0; f < si.faceCount; f++) {
+            const uint4 fc = faces[si.faceOffset + f];
+            const uint32_t vi[3] = {fc.x, fc.y, fc.z};
+            float w[3][3];
+            for (int j = 0; j < 3; j++) {
+                const float4 p = verts[si.vertexOffset + vi[j]];
+                const float pp[3] = {p.x, p.y, p.z};
+                transformPoint(M, pp, w[j]);
+            }
+            t0.insert(t0.end(), w[0], w[0] + 3);
+            t1.insert(t1.end(), w[1], w[1] + 3);
+            t2.insert(t2.end(), w[2], w[2] + 3);
+            triInst.push_back((uint32_t)ei);
+            triPrim.push_back(f);
+        }
+    }
+    s->triangles = triInst.size();
+    rmdhost::GpuBvh bvh;
+    rmdhost::buildBvh(t0, t1, t2, triInst, triPrim, bvh);
+    s->bvhNodeCount = bvh.nodes.size();
+
+    // LightBuilder.build (LightBuilder.swift:179-281)
+    std::vector<float> lightFaces(std::max<uint32_t>(1, lightFaceOffset), 0.0f);
+    std::vector<ShapeLight> shapeLights;
+    for (auto &p : pending) {
+        const ShapeInfo &si = shapes[p.shape];
+        ShapeLight sl;
+        sl.instanceIndex = p.instance;
+        sl.emissiveArea = buildLightDistribution(p.M, idxPacked.data() + 3 * (size_t)si.faceOffset,
+                                                 vertsPacked.data() + 3 * (size_t)si.vertexOffset, si.faceCount,
+                                                 lightFaces.data() + p.lightFaceOffset);
+        shapeLights.push_back(sl);
+    }
+    auto info = [](const rmd_light_info &i) {
+        LightInfo r{};
+        r.shaderIndex = i.shader_index;
+        r.castsShadows = i.casts_shadows;
+        r.usesMIS = i.uses_mis;
+        return r;
+    };
+    std::vector<AreaLight> areas;
+    for (int i = 0; i < d->num_area_lights; i++) {
+        const rmd_area_light &l = d->area_lights[i];
+        AreaLight a{};
+        a.info = info(l.info);
+        for (int c = 0; c < 3; c++)
+            a.transform[c] = make_float4(l.transform[4 * c], l.transform[4 * c + 1], l.transform[4 * c + 2],
+                                         l.transform[4 * c + 3]);
+        a.color = make_float4(l.color[0], l.color[1], l.color[2], l.is_circular ? 1.0f : 0.0f);
+        areas.push_back(a);
+    }
+    std::vector<PointLight> points;
+    for (int i = 0; i < d->num_point_lights; i++) {
+        const rmd_point_light &l = d->point_lights[i];
+        PointLight p{};
+        p.info = info(l.info);
+        p.locationRadius = make_float4(l.location[0], l.location[1], l.location[2], l.radius);
+        p.color = make_float4(l.color[0], l.color[1], l.color[2], 0.0f);
+        points.push_back(p);
+    }
+    std::vector<SunLight> suns;
+    for (int i = 0; i < d->num_sun_lights; i++) {
+        const rmd_sun_light &l = d->sun_lights[i];
+        SunLight p{};
+        p.info = info(l.info);
+        p.directionCosAngle = make_float4(l.direction[0], l.direction[1], l.direction[2], l.cos_angle);
+        p.color = make_float4(l.color[0], l.color[1], l.color[2], 0.0f);
+        suns.push_back(p);
+    }
+    std::vector<SpotLight> spots;
+    for (int i = 0; i < d->num_spot_lights; i++) {
+        const rmd_spot_light &l = d->spot_lights[i];
+        SpotLight p{};
+        p.info = info(l.info);
+        p.locationRadius = make_float4(l.location[0], l.location[1], l.location[2], l.radius);
+        p.directionSpotSize = make_float4(l.direction[0], l.direction[1], l.direction[2], l.spot_size);
+        p.colorSpotBlend = make_float4(l.color[0], l.color[1], l.color[2], l.spot_blend);
+        spots.push_back(p);
+    }
+    auto checkShader = [&](const rmd_light_info &i) { return i.shader_index < d->num_light_materials; };
+    for (int i = 0; i < d->num_area_lights; i++)
+        if (!checkShader(d->area_lights[i].info)) return fail(RMD_ERROR_INVALID_ARGUMENT, "area light shader index");
+    for (int i = 0; i < d->num_point_lights; i++)
+        if (!checkShader(d->point_lights[i].info)) return fail(RMD_ERROR_INVALID_ARGUMENT, "point light shader index");
+    for (int i = 0; i < d->num_sun_lights; i++)
+        if (!checkShader(d->sun_lights[i].info)) return fail(RMD_ERROR_INVALID_ARGUMENT, "sun light shader index");
+    for (int i = 0; i < d->num_spot_lights; i++)
+        if (!checkShader(d->spot_lights[i].info)) return fail(RMD_ERROR_INVALID_ARGUMENT, "spot light shader index");
+
+    // material tables
+    std::vector<uint2> stab, ltab;
+    for (size_t i = 0; i < mod.surface.group.size(); i++) stab.push_back(make_uint2(mod.surface.group[i], mod.surface.offset[i]));
+    for (size_t i = 0; i < mod.light.group.size(); i++) ltab.push_back(make_uint2(mod.light.group[i], mod.light.offset[i]));
+    if (mod.params.empty()) mod.params.push_back(0.0f);
+    if (stab.empty()) stab.push_back(make_uint2(0, 0));
+
+    // uploads
+    RMD_CUDA(s->vertices.upload(verts.data(), verts.size() * sizeof(float4), st));
+    RMD_CUDA(s->normals.upload(norms.data(), norms.size() * sizeof(float4), st));
+    RMD_CUDA(s->texcoords.upload(uvs.data(), uvs.size() * sizeof(float2), st));
+    RMD_CUDA(s->faces.upload(faces.data(), faces.size() * sizeof(uint4), st));
+    RMD_CUDA(s->instances.upload(insts.data(), insts.size() * sizeof(PerInstanceData), st));
+    RMD_CUDA(s->lightFaces.upload(lightFaces.data(), lightFaces.size() * sizeof(float), st));
+    RMD_CUDA(s->areaLights.upload(areas.data(), areas.size() * sizeof(AreaLight), st));
+    RMD_CUDA(s->pointLights.upload(points.data(), points.size() * sizeof(PointLight), st));
+    RMD_CUDA(s->sunLights.upload(suns.data(), suns.size() * sizeof(SunLight), st));
+    RMD_CUDA(s->spotLights.upload(spots.data(), spots.size() * sizeof(SpotLight), st));
+    RMD_CUDA(s->shapeLights.upload(shapeLights.data(), shapeLights.size() * sizeof(ShapeLight), st));
+    RMD_CUDA(s->surfaceTable.upload(stab.data(), stab.size() * sizeof(uint2), st));
+    RMD_CUDA(s->lightTable.upload(ltab.data(), ltab.size() * sizeof(uint2), st));
+    RMD_CUDA(s->materialParams.upload(mod.params.data(), mod.params.size() * sizeof(float), st));
+    RMD_CUDA(s->bvhNodes.upload(bvh.nodes.data(), bvh.nodes.size() * sizeof(rmdhost::GpuBvhNode), st));
+    RMD_CUDA(s->bvhTris.upload(bvh.tris.data(), bvh.tris.size() * sizeof(float), st));
+
+    Context &c = s->dctx;
+    c.vertices = s->vertices.as<float4>();
+    c.normals = s->normals.as<float4>();
+    c.texcoords = s->texcoords.as<float2>();
+    c.faces = s->faces.as<uint4>();
+    c.instances = s->instances.as<PerInstanceData>();
+    c.lightFaces = s->lightFaces.as<float>();
+    c.areaLights = s->areaLights.as<AreaLight>();
+    c.pointLights = s->pointLights.as<PointLight>();
+    c.sunLights = s->sunLights.as<SunLight>();
+    c.spotLights = s->spotLights.as<SpotLight>();
+    c.shapeLights = s->shapeLights.as<ShapeLight>();
+    c.surfaceTable = s->surfaceTable.as<uint2>();
+    c.lightTable = s->lightTable.as<uint2>();
+    c.materialParams = s->materialParams.as<float>();
+    c.numAreaLights = (int)areas.size();
+    c.numPointLights = (int)points.size();
+    c.numSunLights = (int)suns.size();
+    c.numSpotLights = (int)spots.size();
+    c.numShapeLights = (int)shapeLights.size();
+    c.numLightsTotal = 1 + c.numAreaLights + c.numPointLights + c.numSunLights + c.numSpotLights + c.numShapeLights;
+    c.worldShader = d->world_shader;
+    for (int k = 0; k < 4; k++)
+        c.cameraTransform[k] = make_float4(d->camera.transform[4 * k], d->camera.transform[4 * k + 1],
+                                           d->camera.transform[4 * k + 2], d->camera.transform[4 * k + 3]);
+    c.nearClip = d->camera.near_clip;
+    c.farClip = d->camera.far_clip;
+    c.focalLength = d->camera.focal_length;
+    c.shift = make_float2(d->camera.shift[0], d->camera.shift[1]);
+
+    const std::string err = rmdhost::compileModule(mod.source, s->jit);
+    if (!err.empty()) return fail(RMD_ERROR_NVRTC, err);
+    rmd_status r = buildEnvironmentMap(s.get(), d->envmap_exponent);
+    if (r != RMD_OK) return r;
+    s->shadeBlocks = occupancyBlocks((const void *)s->jit.shade, 128, ctx->smCount);
+    *out = s.release();
+    return RMD_OK;
+}
+
+void rmd_scene_destroy(rmd_scene *s) { delete s; }
+
+rmd_status rmd_scene_info(const rmd_scene *s, uint64_t *triangles, uint64_t *bvh_nodes, int32_t *num_lights_total) {
+    if (!s) return fail(RMD_ERROR_INVALID_ARGUMENT, "NULL scene");
+    if (triangles) *triangles = s->triangles;
+    if (bvh_nodes) *bvh_nodes = s->bvhNodeCount;
+    if (num_lights_total) *num_lights_total = s->dctx.numLightsTotal;
+    return RMD_OK;
+}
+
+static rmd_status allocatePool(rmd_renderer *r) {
+    const size_t P = r->capacity;
+    RMD_CUDA(r->rayO.alloc(P * 16));
+    RMD_CUDA(r->rayD.alloc(P * 16));
+    RMD_CUDA(r->tp.alloc(P * 16));
+    RMD_CUDA(r->L.alloc(P * 16));
+    RMD_CUDA(r->rng.alloc(P * 8));
+    RMD_CUDA(r->pixel.alloc(P * 4));
+    RMD_CUDA(r->sample.alloc(P * 4));
+    RMD_CUDA(r->meta.alloc(P * 4));
+    RMD_CUDA(r->hit.alloc(P * 16));
+    RMD_CUDA(r->hitInst.alloc(P * 4));
+    RMD_CUDA(r->q0.alloc(P * 4));
+    RMD_CUDA(r->q1.alloc(P * 4));
+    RMD_CUDA(r->qDone.alloc(P * 4));
+    RMD_CUDA(r->shO.alloc(P * 16));
+    RMD_CUDA(r->shD.alloc(P * 16));
+    RMD_CUDA(r->shW.alloc(P * 16));
+    RMD_CUDA(r->counters.alloc(sizeof(Counters)));
+    return RMD_OK;
+}
+
+static PathPool poolView(rmd_renderer *r) {
+    PathPool p;
+    p.rayO = r->rayO.as<float4>();
+    p.rayD = r->rayD.as<float4>();
+    p.tp = r->tp.as<float4>();
+    p.L = r->L.as<float4>();
+    p.rng = r->rng.as<uint2>();
+    p.pixel = r->pixel.as<uint32_t>();
+    p.sample = r->sample.as<uint32_t>();
+    p.meta = r->meta.as<uint32_t>();
+    p.hit = r->hit.as<float4>();
+    p.hitInst = r->hitInst.as<uint32_t>();
+    p.q[0] = r->q0.as<uint32_t>();
+    p.q[1] = r->q1.as<uint32_t>();
+    p.qDone = r->qDone.as<uint32_t>();
+    p.shO = r->shO.as<float4>();
+    p.shD = r->shD.as<float4>();
+    p.shW = r->shW.as<float4>();
+    p.capacity = r->capacity;
+    return p;
+}
+
+rmd_status rmd_renderer_set_size(rmd_renderer *r, uint32_t width, uint32_t height) {
+    if (!r || width == 0 || height == 0 || width > 65535 || height > 65535)
+        return fail(RMD_ERROR_INVALID_ARGUMENT, "invalid renderer size");
+    RMD_CUDA(cudaSetDevice(r->scene->ctx->device));
+    r->width = width;
+    r->height = height;
+    RMD_CUDA(r->film.alloc((size_t)width * height * sizeof(float4)));
+    r->film64.release();
+    RMD_CUDA(r->resolve.alloc((size_t)width * height * 3 * sizeof(float)));
+    return rmd_renderer_reset(r);
+}
+
+rmd_status rmd_renderer_create(rmd_scene *scene, uint32_t width, uint32_t height, uint32_t pool_size,
+                               rmd_renderer **out) {
+    if (!scene || !out) return fail(RMD_ERROR_INVALID_ARGUMENT, "NULL argument");
+    RMD_CUDA(cudaSetDevice(scene->ctx->device));
+    auto r = std::make_unique<rmd_renderer>();
+    r->scene = scene;
+    r->dctx = scene->dctx;
+    r->capacity = pool_size ? pool_size : (1u << 21);
+    rmd_status st = allocatePool(r.get());
+    if (st != RMD_OK) return st;
+    RMD_CUDA(cudaMallocHost((void **)&r->hostCounters, sizeof(Counters)));
+    for (auto &e : r->ev) RMD_CUDA(cudaEventCreate(&e));
+    st = rmd_renderer_set_size(r.get(), width, height);
+    if (st != RMD_OK) return st;
+    *out = r.release();
+    return RMD_OK;
+}
+
+void rmd_renderer_destroy(rmd_renderer *r) { delete r; }
+
+rmd_status rmd_renderer_reset(rmd_renderer *r) {
+    if (!r) return fail(RMD_ERROR_INVALID_ARGUMENT, "NULL renderer");
+    cudaStream_t st = r->scene->ctx->stream;
+    RMD_CUDA(cudaMemsetAsync(r->film.ptr, 0, r->film.bytes, st));
+    if (r->film64.ptr) RMD_CUDA(cudaMemsetAsync(r->film64.ptr, 0, r->film64.bytes, st));
+    RMD_CUDA(cudaStreamSynchronize(st));
+    r->samples = 0;
+    return RMD_OK;
+}
+
+rmd_status rmd_renderer_set_camera(rmd_renderer *r, const rmd_camera *cam) {
+    if (!r || !cam) return fail(RMD_ERROR_INVALID_ARGUMENT, "NULL argument");
+    Context &c = r->dctx;
+    for (int k = 0; k < 4; k++)
+        c.cameraTransform[k] = make_float4(cam->transform[4 * k], cam->transform[4 * k + 1], cam->transform[4 * k + 2],
+                                           cam->transform[4 * k + 3]);
+    c.nearClip = cam->near_clip;
+    c.farClip = cam->far_clip;
+    c.focalLength = cam->focal_length;
+    c.shift = make_float2(cam->shift[0], cam->shift[1]);
+    return rmd_renderer_reset(r);
+}
+
+rmd_status rmd_render(rmd_renderer *r, const rmd_render_settings *s) {
+    if (!r || !s) return fail(RMD_ERROR_INVALID_ARGUMENT, "NULL argument");
+    if (s->max_depth == 0 || s->max_depth > 65535 || s->sampling_mode > 2 || s->rng > 1)
+        return fail(RMD_ERROR_INVALID_ARGUMENT, "invalid render settings");
+    rmd_scene *scene = r->scene;
+    rmd_context *ctx = scene->ctx;
+    RMD_CUDA(cudaSetDevice(ctx->device));
+    cudaStream_t st = ctx->stream;
+    const uint64_t numPixels = (uint64_t)r->width * r->height;
+    const uint64_t firstSample = s->first_sample >= 0 ? (uint64_t)s->first_sample : r->samples;
+    const uint64_t numPaths = (uint64_t)s->spp * numPixels;
+    if (firstSample + s->spp > 0xffffffffull) return fail(RMD_ERROR_INVALID_ARGUMENT, "sample index overflow");
+    if (s->film_fp64 && !r->film64.ptr) {
+        RMD_CUDA(r->film64.alloc(numPixels * 3 * sizeof(double)));
+        RMD_CUDA(cudaMemsetAsync(r->film64.ptr, 0, r->film64.bytes, st));
+    }
+    std::memset(&r->stats, 0, sizeof(r->stats));
+    r->stats.pool_size = r->capacity;
+    if (numPaths == 0) return RMD_OK;
+
+    FrameParams fp{};
+    fp.width = r->width;
+    fp.height = r->height;
+    fp.numPixels = (uint32_t)numPixels;
+    fp.maxDepth = s->max_depth;
+    fp.samplingMode = s->sampling_mode;
+    fp.rngMode = s->rng;
+    fp.seed = s->seed;
+    fp.filmFp64 = s->film_fp64 ? 1 : 0;
+    fp.film = r->film.as<float4>();
+    fp.film64 = r->film64.as<double>();
+    const PathPool pool = poolView(r);
+    Counters *cnt = r->counters.as<Counters>();
+    const uint64_t firstPath = firstSample * numPixels;
+
+    ShadeParams sp;
+    sp.ctx = r->dctx;
+    sp.pool = pool;
+    sp.fp = fp;
+    sp.counters = cnt;
+    void *shadeArgs[] = {&sp};
+    const int tb = ctx->smCount * 8;
+    const int rb = std::min<int>((r->capacity + 255) / 256, ctx->smCount * 8);
+    const int sb = scene->shadeBlocks;
+
+    RMD_CUDA(cudaEventRecord(r->ev[0], st));
+    RMD_CUDA(rmdLaunchFrameInit(pool, cnt, firstPath, firstPath + numPaths, st));
+    // every path needs at most max_depth iterations after it is generated, and
+    // each iteration generates min(capacity, remaining) paths
+    const uint64_t maxIters = ((numPaths + r->capacity - 1) / r->capacity + 1) * ((uint64_t)s->max_depth + 1) + 8;
+    uint64_t it = 0;
+    uint32_t cur = 0;
+    bool done = false;
+    size_t evi = 0;
+    cudaEvent_t e;
+    RMD_CUDA(r->stageEvent(evi++, e));
+    RMD_CUDA(cudaEventRecord(e, st));
+    while (!done) {
+        for (int k = 0; k < 4; k++, it++) {
+            RMD_CUDA(rmdLaunchFilmRegen(r->dctx, pool, fp, cnt, cur, rb, st));
+            RMD_CUDA(r->stageEvent(evi++, e));
+            RMD_CUDA(cudaEventRecord(e, st));
+            RMD_CUDA(rmdLaunchTraceClosest(scene->bvhNodes.as<BvhNode>(), scene->bvhTris.as<float4>(), pool, cnt, cur, tb, st));
+            RMD_CUDA(r->stageEvent(evi++, e));
+            RMD_CUDA(cudaEventRecord(e, st));
+            sp.cur = cur;
+            RMD_CUDA(cudaLaunchKernel((const void *)scene->jit.shade, dim3(sb), dim3(128), shadeArgs, 0, st));
+            RMD_CUDA(r->stageEvent(evi++, e));
+            RMD_CUDA(cudaEventRecord(e, st));
+            RMD_CUDA(rmdLaunchTraceShadow(scene->bvhNodes.as<BvhNode>(), scene->bvhTris.as<float4>(), pool, cnt, tb, st));
+            RMD_CUDA(r->stageEvent(evi++, e));
+            RMD_CUDA(cudaEventRecord(e, st));
+            cur ^= 1u;
+        }
+        RMD_CUDA(cudaMemcpyAsync(r->hostCounters, cnt, sizeof(Counters), cudaMemcpyDeviceToHost, st));
+        RMD_CUDA(cudaStreamSynchronize(st));
+        const Counters &h = *r->hostCounters;
+        if (h.errors) {
+            r->stats.errors = h.errors;
+            return fail(RMD_ERROR_QUEUE_OVERFLOW, "device error flags " + std::to_string(h.errors));
+        }
+        if (h.pathsDone >= numPaths) done = true;
+        else if (it > maxIters) return fail(RMD_ERROR_WATCHDOG, "render did not drain in the iteration bound");
+    }
+    RMD_CUDA(cudaEventRecord(r->ev[1], st));
+    RMD_CUDA(cudaEventSynchronize(r->ev[1]));
+    float ms = 0;
+    cudaEventElapsedTime(&ms, r->ev[0], r->ev[1]);
+    double stage[4] = {0, 0, 0, 0};  // film+regen, trace, shade, shadow
+    for (size_t i = 1; i < evi; i++) {
+        float t = 0;
+        cudaEventElapsedTime(&t, r->stageEvents[i - 1], r->stageEvents[i]);
+        stage[(i - 1) % 4] += t;
+    }
+    const Counters &h = *r->hostCounters;
+    r->stats.paths = h.pathsDone;
+    r->stats.segments = h.segments;
+    r->stats.shadow_rays = h.shadowRays;
+    r->stats.iterations = it;
+    r->stats.ms_total = ms;
+    r->stats.ms_film = stage[0];
+    r->stats.ms_trace = stage[1];
+    r->stats.ms_shade = stage[2];
+    r->stats.ms_shadow = stage[3];
+    r->samples = std::max<uint64_t>(r->samples, firstSample + s->spp);
+    return RMD_OK;
+}
+
+rmd_status rmd_film_read(rmd_renderer *r, float *rgb, int32_t normalize, uint32_t tonemapping, float exposure) {
+    if (!r || !rgb) return fail(RMD_ERROR_INVALID_ARGUMENT, "NULL argument");
+    if (tonemapping > 2) return fail(RMD_ERROR_INVALID_ARGUMENT, "tonemapping out of range");
+    cudaStream_t st = r->scene->ctx->stream;
+    const uint32_t n = r->width * r->height;
+    float scale = 1.0f;
+    uint32_t tm = 0;
+    if (normalize) {
+        scale = exposure / (float)std::max<uint64_t>(1, r->samples);
+        tm = tonemapping;
+    }
+    RMD_CUDA(rmdLaunchFilmResolve(r->film.as<float4>(), r->film64.as<double>(), 0, r->resolve.as<float>(), n, scale, tm, st));
+    RMD_CUDA(cudaMemcpyAsync(rgb, r->resolve.ptr, (size_t)n * 3 * sizeof(float), cudaMemcpyDeviceToHost, st));
+    RMD_CUDA(cudaStreamSynchronize(st));
+    return RMD_OK;
+}
+
+rmd_status rmd_film_read_f64(rmd_renderer *r, double *rgb) {
+    if (!r || !rgb) return fail(RMD_ERROR_INVALID_ARGUMENT, "NULL argument");
+    if (!r->film64.ptr) return fail(RMD_ERROR_INVALID_ARGUMENT, "no double-precision film (render with film_fp64)");
+    cudaStream_t st = r->scene->ctx->stream;
+    RMD_CUDA(cudaMemcpyAsync(rgb, r->film64.ptr, r->film64.bytes, cudaMemcpyDeviceToHost, st));
+    RMD_CUDA(cudaStreamSynchronize(st));
+    return RMD_OK;
+}
+
+rmd_status rmd_film_samples(const rmd_renderer *r, uint64_t *samples) {
+    if (!r || !samples) return fail(RMD_ERROR_INVALID_ARGUMENT, "NULL argument");
+    *samples = r->samples;
+    return RMD_OK;
+}
+
+rmd_status rmd_renderer_stats(const rmd_renderer *r, rmd_stats *out) {
+    if (!r || !out) return fail(RMD_ERROR_INVALID_ARGUMENT, "NULL argument");
+    *out = r->stats;
+    return RMD_OK;
+}
+
+// --------------------------------------------------------------------- test hooks
+rmd_status rmd_test_prng(uint32_t mode, uint64_t a, uint64_t b, int32_t n, float *out) {
+    if (!out || n < 0) return fail(RMD_ERROR_INVALID_ARGUMENT, "invalid arguments");
+    float *d = nullptr;
+    RMD_CUDA(cudaMalloc(&d, std::max<int>(1, n) * sizeof(float)));
+    cudaError_t e = rmdLaunchDebugPrng(mode, a, b, n, d, 0);
+    if (e == cudaSuccess) e = cudaMemcpy(out, d, n * sizeof(float), cudaMemcpyDeviceToHost);
+    cudaFree(d);
+    if (e != cudaSuccess) return fail(RMD_ERROR_CUDA, cudaGetErrorString(e));
+    return RMD_OK;
+}
+
+rmd_status rmd_test_trace(const rmd_scene *s, const float *rays, int32_t n, int32_t any, float *out,
+                          uint32_t *instances) {
+    if (!s || !rays || !out || !instances || n < 0) return fail(RMD_ERROR_INVALID_ARGUMENT, "invalid arguments");
+    DevBuf dr, dout, dinst, derr;
+    RMD_CUDA(dr.upload(rays, (size_t)n * 8 * sizeof(float), s->ctx->stream));
+    RMD_CUDA(dout.alloc((size_t)std::max(1, n) * 4 * sizeof(float)));
+    RMD_CUDA(dinst.alloc((size_t)std::max(1, n) * sizeof(uint32_t)));
+    RMD_CUDA(derr.alloc(sizeof(uint32_t)));
+    RMD_CUDA(cudaMemset(derr.ptr, 0, sizeof(uint32_t)));
+    if (n > 0)
+        RMD_CUDA(rmdLaunchDebugTrace(s->bvhNodes.as<BvhNode>(), s->bvhTris.as<float4>(), dr.as<float>(), n, any,
+                                     dout.as<float>(), dinst.as<uint32_t>(), derr.as<uint32_t>(), s->ctx->stream));
+    RMD_CUDA(cudaStreamSynchronize(s->ctx->stream));
+    RMD_CUDA(cudaMemcpy(out, dout.ptr, (size_t)n * 4 * sizeof(float), cudaMemcpyDeviceToHost));
+    RMD_CUDA(cudaMemcpy(instances, dinst.ptr, (size_t)n * sizeof(uint32_t), cudaMemcpyDeviceToHost));
+    return RMD_OK;
+}
+
+rmd_status rmd_test_material_eval(const rmd_scene *s, int32_t material, const float *records, int32_t n, float *out) {
+    if (!s || !records || !out || n < 0 || material < 0 || material >= s->numSurface)
+        return fail(RMD_ERROR_INVALID_ARGUMENT, "invalid arguments");
+    DevBuf din, dout;
+    RMD_CUDA(din.upload(records, (size_t)n * 28 * sizeof(float), s->ctx->stream));
+    RMD_CUDA(dout.alloc((size_t)std::max(1, n) * 16 * sizeof(float)));
+    Context c = s->dctx;
+    unsigned m = (unsigned)material;
+    const float *pin = din.as<float>();
+    float *pout = dout.as<float>();
+    int nn = n;
+    void *args[] = {&c, &m, &pin, &pout, &nn};
+    if (n > 0)
+        RMD_CUDA(cudaLaunchKernel((const void *)s->jit.materialEval, dim3((n + 127) / 128), dim3(128), args, 0,
+                                  s->ctx->stream));
+    RMD_CUDA(cudaStreamSynchronize(s->ctx->stream));
+    RMD_CUDA(cudaMemcpy(out, dout.ptr, (size_t)n * 16 * sizeof(float), cudaMemcpyDeviceToHost));
+    return RMD_OK;
+}
+
+rmd_status rmd_test_generate_source(const rmd_scene_desc *d, int32_t hoist, char *buf, int64_t buflen,
+                                    int64_t *needed) {
+    if (!d) return fail(RMD_ERROR_INVALID_ARGUMENT, "NULL desc");
+    try {
+        rmdhost::GeneratedModule mod = rmdhost::generateModule(d->surface_materials, d->num_surface_materials,
+                                                               d->light_materials, d->num_light_materials, hoist != 0);
+        if (needed) *needed = (int64_t)mod.source.size() + 1;
+        if (buf && buflen > 0) {
+            const size_t n = std::min<size_t>((size_t)buflen - 1, mod.source.size());
+            std::memcpy(buf, mod.source.data(), n);
+            buf[n] = 0;
+        }
+    } catch (const rmdhost::CodegenError &e) {
+        return fail(e.status, e.message);
+    }
+    return RMD_OK;
+}
+
+rmd_status rmd_test_jit_compile(const rmd_scene_desc *d, int32_t hoist, char *log, int64_t loglen,
+                                int64_t *cubin_bytes) {
+    if (!d) return fail(RMD_ERROR_INVALID_ARGUMENT, "NULL desc");
+    std::string msg;
+    try {
+        rmdhost::GeneratedModule mod = rmdhost::generateModule(d->surface_materials, d->num_surface_materials,
+                                                               d->light_materials, d->num_light_materials, hoist != 0);
+        std::vector<char> cubin;
+        bool cached = false;
+        std::string err = rmdhost::compileCubin(mod.source, cubin, msg, cached);
+        if (cubin_bytes) *cubin_bytes = (int64_t)cubin.size();
+        if (!err.empty()) {
+            if (log && loglen > 0) {
+                const size_t n = std::min<size_t>((size_t)loglen - 1, err.size());
+                std::memcpy(log, err.data(), n);
+                log[n] = 0;
+            }
+            return fail(RMD_ERROR_NVRTC, err);
+        }
+    } catch (const rmdhost::CodegenError &e) {
+        return fail(e.status, e.message);
+    }
+    if (log && loglen > 0) {
+        const size_t n = std::min<size_t>((size_t)loglen - 1, msg.size());
+        std::memcpy(log, msg.data(), n);
+        log[n] = 0;
+    }
+    return RMD_OK;
+}
+
+}  // extern "C"

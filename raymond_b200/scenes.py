@@ -285,8 +285,8 @@ def spheres_terrain(seed: int = 1, num_spheres: int = 64, subdivisions: int = 5,
         "entities": entities,
         "point_lights": points,
         "sun_lights": suns,
-        "camera": {"transform": look_at((10.0, 16.0, 40.0), (10.0, 3.0, 9.0)), "near_clip": 0.1, "far_clip": 100.0,
-                   "focal_length": 2.0},
+        "camera": {"transform": look_at((10.0, 13.0, 27.0), (10.0, 2.0, 9.0)), "near_clip": 0.1, "far_clip": 100.0,
+                   "focal_length": 1.6},
     }
 
 
