@@ -152,7 +152,12 @@ def main():
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--pool", type=int, default=0)
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--width", type=int, default=W, help="override (profiling runs only)")
+    ap.add_argument("--height", type=int, default=H, help="override (profiling runs only)")
+    ap.add_argument("--spp", type=int, default=SPP, help="override (profiling runs only)")
+    ap.add_argument("--no-e2e", action="store_true")
     args = ap.parse_args()
+    globals().update(W=args.width, H=args.height, SPP=args.spp)
     if args.impl == "reference":
         return run_reference(args)
 
@@ -202,9 +207,9 @@ def main():
     clocks = sampler.stop()
     # end to end through the C ABI with host buffers
     t0 = time.perf_counter()
-    for k in range(args.steps):
+    for k in range(0 if args.no_e2e else args.steps):
         step(k, e2e=True)
-    e2e_s = time.perf_counter() - t0
+    e2e_s = max(time.perf_counter() - t0, 1e-9)
     if dist:
         import torch
 

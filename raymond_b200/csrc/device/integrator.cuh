@@ -17,8 +17,9 @@ RMD_HD float computeMisWeight(float pdf, float other) {
     return pdf / (pdf + other);
 }
 
-// One path vertex: intersection.metal:43-208 for the path in `slot`.
-__device__ __forceinline__ void shadePath(const ShadeParams &p, uint32_t slot) {
+// One path vertex: intersection.metal:43-208 for the path in `slot`; returns
+// whether a surface was hit (a segment was shaded).
+__device__ __forceinline__ bool shadePath(const ShadeParams &p, uint32_t slot) {
     const Context &ctx = p.ctx;
     const PathPool &pool = p.pool;
     const FrameParams &fp = p.fp;
@@ -55,7 +56,6 @@ __device__ __forceinline__ void shadePath(const ShadeParams &p, uint32_t slot) {
             L += misWeight * rayWeight * shading.material.emission;
         }
     } else {
-        warpAdd64(&cnt->segments, 1u);
         const PerInstanceData &inst = ctx.instances[pool.hitInst[slot]];
         uint32_t shaderIndex;
         buildShading(shading, ctx, inst, __float_as_uint(h4.w), make_float2(h4.y, h4.z), h4.x, shaderIndex);
@@ -125,19 +125,22 @@ __device__ __forceinline__ void shadePath(const ShadeParams &p, uint32_t slot) {
         if (k < pool.capacity) pool.q[p.cur ^ 1u][k] = slot;
         else atomicOr(&cnt->errors, ERR_QUEUE_OVERFLOW);
     } else {
-        const uint32_t k = warpAppend(&cnt->nDone);
-        if (k < pool.capacity) pool.qDone[k] = slot;
+        const uint32_t k = warpAppend(&cnt->nD[p.cur]);
+        if (k < pool.capacity) pool.qDone[p.cur][k] = slot;
         else atomicOr(&cnt->errors, ERR_QUEUE_OVERFLOW);
     }
+    return h4.x > 0.0f;
 }
 
 }  // namespace rmd
 
 extern "C" __global__ void __launch_bounds__(128) rmd_shade(const __grid_constant__ rmd::ShadeParams p) {
-    const unsigned n = p.counters->nQ[p.cur];
+    const unsigned n = rmd::activeCount(p.counters, p.cur);
     const unsigned *q = p.pool.q[p.cur];
+    unsigned segments = 0;
     for (unsigned i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x)
-        rmd::shadePath(p, q[i]);
+        segments += rmd::shadePath(p, q[i]) ? 1u : 0u;
+    rmd::blockAdd64(&p.counters->segments, segments);
 }
 
 // kernels/envmap/build.metal:4-51 — the finest level of the importance map:

@@ -18,14 +18,19 @@ constexpr float SHADOW_EPS = 0.001f;  // device/constants.hpp:3
 constexpr uint32_t ERR_QUEUE_OVERFLOW = 1u;
 constexpr uint32_t ERR_STACK_OVERFLOW = 2u;
 
+// Queue bookkeeping without same-address atomics on the regeneration path:
+// iteration i (parity p = i & 1) shades the active queue Q[p]; its first
+// nQ[p] entries are the paths continued by the previous iteration and the
+// next newPaths() entries the camera samples the film kernel wrote there for
+// the slots the previous iteration finished (D[p ^ 1]).  Finished paths of
+// this iteration go to D[p]; continued ones to Q[p ^ 1].
 struct Counters {
-    uint32_t nQ[2];       // active-path queue sizes (ping-pong)
-    uint32_t nDone;       // finished / free slots waiting for the film kernel
+    uint32_t nQ[2];       // continued paths at the head of each active queue
+    uint32_t nD[2];       // finished / free slots
     uint32_t nShadow;     // shadow rays of this iteration
     uint32_t traceWork;   // persistent closest-hit work counter
     uint32_t shadowWork;  // persistent any-hit work counter
     uint32_t errors;
-    uint32_t pad;
     unsigned long long nextPath;    // next path id handed out by the film kernel
     unsigned long long endPath;     // one past the last path id of this render
     unsigned long long pathsDone;   // paths whose radiance reached the film
@@ -33,6 +38,17 @@ struct Counters {
     unsigned long long shadowRays;  // shadow rays traced
     unsigned long long pad2;
 };
+
+// camera samples the film kernel of this iteration appends to Q[p]
+__device__ __forceinline__ uint32_t newPaths(const Counters *c, uint32_t p) {
+    const unsigned long long next = c->nextPath, end = c->endPath;
+    if (next >= end) return 0u;
+    const unsigned long long left = end - next;
+    const uint32_t d = c->nD[p ^ 1u];
+    return left < (unsigned long long)d ? (uint32_t)left : d;
+}
+// size of the active queue Q[p] after the film kernel of this iteration
+__device__ __forceinline__ uint32_t activeCount(const Counters *c, uint32_t p) { return c->nQ[p] + newPaths(c, p); }
 
 struct PathPool {
     float4 *rayO;      // origin.xyz, tmin
@@ -46,7 +62,7 @@ struct PathPool {
     float4 *hit;       // t (<= 0: miss), b0, b1, primitive (bits)
     uint32_t *hitInst; // instance index
     uint32_t *q[2];    // active queues
-    uint32_t *qDone;   // finished slots
+    uint32_t *qDone[2];  // finished slots
     float4 *shO;       // shadow: origin.xyz, tmax
     float4 *shD;       // shadow: direction.xyz, slot (bits)
     float4 *shW;       // shadow: weight.xyz
@@ -81,6 +97,21 @@ __device__ __forceinline__ uint32_t warpAppend(uint32_t *counter) {
     if (lane == leader) base = atomicAdd(counter, (uint32_t)__popc(mask));
     base = __shfl_sync(mask, base, leader);
     return base + (uint32_t)__popc(mask & ((1u << lane) - 1u));
+}
+// Sums v over the block and adds it to *counter with one atomic (all threads must call).
+__device__ __forceinline__ void blockAdd64(unsigned long long *counter, uint32_t v) {
+    __shared__ uint32_t partial[32];
+    const uint32_t w = __reduce_add_sync(0xffffffffu, v);
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    if (lane == 0) partial[warp] = w;
+    __syncthreads();
+    if (warp == 0) {
+        const int nw = (blockDim.x + 31) >> 5;
+        const uint32_t x = lane < nw ? partial[lane] : 0u;
+        const uint32_t t = __reduce_add_sync(0xffffffffu, x);
+        if (lane == 0 && t) atomicAdd(counter, (unsigned long long)t);
+    }
+    __syncthreads();
 }
 __device__ __forceinline__ void warpAdd64(unsigned long long *counter, uint32_t v) {
     const unsigned mask = __activemask();

@@ -11,13 +11,14 @@
 namespace rmd {
 
 // ------------------------------------------------------------- frame set-up
-// Every slot starts on the done queue with no pixel, so the first film pass
-// hands each one a camera sample.
+// Every slot starts as a finished, pixel-less path in D[1], so the first film
+// pass (iteration 0 reads D[1]) hands each one a camera sample.
 __global__ void k_frame_init(PathPool pool, Counters *cnt, uint64_t firstPath, uint64_t endPath) {
     const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i == 0) {
         cnt->nQ[0] = cnt->nQ[1] = 0;
-        cnt->nDone = pool.capacity;
+        cnt->nD[0] = 0;
+        cnt->nD[1] = pool.capacity;
         cnt->nShadow = 0;
         cnt->traceWork = cnt->shadowWork = 0;
         cnt->errors = 0;
@@ -28,22 +29,34 @@ __global__ void k_frame_init(PathPool pool, Counters *cnt, uint64_t firstPath, u
         cnt->shadowRays = 0;
     }
     if (i < pool.capacity) {
-        pool.qDone[i] = i;
+        pool.qDone[1][i] = i;
         pool.pixel[i] = INVALID_PIXEL;
     }
 }
 
 // ------------------------------------------------------------- film + regeneration
-// Adds the radiance of every finished path to the film (the film writes of
-// intersection.metal:84-87,111-116,174-178 and shadow.metal:24-27, gathered
-// per path) and replaces the path with the next camera sample
-// (generate.metal:72-121) while samples remain.
+// Adds the radiance of every path finished by the previous iteration to the
+// film (the film writes of intersection.metal:84-87,111-116,174-178 and
+// shadow.metal:24-27, gathered per path) and gives its slot the next camera
+// sample (generate.metal:72-121): entry j of D[p^1] takes path id nextPath + j
+// and queue position nQ[p] + j, so no counter is contended.
 __global__ void __launch_bounds__(256) k_film_regen(Context ctx, PathPool pool, FrameParams fp, Counters *cnt,
-                                                    uint32_t cur) {
-    if (blockIdx.x == 0 && threadIdx.x == 0) cnt->traceWork = 0;
-    const uint32_t n = cnt->nDone;
-    for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
-        const uint32_t slot = pool.qDone[i];
+                                                    uint32_t p) {
+    if (blockIdx.x == 0 && threadIdx.x == 0) {  // counters of later stages of this iteration
+        cnt->nQ[p ^ 1u] = 0;
+        cnt->nD[p] = 0;
+        cnt->nShadow = 0;
+        cnt->traceWork = 0;
+        cnt->shadowWork = 0;
+    }
+    const uint32_t n = cnt->nD[p ^ 1u];
+    const uint32_t base = cnt->nQ[p];
+    const unsigned long long first = cnt->nextPath, end = cnt->endPath;
+    const uint32_t *done = pool.qDone[p ^ 1u];
+    uint32_t *q = pool.q[p];
+    uint32_t finished = 0;
+    for (uint32_t j = blockIdx.x * blockDim.x + threadIdx.x; j < n; j += gridDim.x * blockDim.x) {
+        const uint32_t slot = done[j];
         const uint32_t px = pool.pixel[slot];
         if (px != INVALID_PIXEL) {
             const float4 L = pool.L[slot];
@@ -54,19 +67,12 @@ __global__ void __launch_bounds__(256) k_film_regen(Context ctx, PathPool pool, 
             } else {
                 atomicAdd(&fp.film[px], make_float4(L.x, L.y, L.z, 1.0f));
             }
-            warpAdd64(&cnt->pathsDone, 1u);
+            finished++;
         }
-        // one 64-bit atomic per warp for the new path ids
-        const unsigned mask = __activemask();
-        const int leader = __ffs(mask) - 1;
-        const int lane = threadIdx.x & 31;
-        unsigned long long base = 0;
-        if (lane == leader) base = atomicAdd(&cnt->nextPath, (unsigned long long)__popc(mask));
-        base = __shfl_sync(mask, base, leader);
-        const uint64_t id = base + (uint64_t)__popc(mask & ((1u << lane) - 1u));
-        if (id < cnt->endPath) {
+        const unsigned long long id = first + j;
+        if (id < end) {
             const uint32_t sample = (uint32_t)(id / fp.numPixels);
-            const uint32_t r = (uint32_t)(id - (uint64_t)sample * fp.numPixels);
+            const uint32_t r = (uint32_t)(id - (unsigned long long)sample * fp.numPixels);
             uint32_t x, y;
             blockLinearToPixel(r, fp.width, fp.height, x, y);
             PrngState prng;
@@ -80,28 +86,21 @@ __global__ void __launch_bounds__(256) k_film_regen(Context ctx, PathPool pool, 
             pool.pixel[slot] = y * fp.width + x;
             pool.sample[slot] = sample;
             pool.meta[slot] = (uint32_t)RayFlagsCamera << 16;
-            const uint32_t k = warpAppend(&cnt->nQ[cur]);
-            if (k < pool.capacity) pool.q[cur][k] = slot;
-            else atomicOr(&cnt->errors, ERR_QUEUE_OVERFLOW);
+            q[base + j] = slot;
         } else {
             pool.pixel[slot] = INVALID_PIXEL;
         }
     }
+    blockAdd64(&cnt->pathsDone, finished);
 }
 
 // ------------------------------------------------------------- traversal
 // Persistent warps pull 32 queue entries at a time (Aila & Laine 2009).
 __global__ void __launch_bounds__(128) k_trace_closest(const BvhNode *__restrict__ nodes,
                                                        const float4 *__restrict__ tris, PathPool pool,
-                                                       Counters *cnt, uint32_t cur) {
-    if (blockIdx.x == 0 && threadIdx.x == 0) {
-        cnt->nQ[cur ^ 1u] = 0;
-        cnt->nDone = 0;
-        cnt->nShadow = 0;
-        cnt->shadowWork = 0;
-    }
-    const uint32_t n = cnt->nQ[cur];
-    const uint32_t *q = pool.q[cur];
+                                                       Counters *cnt, uint32_t p) {
+    const uint32_t n = activeCount(cnt, p);
+    const uint32_t *q = pool.q[p];
     const int lane = threadIdx.x & 31;
     while (true) {
         uint32_t base = 0;
@@ -123,12 +122,15 @@ __global__ void __launch_bounds__(128) k_trace_closest(const BvhNode *__restrict
 }
 
 // raytraceAny fused with handleShadowRays (shadow.metal:6-29): an unoccluded
-// shadow ray adds its weight to its path's radiance.
+// shadow ray adds its weight to its path's radiance.  Thread 0 also advances
+// nextPath past the camera samples this iteration consumed.
 __global__ void __launch_bounds__(128) k_trace_shadow(const BvhNode *__restrict__ nodes,
                                                       const float4 *__restrict__ tris, PathPool pool,
-                                                      Counters *cnt) {
+                                                      Counters *cnt, uint32_t p) {
     const uint32_t n = cnt->nShadow;
+    if (blockIdx.x == 0 && threadIdx.x == 0) cnt->nextPath += newPaths(cnt, p);
     const int lane = threadIdx.x & 31;
+    uint32_t traced = 0;
     while (true) {
         uint32_t base = 0;
         if (lane == 0) base = atomicAdd(&cnt->shadowWork, 32u);
@@ -136,6 +138,7 @@ __global__ void __launch_bounds__(128) k_trace_shadow(const BvhNode *__restrict_
         if (base >= n) break;
         const uint32_t i = base + lane;
         if (i < n) {
+            traced++;
             const float4 o = pool.shO[i];
             const float4 d = pool.shD[i];
             const bool occluded = traceAny(nodes, tris, xyz(o), xyz(d), SHADOW_EPS, o.w, &cnt->errors);
@@ -149,11 +152,8 @@ __global__ void __launch_bounds__(128) k_trace_shadow(const BvhNode *__restrict_
                 pool.L[slot] = L;
             }
         }
-        if (lane == 0) {
-            const uint32_t done = min(32u, n - base);
-            atomicAdd((unsigned long long *)&cnt->shadowRays, (unsigned long long)done);
-        }
     }
+    blockAdd64(&cnt->shadowRays, traced);
 }
 
 // ------------------------------------------------------------- environment map
@@ -255,8 +255,8 @@ cudaError_t rmdLaunchTraceClosest(const BvhNode *nodes, const float4 *tris, cons
     return cudaGetLastError();
 }
 cudaError_t rmdLaunchTraceShadow(const BvhNode *nodes, const float4 *tris, const PathPool &pool, Counters *cnt,
-                                 int blocks, cudaStream_t s) {
-    k_trace_shadow<<<blocks, 128, 0, s>>>(nodes, tris, pool, cnt);
+                                 uint32_t cur, int blocks, cudaStream_t s) {
+    k_trace_shadow<<<blocks, 128, 0, s>>>(nodes, tris, pool, cnt, cur);
     return cudaGetLastError();
 }
 cudaError_t rmdLaunchEnvmapReduce(float *mip, int cur, cudaStream_t s) {

@@ -13,7 +13,7 @@ cudaError_t rmdLaunchFilmRegen(const rmd::Context &ctx, const rmd::PathPool &poo
 cudaError_t rmdLaunchTraceClosest(const rmd::BvhNode *nodes, const float4 *tris, const rmd::PathPool &pool,
                                   rmd::Counters *cnt, uint32_t cur, int blocks, cudaStream_t s);
 cudaError_t rmdLaunchTraceShadow(const rmd::BvhNode *nodes, const float4 *tris, const rmd::PathPool &pool,
-                                 rmd::Counters *cnt, int blocks, cudaStream_t s);
+                                 rmd::Counters *cnt, uint32_t cur, int blocks, cudaStream_t s);
 cudaError_t rmdLaunchEnvmapReduce(float *mip, int cur, cudaStream_t s);
 cudaError_t rmdLaunchEnvmapNormalize(const float *sum, float *pdfs, uint32_t gridSize, cudaStream_t s);
 cudaError_t rmdLaunchFilmResolve(const float4 *film, const double *film64, int fp64, float *out, uint32_t numPixels,

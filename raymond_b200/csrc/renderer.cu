@@ -99,7 +99,7 @@ struct rmd_scene {
 struct rmd_renderer {
     rmd_scene *scene = nullptr;
     uint32_t width = 0, height = 0, capacity = 0;
-    DevBuf rayO, rayD, tp, L, rng, pixel, sample, meta, hit, hitInst, q0, q1, qDone, shO, shD, shW;
+    DevBuf rayO, rayD, tp, L, rng, pixel, sample, meta, hit, hitInst, q0, q1, qDone0, qDone1, shO, shD, shW;
     DevBuf counters, film, film64, resolve;
     Counters *hostCounters = nullptr;  // pinned
     Context dctx{};
@@ -542,7 +542,8 @@ static rmd_status allocatePool(rmd_renderer *r) {
     RMD_CUDA(r->hitInst.alloc(P * 4));
     RMD_CUDA(r->q0.alloc(P * 4));
     RMD_CUDA(r->q1.alloc(P * 4));
-    RMD_CUDA(r->qDone.alloc(P * 4));
+    RMD_CUDA(r->qDone0.alloc(P * 4));
+    RMD_CUDA(r->qDone1.alloc(P * 4));
     RMD_CUDA(r->shO.alloc(P * 16));
     RMD_CUDA(r->shD.alloc(P * 16));
     RMD_CUDA(r->shW.alloc(P * 16));
@@ -564,7 +565,8 @@ static PathPool poolView(rmd_renderer *r) {
     p.hitInst = r->hitInst.as<uint32_t>();
     p.q[0] = r->q0.as<uint32_t>();
     p.q[1] = r->q1.as<uint32_t>();
-    p.qDone = r->qDone.as<uint32_t>();
+    p.qDone[0] = r->qDone0.as<uint32_t>();
+    p.qDone[1] = r->qDone1.as<uint32_t>();
     p.shO = r->shO.as<float4>();
     p.shD = r->shD.as<float4>();
     p.shW = r->shW.as<float4>();
@@ -696,7 +698,7 @@ rmd_status rmd_render(rmd_renderer *r, const rmd_render_settings *s) {
             RMD_CUDA(cudaLaunchKernel((const void *)scene->jit.shade, dim3(sb), dim3(128), shadeArgs, 0, st));
             RMD_CUDA(r->stageEvent(evi++, e));
             RMD_CUDA(cudaEventRecord(e, st));
-            RMD_CUDA(rmdLaunchTraceShadow(scene->bvhNodes.as<BvhNode>(), scene->bvhTris.as<float4>(), pool, cnt, tb, st));
+            RMD_CUDA(rmdLaunchTraceShadow(scene->bvhNodes.as<BvhNode>(), scene->bvhTris.as<float4>(), pool, cnt, cur, tb, st));
             RMD_CUDA(r->stageEvent(evi++, e));
             RMD_CUDA(cudaEventRecord(e, st));
             cur ^= 1u;
