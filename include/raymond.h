@@ -314,6 +314,32 @@ rmd_status rmd_film_samples(const rmd_renderer *r, uint64_t *samples);
  * (RendererCounters, Renderer.swift:13-268). */
 rmd_status rmd_renderer_stats(const rmd_renderer *r, rmd_stats *out);
 
+/* ----------------------------------------------------- allocation-free render */
+/*
+ * No counterpart in the reference.  For callers that cannot allocate GPU
+ * memory at render time (a plug-in whose host application owns every device
+ * allocation, a real-time loop that must not pay allocation latency, a
+ * process held to a fixed memory budget): renders like rmd_render but keeps
+ * its path pool, queues and counters in one fixed device array compiled into
+ * the library (RMD_NOALLOC_MAX_PATHS paths, about 5.5 MB, reserved on every
+ * GPU that loads the library until it is unloaded) and never calls
+ * cudaMalloc, cudaFree or any other allocating routine.
+ *
+ * film: caller-owned DEVICE memory of width * height float4 (RGB radiance
+ * sums and a path count per pixel, row-major from the top-left pixel); the
+ * call adds to it, so clear it first for a fresh image.  settings->first_sample
+ * must be >= 0 and film_fp64 must be 0.  pool_size: paths in flight, 0 for
+ * RMD_NOALLOC_MAX_PATHS; larger values are rejected with
+ * RMD_ERROR_INVALID_ARGUMENT.  The first call on a device looks up the
+ * array's device address; make that first call before any stream capture.
+ * All calls share the array: calls whose GPU work overlaps (several streams or
+ * threads) race and corrupt each other, so serialise them.  Runs on the
+ * scene's stream and returns when the frame is finished.
+ */
+#define RMD_NOALLOC_MAX_PATHS 32768
+rmd_status rmd_render_noalloc(rmd_scene *scene, const rmd_camera *camera, uint32_t width, uint32_t height,
+                              const rmd_render_settings *settings, float *film, uint32_t pool_size);
+
 #ifdef __cplusplus
 }
 #endif

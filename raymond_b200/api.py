@@ -27,7 +27,7 @@ EXPORTS = [
     "rmd_last_error", "rmd_version", "rmd_context_create", "rmd_context_destroy", "rmd_scene_create",
     "rmd_scene_destroy", "rmd_scene_info", "rmd_renderer_create", "rmd_renderer_destroy", "rmd_renderer_set_size",
     "rmd_renderer_reset", "rmd_renderer_set_camera", "rmd_render", "rmd_film_read", "rmd_film_read_f64",
-    "rmd_film_samples", "rmd_renderer_stats",
+    "rmd_film_samples", "rmd_renderer_stats", "rmd_render_noalloc",
     "rmd_test_prng", "rmd_test_trace", "rmd_test_material_eval", "rmd_test_generate_source", "rmd_test_jit_compile",
 ]
 
@@ -69,6 +69,8 @@ def lib() -> C.CDLL:
         "rmd_film_read_f64": ([vp, P(C.c_double)], C.c_int32),
         "rmd_film_samples": ([vp, P(C.c_uint64)], C.c_int32),
         "rmd_renderer_stats": ([vp, P(Stats)], C.c_int32),
+        "rmd_render_noalloc": ([vp, P(_abi.Camera), C.c_uint32, C.c_uint32, P(RenderSettings), C.c_void_p,
+                                C.c_uint32], C.c_int32),
         "rmd_test_prng": ([C.c_uint32, C.c_uint64, C.c_uint64, C.c_int32, P(C.c_float)], C.c_int32),
         "rmd_test_trace": ([vp, P(C.c_float), C.c_int32, C.c_int32, P(C.c_float), P(C.c_uint32)], C.c_int32),
         "rmd_test_material_eval": ([vp, C.c_int32, P(C.c_float), C.c_int32, P(C.c_float)], C.c_int32),
@@ -208,6 +210,17 @@ class Renderer:
             self.close()
         except Exception:
             pass
+
+
+def render_noalloc(scene: Scene, camera: dict[str, Any], width: int, height: int, film_device_ptr: int, spp: int,
+                   first_sample: int, max_depth: int = 8, sampling_mode: int = _abi.SAMPLING_MIS,
+                   rng: int = _abi.RNG_PCG32, seed: int = 1, pool_size: int = 0) -> None:
+    """rmd_render_noalloc: adds `spp` samples to a caller-owned device film of
+    width*height float4 (RGB sums, path count) without allocating memory."""
+    cam = _abi.make_camera(camera)
+    s = RenderSettings(spp, max_depth, sampling_mode, rng, seed, first_sample, 0, 0)
+    check(lib().rmd_render_noalloc(scene.h, C.byref(cam), width, height, C.byref(s), C.c_void_p(film_device_ptr),
+                                   pool_size))
 
 
 def generate_source(scene: dict[str, Any] | SceneDesc, hoist: bool = True) -> str:

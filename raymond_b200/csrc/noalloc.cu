@@ -1,0 +1,180 @@
+// rmd_render_noalloc: rendering without any device or host allocation.
+//
+// Some callers cannot allocate GPU memory when they want a frame: a plug-in
+// hosted by an application that owns every device allocation and forbids new
+// ones, a real-time loop that must not pay allocation latency or fragment
+// the heap mid-session, or a process held to a fixed memory budget.  For
+// them this entry point runs the same wavefront kernels as rmd_render, but
+// the path pool, queues and counters live in one file-scope device array of
+// fixed size instead of memory owned by an rmd_renderer; the caller passes
+// the scene (created earlier) and its own device film.
+//
+// The array is defined in this file and reserved on every GPU that loads the
+// library, for as long as the library stays loaded.  Host code cannot use the
+// array's name as a device address: its address is fetched once per device
+// with cudaGetSymbolAddress and handed to the kernels.  All calls share the
+// array, so two calls whose work overlaps on the GPU (different streams,
+// other threads) corrupt each other.
+#include <cuda_runtime.h>
+
+#include <cstring>
+#include <mutex>
+#include <string>
+#include <algorithm>
+
+#include "../../include/raymond.h"
+#include "kernels.h"
+#include "scene_view.h"
+
+namespace {
+
+using namespace rmd;
+
+constexpr uint32_t kMaxPaths = RMD_NOALLOC_MAX_PATHS;
+// per path: rayO, rayD, tp, L, hit, shO, shD, shW (16 B each), rng (8 B),
+// pixel, sample, meta, hitInst, q[2], qDone[2] (4 B each)
+constexpr size_t kBytesPerPath = 8 * 16 + 8 + 8 * 4;
+constexpr size_t kArrays = 17;
+constexpr size_t kScratchBytes = 256 + kMaxPaths * kBytesPerPath + kArrays * 256;
+
+static __device__ __align__(256) unsigned char g_noallocScratch[kScratchBytes];
+
+std::mutex g_mutex;
+void *g_scratch[64] = {};  // device address of g_noallocScratch per device
+
+// Carves the counters and the path arrays out of the scratch block.
+struct Carver {
+    unsigned char *p;
+    template <class T>
+    T *take(size_t count) {
+        T *r = reinterpret_cast<T *>(p);
+        p += (count * sizeof(T) + 255) & ~size_t(255);
+        return r;
+    }
+};
+
+rmd_status cudaFail(cudaError_t e, const char *what) {
+    std::string msg = std::string("rmd_render_noalloc: ") + what + ": " + cudaGetErrorString(e);
+    return rmdhost::setLastError(RMD_ERROR_CUDA, msg.c_str());
+}
+
+}  // namespace
+
+extern "C" rmd_status rmd_render_noalloc(rmd_scene *scene, const rmd_camera *camera, uint32_t width, uint32_t height,
+                                         const rmd_render_settings *s, float *film, uint32_t pool_size) {
+    rmdhost::SceneView v;
+    if (!rmdhost::sceneView(scene, v) || !camera || !s || !film)
+        return rmdhost::setLastError(RMD_ERROR_INVALID_ARGUMENT, "rmd_render_noalloc: NULL argument");
+    if (width == 0 || height == 0 || width > 65535 || height > 65535)
+        return rmdhost::setLastError(RMD_ERROR_INVALID_ARGUMENT, "rmd_render_noalloc: width/height must be 1..65535");
+    if (pool_size > kMaxPaths)
+        return rmdhost::setLastError(RMD_ERROR_INVALID_ARGUMENT,
+                                     "rmd_render_noalloc: pool_size exceeds RMD_NOALLOC_MAX_PATHS (32768)");
+    if (s->max_depth == 0 || s->max_depth > 65535 || s->sampling_mode > 2 || s->rng > 1 || s->film_fp64)
+        return rmdhost::setLastError(RMD_ERROR_INVALID_ARGUMENT,
+                                     "rmd_render_noalloc: invalid settings (film_fp64 is not supported here)");
+    if (s->first_sample < 0 || (uint64_t)s->first_sample + s->spp > 0xffffffffull)
+        return rmdhost::setLastError(RMD_ERROR_INVALID_ARGUMENT, "rmd_render_noalloc: first_sample must be >= 0");
+    if (v.device < 0 || v.device >= 64)
+        return rmdhost::setLastError(RMD_ERROR_INVALID_ARGUMENT, "rmd_render_noalloc: device index >= 64");
+    cudaError_t e = cudaSetDevice(v.device);
+    if (e != cudaSuccess) return cudaFail(e, "cudaSetDevice");
+
+    void *base;
+    {
+        std::lock_guard<std::mutex> lock(g_mutex);
+        if (!g_scratch[v.device]) {  // first call on this device: resolve the array's device address
+            void *ptr = nullptr;
+            e = cudaGetSymbolAddress(&ptr, g_noallocScratch);
+            if (e != cudaSuccess) return cudaFail(e, "cudaGetSymbolAddress");
+            g_scratch[v.device] = ptr;
+        }
+        base = g_scratch[v.device];
+    }
+    const uint32_t P = pool_size ? pool_size : kMaxPaths;
+    Carver c{static_cast<unsigned char *>(base)};
+    Counters *cnt = c.take<Counters>(1);
+    PathPool pool;
+    pool.rayO = c.take<float4>(P);
+    pool.rayD = c.take<float4>(P);
+    pool.tp = c.take<float4>(P);
+    pool.L = c.take<float4>(P);
+    pool.rng = c.take<uint2>(P);
+    pool.pixel = c.take<uint32_t>(P);
+    pool.sample = c.take<uint32_t>(P);
+    pool.meta = c.take<uint32_t>(P);
+    pool.hit = c.take<float4>(P);
+    pool.hitInst = c.take<uint32_t>(P);
+    pool.q[0] = c.take<uint32_t>(P);
+    pool.q[1] = c.take<uint32_t>(P);
+    pool.qDone[0] = c.take<uint32_t>(P);
+    pool.qDone[1] = c.take<uint32_t>(P);
+    pool.shO = c.take<float4>(P);
+    pool.shD = c.take<float4>(P);
+    pool.shW = c.take<float4>(P);
+    pool.capacity = P;
+
+    Context ctx = v.ctx;
+    for (int k = 0; k < 4; k++)
+        ctx.cameraTransform[k] = make_float4(camera->transform[4 * k], camera->transform[4 * k + 1],
+                                             camera->transform[4 * k + 2], camera->transform[4 * k + 3]);
+    ctx.nearClip = camera->near_clip;
+    ctx.farClip = camera->far_clip;
+    ctx.focalLength = camera->focal_length;
+    ctx.shift = make_float2(camera->shift[0], camera->shift[1]);
+
+    const uint64_t numPixels = (uint64_t)width * height;
+    const uint64_t numPaths = (uint64_t)s->spp * numPixels;
+    if (numPaths == 0) return RMD_OK;
+    FrameParams fp{};
+    fp.width = width;
+    fp.height = height;
+    fp.numPixels = (uint32_t)numPixels;
+    fp.maxDepth = s->max_depth;
+    fp.samplingMode = s->sampling_mode;
+    fp.rngMode = s->rng;
+    fp.seed = s->seed;
+    fp.filmFp64 = 0;
+    fp.film = reinterpret_cast<float4 *>(film);
+    fp.film64 = nullptr;
+    const uint64_t firstPath = (uint64_t)s->first_sample * numPixels;
+    ShadeParams sp;
+    sp.ctx = ctx;
+    sp.pool = pool;
+    sp.fp = fp;
+    sp.counters = cnt;
+    void *shadeArgs[] = {&sp};
+    const cudaStream_t st = v.stream;
+    const int tb = v.smCount * 8;
+    const int rb = (int)std::min<uint32_t>((P + 255) / 256, (uint32_t)v.smCount * 8);
+
+    if ((e = rmdLaunchFrameInit(pool, cnt, firstPath, firstPath + numPaths, st)) != cudaSuccess)
+        return cudaFail(e, "frame init");
+    const uint64_t maxIters = ((numPaths + P - 1) / P + 1) * ((uint64_t)s->max_depth + 1) + 8;
+    uint64_t it = 0;
+    uint32_t cur = 0;
+    Counters h;
+    while (true) {
+        for (int k = 0; k < 4; k++, it++) {
+            if ((e = rmdLaunchFilmRegen(ctx, pool, fp, cnt, cur, rb, st)) != cudaSuccess) return cudaFail(e, "film");
+            if ((e = rmdLaunchTraceClosest(v.nodes, v.tris, pool, cnt, cur, tb, st)) != cudaSuccess)
+                return cudaFail(e, "trace");
+            sp.cur = cur;
+            if ((e = cudaLaunchKernel((const void *)v.shade, dim3(v.shadeBlocks), dim3(128), shadeArgs, 0, st)) !=
+                cudaSuccess)
+                return cudaFail(e, "shade");
+            if ((e = rmdLaunchTraceShadow(v.nodes, v.tris, pool, cnt, cur, tb, st)) != cudaSuccess)
+                return cudaFail(e, "shadow");
+            cur ^= 1u;
+        }
+        // pageable stack destination: no pinned staging buffer is allocated
+        if ((e = cudaMemcpyAsync(&h, cnt, sizeof(Counters), cudaMemcpyDeviceToHost, st)) != cudaSuccess)
+            return cudaFail(e, "counters");
+        if ((e = cudaStreamSynchronize(st)) != cudaSuccess) return cudaFail(e, "synchronize");
+        if (h.errors) return rmdhost::setLastError(RMD_ERROR_QUEUE_OVERFLOW, "rmd_render_noalloc: device error flags");
+        if (h.pathsDone >= numPaths) break;
+        if (it > maxIters)
+            return rmdhost::setLastError(RMD_ERROR_WATCHDOG, "rmd_render_noalloc: render did not drain");
+    }
+    return RMD_OK;
+}

@@ -18,6 +18,7 @@
 #include "device/wavefront.cuh"
 #include "jit.h"
 #include "kernels.h"
+#include "scene_view.h"
 
 using namespace rmd;
 
@@ -225,6 +226,22 @@ int occupancyBlocks(const void *fn, int threads, int smCount) {
 }
 
 }  // namespace
+
+namespace rmdhost {
+bool sceneView(const rmd_scene *s, SceneView &v) {
+    if (!s) return false;
+    v.ctx = s->dctx;
+    v.nodes = s->bvhNodes.as<BvhNode>();
+    v.tris = s->bvhTris.as<float4>();
+    v.shade = s->jit.shade;
+    v.shadeBlocks = s->shadeBlocks;
+    v.stream = s->ctx->stream;
+    v.device = s->ctx->device;
+    v.smCount = s->ctx->smCount;
+    return true;
+}
+rmd_status setLastError(rmd_status status, const char *msg) { return fail(status, msg); }
+}  // namespace rmdhost
 
 // --------------------------------------------------------------------- C ABI
 extern "C" {
