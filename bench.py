@@ -156,6 +156,7 @@ def main():
     ap.add_argument("--height", type=int, default=H, help="override (profiling runs only)")
     ap.add_argument("--spp", type=int, default=SPP, help="override (profiling runs only)")
     ap.add_argument("--no-e2e", action="store_true")
+    ap.add_argument("--no-autotune", action="store_true")
     args = ap.parse_args()
     globals().update(W=args.width, H=args.height, SPP=args.spp)
     if args.impl == "reference":
@@ -177,6 +178,9 @@ def main():
     scene = api.Scene(ctx, desc)
     build_s = time.perf_counter() - t0
     r = api.Renderer(scene, W, H, pool_size=args.pool)
+    t0 = time.perf_counter()
+    tune = None if args.no_autotune else r.autotune(spp=SPP, max_depth=DEPTH, seed=SEED)
+    tune_s = time.perf_counter() - t0
     cam = desc.scene["camera"]
     film_host = np.zeros((H, W, 3), np.float32)
 
@@ -255,6 +259,7 @@ def main():
         "gpu_launches": int(tot["iterations"] * 4 + args.steps),
         "clocks": clocks,
         "scene_build_s": build_s,
+        "autotune": dict(tune, seconds=tune_s) if tune else None,
     }
     if not args.no_cpu_baseline:
         line["cpu_baseline"] = cpu_baseline_sample(desc)

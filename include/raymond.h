@@ -310,6 +310,24 @@ rmd_status rmd_film_read_f64(rmd_renderer *r, double *rgb);
 /* Samples accumulated in the film (frameIndex of Renderer.swift:288). */
 rmd_status rmd_film_samples(const rmd_renderer *r, uint64_t *samples);
 
+/* Launch choices picked by rmd_renderer_autotune. */
+typedef struct rmd_tune_result {
+    uint32_t shade_min_blocks;     /* register budget of the shading kernel (blocks of 128 per SM) */
+    uint32_t trace_blocks_per_sm;  /* persistent traversal blocks per SM */
+    uint32_t pool_size;            /* paths in flight (queue sizes) */
+    uint32_t calibration_spp;
+    double ms_default;             /* calibration render with the previous choices */
+    double ms_best;                /* with the chosen ones */
+} rmd_tune_result;
+
+/* Autotuner.  No counterpart in the reference, which dispatched fixed
+ * 64-thread threadgroups (Renderer.swift:471-474, 616-619).  Times short
+ * calibration renders of this renderer's scene and size with `settings`
+ * (depth, sampling mode, RNG) and keeps the fastest shading-kernel register
+ * budget, traversal grid and path-pool size.  Compiles the shading-kernel
+ * variants it needs (NVRTC, cached on disk).  Clears the film. */
+rmd_status rmd_renderer_autotune(rmd_renderer *r, const rmd_render_settings *settings, rmd_tune_result *out);
+
 /* Per-stage device timings and counters of the last rmd_render
  * (RendererCounters, Renderer.swift:13-268). */
 rmd_status rmd_renderer_stats(const rmd_renderer *r, rmd_stats *out);

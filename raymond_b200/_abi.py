@@ -109,6 +109,11 @@ class RenderSettings(C.Structure):
                 ("film_fp64", C.c_uint32), ("reserved", C.c_uint32)]
 
 
+class TuneResult(C.Structure):
+    _fields_ = [("shade_min_blocks", C.c_uint32), ("trace_blocks_per_sm", C.c_uint32), ("pool_size", C.c_uint32),
+                ("calibration_spp", C.c_uint32), ("ms_default", C.c_double), ("ms_best", C.c_double)]
+
+
 class Stats(C.Structure):
     _fields_ = [("paths", C.c_uint64), ("segments", C.c_uint64), ("shadow_rays", C.c_uint64),
                 ("iterations", C.c_uint64), ("ms_total", C.c_double), ("ms_trace", C.c_double),

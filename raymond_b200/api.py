@@ -27,7 +27,7 @@ EXPORTS = [
     "rmd_last_error", "rmd_version", "rmd_context_create", "rmd_context_destroy", "rmd_scene_create",
     "rmd_scene_destroy", "rmd_scene_info", "rmd_renderer_create", "rmd_renderer_destroy", "rmd_renderer_set_size",
     "rmd_renderer_reset", "rmd_renderer_set_camera", "rmd_render", "rmd_film_read", "rmd_film_read_f64",
-    "rmd_film_samples", "rmd_renderer_stats", "rmd_render_noalloc",
+    "rmd_film_samples", "rmd_renderer_stats", "rmd_render_noalloc", "rmd_renderer_autotune",
     "rmd_test_prng", "rmd_test_trace", "rmd_test_material_eval", "rmd_test_generate_source", "rmd_test_jit_compile",
 ]
 
@@ -69,6 +69,7 @@ def lib() -> C.CDLL:
         "rmd_film_read_f64": ([vp, P(C.c_double)], C.c_int32),
         "rmd_film_samples": ([vp, P(C.c_uint64)], C.c_int32),
         "rmd_renderer_stats": ([vp, P(Stats)], C.c_int32),
+        "rmd_renderer_autotune": ([vp, P(RenderSettings), P(_abi.TuneResult)], C.c_int32),
         "rmd_render_noalloc": ([vp, P(_abi.Camera), C.c_uint32, C.c_uint32, P(RenderSettings), C.c_void_p,
                                 C.c_uint32], C.c_int32),
         "rmd_test_prng": ([C.c_uint32, C.c_uint64, C.c_uint64, C.c_int32, P(C.c_float)], C.c_int32),
@@ -194,6 +195,14 @@ class Renderer:
     def set_camera(self, camera: dict[str, Any]) -> None:
         cam = _abi.make_camera(camera)
         check(lib().rmd_renderer_set_camera(self.h, C.byref(cam)))
+
+    def autotune(self, spp: int = 64, max_depth: int = 8, sampling_mode: int = _abi.SAMPLING_MIS,
+                 rng: int = _abi.RNG_PCG32, seed: int = 1) -> dict[str, float]:
+        """Pick launch choices with short calibration renders (clears the film)."""
+        s = RenderSettings(spp, max_depth, sampling_mode, rng, seed, -1, 0, 0)
+        res = _abi.TuneResult()
+        check(lib().rmd_renderer_autotune(self.h, C.byref(s), C.byref(res)))
+        return {k: getattr(res, k) for k, _ in _abi.TuneResult._fields_}
 
     def stats(self) -> dict[str, float]:
         s = Stats()

@@ -157,13 +157,16 @@ std::string ftoa(float v) {
     return s;
 }
 
+// Literals are emitted as placeholders `@L<k>@`; emitTable later replaces each
+// one by a constant (no hoisting, or the same value in every material of the
+// structure group) or by a load P[j] from the material's parameter block.
 struct Emitter {
     bool hoist;
-    std::vector<float> literals;  // this material's parameter block
+    std::vector<float> literals;  // this material's literals in emission order
     std::string lit(float v) {
         if (!hoist) return ftoa(v);
         literals.push_back(v);
-        return "P[" + std::to_string(literals.size() - 1) + "]";
+        return "@L" + std::to_string(literals.size() - 1) + "@";
     }
     std::string vec(const float *v, int n) {
         if (n == 1) return lit(v[0]);
@@ -458,8 +461,11 @@ void emitTable(const rmd_material *mats, int n, bool hoist, const std::string &p
     std::map<std::string, int> groupOf;
     std::vector<std::string> groupBodies;
     std::vector<std::vector<std::string>> groupNames;
+    std::vector<std::vector<int>> groupMembers;
+    std::vector<MaterialCode> codes;
     for (int i = 0; i < n; i++) {
-        MaterialCode mc = emitMaterial(mats[i], hoist);
+        codes.push_back(emitMaterial(mats[i], hoist));
+        const MaterialCode &mc = codes.back();
         if (emissive) emissive->push_back(mc.emissive);
         int g;
         auto it = groupOf.find(mc.body);
@@ -468,24 +474,56 @@ void emitTable(const rmd_material *mats, int n, bool hoist, const std::string &p
             groupOf[mc.body] = g;
             groupBodies.push_back(mc.body);
             groupNames.push_back({});
+            groupMembers.push_back({});
         } else {
             g = it->second;
         }
         groupNames[g].push_back(mats[i].name ? mats[i].name : "");
+        groupMembers[g].push_back(i);
         table.group.push_back((uint32_t)g);
-        table.offset.push_back((uint32_t)mod.params.size());
-        mod.params.insert(mod.params.end(), mc.literals.begin(), mc.literals.end());
     }
+    table.offset.assign(n, 0);
     groups = (int)groupBodies.size();
     const bool inlineFns = groups <= 8;
     for (int g = 0; g < groups; g++) {
+        // literals equal in every member become constants; the rest are hoisted
+        const std::vector<int> &mem = groupMembers[g];
+        const size_t nl = codes[mem[0]].literals.size();
+        std::vector<int> slot(nl, -1);
+        int varying = 0;
+        for (size_t k = 0; k < nl; k++) {
+            const float v0 = codes[mem[0]].literals[k];
+            bool uniform = true;
+            for (int m : mem) {
+                const float v = codes[m].literals[k];
+                if (!(v == v0 || (v != v && v0 != v0)) || std::signbit(v) != std::signbit(v0)) uniform = false;
+            }
+            if (!uniform) slot[k] = varying++;
+        }
+        for (int m : mem) {
+            table.offset[m] = (uint32_t)mod.params.size();
+            for (size_t k = 0; k < nl; k++)
+                if (slot[k] >= 0) mod.params.push_back(codes[m].literals[k]);
+        }
+        std::string body;
+        const std::string &tpl = groupBodies[g];
+        for (size_t i = 0; i < tpl.size();) {
+            if (tpl[i] == '@' && i + 1 < tpl.size() && tpl[i + 1] == 'L') {
+                const size_t end = tpl.find('@', i + 2);
+                const size_t k = std::stoul(tpl.substr(i + 2, end - i - 2));
+                body += slot[k] >= 0 ? "P[" + std::to_string(slot[k]) + "]" : ftoa(codes[mem[0]].literals[k]);
+                i = end + 1;
+            } else {
+                body += tpl[i++];
+            }
+        }
         functions += "// materials:";
         for (size_t k = 0; k < groupNames[g].size() && k < 8; k++) functions += " " + groupNames[g][k];
         if (groupNames[g].size() > 8) functions += " ... (" + std::to_string(groupNames[g].size()) + ")";
         functions += "\n";
         functions += std::string("__device__ ") + (inlineFns ? "__forceinline__" : "__noinline__") + " void " + prefix +
                      std::to_string(g) + "(const float *__restrict__ P, const Context &ctx, ShadingContext &shading) {\n" +
-                     groupBodies[g] + "}\n\n";
+                     body + "}\n\n";
     }
 }
 

@@ -79,7 +79,7 @@ __device__ __forceinline__ bool shadePath(const ShadeParams &p, uint32_t slot) {
         }
 
         if (fp.samplingMode != 0u) {  // NEE, intersection.metal:149-181
-            LightSample nee = lightsSample(ctx, shading, prng);
+            LightSample nee = lightsSample(ctx, shading.position, shading.rayFlags, prng);
             float bsdfPdf;
             const float3 bsdf = shading.material.evaluate(shading.wo, nee.direction, shNormal, shading.trueNormal, bsdfPdf);
             const float3 contribution = nee.weight * bsdf * rayWeight;
@@ -134,7 +134,10 @@ __device__ __forceinline__ bool shadePath(const ShadeParams &p, uint32_t slot) {
 
 }  // namespace rmd
 
-extern "C" __global__ void __launch_bounds__(128) rmd_shade(const __grid_constant__ rmd::ShadeParams p) {
+#ifndef RMD_SHADE_MIN_BLOCKS
+#define RMD_SHADE_MIN_BLOCKS 1
+#endif
+extern "C" __global__ void __launch_bounds__(128, RMD_SHADE_MIN_BLOCKS) rmd_shade(const __grid_constant__ rmd::ShadeParams p) {
     const unsigned n = rmd::activeCount(p.counters, p.cur);
     const unsigned *q = p.pool.q[p.cur];
     unsigned segments = 0;

@@ -233,8 +233,11 @@ RMD_HD int upperBound(const float *buf, int count, float value) {
     return left;
 }
 
-// Lights.hpp:43-93 with the per-type samplers of lights/*.metal inlined.
-static __device__ __noinline__ LightSample lightsSample(const Context &ctx, const ShadingContext &shading, PrngState &prng) {
+// Lights.hpp:43-93 with the per-type samplers of lights/*.metal inlined.  Of the
+// caller's shading context only the position and ray flags are read (the
+// reference copies just these two into lightShading, Lights.hpp:47-49).
+static __device__ __noinline__ LightSample lightsSample(const Context &ctx, float3 position, uint32_t rayFlags,
+                                                       PrngState &prng) {
     int sampled = prng.sampleInt(ctx.numLightsTotal);
     LightSample s;
     s.isLight = false;
@@ -248,8 +251,8 @@ static __device__ __noinline__ LightSample lightsSample(const Context &ctx, cons
     ShadingContext ls;
     ls.uv = ls.generated = ls.object = ls.normal = ls.trueNormal = ls.tu = ls.tv = ls.rnd = ls.wo = f3(0.0f);
     ls.distance = 0.0f;
-    ls.rayFlags = shading.rayFlags;
-    ls.position = shading.position;
+    ls.rayFlags = rayFlags;
+    ls.position = position;
     if (sampled == 0) {  // Lights.hpp:98-116
         s.direction = worldLightSample(ctx, prng.sample2d(), s.pdf);
         s.distance = inf_f();

@@ -58,10 +58,10 @@ const std::vector<const char *> &options() {
 
 }  // namespace
 
-std::string compileModule(const std::string &source, JitModule &out) {
+std::string compileModule(const std::string &source, JitModule &out, const std::vector<std::string> &extraDefines) {
     std::vector<char> cubin;
     const auto t0 = std::chrono::steady_clock::now();
-    std::string err = compileCubin(source, cubin, out.log, out.fromCache);
+    std::string err = compileCubin(source, cubin, out.log, out.fromCache, extraDefines);
     if (!err.empty()) return err;
     cudaError_t e = cudaLibraryLoadData(&out.library, cubin.data(), nullptr, nullptr, 0, nullptr, nullptr, 0);
     if (e != cudaSuccess) return std::string("cudaLibraryLoadData: ") + cudaGetErrorString(e);
@@ -73,12 +73,14 @@ std::string compileModule(const std::string &source, JitModule &out) {
     return "";
 }
 
-std::string compileCubin(const std::string &source, std::vector<char> &cubin, std::string &logOut, bool &fromCache) {
+std::string compileCubin(const std::string &source, std::vector<char> &cubin, std::string &logOut, bool &fromCache,
+                         const std::vector<std::string> &extraDefines) {
     fromCache = false;
     int major = 0, minor = 0;
     nvrtcVersion(&major, &minor);
     std::string key = source;
     for (auto o : options()) key += o;
+    for (const std::string &d : extraDefines) key += d;
     key += std::to_string(major) + "." + std::to_string(minor);
     for (int i = 0; i < kNumEmbeddedHeaders; i++) key += kEmbeddedHeaders[i].source;
     char hex[32];
@@ -113,6 +115,7 @@ std::string compileCubin(const std::string &source, std::vector<char> &cubin, st
         if (r != NVRTC_SUCCESS) return std::string("nvrtcCreateProgram: ") + nvrtcGetErrorString(r);
         std::vector<const char *> opts = options();
         if (std::getenv("RMD_JIT_VERBOSE")) opts.push_back("--ptxas-options=-v");
+        for (const std::string &d : extraDefines) opts.push_back(d.c_str());
         r = nvrtcCompileProgram(prog, (int)opts.size(), opts.data());
         size_t logSize = 0;
         nvrtcGetProgramLogSize(prog, &logSize);

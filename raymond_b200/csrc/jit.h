@@ -21,9 +21,11 @@ struct JitModule {
 };
 
 // Returns an empty string on success, else the error (NVRTC log included).
-std::string compileModule(const std::string &source, JitModule &out);
+// extraDefines: "-DNAME=VALUE" options (launch-bound and tile choices of the autotuner)
+std::string compileModule(const std::string &source, JitModule &out, const std::vector<std::string> &extraDefines = {});
 void unloadModule(JitModule &m);
 // NVRTC only (no device needed): source -> sm_100a cubin, through the disk cache.
-std::string compileCubin(const std::string &source, std::vector<char> &cubin, std::string &log, bool &fromCache);
+std::string compileCubin(const std::string &source, std::vector<char> &cubin, std::string &log, bool &fromCache,
+                         const std::vector<std::string> &extraDefines = {});
 
 }  // namespace rmdhost

@@ -7,8 +7,10 @@
 #include <chrono>
 #include <cmath>
 #include <cstring>
+#include <map>
 #include <memory>
 #include <string>
+#include <thread>
 #include <vector>
 
 #include "../../include/raymond.h"
@@ -90,16 +92,27 @@ struct rmd_scene {
     DevBuf areaLights, pointLights, sunLights, spotLights, shapeLights;
     DevBuf surfaceTable, lightTable, materialParams;
     DevBuf bvhNodes, bvhTris;
-    rmdhost::JitModule jit;
+    rmdhost::JitModule jit;   // default variant (envmap build, test hooks, default shade kernel)
+    std::string moduleSource;
+    std::map<int, std::unique_ptr<rmdhost::JitModule>> variants;  // shade kernels by minimum blocks per SM
     uint64_t triangles = 0, bvhNodeCount = 0;
     int numSurface = 0, numLight = 0;
     int shadeBlocks = 0, traceBlocks = 0, regenBlocks = 0;
-    ~rmd_scene() { rmdhost::unloadModule(jit); }
+    int defaultMinBlocks = 1;
+    ~rmd_scene() {
+        for (auto &kv : variants) rmdhost::unloadModule(*kv.second);
+        rmdhost::unloadModule(jit);
+    }
 };
 
 struct rmd_renderer {
     rmd_scene *scene = nullptr;
     uint32_t width = 0, height = 0, capacity = 0;
+    // launch choices (rmd_renderer_autotune)
+    cudaKernel_t shade = nullptr;
+    int shadeBlocks = 0;
+    int shadeMinBlocks = 1;
+    int traceBlocksPerSm = 8;
     DevBuf rayO, rayD, tp, L, rng, pixel, sample, meta, hit, hitInst, q0, q1, qDone0, qDone1, shO, shD, shW;
     DevBuf counters, film, film64, resolve;
     Counters *hostCounters = nullptr;  // pinned
@@ -526,8 +539,12 @@ rmd_status rmd_scene_create(rmd_context *ctx, const rmd_scene_desc *d, rmd_scene
     c.focalLength = d->camera.focal_length;
     c.shift = make_float2(d->camera.shift[0], d->camera.shift[1]);
 
-    const std::string err = rmdhost::compileModule(mod.source, s->jit);
+    std::vector<std::string> defs;
+    if (const char *mb = std::getenv("RMD_SHADE_MIN_BLOCKS")) defs.push_back(std::string("-DRMD_SHADE_MIN_BLOCKS=") + mb);
+    const std::string err = rmdhost::compileModule(mod.source, s->jit, defs);
     if (!err.empty()) return fail(RMD_ERROR_NVRTC, err);
+    s->moduleSource = mod.source;
+    s->defaultMinBlocks = std::getenv("RMD_SHADE_MIN_BLOCKS") ? std::atoi(std::getenv("RMD_SHADE_MIN_BLOCKS")) : 1;
     rmd_status r = buildEnvironmentMap(s.get(), d->envmap_exponent);
     if (r != RMD_OK) return r;
     s->shadeBlocks = occupancyBlocks((const void *)s->jit.shade, 128, ctx->smCount);
@@ -610,6 +627,9 @@ rmd_status rmd_renderer_create(rmd_scene *scene, uint32_t width, uint32_t height
     auto r = std::make_unique<rmd_renderer>();
     r->scene = scene;
     r->dctx = scene->dctx;
+    r->shade = scene->jit.shade;
+    r->shadeBlocks = scene->shadeBlocks;
+    r->shadeMinBlocks = scene->defaultMinBlocks;
     r->capacity = pool_size ? pool_size : (1u << 21);
     rmd_status st = allocatePool(r.get());
     if (st != RMD_OK) return st;
@@ -687,9 +707,9 @@ rmd_status rmd_render(rmd_renderer *r, const rmd_render_settings *s) {
     sp.fp = fp;
     sp.counters = cnt;
     void *shadeArgs[] = {&sp};
-    const int tb = ctx->smCount * 8;
+    const int tb = ctx->smCount * r->traceBlocksPerSm;
     const int rb = std::min<int>((r->capacity + 255) / 256, ctx->smCount * 8);
-    const int sb = scene->shadeBlocks;
+    const int sb = r->shadeBlocks;
 
     RMD_CUDA(cudaEventRecord(r->ev[0], st));
     RMD_CUDA(rmdLaunchFrameInit(pool, cnt, firstPath, firstPath + numPaths, st));
@@ -712,7 +732,7 @@ rmd_status rmd_render(rmd_renderer *r, const rmd_render_settings *s) {
             RMD_CUDA(r->stageEvent(evi++, e));
             RMD_CUDA(cudaEventRecord(e, st));
             sp.cur = cur;
-            RMD_CUDA(cudaLaunchKernel((const void *)scene->jit.shade, dim3(sb), dim3(128), shadeArgs, 0, st));
+            RMD_CUDA(cudaLaunchKernel((const void *)r->shade, dim3(sb), dim3(128), shadeArgs, 0, st));
             RMD_CUDA(r->stageEvent(evi++, e));
             RMD_CUDA(cudaEventRecord(e, st));
             RMD_CUDA(rmdLaunchTraceShadow(scene->bvhNodes.as<BvhNode>(), scene->bvhTris.as<float4>(), pool, cnt, cur, tb, st));
@@ -792,6 +812,122 @@ rmd_status rmd_renderer_stats(const rmd_renderer *r, rmd_stats *out) {
     return RMD_OK;
 }
 
+// --------------------------------------------------------------------- autotuner
+static rmd_status ensureVariants(rmd_scene *s, const std::vector<int> &minBlocks) {
+    std::vector<int> missing;
+    for (int mb : minBlocks)
+        if (mb != s->defaultMinBlocks && !s->variants.count(mb)) missing.push_back(mb);
+    // NVRTC is thread-safe: compile the missing variants in parallel, load them serially
+    std::vector<std::vector<char>> cubins(missing.size());
+    std::vector<std::string> errs(missing.size()), logs(missing.size());
+    std::vector<std::thread> th;
+    for (size_t i = 0; i < missing.size(); i++) {
+        th.emplace_back([&, i] {
+            bool cached = false;
+            errs[i] = rmdhost::compileCubin(s->moduleSource, cubins[i], logs[i], cached,
+                                            {"-DRMD_SHADE_MIN_BLOCKS=" + std::to_string(missing[i])});
+        });
+    }
+    for (auto &t : th) t.join();
+    for (size_t i = 0; i < missing.size(); i++) {
+        if (!errs[i].empty()) return fail(RMD_ERROR_NVRTC, errs[i]);
+        auto m = std::make_unique<rmdhost::JitModule>();
+        RMD_CUDA(cudaLibraryLoadData(&m->library, cubins[i].data(), nullptr, nullptr, 0, nullptr, nullptr, 0));
+        RMD_CUDA(cudaLibraryGetKernel(&m->shade, m->library, "rmd_shade"));
+        s->variants[missing[i]] = std::move(m);
+    }
+    return RMD_OK;
+}
+
+static void selectShade(rmd_renderer *r, int mb) {
+    rmd_scene *s = r->scene;
+    cudaKernel_t k = mb == s->defaultMinBlocks ? s->jit.shade : s->variants.at(mb)->shade;
+    r->shade = k;
+    r->shadeMinBlocks = mb;
+    r->shadeBlocks = occupancyBlocks((const void *)k, 128, s->ctx->smCount);
+}
+
+rmd_status rmd_renderer_autotune(rmd_renderer *r, const rmd_render_settings *settings, rmd_tune_result *out) {
+    if (!r || !settings) return fail(RMD_ERROR_INVALID_ARGUMENT, "NULL argument");
+    rmd_scene *s = r->scene;
+    const std::vector<int> mbs = {1, 3, 4, 5, 6};
+    rmd_status st = ensureVariants(s, mbs);
+    if (st != RMD_OK) return st;
+    // calibration: enough paths for several pool generations, capped in time
+    rmd_render_settings cal = *settings;
+    cal.film_fp64 = 0;
+    const uint64_t pixels = (uint64_t)r->width * r->height;
+    cal.spp = (uint32_t)std::max<uint64_t>(1, std::min<uint64_t>(settings->spp, (4ull * r->capacity + pixels - 1) / pixels));
+    cal.first_sample = 1u << 30;  // a sample range the caller does not use
+    auto trial = [&](double &ms) -> rmd_status {
+        double best = 1e30;
+        for (int rep = 0; rep < 2; rep++) {
+            rmd_status e = rmd_render(r, &cal);
+            if (e != RMD_OK) return e;
+            best = std::min(best, r->stats.ms_total);
+        }
+        ms = best;
+        return RMD_OK;
+    };
+    rmd_tune_result res{};
+    double base = 0;
+    if ((st = trial(base)) != RMD_OK) return st;
+    res.ms_default = base;
+    // 1) shading kernel register budget
+    int bestMb = r->shadeMinBlocks;
+    double bestMs = base;
+    for (int mb : mbs) {
+        if (mb == r->shadeMinBlocks) continue;
+        selectShade(r, mb);
+        double ms;
+        if ((st = trial(ms)) != RMD_OK) return st;
+        if (ms < bestMs) {
+            bestMs = ms;
+            bestMb = mb;
+        }
+    }
+    selectShade(r, bestMb);
+    // 2) traversal blocks per SM
+    int bestTb = r->traceBlocksPerSm;
+    for (int tb : {4, 12, 16}) {
+        r->traceBlocksPerSm = tb;
+        double ms;
+        if ((st = trial(ms)) != RMD_OK) return st;
+        if (ms < bestMs) {
+            bestMs = ms;
+            bestTb = tb;
+        }
+    }
+    r->traceBlocksPerSm = bestTb;
+    // 3) paths in flight (queue sizes)
+    const uint32_t cap0 = r->capacity;
+    uint32_t bestCap = cap0;
+    for (uint32_t cap : {cap0 / 2, cap0 * 2}) {
+        if (cap < (1u << 16)) continue;
+        size_t freeB = 0, totalB = 0;
+        if (cudaMemGetInfo(&freeB, &totalB) != cudaSuccess || (size_t)cap * 176 > freeB / 2) continue;
+        r->capacity = cap;
+        if ((st = allocatePool(r)) != RMD_OK) return st;
+        double ms;
+        if ((st = trial(ms)) != RMD_OK) return st;
+        if (ms < bestMs) {
+            bestMs = ms;
+            bestCap = cap;
+        }
+    }
+    if (r->capacity != bestCap) {
+        r->capacity = bestCap;
+        if ((st = allocatePool(r)) != RMD_OK) return st;
+    }
+    res.shade_min_blocks = (uint32_t)r->shadeMinBlocks;
+    res.trace_blocks_per_sm = (uint32_t)r->traceBlocksPerSm;
+    res.pool_size = r->capacity;
+    res.ms_best = bestMs;
+    res.calibration_spp = cal.spp;
+    if (out) *out = res;
+    return rmd_renderer_reset(r);
+}
+
 // --------------------------------------------------------------------- test hooks
 rmd_status rmd_test_prng(uint32_t mode, uint64_t a, uint64_t b, int32_t n, float *out) {
     if (!out || n < 0) return fail(RMD_ERROR_INVALID_ARGUMENT, "invalid arguments");
@@ -869,7 +1005,9 @@ rmd_status rmd_test_jit_compile(const rmd_scene_desc *d, int32_t hoist, char *lo
                                                                d->light_materials, d->num_light_materials, hoist != 0);
         std::vector<char> cubin;
         bool cached = false;
-        std::string err = rmdhost::compileCubin(mod.source, cubin, msg, cached);
+        std::vector<std::string> defs;
+        if (const char *mb = std::getenv("RMD_SHADE_MIN_BLOCKS")) defs.push_back(std::string("-DRMD_SHADE_MIN_BLOCKS=") + mb);
+        std::string err = rmdhost::compileCubin(mod.source, cubin, msg, cached, defs);
         if (cubin_bytes) *cubin_bytes = (int64_t)cubin.size();
         if (!err.empty()) {
             if (log && loglen > 0) {
