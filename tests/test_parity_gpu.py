@@ -145,3 +145,65 @@ def test_material_eval_parity(spheres):
         c = orc.material_eval(m, rec)
         close = np.isclose(g, c, rtol=1e-3, atol=1e-5) | (np.isnan(g) & np.isnan(c))
         assert close.all(axis=1).mean() > 0.999, m
+
+
+def _all_lights_scene():
+    """Cornell box lit by every light type of the reference plus a textured world
+    (Background colour from a noise texture, so the environment importance map is
+    non-uniform); the room's open front lets paths escape to the world."""
+    from raymond_b200 import materials as M
+
+    sc = scenes.cornell(seed=4, envmap_exponent=7)
+    world = M.world((1.0, 1.0, 1.0, 1.0), 2.0)
+    world["Noise Texture"] = {
+        "type": "TEX_NOISE",
+        "inputs": {"Vector": {"type": "VECTOR", "value": [0, 0, 0]}, "W": {"type": "VALUE", "value": 0.0},
+                   "Scale": {"type": "VALUE", "value": 3.0}, "Detail": {"type": "VALUE", "value": 1.0},
+                   "Roughness": {"type": "VALUE", "value": 0.5}, "Distortion": {"type": "VALUE", "value": 0.0}},
+        "parameters": {"noise_dimensions": "3D"}}
+    world["Background"]["inputs"]["Color"] = {"type": "RGBA", "links": [["Noise Texture", "Color"]]}
+    lamp = M.light((1.0, 0.9, 0.8, 1.0), 1.0)
+    sc["light_materials"] = [("world", world), ("lamp", lamp)]
+    tr = np.array([[0.2, 0, 0, 0.5], [0, 0, 0.2, 0.95], [0, -0.2, 0, 0.5]], np.float32)  # facing down
+    sc["area_lights"] = [{"shader": 1, "transform": tr, "color": (4.0, 4.0, 4.0), "is_circular": False},
+                         {"shader": 1, "transform": tr * np.array([[1], [1], [1]]) + np.array([[0, 0, 0, 0.2], [0, 0, 0, 0], [0, 0, 0, 0]]),
+                          "color": (3.0, 2.0, 1.0), "is_circular": True}]
+    sc["point_lights"] = [{"shader": 1, "location": (0.3, 0.7, 0.6), "radius": 0.05, "color": (2.0, 2.0, 2.0)},
+                          {"shader": 1, "location": (0.7, 0.5, 0.7), "radius": 0.0, "color": (1.0, 1.5, 2.0)}]
+    sc["spot_lights"] = [{"shader": 1, "location": (0.5, 0.9, 0.8), "direction": (0.0, -1.0, -0.3), "radius": 0.03,
+                          "color": (6.0, 6.0, 6.0), "spot_size": 1.0, "spot_blend": 0.3}]
+    sc["sun_lights"] = [{"shader": 1, "direction": (0.2, 0.3, 1.0), "angle": 0.1, "color": (1.0, 1.0, 1.0)}]
+    return sc
+
+
+@pytest.mark.parametrize("mode", [SAMPLING_MIS, SAMPLING_NEE])
+def test_all_light_types_per_sample(gpu_ctx, mode):
+    desc = SceneDesc(_all_lights_scene())
+    scene = api.Scene(gpu_ctx, desc)
+    orc = O.OracleScene(desc)
+    assert orc.info()["lights"] == 1 + 2 + 2 + 1 + 1 + 1
+    fr = per_sample(desc, scene, orc, 96, 96, [0, 7], 6, sampling_mode=mode)
+    assert min(fr) >= MIN_MATCH, fr
+
+
+def test_fp64_film_matches_fp32(cornell):
+    desc, scene, orc = cornell
+    r = api.Renderer(scene, 64, 64)
+    r.render(spp=4, max_depth=8, film_fp64=True)
+    f64 = r.film64()
+    cpu, _ = orc.render(64, 64, 4, 8, film_fp64=True)
+    assert match_fraction(f64, cpu) >= MIN_MATCH
+
+
+def test_autotune_keeps_parity(cornell):
+    desc, scene, orc = cornell
+    r = api.Renderer(scene, 128, 128, pool_size=1 << 16)
+    res = r.autotune(spp=8, max_depth=8)
+    assert res["shade_min_blocks"] in (1, 3, 4, 5, 6)
+    assert res["pool_size"] >= 1 << 15 and res["ms_best"] <= res["ms_default"] * 1.0001
+    assert r.samples() == 0  # the film was cleared
+    for s in (0, 9):
+        r.reset()
+        r.render(spp=1, max_depth=8, first_sample=s)
+        cpu, _ = orc.render(128, 128, 1, 8, first_sample=s)
+        assert match_fraction(r.film(), cpu) >= MIN_MATCH
