@@ -17,28 +17,35 @@ RMD_HD float computeMisWeight(float pdf, float other) {
     return pdf / (pdf + other);
 }
 
-// One path vertex: intersection.metal:43-208 for the path in `slot`; returns
-// whether a surface was hit (a segment was shaded).
-__device__ __forceinline__ bool shadePath(const ShadeParams &p, uint32_t slot) {
+// One path vertex: intersection.metal:43-208 for the active path at position
+// i of S[cur]; returns whether a surface was hit (a segment was shaded).
+__device__ __forceinline__ bool shadePath(const ShadeParams &p, uint32_t i) {
     const Context &ctx = p.ctx;
     const PathPool &pool = p.pool;
     const FrameParams &fp = p.fp;
     Counters *cnt = p.counters;
+    const PathState &S = pool.s[p.cur];
 
-    const float4 d4 = pool.rayD[slot];
-    const float4 tp4 = pool.tp[slot];
-    const float4 h4 = pool.hit[slot];
-    const uint32_t meta = pool.meta[slot];
-    const uint32_t pixel = pool.pixel[slot];
-    const uint32_t sample = pool.sample[slot];
-    float3 L = xyz(pool.L[slot]);
+    const float4 d4 = S.rayD[i];
+    const float4 tp4 = S.tp[i];
+    const float4 h4 = pool.hit[i];
+    const float4 L4 = S.L[i];
+    const uint4 id = S.id[i];
+    const uint32_t meta = __float_as_uint(L4.w);
+    const uint32_t pixel = id.x;
+    const uint32_t sample = id.y;
+    float3 L = xyz(L4);
     const float3 rayDir = xyz(d4);
     const float3 rayWeight = xyz(tp4);
     const float rayBsdfPdf = tp4.w;
     const uint32_t depth = meta & 0xffffu;
     const uint32_t rayFlags = (meta >> 16) & 0xffu;
     const bool lastDepth = depth + 1u >= fp.maxDepth;
-    PrngState prng = PrngState::unpack(fp.rngMode, pool.rng[slot], pathSequence(sample, pixel, fp.numPixels));
+    PrngState prng = PrngState::unpack(fp.rngMode, make_uint2(id.z, id.w), pathSequence(sample, pixel, fp.numPixels));
+    uint32_t shadowIndex = 0xffffffffu;  // shadow ray whose target is set once the path's fate is known
+    float3 shadowDir = f3(0.0f);
+    float4 next[3];                      // rayO, rayD, tp of the continued path
+    float L4next = 0.0f;                 // its depth | flags word
 
     const bool needsToCollectEmission = is_inf(rayBsdfPdf) || fp.samplingMode != 1u;
     ShadingContext shading;
@@ -56,7 +63,7 @@ __device__ __forceinline__ bool shadePath(const ShadeParams &p, uint32_t slot) {
             L += misWeight * rayWeight * shading.material.emission;
         }
     } else {
-        const PerInstanceData &inst = ctx.instances[pool.hitInst[slot]];
+        const PerInstanceData &inst = ctx.instances[pool.hitInst[i]];
         uint32_t shaderIndex;
         buildShading(shading, ctx, inst, __float_as_uint(h4.w), make_float2(h4.y, h4.z), h4.x, shaderIndex);
         if (inst.visibility & rayFlags) shadeSurface(shaderIndex, ctx, shading);
@@ -92,8 +99,9 @@ __device__ __forceinline__ bool shadePath(const ShadeParams &p, uint32_t slot) {
                     const uint32_t k = warpAppend(&cnt->nShadow);
                     if (k < pool.capacity) {
                         pool.shO[k] = f4(shading.position, nee.distance - SHADOW_EPS);
-                        pool.shD[k] = f4(nee.direction, __uint_as_float(slot));
                         pool.shW[k] = f4(neeWeight, 0.0f);
+                        shadowIndex = k;
+                        shadowDir = nee.direction;
                     } else {
                         atomicOr(&cnt->errors, ERR_QUEUE_OVERFLOW);
                     }
@@ -111,24 +119,38 @@ __device__ __forceinline__ bool shadePath(const ShadeParams &p, uint32_t slot) {
             const float survivalProb = fminf(meanWeight, 1.0f);
             if (prng.sample() < survivalProb && !lastDepth) {
                 alive = true;
-                pool.rayO[slot] = f4(shading.position, SHADOW_EPS);
-                pool.rayD[slot] = f4(bs.wi, inf_f());
-                pool.tp[slot] = f4(weight * (1.0f / survivalProb), bs.pdf);
-                pool.meta[slot] = (depth + 1u) | ((uint32_t)bs.flags << 16);
-                pool.rng[slot] = prng.pack();
+                next[0] = f4(shading.position, SHADOW_EPS);
+                next[1] = f4(bs.wi, inf_f());
+                next[2] = f4(weight * (1.0f / survivalProb), bs.pdf);
+                L4next = __uint_as_float((depth + 1u) | ((uint32_t)bs.flags << 16));
             }
         }
     }
-    pool.L[slot] = f4(L, 0.0f);
-    if (alive) {
+    uint32_t target = 0xffffffffu;
+    if (alive) {  // continued: next free position of S[cur ^ 1]
         const uint32_t k = warpAppend(&cnt->nQ[p.cur ^ 1u]);
-        if (k < pool.capacity) pool.q[p.cur ^ 1u][k] = slot;
-        else atomicOr(&cnt->errors, ERR_QUEUE_OVERFLOW);
-    } else {
-        const uint32_t k = warpAppend(&cnt->nD[p.cur]);
-        if (k < pool.capacity) pool.qDone[p.cur][k] = slot;
-        else atomicOr(&cnt->errors, ERR_QUEUE_OVERFLOW);
+        if (k < pool.capacity) {
+            const PathState &N = pool.s[p.cur ^ 1u];
+            const uint2 rs = prng.pack();
+            N.rayO[k] = next[0];
+            N.rayD[k] = next[1];
+            N.tp[k] = next[2];
+            N.L[k] = f4(L, L4next);
+            N.id[k] = make_uint4(pixel, sample, rs.x, rs.y);
+            target = k;
+        } else {
+            atomicOr(&cnt->errors, ERR_QUEUE_OVERFLOW);
+        }
+    } else {  // finished: the finish list, added to the film by the next film pass
+        const uint32_t k = warpAppend(&cnt->nF[p.cur]);
+        if (k < pool.capacity) {
+            pool.fin[k] = f4(L, __uint_as_float(pixel));
+            target = k | SHADOW_TO_FINISHED;
+        } else {
+            atomicOr(&cnt->errors, ERR_QUEUE_OVERFLOW);
+        }
     }
+    if (shadowIndex != 0xffffffffu) pool.shD[shadowIndex] = f4(shadowDir, __uint_as_float(target));
     return h4.x > 0.0f;
 }
 
@@ -139,10 +161,9 @@ __device__ __forceinline__ bool shadePath(const ShadeParams &p, uint32_t slot) {
 #endif
 extern "C" __global__ void __launch_bounds__(128, RMD_SHADE_MIN_BLOCKS) rmd_shade(const __grid_constant__ rmd::ShadeParams p) {
     const unsigned n = rmd::activeCount(p.counters, p.cur);
-    const unsigned *q = p.pool.q[p.cur];
     unsigned segments = 0;
     for (unsigned i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x)
-        segments += rmd::shadePath(p, q[i]) ? 1u : 0u;
+        segments += rmd::shadePath(p, i) ? 1u : 0u;
     rmd::blockAdd64(&p.counters->segments, segments);
 }
 

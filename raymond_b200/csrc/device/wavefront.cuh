@@ -1,36 +1,46 @@
-// Path pool, queues and counters of the persistent wavefront, shared by the
+// Path state, queues and counters of the persistent wavefront, shared by the
 // static kernels (film / regeneration, traversal) and the NVRTC shading
-// module.  Paths live in fixed slots (structure of arrays, 16-byte fields);
-// queues hold slot indices.  One iteration is
+// module.  One iteration is
 //     film+regen -> closest-hit trace -> shade (NEE, BSDF sample) -> shadow trace
 // and replaces one depth step of Renderer.execute (Renderer.swift:545-673)
 // for every path in flight; finished paths are replaced by new camera
 // samples, so the pool stays full until the last samples drain.
+//
+// Path state is kept in queue order, not in fixed slots: iteration i (parity
+// p = i & 1) reads the active paths from S[p] at positions 0..n-1, and the
+// shading pass writes every path it continues to the next free position of
+// S[p ^ 1] (one atomic per warp), so each kernel reads and writes its path
+// records with coalesced 16-byte accesses.  Paths that end go to the finish
+// list with their radiance; the next film pass adds them to the film.
 #pragma once
 #include "scene.cuh"
 
 namespace rmd {
 
-constexpr uint32_t INVALID_PIXEL = 0xffffffffu;
 constexpr float SHADOW_EPS = 0.001f;  // device/constants.hpp:3
 
 // error flags
 constexpr uint32_t ERR_QUEUE_OVERFLOW = 1u;
 constexpr uint32_t ERR_STACK_OVERFLOW = 2u;
 
+// target of a shadow ray: position of its path in S[p ^ 1], or in the finish
+// list when this bit is set
+constexpr uint32_t SHADOW_TO_FINISHED = 0x80000000u;
+
 // Queue bookkeeping without same-address atomics on the regeneration path:
-// iteration i (parity p = i & 1) shades the active queue Q[p]; its first
-// nQ[p] entries are the paths continued by the previous iteration and the
-// next newPaths() entries the camera samples the film kernel wrote there for
-// the slots the previous iteration finished (D[p ^ 1]).  Finished paths of
-// this iteration go to D[p]; continued ones to Q[p ^ 1].
+// S[p] holds nQ[p] paths continued by the previous iteration followed by the
+// newPaths() camera samples the film kernel of this iteration appends; the
+// shading pass of parity p appends continued paths to S[p ^ 1] (nQ[p ^ 1])
+// and finished ones to the finish list (nF[p]).
 struct Counters {
-    uint32_t nQ[2];       // continued paths at the head of each active queue
-    uint32_t nD[2];       // finished / free slots
+    uint32_t nQ[2];       // continued paths at the head of each S[p]
+    uint32_t nF[2];       // finished paths written by the shading pass of parity p
     uint32_t nShadow;     // shadow rays of this iteration
     uint32_t traceWork;   // persistent closest-hit work counter
     uint32_t shadowWork;  // persistent any-hit work counter
     uint32_t errors;
+    uint32_t capacity;    // paths in flight at most (size of each S[p])
+    uint32_t pad;
     unsigned long long nextPath;    // next path id handed out by the film kernel
     unsigned long long endPath;     // one past the last path id of this render
     unsigned long long pathsDone;   // paths whose radiance reached the film
@@ -39,35 +49,70 @@ struct Counters {
     unsigned long long pad2;
 };
 
-// camera samples the film kernel of this iteration appends to Q[p]
+// camera samples the film kernel of this iteration appends to S[p]
 __device__ __forceinline__ uint32_t newPaths(const Counters *c, uint32_t p) {
     const unsigned long long next = c->nextPath, end = c->endPath;
     if (next >= end) return 0u;
     const unsigned long long left = end - next;
-    const uint32_t d = c->nD[p ^ 1u];
-    return left < (unsigned long long)d ? (uint32_t)left : d;
+    const uint32_t room = c->capacity - c->nQ[p];
+    return left < (unsigned long long)room ? (uint32_t)left : room;
 }
-// size of the active queue Q[p] after the film kernel of this iteration
+// number of active paths in S[p] after the film kernel of this iteration
 __device__ __forceinline__ uint32_t activeCount(const Counters *c, uint32_t p) { return c->nQ[p] + newPaths(c, p); }
 
+// One queue-ordered copy of the path state (structure of arrays).
+struct PathState {
+    float4 *rayO;  // origin.xyz, tmin
+    float4 *rayD;  // direction.xyz, tmax
+    float4 *tp;    // throughput.xyz, bsdf pdf of the ray
+    float4 *L;     // radiance gathered so far .xyz; .w = depth (bits 0-15) | ray flags (bits 16-23)
+    uint4 *id;     // pixel (y * width + x), sample index, packed PrngState
+};
+
 struct PathPool {
-    float4 *rayO;      // origin.xyz, tmin
-    float4 *rayD;      // direction.xyz, tmax
-    float4 *tp;        // throughput.xyz, bsdfPdf
-    float4 *L;         // radiance gathered so far
-    uint2 *rng;        // PrngState
-    uint32_t *pixel;   // y * width + x, or INVALID_PIXEL
-    uint32_t *sample;  // sample index of the path
-    uint32_t *meta;    // depth (bits 0-15) | ray flags (bits 16-23)
-    float4 *hit;       // t (<= 0: miss), b0, b1, primitive (bits)
-    uint32_t *hitInst; // instance index
-    uint32_t *q[2];    // active queues
-    uint32_t *qDone[2];  // finished slots
-    float4 *shO;       // shadow: origin.xyz, tmax
-    float4 *shD;       // shadow: direction.xyz, slot (bits)
-    float4 *shW;       // shadow: weight.xyz
+    PathState s[2];
+    float4 *hit;        // per active path of this iteration: t (<= 0: miss), b0, b1, primitive (bits)
+    uint32_t *hitInst;  // instance index
+    float4 *fin;        // finished paths: radiance.xyz, pixel (bits)
+    float4 *shO;        // shadow: origin.xyz, tmax
+    float4 *shD;        // shadow: direction.xyz, target (bits; SHADOW_TO_FINISHED)
+    float4 *shW;        // shadow: weight.xyz
     uint32_t capacity;
 };
+
+#ifndef __CUDACC_RTC__
+// Bytes of device memory a pool of `capacity` paths takes (each array padded
+// to 256 bytes), and the pool carved out of such a block.
+constexpr size_t pathPoolBytes(uint32_t capacity) {
+    const size_t P = capacity, pad = 255;
+    const size_t per16 = (P * 16 + pad) & ~pad, per4 = (P * 4 + pad) & ~pad;
+    return 2 * 5 * per16 + 5 * per16 + per4;
+}
+inline PathPool carvePathPool(void *base, uint32_t capacity) {
+    unsigned char *p = static_cast<unsigned char *>(base);
+    auto take = [&](size_t elemBytes) {
+        void *r = p;
+        p += ((size_t)capacity * elemBytes + 255) & ~size_t(255);
+        return r;
+    };
+    PathPool pool;
+    for (int k = 0; k < 2; k++) {
+        pool.s[k].rayO = static_cast<float4 *>(take(16));
+        pool.s[k].rayD = static_cast<float4 *>(take(16));
+        pool.s[k].tp = static_cast<float4 *>(take(16));
+        pool.s[k].L = static_cast<float4 *>(take(16));
+        pool.s[k].id = static_cast<uint4 *>(take(16));
+    }
+    pool.hit = static_cast<float4 *>(take(16));
+    pool.fin = static_cast<float4 *>(take(16));
+    pool.shO = static_cast<float4 *>(take(16));
+    pool.shD = static_cast<float4 *>(take(16));
+    pool.shW = static_cast<float4 *>(take(16));
+    pool.hitInst = static_cast<uint32_t *>(take(4));
+    pool.capacity = capacity;
+    return pool;
+}
+#endif
 
 struct FrameParams {
     uint32_t width, height, numPixels;

@@ -11,66 +11,59 @@
 namespace rmd {
 
 // ------------------------------------------------------------- frame set-up
-// Every slot starts as a finished, pixel-less path in D[1], so the first film
-// pass (iteration 0 reads D[1]) hands each one a camera sample.
-__global__ void k_frame_init(PathPool pool, Counters *cnt, uint64_t firstPath, uint64_t endPath) {
-    const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
-    if (i == 0) {
-        cnt->nQ[0] = cnt->nQ[1] = 0;
-        cnt->nD[0] = 0;
-        cnt->nD[1] = pool.capacity;
-        cnt->nShadow = 0;
-        cnt->traceWork = cnt->shadowWork = 0;
-        cnt->errors = 0;
-        cnt->nextPath = firstPath;
-        cnt->endPath = endPath;
-        cnt->pathsDone = 0;
-        cnt->segments = 0;
-        cnt->shadowRays = 0;
-    }
-    if (i < pool.capacity) {
-        pool.qDone[1][i] = i;
-        pool.pixel[i] = INVALID_PIXEL;
-    }
+__global__ void k_frame_init(Counters *cnt, uint32_t capacity, uint64_t firstPath, uint64_t endPath) {
+    cnt->nQ[0] = cnt->nQ[1] = 0;
+    cnt->nF[0] = cnt->nF[1] = 0;
+    cnt->nShadow = 0;
+    cnt->traceWork = cnt->shadowWork = 0;
+    cnt->errors = 0;
+    cnt->capacity = capacity;
+    cnt->pad = 0;
+    cnt->nextPath = firstPath;
+    cnt->endPath = endPath;
+    cnt->pathsDone = 0;
+    cnt->segments = 0;
+    cnt->shadowRays = 0;
+    cnt->pad2 = 0;
 }
 
 // ------------------------------------------------------------- film + regeneration
 // Adds the radiance of every path finished by the previous iteration to the
 // film (the film writes of intersection.metal:84-87,111-116,174-178 and
-// shadow.metal:24-27, gathered per path) and gives its slot the next camera
-// sample (generate.metal:72-121): entry j of D[p^1] takes path id nextPath + j
-// and queue position nQ[p] + j, so no counter is contended.
+// shadow.metal:24-27, gathered per path) and appends the next camera samples
+// (generate.metal:72-121) to S[p]: sample j takes path id nextPath + j and
+// position nQ[p] + j, so no counter is contended.
 __global__ void __launch_bounds__(256) k_film_regen(Context ctx, PathPool pool, FrameParams fp, Counters *cnt,
                                                     uint32_t p) {
     if (blockIdx.x == 0 && threadIdx.x == 0) {  // counters of later stages of this iteration
         cnt->nQ[p ^ 1u] = 0;
-        cnt->nD[p] = 0;
+        cnt->nF[p] = 0;
         cnt->nShadow = 0;
         cnt->traceWork = 0;
         cnt->shadowWork = 0;
     }
-    const uint32_t n = cnt->nD[p ^ 1u];
+    const uint32_t nFin = cnt->nF[p ^ 1u];
     const uint32_t base = cnt->nQ[p];
-    const unsigned long long first = cnt->nextPath, end = cnt->endPath;
-    const uint32_t *done = pool.qDone[p ^ 1u];
-    uint32_t *q = pool.q[p];
+    const uint32_t nNew = newPaths(cnt, p);
+    const unsigned long long first = cnt->nextPath;
+    const PathState S = pool.s[p];
+    const uint32_t n = max(nFin, nNew);
     uint32_t finished = 0;
     for (uint32_t j = blockIdx.x * blockDim.x + threadIdx.x; j < n; j += gridDim.x * blockDim.x) {
-        const uint32_t slot = done[j];
-        const uint32_t px = pool.pixel[slot];
-        if (px != INVALID_PIXEL) {
-            const float4 L = pool.L[slot];
+        if (j < nFin) {
+            const float4 f = pool.fin[j];
+            const uint32_t px = __float_as_uint(f.w);
             if (fp.filmFp64) {
-                atomicAdd(&fp.film64[3 * (size_t)px + 0], (double)L.x);
-                atomicAdd(&fp.film64[3 * (size_t)px + 1], (double)L.y);
-                atomicAdd(&fp.film64[3 * (size_t)px + 2], (double)L.z);
+                atomicAdd(&fp.film64[3 * (size_t)px + 0], (double)f.x);
+                atomicAdd(&fp.film64[3 * (size_t)px + 1], (double)f.y);
+                atomicAdd(&fp.film64[3 * (size_t)px + 2], (double)f.z);
             } else {
-                atomicAdd(&fp.film[px], make_float4(L.x, L.y, L.z, 1.0f));
+                atomicAdd(&fp.film[px], make_float4(f.x, f.y, f.z, 1.0f));
             }
             finished++;
         }
-        const unsigned long long id = first + j;
-        if (id < end) {
+        if (j < nNew) {
+            const unsigned long long id = first + j;
             const uint32_t sample = (uint32_t)(id / fp.numPixels);
             const uint32_t r = (uint32_t)(id - (unsigned long long)sample * fp.numPixels);
             uint32_t x, y;
@@ -78,17 +71,13 @@ __global__ void __launch_bounds__(256) k_film_regen(Context ctx, PathPool pool, 
             PrngState prng;
             float3 org, dir;
             cameraRay(ctx, fp, x, y, sample, prng, org, dir);
-            pool.rayO[slot] = f4(org, ctx.nearClip);
-            pool.rayD[slot] = f4(dir, ctx.farClip);
-            pool.tp[slot] = make_float4(1.0f, 1.0f, 1.0f, inf_f());
-            pool.L[slot] = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
-            pool.rng[slot] = prng.pack();
-            pool.pixel[slot] = y * fp.width + x;
-            pool.sample[slot] = sample;
-            pool.meta[slot] = (uint32_t)RayFlagsCamera << 16;
-            q[base + j] = slot;
-        } else {
-            pool.pixel[slot] = INVALID_PIXEL;
+            const uint32_t k = base + j;
+            const uint2 rs = prng.pack();
+            S.rayO[k] = f4(org, ctx.nearClip);
+            S.rayD[k] = f4(dir, ctx.farClip);
+            S.tp[k] = make_float4(1.0f, 1.0f, 1.0f, inf_f());
+            S.L[k] = make_float4(0.0f, 0.0f, 0.0f, __uint_as_float((uint32_t)RayFlagsCamera << 16));
+            S.id[k] = make_uint4(y * fp.width + x, sample, rs.x, rs.y);
         }
     }
     blockAdd64(&cnt->pathsDone, finished);
@@ -100,7 +89,7 @@ __global__ void __launch_bounds__(128) k_trace_closest(const BvhNode *__restrict
                                                        const float4 *__restrict__ tris, PathPool pool,
                                                        Counters *cnt, uint32_t p) {
     const uint32_t n = activeCount(cnt, p);
-    const uint32_t *q = pool.q[p];
+    const PathState S = pool.s[p];
     const int lane = threadIdx.x & 31;
     while (true) {
         uint32_t base = 0;
@@ -109,26 +98,27 @@ __global__ void __launch_bounds__(128) k_trace_closest(const BvhNode *__restrict
         if (base >= n) break;
         const uint32_t i = base + lane;
         if (i < n) {
-            const uint32_t slot = q[i];
-            const float4 o = pool.rayO[slot];
-            const float4 d = pool.rayD[slot];
+            const float4 o = S.rayO[i];
+            const float4 d = S.rayD[i];
             float4 hit;
             uint32_t inst;
             traceClosest(nodes, tris, xyz(o), xyz(d), o.w, d.w, hit, inst, &cnt->errors);
-            pool.hit[slot] = hit;
-            pool.hitInst[slot] = inst;
+            pool.hit[i] = hit;
+            pool.hitInst[i] = inst;
         }
     }
 }
 
 // raytraceAny fused with handleShadowRays (shadow.metal:6-29): an unoccluded
-// shadow ray adds its weight to its path's radiance.  Thread 0 also advances
-// nextPath past the camera samples this iteration consumed.
+// shadow ray adds its weight to its path's radiance, in S[p ^ 1] for a path
+// that continues and in the finish list for one that ended.  Thread 0 also
+// advances nextPath past the camera samples this iteration consumed.
 __global__ void __launch_bounds__(128) k_trace_shadow(const BvhNode *__restrict__ nodes,
                                                       const float4 *__restrict__ tris, PathPool pool,
                                                       Counters *cnt, uint32_t p) {
     const uint32_t n = cnt->nShadow;
     if (blockIdx.x == 0 && threadIdx.x == 0) cnt->nextPath += newPaths(cnt, p);
+    float4 *nextL = pool.s[p ^ 1u].L;
     const int lane = threadIdx.x & 31;
     uint32_t traced = 0;
     while (true) {
@@ -142,14 +132,15 @@ __global__ void __launch_bounds__(128) k_trace_shadow(const BvhNode *__restrict_
             const float4 o = pool.shO[i];
             const float4 d = pool.shD[i];
             const bool occluded = traceAny(nodes, tris, xyz(o), xyz(d), SHADOW_EPS, o.w, &cnt->errors);
-            if (!occluded) {
-                const uint32_t slot = __float_as_uint(d.w);
+            const uint32_t target = __float_as_uint(d.w);
+            if (!occluded && target != 0xffffffffu) {  // all ones: the path overflowed its queue
+                float4 *dst = (target & SHADOW_TO_FINISHED) ? &pool.fin[target & ~SHADOW_TO_FINISHED] : &nextL[target];
                 const float4 w = pool.shW[i];
-                float4 L = pool.L[slot];
+                float4 L = *dst;
                 L.x += w.x;
                 L.y += w.y;
                 L.z += w.z;
-                pool.L[slot] = L;
+                *dst = L;
             }
         }
     }
@@ -239,9 +230,7 @@ using namespace rmd;
 
 cudaError_t rmdLaunchFrameInit(const PathPool &pool, Counters *cnt, uint64_t firstPath, uint64_t endPath,
                                cudaStream_t s) {
-    const uint32_t threads = 256;
-    const uint32_t blocks = (pool.capacity + threads - 1) / threads;
-    k_frame_init<<<blocks, threads, 0, s>>>(pool, cnt, firstPath, endPath);
+    k_frame_init<<<1, 1, 0, s>>>(cnt, pool.capacity, firstPath, endPath);
     return cudaGetLastError();
 }
 cudaError_t rmdLaunchFilmRegen(const Context &ctx, const PathPool &pool, const FrameParams &fp, Counters *cnt,

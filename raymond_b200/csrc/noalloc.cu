@@ -31,27 +31,13 @@ namespace {
 using namespace rmd;
 
 constexpr uint32_t kMaxPaths = RMD_NOALLOC_MAX_PATHS;
-// per path: rayO, rayD, tp, L, hit, shO, shD, shW (16 B each), rng (8 B),
-// pixel, sample, meta, hitInst, q[2], qDone[2] (4 B each)
-constexpr size_t kBytesPerPath = 8 * 16 + 8 + 8 * 4;
-constexpr size_t kArrays = 17;
-constexpr size_t kScratchBytes = 256 + kMaxPaths * kBytesPerPath + kArrays * 256;
+// counters (padded to 256 B), then the path pool of the largest size
+constexpr size_t kScratchBytes = 256 + pathPoolBytes(kMaxPaths);
 
 static __device__ __align__(256) unsigned char g_noallocScratch[kScratchBytes];
 
 std::mutex g_mutex;
 void *g_scratch[64] = {};  // device address of g_noallocScratch per device
-
-// Carves the counters and the path arrays out of the scratch block.
-struct Carver {
-    unsigned char *p;
-    template <class T>
-    T *take(size_t count) {
-        T *r = reinterpret_cast<T *>(p);
-        p += (count * sizeof(T) + 255) & ~size_t(255);
-        return r;
-    }
-};
 
 rmd_status cudaFail(cudaError_t e, const char *what) {
     std::string msg = std::string("rmd_render_noalloc: ") + what + ": " + cudaGetErrorString(e);
@@ -92,27 +78,8 @@ extern "C" rmd_status rmd_render_noalloc(rmd_scene *scene, const rmd_camera *cam
         base = g_scratch[v.device];
     }
     const uint32_t P = pool_size ? pool_size : kMaxPaths;
-    Carver c{static_cast<unsigned char *>(base)};
-    Counters *cnt = c.take<Counters>(1);
-    PathPool pool;
-    pool.rayO = c.take<float4>(P);
-    pool.rayD = c.take<float4>(P);
-    pool.tp = c.take<float4>(P);
-    pool.L = c.take<float4>(P);
-    pool.rng = c.take<uint2>(P);
-    pool.pixel = c.take<uint32_t>(P);
-    pool.sample = c.take<uint32_t>(P);
-    pool.meta = c.take<uint32_t>(P);
-    pool.hit = c.take<float4>(P);
-    pool.hitInst = c.take<uint32_t>(P);
-    pool.q[0] = c.take<uint32_t>(P);
-    pool.q[1] = c.take<uint32_t>(P);
-    pool.qDone[0] = c.take<uint32_t>(P);
-    pool.qDone[1] = c.take<uint32_t>(P);
-    pool.shO = c.take<float4>(P);
-    pool.shD = c.take<float4>(P);
-    pool.shW = c.take<float4>(P);
-    pool.capacity = P;
+    Counters *cnt = static_cast<Counters *>(base);
+    const PathPool pool = carvePathPool(static_cast<unsigned char *>(base) + 256, P);
 
     Context ctx = v.ctx;
     for (int k = 0; k < 4; k++)

@@ -113,7 +113,7 @@ struct rmd_renderer {
     int shadeBlocks = 0;
     int shadeMinBlocks = 1;
     int traceBlocksPerSm = 8;
-    DevBuf rayO, rayD, tp, L, rng, pixel, sample, meta, hit, hitInst, q0, q1, qDone0, qDone1, shO, shD, shW;
+    DevBuf pool;  // path state, finish list and shadow rays (carvePathPool)
     DevBuf counters, film, film64, resolve;
     Counters *hostCounters = nullptr;  // pinned
     Context dctx{};
@@ -563,50 +563,12 @@ rmd_status rmd_scene_info(const rmd_scene *s, uint64_t *triangles, uint64_t *bvh
 }
 
 static rmd_status allocatePool(rmd_renderer *r) {
-    const size_t P = r->capacity;
-    RMD_CUDA(r->rayO.alloc(P * 16));
-    RMD_CUDA(r->rayD.alloc(P * 16));
-    RMD_CUDA(r->tp.alloc(P * 16));
-    RMD_CUDA(r->L.alloc(P * 16));
-    RMD_CUDA(r->rng.alloc(P * 8));
-    RMD_CUDA(r->pixel.alloc(P * 4));
-    RMD_CUDA(r->sample.alloc(P * 4));
-    RMD_CUDA(r->meta.alloc(P * 4));
-    RMD_CUDA(r->hit.alloc(P * 16));
-    RMD_CUDA(r->hitInst.alloc(P * 4));
-    RMD_CUDA(r->q0.alloc(P * 4));
-    RMD_CUDA(r->q1.alloc(P * 4));
-    RMD_CUDA(r->qDone0.alloc(P * 4));
-    RMD_CUDA(r->qDone1.alloc(P * 4));
-    RMD_CUDA(r->shO.alloc(P * 16));
-    RMD_CUDA(r->shD.alloc(P * 16));
-    RMD_CUDA(r->shW.alloc(P * 16));
+    RMD_CUDA(r->pool.alloc(pathPoolBytes(r->capacity)));
     RMD_CUDA(r->counters.alloc(sizeof(Counters)));
     return RMD_OK;
 }
 
-static PathPool poolView(rmd_renderer *r) {
-    PathPool p;
-    p.rayO = r->rayO.as<float4>();
-    p.rayD = r->rayD.as<float4>();
-    p.tp = r->tp.as<float4>();
-    p.L = r->L.as<float4>();
-    p.rng = r->rng.as<uint2>();
-    p.pixel = r->pixel.as<uint32_t>();
-    p.sample = r->sample.as<uint32_t>();
-    p.meta = r->meta.as<uint32_t>();
-    p.hit = r->hit.as<float4>();
-    p.hitInst = r->hitInst.as<uint32_t>();
-    p.q[0] = r->q0.as<uint32_t>();
-    p.q[1] = r->q1.as<uint32_t>();
-    p.qDone[0] = r->qDone0.as<uint32_t>();
-    p.qDone[1] = r->qDone1.as<uint32_t>();
-    p.shO = r->shO.as<float4>();
-    p.shD = r->shD.as<float4>();
-    p.shW = r->shW.as<float4>();
-    p.capacity = r->capacity;
-    return p;
-}
+static PathPool poolView(rmd_renderer *r) { return carvePathPool(r->pool.ptr, r->capacity); }
 
 rmd_status rmd_renderer_set_size(rmd_renderer *r, uint32_t width, uint32_t height) {
     if (!r || width == 0 || height == 0 || width > 65535 || height > 65535)
@@ -905,7 +867,7 @@ rmd_status rmd_renderer_autotune(rmd_renderer *r, const rmd_render_settings *set
     for (uint32_t cap : {cap0 / 2, cap0 * 2}) {
         if (cap < (1u << 16)) continue;
         size_t freeB = 0, totalB = 0;
-        if (cudaMemGetInfo(&freeB, &totalB) != cudaSuccess || (size_t)cap * 176 > freeB / 2) continue;
+        if (cudaMemGetInfo(&freeB, &totalB) != cudaSuccess || pathPoolBytes(cap) > freeB / 2) continue;
         r->capacity = cap;
         if ((st = allocatePool(r)) != RMD_OK) return st;
         double ms;
