@@ -26,11 +26,11 @@ __device__ __forceinline__ bool shadePath(const ShadeParams &p, uint32_t i) {
     Counters *cnt = p.counters;
     const PathState &S = pool.s[p.cur];
 
-    const float4 d4 = S.rayD[i];
-    const float4 tp4 = S.tp[i];
-    const float4 h4 = pool.hit[i];
-    const float4 L4 = S.L[i];
-    const uint4 id = S.id[i];
+    const float4 d4 = __ldcs(&S.rayD[i]);
+    const float4 tp4 = __ldcs(&S.tp[i]);
+    const float4 h4 = __ldcs(&pool.hit[i]);
+    const float4 L4 = __ldcs(&S.L[i]);
+    const uint4 id = __ldcs(&S.id[i]);
     const uint32_t meta = __float_as_uint(L4.w);
     const uint32_t pixel = id.x;
     const uint32_t sample = id.y;
@@ -63,7 +63,7 @@ __device__ __forceinline__ bool shadePath(const ShadeParams &p, uint32_t i) {
             L += misWeight * rayWeight * shading.material.emission;
         }
     } else {
-        const PerInstanceData &inst = ctx.instances[pool.hitInst[i]];
+        const PerInstanceData &inst = ctx.instances[__ldcs(&pool.hitInst[i])];
         uint32_t shaderIndex;
         buildShading(shading, ctx, inst, __float_as_uint(h4.w), make_float2(h4.y, h4.z), h4.x, shaderIndex);
         if (inst.visibility & rayFlags) shadeSurface(shaderIndex, ctx, shading);
@@ -98,8 +98,8 @@ __device__ __forceinline__ bool shadePath(const ShadeParams &p, uint32_t i) {
                 if (isfinite3(neeWeight) && any_nonzero(neeWeight) && !lastDepth) {
                     const uint32_t k = warpAppend(&cnt->nShadow);
                     if (k < pool.capacity) {
-                        pool.shO[k] = f4(shading.position, nee.distance - SHADOW_EPS);
-                        pool.shW[k] = f4(neeWeight, 0.0f);
+                        __stcs(&pool.shO[k], f4(shading.position, nee.distance - SHADOW_EPS));
+                        __stcs(&pool.shW[k], f4(neeWeight, 0.0f));
                         shadowIndex = k;
                         shadowDir = nee.direction;
                     } else {
@@ -132,11 +132,11 @@ __device__ __forceinline__ bool shadePath(const ShadeParams &p, uint32_t i) {
         if (k < pool.capacity) {
             const PathState &N = pool.s[p.cur ^ 1u];
             const uint2 rs = prng.pack();
-            N.rayO[k] = next[0];
-            N.rayD[k] = next[1];
-            N.tp[k] = next[2];
-            N.L[k] = f4(L, L4next);
-            N.id[k] = make_uint4(pixel, sample, rs.x, rs.y);
+            __stcs(&N.rayO[k], next[0]);
+            __stcs(&N.rayD[k], next[1]);
+            __stcs(&N.tp[k], next[2]);
+            __stcs(&N.L[k], f4(L, L4next));
+            __stcs(&N.id[k], make_uint4(pixel, sample, rs.x, rs.y));
             target = k;
         } else {
             atomicOr(&cnt->errors, ERR_QUEUE_OVERFLOW);
@@ -144,13 +144,13 @@ __device__ __forceinline__ bool shadePath(const ShadeParams &p, uint32_t i) {
     } else {  // finished: the finish list, added to the film by the next film pass
         const uint32_t k = warpAppend(&cnt->nF[p.cur]);
         if (k < pool.capacity) {
-            pool.fin[k] = f4(L, __uint_as_float(pixel));
+            __stcs(&pool.fin[k], f4(L, __uint_as_float(pixel)));
             target = k | SHADOW_TO_FINISHED;
         } else {
             atomicOr(&cnt->errors, ERR_QUEUE_OVERFLOW);
         }
     }
-    if (shadowIndex != 0xffffffffu) pool.shD[shadowIndex] = f4(shadowDir, __uint_as_float(target));
+    if (shadowIndex != 0xffffffffu) __stcs(&pool.shD[shadowIndex], f4(shadowDir, __uint_as_float(target)));
     return h4.x > 0.0f;
 }
 

@@ -128,123 +128,119 @@ RMD_HD void boxes(const BvhNode &n, const TraceRay &r, float tmin, float tmax, f
     t1 = c1min;
 }
 
-// Closest hit (raytrace.metal:11-50).  hit = (t, b0, b1, prim bits), inst = instance.
-RMD_HD bool traceClosest(const BvhNode *__restrict__ nodes, const float4 *__restrict__ tris, float3 o, float3 d,
-                         float tmin, float tmax, float4 &hit, uint32_t &inst, uint32_t *errors) {
-    if (nodes == nullptr) {  // scene without triangles
-        hit = make_float4(-1.0f, 0.0f, 0.0f, 0.0f);
-        inst = 0xffffffffu;
-        return false;
-    }
-    const TraceRay r = makeTraceRay(o, d);
-    int stack[TRAVERSAL_STACK];
-    int sp = 0;
-    stack[sp++] = STACK_SENTINEL;
-    int node = 0;
-    float best = tmax;
-    int bestTri = -1;
-    float bb0 = 0.0f, bb1 = 0.0f;
-    while (node != STACK_SENTINEL) {
-        if (node >= 0) {
-            const BvhNode n = {__ldg(&nodes[node].c0xy), __ldg(&nodes[node].c1xy), __ldg(&nodes[node].cz),
-                               __ldg(&nodes[node].link)};
+// Traversal state of one ray.
+struct TraversalState {
+    TraceRay r;
+    float tmin, tmax;  // tmax shrinks to the closest hit found so far
+    int node;          // next node (>= 0), leaf (< 0), or STACK_SENTINEL once finished
+    int sp;
+    int hitTri;        // closest (any-hit: first) triangle hit, -1 if none
+    float b0, b1;
+};
+// The node stack is a separate local array, so the scalar state above stays in registers.
+typedef int TraversalStack[TRAVERSAL_STACK];
+
+RMD_HD void beginTraversal(TraversalState &s, TraversalStack &stack, const BvhNode *nodes, float3 o, float3 d,
+                           float tmin, float tmax) {
+    s.r = makeTraceRay(o, d);
+    s.tmin = tmin;
+    s.tmax = tmax;
+    s.sp = 0;
+    stack[s.sp++] = STACK_SENTINEL;
+    s.node = nodes != nullptr ? 0 : STACK_SENTINEL;  // a scene without triangles misses everything
+    s.hitTri = -1;
+    s.b0 = s.b1 = 0.0f;
+}
+
+// Depth-first traversal, one node or one leaf per step, nearer child first;
+// a leaf is intersected as soon as it is reached so the closest hit found so
+// far culls the rest.  ANY: stop at the first hit (raytrace.metal:52-85);
+// otherwise keep the closest (raytrace.metal:11-50).  (The while-while loop
+// and dynamic ray fetch of Aila & Laine, HPG 2009, both measured slower here:
+// warp-vote instructions inside the loop cost more than they recover.)
+template <bool ANY>
+RMD_HD void traverse(TraversalState &s, TraversalStack &stack, const BvhNode *__restrict__ nodes,
+                     const float4 *__restrict__ tris, uint32_t *errors) {
+    while (s.node != STACK_SENTINEL) {
+        if (s.node >= 0) {
+            const BvhNode *np = &nodes[s.node];
+            const BvhNode n = {__ldg(&np->c0xy), __ldg(&np->c1xy), __ldg(&np->cz), __ldg(&np->link)};
             float t0, t1;
             bool h0, h1;
-            boxes(n, r, tmin, best, t0, t1, h0, h1);
+            boxes(n, s.r, s.tmin, s.tmax, t0, t1, h0, h1);
             if (h0 && h1) {
                 int nearN = n.link.x, farN = n.link.y;
                 if (t1 < t0) {
                     nearN = n.link.y;
                     farN = n.link.x;
                 }
-                if (sp < TRAVERSAL_STACK) stack[sp++] = farN;
+                if (s.sp < TRAVERSAL_STACK) stack[s.sp++] = farN;
                 else atomicOr(errors, 2u);
-                node = nearN;
+                s.node = nearN;
             } else if (h0) {
-                node = n.link.x;
+                s.node = n.link.x;
             } else if (h1) {
-                node = n.link.y;
+                s.node = n.link.y;
             } else {
-                node = stack[--sp];
+                s.node = stack[--s.sp];
             }
         } else {
-            const int leaf = ~node;
-            const int first = leaf >> 3, count = (leaf & 7) + 1;
+            const int code = ~s.node;
+            const int first = code >> 3, count = (code & 7) + 1;
+            bool found = false;
             for (int i = 0; i < count; i++) {
                 const int ti = first + i;
                 const float4 a = __ldg(&tris[3 * ti + 0]);
                 const float4 b = __ldg(&tris[3 * ti + 1]);
                 const float4 c = __ldg(&tris[3 * ti + 2]);
                 float t, b0, b1;
-                if (intersectTriangle(r.wr, xyz(a), xyz(b), xyz(c), tmin, best, t, b0, b1)) {
-                    best = t;
-                    bestTri = ti;
-                    bb0 = b0;
-                    bb1 = b1;
+                if (intersectTriangle(s.r.wr, xyz(a), xyz(b), xyz(c), s.tmin, s.tmax, t, b0, b1)) {
+                    s.hitTri = ti;
+                    if (ANY) {
+                        found = true;
+                        break;
+                    }
+                    s.tmax = t;
+                    s.b0 = b0;
+                    s.b1 = b1;
                 }
             }
-            node = stack[--sp];
+            s.node = (ANY && found) ? STACK_SENTINEL : stack[--s.sp];
         }
     }
-    if (bestTri < 0) {
+}
+
+// Closest-hit record of a finished traversal: hit = (t, b0, b1, primitive
+// bits), inst = instance; t = -1 and inst = ~0 on a miss.
+RMD_HD bool closestHit(const TraversalState &s, const float4 *__restrict__ tris, float4 &hit, uint32_t &inst) {
+    if (s.hitTri < 0) {
         hit = make_float4(-1.0f, 0.0f, 0.0f, 0.0f);
         inst = 0xffffffffu;
         return false;
     }
-    const float4 a = __ldg(&tris[3 * bestTri + 0]);
-    const float4 b = __ldg(&tris[3 * bestTri + 1]);
-    hit = make_float4(best, bb0, bb1, b.w);
+    const float4 a = __ldg(&tris[3 * s.hitTri + 0]);
+    const float4 b = __ldg(&tris[3 * s.hitTri + 1]);
+    hit = make_float4(s.tmax, s.b0, s.b1, b.w);
     inst = __float_as_uint(a.w);
     return true;
 }
 
-// Any hit (raytrace.metal:52-85): true if anything lies in [tmin, tmax].
+// Single-ray forms of the two queries (test hooks).
+RMD_HD bool traceClosest(const BvhNode *__restrict__ nodes, const float4 *__restrict__ tris, float3 o, float3 d,
+                         float tmin, float tmax, float4 &hit, uint32_t &inst, uint32_t *errors) {
+    TraversalState s;
+    TraversalStack stack;
+    beginTraversal(s, stack, nodes, o, d, tmin, tmax);
+    traverse<false>(s, stack, nodes, tris, errors);
+    return closestHit(s, tris, hit, inst);
+}
 RMD_HD bool traceAny(const BvhNode *__restrict__ nodes, const float4 *__restrict__ tris, float3 o, float3 d,
                      float tmin, float tmax, uint32_t *errors) {
-    if (nodes == nullptr) return false;
-    const TraceRay r = makeTraceRay(o, d);
-    int stack[TRAVERSAL_STACK];
-    int sp = 0;
-    stack[sp++] = STACK_SENTINEL;
-    int node = 0;
-    while (node != STACK_SENTINEL) {
-        if (node >= 0) {
-            const BvhNode n = {__ldg(&nodes[node].c0xy), __ldg(&nodes[node].c1xy), __ldg(&nodes[node].cz),
-                               __ldg(&nodes[node].link)};
-            float t0, t1;
-            bool h0, h1;
-            boxes(n, r, tmin, tmax, t0, t1, h0, h1);
-            if (h0 && h1) {
-                int nearN = n.link.x, farN = n.link.y;
-                if (t1 < t0) {
-                    nearN = n.link.y;
-                    farN = n.link.x;
-                }
-                if (sp < TRAVERSAL_STACK) stack[sp++] = farN;
-                else atomicOr(errors, 2u);
-                node = nearN;
-            } else if (h0) {
-                node = n.link.x;
-            } else if (h1) {
-                node = n.link.y;
-            } else {
-                node = stack[--sp];
-            }
-        } else {
-            const int leaf = ~node;
-            const int first = leaf >> 3, count = (leaf & 7) + 1;
-            for (int i = 0; i < count; i++) {
-                const int ti = first + i;
-                const float4 a = __ldg(&tris[3 * ti + 0]);
-                const float4 b = __ldg(&tris[3 * ti + 1]);
-                const float4 c = __ldg(&tris[3 * ti + 2]);
-                float t, b0, b1;
-                if (intersectTriangle(r.wr, xyz(a), xyz(b), xyz(c), tmin, tmax, t, b0, b1)) return true;
-            }
-            node = stack[--sp];
-        }
-    }
-    return false;
+    TraversalState s;
+    TraversalStack stack;
+    beginTraversal(s, stack, nodes, o, d, tmin, tmax);
+    traverse<true>(s, stack, nodes, tris, errors);
+    return s.hitTri >= 0;
 }
 
 }  // namespace rmd

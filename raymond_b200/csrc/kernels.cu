@@ -51,7 +51,7 @@ __global__ void __launch_bounds__(256) k_film_regen(Context ctx, PathPool pool, 
     uint32_t finished = 0;
     for (uint32_t j = blockIdx.x * blockDim.x + threadIdx.x; j < n; j += gridDim.x * blockDim.x) {
         if (j < nFin) {
-            const float4 f = pool.fin[j];
+            const float4 f = __ldcs(&pool.fin[j]);
             const uint32_t px = __float_as_uint(f.w);
             if (fp.filmFp64) {
                 atomicAdd(&fp.film64[3 * (size_t)px + 0], (double)f.x);
@@ -73,40 +73,60 @@ __global__ void __launch_bounds__(256) k_film_regen(Context ctx, PathPool pool, 
             cameraRay(ctx, fp, x, y, sample, prng, org, dir);
             const uint32_t k = base + j;
             const uint2 rs = prng.pack();
-            S.rayO[k] = f4(org, ctx.nearClip);
-            S.rayD[k] = f4(dir, ctx.farClip);
-            S.tp[k] = make_float4(1.0f, 1.0f, 1.0f, inf_f());
-            S.L[k] = make_float4(0.0f, 0.0f, 0.0f, __uint_as_float((uint32_t)RayFlagsCamera << 16));
-            S.id[k] = make_uint4(y * fp.width + x, sample, rs.x, rs.y);
+            __stcs(&S.rayO[k], f4(org, ctx.nearClip));
+            __stcs(&S.rayD[k], f4(dir, ctx.farClip));
+            __stcs(&S.tp[k], make_float4(1.0f, 1.0f, 1.0f, inf_f()));
+            __stcs(&S.L[k], make_float4(0.0f, 0.0f, 0.0f, __uint_as_float((uint32_t)RayFlagsCamera << 16)));
+            __stcs(&S.id[k], make_uint4(y * fp.width + x, sample, rs.x, rs.y));
         }
     }
     blockAdd64(&cnt->pathsDone, finished);
 }
 
 // ------------------------------------------------------------- traversal
-// Persistent warps pull 32 queue entries at a time (Aila & Laine 2009).
+// Persistent warps (Aila & Laine 2009): a warp takes 32 consecutive queue
+// entries with one atomic and traces them to the end.  begin(idx, state,
+// stack) starts entry idx, finish(idx, state) consumes the finished query.
+template <bool ANY, class Begin, class Finish>
+__device__ __forceinline__ void persistentTrace(const BvhNode *__restrict__ nodes, const float4 *__restrict__ tris,
+                                                uint32_t *work, uint32_t n, uint32_t *errors, Begin begin,
+                                                Finish finish) {
+    TraversalState s;
+    TraversalStack stack;
+    const int lane = threadIdx.x & 31;
+    while (true) {
+        uint32_t base = 0;
+        if (lane == 0) base = atomicAdd(work, 32u);
+        base = __shfl_sync(0xffffffffu, base, 0);
+        if (base >= n) break;
+        const uint32_t idx = base + lane;
+        if (idx < n) {
+            begin(idx, s, stack);
+            traverse<ANY>(s, stack, nodes, tris, errors);
+            finish(idx, s);
+        }
+    }
+}
+
 __global__ void __launch_bounds__(128) k_trace_closest(const BvhNode *__restrict__ nodes,
                                                        const float4 *__restrict__ tris, PathPool pool,
                                                        Counters *cnt, uint32_t p) {
     const uint32_t n = activeCount(cnt, p);
     const PathState S = pool.s[p];
-    const int lane = threadIdx.x & 31;
-    while (true) {
-        uint32_t base = 0;
-        if (lane == 0) base = atomicAdd(&cnt->traceWork, 32u);
-        base = __shfl_sync(0xffffffffu, base, 0);
-        if (base >= n) break;
-        const uint32_t i = base + lane;
-        if (i < n) {
-            const float4 o = S.rayO[i];
-            const float4 d = S.rayD[i];
+    persistentTrace<false>(
+        nodes, tris, &cnt->traceWork, n, &cnt->errors,
+        [&](uint32_t idx, TraversalState &s, TraversalStack &stack) {
+            const float4 o = __ldcs(&S.rayO[idx]);
+            const float4 d = __ldcs(&S.rayD[idx]);
+            beginTraversal(s, stack, nodes, xyz(o), xyz(d), o.w, d.w);
+        },
+        [&](uint32_t idx, const TraversalState &s) {
             float4 hit;
             uint32_t inst;
-            traceClosest(nodes, tris, xyz(o), xyz(d), o.w, d.w, hit, inst, &cnt->errors);
-            pool.hit[i] = hit;
-            pool.hitInst[i] = inst;
-        }
-    }
+            closestHit(s, tris, hit, inst);
+            __stcs(&pool.hit[idx], hit);
+            __stcs(&pool.hitInst[idx], inst);
+        });
 }
 
 // raytraceAny fused with handleShadowRays (shadow.metal:6-29): an unoccluded
@@ -119,31 +139,27 @@ __global__ void __launch_bounds__(128) k_trace_shadow(const BvhNode *__restrict_
     const uint32_t n = cnt->nShadow;
     if (blockIdx.x == 0 && threadIdx.x == 0) cnt->nextPath += newPaths(cnt, p);
     float4 *nextL = pool.s[p ^ 1u].L;
-    const int lane = threadIdx.x & 31;
-    uint32_t traced = 0;
-    while (true) {
-        uint32_t base = 0;
-        if (lane == 0) base = atomicAdd(&cnt->shadowWork, 32u);
-        base = __shfl_sync(0xffffffffu, base, 0);
-        if (base >= n) break;
-        const uint32_t i = base + lane;
-        if (i < n) {
+    uint32_t target = 0, traced = 0;
+    persistentTrace<true>(
+        nodes, tris, &cnt->shadowWork, n, &cnt->errors,
+        [&](uint32_t idx, TraversalState &s, TraversalStack &stack) {
+            const float4 o = __ldcs(&pool.shO[idx]);
+            const float4 d = __ldcs(&pool.shD[idx]);
+            target = __float_as_uint(d.w);
             traced++;
-            const float4 o = pool.shO[i];
-            const float4 d = pool.shD[i];
-            const bool occluded = traceAny(nodes, tris, xyz(o), xyz(d), SHADOW_EPS, o.w, &cnt->errors);
-            const uint32_t target = __float_as_uint(d.w);
-            if (!occluded && target != 0xffffffffu) {  // all ones: the path overflowed its queue
-                float4 *dst = (target & SHADOW_TO_FINISHED) ? &pool.fin[target & ~SHADOW_TO_FINISHED] : &nextL[target];
-                const float4 w = pool.shW[i];
-                float4 L = *dst;
-                L.x += w.x;
-                L.y += w.y;
-                L.z += w.z;
-                *dst = L;
-            }
-        }
-    }
+            beginTraversal(s, stack, nodes, xyz(o), xyz(d), SHADOW_EPS, o.w);
+        },
+        [&](uint32_t idx, const TraversalState &s) {
+            // all ones: the path overflowed its queue
+            if (s.hitTri >= 0 || target == 0xffffffffu) return;
+            float4 *dst = (target & SHADOW_TO_FINISHED) ? &pool.fin[target & ~SHADOW_TO_FINISHED] : &nextL[target];
+            const float4 w = __ldcs(&pool.shW[idx]);
+            float4 L = *dst;
+            L.x += w.x;
+            L.y += w.y;
+            L.z += w.z;
+            *dst = L;
+        });
     blockAdd64(&cnt->shadowRays, traced);
 }
 
