@@ -38,11 +38,20 @@ sys.path.insert(0, str(ROOT))
 W, H, SPP, DEPTH, SEED = 1920, 1080, 64, 12, 1
 WORKLOAD = "spheres_terrain_1080p_64spp_depth12"
 METRIC = "Mpaths/s (plain tracer, config 2)"
-# algorithmic HBM bytes of the path state each stage must move (per unit)
-BYTES_TRACE_PER_RAY = 32 + 20      # ray in, hit out
-BYTES_SHADE_PER_SEGMENT = 20 + 64 + 32 + 110 + 48  # hit in, path state r/w, next ray, triangle attributes, shadow ray
-BYTES_SHADOW_PER_RAY = 32 + 8 + 16  # shadow ray in, occlusion flag, resolve read
-BYTES_FILM_PER_PATH = 24
+# Algorithmic HBM bytes each stage must move per unit (queue-ordered path
+# state, 16-byte records):
+#   trace   per closest-hit ray: ray in (32), hit record out (16 + 4)
+#   shade   per shaded segment : path state in (5 x 16 + hit 4), triangle
+#           attributes (face 16, 3 x position 16, 3 x normal 16, 3 x uv 8),
+#           continued path state out (5 x 16), shadow ray out (48)
+#   shadow  per shadow ray     : ray + weight in (48), radiance read-modify-write (32)
+#   film    per path           : finish record in (16), film read-modify-write (32),
+#           new path state out (5 x 16)
+BYTES_TRACE_PER_RAY = 32 + 20
+BYTES_SHADE_PER_SEGMENT = 84 + 136 + 80 + 48
+BYTES_SHADOW_PER_RAY = 48 + 32
+BYTES_FILM_PER_PATH = 16 + 32 + 80
+CPU_BASELINE_SPP = 16  # oracle sample: 16 spp of the full frame (about 10 s on 16 cores)
 
 
 def rank_info():
@@ -99,16 +108,17 @@ def make_scene():
 
 
 def cpu_baseline_sample(desc, threads: int = 0):
-    """Oracle (CPU restatement, all host cores) on 1 spp of the full frame."""
+    """Oracle (CPU restatement, all host cores) on CPU_BASELINE_SPP spp of the full frame."""
     sys.path.insert(0, str(ROOT / "oracle"))
     import oracle_ctypes as O
 
     orc = O.OracleScene(desc)
     t0 = time.perf_counter()
-    film, st = orc.render(W, H, 1, DEPTH, first_sample=0, seed=SEED, threads=threads)
+    film, st = orc.render(W, H, CPU_BASELINE_SPP, DEPTH, first_sample=0, seed=SEED, threads=threads)
     dt = time.perf_counter() - t0
     return {"value": st["paths"] / dt / 1e6, "unit": "Mpaths/s", "cores": O.cores(), "kind": "port",
-            "sample": f"1 spp of the 1920x1080 frame ({st['paths']} paths, depth {DEPTH}) on {O.cpu_model()}",
+            "sample": f"{CPU_BASELINE_SPP} spp of the {W}x{H} frame ({st['paths']} paths, depth {DEPTH}) "
+                      f"on {O.cpu_model()}",
             "segments_per_s": st["segments"] / dt, "seconds": dt}
 
 
@@ -157,6 +167,8 @@ def main():
     ap.add_argument("--spp", type=int, default=SPP, help="override (profiling runs only)")
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-autotune", action="store_true")
+    ap.add_argument("--tuning", default="", help="shade_min_blocks,trace_blocks_per_sm,pool_size: apply "
+                    "these launch choices instead of autotuning (profiling runs)")
     args = ap.parse_args()
     globals().update(W=args.width, H=args.height, SPP=args.spp)
     if args.impl == "reference":
@@ -179,7 +191,12 @@ def main():
     build_s = time.perf_counter() - t0
     r = api.Renderer(scene, W, H, pool_size=args.pool)
     t0 = time.perf_counter()
-    tune = None if args.no_autotune else r.autotune(spp=SPP, max_depth=DEPTH, seed=SEED)
+    if args.tuning:
+        mb, tb, pool = (int(x) for x in args.tuning.split(","))
+        tune = {"shade_min_blocks": mb, "trace_blocks_per_sm": tb, "pool_size": pool, "applied": True}
+        r.set_tuning(tune)
+    else:
+        tune = None if args.no_autotune else r.autotune(spp=SPP, max_depth=DEPTH, seed=SEED)
     tune_s = time.perf_counter() - t0
     cam = desc.scene["camera"]
     film_host = np.zeros((H, W, 3), np.float32)
@@ -254,8 +271,8 @@ def main():
         "roofline": {"bound": "hbm", "kernel": dominant, "achieved": achieved, "peak": peak, "unit": "GB/s",
                      "frac": achieved / peak, "peak_source": "measured" if peaks else "fallback",
                      "bytes_per_unit": bpu, "traffic": None},
-        "e2e": {"value": e2e_value, "unit": "Mpaths/s", "h2d_bytes_per_step": 64 + 40,
-                "d2h_bytes_per_step": W * H * 3 * 4},
+        "e2e": None if args.no_e2e else {"value": e2e_value, "unit": "Mpaths/s", "h2d_bytes_per_step": 64 + 40,
+                                         "d2h_bytes_per_step": W * H * 3 * 4},
         "gpu_launches": int(tot["iterations"] * 4 + args.steps),
         "clocks": clocks,
         "scene_build_s": build_s,

@@ -327,6 +327,11 @@ typedef struct rmd_tune_result {
  * budget, traversal grid and path-pool size.  Compiles the shading-kernel
  * variants it needs (NVRTC, cached on disk).  Clears the film. */
 rmd_status rmd_renderer_autotune(rmd_renderer *r, const rmd_render_settings *settings, rmd_tune_result *out);
+/* Apply launch choices found earlier (by rmd_renderer_autotune, possibly in
+ * another process): shade_min_blocks 1..16, trace_blocks_per_sm 1..32,
+ * pool_size 0 (keep) or >= 1024.  The timing fields are ignored.  Results do
+ * not depend on these choices. */
+rmd_status rmd_renderer_set_tuning(rmd_renderer *r, const rmd_tune_result *tuning);
 
 /* Per-stage device timings and counters of the last rmd_render
  * (RendererCounters, Renderer.swift:13-268). */

@@ -3,6 +3,7 @@
 #include "nodes.h"
 
 #include <algorithm>
+#include <atomic>
 #include <cctype>
 #include <functional>
 #include <map>
@@ -935,6 +936,8 @@ static void coerce(const std::string &type, Kind k, const void *src, Kind dstKin
 }
 
 MaterialProgram::MaterialProgram(const rmd_material &m) {
+    static std::atomic<uint64_t> nextSerial{1};
+    serial_ = nextSerial.fetch_add(1);
     name_ = m.name ? m.name : "";
     std::map<std::string, const rmd_node *> nodes;
     for (int i = 0; i < m.num_nodes; i++) nodes[m.nodes[i].name ? m.nodes[i].name : ""] = &m.nodes[i];
@@ -1065,8 +1068,12 @@ MaterialProgram::MaterialProgram(const rmd_material &m) {
 }
 
 void MaterialProgram::run(const SceneData &ctx, ShadingContext &shading) const {
-    thread_local std::map<const MaterialProgram *, std::vector<std::unique_ptr<NodeImpl>>> cache;
-    auto &inst = cache[this];
+    // Per-thread node instances of each program.  Keyed by serial, not by
+    // address: a program built after another was destroyed may reuse its
+    // address, and must not inherit its node instances.
+    thread_local std::map<uint64_t, std::vector<std::unique_ptr<NodeImpl>>> cache;
+    if (cache.size() > 1024 && !cache.count(serial_)) cache.clear();
+    auto &inst = cache[serial_];
     if (inst.size() != steps_.size()) {
         inst.clear();
         for (auto &s : steps_) inst.push_back(s.proto->clone());

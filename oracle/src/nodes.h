@@ -76,6 +76,7 @@ private:
     std::string name_;
     std::vector<Step> steps_;
     bool hasEmission_ = false;
+    uint64_t serial_ = 0;  // unique per program ever built: keys the per-thread node scratch
 };
 
 }  // namespace orc

@@ -28,6 +28,7 @@ EXPORTS = [
     "rmd_scene_destroy", "rmd_scene_info", "rmd_renderer_create", "rmd_renderer_destroy", "rmd_renderer_set_size",
     "rmd_renderer_reset", "rmd_renderer_set_camera", "rmd_render", "rmd_film_read", "rmd_film_read_f64",
     "rmd_film_samples", "rmd_renderer_stats", "rmd_render_noalloc", "rmd_renderer_autotune",
+    "rmd_renderer_set_tuning",
     "rmd_test_prng", "rmd_test_trace", "rmd_test_material_eval", "rmd_test_generate_source", "rmd_test_jit_compile",
 ]
 
@@ -70,6 +71,7 @@ def lib() -> C.CDLL:
         "rmd_film_samples": ([vp, P(C.c_uint64)], C.c_int32),
         "rmd_renderer_stats": ([vp, P(Stats)], C.c_int32),
         "rmd_renderer_autotune": ([vp, P(RenderSettings), P(_abi.TuneResult)], C.c_int32),
+        "rmd_renderer_set_tuning": ([vp, P(_abi.TuneResult)], C.c_int32),
         "rmd_render_noalloc": ([vp, P(_abi.Camera), C.c_uint32, C.c_uint32, P(RenderSettings), C.c_void_p,
                                 C.c_uint32], C.c_int32),
         "rmd_test_prng": ([C.c_uint32, C.c_uint64, C.c_uint64, C.c_int32, P(C.c_float)], C.c_int32),
@@ -203,6 +205,11 @@ class Renderer:
         res = _abi.TuneResult()
         check(lib().rmd_renderer_autotune(self.h, C.byref(s), C.byref(res)))
         return {k: getattr(res, k) for k, _ in _abi.TuneResult._fields_}
+
+    def set_tuning(self, tuning: dict[str, float]) -> None:
+        """Apply launch choices returned by autotune() (here or in another process)."""
+        t = _abi.TuneResult(**{k: tuning.get(k, 0) for k, _ in _abi.TuneResult._fields_})
+        check(lib().rmd_renderer_set_tuning(self.h, C.byref(t)))
 
     def stats(self) -> dict[str, float]:
         s = Stats()

@@ -42,6 +42,15 @@ rmd_status fail(rmd_status s, const std::string &msg) {
     } while (0)
 
 // Device buffer owned by a scene or renderer.
+// Register budget of the shading kernel before autotuning: at least this many
+// 128-thread blocks per SM (measured best on the 1080p benchmark scene: 5-6);
+// RMD_SHADE_MIN_BLOCKS overrides it.
+static int defaultShadeMinBlocks() {
+    const char *e = std::getenv("RMD_SHADE_MIN_BLOCKS");
+    const int v = e ? std::atoi(e) : 5;
+    return v >= 1 && v <= 16 ? v : 5;
+}
+
 struct DevBuf {
     void *ptr = nullptr;
     size_t bytes = 0;
@@ -112,7 +121,7 @@ struct rmd_renderer {
     cudaKernel_t shade = nullptr;
     int shadeBlocks = 0;
     int shadeMinBlocks = 1;
-    int traceBlocksPerSm = 8;
+    int traceBlocksPerSm = 12;
     DevBuf pool;  // path state, finish list and shadow rays (carvePathPool)
     DevBuf counters, film, film64, resolve;
     Counters *hostCounters = nullptr;  // pinned
@@ -539,12 +548,11 @@ rmd_status rmd_scene_create(rmd_context *ctx, const rmd_scene_desc *d, rmd_scene
     c.focalLength = d->camera.focal_length;
     c.shift = make_float2(d->camera.shift[0], d->camera.shift[1]);
 
-    std::vector<std::string> defs;
-    if (const char *mb = std::getenv("RMD_SHADE_MIN_BLOCKS")) defs.push_back(std::string("-DRMD_SHADE_MIN_BLOCKS=") + mb);
-    const std::string err = rmdhost::compileModule(mod.source, s->jit, defs);
+    s->defaultMinBlocks = defaultShadeMinBlocks();
+    const std::string err = rmdhost::compileModule(
+        mod.source, s->jit, {"-DRMD_SHADE_MIN_BLOCKS=" + std::to_string(s->defaultMinBlocks)});
     if (!err.empty()) return fail(RMD_ERROR_NVRTC, err);
     s->moduleSource = mod.source;
-    s->defaultMinBlocks = std::getenv("RMD_SHADE_MIN_BLOCKS") ? std::atoi(std::getenv("RMD_SHADE_MIN_BLOCKS")) : 1;
     rmd_status r = buildEnvironmentMap(s.get(), d->envmap_exponent);
     if (r != RMD_OK) return r;
     s->shadeBlocks = occupancyBlocks((const void *)s->jit.shade, 128, ctx->smCount);
@@ -890,6 +898,24 @@ rmd_status rmd_renderer_autotune(rmd_renderer *r, const rmd_render_settings *set
     return rmd_renderer_reset(r);
 }
 
+rmd_status rmd_renderer_set_tuning(rmd_renderer *r, const rmd_tune_result *t) {
+    if (!r || !t) return fail(RMD_ERROR_INVALID_ARGUMENT, "NULL argument");
+    if (t->shade_min_blocks < 1 || t->shade_min_blocks > 16 || t->trace_blocks_per_sm < 1 ||
+        t->trace_blocks_per_sm > 32 || (t->pool_size != 0 && t->pool_size < 1024))
+        return fail(RMD_ERROR_INVALID_ARGUMENT, "tuning out of range");
+    RMD_CUDA(cudaSetDevice(r->scene->ctx->device));
+    const int mb = (int)t->shade_min_blocks;
+    rmd_status st = ensureVariants(r->scene, {mb});
+    if (st != RMD_OK) return st;
+    selectShade(r, mb);
+    r->traceBlocksPerSm = (int)t->trace_blocks_per_sm;
+    if (t->pool_size != 0 && t->pool_size != r->capacity) {
+        r->capacity = t->pool_size;
+        if ((st = allocatePool(r)) != RMD_OK) return st;
+    }
+    return RMD_OK;
+}
+
 // --------------------------------------------------------------------- test hooks
 rmd_status rmd_test_prng(uint32_t mode, uint64_t a, uint64_t b, int32_t n, float *out) {
     if (!out || n < 0) return fail(RMD_ERROR_INVALID_ARGUMENT, "invalid arguments");
@@ -967,9 +993,8 @@ rmd_status rmd_test_jit_compile(const rmd_scene_desc *d, int32_t hoist, char *lo
                                                                d->light_materials, d->num_light_materials, hoist != 0);
         std::vector<char> cubin;
         bool cached = false;
-        std::vector<std::string> defs;
-        if (const char *mb = std::getenv("RMD_SHADE_MIN_BLOCKS")) defs.push_back(std::string("-DRMD_SHADE_MIN_BLOCKS=") + mb);
-        std::string err = rmdhost::compileCubin(mod.source, cubin, msg, cached, defs);
+        std::string err = rmdhost::compileCubin(mod.source, cubin, msg, cached,
+                                                {"-DRMD_SHADE_MIN_BLOCKS=" + std::to_string(defaultShadeMinBlocks())});
         if (cubin_bytes) *cubin_bytes = (int64_t)cubin.size();
         if (!err.empty()) {
             if (log && loglen > 0) {

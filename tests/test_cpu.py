@@ -139,3 +139,21 @@ def test_oracle_energy_white_furnace():
     film, _ = O.OracleScene(SceneDesc(sc)).render(16, 16, 64, 8)
     mean = film.mean() / 64
     assert 1.5 < mean < 2.1, mean
+
+
+def test_oracle_scenes_are_independent():
+    """A scene built after others were destroyed renders exactly as a fresh one
+    (the oracle's per-thread node scratch must not outlive its program)."""
+    import gc
+
+    from test_parity_gpu import _all_lights_scene
+
+    desc = SceneDesc(_all_lights_scene())
+    ref, _ = O.OracleScene(desc).render(32, 32, 1, 4, sampling_mode=1)
+    for seed in range(3):
+        other = O.OracleScene(SceneDesc(scenes.cornell(seed=seed, envmap_exponent=4)))
+        other.render(16, 16, 1, 4)
+        del other
+        gc.collect()
+        again, _ = O.OracleScene(desc).render(32, 32, 1, 4, sampling_mode=1)
+        assert np.array_equal(again, ref), seed
