@@ -163,7 +163,7 @@ extern "C" __global__ void __launch_bounds__(128, RMD_SHADE_MIN_BLOCKS) rmd_shad
     const unsigned n = rmd::activeCount(p.counters, p.cur);
     unsigned segments = 0;
     for (unsigned i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x)
-        segments += rmd::shadePath(p, i) ? 1u : 0u;
+        segments += rmd::shadePath(p, rmd::shadingOrder(p.pool.order, p.counters, i)) ? 1u : 0u;
     rmd::blockAdd64(&p.counters->segments, segments);
 }
 

@@ -32,15 +32,27 @@ constexpr uint32_t SHADOW_TO_FINISHED = 0x80000000u;
 // newPaths() camera samples the film kernel of this iteration appends; the
 // shading pass of parity p appends continued paths to S[p ^ 1] (nQ[p ^ 1])
 // and finished ones to the finish list (nF[p]).
+//
+// Every counter that warps of many SMs update with atomics sits in its own
+// 256-byte block, so the counters do not queue behind each other in one L2
+// slice.
 struct Counters {
     uint32_t nQ[2];       // continued paths at the head of each S[p]
+    uint32_t padQ[62];
     uint32_t nF[2];       // finished paths written by the shading pass of parity p
+    uint32_t padF[62];
     uint32_t nShadow;     // shadow rays of this iteration
+    uint32_t padS[63];
     uint32_t traceWork;   // persistent closest-hit work counter
+    uint32_t padT[63];
     uint32_t shadowWork;  // persistent any-hit work counter
+    uint32_t padW[63];
+    uint32_t nHit;        // active paths whose closest-hit ray hit a surface (front of `order`)
+    uint32_t padH[63];
+    uint32_t nMiss;       // ... and that missed (back of `order`)
+    uint32_t padM[63];
     uint32_t errors;
     uint32_t capacity;    // paths in flight at most (size of each S[p])
-    uint32_t pad;
     unsigned long long nextPath;    // next path id handed out by the film kernel
     unsigned long long endPath;     // one past the last path id of this render
     unsigned long long pathsDone;   // paths whose radiance reached the film
@@ -48,6 +60,7 @@ struct Counters {
     unsigned long long shadowRays;  // shadow rays traced
     unsigned long long pad2;
 };
+
 
 // camera samples the film kernel of this iteration appends to S[p]
 __device__ __forceinline__ uint32_t newPaths(const Counters *c, uint32_t p) {
@@ -59,6 +72,13 @@ __device__ __forceinline__ uint32_t newPaths(const Counters *c, uint32_t p) {
 }
 // number of active paths in S[p] after the film kernel of this iteration
 __device__ __forceinline__ uint32_t activeCount(const Counters *c, uint32_t p) { return c->nQ[p] + newPaths(c, p); }
+
+// Position in S[p] of the i-th path to shade: the closest-hit pass lists hits
+// first and misses last, so shading warps see one kind or the other.
+__device__ __forceinline__ uint32_t shadingOrder(const uint32_t *order, const Counters *c, uint32_t i) {
+    const uint32_t nHit = c->nHit;
+    return i < nHit ? order[i] : order[c->capacity - 1u - (i - nHit)];
+}
 
 // One queue-ordered copy of the path state (structure of arrays).
 struct PathState {
@@ -73,6 +93,7 @@ struct PathPool {
     PathState s[2];
     float4 *hit;        // per active path of this iteration: t (<= 0: miss), b0, b1, primitive (bits)
     uint32_t *hitInst;  // instance index
+    uint32_t *order;    // shading order: positions of hits from the front, of misses from the back
     float4 *fin;        // finished paths: radiance.xyz, pixel (bits)
     float4 *shO;        // shadow: origin.xyz, tmax
     float4 *shD;        // shadow: direction.xyz, target (bits; SHADOW_TO_FINISHED)
@@ -86,7 +107,7 @@ struct PathPool {
 constexpr size_t pathPoolBytes(uint32_t capacity) {
     const size_t P = capacity, pad = 255;
     const size_t per16 = (P * 16 + pad) & ~pad, per4 = (P * 4 + pad) & ~pad;
-    return 2 * 5 * per16 + 5 * per16 + per4;
+    return 2 * 5 * per16 + 5 * per16 + 2 * per4;
 }
 inline PathPool carvePathPool(void *base, uint32_t capacity) {
     unsigned char *p = static_cast<unsigned char *>(base);
@@ -109,6 +130,7 @@ inline PathPool carvePathPool(void *base, uint32_t capacity) {
     pool.shD = static_cast<float4 *>(take(16));
     pool.shW = static_cast<float4 *>(take(16));
     pool.hitInst = static_cast<uint32_t *>(take(4));
+    pool.order = static_cast<uint32_t *>(take(4));
     pool.capacity = capacity;
     return pool;
 }

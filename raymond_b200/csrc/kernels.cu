@@ -18,7 +18,7 @@ __global__ void k_frame_init(Counters *cnt, uint32_t capacity, uint64_t firstPat
     cnt->traceWork = cnt->shadowWork = 0;
     cnt->errors = 0;
     cnt->capacity = capacity;
-    cnt->pad = 0;
+    cnt->nHit = cnt->nMiss = 0;
     cnt->nextPath = firstPath;
     cnt->endPath = endPath;
     cnt->pathsDone = 0;
@@ -41,6 +41,8 @@ __global__ void __launch_bounds__(256) k_film_regen(Context ctx, PathPool pool, 
         cnt->nShadow = 0;
         cnt->traceWork = 0;
         cnt->shadowWork = 0;
+        cnt->nHit = 0;
+        cnt->nMiss = 0;
     }
     const uint32_t nFin = cnt->nF[p ^ 1u];
     const uint32_t base = cnt->nQ[p];
@@ -123,9 +125,11 @@ __global__ void __launch_bounds__(128) k_trace_closest(const BvhNode *__restrict
         [&](uint32_t idx, const TraversalState &s) {
             float4 hit;
             uint32_t inst;
-            closestHit(s, tris, hit, inst);
+            const bool found = closestHit(s, tris, hit, inst);
             __stcs(&pool.hit[idx], hit);
             __stcs(&pool.hitInst[idx], inst);
+            if (found) pool.order[warpAppend(&cnt->nHit)] = idx;
+            else pool.order[pool.capacity - 1u - warpAppend(&cnt->nMiss)] = idx;
         });
 }
 

@@ -32,7 +32,8 @@ using namespace rmd;
 
 constexpr uint32_t kMaxPaths = RMD_NOALLOC_MAX_PATHS;
 // counters (padded to 256 B), then the path pool of the largest size
-constexpr size_t kScratchBytes = 256 + pathPoolBytes(kMaxPaths);
+constexpr size_t kCountersBytes = (sizeof(Counters) + 255) & ~size_t(255);
+constexpr size_t kScratchBytes = kCountersBytes + pathPoolBytes(kMaxPaths);
 
 static __device__ __align__(256) unsigned char g_noallocScratch[kScratchBytes];
 
@@ -79,7 +80,7 @@ extern "C" rmd_status rmd_render_noalloc(rmd_scene *scene, const rmd_camera *cam
     }
     const uint32_t P = pool_size ? pool_size : kMaxPaths;
     Counters *cnt = static_cast<Counters *>(base);
-    const PathPool pool = carvePathPool(static_cast<unsigned char *>(base) + 256, P);
+    const PathPool pool = carvePathPool(static_cast<unsigned char *>(base) + kCountersBytes, P);
 
     Context ctx = v.ctx;
     for (int k = 0; k < 4; k++)
