@@ -51,6 +51,10 @@ BYTES_TRACE_PER_RAY = 32 + 20
 BYTES_SHADE_PER_SEGMENT = 84 + 136 + 80 + 48
 BYTES_SHADOW_PER_RAY = 48 + 32
 BYTES_FILM_PER_PATH = 16 + 32 + 80
+# DRAM bytes per unit measured by ncu (dram__bytes_read.sum + dram__bytes_write.sum
+# of one steady-state launch divided by the units it processed; small case, see
+# profiles/ncu_full_spheres_terrain_480x270.md); only the closest-hit kernel's is used
+TRAFFIC_PER_UNIT = {"trace": 106.8}
 CPU_BASELINE_SPP = 16  # oracle sample: 16 spp of the full frame (about 10 s on 16 cores)
 
 
@@ -218,7 +222,7 @@ def main():
         dist.barrier()
     sampler = ClockSampler(local)
     sampler.start()
-    tot_ms, tot = 0.0, {"paths": 0, "segments": 0, "shadow_rays": 0, "iterations": 0, "ms_trace": 0.0,
+    tot_ms, tot = 0.0, {"paths": 0, "segments": 0, "rays": 0, "shadow_rays": 0, "iterations": 0, "ms_trace": 0.0,
                         "ms_shade": 0.0, "ms_shadow": 0.0, "ms_film": 0.0}
     for k in range(args.steps):
         s = step(k)
@@ -249,12 +253,14 @@ def main():
     stage_ms = {"film_regen": tot["ms_film"], "trace": tot["ms_trace"], "shade": tot["ms_shade"],
                 "shadow": tot["ms_shadow"]}
     dominant = max(stage_ms, key=stage_ms.get)
-    units = {"trace": (tot["segments"] + 0.0, BYTES_TRACE_PER_RAY),
+    units = {"trace": (tot["rays"] + 0.0, BYTES_TRACE_PER_RAY),
              "shade": (tot["segments"] + 0.0, BYTES_SHADE_PER_SEGMENT),
              "shadow": (tot["shadow_rays"] + 0.0, BYTES_SHADOW_PER_RAY),
              "film_regen": (tot["paths"] + 0.0, BYTES_FILM_PER_PATH)}
     n_units, bpu = units[dominant]
     achieved = n_units * bpu / (stage_ms[dominant] / 1e3) / 1e9
+    launches = max(1, tot["iterations"])  # one launch of each stage per iteration
+    traffic = TRAFFIC_PER_UNIT[dominant] * n_units / launches if dominant in TRAFFIC_PER_UNIT else None
     peaks = json.loads((ROOT / "MEASURED_PEAKS.json").read_text()) if (ROOT / "MEASURED_PEAKS.json").exists() else {}
     peak = peaks.get("hbm_gbs", 6650.0)
     line = {
@@ -266,11 +272,13 @@ def main():
                    "l2": "inputs larger than L2 (path pool + BVH + film)", "pool_size": r.stats()["pool_size"],
                    "parallelism": f"{world} ranks x disjoint sample ranges"},
         "segments_per_s": seg_rate, "msegments_per_s": seg_rate / 1e6,
+        "mrays_per_s": tot["rays"] * world / (tot_ms / 1e3) / 1e6,
         "stage_ms_per_step": {k: v / args.steps for k, v in stage_ms.items()},
         "iterations_per_step": tot["iterations"] / args.steps,
         "roofline": {"bound": "hbm", "kernel": dominant, "achieved": achieved, "peak": peak, "unit": "GB/s",
                      "frac": achieved / peak, "peak_source": "measured" if peaks else "fallback",
-                     "bytes_per_unit": bpu, "traffic": None},
+                     "bytes_per_unit": bpu, "traffic": traffic,
+                     "units_per_launch": n_units / launches},
         "e2e": None if args.no_e2e else {"value": e2e_value, "unit": "Mpaths/s", "h2d_bytes_per_step": 64 + 40,
                                          "d2h_bytes_per_step": W * H * 3 * 4},
         "gpu_launches": int(tot["iterations"] * 4 + args.steps),

@@ -252,7 +252,7 @@ typedef struct rmd_render_settings {
 
 typedef struct rmd_stats {
     uint64_t paths;            /* camera samples traced to termination */
-    uint64_t segments;         /* closest-hit rays traced and shaded */
+    uint64_t segments;         /* closest-hit rays that hit a surface and were shaded */
     uint64_t shadow_rays;      /* shadow rays traced */
     uint64_t iterations;       /* wavefront iterations of the last render */
     double   ms_total;         /* device time of the last render */
@@ -262,6 +262,7 @@ typedef struct rmd_stats {
     double   ms_film;          /* film accumulation and path regeneration */
     uint32_t pool_size;        /* path slots in flight */
     uint32_t errors;           /* device error flags (queue overflow, watchdog) */
+    uint64_t rays;             /* closest-hit rays traced (segments + misses) */
 } rmd_stats;
 
 typedef struct rmd_context rmd_context;

@@ -118,7 +118,7 @@ class Stats(C.Structure):
     _fields_ = [("paths", C.c_uint64), ("segments", C.c_uint64), ("shadow_rays", C.c_uint64),
                 ("iterations", C.c_uint64), ("ms_total", C.c_double), ("ms_trace", C.c_double),
                 ("ms_shade", C.c_double), ("ms_shadow", C.c_double), ("ms_film", C.c_double),
-                ("pool_size", C.c_uint32), ("errors", C.c_uint32)]
+                ("pool_size", C.c_uint32), ("errors", C.c_uint32), ("rays", C.c_uint64)]
 
 
 def _fptr(a: np.ndarray, ctype=C.c_float):

@@ -161,10 +161,13 @@ __device__ __forceinline__ bool shadePath(const ShadeParams &p, uint32_t i) {
 #endif
 extern "C" __global__ void __launch_bounds__(128, RMD_SHADE_MIN_BLOCKS) rmd_shade(const __grid_constant__ rmd::ShadeParams p) {
     const unsigned n = rmd::activeCount(p.counters, p.cur);
-    unsigned segments = 0;
-    for (unsigned i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x)
+    unsigned segments = 0, rays = 0;
+    for (unsigned i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
         segments += rmd::shadePath(p, rmd::shadingOrder(p.pool.order, p.counters, i)) ? 1u : 0u;
+        rays++;
+    }
     rmd::blockAdd64(&p.counters->segments, segments);
+    rmd::blockAdd64(&p.counters->rays, rays);
 }
 
 // kernels/envmap/build.metal:4-51 — the finest level of the importance map:

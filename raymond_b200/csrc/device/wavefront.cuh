@@ -58,7 +58,7 @@ struct Counters {
     unsigned long long pathsDone;   // paths whose radiance reached the film
     unsigned long long segments;    // closest-hit rays shaded
     unsigned long long shadowRays;  // shadow rays traced
-    unsigned long long pad2;
+    unsigned long long rays;        // closest-hit rays traced (hits and misses)
 };
 
 

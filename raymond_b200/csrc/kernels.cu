@@ -24,7 +24,7 @@ __global__ void k_frame_init(Counters *cnt, uint32_t capacity, uint64_t firstPat
     cnt->pathsDone = 0;
     cnt->segments = 0;
     cnt->shadowRays = 0;
-    cnt->pad2 = 0;
+    cnt->rays = 0;
 }
 
 // ------------------------------------------------------------- film + regeneration

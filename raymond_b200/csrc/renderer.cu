@@ -733,6 +733,7 @@ rmd_status rmd_render(rmd_renderer *r, const rmd_render_settings *s) {
     const Counters &h = *r->hostCounters;
     r->stats.paths = h.pathsDone;
     r->stats.segments = h.segments;
+    r->stats.rays = h.rays;
     r->stats.shadow_rays = h.shadowRays;
     r->stats.iterations = it;
     r->stats.ms_total = ms;

@@ -65,6 +65,8 @@ def test_cornell_accumulated_16spp(cornell):
     assert s["paths"] == 16 * 256 * 256
     # segments (closest-hit rays shaded) agree up to the paths that diverged
     assert abs(s["segments"] - st["segments"]) <= 1e-3 * st["segments"]
+    # every path traces at least its camera ray; misses are rays but not segments
+    assert s["rays"] >= s["segments"] and s["rays"] >= s["paths"]
 
 
 @pytest.mark.parametrize("mode", [SAMPLING_BSDF, SAMPLING_NEE])
