@@ -1,0 +1,75 @@
+"""ctypes binding of oracle/_ref/libref.so, the host build of the reference's
+own device code (oracle/ref/Makefile).  TEST INFRASTRUCTURE ONLY."""
+from __future__ import annotations
+
+import ctypes as C
+from pathlib import Path
+
+import numpy as np
+
+LIB = Path(__file__).resolve().parents[1] / "_ref" / "libref.so"
+_fp = C.POINTER(C.c_float)
+_lib = None
+
+
+def available() -> bool:
+    return LIB.exists()
+
+
+def lib():
+    global _lib
+    if _lib is None:
+        L = C.CDLL(str(LIB))
+        L.ref_prng_tea.argtypes = [C.c_uint32, C.c_uint32, C.c_int, _fp]
+        L.ref_fractal_noise3.argtypes = [_fp, C.c_int, C.c_float, C.c_float, _fp]
+        L.ref_num_materials.restype = C.c_int
+        L.ref_material_eval.argtypes = [C.c_int, _fp, C.c_int, _fp]
+        L.ref_material_eval.restype = C.c_int
+        _lib = L
+    return _lib
+
+
+def prng_tea(a: int, b: int, n: int) -> np.ndarray:
+    out = np.zeros(n, np.float32)
+    lib().ref_prng_tea(a, b, n, out.ctypes.data_as(_fp))
+    return out
+
+
+def fractal_noise3(p: np.ndarray, detail: float, roughness: float) -> np.ndarray:
+    p = np.ascontiguousarray(p, np.float32)
+    out = np.zeros(len(p), np.float32)
+    lib().ref_fractal_noise3(p.ctypes.data_as(_fp), len(p), detail, roughness, out.ctypes.data_as(_fp))
+    return out
+
+
+def material_eval(material: int, records: np.ndarray) -> np.ndarray:
+    records = np.ascontiguousarray(records, np.float32)
+    out = np.zeros((len(records), 16), np.float32)
+    if lib().ref_material_eval(material, records.ctypes.data_as(_fp), len(records), out.ctypes.data_as(_fp)) != 0:
+        raise ValueError(f"no material {material}")
+    return out
+
+
+def shading_records(n: int, seed: int) -> np.ndarray:
+    """Random shading inputs in the record layout of ref_material_eval /
+    oracle_material_eval: unit normals, wo in the normal's hemisphere."""
+    rng = np.random.default_rng(seed)
+
+    def unit(k):
+        v = rng.normal(size=(k, 3))
+        return v / np.linalg.norm(v, axis=1, keepdims=True)
+
+    rec = np.zeros((n, 28), np.float32)
+    nrm = unit(n)
+    rec[:, 0:3] = rng.uniform(0, 20, (n, 3))
+    rec[:, 3:6] = nrm
+    rec[:, 6:9] = nrm
+    rec[:, 9:12] = rng.uniform(0, 1, (n, 3))
+    rec[:, 12:15] = rng.uniform(0, 1, (n, 3))
+    wo = unit(n)
+    wo *= np.sign(np.sum(wo * nrm, 1, keepdims=True))
+    rec[:, 15:18] = wo
+    rec[:, 18:21] = unit(n)
+    rec[:, 21:24] = rng.uniform(0, 1, (n, 3))
+    rec[:, 24] = 1  # camera ray
+    return rec

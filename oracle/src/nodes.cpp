@@ -376,7 +376,7 @@ struct CombineVector {  // nodes.hpp:277-284
 struct MapRange {  // nodes.hpp:314-344
     bool clamp = false;
     float fromMin, fromMax, toMin, toMax, steps, value, result;
-    float3 vector;
+    float3 vector, steps_Float3, from_Min_Float3, from_Max_Float3, to_Min_Float3, to_Max_Float3;
     void compute(const SceneData &, ShadingContext &) {
         float v = (value - fromMin) / (fromMax - fromMin);
         if (clamp) v = saturate(v);
@@ -386,6 +386,8 @@ struct MapRange {  // nodes.hpp:314-344
         using T = MapRange;
         FLD(T, fromMin, K_F1); FLD(T, fromMax, K_F1); FLD(T, toMin, K_F1); FLD(T, toMax, K_F1);
         FLD(T, steps, K_F1); FLD(T, value, K_F1); FLD(T, result, K_F1); FLD(T, vector, K_F3);
+        FLD(T, steps_Float3, K_F3); FLD(T, from_Min_Float3, K_F3); FLD(T, from_Max_Float3, K_F3);
+        FLD(T, to_Min_Float3, K_F3); FLD(T, to_Max_Float3, K_F3);
     }
 };
 struct Value {  // nodes.hpp:1716-1719

@@ -1,0 +1,47 @@
+"""Regenerate tests/golden/ref_pin.npz from the host build of the reference's
+own device code (oracle/_ref/libref.so, built by oracle/ref/Makefile from the
+mounted reference).  Run from the repository root:
+
+    make -C oracle/ref && python tests/golden/make_ref_golden.py
+
+Contents: TEA PRNG streams, fractal noise values and the evaluate/sample
+results of every material in oracle/ref/pin_materials.py on seeded shading
+records, all computed by the reference's code.
+"""
+from __future__ import annotations
+
+import sys
+from pathlib import Path
+
+import numpy as np
+
+ROOT = Path(__file__).resolve().parents[2]
+sys.path.insert(0, str(ROOT / "oracle" / "ref"))
+
+import pin_materials  # noqa: E402
+import ref_ctypes as R  # noqa: E402
+
+PRNG_CASES = [(1, 0), (1, 77), (99, 4242), (123456, 7), (0xFFFFFFFF, 0xFFFFFFFF)]
+NOISE_CASES = [(0.0, 0.5), (2.0, 0.5), (3.5, 0.7), (15.0, 1.0)]
+RECORDS, RECORD_SEED = 512, 2024
+
+
+def main() -> None:
+    out = {}
+    out["prng_cases"] = np.array(PRNG_CASES, np.uint64)
+    out["prng"] = np.stack([R.prng_tea(a, b, 256) for a, b in PRNG_CASES])
+    rng = np.random.default_rng(5)
+    pts = rng.uniform(-50, 50, (2048, 3)).astype(np.float32)
+    out["noise_points"] = pts
+    out["noise_cases"] = np.array(NOISE_CASES, np.float32)
+    out["noise"] = np.stack([R.fractal_noise3(pts, d, r) for d, r in NOISE_CASES])
+    rec = R.shading_records(RECORDS, RECORD_SEED)
+    names = [n for n, _ in pin_materials.materials()]
+    out["records"] = rec
+    out["material_names"] = np.array(names)
+    out["materials"] = np.stack([R.material_eval(m, rec) for m in range(len(names))])
+    np.savez_compressed(ROOT / "tests" / "golden" / "ref_pin.npz", **out)
+
+
+if __name__ == "__main__":
+    main()

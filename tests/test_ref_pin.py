@@ -1,0 +1,75 @@
+"""Pinning the oracle against the reference's own device code.
+
+The reference's Metal device library (PrngState, noise, the node structs, the
+BSDF lobes and UberShader) is compiled for the host by oracle/ref/Makefile
+against a Metal stand-in, and run on the same inputs as the oracle's
+restatement.  tests/golden/ref_pin.npz holds its outputs (made by
+tests/golden/make_ref_golden.py), so the comparison also runs where the
+reference is not mounted; with the host build present the live test checks
+fresh inputs too.
+
+Bars: the TEA stream and fractal noise bit for bit; material evaluate/sample
+results within the image parity tolerance (1e-3 relative, 1e-6 absolute) on
+every record, and within 1e-5 relative on at least 99.5 % of them (the rest
+differ by float rounding inside the sampling routines).
+"""
+import sys
+from pathlib import Path
+
+import numpy as np
+import pytest
+
+import oracle_ctypes as O
+from raymond_b200._abi import RNG_TEA, SceneDesc
+
+sys.path.insert(0, str(Path(__file__).resolve().parents[1] / "oracle" / "ref"))
+import pin_materials  # noqa: E402
+import ref_ctypes as R  # noqa: E402
+
+GOLDEN = Path(__file__).resolve().parent / "golden" / "ref_pin.npz"
+
+
+@pytest.fixture(scope="module")
+def oracle_pin_scene():
+    return O.OracleScene(SceneDesc(pin_materials.scene()))
+
+
+def _close_rows(a, b, rtol):
+    ok = np.isclose(a, b, rtol=rtol, atol=1e-6) | (np.isnan(a) & np.isnan(b))
+    return ok.all(axis=1)
+
+
+def _check_materials(orc, records, ref_out, names):
+    for m, name in enumerate(names):
+        got = orc.material_eval(m, records)
+        assert _close_rows(got, ref_out[m], 1e-3).all(), name
+        assert _close_rows(got, ref_out[m], 1e-5).mean() >= 0.995, name
+        # lobe flags and alpha exactly
+        np.testing.assert_array_equal(got[:, 14], ref_out[m][:, 14], err_msg=name)
+        np.testing.assert_array_equal(got[:, 15], ref_out[m][:, 15], err_msg=name)
+
+
+def test_oracle_matches_reference_golden(oracle_pin_scene):
+    g = np.load(GOLDEN)
+    for (a, b), ref in zip(g["prng_cases"], g["prng"]):
+        got = O.prng(RNG_TEA, int(a), int(b), ref.size)
+        assert np.array_equal(got.view(np.uint32), ref.view(np.uint32)), (a, b)
+    for (d, r), ref in zip(g["noise_cases"], g["noise"]):
+        got = O.fractal_noise3(g["noise_points"], float(d), float(r))
+        assert np.array_equal(got.view(np.uint32), ref.view(np.uint32)), (d, r)
+    names = [str(n) for n in g["material_names"]]
+    assert names == [n for n, _ in pin_materials.materials()]
+    _check_materials(oracle_pin_scene, g["records"], g["materials"], names)
+
+
+@pytest.mark.skipif(not R.available(), reason="host build of the reference (oracle/_ref/libref.so) not present")
+def test_oracle_matches_reference_live(oracle_pin_scene):
+    for a, b in [(3, 5), (2**31 + 11, 17), (65536, 1)]:
+        assert np.array_equal(R.prng_tea(a, b, 300).view(np.uint32), O.prng(RNG_TEA, a, b, 300).view(np.uint32))
+    pts = np.random.default_rng(9).uniform(-1e3, 1e3, (4096, 3)).astype(np.float32)
+    for d, r in [(1.0, 0.3), (6.25, 0.55)]:
+        assert np.array_equal(R.fractal_noise3(pts, d, r).view(np.uint32), O.fractal_noise3(pts, d, r).view(np.uint32))
+    rec = R.shading_records(2048, seed=77)
+    names = [n for n, _ in pin_materials.materials()]
+    ref_out = np.stack([R.material_eval(m, rec) for m in range(len(names))])
+    _check_materials(oracle_pin_scene, rec, ref_out, names)
