@@ -15,8 +15,9 @@ weak scaling, no collective on the data path.
 `e2e`    : the same metric through the public C ABI with host buffers: each
            step uploads the camera (rmd_renderer_set_camera), renders and
            reads the film back to host memory (rmd_film_read).
---impl reference times the CPU restatement of the reference's integrator
-(oracle/, all host cores) on a bounded sample of the same workload.
+--impl reference times the reference's own CPU implementation of the path
+(its device code built for the host, oracle/_ref, all host cores; the oracle
+restatement when that build is absent) on a bounded sample of the workload.
 """
 from __future__ import annotations
 
@@ -55,7 +56,7 @@ BYTES_FILM_PER_PATH = 16 + 32 + 80
 # of one steady-state launch divided by the units it processed; small case, see
 # profiles/ncu_full_spheres_terrain_480x270.md); only the closest-hit kernel's is used
 TRAFFIC_PER_UNIT = {"trace": 106.8}
-CPU_BASELINE_SPP = 16  # oracle sample: 16 spp of the full frame (about 10 s on 16 cores)
+CPU_BASELINE_SPP = 16  # CPU sample: 16 one-spp frames of the full image (about 10-20 s on 16 cores)
 
 
 def rank_info():
@@ -111,19 +112,49 @@ def make_scene():
     return scenes.spheres_terrain(seed=SEED)
 
 
-def cpu_baseline_sample(desc, threads: int = 0):
-    """Oracle (CPU restatement, all host cores) on CPU_BASELINE_SPP spp of the full frame."""
-    sys.path.insert(0, str(ROOT / "oracle"))
-    import oracle_ctypes as O
+class CpuReference:
+    """The reference's own CPU implementation of the path when its host build is
+    present (oracle/_ref/libref.so: the reference's kernels, lights, materials
+    and envmap compiled for the host, all cores), else the oracle (the CPU
+    restatement).  One call renders one 1-spp frame of the full image."""
 
-    orc = O.OracleScene(desc)
+    def __init__(self, desc):
+        sys.path.insert(0, str(ROOT / "oracle"))
+        sys.path.insert(0, str(ROOT / "oracle" / "ref"))
+        import oracle_ctypes as O
+        import ref_ctypes as R
+
+        self.O = O
+        self.orc = O.OracleScene(desc)
+        self.ref = None
+        if R.available():
+            self.ref = R.RefScene(desc, "spheres_terrain", self.orc.surface_emissive())
+        self.kind = "reference" if self.ref is not None else "port"
+
+    def frame(self, k: int) -> dict:
+        if self.ref is not None:
+            film = self.ref.render(W, H, 1, DEPTH, sampling_mode=2, first_frame=k)
+            return {"paths": W * H, "segments": None}
+        _, st = self.orc.render(W, H, 1, DEPTH, first_sample=k, seed=SEED)
+        return st
+
+    def describe(self, frames: int) -> str:
+        what = ("the reference's own kernels (host build of raymond/device: handleIntersections, raytrace, "
+                "lights, envmap, node library; TEA generator)" if self.ref is not None
+                else "the oracle (CPU restatement of the reference's integrator, PCG32)")
+        return f"{frames} x 1 spp of the {W}x{H} frame (depth {DEPTH}) with {what} on {self.O.cpu_model()}"
+
+
+def cpu_baseline_sample(desc):
+    """CPU_BASELINE_SPP frames of the workload on all host cores."""
+    ref = CpuReference(desc)
     t0 = time.perf_counter()
-    film, st = orc.render(W, H, CPU_BASELINE_SPP, DEPTH, first_sample=0, seed=SEED, threads=threads)
+    paths = 0
+    for k in range(CPU_BASELINE_SPP):
+        paths += ref.frame(k)["paths"]
     dt = time.perf_counter() - t0
-    return {"value": st["paths"] / dt / 1e6, "unit": "Mpaths/s", "cores": O.cores(), "kind": "port",
-            "sample": f"{CPU_BASELINE_SPP} spp of the {W}x{H} frame ({st['paths']} paths, depth {DEPTH}) "
-                      f"on {O.cpu_model()}",
-            "segments_per_s": st["segments"] / dt, "seconds": dt}
+    return {"value": paths / dt / 1e6, "unit": "Mpaths/s", "cores": ref.O.cores(), "kind": ref.kind,
+            "sample": ref.describe(CPU_BASELINE_SPP), "seconds": dt}
 
 
 def run_reference(args):
@@ -133,27 +164,23 @@ def run_reference(args):
     from raymond_b200._abi import SceneDesc
 
     desc = SceneDesc(make_scene())
-    sys.path.insert(0, str(ROOT / "oracle"))
-    import oracle_ctypes as O
-
-    orc = O.OracleScene(desc)
+    ref = CpuReference(desc)
     # one step = 1 spp of the full frame (a bounded sample of the 64-spp step)
-    for _ in range(args.warmup):
-        orc.render(W, H, 1, DEPTH, first_sample=0, seed=SEED)
+    for k in range(args.warmup):
+        ref.frame(k)
     paths, secs = 0, 0.0
     for k in range(args.steps):
         t0 = time.perf_counter()
-        _, st = orc.render(W, H, 1, DEPTH, first_sample=k, seed=SEED)
+        paths += ref.frame(k)["paths"]
         secs += time.perf_counter() - t0
-        paths += st["paths"]
     v = paths / secs / 1e6
     line = {"impl": "reference", "metric": METRIC, "value": v, "unit": "Mpaths/s", "n_gpus": world,
             "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 * secs / args.steps,
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
             "config": {"workload": WORKLOAD, "width": W, "height": H, "spp": SPP, "max_depth": DEPTH,
                        "step": "1 spp of the frame per step (bounded CPU sample)"},
-            "cpu_baseline": {"value": v, "unit": "Mpaths/s", "cores": O.cores(), "kind": "port",
-                             "sample": f"1 spp of the 1920x1080 frame per step on {O.cpu_model()}"},
+            "cpu_baseline": {"value": v, "unit": "Mpaths/s", "cores": ref.O.cores(), "kind": ref.kind,
+                             "sample": ref.describe(args.steps)},
             "e2e": {"value": v, "unit": "Mpaths/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
     print(json.dumps(line), flush=True)
 

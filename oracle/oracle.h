@@ -42,6 +42,8 @@ typedef struct oracle_settings {
 /* returns 0 or an RMD_ERROR_* code; err receives a message */
 int oracle_scene_create(const rmd_scene_desc *desc, oracle_scene **out, char *err, int errlen);
 void oracle_scene_destroy(oracle_scene *s);
+/* per surface material: 1 if it emits; returns the number of materials */
+int oracle_surface_emissive(const oracle_scene *s, uint8_t *out);
 int oracle_scene_info(const oracle_scene *s, uint64_t *triangles, int32_t *num_lights_total, int32_t *num_shape_lights);
 
 /* Film sums (W*H*3, row-major from the top-left pixel) of `spp` frames;

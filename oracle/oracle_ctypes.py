@@ -39,6 +39,7 @@ def lib():
         L = C.CDLL(str(LIB))
         L.oracle_scene_create.argtypes = [C.c_void_p, C.POINTER(C.c_void_p), C.c_char_p, C.c_int]
         L.oracle_scene_destroy.argtypes = [C.c_void_p]
+        L.oracle_surface_emissive.argtypes = [C.c_void_p, C.POINTER(C.c_uint8)]
         L.oracle_scene_info.argtypes = [C.c_void_p, C.POINTER(C.c_uint64), C.POINTER(C.c_int32),
                                         C.POINTER(C.c_int32)]
         L.oracle_render.argtypes = [C.c_void_p, C.POINTER(OracleSettings), C.POINTER(C.c_double),
@@ -72,6 +73,12 @@ class OracleScene:
         if getattr(self, "h", None) and self.h.value:
             lib().oracle_scene_destroy(self.h)
             self.h = C.c_void_p()
+
+    def surface_emissive(self) -> np.ndarray:
+        """Per surface material: 1 if it emits (a shape carrying it is a shape light)."""
+        out = np.zeros(len(self.desc.scene["materials"]), np.uint8)
+        lib().oracle_surface_emissive(self.h, out.ctypes.data_as(C.POINTER(C.c_uint8)))
+        return out
 
     def info(self):
         t = C.c_uint64()

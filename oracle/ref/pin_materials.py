@@ -164,3 +164,19 @@ def scene() -> dict:
     for sh in sc["shapes"]:
         sh["materials"] = np.zeros_like(sh["materials"])
     return sc
+
+
+def ref_scenes() -> dict[str, dict]:
+    """Scenes whose materials the host build of the reference carries (one
+    dispatch table each), by name: the pinning material set and the scenes of
+    the reference-render comparison."""
+    from raymond_b200 import scenes
+
+    return {
+        "pin": scene(),
+        "cornell": scenes.cornell(seed=1, envmap_exponent=6),
+        "cornell_all_lights": scenes.cornell_all_lights(seed=4, envmap_exponent=5),
+        "spheres_small": scenes.spheres_terrain(seed=3, num_spheres=12, terrain_cells=64, envmap_exponent=6),
+        # the benchmark scene (bench.py's reference arm)
+        "spheres_terrain": scenes.spheres_terrain(seed=1),
+    }

@@ -25,6 +25,11 @@ def lib():
         L.ref_num_materials.restype = C.c_int
         L.ref_material_eval.argtypes = [C.c_int, _fp, C.c_int, _fp]
         L.ref_material_eval.restype = C.c_int
+        L.ref_scene_create.argtypes = [C.c_void_p, C.c_char_p, C.POINTER(C.c_uint8)]
+        L.ref_scene_create.restype = C.c_void_p
+        L.ref_scene_destroy.argtypes = [C.c_void_p]
+        L.ref_render.argtypes = [C.c_void_p] + [C.c_uint32] * 6 + [_fp]
+        L.ref_render.restype = C.c_int
         _lib = L
     return _lib
 
@@ -73,3 +78,29 @@ def shading_records(n: int, seed: int) -> np.ndarray:
     rec[:, 21:24] = rng.uniform(0, 1, (n, 3))
     rec[:, 24] = 1  # camera ray
     return rec
+
+
+class RefScene:
+    """A scene set up for the reference's own kernels (host build).  `table`
+    names its generated materials (pin_materials.ref_scenes); `emissive` is the
+    per-surface-material emission flag (oracle_ctypes.OracleScene.surface_emissive)."""
+
+    def __init__(self, desc, table: str, emissive: np.ndarray):
+        self.desc = desc  # keeps the arrays the C structs point to alive
+        self.emissive = np.ascontiguousarray(emissive, np.uint8)
+        self.h = lib().ref_scene_create(C.byref(desc.c), table.encode(),
+                                        self.emissive.ctypes.data_as(C.POINTER(C.c_uint8)))
+        if not self.h:
+            raise ValueError(f"no material table {table!r} in the reference build")
+
+    def __del__(self):
+        if getattr(self, "h", None):
+            lib().ref_scene_destroy(self.h)
+            self.h = None
+
+    def render(self, width: int, height: int, frames: int, max_depth: int, sampling_mode: int = 2,
+               first_frame: int = 0) -> np.ndarray:
+        """Film (H, W, 4): rgb sums and write counts after `frames` one-sample frames."""
+        film = np.zeros((height, width, 4), np.float32)
+        lib().ref_render(self.h, width, height, frames, max_depth, sampling_mode, first_frame, film.ctypes.data_as(_fp))
+        return film

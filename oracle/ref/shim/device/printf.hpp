@@ -1,4 +1,4 @@
 // Stand-in for the reference's device/printf.hpp (a debug printf into a Metal
-// buffer): the host build of the reference's device code prints nothing.
+// buffer): none of the compiled device code prints, so the host build needs
+// nothing from it.
 #pragma once
-#define printf(...) ((void)0)

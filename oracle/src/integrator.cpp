@@ -507,6 +507,13 @@ extern "C" int oracle_scene_create(const rmd_scene_desc *d, oracle_scene **out, 
 
 extern "C" void oracle_scene_destroy(oracle_scene *s) { delete s; }
 
+// Per surface material: 1 if it emits (Material.hasSurfaceEmission), which makes
+// a shape carrying it a shape light.
+extern "C" int oracle_surface_emissive(const oracle_scene *s, uint8_t *out) {
+    for (size_t i = 0; i < s->data.surfaceShaders.size(); i++) out[i] = s->data.surfaceShaders[i]->hasSurfaceEmission();
+    return (int)s->data.surfaceShaders.size();
+}
+
 extern "C" int oracle_scene_info(const oracle_scene *s, uint64_t *triangles, int32_t *num_lights_total,
                                  int32_t *num_shape_lights) {
     if (triangles) *triangles = s->triangles;

@@ -6,7 +6,10 @@ mounted reference).  Run from the repository root:
 
 Contents: TEA PRNG streams, fractal noise values and the evaluate/sample
 results of every material in oracle/ref/pin_materials.py on seeded shading
-records, all computed by the reference's code.
+records, all computed by the reference's code (ref_pin.npz); and one-sample
+images of the reference-render scenes rendered by the reference's own kernels
+(raytrace, handleIntersections, raytraceAny, handleShadowRays, the lights and
+the environment map) in all three sampling modes (ref_render.npz).
 """
 from __future__ import annotations
 
@@ -18,12 +21,21 @@ import numpy as np
 ROOT = Path(__file__).resolve().parents[2]
 sys.path.insert(0, str(ROOT / "oracle" / "ref"))
 
+sys.path.insert(0, str(ROOT / "oracle"))
+sys.path.insert(0, str(ROOT))
+
+import oracle_ctypes as O  # noqa: E402
 import pin_materials  # noqa: E402
 import ref_ctypes as R  # noqa: E402
+from raymond_b200._abi import SceneDesc  # noqa: E402
 
 PRNG_CASES = [(1, 0), (1, 77), (99, 4242), (123456, 7), (0xFFFFFFFF, 0xFFFFFFFF)]
 NOISE_CASES = [(0.0, 0.5), (2.0, 0.5), (3.5, 0.7), (15.0, 1.0)]
 RECORDS, RECORD_SEED = 512, 2024
+# reference-render images: scene, width, height, max depth, first frames
+RENDER_CASES = [("cornell", 48, 40, 8, [0, 5]), ("cornell_all_lights", 48, 40, 6, [0, 3]),
+                ("spheres_small", 64, 36, 12, [0, 1])]
+SAMPLING_MODES = [0, 1, 2]  # BSDF, NEE, MIS
 
 
 def main() -> None:
@@ -41,6 +53,17 @@ def main() -> None:
     out["material_names"] = np.array(names)
     out["materials"] = np.stack([R.material_eval(m, rec) for m in range(len(names))])
     np.savez_compressed(ROOT / "tests" / "golden" / "ref_pin.npz", **out)
+
+    scenes = pin_materials.ref_scenes()
+    renders = {}
+    for name, w, h, depth, frames in RENDER_CASES:
+        desc = SceneDesc(scenes[name])
+        ref = R.RefScene(desc, name, O.OracleScene(desc).surface_emissive())
+        renders[f"{name}/size"] = np.array([w, h, depth], np.int32)
+        for mode in SAMPLING_MODES:
+            for f in frames:
+                renders[f"{name}/{mode}/{f}"] = ref.render(w, h, 1, depth, sampling_mode=mode, first_frame=f)
+    np.savez_compressed(ROOT / "tests" / "golden" / "ref_render.npz", **renders)
 
 
 if __name__ == "__main__":

@@ -150,32 +150,7 @@ def test_material_eval_parity(spheres):
 
 
 def _all_lights_scene():
-    """Cornell box lit by every light type of the reference plus a textured world
-    (Background colour from a noise texture, so the environment importance map is
-    non-uniform); the room's open front lets paths escape to the world."""
-    from raymond_b200 import materials as M
-
-    sc = scenes.cornell(seed=4, envmap_exponent=7)
-    world = M.world((1.0, 1.0, 1.0, 1.0), 2.0)
-    world["Noise Texture"] = {
-        "type": "TEX_NOISE",
-        "inputs": {"Vector": {"type": "VECTOR", "value": [0, 0, 0]}, "W": {"type": "VALUE", "value": 0.0},
-                   "Scale": {"type": "VALUE", "value": 3.0}, "Detail": {"type": "VALUE", "value": 1.0},
-                   "Roughness": {"type": "VALUE", "value": 0.5}, "Distortion": {"type": "VALUE", "value": 0.0}},
-        "parameters": {"noise_dimensions": "3D"}}
-    world["Background"]["inputs"]["Color"] = {"type": "RGBA", "links": [["Noise Texture", "Color"]]}
-    lamp = M.light((1.0, 0.9, 0.8, 1.0), 1.0)
-    sc["light_materials"] = [("world", world), ("lamp", lamp)]
-    tr = np.array([[0.2, 0, 0, 0.5], [0, 0, 0.2, 0.95], [0, -0.2, 0, 0.5]], np.float32)  # facing down
-    sc["area_lights"] = [{"shader": 1, "transform": tr, "color": (4.0, 4.0, 4.0), "is_circular": False},
-                         {"shader": 1, "transform": tr * np.array([[1], [1], [1]]) + np.array([[0, 0, 0, 0.2], [0, 0, 0, 0], [0, 0, 0, 0]]),
-                          "color": (3.0, 2.0, 1.0), "is_circular": True}]
-    sc["point_lights"] = [{"shader": 1, "location": (0.3, 0.7, 0.6), "radius": 0.05, "color": (2.0, 2.0, 2.0)},
-                          {"shader": 1, "location": (0.7, 0.5, 0.7), "radius": 0.0, "color": (1.0, 1.5, 2.0)}]
-    sc["spot_lights"] = [{"shader": 1, "location": (0.5, 0.9, 0.8), "direction": (0.0, -1.0, -0.3), "radius": 0.03,
-                          "color": (6.0, 6.0, 6.0), "spot_size": 1.0, "spot_blend": 0.3}]
-    sc["sun_lights"] = [{"shader": 1, "direction": (0.2, 0.3, 1.0), "angle": 0.1, "color": (1.0, 1.0, 1.0)}]
-    return sc
+    return scenes.cornell_all_lights(seed=4, envmap_exponent=7)
 
 
 @pytest.mark.parametrize("mode", [SAMPLING_MIS, SAMPLING_NEE])

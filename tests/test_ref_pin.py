@@ -73,3 +73,52 @@ def test_oracle_matches_reference_live(oracle_pin_scene):
     names = [n for n, _ in pin_materials.materials()]
     ref_out = np.stack([R.material_eval(m, rec) for m in range(len(names))])
     _check_materials(oracle_pin_scene, rec, ref_out, names)
+
+
+# ---------------------------------------------------------------- whole images
+# One-sample images rendered by the reference's own kernels (host build, TEA
+# generator as generateRays seeds it) against the oracle's TEA mode: the same
+# per-sample parity bar as the GPU tests.
+RENDER_GOLDEN = Path(__file__).resolve().parent / "golden" / "ref_render.npz"
+REL, ABS, MIN_MATCH = 1e-3, 1e-6, 0.999
+
+
+def _match(ref_film, cpu):
+    ref = ref_film[..., :3].astype(np.float64)
+    ok = np.abs(ref - cpu) <= REL * np.abs(cpu) + ABS
+    return float(ok.all(axis=-1).mean())
+
+
+@pytest.fixture(scope="module")
+def ref_scene_descs():
+    return {k: SceneDesc(v) for k, v in pin_materials.ref_scenes().items() if k != "pin"}
+
+
+def test_oracle_images_match_reference_golden(ref_scene_descs):
+    g = np.load(RENDER_GOLDEN)
+    cases = {}
+    for key in g.files:
+        name, rest = key.split("/", 1)
+        if rest != "size":
+            cases.setdefault(name, []).append(key)
+    assert set(cases) == {"cornell", "cornell_all_lights", "spheres_small"}
+    for name, keys in cases.items():
+        w, h, depth = (int(x) for x in g[f"{name}/size"])
+        orc = O.OracleScene(ref_scene_descs[name])
+        for key in keys:
+            _, mode, frame = key.split("/")
+            cpu, _ = orc.render(w, h, 1, depth, sampling_mode=int(mode), rng=RNG_TEA, first_sample=int(frame))
+            assert _match(g[key], cpu) >= MIN_MATCH, key
+
+
+@pytest.mark.skipif(not R.available(), reason="host build of the reference (oracle/_ref/libref.so) not present")
+@pytest.mark.parametrize("name", ["cornell", "cornell_all_lights", "spheres_small"])
+def test_oracle_images_match_reference_live(ref_scene_descs, name):
+    desc = ref_scene_descs[name]
+    orc = O.OracleScene(desc)
+    ref = R.RefScene(desc, name, orc.surface_emissive())
+    for mode in (0, 1, 2):
+        for frame in (2, 9):
+            rf = ref.render(40, 30, 1, 10, sampling_mode=mode, first_frame=frame)
+            cpu, _ = orc.render(40, 30, 1, 10, sampling_mode=mode, rng=RNG_TEA, first_sample=frame)
+            assert _match(rf, cpu) >= MIN_MATCH, (mode, frame)
