@@ -345,7 +345,7 @@ rmd_status rmd_renderer_stats(const rmd_renderer *r, rmd_stats *out);
  * allocation, a real-time loop that must not pay allocation latency, a
  * process held to a fixed memory budget): renders like rmd_render but keeps
  * its path pool, queues and counters in one fixed device array compiled into
- * the library (RMD_NOALLOC_MAX_PATHS paths, about 5.5 MB, reserved on every
+ * the library (RMD_NOALLOC_MAX_PATHS paths, about 8.1 MB, reserved on every
  * GPU that loads the library until it is unloaded) and never calls
  * cudaMalloc, cudaFree or any other allocating routine.
  *
