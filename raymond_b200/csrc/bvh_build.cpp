@@ -4,9 +4,9 @@
 // primitive structure per shape plus an instance structure
 // (ShapeBuilder.swift:7-94,302-319; EntityBuilder.swift:148-165).  Here all
 // instances are flattened into one binary BVH over world-space triangles,
-// built with binned SAH (32 bins per axis) and OpenMP tasks for subtrees.
-// Leaves hold 1..8 triangles; depth is capped so the 64-entry traversal stack
-// cannot overflow.
+// built with binned SAH (32 bins per axis) and OpenMP tasks for subtrees as a
+// binary tree with leaves of 1..3 triangles, then collapsed into the
+// compressed 8-wide form (80-byte nodes) the traversal kernels walk.
 #include "bvh_build.h"
 
 #include <algorithm>
@@ -51,13 +51,22 @@ struct Prim {
 };
 
 constexpr int kBins = 32;
-constexpr int kMaxLeaf = 8;
+constexpr int kMaxLeaf = 3;
 constexpr int kMaxDepth = 56;
+
+// binary node with its own bounds, the input of the 8-wide collapse
+struct BinNode {
+    Box box;
+    int child[2];           // -1 for a leaf
+    uint32_t first, count;  // the subtree's triangles: [first, first + count) of Builder::prims
+    bool leaf() const { return child[0] < 0; }
+};
 
 struct Builder {
     std::vector<Prim> prims;
-    std::vector<GpuBvhNode> nodes;
+    std::vector<BinNode> bin;
     std::atomic<uint32_t> nodeCount{0};
+    size_t maxLeaf = kMaxLeaf;
 
     static void rangeBounds(const Prim *p, size_t n, Box &box, Box &cbox) {
         for (size_t i = 0; i < n; i++) {
@@ -109,7 +118,7 @@ struct Builder {
         }
         // SAH leaf test: traversal cost 1, intersection cost 1 per triangle
         const float leafCost = box.area() * (float)n;
-        const bool forceSplit = n > (size_t)kMaxLeaf;
+        const bool forceSplit = n > maxLeaf;
         if (!forceSplit && (bestAxis < 0 || bestCost + box.area() >= leafCost)) return b;
         size_t mid = b;
         if (bestAxis >= 0 && depth < kMaxDepth) {
@@ -137,50 +146,192 @@ struct Builder {
         return mid;
     }
 
-    static int leafLink(size_t first, size_t count) { return ~(int)(((uint32_t)first << 3) | (uint32_t)(count - 1)); }
-
-    // builds the subtree of [b, e) whose bounds the parent already stored; returns its link
-    int build(size_t b, size_t e, int depth) {
+    // binary tree with node bounds over [b, e); returns the node index
+    int buildBin(size_t b, size_t e, int depth) {
         Box box, cbox;
         rangeBounds(prims.data() + b, e - b, box, cbox);
-        const size_t mid = split(b, e, box, cbox, depth);
-        if (mid == b) return leafLink(b, e - b);
         const uint32_t id = nodeCount.fetch_add(1);
-        fillNode(id, b, mid, e, depth);
+        bin[id].box = box;
+        const size_t mid = split(b, e, box, cbox, depth);
+        if (mid == b) {
+            bin[id].child[0] = bin[id].child[1] = -1;
+            bin[id].first = (uint32_t)b;
+            bin[id].count = (uint32_t)(e - b);
+            return (int)id;
+        }
+        int l = 0, r = 0;
+        if (e - b > (size_t)(1 << 14)) {
+#pragma omp task shared(l) firstprivate(b, mid, depth)
+            l = buildBin(b, mid, depth + 1);
+#pragma omp task shared(r) firstprivate(mid, e, depth)
+            r = buildBin(mid, e, depth + 1);
+#pragma omp taskwait
+        } else {
+            l = buildBin(b, mid, depth + 1);
+            r = buildBin(mid, e, depth + 1);
+        }
+        bin[id].child[0] = l;
+        bin[id].child[1] = r;
+        bin[id].first = (uint32_t)b;
+        bin[id].count = (uint32_t)(e - b);
         return (int)id;
     }
 
-    void fillNode(uint32_t id, size_t b, size_t mid, size_t e, int depth) {
-        Box lb, lc, rb, rc;
-        rangeBounds(prims.data() + b, mid - b, lb, lc);
-        rangeBounds(prims.data() + mid, e - mid, rb, rc);
-        GpuBvhNode &node = nodes[id];
-        node.c0xy[0] = lb.lo[0]; node.c0xy[1] = lb.hi[0]; node.c0xy[2] = lb.lo[1]; node.c0xy[3] = lb.hi[1];
-        node.c1xy[0] = rb.lo[0]; node.c1xy[1] = rb.hi[0]; node.c1xy[2] = rb.lo[1]; node.c1xy[3] = rb.hi[1];
-        node.cz[0] = lb.lo[2]; node.cz[1] = lb.hi[2]; node.cz[2] = rb.lo[2]; node.cz[3] = rb.hi[2];
-        int l = 0, r = 0;
-        const size_t big = 1 << 14;
-        if (e - b > big) {
-#pragma omp task shared(l) firstprivate(b, mid, depth)
-            l = build(b, mid, depth + 1);
-#pragma omp task shared(r) firstprivate(mid, e, depth)
-            r = build(mid, e, depth + 1);
-#pragma omp taskwait
-        } else {
-            l = build(b, mid, depth + 1);
-            r = build(mid, e, depth + 1);
+};
+
+// Collapses the binary tree into 8-wide nodes (depth first).  Any subtree of
+// at most 3 triangles is a leaf (its triangles are consecutive), so a node
+// holds at most 24 triangles.  A node takes its binary children and opens
+// the inner child of largest surface area while it has fewer than 8.  (Filling
+// the bottom nodes instead, by opening only subtrees of more than 8 leaves,
+// gave fewer nodes but more node visits per ray.)  Children go to the slot whose octant direction best matches
+// their offset from the node centre, so a ray visits them roughly front to
+// back by taking slot ^ (ray octant) in increasing order.
+struct WideCollapse {
+    const std::vector<BinNode> &bin;
+    const std::vector<Prim> &prims;
+    std::vector<GpuWideNode> nodes;
+    std::vector<uint32_t> triOrder;  // output triangle -> index into prims
+
+    static constexpr uint32_t kLeafTris = 3;
+    bool isLeaf(int i) const { return bin[i].leaf() || bin[i].count <= kLeafTris; }
+
+    // Quantised child bounds, conservative in float: origin + q * scale
+    // encloses the child on every side.
+    static void quantise(const Box &node, const Box *kids, const bool *used, GpuWideNode &w) {
+        for (int k = 0; k < 3; k++) {
+            const float lo = node.lo[k], extent = node.hi[k] - node.lo[k];
+            int e = -100;
+            if (extent > 0.0f) {
+                int ex;
+                std::frexp(extent / 255.0f, &ex);
+                e = ex;
+                while (node.lo[k] + 255.0f * std::ldexp(1.0f, e) < node.hi[k]) e++;
+            }
+            e = std::max(-126, std::min(127, e));
+            const float scale = std::ldexp(1.0f, e);
+            w.origin[k] = lo;
+            w.exponent[k] = (uint8_t)(e + 127);
+            for (int c = 0; c < 8; c++) {
+                if (!used[c]) {  // empty slot: an inverted box
+                    w.qlo[k][c] = 255;
+                    w.qhi[k][c] = 0;
+                    continue;
+                }
+                int ql = (int)std::floor((kids[c].lo[k] - lo) / scale);
+                int qh = (int)std::ceil((kids[c].hi[k] - lo) / scale);
+                ql = std::max(0, std::min(255, ql));
+                qh = std::max(0, std::min(255, qh));
+                while (ql > 0 && lo + (float)ql * scale > kids[c].lo[k]) ql--;
+                while (qh < 255 && lo + (float)qh * scale < kids[c].hi[k]) qh++;
+                w.qlo[k][c] = (uint8_t)ql;
+                w.qhi[k][c] = (uint8_t)qh;
+            }
         }
-        node.link[0] = l;
-        node.link[1] = r;
-        node.link[2] = node.link[3] = 0;
+    }
+
+    void emit(int binIdx, uint32_t wideIdx) {
+        int kids[8];
+        int nk = 0;
+        const BinNode &root = bin[binIdx];
+        if (isLeaf(binIdx)) {
+            kids[nk++] = binIdx;  // the whole scene is one leaf
+        } else {
+            kids[nk++] = root.child[0];
+            kids[nk++] = root.child[1];
+        }
+        while (nk < 8) {
+            int best = -1;
+            float bestArea = -1.0f;
+            for (int i = 0; i < nk; i++) {
+                const BinNode &c = bin[kids[i]];
+                if (!isLeaf(kids[i]) && c.box.area() > bestArea) {
+                    bestArea = c.box.area();
+                    best = i;
+                }
+            }
+            if (best < 0) break;
+            const int k = kids[best];
+            kids[best] = bin[k].child[0];
+            kids[nk++] = bin[k].child[1];
+        }
+        // slots: bit k of a slot means "on the high side of axis k"
+        Box nodeBox;
+        for (int i = 0; i < nk; i++) nodeBox.grow(bin[kids[i]].box);
+        float centre[3];
+        for (int k = 0; k < 3; k++) centre[k] = 0.5f * (nodeBox.lo[k] + nodeBox.hi[k]);
+        float score[8][8];
+        for (int i = 0; i < nk; i++) {
+            const Box &b = bin[kids[i]].box;
+            for (int sl = 0; sl < 8; sl++) {
+                float v = 0.0f;
+                for (int k = 0; k < 3; k++) {
+                    const float off = 0.5f * (b.lo[k] + b.hi[k]) - centre[k];
+                    v += ((sl >> k) & 1) ? off : -off;
+                }
+                score[i][sl] = v;
+            }
+        }
+        int slotKid[8] = {-1, -1, -1, -1, -1, -1, -1, -1};
+        bool kidDone[8] = {};
+        for (int round = 0; round < nk; round++) {
+            int bi = -1, bs = -1;
+            float bv = -FLT_MAX;
+            for (int i = 0; i < nk; i++) {
+                if (kidDone[i]) continue;
+                for (int sl = 0; sl < 8; sl++)
+                    if (slotKid[sl] < 0 && score[i][sl] > bv) {
+                        bv = score[i][sl];
+                        bi = i;
+                        bs = sl;
+                    }
+            }
+            kidDone[bi] = true;
+            slotKid[bs] = bi;
+        }
+        GpuWideNode w;
+        std::memset(&w, 0, sizeof(w));
+        Box boxes[8];
+        bool used[8];
+        int numInner = 0;
+        for (int sl = 0; sl < 8; sl++) {
+            used[sl] = slotKid[sl] >= 0;
+            if (used[sl]) {
+                boxes[sl] = bin[kids[slotKid[sl]]].box;
+                if (!isLeaf(kids[slotKid[sl]])) numInner++;
+            }
+        }
+        quantise(nodeBox, boxes, used, w);
+        w.childBase = (uint32_t)nodes.size();
+        nodes.resize(nodes.size() + numInner);
+        w.triBase = (uint32_t)triOrder.size();
+        int innerBin[8];
+        int ni = 0;
+        for (int sl = 0; sl < 8; sl++) {
+            if (!used[sl]) continue;
+            const BinNode &c = bin[kids[slotKid[sl]]];
+            if (!isLeaf(kids[slotKid[sl]])) {
+                w.imask |= (uint8_t)(1u << sl);
+                innerBin[ni++] = kids[slotKid[sl]];
+            } else {
+                const uint32_t offset = (uint32_t)triOrder.size() - w.triBase;
+                w.meta[sl] = (uint8_t)((((1u << c.count) - 1u) << 5) | offset);
+                for (uint32_t t = 0; t < c.count; t++) triOrder.push_back(c.first + t);
+            }
+        }
+        nodes[wideIdx] = w;
+        for (int i = 0; i < ni; i++) emit(innerBin[i], w.childBase + (uint32_t)i);
     }
 };
 
 }  // namespace
 
-void buildBvh(const std::vector<float> &v0, const std::vector<float> &v1, const std::vector<float> &v2,
-              const std::vector<uint32_t> &instance, const std::vector<uint32_t> &prim, GpuBvh &out) {
+void buildWideBvh(const std::vector<float> &v0, const std::vector<float> &v1, const std::vector<float> &v2,
+                  const std::vector<uint32_t> &instance, const std::vector<uint32_t> &prim, GpuWideBvh &out) {
     const size_t n = instance.size();
+    out.nodes.clear();
+    out.tris.clear();
+    if (n == 0) return;  // no nodes: the traversal kernels treat a null node array as "everything misses"
     Builder B;
     B.prims.resize(n);
 #pragma omp parallel for schedule(static)
@@ -193,38 +344,21 @@ void buildBvh(const std::vector<float> &v0, const std::vector<float> &v1, const 
         for (int k = 0; k < 3; k++) p.c[k] = 0.5f * (p.box.lo[k] + p.box.hi[k]);
         p.idx = (uint32_t)i;
     }
-    B.nodes.resize(std::max<size_t>(1, 2 * n));
-    B.nodeCount = 1;  // node 0 is the root
-    if (n == 0) {
-        // no triangles: no nodes; the traversal kernels treat a null node array as "everything misses"
-        out.nodes.clear();
-        out.tris.clear();
-        return;
-    } else {
-        Box box, cbox;
-        Builder::rangeBounds(B.prims.data(), n, box, cbox);
-        size_t mid = B.split(0, n, box, cbox, 0);
-        if (mid == 0) {
-            // the whole scene is one leaf: both children of the root are that leaf
-            GpuBvhNode &root = B.nodes[0];
-            root.c0xy[0] = box.lo[0]; root.c0xy[1] = box.hi[0]; root.c0xy[2] = box.lo[1]; root.c0xy[3] = box.hi[1];
-            root.cz[0] = box.lo[2]; root.cz[1] = box.hi[2];
-            for (int k = 0; k < 4; k++) root.c1xy[k] = root.c0xy[k];
-            root.cz[2] = box.lo[2]; root.cz[3] = box.hi[2];
-            root.link[0] = root.link[1] = Builder::leafLink(0, n);
-            root.link[2] = root.link[3] = 0;
-        } else {
+    B.bin.resize(2 * n);
+    B.nodeCount = 0;
+    int root = 0;
 #pragma omp parallel
 #pragma omp single
-            B.fillNode(0, 0, mid, n, 0);
-        }
-    }
-    const uint32_t numNodes = B.nodeCount.load();
-    out.nodes.assign(B.nodes.begin(), B.nodes.begin() + numNodes);
+    root = B.buildBin(0, n, 0);
+    WideCollapse W{B.bin, B.prims, {}, {}};
+    W.nodes.resize(1);
+    W.triOrder.reserve(n);
+    W.emit(root, 0);
+    out.nodes = std::move(W.nodes);
     out.tris.resize(12 * n);
 #pragma omp parallel for schedule(static)
     for (long long i = 0; i < (long long)n; i++) {
-        const uint32_t s = B.prims[i].idx;
+        const uint32_t s = B.prims[W.triOrder[i]].idx;
         float *t = &out.tris[12 * i];
         std::memcpy(t + 0, &v0[3 * s], 12);
         std::memcpy(t + 4, &v1[3 * s], 12);

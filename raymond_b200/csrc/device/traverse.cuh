@@ -1,11 +1,14 @@
 // BVH traversal replacing Apple's closed `intersector<triangle_data,
 // instancing>` (raymond/device/kernels/shading/raytrace.metal:11-85).
 //
-// Layout (built on the host, see bvh.cpp):
-//   BvhNode, 64 B: both children's boxes in their parent (x/y of child 0,
-//   x/y of child 1, z of both) and the two child links.  A link >= 0 is an
-//   inner node; a link < 0 is a leaf ~(first << 3 | (count - 1)) into the
-//   triangle array.
+// Layout (built on the host, bvh_build.cpp): a compressed 8-wide BVH after
+// Ylitie, Karras and Laine, "Efficient incoherent ray traversal on GPUs
+// through compressed wide BVHs" (HPG 2017).  A node is 80 bytes: its origin
+// and per-axis power-of-two scale, a mask of inner-node slots, the index of
+// its first inner child (inner children are consecutive) and of its first
+// triangle (leaf children's triangles are consecutive, at most 3 per leaf and
+// 24 per node), one meta byte per leaf slot (unary triangle count << 5 |
+// offset), and the child boxes quantised to 8 bits per plane.
 //   Triangles in leaf order, 48 B: world-space v0, v1, v2 (float4 each);
 //   v0.w carries the instance index, v1.w the primitive index within the
 //   instance's shape.
@@ -20,15 +23,15 @@
 
 namespace rmd {
 
-struct BvhNode {
-    float4 c0xy;  // lo.x, hi.x, lo.y, hi.y of child 0
-    float4 c1xy;  // same for child 1
-    float4 cz;    // lo.z, hi.z of child 0, lo.z, hi.z of child 1
-    int4 link;    // child 0, child 1, unused, unused
+struct WideNode {
+    float4 originScale;  // origin.xyz; w bits: exponent x, y, z (bytes 0-2), inner-slot mask (byte 3)
+    uint4 bases;         // first inner child, first triangle, meta bytes of slots 0-3, 4-7
+    uint4 qloXY;         // quantised lower bounds: x slots 0-3, 4-7; y slots 0-3, 4-7
+    uint4 qloZqhiX;      // lower z; upper x
+    uint4 qhiYZ;         // upper y; upper z
 };
 
-constexpr int TRAVERSAL_STACK = 64;
-constexpr int STACK_SENTINEL = 0x7fffffff;
+constexpr int TRAVERSAL_STACK = 32;  // node groups; one per level of the 8-wide tree at most
 
 struct WatertightRay {
     int kx, ky, kz;
@@ -108,88 +111,128 @@ RMD_HD TraceRay makeTraceRay(float3 o, float3 d) {
     return r;
 }
 
-// Slab tests of both children; returns entry distances (or > tmax on a miss).
-RMD_HD void boxes(const BvhNode &n, const TraceRay &r, float tmin, float tmax, float &t0, float &t1, bool &h0,
-                  bool &h1) {
-    const float c0lox = n.c0xy.x * r.idir.x - r.oid.x, c0hix = n.c0xy.y * r.idir.x - r.oid.x;
-    const float c0loy = n.c0xy.z * r.idir.y - r.oid.y, c0hiy = n.c0xy.w * r.idir.y - r.oid.y;
-    const float c0loz = n.cz.x * r.idir.z - r.oid.z, c0hiz = n.cz.y * r.idir.z - r.oid.z;
-    const float c1lox = n.c1xy.x * r.idir.x - r.oid.x, c1hix = n.c1xy.y * r.idir.x - r.oid.x;
-    const float c1loy = n.c1xy.z * r.idir.y - r.oid.y, c1hiy = n.c1xy.w * r.idir.y - r.oid.y;
-    const float c1loz = n.cz.z * r.idir.z - r.oid.z, c1hiz = n.cz.w * r.idir.z - r.oid.z;
-    const float c0min = fmaxf(fmaxf(fminf(c0lox, c0hix), fminf(c0loy, c0hiy)), fmaxf(fminf(c0loz, c0hiz), tmin));
-    const float c0max = fminf(fminf(fmaxf(c0lox, c0hix), fmaxf(c0loy, c0hiy)), fminf(fmaxf(c0loz, c0hiz), tmax));
-    const float c1min = fmaxf(fmaxf(fminf(c1lox, c1hix), fminf(c1loy, c1hiy)), fmaxf(fminf(c1loz, c1hiz), tmin));
-    const float c1max = fminf(fminf(fmaxf(c1lox, c1hix), fmaxf(c1loy, c1hiy)), fminf(fmaxf(c1loz, c1hiz), tmax));
-    // widen the far bound by a few ulps (Ize 2013) so FMA rounding never culls a hit
-    h0 = c0min <= c0max * 1.0000004f;
-    h1 = c1min <= c1max * 1.0000004f;
-    t0 = c0min;
-    t1 = c1min;
+// Byte i of w as a float, exactly: the byte becomes the low mantissa byte of
+// 2^23 (one byte permute) and 2^23 is subtracted.
+RMD_HD float byteToFloat(uint32_t w, uint32_t i) {
+    return __uint_as_float(__byte_perm(w, 0x4B000000u, 0x7540u | i)) - 8388608.0f;
 }
 
-// Traversal state of one ray.
+// Ray/box tests of a node's 8 children.  Returns the children the ray enters
+// within [tmin, tmax]: inner children as bits 24 + (slot ^ octant) (so the
+// lowest bit is the nearest child in the node's octant order), leaf
+// children's triangles as bits (offset .. offset + count - 1).
+RMD_HD uint32_t intersectChildren(const WideNode &n, const float3 idir, const float3 org, uint32_t octant,
+                                  float tmin, float tmax) {
+    const uint32_t ew = __float_as_uint(n.originScale.w);
+    const float sx = __uint_as_float((ew & 0xffu) << 23);
+    const float sy = __uint_as_float(((ew >> 8) & 0xffu) << 23);
+    const float sz = __uint_as_float(((ew >> 16) & 0xffu) << 23);
+    const uint32_t imask = ew >> 24;
+    const float ax = sx * idir.x, ay = sy * idir.y, az = sz * idir.z;  // exact: powers of two
+    const float bx = (n.originScale.x - org.x) * idir.x;
+    const float by = (n.originScale.y - org.y) * idir.y;
+    const float bz = (n.originScale.z - org.z) * idir.z;
+    // per axis the near plane is the lower bound for a positive direction
+    const uint2 loX = make_uint2(n.qloXY.x, n.qloXY.y), hiX = make_uint2(n.qloZqhiX.z, n.qloZqhiX.w);
+    const uint2 loY = make_uint2(n.qloXY.z, n.qloXY.w), hiY = make_uint2(n.qhiYZ.x, n.qhiYZ.y);
+    const uint2 loZ = make_uint2(n.qloZqhiX.x, n.qloZqhiX.y), hiZ = make_uint2(n.qhiYZ.z, n.qhiYZ.w);
+    const bool nx = idir.x < 0.0f, ny = idir.y < 0.0f, nz = idir.z < 0.0f;
+    const uint2 nearX = nx ? hiX : loX, farX = nx ? loX : hiX;
+    const uint2 nearY = ny ? hiY : loY, farY = ny ? loY : hiY;
+    const uint2 nearZ = nz ? hiZ : loZ, farZ = nz ? loZ : hiZ;
+    uint32_t hits = 0;
+#pragma unroll
+    for (int half = 0; half < 2; half++) {
+        const uint32_t nxw = half ? nearX.y : nearX.x, fxw = half ? farX.y : farX.x;
+        const uint32_t nyw = half ? nearY.y : nearY.x, fyw = half ? farY.y : farY.x;
+        const uint32_t nzw = half ? nearZ.y : nearZ.x, fzw = half ? farZ.y : farZ.x;
+        const uint32_t metaw = half ? n.bases.w : n.bases.z;
+#pragma unroll
+        for (uint32_t i = 0; i < 4; i++) {
+            const uint32_t slot = 4 * half + i;
+            const float t0x = fmaf(byteToFloat(nxw, i), ax, bx), t1x = fmaf(byteToFloat(fxw, i), ax, bx);
+            const float t0y = fmaf(byteToFloat(nyw, i), ay, by), t1y = fmaf(byteToFloat(fyw, i), ay, by);
+            const float t0z = fmaf(byteToFloat(nzw, i), az, bz), t1z = fmaf(byteToFloat(fzw, i), az, bz);
+            const float enter = fmaxf(fmaxf(t0x, t0y), fmaxf(t0z, tmin));
+            const float leave = fminf(fminf(t1x, t1y), fminf(t1z, tmax));
+            // widen the far bound by a few ulps (Ize 2013) so FMA rounding never culls a hit
+            if (enter <= leave * 1.0000004f) {
+                if ((imask >> slot) & 1u) {
+                    hits |= 1u << (24u + (slot ^ octant));
+                } else {
+                    const uint32_t meta = (metaw >> (8 * i)) & 0xffu;
+                    hits |= (meta >> 5) << (meta & 31u);
+                }
+            }
+        }
+    }
+    return hits;
+}
+
+// Traversal state of one ray: `group` and the stack hold where the traversal
+// stands (sp < 0 once finished).
 struct TraversalState {
     TraceRay r;
     float tmin, tmax;  // tmax shrinks to the closest hit found so far
-    int node;          // next node (>= 0), leaf (< 0), or STACK_SENTINEL once finished
-    int sp;
     int hitTri;        // closest (any-hit: first) triangle hit, -1 if none
     float b0, b1;
+    uint2 group;       // node group being visited
+    int sp;            // stack depth, -1 when finished
 };
-// The node stack is a separate local array, so the scalar state above stays in registers.
-typedef int TraversalStack[TRAVERSAL_STACK];
+// Node groups waiting to be visited: a separate local array, so the scalar
+// state above stays in registers.
+typedef uint2 TraversalStack[TRAVERSAL_STACK];
 
-RMD_HD void beginTraversal(TraversalState &s, TraversalStack &stack, const BvhNode *nodes, float3 o, float3 d,
-                           float tmin, float tmax) {
+RMD_HD uint32_t rayOctant(float3 idir) {
+    return (idir.x < 0.0f ? 1u : 0u) | (idir.y < 0.0f ? 2u : 0u) | (idir.z < 0.0f ? 4u : 0u);
+}
+
+RMD_HD void beginTraversal(TraversalState &s, const WideNode *nodes, float3 o, float3 d, float tmin, float tmax) {
     s.r = makeTraceRay(o, d);
     s.tmin = tmin;
     s.tmax = tmax;
-    s.sp = 0;
-    stack[s.sp++] = STACK_SENTINEL;
-    s.node = nodes != nullptr ? 0 : STACK_SENTINEL;  // a scene without triangles misses everything
     s.hitTri = -1;
     s.b0 = s.b1 = 0.0f;
+    // a virtual parent whose only inner child, in slot 0, is the root
+    s.group = make_uint2(0u, (1u << (24u + rayOctant(s.r.idir))) | 1u);
+    s.sp = nodes != nullptr ? 0 : -1;  // a scene without triangles misses everything
 }
 
-// Depth-first traversal, one node or one leaf per step, nearer child first;
-// a leaf is intersected as soon as it is reached so the closest hit found so
-// far culls the rest.  ANY: stop at the first hit (raytrace.metal:52-85);
-// otherwise keep the closest (raytrace.metal:11-50).  (The while-while loop
-// and dynamic ray fetch of Aila & Laine, HPG 2009, both measured slower here:
-// warp-vote instructions inside the loop cost more than they recover.)
+// Depth-first traversal of the 8-wide BVH.  A node group (first inner child,
+// bits 24..31: inner children still to visit in octant order, bits 0..7: the
+// node's inner-slot mask) is visited nearest child first; the rest of the
+// group waits on the stack.  The triangles a node's leaf children hit are
+// intersected as soon as the node is visited, so the closest hit found so far
+// culls what follows.  ANY: stop at the first hit (raytrace.metal:52-85);
+// otherwise keep the closest (raytrace.metal:11-50).  (Dynamic ray fetch,
+// Aila & Laine, HPG 2009, measured slower with this tree too.)
 template <bool ANY>
-RMD_HD void traverse(TraversalState &s, TraversalStack &stack, const BvhNode *__restrict__ nodes,
+RMD_HD void traverse(TraversalState &s, TraversalStack &stack, const WideNode *__restrict__ nodes,
                      const float4 *__restrict__ tris, uint32_t *errors) {
-    while (s.node != STACK_SENTINEL) {
-        if (s.node >= 0) {
-            const BvhNode *np = &nodes[s.node];
-            const BvhNode n = {__ldg(&np->c0xy), __ldg(&np->c1xy), __ldg(&np->cz), __ldg(&np->link)};
-            float t0, t1;
-            bool h0, h1;
-            boxes(n, s.r, s.tmin, s.tmax, t0, t1, h0, h1);
-            if (h0 && h1) {
-                int nearN = n.link.x, farN = n.link.y;
-                if (t1 < t0) {
-                    nearN = n.link.y;
-                    farN = n.link.x;
-                }
-                if (s.sp < TRAVERSAL_STACK) stack[s.sp++] = farN;
+    if (s.sp < 0) return;
+    const float3 idir = s.r.idir, org = s.r.org;
+    const uint32_t octant = rayOctant(idir);
+    uint2 group = s.group;
+    int sp = s.sp;
+    while (true) {
+        if (group.y > 0x00ffffffu) {
+            const uint32_t key = __ffs(group.y >> 24) - 1;
+            group.y &= ~(1u << (24u + key));
+            const uint32_t slot = key ^ octant;
+            const uint32_t index = group.x + __popc(group.y & ((1u << slot) - 1u) & 0xffu);
+            if (group.y > 0x00ffffffu) {
+                if (sp < TRAVERSAL_STACK) stack[sp++] = group;
                 else atomicOr(errors, 2u);
-                s.node = nearN;
-            } else if (h0) {
-                s.node = n.link.x;
-            } else if (h1) {
-                s.node = n.link.y;
-            } else {
-                s.node = stack[--s.sp];
             }
-        } else {
-            const int code = ~s.node;
-            const int first = code >> 3, count = (code & 7) + 1;
-            bool found = false;
-            for (int i = 0; i < count; i++) {
-                const int ti = first + i;
+            const WideNode *np = &nodes[index];
+            const WideNode n = {__ldg(&np->originScale), __ldg(&np->bases), __ldg(&np->qloXY),
+                                __ldg(&np->qloZqhiX), __ldg(&np->qhiYZ)};
+            const uint32_t hits = intersectChildren(n, idir, org, octant, s.tmin, s.tmax);
+            group = make_uint2(n.bases.x, (hits & 0xff000000u) | (__float_as_uint(n.originScale.w) >> 24));
+            uint32_t triHits = hits & 0x00ffffffu;
+            while (triHits) {
+                const int ti = (int)n.bases.y + __ffs(triHits) - 1;
+                triHits &= triHits - 1u;
                 const float4 a = __ldg(&tris[3 * ti + 0]);
                 const float4 b = __ldg(&tris[3 * ti + 1]);
                 const float4 c = __ldg(&tris[3 * ti + 2]);
@@ -197,15 +240,21 @@ RMD_HD void traverse(TraversalState &s, TraversalStack &stack, const BvhNode *__
                 if (intersectTriangle(s.r.wr, xyz(a), xyz(b), xyz(c), s.tmin, s.tmax, t, b0, b1)) {
                     s.hitTri = ti;
                     if (ANY) {
-                        found = true;
-                        break;
+                        s.sp = -1;
+                        return;
                     }
                     s.tmax = t;
                     s.b0 = b0;
                     s.b1 = b1;
                 }
             }
-            s.node = (ANY && found) ? STACK_SENTINEL : stack[--s.sp];
+        }
+        if (group.y <= 0x00ffffffu) {
+            if (sp == 0) {
+                s.sp = -1;
+                return;
+            }
+            group = stack[--sp];
         }
     }
 }
@@ -226,19 +275,19 @@ RMD_HD bool closestHit(const TraversalState &s, const float4 *__restrict__ tris,
 }
 
 // Single-ray forms of the two queries (test hooks).
-RMD_HD bool traceClosest(const BvhNode *__restrict__ nodes, const float4 *__restrict__ tris, float3 o, float3 d,
+RMD_HD bool traceClosest(const WideNode *__restrict__ nodes, const float4 *__restrict__ tris, float3 o, float3 d,
                          float tmin, float tmax, float4 &hit, uint32_t &inst, uint32_t *errors) {
     TraversalState s;
     TraversalStack stack;
-    beginTraversal(s, stack, nodes, o, d, tmin, tmax);
+    beginTraversal(s, nodes, o, d, tmin, tmax);
     traverse<false>(s, stack, nodes, tris, errors);
     return closestHit(s, tris, hit, inst);
 }
-RMD_HD bool traceAny(const BvhNode *__restrict__ nodes, const float4 *__restrict__ tris, float3 o, float3 d,
+RMD_HD bool traceAny(const WideNode *__restrict__ nodes, const float4 *__restrict__ tris, float3 o, float3 d,
                      float tmin, float tmax, uint32_t *errors) {
     TraversalState s;
     TraversalStack stack;
-    beginTraversal(s, stack, nodes, o, d, tmin, tmax);
+    beginTraversal(s, nodes, o, d, tmin, tmax);
     traverse<true>(s, stack, nodes, tris, errors);
     return s.hitTri >= 0;
 }

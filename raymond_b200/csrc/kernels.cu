@@ -90,7 +90,7 @@ __global__ void __launch_bounds__(256) k_film_regen(Context ctx, PathPool pool, 
 // entries with one atomic and traces them to the end.  begin(idx, state,
 // stack) starts entry idx, finish(idx, state) consumes the finished query.
 template <bool ANY, class Begin, class Finish>
-__device__ __forceinline__ void persistentTrace(const BvhNode *__restrict__ nodes, const float4 *__restrict__ tris,
+__device__ __forceinline__ void persistentTrace(const WideNode *__restrict__ nodes, const float4 *__restrict__ tris,
                                                 uint32_t *work, uint32_t n, uint32_t *errors, Begin begin,
                                                 Finish finish) {
     TraversalState s;
@@ -110,17 +110,17 @@ __device__ __forceinline__ void persistentTrace(const BvhNode *__restrict__ node
     }
 }
 
-__global__ void __launch_bounds__(128) k_trace_closest(const BvhNode *__restrict__ nodes,
+__global__ void __launch_bounds__(128) k_trace_closest(const WideNode *__restrict__ nodes,
                                                        const float4 *__restrict__ tris, PathPool pool,
                                                        Counters *cnt, uint32_t p) {
     const uint32_t n = activeCount(cnt, p);
     const PathState S = pool.s[p];
     persistentTrace<false>(
         nodes, tris, &cnt->traceWork, n, &cnt->errors,
-        [&](uint32_t idx, TraversalState &s, TraversalStack &stack) {
+        [&](uint32_t idx, TraversalState &s, TraversalStack &) {
             const float4 o = __ldcs(&S.rayO[idx]);
             const float4 d = __ldcs(&S.rayD[idx]);
-            beginTraversal(s, stack, nodes, xyz(o), xyz(d), o.w, d.w);
+            beginTraversal(s, nodes, xyz(o), xyz(d), o.w, d.w);
         },
         [&](uint32_t idx, const TraversalState &s) {
             float4 hit;
@@ -137,7 +137,7 @@ __global__ void __launch_bounds__(128) k_trace_closest(const BvhNode *__restrict
 // shadow ray adds its weight to its path's radiance, in S[p ^ 1] for a path
 // that continues and in the finish list for one that ended.  Thread 0 also
 // advances nextPath past the camera samples this iteration consumed.
-__global__ void __launch_bounds__(128) k_trace_shadow(const BvhNode *__restrict__ nodes,
+__global__ void __launch_bounds__(128) k_trace_shadow(const WideNode *__restrict__ nodes,
                                                       const float4 *__restrict__ tris, PathPool pool,
                                                       Counters *cnt, uint32_t p) {
     const uint32_t n = cnt->nShadow;
@@ -146,12 +146,12 @@ __global__ void __launch_bounds__(128) k_trace_shadow(const BvhNode *__restrict_
     uint32_t target = 0, traced = 0;
     persistentTrace<true>(
         nodes, tris, &cnt->shadowWork, n, &cnt->errors,
-        [&](uint32_t idx, TraversalState &s, TraversalStack &stack) {
+        [&](uint32_t idx, TraversalState &s, TraversalStack &) {
             const float4 o = __ldcs(&pool.shO[idx]);
             const float4 d = __ldcs(&pool.shD[idx]);
             target = __float_as_uint(d.w);
             traced++;
-            beginTraversal(s, stack, nodes, xyz(o), xyz(d), SHADOW_EPS, o.w);
+            beginTraversal(s, nodes, xyz(o), xyz(d), SHADOW_EPS, o.w);
         },
         [&](uint32_t idx, const TraversalState &s) {
             // all ones: the path overflowed its queue
@@ -223,7 +223,7 @@ __global__ void k_debug_prng(uint32_t mode, uint64_t a, uint64_t b, int n, float
     PrngState p = mode == RNG_TEA ? PrngState::tea((uint32_t)a, (uint32_t)b) : PrngState::pcg(a, b);
     for (int i = 0; i < n; i++) out[i] = p.sample();
 }
-__global__ void k_debug_trace(const BvhNode *nodes, const float4 *tris, const float *rays, int n, int any, float *out,
+__global__ void k_debug_trace(const WideNode *nodes, const float4 *tris, const float *rays, int n, int any, float *out,
                               uint32_t *inst, uint32_t *errors) {
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= n) return;
@@ -258,12 +258,12 @@ cudaError_t rmdLaunchFilmRegen(const Context &ctx, const PathPool &pool, const F
     k_film_regen<<<blocks, 256, 0, s>>>(ctx, pool, fp, cnt, cur);
     return cudaGetLastError();
 }
-cudaError_t rmdLaunchTraceClosest(const BvhNode *nodes, const float4 *tris, const PathPool &pool, Counters *cnt,
+cudaError_t rmdLaunchTraceClosest(const WideNode *nodes, const float4 *tris, const PathPool &pool, Counters *cnt,
                                   uint32_t cur, int blocks, cudaStream_t s) {
     k_trace_closest<<<blocks, 128, 0, s>>>(nodes, tris, pool, cnt, cur);
     return cudaGetLastError();
 }
-cudaError_t rmdLaunchTraceShadow(const BvhNode *nodes, const float4 *tris, const PathPool &pool, Counters *cnt,
+cudaError_t rmdLaunchTraceShadow(const WideNode *nodes, const float4 *tris, const PathPool &pool, Counters *cnt,
                                  uint32_t cur, int blocks, cudaStream_t s) {
     k_trace_shadow<<<blocks, 128, 0, s>>>(nodes, tris, pool, cnt, cur);
     return cudaGetLastError();
@@ -286,7 +286,7 @@ cudaError_t rmdLaunchDebugPrng(uint32_t mode, uint64_t a, uint64_t b, int n, flo
     k_debug_prng<<<1, 1, 0, s>>>(mode, a, b, n, out);
     return cudaGetLastError();
 }
-cudaError_t rmdLaunchDebugTrace(const BvhNode *nodes, const float4 *tris, const float *rays, int n, int any, float *out,
+cudaError_t rmdLaunchDebugTrace(const WideNode *nodes, const float4 *tris, const float *rays, int n, int any, float *out,
                                 uint32_t *inst, uint32_t *errors, cudaStream_t s) {
     k_debug_trace<<<(n + 127) / 128, 128, 0, s>>>(nodes, tris, rays, n, any, out, inst, errors);
     return cudaGetLastError();

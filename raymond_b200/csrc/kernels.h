@@ -10,14 +10,14 @@ cudaError_t rmdLaunchFrameInit(const rmd::PathPool &pool, rmd::Counters *cnt, ui
                                cudaStream_t s);
 cudaError_t rmdLaunchFilmRegen(const rmd::Context &ctx, const rmd::PathPool &pool, const rmd::FrameParams &fp,
                                rmd::Counters *cnt, uint32_t cur, int blocks, cudaStream_t s);
-cudaError_t rmdLaunchTraceClosest(const rmd::BvhNode *nodes, const float4 *tris, const rmd::PathPool &pool,
+cudaError_t rmdLaunchTraceClosest(const rmd::WideNode *nodes, const float4 *tris, const rmd::PathPool &pool,
                                   rmd::Counters *cnt, uint32_t cur, int blocks, cudaStream_t s);
-cudaError_t rmdLaunchTraceShadow(const rmd::BvhNode *nodes, const float4 *tris, const rmd::PathPool &pool,
+cudaError_t rmdLaunchTraceShadow(const rmd::WideNode *nodes, const float4 *tris, const rmd::PathPool &pool,
                                  rmd::Counters *cnt, uint32_t cur, int blocks, cudaStream_t s);
 cudaError_t rmdLaunchEnvmapReduce(float *mip, int cur, cudaStream_t s);
 cudaError_t rmdLaunchEnvmapNormalize(const float *sum, float *pdfs, uint32_t gridSize, cudaStream_t s);
 cudaError_t rmdLaunchFilmResolve(const float4 *film, const double *film64, int fp64, float *out, uint32_t numPixels,
                                  float scale, uint32_t tonemapping, cudaStream_t s);
 cudaError_t rmdLaunchDebugPrng(uint32_t mode, uint64_t a, uint64_t b, int n, float *out, cudaStream_t s);
-cudaError_t rmdLaunchDebugTrace(const rmd::BvhNode *nodes, const float4 *tris, const float *rays, int n, int any,
+cudaError_t rmdLaunchDebugTrace(const rmd::WideNode *nodes, const float4 *tris, const float *rays, int n, int any,
                                 float *out, uint32_t *inst, uint32_t *errors, cudaStream_t s);

@@ -253,7 +253,7 @@ namespace rmdhost {
 bool sceneView(const rmd_scene *s, SceneView &v) {
     if (!s) return false;
     v.ctx = s->dctx;
-    v.nodes = s->bvhNodes.as<BvhNode>();
+    v.nodes = s->bvhNodes.as<WideNode>();
     v.tris = s->bvhTris.as<float4>();
     v.shade = s->jit.shade;
     v.shadeBlocks = s->shadeBlocks;
@@ -421,8 +421,8 @@ rmd_status rmd_scene_create(rmd_context *ctx, const rmd_scene_desc *d, rmd_scene
         }
     }
     s->triangles = triInst.size();
-    rmdhost::GpuBvh bvh;
-    rmdhost::buildBvh(t0, t1, t2, triInst, triPrim, bvh);
+    rmdhost::GpuWideBvh bvh;
+    rmdhost::buildWideBvh(t0, t1, t2, triInst, triPrim, bvh);
     s->bvhNodeCount = bvh.nodes.size();
 
     // LightBuilder.build (LightBuilder.swift:179-281)
@@ -515,7 +515,7 @@ rmd_status rmd_scene_create(rmd_context *ctx, const rmd_scene_desc *d, rmd_scene
     RMD_CUDA(s->surfaceTable.upload(stab.data(), stab.size() * sizeof(uint2), st));
     RMD_CUDA(s->lightTable.upload(ltab.data(), ltab.size() * sizeof(uint2), st));
     RMD_CUDA(s->materialParams.upload(mod.params.data(), mod.params.size() * sizeof(float), st));
-    RMD_CUDA(s->bvhNodes.upload(bvh.nodes.data(), bvh.nodes.size() * sizeof(rmdhost::GpuBvhNode), st));
+    RMD_CUDA(s->bvhNodes.upload(bvh.nodes.data(), bvh.nodes.size() * sizeof(rmdhost::GpuWideNode), st));
     RMD_CUDA(s->bvhTris.upload(bvh.tris.data(), bvh.tris.size() * sizeof(float), st));
 
     Context &c = s->dctx;
@@ -698,14 +698,14 @@ rmd_status rmd_render(rmd_renderer *r, const rmd_render_settings *s) {
             RMD_CUDA(rmdLaunchFilmRegen(r->dctx, pool, fp, cnt, cur, rb, st));
             RMD_CUDA(r->stageEvent(evi++, e));
             RMD_CUDA(cudaEventRecord(e, st));
-            RMD_CUDA(rmdLaunchTraceClosest(scene->bvhNodes.as<BvhNode>(), scene->bvhTris.as<float4>(), pool, cnt, cur, tb, st));
+            RMD_CUDA(rmdLaunchTraceClosest(scene->bvhNodes.as<WideNode>(), scene->bvhTris.as<float4>(), pool, cnt, cur, tb, st));
             RMD_CUDA(r->stageEvent(evi++, e));
             RMD_CUDA(cudaEventRecord(e, st));
             sp.cur = cur;
             RMD_CUDA(cudaLaunchKernel((const void *)r->shade, dim3(sb), dim3(128), shadeArgs, 0, st));
             RMD_CUDA(r->stageEvent(evi++, e));
             RMD_CUDA(cudaEventRecord(e, st));
-            RMD_CUDA(rmdLaunchTraceShadow(scene->bvhNodes.as<BvhNode>(), scene->bvhTris.as<float4>(), pool, cnt, cur, tb, st));
+            RMD_CUDA(rmdLaunchTraceShadow(scene->bvhNodes.as<WideNode>(), scene->bvhTris.as<float4>(), pool, cnt, cur, tb, st));
             RMD_CUDA(r->stageEvent(evi++, e));
             RMD_CUDA(cudaEventRecord(e, st));
             cur ^= 1u;
@@ -939,7 +939,7 @@ rmd_status rmd_test_trace(const rmd_scene *s, const float *rays, int32_t n, int3
     RMD_CUDA(derr.alloc(sizeof(uint32_t)));
     RMD_CUDA(cudaMemset(derr.ptr, 0, sizeof(uint32_t)));
     if (n > 0)
-        RMD_CUDA(rmdLaunchDebugTrace(s->bvhNodes.as<BvhNode>(), s->bvhTris.as<float4>(), dr.as<float>(), n, any,
+        RMD_CUDA(rmdLaunchDebugTrace(s->bvhNodes.as<WideNode>(), s->bvhTris.as<float4>(), dr.as<float>(), n, any,
                                      dout.as<float>(), dinst.as<uint32_t>(), derr.as<uint32_t>(), s->ctx->stream));
     RMD_CUDA(cudaStreamSynchronize(s->ctx->stream));
     RMD_CUDA(cudaMemcpy(out, dout.ptr, (size_t)n * 4 * sizeof(float), cudaMemcpyDeviceToHost));

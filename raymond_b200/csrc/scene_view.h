@@ -10,7 +10,7 @@ namespace rmdhost {
 
 struct SceneView {
     rmd::Context ctx;              // device view of geometry, lights, materials, camera
-    const rmd::BvhNode *nodes;     // nullptr for a scene without triangles
+    const rmd::WideNode *nodes;     // nullptr for a scene without triangles
     const float4 *tris;
     cudaKernel_t shade;            // shading megakernel of the scene's material module
     int shadeBlocks;

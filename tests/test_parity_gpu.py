@@ -189,11 +189,11 @@ def test_autotune_keeps_parity(cornell):
 def test_set_tuning_keeps_parity(cornell):
     """Launch choices applied by hand (another process's autotune result)."""
     desc, scene, orc = cornell
+    cpu, _ = orc.render(128, 128, 1, 8, first_sample=2)
     r = api.Renderer(scene, 128, 128)
     r.set_tuning({"shade_min_blocks": 3, "trace_blocks_per_sm": 4, "pool_size": 4096})
     r.render(spp=1, max_depth=8, first_sample=2)
     assert r.stats()["pool_size"] == 4096
-    cpu, _ = orc.render(128, 128, 1, 8, first_sample=2)
     assert match_fraction(r.film(), cpu) >= MIN_MATCH
     with pytest.raises(api.RmdError):
         r.set_tuning({"shade_min_blocks": 0, "trace_blocks_per_sm": 4, "pool_size": 0})
