@@ -263,6 +263,7 @@ typedef struct rmd_stats {
     uint32_t pool_size;        /* path slots in flight */
     uint32_t errors;           /* device error flags (queue overflow, watchdog) */
     uint64_t rays;             /* closest-hit rays traced (segments + misses) */
+    double   ms_guide;         /* guide inference and training (0 without guiding) */
 } rmd_stats;
 
 typedef struct rmd_context rmd_context;
@@ -337,6 +338,48 @@ rmd_status rmd_renderer_set_tuning(rmd_renderer *r, const rmd_tune_result *tunin
 /* Per-stage device timings and counters of the last rmd_render
  * (RendererCounters, Renderer.swift:13-268). */
 rmd_status rmd_renderer_stats(const rmd_renderer *r, rmd_stats *out);
+
+/* ----------------------------------------------------- learned path guiding */
+/* No counterpart in the reference.  A small MLP (160 one-blob inputs from
+ * position, normal and view; 3 hidden layers of 64; BF16 weights, FP32
+ * accumulation, on the tensor cores) maps each shading point to a mixture of
+ * 8 von Mises-Fisher lobes and a selection probability.  Directions are drawn
+ * from the BSDF or the mixture by one-sample MIS, so the estimator stays
+ * unbiased whatever the network says.  The network trains online with Adam
+ * on the radiance the tracer itself gathers: each path contributes one
+ * sample (a vertex chosen uniformly among its eligible ones, with the
+ * radiance that arrived through its sampled direction) and every light
+ * sample one more; the samples with a nonzero target go to a replay ring from
+ * which each step draws its records. */
+typedef struct rmd_guide_settings {
+    uint32_t sampling;       /* 1: sample directions from the guide as well as the BSDF */
+    uint32_t training;       /* 1: collect records and take Adam steps during rmd_render */
+    uint32_t batch_size;     /* tracer samples (paths) per Adam step; 0 = 1 << 20 */
+    float learning_rate;     /* 0 = 1e-3 */
+    uint32_t reset;          /* 1: re-initialise the network from `seed` */
+    uint32_t seed;
+    uint32_t step_records;   /* records each step trains on, drawn from the replay ring; 0 = 1 << 14 */
+    uint32_t replay_records; /* ring of the latest nonzero-target records; power of two, 0 = 1 << 18 */
+    uint32_t steps_per_batch; /* Adam steps per `batch_size` samples; 0 = 1 */
+    uint32_t skip_light_records; /* 1: train on the paths' samples only, not on the light samples */
+    uint32_t guided_depth;   /* guide the vertices of path depth below this; 0 = all */
+} rmd_guide_settings;
+
+typedef struct rmd_guide_stats {
+    uint64_t steps;          /* Adam steps taken */
+    uint64_t samples;        /* training samples consumed (one per path with an eligible vertex) */
+    uint64_t records;        /* records with a nonzero target written to the replay ring so far */
+    float last_loss;         /* mean loss of the last step (normalised targets) */
+    float reserved;
+} rmd_guide_stats;
+
+rmd_status rmd_renderer_set_guide(rmd_renderer *r, const rmd_guide_settings *settings);
+rmd_status rmd_renderer_guide_stats(const rmd_renderer *r, rmd_guide_stats *out);
+/* Read (write = 0) or replace (write = 1) the network's FP32 parameters:
+ * rmd_guide_param_count() floats, layers W1 [64][160], b1, W2 [64][64], b2,
+ * W3 [64][64], b3, W4 [48][64], b4 (row-major, output-major). */
+int32_t rmd_guide_param_count(void);
+rmd_status rmd_renderer_guide_params(rmd_renderer *r, float *params, int32_t write);
 
 /* ----------------------------------------------------- allocation-free render */
 /*

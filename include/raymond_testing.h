@@ -47,6 +47,18 @@ rmd_status rmd_test_generate_source(const rmd_scene_desc *desc, int32_t hoist, c
 rmd_status rmd_test_jit_compile(const rmd_scene_desc *desc, int32_t hoist, char *log, int64_t loglen,
                                 int64_t *cubin_bytes);
 
+/* Path-guiding network test hooks (no counterpart in the reference).
+ * Forward pass of explicit features (n x 7) with FP32 parameters, raw
+ * outputs (n x 48). */
+rmd_status rmd_test_guide_forward(const float *params, const float *features, int32_t n, float *out);
+/* Gradient of the mean training loss over n records of 12 floats (features
+ * 7, direction 3, BSDF pdf, target), and the loss. */
+rmd_status rmd_test_guide_gradient(const float *params, const float *records, int32_t n, float *grad, float *loss);
+/* Packed mixture of one output vector (48): a direction and its pdf per row
+ * of u (n x 3, into dirs_pdf n x 4), and the pdf at m query directions. */
+rmd_status rmd_test_guide_mixture(const float *outputs, const float *u, int32_t n, float *dirs_pdf,
+                                  const float *queries, int32_t m, float *pdfs);
+
 #ifdef __cplusplus
 }
 #endif

@@ -118,7 +118,20 @@ class Stats(C.Structure):
     _fields_ = [("paths", C.c_uint64), ("segments", C.c_uint64), ("shadow_rays", C.c_uint64),
                 ("iterations", C.c_uint64), ("ms_total", C.c_double), ("ms_trace", C.c_double),
                 ("ms_shade", C.c_double), ("ms_shadow", C.c_double), ("ms_film", C.c_double),
-                ("pool_size", C.c_uint32), ("errors", C.c_uint32), ("rays", C.c_uint64)]
+                ("pool_size", C.c_uint32), ("errors", C.c_uint32), ("rays", C.c_uint64),
+                ("ms_guide", C.c_double)]
+
+
+class GuideSettings(C.Structure):
+    _fields_ = [("sampling", C.c_uint32), ("training", C.c_uint32), ("batch_size", C.c_uint32),
+                ("learning_rate", C.c_float), ("reset", C.c_uint32), ("seed", C.c_uint32),
+                ("step_records", C.c_uint32), ("replay_records", C.c_uint32), ("steps_per_batch", C.c_uint32),
+                ("skip_light_records", C.c_uint32), ("guided_depth", C.c_uint32)]
+
+
+class GuideStats(C.Structure):
+    _fields_ = [("steps", C.c_uint64), ("samples", C.c_uint64), ("records", C.c_uint64), ("last_loss", C.c_float),
+                ("reserved", C.c_float)]
 
 
 def _fptr(a: np.ndarray, ctype=C.c_float):

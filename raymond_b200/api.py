@@ -28,8 +28,10 @@ EXPORTS = [
     "rmd_scene_destroy", "rmd_scene_info", "rmd_renderer_create", "rmd_renderer_destroy", "rmd_renderer_set_size",
     "rmd_renderer_reset", "rmd_renderer_set_camera", "rmd_render", "rmd_film_read", "rmd_film_read_f64",
     "rmd_film_samples", "rmd_renderer_stats", "rmd_render_noalloc", "rmd_renderer_autotune",
-    "rmd_renderer_set_tuning",
+    "rmd_renderer_set_tuning", "rmd_renderer_set_guide", "rmd_renderer_guide_stats", "rmd_guide_param_count",
+    "rmd_renderer_guide_params",
     "rmd_test_prng", "rmd_test_trace", "rmd_test_material_eval", "rmd_test_generate_source", "rmd_test_jit_compile",
+    "rmd_test_guide_forward", "rmd_test_guide_gradient", "rmd_test_guide_mixture",
 ]
 
 
@@ -72,6 +74,14 @@ def lib() -> C.CDLL:
         "rmd_renderer_stats": ([vp, P(Stats)], C.c_int32),
         "rmd_renderer_autotune": ([vp, P(RenderSettings), P(_abi.TuneResult)], C.c_int32),
         "rmd_renderer_set_tuning": ([vp, P(_abi.TuneResult)], C.c_int32),
+        "rmd_renderer_set_guide": ([vp, P(_abi.GuideSettings)], C.c_int32),
+        "rmd_renderer_guide_stats": ([vp, P(_abi.GuideStats)], C.c_int32),
+        "rmd_guide_param_count": ([], C.c_int32),
+        "rmd_renderer_guide_params": ([vp, P(C.c_float), C.c_int32], C.c_int32),
+        "rmd_test_guide_forward": ([P(C.c_float), P(C.c_float), C.c_int32, P(C.c_float)], C.c_int32),
+        "rmd_test_guide_gradient": ([P(C.c_float), P(C.c_float), C.c_int32, P(C.c_float), P(C.c_float)], C.c_int32),
+        "rmd_test_guide_mixture": ([P(C.c_float), P(C.c_float), C.c_int32, P(C.c_float), P(C.c_float), C.c_int32,
+                                    P(C.c_float)], C.c_int32),
         "rmd_render_noalloc": ([vp, P(_abi.Camera), C.c_uint32, C.c_uint32, P(RenderSettings), C.c_void_p,
                                 C.c_uint32], C.c_int32),
         "rmd_test_prng": ([C.c_uint32, C.c_uint64, C.c_uint64, C.c_int32, P(C.c_float)], C.c_int32),
@@ -216,6 +226,40 @@ class Renderer:
         check(lib().rmd_renderer_stats(self.h, C.byref(s)))
         return {k: getattr(s, k) for k, _ in Stats._fields_}
 
+    def set_guide(self, sampling: bool = True, training: bool = True, batch_size: int = 0,
+                  learning_rate: float = 0.0, reset: bool = False, seed: int = 0, step_records: int = 0,
+                  replay_records: int = 0, steps_per_batch: int = 0, light_records: bool = True,
+                  guided_depth: int = 0) -> None:
+        """Learned path guiding (rmd_renderer_set_guide): sample directions from
+        the guide mixture by one-sample MIS and/or train the network online
+        during render().  One Adam step per `batch_size` tracer samples (0 =
+        2^20), learning rate 0 = 1e-3, each step on `step_records` records
+        (0 = 2^14) drawn from a ring of the latest `replay_records` (0 = 2^18);
+        `steps_per_batch` (0 = 1) Adam steps per batch; `light_records`: the
+        light samples of every vertex are training samples too; vertices of
+        path depth below `guided_depth` (0 = all) sample from the guide.  The
+        network is initialised from `seed` on first use or when `reset` is set."""
+        g = _abi.GuideSettings(int(sampling), int(training), batch_size, learning_rate, int(reset), seed,
+                               step_records, replay_records, steps_per_batch, int(not light_records), guided_depth)
+        check(lib().rmd_renderer_set_guide(self.h, C.byref(g)))
+
+    def guide_stats(self) -> dict[str, float]:
+        g = _abi.GuideStats()
+        check(lib().rmd_renderer_guide_stats(self.h, C.byref(g)))
+        return {k: getattr(g, k) for k, _ in _abi.GuideStats._fields_ if k != "reserved"}
+
+    def guide_params(self) -> np.ndarray:
+        """The guide network's FP32 parameters (layout of rmd_renderer_guide_params)."""
+        out = np.zeros(guide_param_count(), np.float32)
+        check(lib().rmd_renderer_guide_params(self.h, _f32p(out), 0))
+        return out
+
+    def set_guide_params(self, params: np.ndarray) -> None:
+        p = np.ascontiguousarray(params, np.float32)
+        if p.size != guide_param_count():
+            raise ValueError(f"expected {guide_param_count()} parameters, got {p.size}")
+        check(lib().rmd_renderer_guide_params(self.h, _f32p(p), 1))
+
     def close(self):
         if self.h.value:
             lib().rmd_renderer_destroy(self.h)
@@ -237,6 +281,43 @@ def render_noalloc(scene: Scene, camera: dict[str, Any], width: int, height: int
     s = RenderSettings(spp, max_depth, sampling_mode, rng, seed, first_sample, 0, 0)
     check(lib().rmd_render_noalloc(scene.h, C.byref(cam), width, height, C.byref(s), C.c_void_p(film_device_ptr),
                                    pool_size))
+
+
+def guide_param_count() -> int:
+    return int(lib().rmd_guide_param_count())
+
+
+def guide_forward(params: np.ndarray, features: np.ndarray) -> np.ndarray:
+    """Test hook: the guide network's raw outputs (n, 48) for explicit features (n, 7)."""
+    p = np.ascontiguousarray(params, np.float32)
+    f = np.ascontiguousarray(features, np.float32).reshape(-1, 7)
+    out = np.zeros((f.shape[0], 48), np.float32)
+    check(lib().rmd_test_guide_forward(_f32p(p), _f32p(f), f.shape[0], _f32p(out)))
+    return out
+
+
+def guide_gradient(params: np.ndarray, records: np.ndarray) -> tuple[np.ndarray, float]:
+    """Test hook: gradient of the mean training loss over `records` (n, 12:
+    features 7, direction 3, BSDF pdf, target) and the loss itself."""
+    p = np.ascontiguousarray(params, np.float32)
+    r = np.ascontiguousarray(records, np.float32).reshape(-1, 12)
+    grad = np.zeros(p.size, np.float32)
+    loss = C.c_float()
+    check(lib().rmd_test_guide_gradient(_f32p(p), _f32p(r), r.shape[0], _f32p(grad), C.byref(loss)))
+    return grad, loss.value
+
+
+def guide_mixture(outputs: np.ndarray, u: np.ndarray, queries: np.ndarray) -> tuple[np.ndarray, np.ndarray]:
+    """Test hook: decode one output vector (48) into the packed mixture, draw a
+    direction per row of u (n, 3) with its pdf (n, 4), and evaluate the pdf at
+    queries (m, 3)."""
+    o = np.ascontiguousarray(outputs, np.float32).reshape(48)
+    uu = np.ascontiguousarray(u, np.float32).reshape(-1, 3)
+    q = np.ascontiguousarray(queries, np.float32).reshape(-1, 3)
+    dp = np.zeros((uu.shape[0], 4), np.float32)
+    pdf = np.zeros(q.shape[0], np.float32)
+    check(lib().rmd_test_guide_mixture(_f32p(o), _f32p(uu), uu.shape[0], _f32p(dp), _f32p(q), q.shape[0], _f32p(pdf)))
+    return dp, pdf
 
 
 def generate_source(scene: dict[str, Any] | SceneDesc, hoist: bool = True) -> str:

@@ -46,6 +46,9 @@ __device__ __forceinline__ bool shadePath(const ShadeParams &p, uint32_t i) {
     float3 shadowDir = f3(0.0f);
     float4 next[3];                      // rayO, rayD, tp of the continued path
     float L4next = 0.0f;                 // its depth | flags word
+    const bool training = S.rec != nullptr;
+    float4 record[4] = {f4(0.0f), f4(0.0f), f4(0.0f), f4(0.0f)};  // guide training record
+    bool recorded = false;  // this vertex replaced the path's record
 
     const bool needsToCollectEmission = is_inf(rayBsdfPdf) || fp.samplingMode != 1u;
     ShadingContext shading;
@@ -85,10 +88,28 @@ __device__ __forceinline__ bool shadePath(const ShadeParams &p, uint32_t i) {
             shNormal = ensure_valid_reflection(geoNormal, shading.wo, shading.material.normal);
         }
 
+        // Guiding: directions come from the BSDF or, with probability alpha, from
+        // the guide mixture of this point (one-sample MIS); the technique's pdf is
+        // then alpha q + (1 - alpha) p_bsdf in every MIS weight that uses it.
+        const bool guided = depth < fp.guideDepth;
+        GuideMixture gm;
+        float alpha = 0.0f;
+        if (guided) {
+            gm = pool.guide[i];
+            alpha = gm.alpha.x;
+        }
+        GuideFeatures gf;  // training: the guide's input features of this vertex
+        const float meanThroughput = mean(rayWeight);
+        if (training)
+            gf = guideFeatures(shading.position, shading.trueNormal, shading.wo, fp.guideSceneMin,
+                               fp.guideSceneInvExtent);
+
         if (fp.samplingMode != 0u) {  // NEE, intersection.metal:149-181
             LightSample nee = lightsSample(ctx, shading.position, shading.rayFlags, prng);
             float bsdfPdf;
             const float3 bsdf = shading.material.evaluate(shading.wo, nee.direction, shNormal, shading.trueNormal, bsdfPdf);
+            const float neeBsdfPdf = bsdfPdf;
+            if (guided) bsdfPdf = alpha * guidePdf(gm, nee.direction) + (1.0f - alpha) * bsdfPdf;
             const float3 contribution = nee.weight * bsdf * rayWeight;
             if (nee.castsShadows) {
                 const float misWeight =
@@ -99,7 +120,13 @@ __device__ __forceinline__ bool shadePath(const ShadeParams &p, uint32_t i) {
                     const uint32_t k = warpAppend(&cnt->nShadow);
                     if (k < pool.capacity) {
                         __stcs(&pool.shO[k], f4(shading.position, nee.distance - SHADOW_EPS));
-                        __stcs(&pool.shW[k], f4(neeWeight, 0.0f));
+                        // training: the light sample is a training sample of this vertex too
+                        const bool neeRecord = pool.shRec && meanThroughput > 0.0f && neeBsdfPdf > 0.0f;
+                        __stcs(&pool.shW[k], f4(neeWeight, neeRecord ? 1.0f / meanThroughput : 0.0f));
+                        if (neeRecord) {
+                            __stcs(&pool.shRec[2 * k], make_float4(gf.v[0], gf.v[1], gf.v[2], gf.v[3]));
+                            __stcs(&pool.shRec[2 * k + 1], make_float4(gf.v[4], gf.v[5], gf.v[6], neeBsdfPdf));
+                        }
                         shadowIndex = k;
                         shadowDir = nee.direction;
                     } else {
@@ -112,17 +139,62 @@ __device__ __forceinline__ bool shadePath(const ShadeParams &p, uint32_t i) {
         }
 
         // BSDF sampling and Russian roulette, intersection.metal:185-208
-        const BsdfSample bs = shading.material.sample(shading.rnd, -rayDir, shNormal, shading.trueNormal, (uint8_t)rayFlags);
+        BsdfSample bs;
+        float pdfBsdf = 0.0f;  // the BSDF's own pdf of the sampled direction
+        float3 bsdfWeight;     // guided: f / pdfBsdf, the weight BSDF sampling gives the direction
+        if (guided && prng.sample() < alpha) {
+            bs.wi = guideSample(gm, prng.sample3d());
+            const float3 f = shading.material.evaluate(shading.wo, bs.wi, shNormal, shading.trueNormal, pdfBsdf);
+            bs.pdf = alpha * guidePdf(gm, bs.wi) + (1.0f - alpha) * pdfBsdf;
+            bs.weight = bs.pdf > 0.0f ? f * (1.0f / bs.pdf) : f3(0.0f);
+            bsdfWeight = pdfBsdf > 0.0f ? f * (1.0f / pdfBsdf) : f3(0.0f);
+            const bool reflect = dot(bs.wi, shading.trueNormal) * dot(shading.wo, shading.trueNormal) >= 0.0f;
+            bs.flags = (uint8_t)((reflect ? RayFlagsReflection : RayFlagsTransmission) | RayFlagsGlossy);
+        } else {
+            bs = shading.material.sample(shading.rnd, -rayDir, shNormal, shading.trueNormal, (uint8_t)rayFlags);
+            pdfBsdf = bs.pdf;
+            bsdfWeight = bs.weight;
+            if (guided) {
+                if (bs.flags & RayFlagsSingular) {  // only the BSDF technique produces it
+                    bs.weight = bs.weight * (1.0f / (1.0f - alpha));
+                } else if (bs.pdf > 0.0f) {
+                    const float pmix = alpha * guidePdf(gm, bs.wi) + (1.0f - alpha) * bs.pdf;
+                    bs.weight = bs.weight * (bs.pdf / pmix);
+                    bs.pdf = pmix;
+                }
+            }
+        }
         const float3 weight = rayWeight * bs.weight;
         const float meanWeight = mean(weight);
         if (is_finite(meanWeight)) {
-            const float survivalProb = fminf(meanWeight, 1.0f);
+            // Guided, roulette keeps the path with the probability BSDF sampling
+            // would give its direction, so directions the guide favours (high
+            // pdf, small weight) are not culled for it
+            const float survivalProb = fminf(guided ? mean(rayWeight * bsdfWeight) : meanWeight, 1.0f);
             if (prng.sample() < survivalProb && !lastDepth) {
                 alive = true;
                 next[0] = f4(shading.position, SHADOW_EPS);
                 next[1] = f4(bs.wi, inf_f());
                 next[2] = f4(weight * (1.0f / survivalProb), bs.pdf);
-                L4next = __uint_as_float((depth + 1u) | ((uint32_t)bs.flags << 16));
+                // bits 24-31: eligible guide-record vertices so far
+                L4next = __uint_as_float((depth + 1u) | ((uint32_t)bs.flags << 16) | (meta & 0xff000000u));
+                if (training && !(bs.flags & RayFlagsSingular) && pdfBsdf > 0.0f && meanThroughput > 0.0f) {
+                    // Reservoir of one over the path's eligible vertices: the n-th
+                    // replaces the pending record with probability 1 / n (a hash of
+                    // the path and depth, so the PCG stream is untouched).  The
+                    // radiance-weighted target f Li cos / p of the sampled direction
+                    // is survival * (final radiance - radiance so far) / throughput,
+                    // completed when the path ends.
+                    const uint32_t seen = min((meta >> 24) + 1u, 255u);
+                    L4next = __uint_as_float((__float_as_uint(L4next) & 0x00ffffffu) | (seen << 24));
+                    if (seen == 1u || recordHash(pixel, sample, depth) * (float)seen < 1.0f) {
+                        record[0] = make_float4(gf.v[0], gf.v[1], gf.v[2], gf.v[3]);
+                        record[1] = make_float4(gf.v[4], gf.v[5], gf.v[6], pdfBsdf);
+                        record[2] = f4(bs.wi, survivalProb);
+                        record[3] = f4(L, 1.0f / meanThroughput);
+                        recorded = true;
+                    }
+                }
             }
         }
     }
@@ -137,6 +209,11 @@ __device__ __forceinline__ bool shadePath(const ShadeParams &p, uint32_t i) {
             __stcs(&N.tp[k], next[2]);
             __stcs(&N.L[k], f4(L, L4next));
             __stcs(&N.id[k], make_uint4(pixel, sample, rs.x, rs.y));
+            if (training) {
+                if (!recorded && depth > 0u)
+                    for (int r = 0; r < 4; r++) record[r] = __ldcs(&S.rec[4 * i + r]);
+                for (int r = 0; r < 4; r++) __stcs(&N.rec[4 * k + r], record[r]);
+            }
             target = k;
         } else {
             atomicOr(&cnt->errors, ERR_QUEUE_OVERFLOW);
@@ -145,12 +222,20 @@ __device__ __forceinline__ bool shadePath(const ShadeParams &p, uint32_t i) {
         const uint32_t k = warpAppend(&cnt->nF[p.cur]);
         if (k < pool.capacity) {
             __stcs(&pool.fin[k], f4(L, __uint_as_float(pixel)));
+            if (training) {
+                if (depth > 0u)  // a finishing vertex never records
+                    for (int r = 0; r < 4; r++) record[r] = __ldcs(&S.rec[4 * i + r]);
+                for (int r = 0; r < 4; r++) __stcs(&pool.finRec[4 * k + r], record[r]);
+            }
             target = k | SHADOW_TO_FINISHED;
         } else {
             atomicOr(&cnt->errors, ERR_QUEUE_OVERFLOW);
         }
     }
-    if (shadowIndex != 0xffffffffu) __stcs(&pool.shD[shadowIndex], f4(shadowDir, __uint_as_float(target)));
+    if (shadowIndex != 0xffffffffu) {
+        if (recorded && target != 0xffffffffu) target |= SHADOW_TO_RECORD;
+        __stcs(&pool.shD[shadowIndex], f4(shadowDir, __uint_as_float(target)));
+    }
     return h4.x > 0.0f;
 }
 

@@ -13,6 +13,7 @@
 // records with coalesced 16-byte accesses.  Paths that end go to the finish
 // list with their radiance; the next film pass adds them to the film.
 #pragma once
+#include "guide.cuh"
 #include "scene.cuh"
 
 namespace rmd {
@@ -26,6 +27,10 @@ constexpr uint32_t ERR_STACK_OVERFLOW = 2u;
 // target of a shadow ray: position of its path in S[p ^ 1], or in the finish
 // list when this bit is set
 constexpr uint32_t SHADOW_TO_FINISHED = 0x80000000u;
+// set beside it when the ray's light also counts towards the radiance before
+// the path's guide training record (the light sample of the recorded vertex)
+constexpr uint32_t SHADOW_TO_RECORD = 0x40000000u;
+constexpr uint32_t SHADOW_TARGET_MASK = 0x3fffffffu;
 
 // Queue bookkeeping without same-address atomics on the regeneration path:
 // S[p] holds nQ[p] paths continued by the previous iteration followed by the
@@ -51,6 +56,9 @@ struct Counters {
     uint32_t padH[63];
     uint32_t nMiss;       // ... and that missed (back of `order`)
     uint32_t padM[63];
+    uint32_t numRecords;  // guide training records with a nonzero target written so far (a ring index)
+    uint32_t numSamples;  // guide training samples completed since the last training step
+    uint32_t padR[62];
     uint32_t errors;
     uint32_t capacity;    // paths in flight at most (size of each S[p])
     unsigned long long nextPath;    // next path id handed out by the film kernel
@@ -85,8 +93,12 @@ struct PathState {
     float4 *rayO;  // origin.xyz, tmin
     float4 *rayD;  // direction.xyz, tmax
     float4 *tp;    // throughput.xyz, bsdf pdf of the ray
-    float4 *L;     // radiance gathered so far .xyz; .w = depth (bits 0-15) | ray flags (bits 16-23)
+    float4 *L;     // radiance gathered so far .xyz; .w = depth (bits 0-15) | ray flags (bits 16-23) |
+                   // guide-record vertices seen (bits 24-31, training only)
     uint4 *id;     // pixel (y * width + x), sample index, packed PrngState
+    float4 *rec;   // guide training: the pending record of one of the path's vertices, 4 per path
+                   // (features 0-3 | features 4-6, bsdf pdf | direction, survival (0: none) |
+                   //  radiance before, 1 / mean throughput at the vertex); nullptr when not training
 };
 
 struct PathPool {
@@ -96,8 +108,14 @@ struct PathPool {
     uint32_t *order;    // shading order: positions of hits from the front, of misses from the back
     float4 *fin;        // finished paths: radiance.xyz, pixel (bits)
     float4 *shO;        // shadow: origin.xyz, tmax
-    float4 *shD;        // shadow: direction.xyz, target (bits; SHADOW_TO_FINISHED)
-    float4 *shW;        // shadow: weight.xyz
+    float4 *shD;        // shadow: direction.xyz, target (bits; SHADOW_TO_FINISHED, SHADOW_TO_RECORD)
+    float4 *shW;        // shadow: weight.xyz; w: 1 / mean throughput of its vertex for a light record (else 0)
+    // guide training (nullptr when not training)
+    float4 *finRec;       // the pending records of finished paths (4 per entry)
+    float4 *shRec;        // per shadow ray: its vertex's features 0-3 | features 4-6, BSDF pdf of the ray
+    GuideRecord *records; // ring of the latest records with a nonzero target (Counters::numRecords)
+    uint32_t recordCapacity;  // a power of two
+    GuideMixture *guide;  // guiding: the mixture of each hit of this iteration (by position), or nullptr
     uint32_t capacity;
 };
 
@@ -123,6 +141,7 @@ inline PathPool carvePathPool(void *base, uint32_t capacity) {
         pool.s[k].tp = static_cast<float4 *>(take(16));
         pool.s[k].L = static_cast<float4 *>(take(16));
         pool.s[k].id = static_cast<uint4 *>(take(16));
+        pool.s[k].rec = nullptr;  // guiding buffers are allocated by the renderer when enabled
     }
     pool.hit = static_cast<float4 *>(take(16));
     pool.fin = static_cast<float4 *>(take(16));
@@ -131,6 +150,11 @@ inline PathPool carvePathPool(void *base, uint32_t capacity) {
     pool.shW = static_cast<float4 *>(take(16));
     pool.hitInst = static_cast<uint32_t *>(take(4));
     pool.order = static_cast<uint32_t *>(take(4));
+    pool.finRec = nullptr;
+    pool.shRec = nullptr;
+    pool.records = nullptr;
+    pool.recordCapacity = 0;
+    pool.guide = nullptr;
     pool.capacity = capacity;
     return pool;
 }
@@ -143,6 +167,8 @@ struct FrameParams {
     int filmFp64;
     float4 *film;      // rgb sums (w unused)
     double *film64;    // rgb sums, 3 per pixel
+    uint32_t guideDepth;                        // guided sampling at path depths below this (0: none)
+    float3 guideSceneMin, guideSceneInvExtent;  // frame of the guide's position encoding
 };
 
 // kernel parameters of the shading megakernel (device/integrator.cuh)

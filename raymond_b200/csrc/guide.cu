@@ -1,0 +1,734 @@
+// The path-guiding network on the tensor cores: BF16 inference of the vMF
+// mixtures for the hits of one wavefront iteration, and BF16 training
+// (forward, loss gradient, backward, Adam) on the records the tracer
+// produces.  No counterpart in the reference.
+//
+// Each warp processes 16 samples at a time with mma.sync m16n8k16 (BF16
+// inputs, FP32 accumulation): activations live in per-warp shared memory as
+// BF16 rows, weights are read as BF16 [out][in] rows through the read-only
+// cache.  Training accumulates the weight gradient of a block in shared
+// memory (FP32) and adds it to the global gradient once per block.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cmath>
+#include <string>
+#include <vector>
+
+#include "device/guide.cuh"
+#include "device/scene.cuh"
+#include "device/wavefront.cuh"
+#include "guide.h"
+
+namespace rmd {
+namespace {
+
+constexpr int kWarps = 4;  // warps per block; each owns 16 samples at a time
+constexpr int kLd0 = GUIDE_INPUTS + 8, kLdH = GUIDE_HIDDEN + 8, kLdO = GUIDE_OUTPUTS + 4;  // padded rows
+
+// per-warp shared scratch (bf16 activations as uint16_t)
+struct WarpScratch {
+    uint16_t x[16 * kLd0];
+    uint16_t h[3][16 * kLdH];
+    float o[16 * kLdO];
+    uint16_t d[2][16 * kLdH];  // deltas (ping-pong); the output delta uses the first 48 columns
+};
+
+__device__ __forceinline__ uint16_t toBf16(float x) { return (uint16_t)bf16Bits(x); }
+__device__ __forceinline__ float fromBf16(uint16_t b) { return __uint_as_float((uint32_t)b << 16); }
+__device__ __forceinline__ uint32_t pack2(uint16_t lo, uint16_t hi) { return (uint32_t)lo | ((uint32_t)hi << 16); }
+
+__device__ __forceinline__ void mma16816(float c[4], const uint32_t a[4], const uint32_t b[2]) {
+    asm volatile(
+        "mma.sync.aligned.m16n8k16.row.col.f32.bf16.bf16.f32 {%0, %1, %2, %3}, {%4, %5, %6, %7}, {%8, %9}, "
+        "{%0, %1, %2, %3};\n"
+        : "+f"(c[0]), "+f"(c[1]), "+f"(c[2]), "+f"(c[3])
+        : "r"(a[0]), "r"(a[1]), "r"(a[2]), "r"(a[3]), "r"(b[0]), "r"(b[1]));
+}
+
+// Fragment loads.  g = lane / 4, t = lane % 4.  A(m, k) 16 x 16, B(k, n) 16 x 8.
+// A from a row-major [m][k] matrix
+__device__ __forceinline__ void loadA(uint32_t a[4], const uint16_t *m, int ld, int k0, int g, int t) {
+    a[0] = *reinterpret_cast<const uint32_t *>(&m[g * ld + k0 + 2 * t]);
+    a[1] = *reinterpret_cast<const uint32_t *>(&m[(g + 8) * ld + k0 + 2 * t]);
+    a[2] = *reinterpret_cast<const uint32_t *>(&m[g * ld + k0 + 8 + 2 * t]);
+    a[3] = *reinterpret_cast<const uint32_t *>(&m[(g + 8) * ld + k0 + 8 + 2 * t]);
+}
+// A = M^T for a row-major [k][m] matrix M (rows m0.., columns of the 16 samples)
+__device__ __forceinline__ void loadAT(uint32_t a[4], const uint16_t *m, int ld, int m0, int g, int t) {
+    a[0] = pack2(m[(2 * t) * ld + m0 + g], m[(2 * t + 1) * ld + m0 + g]);
+    a[1] = pack2(m[(2 * t) * ld + m0 + g + 8], m[(2 * t + 1) * ld + m0 + g + 8]);
+    a[2] = pack2(m[(2 * t + 8) * ld + m0 + g], m[(2 * t + 9) * ld + m0 + g]);
+    a[3] = pack2(m[(2 * t + 8) * ld + m0 + g + 8], m[(2 * t + 9) * ld + m0 + g + 8]);
+}
+// B(k, n) = W[n][k] for a row-major [n][k] matrix (forward weights)
+__device__ __forceinline__ void loadBnk(uint32_t b[2], const uint16_t *w, int ld, int n0, int k0, int g, int t) {
+    b[0] = __ldg(reinterpret_cast<const uint32_t *>(&w[(n0 + g) * ld + k0 + 2 * t]));
+    b[1] = __ldg(reinterpret_cast<const uint32_t *>(&w[(n0 + g) * ld + k0 + 8 + 2 * t]));
+}
+// B(k, n) = M[k][n] for a row-major [k][n] matrix
+template <bool GLOBAL>
+__device__ __forceinline__ void loadBkn(uint32_t b[2], const uint16_t *m, int ld, int n0, int k0, int g, int t) {
+    if (GLOBAL) {
+        b[0] = pack2(__ldg(&m[(k0 + 2 * t) * ld + n0 + g]), __ldg(&m[(k0 + 2 * t + 1) * ld + n0 + g]));
+        b[1] = pack2(__ldg(&m[(k0 + 2 * t + 8) * ld + n0 + g]), __ldg(&m[(k0 + 2 * t + 9) * ld + n0 + g]));
+    } else {
+        b[0] = pack2(m[(k0 + 2 * t) * ld + n0 + g], m[(k0 + 2 * t + 1) * ld + n0 + g]);
+        b[1] = pack2(m[(k0 + 2 * t + 8) * ld + n0 + g], m[(k0 + 2 * t + 9) * ld + n0 + g]);
+    }
+}
+
+// out[16][N] = act(in[16][K] . W^T + b): W row-major [N][K] (bf16), b fp32
+template <int K, int N, bool RELU>
+__device__ __forceinline__ void denseForward(const uint16_t *in, int ldIn, const uint16_t *w, const float *bias,
+                                             uint16_t *outBf, float *outF, int ldOut, int g, int t) {
+#pragma unroll 1
+    for (int n0 = 0; n0 < N; n0 += 8) {
+        float c[4] = {0.0f, 0.0f, 0.0f, 0.0f};
+#pragma unroll
+        for (int k0 = 0; k0 < K; k0 += 16) {
+            uint32_t a[4], b[2];
+            loadA(a, in, ldIn, k0, g, t);
+            loadBnk(b, w, K, n0, k0, g, t);
+            mma16816(c, a, b);
+        }
+        const float b0 = __ldg(&bias[n0 + 2 * t]), b1 = __ldg(&bias[n0 + 2 * t + 1]);
+        float v[4] = {c[0] + b0, c[1] + b1, c[2] + b0, c[3] + b1};
+        if (RELU)
+#pragma unroll
+            for (int q = 0; q < 4; q++) v[q] = fmaxf(v[q], 0.0f);
+        const int r0 = g, r1 = g + 8, col = n0 + 2 * t;
+        if (outBf) {
+            outBf[r0 * ldOut + col] = toBf16(v[0]);
+            outBf[r0 * ldOut + col + 1] = toBf16(v[1]);
+            outBf[r1 * ldOut + col] = toBf16(v[2]);
+            outBf[r1 * ldOut + col + 1] = toBf16(v[3]);
+        } else {
+            outF[r0 * ldOut + col] = v[0];
+            outF[r0 * ldOut + col + 1] = v[1];
+            outF[r1 * ldOut + col] = v[2];
+            outF[r1 * ldOut + col + 1] = v[3];
+        }
+    }
+}
+
+// the whole forward pass for the 16 samples whose inputs are in s.x
+__device__ void forward(WarpScratch &s, const GuideNetView &net, int g, int t) {
+    denseForward<GUIDE_INPUTS, GUIDE_HIDDEN, true>(s.x, kLd0, net.w[0], net.b[0], s.h[0], nullptr, kLdH, g, t);
+    __syncwarp();
+    denseForward<GUIDE_HIDDEN, GUIDE_HIDDEN, true>(s.h[0], kLdH, net.w[1], net.b[1], s.h[1], nullptr, kLdH, g, t);
+    __syncwarp();
+    denseForward<GUIDE_HIDDEN, GUIDE_HIDDEN, true>(s.h[1], kLdH, net.w[2], net.b[2], s.h[2], nullptr, kLdH, g, t);
+    __syncwarp();
+    denseForward<GUIDE_HIDDEN, GUIDE_OUTPUTS, false>(s.h[2], kLdH, net.w[3], net.b[3], nullptr, s.o, kLdO, g, t);
+    __syncwarp();
+}
+
+// one-blob inputs of 16 samples (features held by lanes 0..15): lane l fills half a row
+__device__ void encodeInputs(WarpScratch &s, const GuideFeatures &f, int lane) {
+    const int row = lane & 15, c0 = (lane >> 4) * (GUIDE_INPUTS / 2);
+    GuideFeatures fr;
+#pragma unroll
+    for (int k = 0; k < 7; k++) fr.v[k] = __shfl_sync(0xffffffffu, f.v[k], row);
+    for (int c = c0; c < c0 + GUIDE_INPUTS / 2; c++) s.x[row * kLd0 + c] = toBf16(guideInput(fr, c));
+    __syncwarp();
+}
+
+__device__ __forceinline__ float sigmoid(float x) { return 1.0f / (1.0f + __expf(-x)); }
+
+// decoded network output of one sample
+struct Decoded {
+    float theta[GUIDE_LOBES], phi[GUIDE_LOBES], st[GUIDE_LOBES], sp[GUIDE_LOBES];  // sigmoids of the raw values
+    float logKappa[GUIDE_LOBES];
+    bool kappaClamped[GUIDE_LOBES];
+    float lambda[GUIDE_LOBES];
+    float alpha, alphaSig;
+};
+
+__device__ Decoded decode(const float *o) {
+    Decoded d;
+    float maxLogit = -1e30f;
+    for (int j = 0; j < GUIDE_LOBES; j++) maxLogit = fmaxf(maxLogit, o[4 * j + 3]);
+    float sum = 0.0f;
+    for (int j = 0; j < GUIDE_LOBES; j++) {
+        d.st[j] = sigmoid(o[4 * j + 0]);
+        d.sp[j] = sigmoid(o[4 * j + 1]);
+        d.theta[j] = M_PI_F * d.st[j];
+        d.phi[j] = 2.0f * M_PI_F * d.sp[j];
+        const float lk = o[4 * j + 2];
+        d.kappaClamped[j] = lk < GUIDE_LOG_KAPPA_MIN || lk > GUIDE_LOG_KAPPA_MAX;
+        d.logKappa[j] = fminf(GUIDE_LOG_KAPPA_MAX, fmaxf(GUIDE_LOG_KAPPA_MIN, lk));
+        d.lambda[j] = __expf(o[4 * j + 3] - maxLogit);
+        sum += d.lambda[j];
+    }
+    for (int j = 0; j < GUIDE_LOBES; j++) d.lambda[j] /= sum;
+    d.alphaSig = sigmoid(o[4 * GUIDE_LOBES]);
+    d.alpha = GUIDE_ALPHA_MIN + (GUIDE_ALPHA_MAX - GUIDE_ALPHA_MIN) * d.alphaSig;
+    return d;
+}
+
+__device__ float3 lobeMean(float theta, float phi) {
+    float st, ct, sp, cp;
+    sincosf(theta, &st, &ct);
+    sincosf(phi, &sp, &cp);
+    return make_float3(st * cp, st * sp, ct);
+}
+
+__device__ GuideMixture pack(const Decoded &d) {
+    GuideMixture m;
+    uint32_t w[4];
+    float total = 0.0f;
+    for (int j = 0; j < GUIDE_LOBES; j++) {
+        const float3 mu = lobeMean(d.theta[j], d.phi[j]);
+        const float kappa = __expf(d.logKappa[j]);
+        total += bf16Lo(bf16Bits(d.lambda[j]));
+        m.lobe[j] = make_uint2(bf16Bits(mu.x) | (bf16Bits(mu.y) << 16), bf16Bits(mu.z) | (bf16Bits(kappa) << 16));
+        if (j & 1) w[j >> 1] |= bf16Bits(d.lambda[j]) << 16;
+        else w[j >> 1] = bf16Bits(d.lambda[j]);
+    }
+    m.weights = make_uint4(w[0], w[1], w[2], w[3]);
+    m.alpha = make_float4(d.alpha, 1.0f / total, 0.0f, 0.0f);
+    return m;
+}
+
+// Loss of one sample and its gradient with respect to the 48 raw outputs
+// (unused ones zero), scaled by `scale`.  Two terms, as in neural parametric
+// mixtures (Dong et al. 2023): the mixture q learns the target distribution
+// alone, -y log q(w); the selection probability a learns the MIS combination,
+// -y log(a q(w) + (1 - a) pb), with q held fixed.  The returned loss is the
+// second (the cross entropy of the distribution that is sampled).
+__device__ float lossGradient(const float *o, float3 w, float pb, float y, float scale, float *grad) {
+    const Decoded d = decode(o);
+    float v[GUIDE_LOBES], q = 0.0f;
+    float3 mu[GUIDE_LOBES];
+    float kappa[GUIDE_LOBES], cosw[GUIDE_LOBES];
+    for (int j = 0; j < GUIDE_LOBES; j++) {
+        mu[j] = lobeMean(d.theta[j], d.phi[j]);
+        kappa[j] = __expf(d.logKappa[j]);
+        cosw[j] = dot(mu[j], w);
+        v[j] = vmfNorm(kappa[j]) * __expf(kappa[j] * (cosw[j] - 1.0f));
+        q += d.lambda[j] * v[j];
+    }
+    const float a = d.alpha;
+    const float pmix = fmaxf(a * q + (1.0f - a) * pb, 1e-20f);
+    const float loss = -y * logf(pmix);
+    for (int c = 0; c < GUIDE_OUTPUTS; c++) grad[c] = 0.0f;
+    // selection probability: a = amin + (amax - amin) sigmoid(z)
+    grad[4 * GUIDE_LOBES] = -y / pmix * scale * (q - pb) * (GUIDE_ALPHA_MAX - GUIDE_ALPHA_MIN) * d.alphaSig *
+                            (1.0f - d.alphaSig);
+    const float gq = -y / fmaxf(q, 1e-20f) * scale;  // dL/dq of -y log q
+    for (int j = 0; j < GUIDE_LOBES; j++) {
+        // softmax weights
+        grad[4 * j + 3] = gq * d.lambda[j] * (v[j] - q);
+        const float gv = gq * d.lambda[j];  // dL/dv_j
+        // concentration: dv/dk = v (1/k - 2 / (e^{2k} - 1) + cos - 1), dk/dlogk = k
+        if (!d.kappaClamped[j]) {
+            const float k = kappa[j];
+            const float dlogC = 1.0f / k - 2.0f / expm1f(2.0f * k);
+            grad[4 * j + 2] = gv * v[j] * (dlogC + cosw[j] - 1.0f) * k;
+        }
+        // mean direction: dv/dmu = v k w; mu(theta, phi)
+        const float gmu = gv * v[j] * kappa[j];
+        float st, ct, sp, cp;
+        sincosf(d.theta[j], &st, &ct);
+        sincosf(d.phi[j], &sp, &cp);
+        const float3 dmu_dtheta = make_float3(ct * cp, ct * sp, -st);
+        const float3 dmu_dphi = make_float3(-st * sp, st * cp, 0.0f);
+        grad[4 * j + 0] = gmu * dot(w, dmu_dtheta) * M_PI_F * d.st[j] * (1.0f - d.st[j]);
+        grad[4 * j + 1] = gmu * dot(w, dmu_dphi) * 2.0f * M_PI_F * d.sp[j] * (1.0f - d.sp[j]);
+    }
+    return loss;
+}
+
+// A training batch: records 0..n-1 of `rec` when n covers all `total` stored
+// records, else n draws (with replacement) from them by a hash of the step.
+struct RecordBatch {
+    const GuideRecord *rec;
+    uint32_t total, n, seed;
+    __device__ const GuideRecord &pick(uint32_t i) const {
+        if (n >= total) return rec[i];
+        uint32_t h = (i * 0x9E3779B1u) ^ (seed * 0x85EBCA77u);
+        h ^= h >> 16;
+        h *= 0x7feb352du;
+        h ^= h >> 15;
+        h *= 0x846ca68bu;
+        h ^= h >> 16;
+        return rec[h % total];
+    }
+};
+
+// ------------------------------------------------------------------ kernels
+// Guide mixtures of the shading points of this iteration's hits (shading
+// order 0..nHit-1) on paths shallower than guideDepth; the features follow
+// the shading kernel's: position on the ray, the triangle's geometric normal,
+// the reversed ray direction.
+__global__ void __launch_bounds__(32 * kWarps) k_guide_infer(Context ctx, PathPool pool, Counters *cnt, uint32_t p,
+                                                          uint32_t guideDepth, GuideNetView net, GuideMixture *out) {
+    extern __shared__ __align__(16) unsigned char smem[];
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31, g = lane >> 2, t = lane & 3;
+    WarpScratch &s = reinterpret_cast<WarpScratch *>(smem)[warp];
+    const uint32_t nHit = cnt->nHit;
+    const PathState S = pool.s[p];
+    const uint32_t tiles = (nHit + 15) / 16;
+    for (uint32_t tile = blockIdx.x * kWarps + warp; tile < tiles; tile += gridDim.x * kWarps) {
+        const uint32_t q = tile * 16 + (lane & 15);
+        bool valid = q < nHit && lane < 16;
+        GuideFeatures f = {};
+        uint32_t idx = 0;
+        if (valid) {
+            idx = pool.order[q];
+            valid = (__float_as_uint(S.L[idx].w) & 0xffffu) < guideDepth;  // the path's depth
+        }
+        if (valid) {
+            const float4 o = S.rayO[idx], dd = S.rayD[idx], h = pool.hit[idx];
+            const PerInstanceData &inst = ctx.instances[pool.hitInst[idx]];
+            const uint4 face = ctx.faces[inst.faceOffset + __float_as_uint(h.w)];
+            const float3 Pc = xyz(ctx.vertices[inst.vertexOffset + face.z]);
+            const float3 P0 = xyz(ctx.vertices[inst.vertexOffset + face.x]) - Pc;
+            const float3 P1 = xyz(ctx.vertices[inst.vertexOffset + face.y]) - Pc;
+            const float3 n = normalize(mul3(inst.normalTransform, cross(P0, P1)));
+            f = guideFeatures(xyz(o) + xyz(dd) * h.x, n, -xyz(dd), net.sceneMin, net.sceneInvExtent);
+        }
+        encodeInputs(s, f, lane);
+        forward(s, net, g, t);
+        if (valid) out[idx] = pack(decode(&s.o[(lane & 15) * kLdO]));
+        __syncwarp();
+    }
+}
+
+// Gradient of the mean loss over a batch of records, accumulated into net.grad.
+__global__ void __launch_bounds__(32 * kWarps) k_guide_train(RecordBatch batch, const float *sumY, GuideNetView net,
+                                                          float *lossOut) {
+    extern __shared__ __align__(16) unsigned char smem[];
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31, g = lane >> 2, t = lane & 3;
+    WarpScratch &s = reinterpret_cast<WarpScratch *>(smem)[warp];
+    float *acc = reinterpret_cast<float *>(smem + kWarps * sizeof(WarpScratch));  // block gradient, GUIDE_PARAMS
+    for (int i = threadIdx.x; i < GUIDE_PARAMS; i += blockDim.x) acc[i] = 0.0f;
+    __syncthreads();
+    const uint32_t n = batch.n;
+    const float scale = 1.0f / (float)n;
+    const float invMeanY = sumY[0] > 0.0f ? (float)n / sumY[0] : 0.0f;
+    float lossSum = 0.0f;
+    const uint32_t tiles = (n + 15) / 16;
+    for (uint32_t tile = blockIdx.x * kWarps + warp; tile < tiles; tile += gridDim.x * kWarps) {
+        const uint32_t r = tile * 16 + (lane & 15);
+        GuideRecord rc = {};
+        if (lane < 16 && r < n) rc = batch.pick(r);
+        GuideFeatures f;
+        for (int k = 0; k < 7; k++) f.v[k] = rc.features[k];
+        encodeInputs(s, f, lane);
+        forward(s, net, g, t);
+        // output deltas: lanes 0..15, one sample each (zero for padding rows)
+        if (lane < 16) {
+            float grad[GUIDE_OUTPUTS];
+            if (r < n) {
+                const float y = fminf(rc.y * invMeanY, 100.0f);
+                lossSum += lossGradient(&s.o[lane * kLdO], make_float3(rc.dir[0], rc.dir[1], rc.dir[2]), rc.pdfBsdf,
+                                        y, scale, grad);
+            } else {
+                for (int c = 0; c < GUIDE_OUTPUTS; c++) grad[c] = 0.0f;
+            }
+            for (int c = 0; c < GUIDE_OUTPUTS; c++) s.d[0][lane * kLdH + c] = toBf16(grad[c]);
+        }
+        __syncwarp();
+        // backward through the four layers: layer l maps h[l-1] (x for l = 0) to h[l]
+        const uint16_t *acts[4] = {s.x, s.h[0], s.h[1], s.h[2]};
+        const int ldActs[4] = {kLd0, kLdH, kLdH, kLdH};
+        int cur = 0;  // delta of layer l's output in s.d[cur]
+#pragma unroll 1
+        for (int l = 3; l >= 0; l--) {
+            const int nOut = l == 3 ? GUIDE_OUTPUTS : GUIDE_HIDDEN;
+            const int nIn = l == 0 ? GUIDE_INPUTS : GUIDE_HIDDEN;
+            const uint16_t *delta = s.d[cur];
+            const uint16_t *in = acts[l];
+            const int ldIn = ldActs[l];
+            float *gW = acc + net.wOffset[l];
+            float *gB = acc + net.bOffset[l];
+            // dW[nOut][nIn] += delta^T . in
+            for (int m0 = 0; m0 < nOut; m0 += 16) {
+                uint32_t a[4];
+                loadAT(a, delta, kLdH, m0, g, t);
+                for (int n0 = 0; n0 < nIn; n0 += 8) {
+                    uint32_t b[2];
+                    loadBkn<false>(b, in, ldIn, n0, 0, g, t);
+                    float c[4] = {0.0f, 0.0f, 0.0f, 0.0f};
+                    mma16816(c, a, b);
+                    atomicAdd(&gW[(m0 + g) * nIn + n0 + 2 * t], c[0]);
+                    atomicAdd(&gW[(m0 + g) * nIn + n0 + 2 * t + 1], c[1]);
+                    atomicAdd(&gW[(m0 + g + 8) * nIn + n0 + 2 * t], c[2]);
+                    atomicAdd(&gW[(m0 + g + 8) * nIn + n0 + 2 * t + 1], c[3]);
+                }
+            }
+            // db[nOut] += column sums of delta
+            for (int c = lane; c < nOut; c += 32) {
+                float sum = 0.0f;
+                for (int row = 0; row < 16; row++) sum += fromBf16(delta[row * kLdH + c]);
+                atomicAdd(&gB[c], sum);
+            }
+            if (l == 0) break;
+            // delta of the layer input: (delta . W) masked by ReLU'(in)
+            uint16_t *next = s.d[cur ^ 1];
+            for (int n0 = 0; n0 < nIn; n0 += 8) {
+                float c[4] = {0.0f, 0.0f, 0.0f, 0.0f};
+                for (int k0 = 0; k0 < nOut; k0 += 16) {
+                    uint32_t a[4], b[2];
+                    loadA(a, delta, kLdH, k0, g, t);
+                    loadBkn<true>(b, net.w[l], nIn, n0, k0, g, t);
+                    mma16816(c, a, b);
+                }
+                const int col = n0 + 2 * t;
+                const float m00 = fromBf16(in[g * ldIn + col]) > 0.0f ? 1.0f : 0.0f;
+                const float m01 = fromBf16(in[g * ldIn + col + 1]) > 0.0f ? 1.0f : 0.0f;
+                const float m10 = fromBf16(in[(g + 8) * ldIn + col]) > 0.0f ? 1.0f : 0.0f;
+                const float m11 = fromBf16(in[(g + 8) * ldIn + col + 1]) > 0.0f ? 1.0f : 0.0f;
+                next[g * kLdH + col] = toBf16(c[0] * m00);
+                next[g * kLdH + col + 1] = toBf16(c[1] * m01);
+                next[(g + 8) * kLdH + col] = toBf16(c[2] * m10);
+                next[(g + 8) * kLdH + col + 1] = toBf16(c[3] * m11);
+            }
+            __syncwarp();
+            cur ^= 1;
+        }
+        __syncwarp();
+    }
+    for (int off = 16; off > 0; off >>= 1) lossSum += __shfl_xor_sync(0xffffffffu, lossSum, off);
+    if (lane == 0 && lossOut) atomicAdd(lossOut, lossSum * scale);
+    __syncthreads();
+    for (int i = threadIdx.x; i < GUIDE_PARAMS; i += blockDim.x)
+        if (acc[i] != 0.0f) atomicAdd(&net.grad[i], acc[i]);
+}
+
+// Adam step on every parameter; refreshes the bf16 weight copies and clears
+// the gradient.
+__global__ void k_guide_adam(GuideNetView net, float lr, float beta1, float beta2, float eps, float corr1,
+                             float corr2) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= GUIDE_PARAMS) return;
+    const float gr = net.grad[i];
+    const float m = beta1 * net.adamM[i] + (1.0f - beta1) * gr;
+    const float v = beta2 * net.adamV[i] + (1.0f - beta2) * gr * gr;
+    net.adamM[i] = m;
+    net.adamV[i] = v;
+    const float w = net.master[i] - lr * (m * corr1) / (sqrtf(v * corr2) + eps);
+    net.master[i] = w;
+    net.grad[i] = 0.0f;
+    if (net.bf16Index[i] >= 0) net.weightsBf16[net.bf16Index[i]] = (uint16_t)bf16Bits(w);
+}
+
+// Sum of the batch's target weights (for the loss normalisation).
+__global__ void k_guide_mean_y(RecordBatch batch, float *sum) {
+    float s = 0.0f;
+    for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < batch.n; i += gridDim.x * blockDim.x)
+        s += batch.pick(i).y;
+    for (int off = 16; off > 0; off >>= 1) s += __shfl_xor_sync(0xffffffffu, s, off);
+    if ((threadIdx.x & 31) == 0 && s != 0.0f) atomicAdd(sum, s);
+}
+
+// Test hook: forward pass of explicit feature vectors, raw outputs.
+__global__ void __launch_bounds__(32 * kWarps) k_guide_forward_test(const float *features, uint32_t n, GuideNetView net,
+                                                                 float *out) {
+    extern __shared__ __align__(16) unsigned char smem[];
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31, g = lane >> 2, t = lane & 3;
+    WarpScratch &s = reinterpret_cast<WarpScratch *>(smem)[warp];
+    const uint32_t tiles = (n + 15) / 16;
+    for (uint32_t tile = blockIdx.x * kWarps + warp; tile < tiles; tile += gridDim.x * kWarps) {
+        const uint32_t q = tile * 16 + (lane & 15);
+        GuideFeatures f = {};
+        if (q < n)
+            for (int k = 0; k < 7; k++) f.v[k] = features[7 * q + k];
+        encodeInputs(s, f, lane);
+        forward(s, net, g, t);
+        if (lane < 16 && q < n)
+            for (int c = 0; c < GUIDE_OUTPUTS; c++) out[GUIDE_OUTPUTS * q + c] = s.o[lane * kLdO + c];
+        __syncwarp();
+    }
+}
+
+// Uploaded parameters: clear Adam and the gradient, refresh the bf16 copies.
+__global__ void k_guide_refresh(GuideNetView net) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= GUIDE_PARAMS) return;
+    net.adamM[i] = 0.0f;
+    net.adamV[i] = 0.0f;
+    net.grad[i] = 0.0f;
+    if (net.bf16Index[i] >= 0) net.weightsBf16[net.bf16Index[i]] = (uint16_t)bf16Bits(net.master[i]);
+}
+
+// Test hook: the packed mixture of one output vector, n samples with their
+// pdf and the pdf at m query directions.
+__global__ void k_guide_mixture_test(const float *outputs, const float *u, int n, float *dirsPdf, const float *queries,
+                                     int m, float *pdfs) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n && i >= m) return;
+    const GuideMixture mix = pack(decode(outputs));
+    if (i < n) {
+        const float3 d = guideSample(mix, make_float3(u[3 * i], u[3 * i + 1], u[3 * i + 2]));
+        dirsPdf[4 * i + 0] = d.x;
+        dirsPdf[4 * i + 1] = d.y;
+        dirsPdf[4 * i + 2] = d.z;
+        dirsPdf[4 * i + 3] = guidePdf(mix, d);
+    }
+    if (i < m) pdfs[i] = guidePdf(mix, make_float3(queries[3 * i], queries[3 * i + 1], queries[3 * i + 2]));
+}
+
+}  // namespace
+}  // namespace rmd
+
+using namespace rmd;
+
+size_t rmdGuideSharedBytes(bool training) {
+    return kWarps * sizeof(WarpScratch) + (training ? GUIDE_PARAMS * sizeof(float) : 0);
+}
+
+cudaError_t rmdGuideConfigure() {
+    cudaError_t e = cudaFuncSetAttribute(k_guide_train, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                         (int)rmdGuideSharedBytes(true));
+    if (e != cudaSuccess) return e;
+    e = cudaFuncSetAttribute(k_guide_infer, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                             (int)rmdGuideSharedBytes(false));
+    if (e != cudaSuccess) return e;
+    return cudaFuncSetAttribute(k_guide_forward_test, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                (int)rmdGuideSharedBytes(false));
+}
+
+cudaError_t rmdLaunchGuideInfer(const Context &ctx, const PathPool &pool, Counters *cnt, uint32_t cur,
+                                uint32_t guideDepth, const GuideNetView &net, GuideMixture *out, int blocks,
+                                cudaStream_t s) {
+    k_guide_infer<<<blocks, 32 * kWarps, rmdGuideSharedBytes(false), s>>>(ctx, pool, cnt, cur, guideDepth, net, out);
+    return cudaGetLastError();
+}
+
+cudaError_t rmdLaunchGuideTrain(const GuideRecord *rec, uint32_t total, uint32_t n, uint32_t seed,
+                                const GuideNetView &net, float *scratch, int blocks, float lr, int step, cudaStream_t s) {
+    // scratch[0]: sum of the target weights, scratch[1]: mean loss
+    cudaError_t e = cudaMemsetAsync(scratch, 0, 2 * sizeof(float), s);
+    if (e != cudaSuccess || total == 0) return e;
+    RecordBatch batch{rec, total, std::min(n, total), seed};
+    k_guide_mean_y<<<256, 256, 0, s>>>(batch, scratch);
+    if ((e = cudaGetLastError()) != cudaSuccess) return e;
+    k_guide_train<<<blocks, 32 * kWarps, rmdGuideSharedBytes(true), s>>>(batch, scratch, net, scratch + 1);
+    if ((e = cudaGetLastError()) != cudaSuccess) return e;
+    const float beta1 = 0.9f, beta2 = 0.999f;
+    const float corr1 = 1.0f / (1.0f - powf(beta1, (float)step)), corr2 = 1.0f / (1.0f - powf(beta2, (float)step));
+    k_guide_adam<<<(GUIDE_PARAMS + 255) / 256, 256, 0, s>>>(net, lr, beta1, beta2, 1e-8f, corr1, corr2);
+    return cudaGetLastError();
+}
+
+cudaError_t rmdLaunchGuideForwardTest(const float *features, uint32_t n, const GuideNetView &net, float *out,
+                                      cudaStream_t s) {
+    const int blocks = (int)std::min<uint32_t>(1024, (n + 16 * kWarps - 1) / (16 * kWarps));
+    k_guide_forward_test<<<std::max(1, blocks), 32 * kWarps, rmdGuideSharedBytes(false), s>>>(features, n, net, out);
+    return cudaGetLastError();
+}
+
+cudaError_t rmdLaunchGuideGradientTest(const GuideRecord *rec, uint32_t n, const GuideNetView &net, float *scratch,
+                                       cudaStream_t s) {
+    cudaError_t e = cudaMemsetAsync(scratch, 0, 2 * sizeof(float), s);
+    if (e != cudaSuccess || n == 0) return e;
+    RecordBatch batch{rec, n, n, 0};
+    k_guide_mean_y<<<256, 256, 0, s>>>(batch, scratch);
+    if ((e = cudaGetLastError()) != cudaSuccess) return e;
+    k_guide_train<<<64, 32 * kWarps, rmdGuideSharedBytes(true), s>>>(batch, scratch, net, scratch + 1);
+    return cudaGetLastError();
+}
+
+// ---------------------------------------------------------------- host side
+namespace rmdhost {
+
+void GuideNet::layout(int wOffset[4], int bOffset[4], int bf16Offset[4]) {
+    const int in[4] = {GUIDE_INPUTS, GUIDE_HIDDEN, GUIDE_HIDDEN, GUIDE_HIDDEN};
+    const int out[4] = {GUIDE_HIDDEN, GUIDE_HIDDEN, GUIDE_HIDDEN, GUIDE_OUTPUTS};
+    int p = 0, q = 0;
+    for (int l = 0; l < 4; l++) {
+        wOffset[l] = p;
+        bf16Offset[l] = q;
+        p += in[l] * out[l];
+        q += in[l] * out[l];
+        bOffset[l] = p;
+        p += out[l];
+    }
+}
+
+void GuideNet::release() {
+    for (void *ptr : {(void *)master, (void *)adamM, (void *)adamV, (void *)grad, (void *)scratch,
+                      (void *)weightsBf16, (void *)bf16Index})
+        if (ptr) cudaFree(ptr);
+    master = adamM = adamV = grad = scratch = nullptr;
+    weightsBf16 = nullptr;
+    bf16Index = nullptr;
+}
+
+cudaError_t GuideNet::allocate() {
+    release();
+    const size_t pb = GUIDE_PARAMS * sizeof(float);
+    cudaError_t e;
+    if ((e = cudaMalloc(&master, pb)) != cudaSuccess || (e = cudaMalloc(&adamM, pb)) != cudaSuccess ||
+        (e = cudaMalloc(&adamV, pb)) != cudaSuccess || (e = cudaMalloc(&grad, pb)) != cudaSuccess ||
+        (e = cudaMalloc(&scratch, 64 * sizeof(float))) != cudaSuccess ||
+        (e = cudaMalloc(&weightsBf16, GUIDE_WEIGHTS * sizeof(uint16_t))) != cudaSuccess ||
+        (e = cudaMalloc(&bf16Index, GUIDE_PARAMS * sizeof(int))) != cudaSuccess)
+        return e;
+    std::vector<int> idx(GUIDE_PARAMS, -1);
+    int wOff[4], bOff[4], qOff[4];
+    layout(wOff, bOff, qOff);
+    for (int l = 0; l < 4; l++)
+        for (int k = 0; k < bOff[l] - wOff[l]; k++) idx[wOff[l] + k] = qOff[l] + k;
+    if ((e = cudaMemcpy(bf16Index, idx.data(), idx.size() * sizeof(int), cudaMemcpyHostToDevice)) != cudaSuccess)
+        return e;
+    return rmdGuideConfigure();
+}
+
+cudaError_t GuideNet::setParams(const float *host, cudaStream_t s) {
+    cudaError_t e = cudaMemcpyAsync(master, host, GUIDE_PARAMS * sizeof(float), cudaMemcpyHostToDevice, s);
+    if (e != cudaSuccess) return e;
+    k_guide_refresh<<<(GUIDE_PARAMS + 255) / 256, 256, 0, s>>>(view(make_float3(0, 0, 0), make_float3(1, 1, 1)));
+    steps = 0;
+    if ((e = cudaGetLastError()) != cudaSuccess) return e;
+    return cudaStreamSynchronize(s);
+}
+
+cudaError_t GuideNet::getParams(float *host, cudaStream_t s) const {
+    cudaError_t e = cudaMemcpyAsync(host, master, GUIDE_PARAMS * sizeof(float), cudaMemcpyDeviceToHost, s);
+    if (e != cudaSuccess) return e;
+    return cudaStreamSynchronize(s);
+}
+
+GuideNetView GuideNet::view(float3 sceneMin, float3 sceneInvExtent) const {
+    GuideNetView v;
+    int qOff[4];
+    layout(v.wOffset, v.bOffset, qOff);
+    for (int l = 0; l < 4; l++) {
+        v.w[l] = weightsBf16 + qOff[l];
+        v.b[l] = master + v.bOffset[l];
+    }
+    v.master = master;
+    v.adamM = adamM;
+    v.adamV = adamV;
+    v.grad = grad;
+    v.weightsBf16 = weightsBf16;
+    v.bf16Index = bf16Index;
+    v.sceneMin = sceneMin;
+    v.sceneInvExtent = sceneInvExtent;
+    return v;
+}
+
+void GuideNet::initParams(float *params, uint32_t seed) {
+    uint64_t state = 0x9E3779B97F4A7C15ull ^ seed;
+    auto uniform = [&]() {  // splitmix64 -> [0, 1)
+        state += 0x9E3779B97F4A7C15ull;
+        uint64_t z = state;
+        z = (z ^ (z >> 30)) * 0xBF58476D1CE4E5B9ull;
+        z = (z ^ (z >> 27)) * 0x94D049BB133111EBull;
+        z ^= z >> 31;
+        return (double)(z >> 11) * (1.0 / 9007199254740992.0);
+    };
+    const int in[4] = {GUIDE_INPUTS, GUIDE_HIDDEN, GUIDE_HIDDEN, GUIDE_HIDDEN};
+    const int out[4] = {GUIDE_HIDDEN, GUIDE_HIDDEN, GUIDE_HIDDEN, GUIDE_OUTPUTS};
+    int wOff[4], bOff[4], qOff[4];
+    layout(wOff, bOff, qOff);
+    for (int l = 0; l < 4; l++) {
+        const double a = std::sqrt(6.0 / (in[l] + out[l]));
+        for (int k = 0; k < in[l] * out[l]; k++) params[wOff[l] + k] = (float)((2.0 * uniform() - 1.0) * a);
+        for (int k = 0; k < out[l]; k++) params[bOff[l] + k] = 0.0f;
+    }
+    float *b4 = params + bOff[3];
+    for (int j = 0; j < GUIDE_LOBES; j++) b4[4 * j + 2] = 1.0f;  // log kappa
+    // alpha = amin + (amax - amin) sigmoid(z) = 0.2
+    const double sig = (0.2 - GUIDE_ALPHA_MIN) / (GUIDE_ALPHA_MAX - GUIDE_ALPHA_MIN);
+    b4[4 * GUIDE_LOBES] = (float)std::log(sig / (1.0 - sig));
+}
+
+}  // namespace rmdhost
+
+// ---------------------------------------------------------------- test hooks
+#include "../../include/raymond.h"
+#include "../../include/raymond_testing.h"
+
+namespace rmdhost {
+rmd_status setLastError(rmd_status status, const char *msg);
+}
+
+namespace {
+rmd_status guideFail(cudaError_t e, const char *what) {
+    std::string m = std::string(what) + ": " + cudaGetErrorString(e);
+    return rmdhost::setLastError(RMD_ERROR_CUDA, m.c_str());
+}
+struct DeviceArray {
+    void *p = nullptr;
+    ~DeviceArray() {
+        if (p) cudaFree(p);
+    }
+    cudaError_t upload(const void *h, size_t n) {
+        cudaError_t e = cudaMalloc(&p, std::max<size_t>(n, 16));
+        if (e != cudaSuccess || n == 0) return e;
+        return cudaMemcpy(p, h, n, cudaMemcpyHostToDevice);
+    }
+    cudaError_t alloc(size_t n) { return cudaMalloc(&p, std::max<size_t>(n, 16)); }
+};
+}  // namespace
+
+extern "C" int32_t rmd_guide_param_count(void) { return GUIDE_PARAMS; }
+
+extern "C" rmd_status rmd_test_guide_forward(const float *params, const float *features, int32_t n, float *out) {
+    if (!params || !features || !out || n < 0)
+        return rmdhost::setLastError(RMD_ERROR_INVALID_ARGUMENT, "rmd_test_guide_forward: invalid arguments");
+    rmdhost::GuideNet net;
+    cudaError_t e;
+    if ((e = net.allocate()) != cudaSuccess) return guideFail(e, "guide allocate");
+    if ((e = net.setParams(params, 0)) != cudaSuccess) return guideFail(e, "guide params");
+    DeviceArray f, o;
+    if ((e = f.upload(features, (size_t)n * 7 * sizeof(float))) != cudaSuccess ||
+        (e = o.alloc((size_t)n * GUIDE_OUTPUTS * sizeof(float))) != cudaSuccess)
+        return guideFail(e, "guide buffers");
+    if ((e = rmdLaunchGuideForwardTest((const float *)f.p, (uint32_t)n,
+                                       net.view(make_float3(0, 0, 0), make_float3(1, 1, 1)), (float *)o.p, 0)) !=
+            cudaSuccess ||
+        (e = cudaMemcpy(out, o.p, (size_t)n * GUIDE_OUTPUTS * sizeof(float), cudaMemcpyDeviceToHost)) != cudaSuccess)
+        return guideFail(e, "guide forward");
+    return RMD_OK;
+}
+
+extern "C" rmd_status rmd_test_guide_gradient(const float *params, const float *records, int32_t n, float *grad,
+                                              float *loss) {
+    if (!params || !records || !grad || n <= 0)
+        return rmdhost::setLastError(RMD_ERROR_INVALID_ARGUMENT, "rmd_test_guide_gradient: invalid arguments");
+    static_assert(sizeof(GuideRecord) == 12 * sizeof(float), "GuideRecord is 12 floats");
+    rmdhost::GuideNet net;
+    cudaError_t e;
+    if ((e = net.allocate()) != cudaSuccess) return guideFail(e, "guide allocate");
+    if ((e = net.setParams(params, 0)) != cudaSuccess) return guideFail(e, "guide params");
+    DeviceArray r;
+    if ((e = r.upload(records, (size_t)n * sizeof(GuideRecord))) != cudaSuccess) return guideFail(e, "guide records");
+    if ((e = rmdLaunchGuideGradientTest((const GuideRecord *)r.p, (uint32_t)n,
+                                        net.view(make_float3(0, 0, 0), make_float3(1, 1, 1)), net.scratch, 0)) !=
+            cudaSuccess ||
+        (e = cudaMemcpy(grad, net.grad, GUIDE_PARAMS * sizeof(float), cudaMemcpyDeviceToHost)) != cudaSuccess)
+        return guideFail(e, "guide gradient");
+    float s[2];
+    if ((e = cudaMemcpy(s, net.scratch, sizeof(s), cudaMemcpyDeviceToHost)) != cudaSuccess)
+        return guideFail(e, "guide loss");
+    if (loss) *loss = s[1];
+    return RMD_OK;
+}
+
+extern "C" rmd_status rmd_test_guide_mixture(const float *outputs, const float *u, int32_t n, float *dirsPdf,
+                                             const float *queries, int32_t m, float *pdfs) {
+    if (!outputs || n < 0 || m < 0 || (n && (!u || !dirsPdf)) || (m && (!queries || !pdfs)))
+        return rmdhost::setLastError(RMD_ERROR_INVALID_ARGUMENT, "rmd_test_guide_mixture: invalid arguments");
+    DeviceArray o, du, dd, dq, dp;
+    cudaError_t e;
+    if ((e = o.upload(outputs, GUIDE_OUTPUTS * sizeof(float))) != cudaSuccess ||
+        (e = du.upload(u, (size_t)n * 3 * sizeof(float))) != cudaSuccess ||
+        (e = dd.alloc((size_t)n * 4 * sizeof(float))) != cudaSuccess ||
+        (e = dq.upload(queries, (size_t)m * 3 * sizeof(float))) != cudaSuccess ||
+        (e = dp.alloc((size_t)m * sizeof(float))) != cudaSuccess)
+        return guideFail(e, "guide mixture buffers");
+    const int total = std::max(n, m);
+    k_guide_mixture_test<<<(total + 127) / 128 + 1, 128>>>((const float *)o.p, (const float *)du.p, n, (float *)dd.p,
+                                                           (const float *)dq.p, m, (float *)dp.p);
+    if ((e = cudaGetLastError()) != cudaSuccess ||
+        (n && (e = cudaMemcpy(dirsPdf, dd.p, (size_t)n * 4 * sizeof(float), cudaMemcpyDeviceToHost)) != cudaSuccess) ||
+        (m && (e = cudaMemcpy(pdfs, dp.p, (size_t)m * sizeof(float), cudaMemcpyDeviceToHost)) != cudaSuccess))
+        return guideFail(e, "guide mixture");
+    return RMD_OK;
+}

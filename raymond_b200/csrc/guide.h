@@ -1,0 +1,76 @@
+// Host interface of the path-guiding network kernels (guide.cu).  No
+// counterpart in the reference.
+#pragma once
+#include <cuda_runtime.h>
+
+#include <cstdint>
+
+#include "device/wavefront.cuh"
+
+namespace rmd {
+
+// 160 -> 64 -> 64 -> 64 -> 48: weights and biases of the four layers
+constexpr int GUIDE_PARAMS = GUIDE_HIDDEN * GUIDE_INPUTS + GUIDE_HIDDEN + 2 * (GUIDE_HIDDEN * GUIDE_HIDDEN + GUIDE_HIDDEN) +
+                             GUIDE_OUTPUTS * GUIDE_HIDDEN + GUIDE_OUTPUTS;
+constexpr int GUIDE_WEIGHTS = GUIDE_HIDDEN * GUIDE_INPUTS + 2 * GUIDE_HIDDEN * GUIDE_HIDDEN + GUIDE_OUTPUTS * GUIDE_HIDDEN;
+
+// Device view of the network: FP32 master parameters (row-major [out][in]
+// weights then biases, layer by layer), their BF16 copies for the tensor
+// cores, and the Adam state.
+struct GuideNetView {
+    const uint16_t *w[4];  // bf16 weights per layer, row-major [out][in]
+    const float *b[4];     // fp32 biases (inside `master`)
+    float *master, *adamM, *adamV, *grad;  // GUIDE_PARAMS each
+    uint16_t *weightsBf16;                  // GUIDE_WEIGHTS
+    const int *bf16Index;                   // per parameter: index into weightsBf16, or -1 (bias)
+    int wOffset[4], bOffset[4];             // parameter offsets of each layer's weights / biases
+    float3 sceneMin, sceneInvExtent;        // position encoding frame
+};
+
+}  // namespace rmd
+
+size_t rmdGuideSharedBytes(bool training);
+cudaError_t rmdGuideConfigure();
+// mixtures of this iteration's hits whose path depth is below guideDepth
+cudaError_t rmdLaunchGuideInfer(const rmd::Context &ctx, const rmd::PathPool &pool, rmd::Counters *cnt, uint32_t cur,
+                                uint32_t guideDepth, const rmd::GuideNetView &net, rmd::GuideMixture *out, int blocks,
+                                cudaStream_t s);
+// One Adam step (`step` counts from 1) on the mean loss over a batch of n
+// records drawn from the `total` stored ones (all of them when n >= total;
+// `seed` varies the draw)
+cudaError_t rmdLaunchGuideTrain(const rmd::GuideRecord *rec, uint32_t total, uint32_t n, uint32_t seed,
+                                const rmd::GuideNetView &net, float *scratch, int blocks, float lr, int step,
+                                cudaStream_t s);
+cudaError_t rmdLaunchGuideForwardTest(const float *features, uint32_t n, const rmd::GuideNetView &net, float *out,
+                                      cudaStream_t s);
+// gradient only (no Adam step): net.grad += d(mean loss); scratch[1] = mean loss
+cudaError_t rmdLaunchGuideGradientTest(const rmd::GuideRecord *rec, uint32_t n, const rmd::GuideNetView &net,
+                                       float *scratch, cudaStream_t s);
+
+namespace rmdhost {
+
+// Device buffers of the guiding network (FP32 master parameters, Adam
+// moments, gradient, BF16 weight copy).
+struct GuideNet {
+    float *master = nullptr, *adamM = nullptr, *adamV = nullptr, *grad = nullptr, *scratch = nullptr;
+    uint16_t *weightsBf16 = nullptr;
+    int *bf16Index = nullptr;
+    int steps = 0;
+    GuideNet() = default;
+    GuideNet(const GuideNet &) = delete;
+    GuideNet &operator=(const GuideNet &) = delete;
+    ~GuideNet() { release(); }
+    void release();
+    bool allocated() const { return master != nullptr; }
+    cudaError_t allocate();
+    // upload FP32 parameters (refreshes the BF16 copy, clears Adam and the gradient)
+    cudaError_t setParams(const float *host, cudaStream_t s);
+    cudaError_t getParams(float *host, cudaStream_t s) const;
+    rmd::GuideNetView view(float3 sceneMin, float3 sceneInvExtent) const;
+    // seeded initialisation: uniform Xavier weights, biases that start the
+    // mixture broad (log kappa 1) and the guide rarely selected (alpha 0.2)
+    static void initParams(float *params, uint32_t seed);
+    static void layout(int wOffset[4], int bOffset[4], int bf16Offset[4]);
+};
+
+}  // namespace rmdhost

@@ -18,7 +18,7 @@ __global__ void k_frame_init(Counters *cnt, uint32_t capacity, uint64_t firstPat
     cnt->traceWork = cnt->shadowWork = 0;
     cnt->errors = 0;
     cnt->capacity = capacity;
-    cnt->nHit = cnt->nMiss = 0;
+    cnt->nHit = cnt->nMiss = 0;  // numRecords / numSamples persist across frames (the renderer resets them)
     cnt->nextPath = firstPath;
     cnt->endPath = endPath;
     cnt->pathsDone = 0;
@@ -50,7 +50,7 @@ __global__ void __launch_bounds__(256) k_film_regen(Context ctx, PathPool pool, 
     const unsigned long long first = cnt->nextPath;
     const PathState S = pool.s[p];
     const uint32_t n = max(nFin, nNew);
-    uint32_t finished = 0;
+    uint32_t finished = 0, samples = 0;
     for (uint32_t j = blockIdx.x * blockDim.x + threadIdx.x; j < n; j += gridDim.x * blockDim.x) {
         if (j < nFin) {
             const float4 f = __ldcs(&pool.fin[j]);
@@ -63,6 +63,26 @@ __global__ void __launch_bounds__(256) k_film_regen(Context ctx, PathPool pool, 
                 atomicAdd(&fp.film[px], make_float4(f.x, f.y, f.z, 1.0f));
             }
             finished++;
+            if (pool.records) {  // complete the path's guide training record
+                const float4 r2 = __ldcs(&pool.finRec[4 * j + 2]);
+                if (r2.w > 0.0f) {
+                    samples++;  // a training sample; only nonzero targets are stored
+                    const float4 r0 = __ldcs(&pool.finRec[4 * j + 0]), r1 = __ldcs(&pool.finRec[4 * j + 1]);
+                    const float4 r3 = __ldcs(&pool.finRec[4 * j + 3]);
+                    const float y = r2.w * r3.w * ((f.x - r3.x) + (f.y - r3.y) + (f.z - r3.z)) * (1.0f / 3.0f);
+                    if (y > 0.0f && isfinite(y)) {
+                        // a ring: the newest records replace the oldest
+                        const uint32_t k = warpAppend(&cnt->numRecords) & (pool.recordCapacity - 1u);
+                        GuideRecord g;
+                        g.features[0] = r0.x; g.features[1] = r0.y; g.features[2] = r0.z; g.features[3] = r0.w;
+                        g.features[4] = r1.x; g.features[5] = r1.y; g.features[6] = r1.z;
+                        g.pdfBsdf = r1.w;
+                        g.dir[0] = r2.x; g.dir[1] = r2.y; g.dir[2] = r2.z;
+                        g.y = y;
+                        pool.records[k] = g;
+                    }
+                }
+            }
         }
         if (j < nNew) {
             const unsigned long long id = first + j;
@@ -83,6 +103,10 @@ __global__ void __launch_bounds__(256) k_film_regen(Context ctx, PathPool pool, 
         }
     }
     blockAdd64(&cnt->pathsDone, finished);
+    if (pool.records) {
+        samples = __reduce_add_sync(0xffffffffu, samples);
+        if ((threadIdx.x & 31) == 0 && samples) atomicAdd(&cnt->numSamples, samples);
+    }
 }
 
 // ------------------------------------------------------------- traversal
@@ -143,6 +167,7 @@ __global__ void __launch_bounds__(128) k_trace_shadow(const WideNode *__restrict
     const uint32_t n = cnt->nShadow;
     if (blockIdx.x == 0 && threadIdx.x == 0) cnt->nextPath += newPaths(cnt, p);
     float4 *nextL = pool.s[p ^ 1u].L;
+    float4 *nextRec = pool.s[p ^ 1u].rec;
     uint32_t target = 0, traced = 0;
     persistentTrace<true>(
         nodes, tris, &cnt->shadowWork, n, &cnt->errors,
@@ -156,13 +181,40 @@ __global__ void __launch_bounds__(128) k_trace_shadow(const WideNode *__restrict
         [&](uint32_t idx, const TraversalState &s) {
             // all ones: the path overflowed its queue
             if (s.hitTri >= 0 || target == 0xffffffffu) return;
-            float4 *dst = (target & SHADOW_TO_FINISHED) ? &pool.fin[target & ~SHADOW_TO_FINISHED] : &nextL[target];
+            const bool finished = (target & SHADOW_TO_FINISHED) != 0u;
+            const uint32_t at = target & SHADOW_TARGET_MASK;
+            float4 *dst = finished ? &pool.fin[at] : &nextL[at];
             const float4 w = __ldcs(&pool.shW[idx]);
             float4 L = *dst;
             L.x += w.x;
             L.y += w.y;
             L.z += w.z;
             *dst = L;
+            if (target & SHADOW_TO_RECORD) {  // light sample of the recorded vertex: not through its sampled direction
+                float4 *rec = finished ? &pool.finRec[4 * at + 3] : &nextRec[4 * at + 3];
+                float4 r = *rec;
+                r.x += w.x;
+                r.y += w.y;
+                r.z += w.z;
+                *rec = r;
+            }
+            if (pool.shRec && w.w > 0.0f) {
+                // a training record of the vertex's light sample: its direction,
+                // target (MIS-weighted contribution / throughput) and features
+                const float y = (w.x + w.y + w.z) * (1.0f / 3.0f) * w.w;
+                if (y > 0.0f && isfinite(y)) {
+                    const uint32_t k = atomicAdd(&cnt->numRecords, 1u) & (pool.recordCapacity - 1u);
+                    const float4 r0 = __ldcs(&pool.shRec[2 * idx]), r1 = __ldcs(&pool.shRec[2 * idx + 1]);
+                    const float4 d = __ldcs(&pool.shD[idx]);
+                    GuideRecord g;
+                    g.features[0] = r0.x; g.features[1] = r0.y; g.features[2] = r0.z; g.features[3] = r0.w;
+                    g.features[4] = r1.x; g.features[5] = r1.y; g.features[6] = r1.z;
+                    g.pdfBsdf = r1.w;
+                    g.dir[0] = d.x; g.dir[1] = d.y; g.dir[2] = d.z;
+                    g.y = y;
+                    pool.records[k] = g;
+                }
+            }
         });
     blockAdd64(&cnt->shadowRays, traced);
 }

@@ -18,6 +18,7 @@
 #include "bvh_build.h"
 #include "codegen.h"
 #include "device/wavefront.cuh"
+#include "guide.h"
 #include "jit.h"
 #include "kernels.h"
 #include "scene_view.h"
@@ -105,6 +106,7 @@ struct rmd_scene {
     std::string moduleSource;
     std::map<int, std::unique_ptr<rmdhost::JitModule>> variants;  // shade kernels by minimum blocks per SM
     uint64_t triangles = 0, bvhNodeCount = 0;
+    float boundsMin[3] = {0, 0, 0}, boundsMax[3] = {1, 1, 1};  // world-space triangle bounds
     int numSurface = 0, numLight = 0;
     int shadeBlocks = 0, traceBlocks = 0, regenBlocks = 0;
     int defaultMinBlocks = 1;
@@ -129,22 +131,35 @@ struct rmd_renderer {
     uint64_t samples = 0;
     rmd_stats stats{};
     cudaEvent_t ev[4] = {};
-    std::vector<cudaEvent_t> stageEvents;  // 4 per iteration + 1, recorded between the stage kernels
+    std::vector<cudaEvent_t> stageEvents;  // recorded between the stage kernels
+    std::vector<int> stageOf;              // stage of the interval that ends at each event
+    // learned path guiding
+    struct Guide {
+        rmd_guide_settings settings{};
+        rmd_guide_stats stats{};
+        rmdhost::GuideNet net;
+        DevBuf mixtures, rec, finRec, shRec, records;
+        uint32_t pathCapacity = 0;    // paths the mixtures / pending-record buffers hold
+        uint32_t recordCapacity = 0;  // nonzero-target records the replay ring holds
+        bool initialised = false;
+    } guide;
     ~rmd_renderer() {
         if (hostCounters) cudaFreeHost(hostCounters);
         for (auto &e : ev)
             if (e) cudaEventDestroy(e);
         for (auto &e : stageEvents) cudaEventDestroy(e);
     }
-    cudaError_t stageEvent(size_t i, cudaEvent_t &out) {
+    // records event i on `st`, closing an interval of stage `stage`
+    cudaError_t stageEvent(size_t i, int stage, cudaStream_t st) {
         while (stageEvents.size() <= i) {
             cudaEvent_t e;
             cudaError_t err = cudaEventCreate(&e);
             if (err != cudaSuccess) return err;
             stageEvents.push_back(e);
+            stageOf.push_back(0);
         }
-        out = stageEvents[i];
-        return cudaSuccess;
+        stageOf[i] = stage;
+        return cudaEventRecord(stageEvents[i], st);
     }
 };
 
@@ -421,6 +436,17 @@ rmd_status rmd_scene_create(rmd_context *ctx, const rmd_scene_desc *d, rmd_scene
         }
     }
     s->triangles = triInst.size();
+    if (!t0.empty()) {
+        for (int k = 0; k < 3; k++) {
+            s->boundsMin[k] = INFINITY;
+            s->boundsMax[k] = -INFINITY;
+        }
+        for (const std::vector<float> *t : {&t0, &t1, &t2})
+            for (size_t i = 0; i < t->size(); i++) {
+                s->boundsMin[i % 3] = std::min(s->boundsMin[i % 3], (*t)[i]);
+                s->boundsMax[i % 3] = std::max(s->boundsMax[i % 3], (*t)[i]);
+            }
+    }
     rmdhost::GpuWideBvh bvh;
     rmdhost::buildWideBvh(t0, t1, t2, triInst, triPrim, bvh);
     s->bvhNodeCount = bvh.nodes.size();
@@ -570,13 +596,70 @@ rmd_status rmd_scene_info(const rmd_scene *s, uint64_t *triangles, uint64_t *bvh
     return RMD_OK;
 }
 
+static rmd_status ensureGuideBuffers(rmd_renderer *r);
+
 static rmd_status allocatePool(rmd_renderer *r) {
     RMD_CUDA(r->pool.alloc(pathPoolBytes(r->capacity)));
     RMD_CUDA(r->counters.alloc(sizeof(Counters)));
-    return RMD_OK;
+    RMD_CUDA(cudaMemset(r->counters.ptr, 0, sizeof(Counters)));
+    return ensureGuideBuffers(r);
 }
 
-static PathPool poolView(rmd_renderer *r) { return carvePathPool(r->pool.ptr, r->capacity); }
+static PathPool poolView(rmd_renderer *r) {
+    PathPool pool = carvePathPool(r->pool.ptr, r->capacity);
+    const auto &g = r->guide;
+    if (g.settings.training && g.pathCapacity >= r->capacity) {
+        pool.s[0].rec = g.rec.as<float4>();
+        pool.s[1].rec = g.rec.as<float4>() + 4 * (size_t)r->capacity;
+        pool.finRec = g.finRec.as<float4>();
+        pool.shRec = g.settings.skip_light_records ? nullptr : g.shRec.as<float4>();
+        pool.records = g.records.as<GuideRecord>();
+        pool.recordCapacity = g.recordCapacity;
+    }
+    if (g.settings.sampling && g.pathCapacity >= r->capacity) pool.guide = g.mixtures.as<GuideMixture>();
+    return pool;
+}
+
+// frame of the guide's position encoding: the scene bounds, slightly padded
+static void guideFrame(const rmd_scene *s, float3 &lo, float3 &invExtent) {
+    float l[3], inv[3];
+    for (int k = 0; k < 3; k++) {
+        const float pad = 1e-3f * std::max(1.0f, s->boundsMax[k] - s->boundsMin[k]);
+        l[k] = s->boundsMin[k] - pad;
+        inv[k] = 1.0f / (s->boundsMax[k] - s->boundsMin[k] + 2.0f * pad);
+    }
+    lo = make_float3(l[0], l[1], l[2]);
+    invExtent = make_float3(inv[0], inv[1], inv[2]);
+}
+
+// (re)allocates the guide's buffers for the renderer's pool size
+static rmd_status ensureGuideBuffers(rmd_renderer *r) {
+    auto &g = r->guide;
+    if (!g.settings.sampling && !g.settings.training) return RMD_OK;
+    if (g.pathCapacity < r->capacity) {
+        g.pathCapacity = 0;
+        g.mixtures.release();
+        g.rec.release();
+        g.finRec.release();
+        g.shRec.release();
+    }
+    if (g.settings.sampling && !g.mixtures.ptr)
+        RMD_CUDA(g.mixtures.alloc((size_t)r->capacity * sizeof(GuideMixture)));
+    if (g.settings.training && !g.rec.ptr) {
+        RMD_CUDA(g.rec.alloc((size_t)r->capacity * 2 * 4 * sizeof(float4)));
+        RMD_CUDA(g.finRec.alloc((size_t)r->capacity * 4 * sizeof(float4)));
+        RMD_CUDA(g.shRec.alloc((size_t)r->capacity * 2 * sizeof(float4)));
+    }
+    g.pathCapacity = r->capacity;
+    const uint32_t want = g.settings.replay_records;
+    if (g.settings.training && g.recordCapacity != want) {
+        g.recordCapacity = 0;
+        RMD_CUDA(g.records.alloc((size_t)want * sizeof(GuideRecord)));
+        g.recordCapacity = want;
+        RMD_CUDA(cudaMemset(&r->counters.as<Counters>()->numRecords, 0, 2 * sizeof(uint32_t)));
+    }
+    return RMD_OK;
+}
 
 rmd_status rmd_renderer_set_size(rmd_renderer *r, uint32_t width, uint32_t height) {
     if (!r || width == 0 || height == 0 || width > 65535 || height > 65535)
@@ -667,20 +750,41 @@ rmd_status rmd_render(rmd_renderer *r, const rmd_render_settings *s) {
     fp.filmFp64 = s->film_fp64 ? 1 : 0;
     fp.film = r->film.as<float4>();
     fp.film64 = r->film64.as<double>();
-    const PathPool pool = poolView(r);
     Counters *cnt = r->counters.as<Counters>();
     const uint64_t firstPath = firstSample * numPixels;
 
     ShadeParams sp;
     sp.ctx = r->dctx;
-    sp.pool = pool;
-    sp.fp = fp;
     sp.counters = cnt;
     void *shadeArgs[] = {&sp};
     const int tb = ctx->smCount * r->traceBlocksPerSm;
     const int rb = std::min<int>((r->capacity + 255) / 256, ctx->smCount * 8);
     const int sb = r->shadeBlocks;
 
+    // guiding
+    auto &guide = r->guide;
+    const bool guideSampling = guide.settings.sampling != 0;
+    const bool guideTraining = guide.settings.training != 0;
+    GuideNetView net{};
+    if (guideSampling || guideTraining) {
+        rmd_status gs = ensureGuideBuffers(r);
+        if (gs != RMD_OK) return gs;
+        float3 lo, inv;
+        guideFrame(scene, lo, inv);
+        net = guide.net.view(lo, inv);
+        fp.guideDepth = guideSampling ? guide.settings.guided_depth : 0u;
+        fp.guideSceneMin = lo;
+        fp.guideSceneInvExtent = inv;
+    }
+    const PathPool pool = poolView(r);
+    sp.pool = pool;
+    sp.fp = fp;
+    const int guideBlocks = ctx->smCount * 4;
+    const int trainBlocks = ctx->smCount;
+    const uint32_t batch = guide.settings.batch_size;
+    uint64_t trainSteps = 0;
+
+    enum { STAGE_FILM, STAGE_TRACE, STAGE_GUIDE, STAGE_SHADE, STAGE_SHADOW, STAGES };
     RMD_CUDA(cudaEventRecord(r->ev[0], st));
     RMD_CUDA(rmdLaunchFrameInit(pool, cnt, firstPath, firstPath + numPaths, st));
     // every path needs at most max_depth iterations after it is generated, and
@@ -690,24 +794,22 @@ rmd_status rmd_render(rmd_renderer *r, const rmd_render_settings *s) {
     uint32_t cur = 0;
     bool done = false;
     size_t evi = 0;
-    cudaEvent_t e;
-    RMD_CUDA(r->stageEvent(evi++, e));
-    RMD_CUDA(cudaEventRecord(e, st));
+    RMD_CUDA(r->stageEvent(evi++, STAGE_FILM, st));
     while (!done) {
         for (int k = 0; k < 4; k++, it++) {
             RMD_CUDA(rmdLaunchFilmRegen(r->dctx, pool, fp, cnt, cur, rb, st));
-            RMD_CUDA(r->stageEvent(evi++, e));
-            RMD_CUDA(cudaEventRecord(e, st));
+            RMD_CUDA(r->stageEvent(evi++, STAGE_FILM, st));
             RMD_CUDA(rmdLaunchTraceClosest(scene->bvhNodes.as<WideNode>(), scene->bvhTris.as<float4>(), pool, cnt, cur, tb, st));
-            RMD_CUDA(r->stageEvent(evi++, e));
-            RMD_CUDA(cudaEventRecord(e, st));
+            RMD_CUDA(r->stageEvent(evi++, STAGE_TRACE, st));
+            if (guideSampling) {
+                RMD_CUDA(rmdLaunchGuideInfer(r->dctx, pool, cnt, cur, fp.guideDepth, net, pool.guide, guideBlocks, st));
+                RMD_CUDA(r->stageEvent(evi++, STAGE_GUIDE, st));
+            }
             sp.cur = cur;
             RMD_CUDA(cudaLaunchKernel((const void *)r->shade, dim3(sb), dim3(128), shadeArgs, 0, st));
-            RMD_CUDA(r->stageEvent(evi++, e));
-            RMD_CUDA(cudaEventRecord(e, st));
+            RMD_CUDA(r->stageEvent(evi++, STAGE_SHADE, st));
             RMD_CUDA(rmdLaunchTraceShadow(scene->bvhNodes.as<WideNode>(), scene->bvhTris.as<float4>(), pool, cnt, cur, tb, st));
-            RMD_CUDA(r->stageEvent(evi++, e));
-            RMD_CUDA(cudaEventRecord(e, st));
+            RMD_CUDA(r->stageEvent(evi++, STAGE_SHADOW, st));
             cur ^= 1u;
         }
         RMD_CUDA(cudaMemcpyAsync(r->hostCounters, cnt, sizeof(Counters), cudaMemcpyDeviceToHost, st));
@@ -717,6 +819,24 @@ rmd_status rmd_render(rmd_renderer *r, const rmd_render_settings *s) {
             r->stats.errors = h.errors;
             return fail(RMD_ERROR_QUEUE_OVERFLOW, "device error flags " + std::to_string(h.errors));
         }
+        if (guideTraining && h.numSamples >= batch) {
+            // one Adam step per `batch` samples gathered since the last check,
+            // each on records drawn from the replay ring
+            const uint32_t stored = std::min(h.numRecords, guide.recordCapacity);
+            const uint32_t steps = h.numSamples / batch * guide.settings.steps_per_batch;
+            for (uint32_t k = 0; k < steps && stored > 0; k++) {
+                RMD_CUDA(rmdLaunchGuideTrain(guide.records.as<GuideRecord>(), stored, guide.settings.step_records,
+                                             (uint32_t)guide.net.steps + 1u, net, guide.net.scratch, trainBlocks,
+                                             guide.settings.learning_rate, guide.net.steps + 1, st));
+                guide.net.steps++;
+                trainSteps++;
+                guide.stats.steps++;
+            }
+            RMD_CUDA(cudaMemsetAsync(&cnt->numSamples, 0, sizeof(uint32_t), st));
+            guide.stats.samples += h.numSamples;
+            guide.stats.records = h.numRecords;
+            RMD_CUDA(r->stageEvent(evi++, STAGE_GUIDE, st));
+        }
         if (h.pathsDone >= numPaths) done = true;
         else if (it > maxIters) return fail(RMD_ERROR_WATCHDOG, "render did not drain in the iteration bound");
     }
@@ -724,11 +844,16 @@ rmd_status rmd_render(rmd_renderer *r, const rmd_render_settings *s) {
     RMD_CUDA(cudaEventSynchronize(r->ev[1]));
     float ms = 0;
     cudaEventElapsedTime(&ms, r->ev[0], r->ev[1]);
-    double stage[4] = {0, 0, 0, 0};  // film+regen, trace, shade, shadow
+    double stage[STAGES] = {};
     for (size_t i = 1; i < evi; i++) {
         float t = 0;
         cudaEventElapsedTime(&t, r->stageEvents[i - 1], r->stageEvents[i]);
-        stage[(i - 1) % 4] += t;
+        stage[r->stageOf[i]] += t;
+    }
+    if (trainSteps) {
+        float loss = 0;
+        RMD_CUDA(cudaMemcpy(&loss, guide.net.scratch + 1, sizeof(float), cudaMemcpyDeviceToHost));
+        guide.stats.last_loss = loss;
     }
     const Counters &h = *r->hostCounters;
     r->stats.paths = h.pathsDone;
@@ -737,10 +862,11 @@ rmd_status rmd_render(rmd_renderer *r, const rmd_render_settings *s) {
     r->stats.shadow_rays = h.shadowRays;
     r->stats.iterations = it;
     r->stats.ms_total = ms;
-    r->stats.ms_film = stage[0];
-    r->stats.ms_trace = stage[1];
-    r->stats.ms_shade = stage[2];
-    r->stats.ms_shadow = stage[3];
+    r->stats.ms_film = stage[STAGE_FILM];
+    r->stats.ms_trace = stage[STAGE_TRACE];
+    r->stats.ms_shade = stage[STAGE_SHADE];
+    r->stats.ms_shadow = stage[STAGE_SHADOW];
+    r->stats.ms_guide = stage[STAGE_GUIDE];
     r->samples = std::max<uint64_t>(r->samples, firstSample + s->spp);
     return RMD_OK;
 }
@@ -913,6 +1039,64 @@ rmd_status rmd_renderer_set_tuning(rmd_renderer *r, const rmd_tune_result *t) {
     if (t->pool_size != 0 && t->pool_size != r->capacity) {
         r->capacity = t->pool_size;
         if ((st = allocatePool(r)) != RMD_OK) return st;
+    }
+    return RMD_OK;
+}
+
+// --------------------------------------------------------------------- guiding
+rmd_status rmd_renderer_set_guide(rmd_renderer *r, const rmd_guide_settings *settings) {
+    if (!r || !settings) return fail(RMD_ERROR_INVALID_ARGUMENT, "NULL argument");
+    const uint32_t ring = settings->replay_records;
+    if (settings->sampling > 1 || settings->training > 1 || settings->reset > 1 || settings->learning_rate < 0.0f ||
+        !std::isfinite(settings->learning_rate) || settings->batch_size > (1u << 26) ||
+        (settings->batch_size != 0 && settings->batch_size < 16) || settings->step_records > (1u << 24) ||
+        settings->steps_per_batch > 1024 || settings->skip_light_records > 1 || settings->guided_depth > 65535 ||
+        (ring != 0 && (ring < 1024 || ring > (1u << 26) || (ring & (ring - 1)) != 0)))
+        return fail(RMD_ERROR_INVALID_ARGUMENT, "invalid guide settings");
+    RMD_CUDA(cudaSetDevice(r->scene->ctx->device));
+    auto &g = r->guide;
+    rmd_guide_settings next = *settings;
+    if (next.batch_size == 0) next.batch_size = 1u << 20;
+    if (next.learning_rate == 0.0f) next.learning_rate = 1e-3f;
+    if (next.step_records == 0) next.step_records = 1u << 14;
+    if (next.replay_records == 0) next.replay_records = 1u << 18;
+    if (next.steps_per_batch == 0) next.steps_per_batch = 1;
+    if (next.guided_depth == 0) next.guided_depth = 65535;
+    if (!g.net.allocated()) RMD_CUDA(g.net.allocate());
+    if (!g.initialised || next.reset) {
+        std::vector<float> params(GUIDE_PARAMS);
+        rmdhost::GuideNet::initParams(params.data(), next.seed);
+        RMD_CUDA(g.net.setParams(params.data(), r->scene->ctx->stream));
+        g.initialised = true;
+        g.stats = rmd_guide_stats{};
+        // records gathered by an earlier network are dropped with it
+        RMD_CUDA(cudaMemset(&r->counters.as<Counters>()->numRecords, 0, 2 * sizeof(uint32_t)));
+    }
+    next.reset = 0;
+    g.settings = next;
+    return ensureGuideBuffers(r);
+}
+
+rmd_status rmd_renderer_guide_stats(const rmd_renderer *r, rmd_guide_stats *out) {
+    if (!r || !out) return fail(RMD_ERROR_INVALID_ARGUMENT, "NULL argument");
+    *out = r->guide.stats;
+    return RMD_OK;
+}
+
+rmd_status rmd_renderer_guide_params(rmd_renderer *r, float *params, int32_t write) {
+    if (!r || !params || write < 0 || write > 1) return fail(RMD_ERROR_INVALID_ARGUMENT, "invalid argument");
+    RMD_CUDA(cudaSetDevice(r->scene->ctx->device));
+    auto &g = r->guide;
+    if (!g.net.allocated()) RMD_CUDA(g.net.allocate());
+    if (write) {
+        for (int i = 0; i < GUIDE_PARAMS; i++)
+            if (!std::isfinite(params[i])) return fail(RMD_ERROR_INVALID_ARGUMENT, "non-finite guide parameter");
+        RMD_CUDA(g.net.setParams(params, r->scene->ctx->stream));
+        g.initialised = true;
+        g.stats = rmd_guide_stats{};
+    } else {
+        if (!g.initialised) return fail(RMD_ERROR_INVALID_ARGUMENT, "the guide has not been set up");
+        RMD_CUDA(g.net.getParams(params, r->scene->ctx->stream));
     }
     return RMD_OK;
 }

@@ -323,3 +323,85 @@ def cornell_all_lights(seed: int = 4, envmap_exponent: int = 7) -> dict[str, Any
     sc["sun_lights"] = [{"shader": 1, "direction": (0.2, 0.3, 1.0), "angle": 0.1, "color": (1.0, 1.0, 1.0)}]
     sc["name"] = "cornell_all_lights"
     return sc
+
+
+def _boxes_mesh(lo: np.ndarray, hi: np.ndarray, materials: np.ndarray) -> dict[str, Any]:
+    """Many axis-aligned boxes in one mesh (vectorised box_mesh): 24 vertices
+    and 12 outward-facing triangles per box."""
+    lo = np.asarray(lo, np.float32)
+    hi = np.asarray(hi, np.float32)
+    nb = lo.shape[0]
+    verts, norms = [], []
+    for axis in range(3):
+        a, b = [k for k in range(3) if k != axis]
+        for side in (-1, 1):
+            c = np.zeros((nb, 4, 3), np.float32)
+            c[:, :, axis] = (lo if side < 0 else hi)[:, None, axis]
+            for i, (ua, ub) in enumerate(((0, 0), (1, 0), (1, 1), (0, 1))):
+                c[:, i, a] = (lo if ua == 0 else hi)[:, a]
+                c[:, i, b] = (lo if ub == 0 else hi)[:, b]
+            nrm = np.zeros(3, np.float32)
+            nrm[axis] = side
+            verts.append(c)
+            norms.append(np.broadcast_to(nrm, (nb, 4, 3)))
+    V = np.stack(verts, 1).reshape(nb * 24, 3)
+    N = np.stack(norms, 1).reshape(nb * 24, 3).astype(np.float32)
+    quad = np.array([[0, 1, 2], [0, 2, 3]], np.uint32)
+    idx = (np.arange(nb * 6, dtype=np.uint32)[:, None, None] * 4 + quad[None]).reshape(-1, 3)
+    idx = _orient(V, idx, N[idx[:, 0]])
+    T = np.tile(np.array([[0, 0], [1, 0], [1, 1], [0, 1]], np.float32), (nb * 6, 1))
+    mats = np.repeat(np.asarray(materials, np.uint16), 12)
+    return {"vertices": V, "normals": N, "texcoords": T, "indices": idx.astype(np.uint32), "materials": mats}
+
+
+def glossy_room(seed: int = 1, num_boxes: int = 16667, num_materials: int = 64,
+                envmap_exponent: int = 8) -> dict[str, Any]:
+    """A closed 10 x 10 x 4 room lit only through a 0.5 x 0.5 window (in the
+    wall z = 10) by an environment of constant radiance 5, filled with random
+    furniture boxes (16,667 boxes: 200,022 triangles with the room) standing
+    on the floor or floating as shelves.  Every surface is Principled with
+    roughness U[0.02, 0.3], base colour U[0.2, 0.9]^3, metallic 0; boxes draw
+    one of `num_materials` such materials.  The camera stands inside looking
+    across the room towards the window."""
+    rng = np.random.default_rng(seed)
+    mats = []
+    for i in range(num_materials + 6):
+        mats.append((f"glossy{i}", M.principled(base_color=tuple(rng.uniform(0.2, 0.9, 3)),
+                                                 roughness=float(rng.uniform(0.02, 0.3)), metallic=0.0)))
+    W, D, Hh = 10.0, 10.0, 4.0
+    wx0, wx1, wy0, wy1 = 4.75, 5.25, 2.25, 2.75  # the window in the wall z = D
+    walls = [
+        quad_mesh([[0, 0, 0], [W, 0, 0], [W, 0, D], [0, 0, D]], [0, 1, 0], num_materials + 0),        # floor
+        quad_mesh([[0, Hh, 0], [W, Hh, 0], [W, Hh, D], [0, Hh, D]], [0, -1, 0], num_materials + 1),   # ceiling
+        quad_mesh([[0, 0, 0], [W, 0, 0], [W, Hh, 0], [0, Hh, 0]], [0, 0, 1], num_materials + 2),      # z = 0
+        quad_mesh([[0, 0, 0], [0, Hh, 0], [0, Hh, D], [0, 0, D]], [1, 0, 0], num_materials + 3),      # x = 0
+        quad_mesh([[W, 0, 0], [W, Hh, 0], [W, Hh, D], [W, 0, D]], [-1, 0, 0], num_materials + 4),     # x = W
+    ]
+    # wall z = D with the window hole: four quads around it
+    for (x0, x1, y0, y1) in [(0, W, 0, wy0), (0, W, wy1, Hh), (0, wx0, wy0, wy1), (wx1, W, wy0, wy1)]:
+        walls.append(quad_mesh([[x0, y0, D], [x1, y0, D], [x1, y1, D], [x0, y1, D]], [0, 0, -1], num_materials + 5))
+    room = merge_meshes(walls)
+    # furniture: sizes U[0.05, 0.6]^3; 70 % stand on the floor, 30 % float (shelves);
+    # a clear corridor is kept around the camera
+    size = rng.uniform(0.05, 0.6, (num_boxes, 3)).astype(np.float32)
+    pos = np.stack([rng.uniform(0.2, W - 0.8, num_boxes), np.zeros(num_boxes),
+                    rng.uniform(0.2, D - 1.5, num_boxes)], 1).astype(np.float32)
+    floating = rng.uniform(0, 1, num_boxes) < 0.3
+    pos[floating, 1] = rng.uniform(0.5, Hh - 0.8, floating.sum())
+    near_cam = (np.abs(pos[:, 0] - 2.0) < 1.2) & (np.abs(pos[:, 2] - 1.5) < 1.2)
+    pos[near_cam, 0] += 2.5
+    hi = np.minimum(pos + size, [W - 0.05, Hh - 0.05, D - 0.05]).astype(np.float32)
+    boxes = _boxes_mesh(pos, hi, rng.integers(0, num_materials, num_boxes))
+    ident = _identity()
+    return {
+        "name": "glossy_room",
+        "materials": mats,
+        "light_materials": [("world", M.world((1.0, 1.0, 1.0, 1.0), 5.0))],
+        "shapes": [room, boxes],
+        "entities": [{"shape": 0, "matrix": ident, "visibility": VISIBLE_ALL},
+                     {"shape": 1, "matrix": ident, "visibility": VISIBLE_ALL}],
+        "camera": {"transform": look_at((2.0, 1.6, 1.5), (6.0, 1.4, 9.0)), "near_clip": 1e-3,
+                   "far_clip": 100.0, "focal_length": 1.2},
+        "world_shader": 0,
+        "envmap_exponent": envmap_exponent,
+    }

@@ -19,7 +19,7 @@ GOLDEN = ROOT / "tests" / "golden"
 def declared_symbols():
     names = []
     for h in (ROOT / "include").glob("*.h"):
-        names += re.findall(r"^\s*(?:rmd_status|void|const char \*)\s*(rmd_\w+)\s*\(", h.read_text(), re.M)
+        names += re.findall(r"^\s*(?:rmd_status|void|int32_t|const char \*)\s*(rmd_\w+)\s*\(", h.read_text(), re.M)
     return sorted(set(names))
 
 
