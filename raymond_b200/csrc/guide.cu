@@ -257,22 +257,169 @@ struct RecordBatch {
     }
 };
 
+// ------------------------------------------------------- inference core
+// Inference keeps activations in registers: the FP32 accumulator fragment of
+// an m16n8k16 product (rows g, g + 8; columns 2t, 2t + 1 of an n8 tile) is,
+// rounded to BF16 and paired, exactly the A fragment of the next layer for
+// the k16 block made of two adjacent n8 tiles.  A warp runs 32 samples (two
+// m16 tiles) so every weight fragment, read from shared memory, feeds two
+// products, and all 32 lanes decode one sample each at the end.
+constexpr int kInferWarps = 4;
+constexpr int kLdW1 = GUIDE_INPUTS + 8, kLdW = GUIDE_HIDDEN + 8;  // padded weight rows (conflict-free fragments)
+constexpr int kLdOut = GUIDE_OUTPUTS + 1;                          // odd stride: conflict-free per-sample reads
+
+struct InferSmem {
+    uint16_t w1[GUIDE_HIDDEN * kLdW1];
+    uint16_t w2[GUIDE_HIDDEN * kLdW];
+    uint16_t w3[GUIDE_HIDDEN * kLdW];
+    uint16_t w4[GUIDE_OUTPUTS * kLdW];
+    float b[3 * GUIDE_HIDDEN + GUIDE_OUTPUTS];
+    float out[kInferWarps][32 * kLdOut];
+};
+
+// copies the bf16 weights (padded rows) and the biases into shared memory
+__device__ void loadInferWeights(InferSmem &sm, const GuideNetView &net) {
+    auto copy = [&](uint16_t *dst, const uint16_t *src, int rows, int cols, int ld) {
+        const int vecs = cols / 8;  // 16-byte vectors per row
+        for (int i = threadIdx.x; i < rows * vecs; i += blockDim.x) {
+            const int r = i / vecs, c = i - r * vecs;
+            *reinterpret_cast<uint4 *>(&dst[r * ld + 8 * c]) = __ldg(reinterpret_cast<const uint4 *>(&src[r * cols + 8 * c]));
+        }
+    };
+    copy(sm.w1, net.w[0], GUIDE_HIDDEN, GUIDE_INPUTS, kLdW1);
+    copy(sm.w2, net.w[1], GUIDE_HIDDEN, GUIDE_HIDDEN, kLdW);
+    copy(sm.w3, net.w[2], GUIDE_HIDDEN, GUIDE_HIDDEN, kLdW);
+    copy(sm.w4, net.w[3], GUIDE_OUTPUTS, GUIDE_HIDDEN, kLdW);
+    for (int i = threadIdx.x; i < 3 * GUIDE_HIDDEN + GUIDE_OUTPUTS; i += blockDim.x) {
+        const int l = min(i / GUIDE_HIDDEN, 3);
+        sm.b[i] = __ldg(&net.b[l][i - l * GUIDE_HIDDEN]);
+    }
+    __syncthreads();
+}
+
+__device__ __forceinline__ uint32_t packBf16(float lo, float hi) { return bf16Bits(lo) | (bf16Bits(hi) << 16); }
+
+// one-blob value of bin `bin` of a feature with `bins` bins
+__device__ __forceinline__ float oneBlob(float v, int bins, int bin) {
+    const float d = v * (float)bins - ((float)bin + 0.5f);
+    const float x = fmaxf(0.0f, 1.0f - d * d);
+    return x * x;
+}
+
+// B fragment of W (row-major [n][k], padded stride ld) for n tile n0, k block k0
+__device__ __forceinline__ void loadBs(uint32_t b[2], const uint16_t *w, int ld, int n0, int k0, int g, int t) {
+    b[0] = *reinterpret_cast<const uint32_t *>(&w[(n0 + g) * ld + k0 + 2 * t]);
+    b[1] = *reinterpret_cast<const uint32_t *>(&w[(n0 + g) * ld + k0 + 8 + 2 * t]);
+}
+
+// accumulators (2 m tiles x 8 n tiles) -> bias, ReLU, bf16 A fragments (2 m tiles x 4 k blocks)
+__device__ __forceinline__ void hiddenToA(const float acc[2][8][4], const float *bias, uint32_t h[2][4][4], int t) {
+#pragma unroll
+    for (int mt = 0; mt < 2; mt++)
+#pragma unroll
+        for (int nt = 0; nt < 8; nt++) {
+            const float b0 = bias[nt * 8 + 2 * t], b1 = bias[nt * 8 + 2 * t + 1];
+            const uint32_t lo = packBf16(fmaxf(acc[mt][nt][0] + b0, 0.0f), fmaxf(acc[mt][nt][1] + b1, 0.0f));
+            const uint32_t hi = packBf16(fmaxf(acc[mt][nt][2] + b0, 0.0f), fmaxf(acc[mt][nt][3] + b1, 0.0f));
+            h[mt][nt >> 1][(nt & 1) * 2 + 0] = lo;  // a0 / a2: row g
+            h[mt][nt >> 1][(nt & 1) * 2 + 1] = hi;  // a1 / a3: row g + 8
+        }
+}
+
+// hidden 64 -> 64 layer on register fragments
+__device__ __forceinline__ void hiddenLayer(const uint32_t in[2][4][4], const uint16_t *w, const float *bias,
+                                            uint32_t out[2][4][4], int g, int t) {
+    float acc[2][8][4] = {};
+#pragma unroll
+    for (int kb = 0; kb < 4; kb++)
+#pragma unroll
+        for (int nt = 0; nt < 8; nt++) {
+            uint32_t b[2];
+            loadBs(b, w, kLdW, nt * 8, kb * 16, g, t);
+            mma16816(acc[0][nt], in[0][kb], b);
+            mma16816(acc[1][nt], in[1][kb], b);
+        }
+    hiddenToA(acc, bias, out, t);
+}
+
+// Forward pass of the 32 samples of a warp (lane l holds the features of
+// sample l); raw outputs (with bias) land in `out` rows of kLdOut floats.
+__device__ void inferWarp(const InferSmem &sm, const GuideFeatures &f, float *out, int lane) {
+    const int g = lane >> 2, t = lane & 3;
+    // layer 1: the one-blob inputs are built in the A fragment registers; k
+    // block kb covers 16 bins of one feature
+    float acc[2][8][4] = {};
+#pragma unroll
+    for (int kb = 0; kb < GUIDE_INPUTS / 16; kb++) {
+        const int feature = kb < 6 ? kb >> 1 : kb - 3;
+        const int bins = kb < 6 ? 32 : 16;
+        const int bin0 = kb < 6 ? (kb & 1) * 16 : 0;
+        uint32_t a[2][4];
+#pragma unroll
+        for (int mt = 0; mt < 2; mt++) {
+            const float vg = __shfl_sync(0xffffffffu, f.v[feature], mt * 16 + g);
+            const float vh = __shfl_sync(0xffffffffu, f.v[feature], mt * 16 + g + 8);
+            const int c = bin0 + 2 * t;
+            a[mt][0] = packBf16(oneBlob(vg, bins, c), oneBlob(vg, bins, c + 1));
+            a[mt][1] = packBf16(oneBlob(vh, bins, c), oneBlob(vh, bins, c + 1));
+            a[mt][2] = packBf16(oneBlob(vg, bins, c + 8), oneBlob(vg, bins, c + 9));
+            a[mt][3] = packBf16(oneBlob(vh, bins, c + 8), oneBlob(vh, bins, c + 9));
+        }
+#pragma unroll
+        for (int nt = 0; nt < 8; nt++) {
+            uint32_t b[2];
+            loadBs(b, sm.w1, kLdW1, nt * 8, kb * 16, g, t);
+            mma16816(acc[0][nt], a[0], b);
+            mma16816(acc[1][nt], a[1], b);
+        }
+    }
+    uint32_t h1[2][4][4], h2[2][4][4];
+    hiddenToA(acc, sm.b, h1, t);
+    hiddenLayer(h1, sm.w2, sm.b + GUIDE_HIDDEN, h2, g, t);
+    hiddenLayer(h2, sm.w3, sm.b + 2 * GUIDE_HIDDEN, h1, g, t);
+    // output layer: 48 columns (6 n tiles)
+    float o[2][6][4] = {};
+#pragma unroll
+    for (int kb = 0; kb < 4; kb++)
+#pragma unroll
+        for (int nt = 0; nt < 6; nt++) {
+            uint32_t b[2];
+            loadBs(b, sm.w4, kLdW, nt * 8, kb * 16, g, t);
+            mma16816(o[0][nt], h1[0][kb], b);
+            mma16816(o[1][nt], h1[1][kb], b);
+        }
+    const float *b4 = sm.b + 3 * GUIDE_HIDDEN;
+#pragma unroll
+    for (int mt = 0; mt < 2; mt++)
+#pragma unroll
+        for (int nt = 0; nt < 6; nt++) {
+            const int col = nt * 8 + 2 * t, r0 = mt * 16 + g, r1 = r0 + 8;
+            out[r0 * kLdOut + col] = o[mt][nt][0] + b4[col];
+            out[r0 * kLdOut + col + 1] = o[mt][nt][1] + b4[col + 1];
+            out[r1 * kLdOut + col] = o[mt][nt][2] + b4[col];
+            out[r1 * kLdOut + col + 1] = o[mt][nt][3] + b4[col + 1];
+        }
+    __syncwarp();
+}
+
 // ------------------------------------------------------------------ kernels
 // Guide mixtures of the shading points of this iteration's hits (shading
 // order 0..nHit-1) on paths shallower than guideDepth; the features follow
 // the shading kernel's: position on the ray, the triangle's geometric normal,
 // the reversed ray direction.
-__global__ void __launch_bounds__(32 * kWarps) k_guide_infer(Context ctx, PathPool pool, Counters *cnt, uint32_t p,
-                                                          uint32_t guideDepth, GuideNetView net, GuideMixture *out) {
+__global__ void __launch_bounds__(32 * kInferWarps) k_guide_infer(Context ctx, PathPool pool, Counters *cnt,
+                                                               uint32_t p, uint32_t guideDepth, GuideNetView net,
+                                                               GuideMixture *out) {
     extern __shared__ __align__(16) unsigned char smem[];
-    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31, g = lane >> 2, t = lane & 3;
-    WarpScratch &s = reinterpret_cast<WarpScratch *>(smem)[warp];
+    InferSmem &sm = *reinterpret_cast<InferSmem *>(smem);
+    loadInferWeights(sm, net);
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
     const uint32_t nHit = cnt->nHit;
     const PathState S = pool.s[p];
-    const uint32_t tiles = (nHit + 15) / 16;
-    for (uint32_t tile = blockIdx.x * kWarps + warp; tile < tiles; tile += gridDim.x * kWarps) {
-        const uint32_t q = tile * 16 + (lane & 15);
-        bool valid = q < nHit && lane < 16;
+    const uint32_t tiles = (nHit + 31) / 32;
+    for (uint32_t tile = blockIdx.x * kInferWarps + warp; tile < tiles; tile += gridDim.x * kInferWarps) {
+        const uint32_t q = tile * 32 + lane;
+        bool valid = q < nHit;
         GuideFeatures f = {};
         uint32_t idx = 0;
         if (valid) {
@@ -289,9 +436,9 @@ __global__ void __launch_bounds__(32 * kWarps) k_guide_infer(Context ctx, PathPo
             const float3 n = normalize(mul3(inst.normalTransform, cross(P0, P1)));
             f = guideFeatures(xyz(o) + xyz(dd) * h.x, n, -xyz(dd), net.sceneMin, net.sceneInvExtent);
         }
-        encodeInputs(s, f, lane);
-        forward(s, net, g, t);
-        if (valid) out[idx] = pack(decode(&s.o[(lane & 15) * kLdO]));
+        float *o = sm.out[warp];
+        inferWarp(sm, f, o, lane);
+        if (valid) out[idx] = pack(decode(&o[lane * kLdOut]));
         __syncwarp();
     }
 }
@@ -424,22 +571,24 @@ __global__ void k_guide_mean_y(RecordBatch batch, float *sum) {
     if ((threadIdx.x & 31) == 0 && s != 0.0f) atomicAdd(sum, s);
 }
 
-// Test hook: forward pass of explicit feature vectors, raw outputs.
-__global__ void __launch_bounds__(32 * kWarps) k_guide_forward_test(const float *features, uint32_t n, GuideNetView net,
-                                                                 float *out) {
+// Test hook: forward pass of explicit feature vectors through the inference
+// core, raw outputs.
+__global__ void __launch_bounds__(32 * kInferWarps) k_guide_forward_test(const float *features, uint32_t n,
+                                                                      GuideNetView net, float *out) {
     extern __shared__ __align__(16) unsigned char smem[];
-    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31, g = lane >> 2, t = lane & 3;
-    WarpScratch &s = reinterpret_cast<WarpScratch *>(smem)[warp];
-    const uint32_t tiles = (n + 15) / 16;
-    for (uint32_t tile = blockIdx.x * kWarps + warp; tile < tiles; tile += gridDim.x * kWarps) {
-        const uint32_t q = tile * 16 + (lane & 15);
+    InferSmem &sm = *reinterpret_cast<InferSmem *>(smem);
+    loadInferWeights(sm, net);
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const uint32_t tiles = (n + 31) / 32;
+    for (uint32_t tile = blockIdx.x * kInferWarps + warp; tile < tiles; tile += gridDim.x * kInferWarps) {
+        const uint32_t q = tile * 32 + lane;
         GuideFeatures f = {};
         if (q < n)
             for (int k = 0; k < 7; k++) f.v[k] = features[7 * q + k];
-        encodeInputs(s, f, lane);
-        forward(s, net, g, t);
-        if (lane < 16 && q < n)
-            for (int c = 0; c < GUIDE_OUTPUTS; c++) out[GUIDE_OUTPUTS * q + c] = s.o[lane * kLdO + c];
+        float *o = sm.out[warp];
+        inferWarp(sm, f, o, lane);
+        if (q < n)
+            for (int c = 0; c < GUIDE_OUTPUTS; c++) out[GUIDE_OUTPUTS * q + c] = o[lane * kLdOut + c];
         __syncwarp();
     }
 }
@@ -477,7 +626,7 @@ __global__ void k_guide_mixture_test(const float *outputs, const float *u, int n
 using namespace rmd;
 
 size_t rmdGuideSharedBytes(bool training) {
-    return kWarps * sizeof(WarpScratch) + (training ? GUIDE_PARAMS * sizeof(float) : 0);
+    return training ? kWarps * sizeof(WarpScratch) + GUIDE_PARAMS * sizeof(float) : sizeof(InferSmem);
 }
 
 cudaError_t rmdGuideConfigure() {
@@ -494,7 +643,8 @@ cudaError_t rmdGuideConfigure() {
 cudaError_t rmdLaunchGuideInfer(const Context &ctx, const PathPool &pool, Counters *cnt, uint32_t cur,
                                 uint32_t guideDepth, const GuideNetView &net, GuideMixture *out, int blocks,
                                 cudaStream_t s) {
-    k_guide_infer<<<blocks, 32 * kWarps, rmdGuideSharedBytes(false), s>>>(ctx, pool, cnt, cur, guideDepth, net, out);
+    k_guide_infer<<<blocks, 32 * kInferWarps, rmdGuideSharedBytes(false), s>>>(ctx, pool, cnt, cur, guideDepth, net,
+                                                                              out);
     return cudaGetLastError();
 }
 
@@ -516,8 +666,9 @@ cudaError_t rmdLaunchGuideTrain(const GuideRecord *rec, uint32_t total, uint32_t
 
 cudaError_t rmdLaunchGuideForwardTest(const float *features, uint32_t n, const GuideNetView &net, float *out,
                                       cudaStream_t s) {
-    const int blocks = (int)std::min<uint32_t>(1024, (n + 16 * kWarps - 1) / (16 * kWarps));
-    k_guide_forward_test<<<std::max(1, blocks), 32 * kWarps, rmdGuideSharedBytes(false), s>>>(features, n, net, out);
+    const int blocks = (int)std::min<uint32_t>(1024, (n + 32 * kInferWarps - 1) / (32 * kInferWarps));
+    k_guide_forward_test<<<std::max(1, blocks), 32 * kInferWarps, rmdGuideSharedBytes(false), s>>>(features, n, net,
+                                                                                                   out);
     return cudaGetLastError();
 }
 

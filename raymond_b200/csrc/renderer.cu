@@ -779,7 +779,7 @@ rmd_status rmd_render(rmd_renderer *r, const rmd_render_settings *s) {
     const PathPool pool = poolView(r);
     sp.pool = pool;
     sp.fp = fp;
-    const int guideBlocks = ctx->smCount * 4;
+    const int guideBlocks = ctx->smCount * 3;  // resident blocks of the inference kernel (shared memory)
     const int trainBlocks = ctx->smCount;
     const uint32_t batch = guide.settings.batch_size;
     uint64_t trainSteps = 0;

@@ -325,44 +325,50 @@ def cornell_all_lights(seed: int = 4, envmap_exponent: int = 7) -> dict[str, Any
     return sc
 
 
-def _boxes_mesh(lo: np.ndarray, hi: np.ndarray, materials: np.ndarray) -> dict[str, Any]:
-    """Many axis-aligned boxes in one mesh (vectorised box_mesh): 24 vertices
-    and 12 outward-facing triangles per box."""
+def _boxes_mesh(lo: np.ndarray, hi: np.ndarray, materials: np.ndarray, tess: int = 1) -> dict[str, Any]:
+    """Many axis-aligned boxes in one mesh (vectorised box_mesh), each face a
+    tess x tess grid of quads: 12 tess^2 outward-facing triangles per box."""
     lo = np.asarray(lo, np.float32)
     hi = np.asarray(hi, np.float32)
     nb = lo.shape[0]
+    g = np.linspace(0.0, 1.0, tess + 1, dtype=np.float32)
+    u0, v0 = np.meshgrid(g[:-1], g[:-1], indexing="ij")
+    u1, v1 = u0 + 1.0 / tess, v0 + 1.0 / tess
+    cu = np.stack([u0, u1, u1, u0], -1).reshape(-1, 4)  # (tess^2, 4) quad corners in face coordinates
+    cv = np.stack([v0, v0, v1, v1], -1).reshape(-1, 4)
     verts, norms = [], []
     for axis in range(3):
         a, b = [k for k in range(3) if k != axis]
         for side in (-1, 1):
-            c = np.zeros((nb, 4, 3), np.float32)
-            c[:, :, axis] = (lo if side < 0 else hi)[:, None, axis]
-            for i, (ua, ub) in enumerate(((0, 0), (1, 0), (1, 1), (0, 1))):
-                c[:, i, a] = (lo if ua == 0 else hi)[:, a]
-                c[:, i, b] = (lo if ub == 0 else hi)[:, b]
+            c = np.zeros((nb, tess * tess, 4, 3), np.float32)
+            c[..., axis] = (lo if side < 0 else hi)[:, None, None, axis]
+            c[..., a] = lo[:, None, None, a] + (hi - lo)[:, None, None, a] * cu[None]
+            c[..., b] = lo[:, None, None, b] + (hi - lo)[:, None, None, b] * cv[None]
             nrm = np.zeros(3, np.float32)
             nrm[axis] = side
             verts.append(c)
-            norms.append(np.broadcast_to(nrm, (nb, 4, 3)))
-    V = np.stack(verts, 1).reshape(nb * 24, 3)
-    N = np.stack(norms, 1).reshape(nb * 24, 3).astype(np.float32)
+            norms.append(np.broadcast_to(nrm, c.shape))
+    nq = nb * 6 * tess * tess
+    V = np.stack(verts, 1).reshape(nq * 4, 3)
+    N = np.stack(norms, 1).reshape(nq * 4, 3).astype(np.float32)
     quad = np.array([[0, 1, 2], [0, 2, 3]], np.uint32)
-    idx = (np.arange(nb * 6, dtype=np.uint32)[:, None, None] * 4 + quad[None]).reshape(-1, 3)
+    idx = (np.arange(nq, dtype=np.uint32)[:, None, None] * 4 + quad[None]).reshape(-1, 3)
     idx = _orient(V, idx, N[idx[:, 0]])
-    T = np.tile(np.array([[0, 0], [1, 0], [1, 1], [0, 1]], np.float32), (nb * 6, 1))
-    mats = np.repeat(np.asarray(materials, np.uint16), 12)
+    T = np.tile(np.array([[0, 0], [1, 0], [1, 1], [0, 1]], np.float32), (nq, 1))
+    mats = np.repeat(np.asarray(materials, np.uint16), 12 * tess * tess)
     return {"vertices": V, "normals": N, "texcoords": T, "indices": idx.astype(np.uint32), "materials": mats}
 
 
-def glossy_room(seed: int = 1, num_boxes: int = 16667, num_materials: int = 64,
+def glossy_room(seed: int = 1, num_boxes: int = 136, tess: int = 11, num_materials: int = 64,
                 envmap_exponent: int = 8) -> dict[str, Any]:
     """A closed 10 x 10 x 4 room lit only through a 0.5 x 0.5 window (in the
-    wall z = 10) by an environment of constant radiance 5, filled with random
-    furniture boxes (16,667 boxes: 200,022 triangles with the room) standing
-    on the floor or floating as shelves.  Every surface is Principled with
-    roughness U[0.02, 0.3], base colour U[0.2, 0.9]^3, metallic 0; boxes draw
-    one of `num_materials` such materials.  The camera stands inside looking
-    across the room towards the window."""
+    wall z = 10) by an environment of constant radiance 5, furnished with
+    random boxes standing on the floor or floating as shelves, each face
+    tessellated into tess x tess quads (136 boxes of 1,452 triangles: 197,490
+    triangles with the room).  Every surface is Principled with roughness
+    U[0.02, 0.3], base colour U[0.2, 0.9]^3, metallic 0; boxes draw one of
+    `num_materials` such materials.  The camera stands inside looking across
+    the room towards the window."""
     rng = np.random.default_rng(seed)
     mats = []
     for i in range(num_materials + 6):
@@ -381,17 +387,18 @@ def glossy_room(seed: int = 1, num_boxes: int = 16667, num_materials: int = 64,
     for (x0, x1, y0, y1) in [(0, W, 0, wy0), (0, W, wy1, Hh), (0, wx0, wy0, wy1), (wx1, W, wy0, wy1)]:
         walls.append(quad_mesh([[x0, y0, D], [x1, y0, D], [x1, y1, D], [x0, y1, D]], [0, 0, -1], num_materials + 5))
     room = merge_meshes(walls)
-    # furniture: sizes U[0.05, 0.6]^3; 70 % stand on the floor, 30 % float (shelves);
-    # a clear corridor is kept around the camera
-    size = rng.uniform(0.05, 0.6, (num_boxes, 3)).astype(np.float32)
-    pos = np.stack([rng.uniform(0.2, W - 0.8, num_boxes), np.zeros(num_boxes),
-                    rng.uniform(0.2, D - 1.5, num_boxes)], 1).astype(np.float32)
+    # furniture: footprint U[0.3, 1.2]^2, height U[0.2, 1.5]; 70 % stand on the
+    # floor, 30 % float as shelves; the camera's surroundings are kept clear
+    size = np.stack([rng.uniform(0.3, 1.2, num_boxes), rng.uniform(0.2, 1.5, num_boxes),
+                     rng.uniform(0.3, 1.2, num_boxes)], 1).astype(np.float32)
+    pos = np.stack([rng.uniform(0.1, W - 1.3, num_boxes), np.zeros(num_boxes),
+                    rng.uniform(0.1, D - 1.3, num_boxes)], 1).astype(np.float32)
     floating = rng.uniform(0, 1, num_boxes) < 0.3
-    pos[floating, 1] = rng.uniform(0.5, Hh - 0.8, floating.sum())
-    near_cam = (np.abs(pos[:, 0] - 2.0) < 1.2) & (np.abs(pos[:, 2] - 1.5) < 1.2)
-    pos[near_cam, 0] += 2.5
+    pos[floating, 1] = rng.uniform(0.5, Hh - 1.6, floating.sum())
+    near_cam = (np.abs(pos[:, 0] + 0.5 * size[:, 0] - 2.0) < 1.5) & (np.abs(pos[:, 2] + 0.5 * size[:, 2] - 1.5) < 1.5)
+    pos[near_cam, 0] += 3.0
     hi = np.minimum(pos + size, [W - 0.05, Hh - 0.05, D - 0.05]).astype(np.float32)
-    boxes = _boxes_mesh(pos, hi, rng.integers(0, num_materials, num_boxes))
+    boxes = _boxes_mesh(pos, hi, rng.integers(0, num_materials, num_boxes), tess)
     ident = _identity()
     return {
         "name": "glossy_room",
