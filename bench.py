@@ -15,6 +15,14 @@ weak scaling, no collective on the data path.
 `e2e`    : the same metric through the public C ABI with host buffers: each
            step uploads the camera (rmd_renderer_set_camera), renders and
            reads the film back to host memory (rmd_film_read).
+`guided` : the learned path guide on the glossy room (config 4: 197,490
+           triangles, lit through a 0.5 x 0.5 window, 1280x720, max depth 16):
+           relMSE against an FP64 oracle of 65,536 spp of the plain tracer,
+           plain tracer at 1,024 spp against the guided tracer (online
+           training, 2^20 samples per Adam step, lr 1e-3) rendered in 32-spp
+           chunks for up to 3x the plain tracer's device time: the guided
+           tracer's time to the plain tracer's 1,024-spp relMSE and its relMSE
+           at equal time.  Rank 0 only; --no-guided skips it.
 --impl reference times the reference's own CPU implementation of the path
 (its device code built for the host, oracle/_ref, all host cores; the oracle
 restatement when that build is absent) on a bounded sample of the workload.
@@ -56,6 +64,7 @@ BYTES_FILM_PER_PATH = 16 + 32 + 80
 # of one steady-state launch divided by the units it processed; small case, see
 # profiles/ncu_full_spheres_terrain_480x270.md); only the closest-hit kernel's is used
 TRAFFIC_PER_UNIT = {"trace": 106.8}
+GUIDED_W, GUIDED_H, GUIDED_DEPTH, GUIDED_ORACLE_SPP, GUIDED_PLAIN_SPP, GUIDED_CHUNK = 1280, 720, 16, 65536, 1024, 32
 CPU_BASELINE_SPP = 16  # CPU sample: 16 one-spp frames of the full image (about 10-20 s on 16 cores)
 
 
@@ -185,6 +194,70 @@ def run_reference(args):
     print(json.dumps(line), flush=True)
 
 
+def guided_leg(api, ctx, oracle_spp: int) -> dict:
+    """Equal-time relMSE of the guided tracer against the plain one (config 4)."""
+    from raymond_b200 import scenes
+    from raymond_b200._abi import SceneDesc
+    from raymond_b200.metrics import relmse
+
+    desc = SceneDesc(scenes.glossy_room(seed=1))
+    scene = api.Scene(ctx, desc)
+    W, H, depth = GUIDED_W, GUIDED_H, GUIDED_DEPTH
+    oracle = api.Renderer(scene, W, H)
+    per_call = max(1, min(oracle_spp, (1 << 27) // (W * H)))
+    done, oracle_ms = 0, 0.0
+    while done < oracle_spp:
+        n = min(per_call, oracle_spp - done)
+        oracle.render(spp=n, max_depth=depth, film_fp64=True, seed=77)
+        oracle_ms += oracle.stats()["ms_total"]
+        done += n
+    reference = oracle.film64() / oracle_spp
+    oracle.close()
+    plain = api.Renderer(scene, W, H)
+    plain_ms = 0.0
+    for _ in range(GUIDED_PLAIN_SPP // GUIDED_CHUNK):
+        plain.render(spp=GUIDED_CHUNK, max_depth=depth, seed=1)
+        plain_ms += plain.stats()["ms_total"]
+    e_plain = relmse(plain.film(normalize=True), reference)
+    plain.close()
+    settings = {"batch_size": 1 << 20, "learning_rate": 1e-3}
+    g = api.Renderer(scene, W, H)
+    g.set_guide(sampling=True, training=True, seed=1, **settings)
+    ms, spp, curve, parity = 0.0, 0, [], None
+    guide_ms = train_ms = 0.0
+    while ms < 3 * plain_ms:
+        g.render(spp=GUIDED_CHUNK, max_depth=depth, seed=2)
+        st = g.stats()
+        ms += st["ms_total"]
+        guide_ms += st["ms_guide"]
+        train_ms += st["ms_guide_train"]
+        spp += GUIDED_CHUNK
+        e = relmse(g.film(normalize=True), reference)
+        curve.append((spp, ms, e))
+        if parity is None and e <= e_plain:
+            parity = (spp, ms)
+            if ms >= plain_ms:
+                break
+    # relMSE at the plain tracer's time (interpolated between chunks)
+    e_eq = None
+    for (s0, t0, e0), (s1, t1, e1) in zip(curve, curve[1:]):
+        if t0 <= plain_ms <= t1:
+            e_eq = e0 + (e1 - e0) * (plain_ms - t0) / (t1 - t0)
+    stats = g.guide_stats()
+    g.close()
+    return {
+        "workload": f"glossy_room_{W}x{H}_depth{depth}", "triangles": scene.info()["triangles"],
+        "oracle": {"spp": oracle_spp, "film": "fp64", "tracer": "plain", "device_s": oracle_ms / 1e3},
+        "plain": {"spp": GUIDED_PLAIN_SPP, "ms": plain_ms, "relmse": e_plain},
+        "guided": {"relmse_at_equal_time": e_eq, "ms_to_plain_relmse": parity[1] if parity else None,
+                   "spp_to_plain_relmse": parity[0] if parity else None,
+                   "time_ratio": parity[1] / plain_ms if parity else None, "target_time_ratio": 1.0 / 3.0,
+                   "ms_guide": guide_ms, "ms_guide_train": train_ms, "adam_steps": stats["steps"],
+                   "records": stats["records"], "settings": settings,
+                   "curve": [{"spp": s_, "ms": round(t_, 2), "relmse": e_} for s_, t_, e_ in curve[::4]]},
+    }
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -197,6 +270,8 @@ def main():
     ap.add_argument("--height", type=int, default=H, help="override (profiling runs only)")
     ap.add_argument("--spp", type=int, default=SPP, help="override (profiling runs only)")
     ap.add_argument("--no-e2e", action="store_true")
+    ap.add_argument("--no-guided", action="store_true")
+    ap.add_argument("--oracle-spp", type=int, default=GUIDED_ORACLE_SPP, help="guided leg: oracle samples")
     ap.add_argument("--no-autotune", action="store_true")
     ap.add_argument("--tuning", default="", help="shade_min_blocks,trace_blocks_per_sm,pool_size: apply "
                     "these launch choices instead of autotuning (profiling runs)")
@@ -313,6 +388,8 @@ def main():
         "scene_build_s": build_s,
         "autotune": dict(tune, seconds=tune_s) if tune else None,
     }
+    if not args.no_guided and world == 1:
+        line["guided"] = guided_leg(api, ctx, args.oracle_spp)
     if not args.no_cpu_baseline:
         line["cpu_baseline"] = cpu_baseline_sample(desc)
     print(json.dumps(line), flush=True)

@@ -264,6 +264,7 @@ typedef struct rmd_stats {
     uint32_t errors;           /* device error flags (queue overflow, watchdog) */
     uint64_t rays;             /* closest-hit rays traced (segments + misses) */
     double   ms_guide;         /* guide inference and training (0 without guiding) */
+    double   ms_guide_train;   /* of which training (gradient and Adam steps) */
 } rmd_stats;
 
 typedef struct rmd_context rmd_context;

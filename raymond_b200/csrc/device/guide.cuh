@@ -27,15 +27,18 @@ constexpr int GUIDE_USED_OUTPUTS = 4 * GUIDE_LOBES + 1;
 constexpr float GUIDE_LOG_KAPPA_MIN = -3.0f, GUIDE_LOG_KAPPA_MAX = 5.0f;
 constexpr float GUIDE_ALPHA_MIN = 0.02f, GUIDE_ALPHA_MAX = 0.5f;
 
-// Packed mixture of one shading point, 96 bytes: lobe j as bf16 pairs
-// (mu.x, mu.y), (mu.z, kappa); the 8 weights as bf16; the selection
-// probability of the guide and the normalisation of the stored weights.
-// Sampling and pdf both read these values, so they describe exactly the same
-// distribution.
+// Packed mixture of one shading point, 128 bytes: lobe j as bf16 pairs
+// (mu.x, mu.y), (mu.z, kappa) (mu renormalised on use); its pdf coefficient
+// weight_j / sum(weights) * C(kappa_j) in FP32; the 8 selection weights as
+// bf16; the selection probability of the guide.  Sampling and pdf read the
+// same rounded values, so they describe the same distribution.
 struct GuideMixture {
     uint2 lobe[GUIDE_LOBES];
+    float coef[GUIDE_LOBES];
     uint4 weights;
-    float4 alpha;  // x: selection probability of the guide, y: 1 / sum of the bf16 weights
+    float alpha;     // selection probability of the guide
+    float invTotal;  // 1 / sum of the bf16 weights
+    float pad[2];
 };
 
 RMD_HD uint32_t bf16Bits(float x) {  // round to nearest even
@@ -45,55 +48,47 @@ RMD_HD uint32_t bf16Bits(float x) {  // round to nearest even
 RMD_HD float bf16Lo(uint32_t w) { return __uint_as_float(w << 16); }
 RMD_HD float bf16Hi(uint32_t w) { return __uint_as_float(w & 0xffff0000u); }
 
-struct GuideLobe {
-    float3 mu;
-    float kappa, weight, norm;  // norm: kappa / (2 pi (1 - exp(-2 kappa)))
-};
-
+// C(kappa) = kappa / (2 pi (1 - exp(-2 kappa))), the vMF normalisation on S2
 RMD_HD float vmfNorm(float kappa) { return kappa / (2.0f * M_PI_F * -expm1f(-2.0f * kappa)); }
 
-RMD_HD GuideLobe guideLobe(const GuideMixture &m, int j) {
-    GuideLobe l;
-    const uint2 p = m.lobe[j];
-    l.mu = normalize(make_float3(bf16Lo(p.x), bf16Hi(p.x), bf16Lo(p.y)));
-    l.kappa = bf16Hi(p.y);
-    const uint32_t w = j < 2 ? m.weights.x : j < 4 ? m.weights.y : j < 6 ? m.weights.z : m.weights.w;
-    l.weight = (j & 1) ? bf16Hi(w) : bf16Lo(w);
-    l.norm = vmfNorm(l.kappa);
-    return l;
-}
+RMD_HD float3 lobeMu(uint2 l) { return normalize(make_float3(bf16Lo(l.x), bf16Hi(l.x), bf16Lo(l.y))); }
 
 // pdf of the mixture (solid angle)
-RMD_HD float guidePdf(const GuideMixture &m, float3 w) {
+RMD_HD float guidePdf(const GuideMixture *m, float3 w) {
     float p = 0.0f;
 #pragma unroll
     for (int j = 0; j < GUIDE_LOBES; j++) {
-        const GuideLobe l = guideLobe(m, j);
-        p += l.weight * l.norm * __expf(l.kappa * (dot(l.mu, w) - 1.0f));
+        const uint2 l = m->lobe[j];
+        p += m->coef[j] * __expf(bf16Hi(l.y) * (dot(lobeMu(l), w) - 1.0f));
     }
-    return p * m.alpha.y;
+    return p;
 }
 
 // direction from the mixture: lobe by u.x, then the vMF sample (Wenzel
 // Jakob, "Numerically stable sampling of the von Mises Fisher distribution on
 // S2", 2012) by u.y, u.z
-RMD_HD float3 guideSample(const GuideMixture &m, float3 u) {
-    const float target = u.x / m.alpha.y;  // the stored weights sum to 1 / alpha.y
+RMD_HD float3 guideSample(const GuideMixture *m, float3 u) {
+    const float target = u.x / m->invTotal;  // the stored weights sum to 1 / invTotal
+    const uint4 wq = m->weights;
     float acc = 0.0f;
     int k = GUIDE_LOBES - 1;
+    bool found = false;
+#pragma unroll
     for (int j = 0; j < GUIDE_LOBES; j++) {
-        acc += guideLobe(m, j).weight;
-        if (target < acc) {
+        const uint32_t w = j < 2 ? wq.x : j < 4 ? wq.y : j < 6 ? wq.z : wq.w;
+        acc += (j & 1) ? bf16Hi(w) : bf16Lo(w);
+        if (!found && target < acc) {
             k = j;
-            break;
+            found = true;
         }
     }
-    const GuideLobe l = guideLobe(m, k);
+    const uint2 l = m->lobe[k];
+    const float kappa = bf16Hi(l.y);
     const float uy = fmaxf(u.y, 1e-7f);
-    const float wz = 1.0f + logf(uy + (1.0f - uy) * __expf(-2.0f * l.kappa)) / l.kappa;
+    const float wz = 1.0f + logf(uy + (1.0f - uy) * __expf(-2.0f * kappa)) / kappa;
     const float r = sqrtf(fmaxf(0.0f, 1.0f - wz * wz));
     const float phi = 2.0f * M_PI_F * u.z;
-    return normalize(toWorld(buildOrthonormalBasis(l.mu), make_float3(r * cosf(phi), r * sinf(phi), wz)));
+    return normalize(toWorld(buildOrthonormalBasis(lobeMu(l)), make_float3(r * cosf(phi), r * sinf(phi), wz)));
 }
 
 // One training sample: a path vertex's features, a direction sampled there,

@@ -92,12 +92,8 @@ __device__ __forceinline__ bool shadePath(const ShadeParams &p, uint32_t i) {
         // the guide mixture of this point (one-sample MIS); the technique's pdf is
         // then alpha q + (1 - alpha) p_bsdf in every MIS weight that uses it.
         const bool guided = depth < fp.guideDepth;
-        GuideMixture gm;
-        float alpha = 0.0f;
-        if (guided) {
-            gm = pool.guide[i];
-            alpha = gm.alpha.x;
-        }
+        const GuideMixture *gm = &pool.guide[i];
+        const float alpha = guided ? gm->alpha : 0.0f;
         GuideFeatures gf;  // training: the guide's input features of this vertex
         const float meanThroughput = mean(rayWeight);
         if (training)

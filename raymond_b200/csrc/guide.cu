@@ -177,17 +177,22 @@ __device__ float3 lobeMean(float theta, float phi) {
 __device__ GuideMixture pack(const Decoded &d) {
     GuideMixture m;
     uint32_t w[4];
-    float total = 0.0f;
+    float total = 0.0f, kappa[GUIDE_LOBES];
     for (int j = 0; j < GUIDE_LOBES; j++) {
         const float3 mu = lobeMean(d.theta[j], d.phi[j]);
-        const float kappa = __expf(d.logKappa[j]);
+        const uint32_t kb = bf16Bits(__expf(d.logKappa[j]));
+        kappa[j] = bf16Lo(kb);
         total += bf16Lo(bf16Bits(d.lambda[j]));
-        m.lobe[j] = make_uint2(bf16Bits(mu.x) | (bf16Bits(mu.y) << 16), bf16Bits(mu.z) | (bf16Bits(kappa) << 16));
+        m.lobe[j] = make_uint2(bf16Bits(mu.x) | (bf16Bits(mu.y) << 16), bf16Bits(mu.z) | (kb << 16));
         if (j & 1) w[j >> 1] |= bf16Bits(d.lambda[j]) << 16;
         else w[j >> 1] = bf16Bits(d.lambda[j]);
     }
+    const float inv = 1.0f / total;
+    for (int j = 0; j < GUIDE_LOBES; j++) m.coef[j] = bf16Lo(bf16Bits(d.lambda[j])) * inv * vmfNorm(kappa[j]);
     m.weights = make_uint4(w[0], w[1], w[2], w[3]);
-    m.alpha = make_float4(d.alpha, 1.0f / total, 0.0f, 0.0f);
+    m.alpha = d.alpha;
+    m.invTotal = inv;
+    m.pad[0] = m.pad[1] = 0.0f;
     return m;
 }
 
@@ -611,13 +616,13 @@ __global__ void k_guide_mixture_test(const float *outputs, const float *u, int n
     if (i >= n && i >= m) return;
     const GuideMixture mix = pack(decode(outputs));
     if (i < n) {
-        const float3 d = guideSample(mix, make_float3(u[3 * i], u[3 * i + 1], u[3 * i + 2]));
+        const float3 d = guideSample(&mix, make_float3(u[3 * i], u[3 * i + 1], u[3 * i + 2]));
         dirsPdf[4 * i + 0] = d.x;
         dirsPdf[4 * i + 1] = d.y;
         dirsPdf[4 * i + 2] = d.z;
-        dirsPdf[4 * i + 3] = guidePdf(mix, d);
+        dirsPdf[4 * i + 3] = guidePdf(&mix, d);
     }
-    if (i < m) pdfs[i] = guidePdf(mix, make_float3(queries[3 * i], queries[3 * i + 1], queries[3 * i + 2]));
+    if (i < m) pdfs[i] = guidePdf(&mix, make_float3(queries[3 * i], queries[3 * i + 1], queries[3 * i + 2]));
 }
 
 }  // namespace

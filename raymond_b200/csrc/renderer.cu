@@ -784,7 +784,7 @@ rmd_status rmd_render(rmd_renderer *r, const rmd_render_settings *s) {
     const uint32_t batch = guide.settings.batch_size;
     uint64_t trainSteps = 0;
 
-    enum { STAGE_FILM, STAGE_TRACE, STAGE_GUIDE, STAGE_SHADE, STAGE_SHADOW, STAGES };
+    enum { STAGE_FILM, STAGE_TRACE, STAGE_GUIDE, STAGE_SHADE, STAGE_SHADOW, STAGE_TRAIN, STAGES };
     RMD_CUDA(cudaEventRecord(r->ev[0], st));
     RMD_CUDA(rmdLaunchFrameInit(pool, cnt, firstPath, firstPath + numPaths, st));
     // every path needs at most max_depth iterations after it is generated, and
@@ -835,7 +835,7 @@ rmd_status rmd_render(rmd_renderer *r, const rmd_render_settings *s) {
             RMD_CUDA(cudaMemsetAsync(&cnt->numSamples, 0, sizeof(uint32_t), st));
             guide.stats.samples += h.numSamples;
             guide.stats.records = h.numRecords;
-            RMD_CUDA(r->stageEvent(evi++, STAGE_GUIDE, st));
+            RMD_CUDA(r->stageEvent(evi++, STAGE_TRAIN, st));
         }
         if (h.pathsDone >= numPaths) done = true;
         else if (it > maxIters) return fail(RMD_ERROR_WATCHDOG, "render did not drain in the iteration bound");
@@ -866,7 +866,8 @@ rmd_status rmd_render(rmd_renderer *r, const rmd_render_settings *s) {
     r->stats.ms_trace = stage[STAGE_TRACE];
     r->stats.ms_shade = stage[STAGE_SHADE];
     r->stats.ms_shadow = stage[STAGE_SHADOW];
-    r->stats.ms_guide = stage[STAGE_GUIDE];
+    r->stats.ms_guide = stage[STAGE_GUIDE] + stage[STAGE_TRAIN];
+    r->stats.ms_guide_train = stage[STAGE_TRAIN];
     r->samples = std::max<uint64_t>(r->samples, firstSample + s->spp);
     return RMD_OK;
 }
