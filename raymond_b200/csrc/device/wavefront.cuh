@@ -116,6 +116,8 @@ struct PathPool {
     GuideRecord *records; // ring of the latest records with a nonzero target (Counters::numRecords)
     uint32_t recordCapacity;  // a power of two
     GuideMixture *guide;  // guiding: the mixture of each hit of this iteration (by position), or nullptr
+    uint4 *guideFeat;     // guiding: the guide's input features of each hit (by position; 7 x unorm16), or nullptr
+    float3 guideMin, guideInvExtent;  // frame of the position features
     uint32_t capacity;
 };
 
@@ -155,6 +157,9 @@ inline PathPool carvePathPool(void *base, uint32_t capacity) {
     pool.records = nullptr;
     pool.recordCapacity = 0;
     pool.guide = nullptr;
+    pool.guideFeat = nullptr;
+    pool.guideMin = make_float3(0.0f, 0.0f, 0.0f);
+    pool.guideInvExtent = make_float3(1.0f, 1.0f, 1.0f);
     pool.capacity = capacity;
     return pool;
 }

@@ -269,7 +269,7 @@ struct RecordBatch {
 // the k16 block made of two adjacent n8 tiles.  A warp runs 32 samples (two
 // m16 tiles) so every weight fragment, read from shared memory, feeds two
 // products, and all 32 lanes decode one sample each at the end.
-constexpr int kInferWarps = 4;
+constexpr int kInferWarps = 8;  // 8 warps share one copy of the weights; 2 blocks per SM (registers)
 constexpr int kLdW1 = GUIDE_INPUTS + 8, kLdW = GUIDE_HIDDEN + 8;  // padded weight rows (conflict-free fragments)
 constexpr int kLdOut = GUIDE_OUTPUTS + 1;                          // odd stride: conflict-free per-sample reads
 
@@ -408,10 +408,31 @@ __device__ void inferWarp(const InferSmem &sm, const GuideFeatures &f, float *ou
 }
 
 // ------------------------------------------------------------------ kernels
+// The guide's input features of this iteration's hits (shading order
+// 0..nHit-1): position on the ray, the triangle's geometric normal, the
+// reversed ray direction (as the shading kernel computes them), packed per
+// path position.  A light kernel of dependent gathers at full occupancy, so
+// the inference kernel reads one 16-byte record per hit.
+__global__ void __launch_bounds__(256) k_guide_features(Context ctx, PathPool pool, Counters *cnt, uint32_t p) {
+    const uint32_t nHit = cnt->nHit;
+    const PathState S = pool.s[p];
+    for (uint32_t q = blockIdx.x * blockDim.x + threadIdx.x; q < nHit; q += gridDim.x * blockDim.x) {
+        const uint32_t idx = pool.order[q];
+        const float4 o = __ldcs(&S.rayO[idx]), dd = __ldcs(&S.rayD[idx]), h = pool.hit[idx];
+        const PerInstanceData &inst = ctx.instances[pool.hitInst[idx]];
+        const uint4 face = ctx.faces[inst.faceOffset + __float_as_uint(h.w)];
+        const float3 Pc = xyz(ctx.vertices[inst.vertexOffset + face.z]);
+        const float3 P0 = xyz(ctx.vertices[inst.vertexOffset + face.x]) - Pc;
+        const float3 P1 = xyz(ctx.vertices[inst.vertexOffset + face.y]) - Pc;
+        const float3 n = normalize(mul3(inst.normalTransform, cross(P0, P1)));
+        pool.guideFeat[idx] =
+            packFeatures(guideFeatures(xyz(o) + xyz(dd) * h.x, n, -xyz(dd), pool.guideMin, pool.guideInvExtent));
+    }
+}
+
 // Guide mixtures of the shading points of this iteration's hits (shading
-// order 0..nHit-1) on paths shallower than guideDepth; the features follow
-// the shading kernel's: position on the ray, the triangle's geometric normal,
-// the reversed ray direction.
+// order 0..nHit-1) on paths shallower than guideDepth, from the features
+// k_guide_features stored for each hit.
 __global__ void __launch_bounds__(32 * kInferWarps) k_guide_infer(Context ctx, PathPool pool, Counters *cnt,
                                                                uint32_t p, uint32_t guideDepth, GuideNetView net,
                                                                GuideMixture *out) {
@@ -431,16 +452,7 @@ __global__ void __launch_bounds__(32 * kInferWarps) k_guide_infer(Context ctx, P
             idx = pool.order[q];
             valid = (__float_as_uint(S.L[idx].w) & 0xffffu) < guideDepth;  // the path's depth
         }
-        if (valid) {
-            const float4 o = S.rayO[idx], dd = S.rayD[idx], h = pool.hit[idx];
-            const PerInstanceData &inst = ctx.instances[pool.hitInst[idx]];
-            const uint4 face = ctx.faces[inst.faceOffset + __float_as_uint(h.w)];
-            const float3 Pc = xyz(ctx.vertices[inst.vertexOffset + face.z]);
-            const float3 P0 = xyz(ctx.vertices[inst.vertexOffset + face.x]) - Pc;
-            const float3 P1 = xyz(ctx.vertices[inst.vertexOffset + face.y]) - Pc;
-            const float3 n = normalize(mul3(inst.normalTransform, cross(P0, P1)));
-            f = guideFeatures(xyz(o) + xyz(dd) * h.x, n, -xyz(dd), net.sceneMin, net.sceneInvExtent);
-        }
+        if (valid) f = unpackFeatures(pool.guideFeat[idx]);  // written by the closest-hit kernel
         float *o = sm.out[warp];
         inferWarp(sm, f, o, lane);
         if (valid) out[idx] = pack(decode(&o[lane * kLdOut]));
@@ -648,6 +660,9 @@ cudaError_t rmdGuideConfigure() {
 cudaError_t rmdLaunchGuideInfer(const Context &ctx, const PathPool &pool, Counters *cnt, uint32_t cur,
                                 uint32_t guideDepth, const GuideNetView &net, GuideMixture *out, int blocks,
                                 cudaStream_t s) {
+    k_guide_features<<<pool.capacity / 256 < 1184u ? pool.capacity / 256 + 1 : 1184, 256, 0, s>>>(ctx, pool, cnt, cur);
+    cudaError_t e = cudaGetLastError();
+    if (e != cudaSuccess) return e;
     k_guide_infer<<<blocks, 32 * kInferWarps, rmdGuideSharedBytes(false), s>>>(ctx, pool, cnt, cur, guideDepth, net,
                                                                               out);
     return cudaGetLastError();

@@ -152,6 +152,7 @@ __global__ void __launch_bounds__(128) k_trace_closest(const WideNode *__restric
             const bool found = closestHit(s, tris, hit, inst);
             __stcs(&pool.hit[idx], hit);
             __stcs(&pool.hitInst[idx], inst);
+
             if (found) pool.order[warpAppend(&cnt->nHit)] = idx;
             else pool.order[pool.capacity - 1u - warpAppend(&cnt->nMiss)] = idx;
         });

@@ -138,7 +138,7 @@ struct rmd_renderer {
         rmd_guide_settings settings{};
         rmd_guide_stats stats{};
         rmdhost::GuideNet net;
-        DevBuf mixtures, rec, finRec, shRec, records;
+        DevBuf mixtures, features, rec, finRec, shRec, records;
         uint32_t pathCapacity = 0;    // paths the mixtures / pending-record buffers hold
         uint32_t recordCapacity = 0;  // nonzero-target records the replay ring holds
         bool initialised = false;
@@ -597,6 +597,7 @@ rmd_status rmd_scene_info(const rmd_scene *s, uint64_t *triangles, uint64_t *bvh
 }
 
 static rmd_status ensureGuideBuffers(rmd_renderer *r);
+static void guideFrame(const rmd_scene *s, float3 &lo, float3 &invExtent);
 
 static rmd_status allocatePool(rmd_renderer *r) {
     RMD_CUDA(r->pool.alloc(pathPoolBytes(r->capacity)));
@@ -616,7 +617,11 @@ static PathPool poolView(rmd_renderer *r) {
         pool.records = g.records.as<GuideRecord>();
         pool.recordCapacity = g.recordCapacity;
     }
-    if (g.settings.sampling && g.pathCapacity >= r->capacity) pool.guide = g.mixtures.as<GuideMixture>();
+    if (g.settings.sampling && g.pathCapacity >= r->capacity) {
+        pool.guide = g.mixtures.as<GuideMixture>();
+        pool.guideFeat = g.features.as<uint4>();
+        guideFrame(r->scene, pool.guideMin, pool.guideInvExtent);
+    }
     return pool;
 }
 
@@ -639,12 +644,15 @@ static rmd_status ensureGuideBuffers(rmd_renderer *r) {
     if (g.pathCapacity < r->capacity) {
         g.pathCapacity = 0;
         g.mixtures.release();
+        g.features.release();
         g.rec.release();
         g.finRec.release();
         g.shRec.release();
     }
-    if (g.settings.sampling && !g.mixtures.ptr)
+    if (g.settings.sampling && !g.mixtures.ptr) {
         RMD_CUDA(g.mixtures.alloc((size_t)r->capacity * sizeof(GuideMixture)));
+        RMD_CUDA(g.features.alloc((size_t)r->capacity * sizeof(uint4)));
+    }
     if (g.settings.training && !g.rec.ptr) {
         RMD_CUDA(g.rec.alloc((size_t)r->capacity * 2 * 4 * sizeof(float4)));
         RMD_CUDA(g.finRec.alloc((size_t)r->capacity * 4 * sizeof(float4)));
@@ -779,7 +787,7 @@ rmd_status rmd_render(rmd_renderer *r, const rmd_render_settings *s) {
     const PathPool pool = poolView(r);
     sp.pool = pool;
     sp.fp = fp;
-    const int guideBlocks = ctx->smCount * 3;  // resident blocks of the inference kernel (shared memory)
+    const int guideBlocks = ctx->smCount * 2;  // resident blocks of the inference kernel (registers)
     const int trainBlocks = ctx->smCount;
     const uint32_t batch = guide.settings.batch_size;
     uint64_t trainSteps = 0;
