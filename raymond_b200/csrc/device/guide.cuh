@@ -142,13 +142,13 @@ RMD_HD GuideFeatures guideFeatures(float3 position, float3 normal, float3 wo, fl
     return f;
 }
 
-// features in [0, 1] as 16-bit fixed point (the hit's record between the
-// closest-hit and inference kernels)
-RMD_HD uint4 packFeatures(const GuideFeatures &f) {
+// features in [0, 1] as 16-bit fixed point and the path's depth (the hit's
+// record between the feature and inference kernels)
+RMD_HD uint4 packFeatures(const GuideFeatures &f, uint32_t depth) {
     uint32_t q[8];
 #pragma unroll
     for (int k = 0; k < 7; k++) q[k] = (uint32_t)(fminf(1.0f, fmaxf(0.0f, f.v[k])) * 65535.0f + 0.5f);
-    q[7] = 0u;
+    q[7] = min(depth, 0xffffu);  // the path's depth
     return make_uint4(q[0] | (q[1] << 16), q[2] | (q[3] << 16), q[4] | (q[5] << 16), q[6] | (q[7] << 16));
 }
 RMD_HD GuideFeatures unpackFeatures(uint4 p) {

@@ -18,8 +18,9 @@ RMD_HD float computeMisWeight(float pdf, float other) {
 }
 
 // One path vertex: intersection.metal:43-208 for the active path at position
-// i of S[cur]; returns whether a surface was hit (a segment was shaded).
-__device__ __forceinline__ bool shadePath(const ShadeParams &p, uint32_t i) {
+// i of S[cur], the orderPos-th in shading order; returns whether a surface
+// was hit (a segment was shaded).
+__device__ __forceinline__ bool shadePath(const ShadeParams &p, uint32_t i, uint32_t orderPos) {
     const Context &ctx = p.ctx;
     const PathPool &pool = p.pool;
     const FrameParams &fp = p.fp;
@@ -92,7 +93,7 @@ __device__ __forceinline__ bool shadePath(const ShadeParams &p, uint32_t i) {
         // the guide mixture of this point (one-sample MIS); the technique's pdf is
         // then alpha q + (1 - alpha) p_bsdf in every MIS weight that uses it.
         const bool guided = depth < fp.guideDepth;
-        const GuideMixture *gm = &pool.guide[i];
+        const GuideMixture *gm = &pool.guide[orderPos];  // hits are shaded in order: mixture by that position
         const float alpha = guided ? gm->alpha : 0.0f;
         GuideFeatures gf;  // training: the guide's input features of this vertex
         const float meanThroughput = mean(rayWeight);
@@ -138,7 +139,16 @@ __device__ __forceinline__ bool shadePath(const ShadeParams &p, uint32_t i) {
         BsdfSample bs;
         float pdfBsdf = 0.0f;  // the BSDF's own pdf of the sampled direction
         float3 bsdfWeight;     // guided: f / pdfBsdf, the weight BSDF sampling gives the direction
-        if (guided && prng.sample() < alpha) {
+        // The technique is chosen with one uniform number per warp (each lane
+        // still draws its own): every path still takes the guide with its
+        // probability alpha, and lanes of similar alpha stay converged.
+        bool useGuide = false;
+        if (guided) {
+            const float own = prng.sample();
+            const unsigned mask = __activemask();
+            useGuide = __shfl_sync(mask, own, __ffs(mask) - 1) < alpha;
+        }
+        if (useGuide) {
             bs.wi = guideSample(gm, prng.sample3d());
             const float3 f = shading.material.evaluate(shading.wo, bs.wi, shNormal, shading.trueNormal, pdfBsdf);
             bs.pdf = alpha * guidePdf(gm, bs.wi) + (1.0f - alpha) * pdfBsdf;
@@ -244,7 +254,7 @@ extern "C" __global__ void __launch_bounds__(128, RMD_SHADE_MIN_BLOCKS) rmd_shad
     const unsigned n = rmd::activeCount(p.counters, p.cur);
     unsigned segments = 0, rays = 0;
     for (unsigned i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
-        segments += rmd::shadePath(p, rmd::shadingOrder(p.pool.order, p.counters, i)) ? 1u : 0u;
+        segments += rmd::shadePath(p, rmd::shadingOrder(p.pool.order, p.counters, i), i) ? 1u : 0u;
         rays++;
     }
     rmd::blockAdd64(&p.counters->segments, segments);

@@ -115,8 +115,8 @@ struct PathPool {
     float4 *shRec;        // per shadow ray: its vertex's features 0-3 | features 4-6, BSDF pdf of the ray
     GuideRecord *records; // ring of the latest records with a nonzero target (Counters::numRecords)
     uint32_t recordCapacity;  // a power of two
-    GuideMixture *guide;  // guiding: the mixture of each hit of this iteration (by position), or nullptr
-    uint4 *guideFeat;     // guiding: the guide's input features of each hit (by position; 7 x unorm16), or nullptr
+    GuideMixture *guide;  // guiding: the mixture of each hit of this iteration (by shading-order position), or nullptr
+    uint4 *guideFeat;     // guiding: each hit's input features (7 x unorm16) and depth, by shading-order position
     float3 guideMin, guideInvExtent;  // frame of the position features
     uint32_t capacity;
 };

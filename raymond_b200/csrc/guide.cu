@@ -410,52 +410,55 @@ __device__ void inferWarp(const InferSmem &sm, const GuideFeatures &f, float *ou
 // ------------------------------------------------------------------ kernels
 // The guide's input features of this iteration's hits (shading order
 // 0..nHit-1): position on the ray, the triangle's geometric normal, the
-// reversed ray direction (as the shading kernel computes them), packed per
-// path position.  A light kernel of dependent gathers at full occupancy, so
-// the inference kernel reads one 16-byte record per hit.
-__global__ void __launch_bounds__(256) k_guide_features(Context ctx, PathPool pool, Counters *cnt, uint32_t p) {
+// reversed ray direction (as the shading kernel computes them) and the
+// path's depth, stored by shading-order position.  A light kernel of
+// dependent gathers at full occupancy, so the inference kernel reads one
+// coalesced 16-byte record per hit.
+__global__ void __launch_bounds__(256) k_guide_features(Context ctx, PathPool pool, Counters *cnt, uint32_t p,
+                                                        uint32_t guideDepth) {
     const uint32_t nHit = cnt->nHit;
     const PathState S = pool.s[p];
     for (uint32_t q = blockIdx.x * blockDim.x + threadIdx.x; q < nHit; q += gridDim.x * blockDim.x) {
         const uint32_t idx = pool.order[q];
-        const float4 o = __ldcs(&S.rayO[idx]), dd = __ldcs(&S.rayD[idx]), h = pool.hit[idx];
-        const PerInstanceData &inst = ctx.instances[pool.hitInst[idx]];
-        const uint4 face = ctx.faces[inst.faceOffset + __float_as_uint(h.w)];
-        const float3 Pc = xyz(ctx.vertices[inst.vertexOffset + face.z]);
-        const float3 P0 = xyz(ctx.vertices[inst.vertexOffset + face.x]) - Pc;
-        const float3 P1 = xyz(ctx.vertices[inst.vertexOffset + face.y]) - Pc;
-        const float3 n = normalize(mul3(inst.normalTransform, cross(P0, P1)));
-        pool.guideFeat[idx] =
-            packFeatures(guideFeatures(xyz(o) + xyz(dd) * h.x, n, -xyz(dd), pool.guideMin, pool.guideInvExtent));
+        const uint32_t depth = __float_as_uint(S.L[idx].w) & 0xffffu;
+        GuideFeatures f = {};
+        if (depth < guideDepth) {  // only guided vertices need the features
+            const float4 o = __ldcs(&S.rayO[idx]), dd = __ldcs(&S.rayD[idx]), h = pool.hit[idx];
+            const PerInstanceData &inst = ctx.instances[pool.hitInst[idx]];
+            const uint4 face = ctx.faces[inst.faceOffset + __float_as_uint(h.w)];
+            const float3 Pc = xyz(ctx.vertices[inst.vertexOffset + face.z]);
+            const float3 P0 = xyz(ctx.vertices[inst.vertexOffset + face.x]) - Pc;
+            const float3 P1 = xyz(ctx.vertices[inst.vertexOffset + face.y]) - Pc;
+            const float3 n = normalize(mul3(inst.normalTransform, cross(P0, P1)));
+            f = guideFeatures(xyz(o) + xyz(dd) * h.x, n, -xyz(dd), pool.guideMin, pool.guideInvExtent);
+        }
+        pool.guideFeat[q] = packFeatures(f, depth);
     }
 }
 
-// Guide mixtures of the shading points of this iteration's hits (shading
-// order 0..nHit-1) on paths shallower than guideDepth, from the features
-// k_guide_features stored for each hit.
-__global__ void __launch_bounds__(32 * kInferWarps) k_guide_infer(Context ctx, PathPool pool, Counters *cnt,
-                                                               uint32_t p, uint32_t guideDepth, GuideNetView net,
+// Guide mixtures of the shading points of this iteration's hits on paths
+// shallower than guideDepth, by shading-order position (the shading kernel's
+// thread for hit q reads mixture q), from the features k_guide_features
+// stored.
+__global__ void __launch_bounds__(32 * kInferWarps) k_guide_infer(Counters *cnt, const uint4 *features,
+                                                               uint32_t guideDepth, GuideNetView net,
                                                                GuideMixture *out) {
     extern __shared__ __align__(16) unsigned char smem[];
     InferSmem &sm = *reinterpret_cast<InferSmem *>(smem);
     loadInferWeights(sm, net);
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
     const uint32_t nHit = cnt->nHit;
-    const PathState S = pool.s[p];
     const uint32_t tiles = (nHit + 31) / 32;
     for (uint32_t tile = blockIdx.x * kInferWarps + warp; tile < tiles; tile += gridDim.x * kInferWarps) {
         const uint32_t q = tile * 32 + lane;
-        bool valid = q < nHit;
-        GuideFeatures f = {};
-        uint32_t idx = 0;
-        if (valid) {
-            idx = pool.order[q];
-            valid = (__float_as_uint(S.L[idx].w) & 0xffffu) < guideDepth;  // the path's depth
-        }
-        if (valid) f = unpackFeatures(pool.guideFeat[idx]);  // written by the closest-hit kernel
+        uint4 packed = make_uint4(0u, 0u, 0u, 0xffff0000u);
+        if (q < nHit) packed = __ldcs(&features[q]);
+        const bool valid = q < nHit && (packed.w >> 16) < guideDepth;
+        if (!__any_sync(0xffffffffu, valid)) continue;  // no guided vertex in this tile
+        const GuideFeatures f = unpackFeatures(packed);
         float *o = sm.out[warp];
         inferWarp(sm, f, o, lane);
-        if (valid) out[idx] = pack(decode(&o[lane * kLdOut]));
+        if (valid) out[q] = pack(decode(&o[lane * kLdOut]));
         __syncwarp();
     }
 }
@@ -660,10 +663,11 @@ cudaError_t rmdGuideConfigure() {
 cudaError_t rmdLaunchGuideInfer(const Context &ctx, const PathPool &pool, Counters *cnt, uint32_t cur,
                                 uint32_t guideDepth, const GuideNetView &net, GuideMixture *out, int blocks,
                                 cudaStream_t s) {
-    k_guide_features<<<pool.capacity / 256 < 1184u ? pool.capacity / 256 + 1 : 1184, 256, 0, s>>>(ctx, pool, cnt, cur);
+    k_guide_features<<<pool.capacity / 256 < 1184u ? pool.capacity / 256 + 1 : 1184, 256, 0, s>>>(ctx, pool, cnt, cur,
+                                                                                              guideDepth);
     cudaError_t e = cudaGetLastError();
     if (e != cudaSuccess) return e;
-    k_guide_infer<<<blocks, 32 * kInferWarps, rmdGuideSharedBytes(false), s>>>(ctx, pool, cnt, cur, guideDepth, net,
+    k_guide_infer<<<blocks, 32 * kInferWarps, rmdGuideSharedBytes(false), s>>>(cnt, pool.guideFeat, guideDepth, net,
                                                                               out);
     return cudaGetLastError();
 }
