@@ -382,6 +382,39 @@ rmd_status rmd_renderer_guide_stats(const rmd_renderer *r, rmd_guide_stats *out)
 int32_t rmd_guide_param_count(void);
 rmd_status rmd_renderer_guide_params(rmd_renderer *r, float *params, int32_t write);
 
+/* ------------------------------------------------------------------ batches */
+/* Many scenes and views traced by one wavefront: the paths of every view share
+ * one pool and every stage is one launch over all of them (each path carries
+ * its view; traversal and shading use that view's scene), and the render is
+ * one CUDA-graph launch whose loop the device drives (a conditional while
+ * node).  Each view renders as it would alone (same camera ray, same PCG
+ * stream of its own pixel index).  The scenes' materials share one NVRTC
+ * module.  No counterpart in the reference (one scene, one view per frame,
+ * Renderer.swift:480-696). */
+typedef struct rmd_batch rmd_batch;
+
+typedef struct rmd_batch_view {
+    int32_t scene;            /* index into the batch's scene descriptions */
+    uint32_t width, height;
+    rmd_camera camera;
+} rmd_batch_view;
+
+#define RMD_BATCH_NO_GRAPH 1u /* flags: host-driven loop (counter checks) instead of the graph */
+
+rmd_status rmd_batch_create(rmd_context *ctx, const rmd_scene_desc *scenes, int32_t num_scenes,
+                            const rmd_batch_view *views, int32_t num_views, uint32_t pool_size, uint32_t flags,
+                            rmd_batch **out);
+void rmd_batch_destroy(rmd_batch *batch);
+rmd_status rmd_batch_reset(rmd_batch *batch);
+/* settings->spp samples of every view (sample indices below 2^24) */
+rmd_status rmd_batch_render(rmd_batch *batch, const rmd_render_settings *settings);
+rmd_status rmd_batch_film_read(rmd_batch *batch, int32_t view, float *rgb, int32_t normalize, uint32_t tonemapping,
+                               float exposure);
+rmd_status rmd_batch_film_read_f64(rmd_batch *batch, int32_t view, double *rgb);
+/* aggregate over the views (per-stage times are not taken inside the graph) */
+rmd_status rmd_batch_stats(const rmd_batch *batch, rmd_stats *out);
+rmd_status rmd_batch_autotune(rmd_batch *batch, const rmd_render_settings *settings, rmd_tune_result *out);
+
 /* ----------------------------------------------------- allocation-free render */
 /*
  * No counterpart in the reference.  For callers that cannot allocate GPU

@@ -90,6 +90,13 @@ class Camera(C.Structure):
                 ("focal_length", C.c_float), ("shift", C.c_float * 2)]
 
 
+class BatchView(C.Structure):
+    _fields_ = [("scene", C.c_int32), ("width", C.c_uint32), ("height", C.c_uint32), ("camera", Camera)]
+
+
+BATCH_NO_GRAPH = 1
+
+
 class SceneDescC(C.Structure):
     _fields_ = [("num_surface_materials", C.c_int32), ("surface_materials", C.POINTER(Material)),
                 ("num_light_materials", C.c_int32), ("light_materials", C.POINTER(Material)),

@@ -29,7 +29,8 @@ EXPORTS = [
     "rmd_renderer_reset", "rmd_renderer_set_camera", "rmd_render", "rmd_film_read", "rmd_film_read_f64",
     "rmd_film_samples", "rmd_renderer_stats", "rmd_render_noalloc", "rmd_renderer_autotune",
     "rmd_renderer_set_tuning", "rmd_renderer_set_guide", "rmd_renderer_guide_stats", "rmd_guide_param_count",
-    "rmd_renderer_guide_params",
+    "rmd_renderer_guide_params", "rmd_batch_create", "rmd_batch_destroy", "rmd_batch_reset", "rmd_batch_render",
+    "rmd_batch_film_read", "rmd_batch_film_read_f64", "rmd_batch_stats", "rmd_batch_autotune",
     "rmd_test_prng", "rmd_test_trace", "rmd_test_material_eval", "rmd_test_generate_source", "rmd_test_jit_compile",
     "rmd_test_guide_forward", "rmd_test_guide_gradient", "rmd_test_guide_mixture",
 ]
@@ -82,6 +83,15 @@ def lib() -> C.CDLL:
         "rmd_test_guide_gradient": ([P(C.c_float), P(C.c_float), C.c_int32, P(C.c_float), P(C.c_float)], C.c_int32),
         "rmd_test_guide_mixture": ([P(C.c_float), P(C.c_float), C.c_int32, P(C.c_float), P(C.c_float), C.c_int32,
                                     P(C.c_float)], C.c_int32),
+        "rmd_batch_create": ([vp, P(_abi.SceneDescC), C.c_int32, P(_abi.BatchView), C.c_int32, C.c_uint32, C.c_uint32,
+                              P(vp)], C.c_int32),
+        "rmd_batch_destroy": ([vp], None),
+        "rmd_batch_reset": ([vp], C.c_int32),
+        "rmd_batch_render": ([vp, P(RenderSettings)], C.c_int32),
+        "rmd_batch_film_read": ([vp, C.c_int32, P(C.c_float), C.c_int32, C.c_uint32, C.c_float], C.c_int32),
+        "rmd_batch_film_read_f64": ([vp, C.c_int32, P(C.c_double)], C.c_int32),
+        "rmd_batch_stats": ([vp, P(Stats)], C.c_int32),
+        "rmd_batch_autotune": ([vp, P(RenderSettings), P(_abi.TuneResult)], C.c_int32),
         "rmd_render_noalloc": ([vp, P(_abi.Camera), C.c_uint32, C.c_uint32, P(RenderSettings), C.c_void_p,
                                 C.c_uint32], C.c_int32),
         "rmd_test_prng": ([C.c_uint32, C.c_uint64, C.c_uint64, C.c_int32, P(C.c_float)], C.c_int32),
@@ -263,6 +273,74 @@ class Renderer:
     def close(self):
         if self.h.value:
             lib().rmd_renderer_destroy(self.h)
+            self.h = C.c_void_p()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+class Batch:
+    """Many scenes and views traced by one wavefront and one CUDA-graph
+    launch (rmd_batch): `views` is a list of dicts {scene: index into
+    `scenes`, width, height, camera (optional; the scene's camera)}."""
+
+    def __init__(self, ctx: Context, scenes: list, views: list[dict[str, Any]], pool_size: int = 0,
+                 graph: bool = True):
+        self.ctx = ctx
+        self.descs = [s if isinstance(s, SceneDesc) else SceneDesc(s) for s in scenes]
+        arr = (_abi.SceneDescC * len(self.descs))(*[d.c for d in self.descs])
+        self._arr = arr
+        vs = (_abi.BatchView * len(views))()
+        self.sizes = []
+        for i, v in enumerate(views):
+            known = 0 <= v["scene"] < len(self.descs)  # an unknown index is the library's to reject
+            cam = v.get("camera") or self.descs[v["scene"] if known else 0].scene["camera"]
+            vs[i] = _abi.BatchView(v["scene"], v["width"], v["height"], _abi.make_camera(cam))
+            self.sizes.append((v["height"], v["width"]))
+        self.h = C.c_void_p()
+        flags = 0 if graph else _abi.BATCH_NO_GRAPH
+        check(lib().rmd_batch_create(ctx.h, arr, len(self.descs), vs, len(views), pool_size, flags,
+                                     C.byref(self.h)))
+
+    def render(self, spp: int, max_depth: int = 8, sampling_mode: int = _abi.SAMPLING_MIS, rng: int = _abi.RNG_PCG32,
+               seed: int = 1, first_sample: int = -1, film_fp64: bool = False) -> None:
+        s = RenderSettings(spp, max_depth, sampling_mode, rng, seed, first_sample, int(film_fp64), 0)
+        check(lib().rmd_batch_render(self.h, C.byref(s)))
+
+    def film(self, view: int, normalize: bool = False, tonemapping: int = _abi.TONEMAP_LINEAR,
+             exposure: float = 1.0) -> np.ndarray:
+        h, w = self.sizes[view]
+        out = np.zeros((h, w, 3), np.float32)
+        check(lib().rmd_batch_film_read(self.h, view, _f32p(out), int(normalize), tonemapping, exposure))
+        return out
+
+    def film64(self, view: int) -> np.ndarray:
+        h, w = self.sizes[view]
+        out = np.zeros((h, w, 3), np.float64)
+        check(lib().rmd_batch_film_read_f64(self.h, view, out.ctypes.data_as(C.POINTER(C.c_double))))
+        return out
+
+    def reset(self) -> None:
+        check(lib().rmd_batch_reset(self.h))
+
+    def stats(self) -> dict[str, float]:
+        s = Stats()
+        check(lib().rmd_batch_stats(self.h, C.byref(s)))
+        return {k: getattr(s, k) for k, _ in Stats._fields_}
+
+    def autotune(self, spp: int = 32, max_depth: int = 10, sampling_mode: int = _abi.SAMPLING_MIS,
+                 rng: int = _abi.RNG_PCG32, seed: int = 1) -> dict[str, float]:
+        s = RenderSettings(spp, max_depth, sampling_mode, rng, seed, -1, 0, 0)
+        res = _abi.TuneResult()
+        check(lib().rmd_batch_autotune(self.h, C.byref(s), C.byref(res)))
+        return {k: getattr(res, k) for k, _ in _abi.TuneResult._fields_}
+
+    def close(self):
+        if self.h.value:
+            lib().rmd_batch_destroy(self.h)
             self.h = C.c_void_p()
 
     def __del__(self):

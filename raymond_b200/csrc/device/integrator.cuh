@@ -21,7 +21,6 @@ RMD_HD float computeMisWeight(float pdf, float other) {
 // i of S[cur], the orderPos-th in shading order; returns whether a surface
 // was hit (a segment was shaded).
 __device__ __forceinline__ bool shadePath(const ShadeParams &p, uint32_t i, uint32_t orderPos) {
-    const Context &ctx = p.ctx;
     const PathPool &pool = p.pool;
     const FrameParams &fp = p.fp;
     Counters *cnt = p.counters;
@@ -34,7 +33,19 @@ __device__ __forceinline__ bool shadePath(const ShadeParams &p, uint32_t i, uint
     const uint4 id = __ldcs(&S.id[i]);
     const uint32_t meta = __float_as_uint(L4.w);
     const uint32_t pixel = id.x;
+#ifdef RMD_BATCH
+    // a batch path: its view (top bits of the sample word) gives the scene
+    // context and the PCG stream of the view's own pixel index
+    const uint32_t view = id.y >> BATCH_SAMPLE_BITS;
+    const BatchView &bv = pool.views[view];
+    const Context &ctx = bv.ctx;
+    const uint32_t sample = id.y & BATCH_SAMPLE_MASK;
+    const uint32_t seqPixel = pixel - bv.pixelOffset, numPixels = bv.numPixels;
+#else
+    const Context &ctx = p.ctx;
     const uint32_t sample = id.y;
+    const uint32_t seqPixel = pixel, numPixels = fp.numPixels;
+#endif
     float3 L = xyz(L4);
     const float3 rayDir = xyz(d4);
     const float3 rayWeight = xyz(tp4);
@@ -42,7 +53,7 @@ __device__ __forceinline__ bool shadePath(const ShadeParams &p, uint32_t i, uint
     const uint32_t depth = meta & 0xffffu;
     const uint32_t rayFlags = (meta >> 16) & 0xffu;
     const bool lastDepth = depth + 1u >= fp.maxDepth;
-    PrngState prng = PrngState::unpack(fp.rngMode, make_uint2(id.z, id.w), pathSequence(sample, pixel, fp.numPixels));
+    PrngState prng = PrngState::unpack(fp.rngMode, make_uint2(id.z, id.w), pathSequence(sample, seqPixel, numPixels));
     uint32_t shadowIndex = 0xffffffffu;  // shadow ray whose target is set once the path's fate is known
     float3 shadowDir = f3(0.0f);
     float4 next[3];                      // rayO, rayD, tp of the continued path
@@ -119,7 +130,11 @@ __device__ __forceinline__ bool shadePath(const ShadeParams &p, uint32_t i, uint
                         __stcs(&pool.shO[k], f4(shading.position, nee.distance - SHADOW_EPS));
                         // training: the light sample is a training sample of this vertex too
                         const bool neeRecord = pool.shRec && meanThroughput > 0.0f && neeBsdfPdf > 0.0f;
+#ifdef RMD_BATCH
+                        __stcs(&pool.shW[k], f4(neeWeight, __uint_as_float(view)));  // the shadow ray's scene
+#else
                         __stcs(&pool.shW[k], f4(neeWeight, neeRecord ? 1.0f / meanThroughput : 0.0f));
+#endif
                         if (neeRecord) {
                             __stcs(&pool.shRec[2 * k], make_float4(gf.v[0], gf.v[1], gf.v[2], gf.v[3]));
                             __stcs(&pool.shRec[2 * k + 1], make_float4(gf.v[4], gf.v[5], gf.v[6], neeBsdfPdf));
@@ -214,7 +229,7 @@ __device__ __forceinline__ bool shadePath(const ShadeParams &p, uint32_t i, uint
             __stcs(&N.rayD[k], next[1]);
             __stcs(&N.tp[k], next[2]);
             __stcs(&N.L[k], f4(L, L4next));
-            __stcs(&N.id[k], make_uint4(pixel, sample, rs.x, rs.y));
+            __stcs(&N.id[k], make_uint4(pixel, id.y, rs.x, rs.y));
             if (training) {
                 if (!recorded && depth > 0u)
                     for (int r = 0; r < 4; r++) record[r] = __ldcs(&S.rec[4 * i + r]);

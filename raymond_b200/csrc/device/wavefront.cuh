@@ -23,6 +23,7 @@ constexpr float SHADOW_EPS = 0.001f;  // device/constants.hpp:3
 // error flags
 constexpr uint32_t ERR_QUEUE_OVERFLOW = 1u;
 constexpr uint32_t ERR_STACK_OVERFLOW = 2u;
+constexpr uint32_t ERR_LOOP_BOUND = 4u;  // a device-driven render loop reached its iteration bound
 
 // target of a shadow ray: position of its path in S[p ^ 1], or in the finish
 // list when this bit is set
@@ -61,6 +62,9 @@ struct Counters {
     uint32_t padR[62];
     uint32_t errors;
     uint32_t capacity;    // paths in flight at most (size of each S[p])
+    uint32_t loopIterations;  // device-driven render loop: wavefront iterations so far
+    uint32_t padL;
+    unsigned long long numPaths;    // paths of this render
     unsigned long long nextPath;    // next path id handed out by the film kernel
     unsigned long long endPath;     // one past the last path id of this render
     unsigned long long pathsDone;   // paths whose radiance reached the film
@@ -87,6 +91,19 @@ __device__ __forceinline__ uint32_t shadingOrder(const uint32_t *order, const Co
     const uint32_t nHit = c->nHit;
     return i < nHit ? order[i] : order[c->capacity - 1u - (i - nHit)];
 }
+
+// One view of a batch (many scenes and views traced by one wavefront): its
+// scene's device context with the view's camera, its scene's BVH, and its
+// place in the batch's film.  Paths of a batch carry the view in the top 8
+// bits of their sample index and their film pixel (batch-global) in id.x.
+struct BatchView {
+    Context ctx;
+    const void *nodes;   // the scene's wide BVH nodes (WideNode)
+    const float4 *tris;  // the scene's BVH triangles
+    uint32_t width, height, numPixels, pixelOffset;
+};
+constexpr uint32_t BATCH_SAMPLE_BITS = 24;
+constexpr uint32_t BATCH_SAMPLE_MASK = (1u << BATCH_SAMPLE_BITS) - 1u;
 
 // One queue-ordered copy of the path state (structure of arrays).
 struct PathState {
@@ -118,6 +135,8 @@ struct PathPool {
     GuideMixture *guide;  // guiding: the mixture of each hit of this iteration (by shading-order position), or nullptr
     uint4 *guideFeat;     // guiding: each hit's input features (7 x unorm16) and depth, by shading-order position
     float3 guideMin, guideInvExtent;  // frame of the position features
+    const BatchView *views;           // batch: the views (nullptr: one scene, one view)
+    uint32_t numViews;
     uint32_t capacity;
 };
 
@@ -160,6 +179,8 @@ inline PathPool carvePathPool(void *base, uint32_t capacity) {
     pool.guideFeat = nullptr;
     pool.guideMin = make_float3(0.0f, 0.0f, 0.0f);
     pool.guideInvExtent = make_float3(1.0f, 1.0f, 1.0f);
+    pool.views = nullptr;
+    pool.numViews = 0;
     pool.capacity = capacity;
     return pool;
 }
@@ -234,6 +255,17 @@ RMD_HD void blockLinearToPixel(uint32_t r, uint32_t W, uint32_t H, uint32_t &x, 
     const uint32_t ty = rr / awx, tx = rr - ty * awx;
     x = gx * 8 + tx;
     y = gy * 8 + ty;
+}
+
+// batch: the view whose pixel range holds batch pixel r (views sorted by pixelOffset)
+__device__ __forceinline__ uint32_t batchViewOf(const BatchView *views, uint32_t numViews, uint32_t r) {
+    uint32_t lo = 0, hi = numViews;  // views[lo].pixelOffset <= r < views[hi].pixelOffset
+    while (hi - lo > 1) {
+        const uint32_t mid = (lo + hi) >> 1;
+        if (views[mid].pixelOffset <= r) lo = mid;
+        else hi = mid;
+    }
+    return lo;
 }
 
 RMD_HD uint64_t pathSequence(uint32_t sample, uint32_t pixel, uint32_t numPixels) {

@@ -21,6 +21,8 @@ __global__ void k_frame_init(Counters *cnt, uint32_t capacity, uint64_t firstPat
     cnt->nHit = cnt->nMiss = 0;  // numRecords / numSamples persist across frames (the renderer resets them)
     cnt->nextPath = firstPath;
     cnt->endPath = endPath;
+    cnt->numPaths = endPath - firstPath;
+    cnt->loopIterations = 0;
     cnt->pathsDone = 0;
     cnt->segments = 0;
     cnt->shadowRays = 0;
@@ -32,7 +34,11 @@ __global__ void k_frame_init(Counters *cnt, uint32_t capacity, uint64_t firstPat
 // film (the film writes of intersection.metal:84-87,111-116,174-178 and
 // shadow.metal:24-27, gathered per path) and appends the next camera samples
 // (generate.metal:72-121) to S[p]: sample j takes path id nextPath + j and
-// position nQ[p] + j, so no counter is contended.
+// position nQ[p] + j, so no counter is contended.  BATCH: path ids run over
+// the concatenated pixels of all views (fp.numPixels in total); each sample
+// takes its view's camera, size and PCG stream (the view's own pixel index),
+// so a view renders as it would alone.
+template <bool BATCH>
 __global__ void __launch_bounds__(256) k_film_regen(Context ctx, PathPool pool, FrameParams fp, Counters *cnt,
                                                     uint32_t p) {
     if (blockIdx.x == 0 && threadIdx.x == 0) {  // counters of later stages of this iteration
@@ -88,18 +94,38 @@ __global__ void __launch_bounds__(256) k_film_regen(Context ctx, PathPool pool, 
             const unsigned long long id = first + j;
             const uint32_t sample = (uint32_t)(id / fp.numPixels);
             const uint32_t r = (uint32_t)(id - (unsigned long long)sample * fp.numPixels);
-            uint32_t x, y;
-            blockLinearToPixel(r, fp.width, fp.height, x, y);
+            uint32_t x, y, pixel, sampleWord;
             PrngState prng;
             float3 org, dir;
-            cameraRay(ctx, fp, x, y, sample, prng, org, dir);
+            float nearClip, farClip;
+            if constexpr (BATCH) {
+                const uint32_t view = batchViewOf(pool.views, pool.numViews, r);
+                const BatchView &bv = pool.views[view];
+                FrameParams vf = fp;  // the view's frame
+                vf.width = bv.width;
+                vf.height = bv.height;
+                vf.numPixels = bv.numPixels;
+                blockLinearToPixel(r - bv.pixelOffset, bv.width, bv.height, x, y);
+                cameraRay(bv.ctx, vf, x, y, sample, prng, org, dir);
+                nearClip = bv.ctx.nearClip;
+                farClip = bv.ctx.farClip;
+                pixel = bv.pixelOffset + y * bv.width + x;
+                sampleWord = (view << BATCH_SAMPLE_BITS) | sample;
+            } else {
+                blockLinearToPixel(r, fp.width, fp.height, x, y);
+                cameraRay(ctx, fp, x, y, sample, prng, org, dir);
+                nearClip = ctx.nearClip;
+                farClip = ctx.farClip;
+                pixel = y * fp.width + x;
+                sampleWord = sample;
+            }
             const uint32_t k = base + j;
             const uint2 rs = prng.pack();
-            __stcs(&S.rayO[k], f4(org, ctx.nearClip));
-            __stcs(&S.rayD[k], f4(dir, ctx.farClip));
+            __stcs(&S.rayO[k], f4(org, nearClip));
+            __stcs(&S.rayD[k], f4(dir, farClip));
             __stcs(&S.tp[k], make_float4(1.0f, 1.0f, 1.0f, inf_f()));
             __stcs(&S.L[k], make_float4(0.0f, 0.0f, 0.0f, __uint_as_float((uint32_t)RayFlagsCamera << 16)));
-            __stcs(&S.id[k], make_uint4(y * fp.width + x, sample, rs.x, rs.y));
+            __stcs(&S.id[k], make_uint4(pixel, sampleWord, rs.x, rs.y));
         }
     }
     blockAdd64(&cnt->pathsDone, finished);
@@ -113,10 +139,11 @@ __global__ void __launch_bounds__(256) k_film_regen(Context ctx, PathPool pool, 
 // Persistent warps (Aila & Laine 2009): a warp takes 32 consecutive queue
 // entries with one atomic and traces them to the end.  begin(idx, state,
 // stack) starts entry idx, finish(idx, state) consumes the finished query.
+// BATCH: begin() may point `nodes` / `tris` at the entry's own scene.
 template <bool ANY, class Begin, class Finish>
-__device__ __forceinline__ void persistentTrace(const WideNode *__restrict__ nodes, const float4 *__restrict__ tris,
-                                                uint32_t *work, uint32_t n, uint32_t *errors, Begin begin,
-                                                Finish finish) {
+__device__ __forceinline__ void persistentTrace(const WideNode *__restrict__ sceneNodes,
+                                                const float4 *__restrict__ sceneTris, uint32_t *work, uint32_t n,
+                                                uint32_t *errors, Begin begin, Finish finish) {
     TraversalState s;
     TraversalStack stack;
     const int lane = threadIdx.x & 31;
@@ -127,26 +154,34 @@ __device__ __forceinline__ void persistentTrace(const WideNode *__restrict__ nod
         if (base >= n) break;
         const uint32_t idx = base + lane;
         if (idx < n) {
-            begin(idx, s, stack);
+            const WideNode *nodes = sceneNodes;
+            const float4 *tris = sceneTris;
+            begin(idx, s, stack, nodes, tris);
             traverse<ANY>(s, stack, nodes, tris, errors);
-            finish(idx, s);
+            finish(idx, s, tris);
         }
     }
 }
 
-__global__ void __launch_bounds__(128) k_trace_closest(const WideNode *__restrict__ nodes,
-                                                       const float4 *__restrict__ tris, PathPool pool,
+template <bool BATCH>
+__global__ void __launch_bounds__(128) k_trace_closest(const WideNode *__restrict__ sceneNodes,
+                                                       const float4 *__restrict__ sceneTris, PathPool pool,
                                                        Counters *cnt, uint32_t p) {
     const uint32_t n = activeCount(cnt, p);
     const PathState S = pool.s[p];
     persistentTrace<false>(
-        nodes, tris, &cnt->traceWork, n, &cnt->errors,
-        [&](uint32_t idx, TraversalState &s, TraversalStack &) {
+        sceneNodes, sceneTris, &cnt->traceWork, n, &cnt->errors,
+        [&](uint32_t idx, TraversalState &s, TraversalStack &, const WideNode *&nodes, const float4 *&tris) {
+            if constexpr (BATCH) {
+                const BatchView &bv = pool.views[__ldg(&S.id[idx].y) >> BATCH_SAMPLE_BITS];
+                nodes = static_cast<const WideNode *>(bv.nodes);
+                tris = bv.tris;
+            }
             const float4 o = __ldcs(&S.rayO[idx]);
             const float4 d = __ldcs(&S.rayD[idx]);
             beginTraversal(s, nodes, xyz(o), xyz(d), o.w, d.w);
         },
-        [&](uint32_t idx, const TraversalState &s) {
+        [&](uint32_t idx, const TraversalState &s, const float4 *tris) {
             float4 hit;
             uint32_t inst;
             const bool found = closestHit(s, tris, hit, inst);
@@ -162,8 +197,10 @@ __global__ void __launch_bounds__(128) k_trace_closest(const WideNode *__restric
 // shadow ray adds its weight to its path's radiance, in S[p ^ 1] for a path
 // that continues and in the finish list for one that ended.  Thread 0 also
 // advances nextPath past the camera samples this iteration consumed.
-__global__ void __launch_bounds__(128) k_trace_shadow(const WideNode *__restrict__ nodes,
-                                                      const float4 *__restrict__ tris, PathPool pool,
+// BATCH: the ray's view is in the bits of shW.w.
+template <bool BATCH>
+__global__ void __launch_bounds__(128) k_trace_shadow(const WideNode *__restrict__ sceneNodes,
+                                                      const float4 *__restrict__ sceneTris, PathPool pool,
                                                       Counters *cnt, uint32_t p) {
     const uint32_t n = cnt->nShadow;
     if (blockIdx.x == 0 && threadIdx.x == 0) cnt->nextPath += newPaths(cnt, p);
@@ -171,15 +208,20 @@ __global__ void __launch_bounds__(128) k_trace_shadow(const WideNode *__restrict
     float4 *nextRec = pool.s[p ^ 1u].rec;
     uint32_t target = 0, traced = 0;
     persistentTrace<true>(
-        nodes, tris, &cnt->shadowWork, n, &cnt->errors,
-        [&](uint32_t idx, TraversalState &s, TraversalStack &) {
+        sceneNodes, sceneTris, &cnt->shadowWork, n, &cnt->errors,
+        [&](uint32_t idx, TraversalState &s, TraversalStack &, const WideNode *&nodes, const float4 *&tris) {
+            if constexpr (BATCH) {
+                const BatchView &bv = pool.views[__float_as_uint(__ldg(&pool.shW[idx].w))];
+                nodes = static_cast<const WideNode *>(bv.nodes);
+                tris = bv.tris;
+            }
             const float4 o = __ldcs(&pool.shO[idx]);
             const float4 d = __ldcs(&pool.shD[idx]);
             target = __float_as_uint(d.w);
             traced++;
             beginTraversal(s, nodes, xyz(o), xyz(d), SHADOW_EPS, o.w);
         },
-        [&](uint32_t idx, const TraversalState &s) {
+        [&](uint32_t idx, const TraversalState &s, const float4 *) {
             // all ones: the path overflowed its queue
             if (s.hitTri >= 0 || target == 0xffffffffu) return;
             const bool finished = (target & SHADOW_TO_FINISHED) != 0u;
@@ -199,7 +241,7 @@ __global__ void __launch_bounds__(128) k_trace_shadow(const WideNode *__restrict
                 r.z += w.z;
                 *rec = r;
             }
-            if (pool.shRec && w.w > 0.0f) {
+            if (!BATCH && pool.shRec && w.w > 0.0f) {
                 // a training record of the vertex's light sample: its direction,
                 // target (MIS-weighted contribution / throughput) and features
                 const float y = (w.x + w.y + w.z) * (1.0f / 3.0f) * w.w;
@@ -218,6 +260,20 @@ __global__ void __launch_bounds__(128) k_trace_shadow(const WideNode *__restrict
             }
         });
     blockAdd64(&cnt->shadowRays, traced);
+}
+
+// ------------------------------------------------------------- device-driven loop
+// Last node of the body of a CUDA-graph while loop of `itersPerBody`
+// wavefront iterations: continue while paths remain, no error was flagged
+// and the iteration bound (which every render reaches only on a fault) is
+// not passed.  The bound also guarantees that the loop ends.
+__global__ void k_loop_condition(Counters *cnt, cudaGraphConditionalHandle handle, uint32_t itersPerBody,
+                                 uint32_t maxIterations) {
+    const uint32_t it = cnt->loopIterations + itersPerBody;
+    cnt->loopIterations = it;
+    const bool more = cnt->pathsDone < cnt->numPaths && cnt->errors == 0u && it < maxIterations;
+    if (!more && cnt->pathsDone < cnt->numPaths && cnt->errors == 0u) atomicOr(&cnt->errors, ERR_LOOP_BOUND);
+    cudaGraphSetConditional(handle, more ? 1u : 0u);
 }
 
 // ------------------------------------------------------------- environment map
@@ -301,6 +357,12 @@ __global__ void k_debug_trace(const WideNode *nodes, const float4 *tris, const f
 // ------------------------------------------------------------- launch wrappers
 using namespace rmd;
 
+cudaError_t rmdLaunchLoopCondition(Counters *cnt, cudaGraphConditionalHandle handle, uint32_t itersPerBody,
+                                   uint32_t maxIterations, cudaStream_t s) {
+    k_loop_condition<<<1, 1, 0, s>>>(cnt, handle, itersPerBody, maxIterations);
+    return cudaGetLastError();
+}
+
 cudaError_t rmdLaunchFrameInit(const PathPool &pool, Counters *cnt, uint64_t firstPath, uint64_t endPath,
                                cudaStream_t s) {
     k_frame_init<<<1, 1, 0, s>>>(cnt, pool.capacity, firstPath, endPath);
@@ -308,17 +370,20 @@ cudaError_t rmdLaunchFrameInit(const PathPool &pool, Counters *cnt, uint64_t fir
 }
 cudaError_t rmdLaunchFilmRegen(const Context &ctx, const PathPool &pool, const FrameParams &fp, Counters *cnt,
                                uint32_t cur, int blocks, cudaStream_t s) {
-    k_film_regen<<<blocks, 256, 0, s>>>(ctx, pool, fp, cnt, cur);
+    if (pool.views) k_film_regen<true><<<blocks, 256, 0, s>>>(ctx, pool, fp, cnt, cur);
+    else k_film_regen<false><<<blocks, 256, 0, s>>>(ctx, pool, fp, cnt, cur);
     return cudaGetLastError();
 }
 cudaError_t rmdLaunchTraceClosest(const WideNode *nodes, const float4 *tris, const PathPool &pool, Counters *cnt,
                                   uint32_t cur, int blocks, cudaStream_t s) {
-    k_trace_closest<<<blocks, 128, 0, s>>>(nodes, tris, pool, cnt, cur);
+    if (pool.views) k_trace_closest<true><<<blocks, 128, 0, s>>>(nodes, tris, pool, cnt, cur);
+    else k_trace_closest<false><<<blocks, 128, 0, s>>>(nodes, tris, pool, cnt, cur);
     return cudaGetLastError();
 }
 cudaError_t rmdLaunchTraceShadow(const WideNode *nodes, const float4 *tris, const PathPool &pool, Counters *cnt,
                                  uint32_t cur, int blocks, cudaStream_t s) {
-    k_trace_shadow<<<blocks, 128, 0, s>>>(nodes, tris, pool, cnt, cur);
+    if (pool.views) k_trace_shadow<true><<<blocks, 128, 0, s>>>(nodes, tris, pool, cnt, cur);
+    else k_trace_shadow<false><<<blocks, 128, 0, s>>>(nodes, tris, pool, cnt, cur);
     return cudaGetLastError();
 }
 cudaError_t rmdLaunchEnvmapReduce(float *mip, int cur, cudaStream_t s) {

@@ -6,6 +6,9 @@
 #include "device/traverse.cuh"
 #include "device/wavefront.cuh"
 
+// device-driven render loop: condition node of a CUDA-graph while loop
+cudaError_t rmdLaunchLoopCondition(rmd::Counters *cnt, cudaGraphConditionalHandle handle, uint32_t itersPerBody,
+                                   uint32_t maxIterations, cudaStream_t s);
 cudaError_t rmdLaunchFrameInit(const rmd::PathPool &pool, rmd::Counters *cnt, uint64_t firstPath, uint64_t endPath,
                                cudaStream_t s);
 cudaError_t rmdLaunchFilmRegen(const rmd::Context &ctx, const rmd::PathPool &pool, const rmd::FrameParams &fp,

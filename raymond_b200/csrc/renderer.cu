@@ -110,9 +110,10 @@ struct rmd_scene {
     int numSurface = 0, numLight = 0;
     int shadeBlocks = 0, traceBlocks = 0, regenBlocks = 0;
     int defaultMinBlocks = 1;
+    bool ownsModule = true;  // false for the scenes of a batch (the batch owns the shared module)
     ~rmd_scene() {
         for (auto &kv : variants) rmdhost::unloadModule(*kv.second);
-        rmdhost::unloadModule(jit);
+        if (ownsModule) rmdhost::unloadModule(jit);
     }
 };
 
@@ -160,6 +161,43 @@ struct rmd_renderer {
         }
         stageOf[i] = stage;
         return cudaEventRecord(stageEvents[i], st);
+    }
+};
+
+// Many scenes and views traced by one wavefront (one pool, one launch per
+// stage), the whole render one CUDA-graph launch whose while loop the device
+// drives.
+struct rmd_batch {
+    rmd_context *ctx = nullptr;
+    std::vector<std::unique_ptr<rmd_scene>> scenes;
+    rmdhost::JitModule jit;  // the merged material module of all scenes (batch shading kernel)
+    std::string moduleSource;
+    std::map<int, std::unique_ptr<rmdhost::JitModule>> variants;  // shading kernels by minimum blocks per SM
+    std::vector<rmd_batch_view> views;
+    std::vector<uint32_t> offsets;  // film pixel offset of each view
+    uint32_t totalPixels = 0;
+    DevBuf viewTable, pool, counters, film, film64, resolve;
+    Counters *hostCounters = nullptr;
+    uint32_t capacity = 0;
+    cudaKernel_t shade = nullptr;
+    int shadeBlocks = 0, shadeMinBlocks = 1, defaultMinBlocks = 1, traceBlocksPerSm = 12;
+    bool useGraph = true;
+    uint64_t samples = 0;
+    rmd_stats stats{};
+    cudaEvent_t ev[2] = {};
+    // the instantiated render graph and the settings it was captured for
+    cudaGraph_t graph = nullptr;
+    cudaGraphExec_t graphExec = nullptr;
+    std::vector<uint64_t> graphKey;
+    ~rmd_batch() {
+        if (graphExec) cudaGraphExecDestroy(graphExec);
+        if (graph) cudaGraphDestroy(graph);
+        if (hostCounters) cudaFreeHost(hostCounters);
+        for (auto &e : ev)
+            if (e) cudaEventDestroy(e);
+        scenes.clear();  // before the module their envmaps were built with goes
+        for (auto &kv : variants) rmdhost::unloadModule(*kv.second);
+        rmdhost::unloadModule(jit);
     }
 };
 
@@ -306,27 +344,24 @@ void rmd_context_destroy(rmd_context *c) {
     delete c;
 }
 
-rmd_status rmd_scene_create(rmd_context *ctx, const rmd_scene_desc *d, rmd_scene **out) {
-    if (!ctx || !d || !out) return fail(RMD_ERROR_INVALID_ARGUMENT, "NULL argument");
+static rmd_status validateSceneDesc(const rmd_scene_desc *d) {
     if (d->num_surface_materials < 0 || d->num_light_materials <= 0 || d->num_shapes < 0 || d->num_entities < 0)
         return fail(RMD_ERROR_INVALID_ARGUMENT, "invalid counts (at least the world material is required)");
     if (d->world_shader >= d->num_light_materials) return fail(RMD_ERROR_INVALID_ARGUMENT, "world_shader out of range");
     if (d->envmap_exponent < 0 || d->envmap_exponent > 12)
         return fail(RMD_ERROR_INVALID_ARGUMENT, "envmap_exponent out of range (0..12)");
-    RMD_CUDA(cudaSetDevice(ctx->device));
-    auto s = std::make_unique<rmd_scene>();
-    s->ctx = ctx;
-    cudaStream_t st = ctx->stream;
+    return RMD_OK;
+}
 
-    // MaterialBuilder.build: generate and JIT-compile the material module
-    rmdhost::GeneratedModule mod;
-    try {
-        const bool hoist = std::getenv("RMD_NO_HOIST") == nullptr;
-        mod = rmdhost::generateModule(d->surface_materials, d->num_surface_materials, d->light_materials,
-                                      d->num_light_materials, hoist);
-    } catch (const rmdhost::CodegenError &e) {
-        return fail(e.status, e.message);
-    }
+// Everything of a scene but its material module: geometry, BVH, lights,
+// material tables and the device Context.  `mod` is the generated module
+// that holds this scene's materials from index surfaceBase / lightBase on
+// (0 for a scene of its own; the scene's slice of a module shared by the
+// scenes of a batch).
+static rmd_status buildSceneData(rmd_context *ctx, const rmd_scene_desc *d, rmd_scene *s,
+                                 const rmdhost::GeneratedModule &mod, int surfaceBase, int lightBase) {
+    cudaStream_t st = ctx->stream;
+    s->ctx = ctx;
     s->numSurface = d->num_surface_materials;
     s->numLight = d->num_light_materials;
 
@@ -377,7 +412,7 @@ rmd_status rmd_scene_create(rmd_context *ctx, const rmd_scene_desc *d, rmd_scene
                 return fail(RMD_ERROR_INVALID_ARGUMENT, "face material out of range in shape " + std::to_string(si));
             faces.push_back(make_uint4(ix[0], ix[1], ix[2], m));
             idxPacked.insert(idxPacked.end(), ix, ix + 3);
-            if (mod.surfaceEmissive[m]) info.hasEmission = true;
+            if (mod.surfaceEmissive[surfaceBase + m]) info.hasEmission = true;
         }
         shapes.push_back(info);
     }
@@ -521,9 +556,11 @@ rmd_status rmd_scene_create(rmd_context *ctx, const rmd_scene_desc *d, rmd_scene
 
     // material tables
     std::vector<uint2> stab, ltab;
-    for (size_t i = 0; i < mod.surface.group.size(); i++) stab.push_back(make_uint2(mod.surface.group[i], mod.surface.offset[i]));
-    for (size_t i = 0; i < mod.light.group.size(); i++) ltab.push_back(make_uint2(mod.light.group[i], mod.light.offset[i]));
-    if (mod.params.empty()) mod.params.push_back(0.0f);
+    for (int i = surfaceBase; i < surfaceBase + d->num_surface_materials; i++)
+        stab.push_back(make_uint2(mod.surface.group[i], mod.surface.offset[i]));
+    for (int i = lightBase; i < lightBase + d->num_light_materials; i++)
+        ltab.push_back(make_uint2(mod.light.group[i], mod.light.offset[i]));
+    const std::vector<float> params = mod.params.empty() ? std::vector<float>{0.0f} : mod.params;
     if (stab.empty()) stab.push_back(make_uint2(0, 0));
 
     // uploads
@@ -540,7 +577,7 @@ rmd_status rmd_scene_create(rmd_context *ctx, const rmd_scene_desc *d, rmd_scene
     RMD_CUDA(s->shapeLights.upload(shapeLights.data(), shapeLights.size() * sizeof(ShapeLight), st));
     RMD_CUDA(s->surfaceTable.upload(stab.data(), stab.size() * sizeof(uint2), st));
     RMD_CUDA(s->lightTable.upload(ltab.data(), ltab.size() * sizeof(uint2), st));
-    RMD_CUDA(s->materialParams.upload(mod.params.data(), mod.params.size() * sizeof(float), st));
+    RMD_CUDA(s->materialParams.upload(params.data(), params.size() * sizeof(float), st));
     RMD_CUDA(s->bvhNodes.upload(bvh.nodes.data(), bvh.nodes.size() * sizeof(rmdhost::GpuWideNode), st));
     RMD_CUDA(s->bvhTris.upload(bvh.tris.data(), bvh.tris.size() * sizeof(float), st));
 
@@ -575,12 +612,30 @@ rmd_status rmd_scene_create(rmd_context *ctx, const rmd_scene_desc *d, rmd_scene
     c.shift = make_float2(d->camera.shift[0], d->camera.shift[1]);
 
     s->defaultMinBlocks = defaultShadeMinBlocks();
+    return RMD_OK;
+}
+
+rmd_status rmd_scene_create(rmd_context *ctx, const rmd_scene_desc *d, rmd_scene **out) {
+    if (!ctx || !d || !out) return fail(RMD_ERROR_INVALID_ARGUMENT, "NULL argument");
+    rmd_status r = validateSceneDesc(d);
+    if (r != RMD_OK) return r;
+    RMD_CUDA(cudaSetDevice(ctx->device));
+    auto s = std::make_unique<rmd_scene>();
+    // MaterialBuilder.build: generate and JIT-compile the material module
+    rmdhost::GeneratedModule mod;
+    try {
+        const bool hoist = std::getenv("RMD_NO_HOIST") == nullptr;
+        mod = rmdhost::generateModule(d->surface_materials, d->num_surface_materials, d->light_materials,
+                                      d->num_light_materials, hoist);
+    } catch (const rmdhost::CodegenError &e) {
+        return fail(e.status, e.message);
+    }
+    if ((r = buildSceneData(ctx, d, s.get(), mod, 0, 0)) != RMD_OK) return r;
     const std::string err = rmdhost::compileModule(
         mod.source, s->jit, {"-DRMD_SHADE_MIN_BLOCKS=" + std::to_string(s->defaultMinBlocks)});
     if (!err.empty()) return fail(RMD_ERROR_NVRTC, err);
     s->moduleSource = mod.source;
-    rmd_status r = buildEnvironmentMap(s.get(), d->envmap_exponent);
-    if (r != RMD_OK) return r;
+    if ((r = buildEnvironmentMap(s.get(), d->envmap_exponent)) != RMD_OK) return r;
     s->shadeBlocks = occupancyBlocks((const void *)s->jit.shade, 128, ctx->smCount);
     *out = s.release();
     return RMD_OK;
@@ -1207,6 +1262,409 @@ rmd_status rmd_test_jit_compile(const rmd_scene_desc *d, int32_t hoist, char *lo
         log[n] = 0;
     }
     return RMD_OK;
+}
+
+// --------------------------------------------------------------------- batches
+static rmd_status batchAllocatePool(rmd_batch *b) {
+    if (b->graphExec) {
+        cudaGraphExecDestroy(b->graphExec);
+        b->graphExec = nullptr;
+    }
+    if (b->graph) {
+        cudaGraphDestroy(b->graph);
+        b->graph = nullptr;
+    }
+    b->graphKey.clear();
+    RMD_CUDA(b->pool.alloc(pathPoolBytes(b->capacity)));
+    RMD_CUDA(b->counters.alloc(sizeof(Counters)));
+    RMD_CUDA(cudaMemset(b->counters.ptr, 0, sizeof(Counters)));
+    return RMD_OK;
+}
+
+static PathPool batchPoolView(const rmd_batch *b) {
+    PathPool pool = carvePathPool(b->pool.ptr, b->capacity);
+    pool.views = b->viewTable.as<BatchView>();
+    pool.numViews = (uint32_t)b->views.size();
+    return pool;
+}
+
+static void batchSelectShade(rmd_batch *b, int mb) {
+    cudaKernel_t k = mb == b->defaultMinBlocks ? b->jit.shade : b->variants.at(mb)->shade;
+    b->shade = k;
+    b->shadeMinBlocks = mb;
+    b->shadeBlocks = occupancyBlocks((const void *)k, 128, b->ctx->smCount);
+    if (b->graphExec) {
+        cudaGraphExecDestroy(b->graphExec);
+        b->graphExec = nullptr;
+    }
+    b->graphKey.clear();
+}
+
+static rmd_status batchEnsureVariants(rmd_batch *b, const std::vector<int> &minBlocks) {
+    for (int mb : minBlocks) {
+        if (mb == b->defaultMinBlocks || b->variants.count(mb)) continue;
+        auto m = std::make_unique<rmdhost::JitModule>();
+        const std::string err =
+            rmdhost::compileModule(b->moduleSource, *m, {"-DRMD_SHADE_MIN_BLOCKS=" + std::to_string(mb), "-DRMD_BATCH"});
+        if (!err.empty()) return fail(RMD_ERROR_NVRTC, err);
+        b->variants[mb] = std::move(m);
+    }
+    return RMD_OK;
+}
+
+rmd_status rmd_batch_create(rmd_context *ctx, const rmd_scene_desc *descs, int32_t numScenes,
+                            const rmd_batch_view *views, int32_t numViews, uint32_t poolSize, uint32_t flags,
+                            rmd_batch **out) {
+    if (!ctx || !descs || !views || !out || numScenes <= 0 || numViews <= 0)
+        return fail(RMD_ERROR_INVALID_ARGUMENT, "NULL argument or empty batch");
+    if (numViews > 256) return fail(RMD_ERROR_INVALID_ARGUMENT, "at most 256 views per batch");
+    if (flags & ~RMD_BATCH_NO_GRAPH) return fail(RMD_ERROR_INVALID_ARGUMENT, "unknown batch flags");
+    uint64_t total = 0;
+    for (int v = 0; v < numViews; v++) {
+        const rmd_batch_view &bv = views[v];
+        if (bv.scene < 0 || bv.scene >= numScenes || bv.width == 0 || bv.height == 0 || bv.width > 65535 ||
+            bv.height > 65535)
+            return fail(RMD_ERROR_INVALID_ARGUMENT, "invalid batch view " + std::to_string(v));
+        total += (uint64_t)bv.width * bv.height;
+    }
+    if (total > 0x7fffffffull) return fail(RMD_ERROR_INVALID_ARGUMENT, "batch films exceed 2^31 pixels");
+    for (int i = 0; i < numScenes; i++) {
+        rmd_status r = validateSceneDesc(&descs[i]);
+        if (r != RMD_OK) return fail(r, "scene " + std::to_string(i) + ": " + g_lastError);
+    }
+    RMD_CUDA(cudaSetDevice(ctx->device));
+    auto b = std::make_unique<rmd_batch>();
+    b->ctx = ctx;
+    b->useGraph = !(flags & RMD_BATCH_NO_GRAPH);
+    // one material module for all scenes: their materials concatenated
+    std::vector<rmd_material> surf, light;
+    std::vector<int> surfBase, lightBase;
+    for (int i = 0; i < numScenes; i++) {
+        surfBase.push_back((int)surf.size());
+        lightBase.push_back((int)light.size());
+        surf.insert(surf.end(), descs[i].surface_materials, descs[i].surface_materials + descs[i].num_surface_materials);
+        light.insert(light.end(), descs[i].light_materials, descs[i].light_materials + descs[i].num_light_materials);
+    }
+    rmdhost::GeneratedModule mod;
+    try {
+        mod = rmdhost::generateModule(surf.data(), (int)surf.size(), light.data(), (int)light.size(), true);
+    } catch (const rmdhost::CodegenError &e) {
+        return fail(e.status, e.message);
+    }
+    b->defaultMinBlocks = defaultShadeMinBlocks();
+    const std::string err = rmdhost::compileModule(
+        mod.source, b->jit, {"-DRMD_SHADE_MIN_BLOCKS=" + std::to_string(b->defaultMinBlocks), "-DRMD_BATCH"});
+    if (!err.empty()) return fail(RMD_ERROR_NVRTC, err);
+    b->moduleSource = mod.source;
+    for (int i = 0; i < numScenes; i++) {
+        auto sc = std::make_unique<rmd_scene>();
+        rmd_status r = buildSceneData(ctx, &descs[i], sc.get(), mod, surfBase[i], lightBase[i]);
+        if (r != RMD_OK) return r;
+        sc->jit = b->jit;  // the batch's module builds the scene's environment map
+        sc->ownsModule = false;
+        if ((r = buildEnvironmentMap(sc.get(), descs[i].envmap_exponent)) != RMD_OK) return r;
+        b->scenes.push_back(std::move(sc));
+    }
+    // views: their scene's context with the view's camera, in film order
+    std::vector<BatchView> table(numViews);
+    uint32_t offset = 0;
+    for (int v = 0; v < numViews; v++) {
+        const rmd_batch_view &bv = views[v];
+        const rmd_scene *sc = b->scenes[bv.scene].get();
+        BatchView &t = table[v];
+        t.ctx = sc->dctx;
+        for (int k = 0; k < 4; k++)
+            t.ctx.cameraTransform[k] = make_float4(bv.camera.transform[4 * k], bv.camera.transform[4 * k + 1],
+                                                   bv.camera.transform[4 * k + 2], bv.camera.transform[4 * k + 3]);
+        t.ctx.nearClip = bv.camera.near_clip;
+        t.ctx.farClip = bv.camera.far_clip;
+        t.ctx.focalLength = bv.camera.focal_length;
+        t.ctx.shift = make_float2(bv.camera.shift[0], bv.camera.shift[1]);
+        t.nodes = sc->bvhNodes.ptr;
+        t.tris = sc->bvhTris.as<float4>();
+        t.width = bv.width;
+        t.height = bv.height;
+        t.numPixels = bv.width * bv.height;
+        t.pixelOffset = offset;
+        b->views.push_back(bv);
+        b->offsets.push_back(offset);
+        offset += t.numPixels;
+    }
+    b->totalPixels = offset;
+    RMD_CUDA(b->viewTable.upload(table.data(), table.size() * sizeof(BatchView), ctx->stream));
+    RMD_CUDA(b->film.alloc((size_t)offset * sizeof(float4)));
+    RMD_CUDA(cudaMemset(b->film.ptr, 0, b->film.bytes));
+    RMD_CUDA(b->resolve.alloc((size_t)offset * 3 * sizeof(float)));
+    b->capacity = poolSize ? poolSize : (1u << 21);
+    rmd_status r = batchAllocatePool(b.get());
+    if (r != RMD_OK) return r;
+    RMD_CUDA(cudaMallocHost((void **)&b->hostCounters, sizeof(Counters)));
+    for (auto &e : b->ev) RMD_CUDA(cudaEventCreate(&e));
+    batchSelectShade(b.get(), b->defaultMinBlocks);
+    *out = b.release();
+    return RMD_OK;
+}
+
+void rmd_batch_destroy(rmd_batch *b) { delete b; }
+
+rmd_status rmd_batch_reset(rmd_batch *b) {
+    if (!b) return fail(RMD_ERROR_INVALID_ARGUMENT, "NULL batch");
+    cudaStream_t st = b->ctx->stream;
+    RMD_CUDA(cudaMemsetAsync(b->film.ptr, 0, b->film.bytes, st));
+    if (b->film64.ptr) RMD_CUDA(cudaMemsetAsync(b->film64.ptr, 0, b->film64.bytes, st));
+    RMD_CUDA(cudaStreamSynchronize(st));
+    b->samples = 0;
+    return RMD_OK;
+}
+
+// Records the render's wavefront loop on `st`: host-driven (counter checks
+// every 4 iterations) or, with `handle`, as the body of a graph while loop
+// (2 iterations and the condition kernel).
+static rmd_status batchEnqueueIterations(rmd_batch *b, const PathPool &pool, const FrameParams &fp, ShadeParams &sp,
+                                         int iterations, cudaStream_t st) {
+    Counters *cnt = b->counters.as<Counters>();
+    const int tb = b->ctx->smCount * b->traceBlocksPerSm;
+    const int rb = std::min<int>((b->capacity + 255) / 256, b->ctx->smCount * 8);
+    void *shadeArgs[] = {&sp};
+    for (int k = 0; k < iterations; k++) {
+        const uint32_t cur = (uint32_t)k & 1u;
+        RMD_CUDA(rmdLaunchFilmRegen(b->scenes[0]->dctx, pool, fp, cnt, cur, rb, st));
+        RMD_CUDA(rmdLaunchTraceClosest(nullptr, nullptr, pool, cnt, cur, tb, st));
+        sp.cur = cur;
+        RMD_CUDA(cudaLaunchKernel((const void *)b->shade, dim3(b->shadeBlocks), dim3(128), shadeArgs, 0, st));
+        RMD_CUDA(rmdLaunchTraceShadow(nullptr, nullptr, pool, cnt, cur, tb, st));
+    }
+    return RMD_OK;
+}
+
+rmd_status rmd_batch_render(rmd_batch *b, const rmd_render_settings *s) {
+    if (!b || !s) return fail(RMD_ERROR_INVALID_ARGUMENT, "NULL argument");
+    if (s->max_depth == 0 || s->max_depth > 65535 || s->sampling_mode > 2 || s->rng > 1)
+        return fail(RMD_ERROR_INVALID_ARGUMENT, "invalid render settings");
+    rmd_context *ctx = b->ctx;
+    RMD_CUDA(cudaSetDevice(ctx->device));
+    cudaStream_t st = ctx->stream;
+    const uint64_t firstSample = s->first_sample >= 0 ? (uint64_t)s->first_sample : b->samples;
+    if (firstSample + s->spp > BATCH_SAMPLE_MASK)
+        return fail(RMD_ERROR_INVALID_ARGUMENT, "batch sample index beyond 2^24");
+    const uint64_t numPaths = (uint64_t)s->spp * b->totalPixels;
+    if (s->film_fp64 && !b->film64.ptr) {
+        RMD_CUDA(b->film64.alloc((size_t)b->totalPixels * 3 * sizeof(double)));
+        RMD_CUDA(cudaMemsetAsync(b->film64.ptr, 0, b->film64.bytes, st));
+    }
+    std::memset(&b->stats, 0, sizeof(b->stats));
+    b->stats.pool_size = b->capacity;
+    if (numPaths == 0) return RMD_OK;
+    FrameParams fp{};
+    fp.width = 0;  // per view (BatchView)
+    fp.height = 0;
+    fp.numPixels = b->totalPixels;
+    fp.maxDepth = s->max_depth;
+    fp.samplingMode = s->sampling_mode;
+    fp.rngMode = s->rng;
+    fp.seed = s->seed;
+    fp.filmFp64 = s->film_fp64 ? 1 : 0;
+    fp.film = b->film.as<float4>();
+    fp.film64 = b->film64.as<double>();
+    const PathPool pool = batchPoolView(b);
+    Counters *cnt = b->counters.as<Counters>();
+    ShadeParams sp;
+    sp.ctx = b->scenes[0]->dctx;  // per path from its view
+    sp.pool = pool;
+    sp.fp = fp;
+    sp.counters = cnt;
+    const uint64_t firstPath = firstSample * b->totalPixels;
+    const uint64_t maxIters = ((numPaths + b->capacity - 1) / b->capacity + 1) * ((uint64_t)s->max_depth + 1) + 8;
+    if (maxIters > 0xffffffffull) return fail(RMD_ERROR_INVALID_ARGUMENT, "render too long for one call");
+
+    RMD_CUDA(cudaEventRecord(b->ev[0], st));
+    RMD_CUDA(rmdLaunchFrameInit(pool, cnt, firstPath, firstPath + numPaths, st));
+    uint64_t iterations = 0;
+    if (b->useGraph) {
+        // the graph depends on everything but the sample range (frame init sets that)
+        const std::vector<uint64_t> key = {s->max_depth, s->sampling_mode, s->rng, s->seed, (uint64_t)fp.filmFp64,
+                                           maxIters, (uint64_t)b->capacity, (uint64_t)b->shadeMinBlocks,
+                                           (uint64_t)b->traceBlocksPerSm};
+        if (!b->graphExec || b->graphKey != key) {
+            if (b->graphExec) cudaGraphExecDestroy(b->graphExec);
+            if (b->graph) cudaGraphDestroy(b->graph);
+            b->graphExec = nullptr;
+            b->graph = nullptr;
+            RMD_CUDA(cudaGraphCreate(&b->graph, 0));
+            cudaGraphConditionalHandle handle;
+            RMD_CUDA(cudaGraphConditionalHandleCreate(&handle, b->graph, 1, cudaGraphCondAssignDefault));
+            cudaGraphNodeParams cp = {};
+            cp.type = cudaGraphNodeTypeConditional;
+            cp.conditional.handle = handle;
+            cp.conditional.type = cudaGraphCondTypeWhile;
+            cp.conditional.size = 1;
+            cudaGraphNode_t loop;
+            RMD_CUDA(cudaGraphAddNode(&loop, b->graph, nullptr, 0, &cp));
+            cudaGraph_t body = cp.conditional.phGraph_out[0];
+            // the body: two iterations (both parities) and the condition kernel
+            RMD_CUDA(cudaStreamBeginCaptureToGraph(st, body, nullptr, nullptr, 0, cudaStreamCaptureModeThreadLocal));
+            rmd_status e = batchEnqueueIterations(b, pool, fp, sp, 2, st);
+            cudaError_t ce = e == RMD_OK ? rmdLaunchLoopCondition(cnt, handle, 2, (uint32_t)maxIters, st) : cudaSuccess;
+            cudaGraph_t captured = nullptr;
+            cudaError_t endErr = cudaStreamEndCapture(st, &captured);
+            if (e != RMD_OK) return e;
+            RMD_CUDA(ce);
+            RMD_CUDA(endErr);
+            RMD_CUDA(cudaGraphInstantiate(&b->graphExec, b->graph, 0));
+            b->graphKey = key;
+        }
+        RMD_CUDA(cudaGraphLaunch(b->graphExec, st));
+        RMD_CUDA(cudaMemcpyAsync(b->hostCounters, cnt, sizeof(Counters), cudaMemcpyDeviceToHost, st));
+        RMD_CUDA(cudaStreamSynchronize(st));
+        const Counters &h = *b->hostCounters;
+        iterations = h.loopIterations;
+        if (h.errors) {
+            b->stats.errors = h.errors;
+            return fail(h.errors & ERR_LOOP_BOUND ? RMD_ERROR_WATCHDOG : RMD_ERROR_QUEUE_OVERFLOW,
+                        "device error flags " + std::to_string(h.errors));
+        }
+    } else {
+        bool done = false;
+        while (!done) {
+            rmd_status e = batchEnqueueIterations(b, pool, fp, sp, 4, st);
+            if (e != RMD_OK) return e;
+            iterations += 4;
+            RMD_CUDA(cudaMemcpyAsync(b->hostCounters, cnt, sizeof(Counters), cudaMemcpyDeviceToHost, st));
+            RMD_CUDA(cudaStreamSynchronize(st));
+            const Counters &h = *b->hostCounters;
+            if (h.errors) {
+                b->stats.errors = h.errors;
+                return fail(RMD_ERROR_QUEUE_OVERFLOW, "device error flags " + std::to_string(h.errors));
+            }
+            if (h.pathsDone >= numPaths) done = true;
+            else if (iterations > maxIters) return fail(RMD_ERROR_WATCHDOG, "render did not drain in the iteration bound");
+        }
+    }
+    RMD_CUDA(cudaEventRecord(b->ev[1], st));
+    RMD_CUDA(cudaEventSynchronize(b->ev[1]));
+    float ms = 0;
+    cudaEventElapsedTime(&ms, b->ev[0], b->ev[1]);
+    const Counters &h = *b->hostCounters;
+    b->stats.paths = h.pathsDone;
+    b->stats.segments = h.segments;
+    b->stats.rays = h.rays;
+    b->stats.shadow_rays = h.shadowRays;
+    b->stats.iterations = iterations;
+    b->stats.ms_total = ms;
+    b->samples = std::max<uint64_t>(b->samples, firstSample + s->spp);
+    return RMD_OK;
+}
+
+rmd_status rmd_batch_film_read(rmd_batch *b, int32_t view, float *rgb, int32_t normalize, uint32_t tonemapping,
+                               float exposure) {
+    if (!b || !rgb || view < 0 || view >= (int32_t)b->views.size()) return fail(RMD_ERROR_INVALID_ARGUMENT, "invalid argument");
+    if (tonemapping > 2) return fail(RMD_ERROR_INVALID_ARGUMENT, "tonemapping out of range");
+    cudaStream_t st = b->ctx->stream;
+    const uint32_t n = b->views[view].width * b->views[view].height, off = b->offsets[view];
+    float scale = 1.0f;
+    uint32_t tm = 0;
+    if (normalize) {
+        scale = exposure / (float)std::max<uint64_t>(1, b->samples);
+        tm = tonemapping;
+    }
+    RMD_CUDA(rmdLaunchFilmResolve(b->film.as<float4>() + off, b->film64.ptr ? b->film64.as<double>() + 3 * (size_t)off : nullptr,
+                                  0, b->resolve.as<float>(), n, scale, tm, st));
+    RMD_CUDA(cudaMemcpyAsync(rgb, b->resolve.ptr, (size_t)n * 3 * sizeof(float), cudaMemcpyDeviceToHost, st));
+    RMD_CUDA(cudaStreamSynchronize(st));
+    return RMD_OK;
+}
+
+rmd_status rmd_batch_film_read_f64(rmd_batch *b, int32_t view, double *rgb) {
+    if (!b || !rgb || view < 0 || view >= (int32_t)b->views.size()) return fail(RMD_ERROR_INVALID_ARGUMENT, "invalid argument");
+    if (!b->film64.ptr) return fail(RMD_ERROR_INVALID_ARGUMENT, "no double-precision film (render with film_fp64)");
+    cudaStream_t st = b->ctx->stream;
+    const size_t n = (size_t)b->views[view].width * b->views[view].height;
+    RMD_CUDA(cudaMemcpyAsync(rgb, b->film64.as<double>() + 3 * (size_t)b->offsets[view], n * 3 * sizeof(double),
+                             cudaMemcpyDeviceToHost, st));
+    RMD_CUDA(cudaStreamSynchronize(st));
+    return RMD_OK;
+}
+
+rmd_status rmd_batch_stats(const rmd_batch *b, rmd_stats *out) {
+    if (!b || !out) return fail(RMD_ERROR_INVALID_ARGUMENT, "NULL argument");
+    *out = b->stats;
+    return RMD_OK;
+}
+
+rmd_status rmd_batch_autotune(rmd_batch *b, const rmd_render_settings *settings, rmd_tune_result *out) {
+    if (!b || !settings) return fail(RMD_ERROR_INVALID_ARGUMENT, "NULL argument");
+    const std::vector<int> mbs = {1, 3, 4, 5, 6};
+    rmd_status st = batchEnsureVariants(b, mbs);
+    if (st != RMD_OK) return st;
+    rmd_render_settings cal = *settings;
+    cal.film_fp64 = 0;
+    cal.spp = (uint32_t)std::max<uint64_t>(
+        1, std::min<uint64_t>(settings->spp, (4ull * b->capacity + b->totalPixels - 1) / b->totalPixels));
+    cal.first_sample = BATCH_SAMPLE_MASK - 2 * cal.spp;  // a sample range the caller does not use
+    auto trial = [&](double &ms) -> rmd_status {
+        double best = 1e30;
+        for (int rep = 0; rep < 2; rep++) {
+            rmd_status e = rmd_batch_render(b, &cal);
+            if (e != RMD_OK) return e;
+            best = std::min(best, b->stats.ms_total);
+        }
+        ms = best;
+        return RMD_OK;
+    };
+    rmd_tune_result res{};
+    double base = 0;
+    if ((st = trial(base)) != RMD_OK) return st;
+    res.ms_default = base;
+    int bestMb = b->shadeMinBlocks;
+    double bestMs = base;
+    for (int mb : mbs) {
+        if (mb == b->shadeMinBlocks) continue;
+        batchSelectShade(b, mb);
+        double ms;
+        if ((st = trial(ms)) != RMD_OK) return st;
+        if (ms < bestMs) {
+            bestMs = ms;
+            bestMb = mb;
+        }
+    }
+    batchSelectShade(b, bestMb);
+    int bestTb = b->traceBlocksPerSm;
+    for (int tb : {4, 12, 16}) {
+        b->traceBlocksPerSm = tb;
+        double ms;
+        if ((st = trial(ms)) != RMD_OK) return st;
+        if (ms < bestMs) {
+            bestMs = ms;
+            bestTb = tb;
+        }
+    }
+    b->traceBlocksPerSm = bestTb;
+    const uint32_t cap0 = b->capacity;
+    uint32_t bestCap = cap0;
+    for (uint32_t cap : {cap0 / 2, cap0 * 2}) {
+        if (cap < (1u << 16)) continue;
+        size_t freeB = 0, totalB = 0;
+        if (cudaMemGetInfo(&freeB, &totalB) != cudaSuccess || pathPoolBytes(cap) > freeB / 2) continue;
+        b->capacity = cap;
+        if ((st = batchAllocatePool(b)) != RMD_OK) return st;
+        double ms;
+        if ((st = trial(ms)) != RMD_OK) return st;
+        if (ms < bestMs) {
+            bestMs = ms;
+            bestCap = cap;
+        }
+    }
+    if (b->capacity != bestCap) {
+        b->capacity = bestCap;
+        if ((st = batchAllocatePool(b)) != RMD_OK) return st;
+    }
+    res.shade_min_blocks = (uint32_t)b->shadeMinBlocks;
+    res.trace_blocks_per_sm = (uint32_t)b->traceBlocksPerSm;
+    res.pool_size = b->capacity;
+    res.ms_best = bestMs;
+    res.calibration_spp = cal.spp;
+    if (out) *out = res;
+    return rmd_batch_reset(b);
 }
 
 }  // extern "C"
