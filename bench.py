@@ -23,6 +23,11 @@ weak scaling, no collective on the data path.
            chunks for up to 3x the plain tracer's device time: the guided
            tracer's time to the plain tracer's 1,024-spp relMSE and its relMSE
            at equal time.  Rank 0 only; --no-guided skips it.
+--workload batch: config 3 instead: 64 independent config-2-style scenes
+           (seed i, triangles log-uniform in [10k, 2M], resolution 2^U[7,10]
+           squared) traced as one batch (one wavefront, one CUDA-graph
+           launch per step), 32 spp, depth 10, autotuned; value = aggregate
+           Mpaths/s, with each instance's paths and resolution in `instances`.
 --impl reference times the reference's own CPU implementation of the path
 (its device code built for the host, oracle/_ref, all host cores; the oracle
 restatement when that build is absent) on a bounded sample of the workload.
@@ -194,6 +199,81 @@ def run_reference(args):
     print(json.dumps(line), flush=True)
 
 
+BATCH_INSTANCES, BATCH_SPP, BATCH_DEPTH = 64, 32, 10
+
+
+def batch_instance(i: int, rng) -> tuple[dict, int, int]:
+    """Config-2-style scene i with its triangle target and square resolution."""
+    from raymond_b200 import scenes
+
+    target = int(np.exp(rng.uniform(np.log(1e4), np.log(2e6))))
+    res = 1 << int(rng.integers(7, 11))
+    # 64 icospheres of 5 * 4^s faces take about half the triangles, the terrain the rest
+    sub = max(1, min(6, int(np.floor(np.log(max(target / 2, 320) / 320) / np.log(4))) + 1))
+    while sub > 1 and 64 * 5 * 4 ** sub > target / 2:
+        sub -= 1
+    cells = max(8, int(np.sqrt(max(target - 64 * 5 * 4 ** sub, 128) / 2)))
+    sc = scenes.spheres_terrain(seed=i, subdivisions=sub, terrain_cells=cells, envmap_exponent=4)
+    return sc, res, target
+
+
+def run_batch(args, ctx=None, steps=None, warmup=None) -> dict:
+    """Config 3: 64 scenes / views in one batch; returns the bench line."""
+    from raymond_b200 import api, scenes
+    from raymond_b200._abi import SceneDesc
+
+    rng = np.random.default_rng(3)
+    t0 = time.perf_counter()
+    descs, views, targets = [], [], []
+    for i in range(BATCH_INSTANCES):
+        sc, res, target = batch_instance(i, rng)
+        descs.append(SceneDesc(sc))
+        views.append({"scene": i, "width": res, "height": res})
+        targets.append(target)
+    ctx = ctx or api.Context(0)
+    steps = args.steps if steps is None else steps
+    warmup = args.warmup if warmup is None else warmup
+    b = api.Batch(ctx, descs, views)
+    build_s = time.perf_counter() - t0
+    t0 = time.perf_counter()
+    tune = b.autotune(spp=BATCH_SPP, max_depth=BATCH_DEPTH, seed=SEED)
+    tune_s = time.perf_counter() - t0
+    for k in range(warmup):
+        b.reset()
+        b.render(spp=BATCH_SPP, max_depth=BATCH_DEPTH, seed=SEED, first_sample=k * BATCH_SPP)
+    sampler = ClockSampler(0)
+    sampler.start()
+    tot_ms, paths, segments = 0.0, 0, 0
+    for k in range(steps):
+        b.reset()
+        b.render(spp=BATCH_SPP, max_depth=BATCH_DEPTH, seed=SEED, first_sample=k * BATCH_SPP)
+        st = b.stats()
+        tot_ms += st["ms_total"]
+        paths += st["paths"]
+        segments += st["segments"]
+    clocks = sampler.stop()
+    tris = [int(sum(len(s["indices"]) for s in d.scene["shapes"])) for d in descs]
+    pixels = [v["width"] * v["height"] for v in views]
+    value = paths / (tot_ms / 1e3) / 1e6
+    line = {
+        "metric": "Mpaths/s (batched, config 3)", "value": value, "unit": "Mpaths/s", "n_gpus": 1,
+        "steps": steps, "warmup": warmup, "ms_per_step": tot_ms / steps, "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic (seeded procedural scenes)",
+        "config": {"workload": f"batch_{BATCH_INSTANCES}_instances_{BATCH_SPP}spp_depth{BATCH_DEPTH}",
+                   "instances": BATCH_INSTANCES, "total_pixels": sum(pixels), "total_triangles": sum(tris),
+                   "launch": "one wavefront, one CUDA-graph launch per step (device-driven while loop)",
+                   "l2": "inputs larger than L2 (path pool + BVHs + films)"},
+        "msegments_per_s": segments / (tot_ms / 1e3) / 1e6,
+        "instances": [{"triangles": t, "resolution": v["width"], "paths_per_step": p * BATCH_SPP,
+                       "share_of_step_mpaths_per_s": p * BATCH_SPP / (tot_ms / steps / 1e3) / 1e6}
+                      for t, v, p in zip(tris, views, pixels)],
+        "clocks": clocks, "scene_build_s": build_s, "autotune": dict(tune, seconds=tune_s),
+        "gpu_launches": steps,
+    }
+    b.close()
+    return line
+
+
 def guided_leg(api, ctx, oracle_spp: int) -> dict:
     """Equal-time relMSE of the guided tracer against the plain one (config 4)."""
     from raymond_b200 import scenes
@@ -271,6 +351,8 @@ def main():
     ap.add_argument("--spp", type=int, default=SPP, help="override (profiling runs only)")
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-guided", action="store_true")
+    ap.add_argument("--no-batch", action="store_true")
+    ap.add_argument("--workload", default="plain", choices=["plain", "batch"])
     ap.add_argument("--oracle-spp", type=int, default=GUIDED_ORACLE_SPP, help="guided leg: oracle samples")
     ap.add_argument("--no-autotune", action="store_true")
     ap.add_argument("--tuning", default="", help="shade_min_blocks,trace_blocks_per_sm,pool_size: apply "
@@ -279,6 +361,9 @@ def main():
     globals().update(W=args.width, H=args.height, SPP=args.spp)
     if args.impl == "reference":
         return run_reference(args)
+    if args.workload == "batch":
+        print(json.dumps(run_batch(args)), flush=True)
+        return
 
     rank, world, local = rank_info()
     dist = None
@@ -390,6 +475,10 @@ def main():
     }
     if not args.no_guided and world == 1:
         line["guided"] = guided_leg(api, ctx, args.oracle_spp)
+    if not args.no_batch and world == 1:
+        bl = run_batch(args, ctx, steps=2, warmup=1)
+        line["batched"] = {k: bl[k] for k in ("metric", "value", "unit", "ms_per_step", "msegments_per_s", "config",
+                                              "autotune", "clocks", "scene_build_s")}
     if not args.no_cpu_baseline:
         line["cpu_baseline"] = cpu_baseline_sample(desc)
     print(json.dumps(line), flush=True)
