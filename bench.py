@@ -68,7 +68,7 @@ BYTES_FILM_PER_PATH = 16 + 32 + 80
 # DRAM bytes per unit measured by ncu (dram__bytes_read.sum + dram__bytes_write.sum
 # of one steady-state launch divided by the units it processed; small case, see
 # profiles/ncu_full_spheres_terrain_480x270.md); only the closest-hit kernel's is used
-TRAFFIC_PER_UNIT = {"trace": 106.8}
+TRAFFIC_PER_UNIT = {"trace": 78.5}
 GUIDED_W, GUIDED_H, GUIDED_DEPTH, GUIDED_ORACLE_SPP, GUIDED_PLAIN_SPP, GUIDED_CHUNK = 1280, 720, 16, 65536, 1024, 32
 CPU_BASELINE_SPP = 16  # CPU sample: 16 one-spp frames of the full image (about 10-20 s on 16 cores)
 
@@ -274,7 +274,7 @@ def run_batch(args, ctx=None, steps=None, warmup=None) -> dict:
     return line
 
 
-def guided_leg(api, ctx, oracle_spp: int) -> dict:
+def guided_leg(api, ctx, oracle_spp: int, size=(GUIDED_W, GUIDED_H)) -> dict:
     """Equal-time relMSE of the guided tracer against the plain one (config 4)."""
     from raymond_b200 import scenes
     from raymond_b200._abi import SceneDesc
@@ -282,7 +282,7 @@ def guided_leg(api, ctx, oracle_spp: int) -> dict:
 
     desc = SceneDesc(scenes.glossy_room(seed=1))
     scene = api.Scene(ctx, desc)
-    W, H, depth = GUIDED_W, GUIDED_H, GUIDED_DEPTH
+    (W, H), depth = size, GUIDED_DEPTH
     oracle = api.Renderer(scene, W, H)
     per_call = max(1, min(oracle_spp, (1 << 27) // (W * H)))
     done, oracle_ms = 0, 0.0
@@ -352,7 +352,8 @@ def main():
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-guided", action="store_true")
     ap.add_argument("--no-batch", action="store_true")
-    ap.add_argument("--workload", default="plain", choices=["plain", "batch"])
+    ap.add_argument("--workload", default="plain", choices=["plain", "batch", "guided", "guided-render"])
+    ap.add_argument("--guided-size", default=f"{GUIDED_W}x{GUIDED_H}", help="guided leg resolution (profiling runs)")
     ap.add_argument("--oracle-spp", type=int, default=GUIDED_ORACLE_SPP, help="guided leg: oracle samples")
     ap.add_argument("--no-autotune", action="store_true")
     ap.add_argument("--tuning", default="", help="shade_min_blocks,trace_blocks_per_sm,pool_size: apply "
@@ -363,6 +364,21 @@ def main():
         return run_reference(args)
     if args.workload == "batch":
         print(json.dumps(run_batch(args)), flush=True)
+        return
+    guided_size = tuple(int(x) for x in args.guided_size.split("x"))
+    if args.workload == "guided-render":  # the guided tracer alone, --steps chunks of 32 spp (profiling runs)
+        from raymond_b200 import api as api_, scenes
+        from raymond_b200._abi import SceneDesc as SceneDesc_
+        ctx_ = api_.Context(0)
+        g = api_.Renderer(api_.Scene(ctx_, SceneDesc_(scenes.glossy_room(seed=1))), *guided_size)
+        g.set_guide(sampling=True, training=True, seed=1, batch_size=1 << 20, learning_rate=1e-3)
+        for _ in range(args.steps):
+            g.render(spp=GUIDED_CHUNK, max_depth=GUIDED_DEPTH, seed=2)
+        print(json.dumps({"workload": "guided-render", "stats": g.stats(), "guide": g.guide_stats()}), flush=True)
+        return
+    if args.workload == "guided":  # the config-4 leg alone
+        from raymond_b200 import api as api_
+        print(json.dumps(guided_leg(api_, api_.Context(0), args.oracle_spp, guided_size)), flush=True)
         return
 
     rank, world, local = rank_info()
@@ -474,7 +490,7 @@ def main():
         "autotune": dict(tune, seconds=tune_s) if tune else None,
     }
     if not args.no_guided and world == 1:
-        line["guided"] = guided_leg(api, ctx, args.oracle_spp)
+        line["guided"] = guided_leg(api, ctx, args.oracle_spp, guided_size)
     if not args.no_batch and world == 1:
         bl = run_batch(args, ctx, steps=2, warmup=1)
         line["batched"] = {k: bl[k] for k in ("metric", "value", "unit", "ms_per_step", "msegments_per_s", "config",
