@@ -403,7 +403,7 @@ typedef struct rmd_batch_view {
 
 rmd_status rmd_batch_create(rmd_context *ctx, const rmd_scene_desc *scenes, int32_t num_scenes,
                             const rmd_batch_view *views, int32_t num_views, uint32_t pool_size, uint32_t flags,
-                            rmd_batch **out);
+                            rmd_batch **out);  /* pool_size <= 2^22 (0: 2^21) */
 void rmd_batch_destroy(rmd_batch *batch);
 rmd_status rmd_batch_reset(rmd_batch *batch);
 /* settings->spp samples of every view (sample indices below 2^24) */
@@ -414,6 +414,12 @@ rmd_status rmd_batch_film_read_f64(rmd_batch *batch, int32_t view, double *rgb);
 /* aggregate over the views (per-stage times are not taken inside the graph) */
 rmd_status rmd_batch_stats(const rmd_batch *batch, rmd_stats *out);
 rmd_status rmd_batch_autotune(rmd_batch *batch, const rmd_render_settings *settings, rmd_tune_result *out);
+/* Learned path guiding of a batch whose views all show one scene (one
+ * network for the scene; rmd_guide_settings as for a renderer).  While
+ * training, the batch renders with the host-driven loop, since the Adam
+ * steps run between its counter checks. */
+rmd_status rmd_batch_set_guide(rmd_batch *batch, const rmd_guide_settings *settings);
+rmd_status rmd_batch_guide_stats(const rmd_batch *batch, rmd_guide_stats *out);
 
 /* ----------------------------------------------------- allocation-free render */
 /*

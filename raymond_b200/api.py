@@ -31,6 +31,7 @@ EXPORTS = [
     "rmd_renderer_set_tuning", "rmd_renderer_set_guide", "rmd_renderer_guide_stats", "rmd_guide_param_count",
     "rmd_renderer_guide_params", "rmd_batch_create", "rmd_batch_destroy", "rmd_batch_reset", "rmd_batch_render",
     "rmd_batch_film_read", "rmd_batch_film_read_f64", "rmd_batch_stats", "rmd_batch_autotune",
+    "rmd_batch_set_guide", "rmd_batch_guide_stats",
     "rmd_test_prng", "rmd_test_trace", "rmd_test_material_eval", "rmd_test_generate_source", "rmd_test_jit_compile",
     "rmd_test_guide_forward", "rmd_test_guide_gradient", "rmd_test_guide_mixture",
 ]
@@ -92,6 +93,8 @@ def lib() -> C.CDLL:
         "rmd_batch_film_read_f64": ([vp, C.c_int32, P(C.c_double)], C.c_int32),
         "rmd_batch_stats": ([vp, P(Stats)], C.c_int32),
         "rmd_batch_autotune": ([vp, P(RenderSettings), P(_abi.TuneResult)], C.c_int32),
+        "rmd_batch_set_guide": ([vp, P(_abi.GuideSettings)], C.c_int32),
+        "rmd_batch_guide_stats": ([vp, P(_abi.GuideStats)], C.c_int32),
         "rmd_render_noalloc": ([vp, P(_abi.Camera), C.c_uint32, C.c_uint32, P(RenderSettings), C.c_void_p,
                                 C.c_uint32], C.c_int32),
         "rmd_test_prng": ([C.c_uint32, C.c_uint64, C.c_uint64, C.c_int32, P(C.c_float)], C.c_int32),
@@ -337,6 +340,21 @@ class Batch:
         res = _abi.TuneResult()
         check(lib().rmd_batch_autotune(self.h, C.byref(s), C.byref(res)))
         return {k: getattr(res, k) for k, _ in _abi.TuneResult._fields_}
+
+    def set_guide(self, sampling: bool = True, training: bool = True, batch_size: int = 0,
+                  learning_rate: float = 0.0, reset: bool = False, seed: int = 0, step_records: int = 0,
+                  replay_records: int = 0, steps_per_batch: int = 0, light_records: bool = True,
+                  guided_depth: int = 0) -> None:
+        """Learned path guiding for a batch whose views all show one scene
+        (same settings as Renderer.set_guide)."""
+        g = _abi.GuideSettings(int(sampling), int(training), batch_size, learning_rate, int(reset), seed,
+                               step_records, replay_records, steps_per_batch, int(not light_records), guided_depth)
+        check(lib().rmd_batch_set_guide(self.h, C.byref(g)))
+
+    def guide_stats(self) -> dict[str, float]:
+        g = _abi.GuideStats()
+        check(lib().rmd_batch_guide_stats(self.h, C.byref(g)))
+        return {k: getattr(g, k) for k, _ in _abi.GuideStats._fields_ if k != "reserved"}
 
     def close(self):
         if self.h.value:

@@ -130,11 +130,7 @@ __device__ __forceinline__ bool shadePath(const ShadeParams &p, uint32_t i, uint
                         __stcs(&pool.shO[k], f4(shading.position, nee.distance - SHADOW_EPS));
                         // training: the light sample is a training sample of this vertex too
                         const bool neeRecord = pool.shRec && meanThroughput > 0.0f && neeBsdfPdf > 0.0f;
-#ifdef RMD_BATCH
-                        __stcs(&pool.shW[k], f4(neeWeight, __uint_as_float(view)));  // the shadow ray's scene
-#else
                         __stcs(&pool.shW[k], f4(neeWeight, neeRecord ? 1.0f / meanThroughput : 0.0f));
-#endif
                         if (neeRecord) {
                             __stcs(&pool.shRec[2 * k], make_float4(gf.v[0], gf.v[1], gf.v[2], gf.v[3]));
                             __stcs(&pool.shRec[2 * k + 1], make_float4(gf.v[4], gf.v[5], gf.v[6], neeBsdfPdf));
@@ -255,6 +251,9 @@ __device__ __forceinline__ bool shadePath(const ShadeParams &p, uint32_t i, uint
     }
     if (shadowIndex != 0xffffffffu) {
         if (recorded && target != 0xffffffffu) target |= SHADOW_TO_RECORD;
+#ifdef RMD_BATCH
+        if (target != 0xffffffffu) target |= view << BATCH_TARGET_BITS;  // the shadow ray's scene
+#endif
         __stcs(&pool.shD[shadowIndex], f4(shadowDir, __uint_as_float(target)));
     }
     return h4.x > 0.0f;

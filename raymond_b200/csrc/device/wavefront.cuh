@@ -102,6 +102,11 @@ struct BatchView {
     const float4 *tris;  // the scene's BVH triangles
     uint32_t width, height, numPixels, pixelOffset;
 };
+// a batch's shadow-ray target carries the ray's view in bits 22-29 (batch
+// pools hold at most 2^22 paths)
+constexpr uint32_t BATCH_TARGET_BITS = 22;
+constexpr uint32_t BATCH_TARGET_MASK = (1u << BATCH_TARGET_BITS) - 1u;
+constexpr uint32_t BATCH_MAX_CAPACITY = 1u << BATCH_TARGET_BITS;
 constexpr uint32_t BATCH_SAMPLE_BITS = 24;
 constexpr uint32_t BATCH_SAMPLE_MASK = (1u << BATCH_SAMPLE_BITS) - 1u;
 

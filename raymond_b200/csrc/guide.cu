@@ -423,12 +423,14 @@ __global__ void __launch_bounds__(256) k_guide_features(Context ctx, PathPool po
         const uint32_t depth = __float_as_uint(S.L[idx].w) & 0xffffu;
         GuideFeatures f = {};
         if (depth < guideDepth) {  // only guided vertices need the features
+            // a batch path's scene is its view's (the view in the top bits of its sample word)
+            const Context &c = pool.views ? pool.views[__ldg(&S.id[idx].y) >> BATCH_SAMPLE_BITS].ctx : ctx;
             const float4 o = __ldcs(&S.rayO[idx]), dd = __ldcs(&S.rayD[idx]), h = pool.hit[idx];
-            const PerInstanceData &inst = ctx.instances[pool.hitInst[idx]];
-            const uint4 face = ctx.faces[inst.faceOffset + __float_as_uint(h.w)];
-            const float3 Pc = xyz(ctx.vertices[inst.vertexOffset + face.z]);
-            const float3 P0 = xyz(ctx.vertices[inst.vertexOffset + face.x]) - Pc;
-            const float3 P1 = xyz(ctx.vertices[inst.vertexOffset + face.y]) - Pc;
+            const PerInstanceData &inst = c.instances[pool.hitInst[idx]];
+            const uint4 face = c.faces[inst.faceOffset + __float_as_uint(h.w)];
+            const float3 Pc = xyz(c.vertices[inst.vertexOffset + face.z]);
+            const float3 P0 = xyz(c.vertices[inst.vertexOffset + face.x]) - Pc;
+            const float3 P1 = xyz(c.vertices[inst.vertexOffset + face.y]) - Pc;
             const float3 n = normalize(mul3(inst.normalTransform, cross(P0, P1)));
             f = guideFeatures(xyz(o) + xyz(dd) * h.x, n, -xyz(dd), pool.guideMin, pool.guideInvExtent);
         }

@@ -197,7 +197,7 @@ __global__ void __launch_bounds__(128) k_trace_closest(const WideNode *__restric
 // shadow ray adds its weight to its path's radiance, in S[p ^ 1] for a path
 // that continues and in the finish list for one that ended.  Thread 0 also
 // advances nextPath past the camera samples this iteration consumed.
-// BATCH: the ray's view is in the bits of shW.w.
+// BATCH: the ray's view is in bits 22-29 of its target.
 template <bool BATCH>
 __global__ void __launch_bounds__(128) k_trace_shadow(const WideNode *__restrict__ sceneNodes,
                                                       const float4 *__restrict__ sceneTris, PathPool pool,
@@ -211,7 +211,8 @@ __global__ void __launch_bounds__(128) k_trace_shadow(const WideNode *__restrict
         sceneNodes, sceneTris, &cnt->shadowWork, n, &cnt->errors,
         [&](uint32_t idx, TraversalState &s, TraversalStack &, const WideNode *&nodes, const float4 *&tris) {
             if constexpr (BATCH) {
-                const BatchView &bv = pool.views[__float_as_uint(__ldg(&pool.shW[idx].w))];
+                const uint32_t t = __float_as_uint(__ldg(&pool.shD[idx].w));
+                const BatchView &bv = pool.views[(t >> BATCH_TARGET_BITS) & 0xffu];
                 nodes = static_cast<const WideNode *>(bv.nodes);
                 tris = bv.tris;
             }
@@ -225,7 +226,7 @@ __global__ void __launch_bounds__(128) k_trace_shadow(const WideNode *__restrict
             // all ones: the path overflowed its queue
             if (s.hitTri >= 0 || target == 0xffffffffu) return;
             const bool finished = (target & SHADOW_TO_FINISHED) != 0u;
-            const uint32_t at = target & SHADOW_TARGET_MASK;
+            const uint32_t at = target & (BATCH ? BATCH_TARGET_MASK : SHADOW_TARGET_MASK);
             float4 *dst = finished ? &pool.fin[at] : &nextL[at];
             const float4 w = __ldcs(&pool.shW[idx]);
             float4 L = *dst;
@@ -241,7 +242,7 @@ __global__ void __launch_bounds__(128) k_trace_shadow(const WideNode *__restrict
                 r.z += w.z;
                 *rec = r;
             }
-            if (!BATCH && pool.shRec && w.w > 0.0f) {
+            if (pool.shRec && w.w > 0.0f) {
                 // a training record of the vertex's light sample: its direction,
                 // target (MIS-weighted contribution / throughput) and features
                 const float y = (w.x + w.y + w.z) * (1.0f / 3.0f) * w.w;

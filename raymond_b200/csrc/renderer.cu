@@ -117,6 +117,19 @@ struct rmd_scene {
     }
 };
 
+// Learned path guiding of one renderer or batch: the network and the
+// per-path buffers of its pool.
+struct GuideState {
+    rmd_guide_settings settings{};
+    rmd_guide_stats stats{};
+    rmdhost::GuideNet net;
+    DevBuf mixtures, features, rec, finRec, shRec, records;
+    uint32_t pathCapacity = 0;    // paths the mixtures / pending-record buffers hold
+    uint32_t recordCapacity = 0;  // nonzero-target records the replay ring holds
+    bool initialised = false;
+    float3 frameMin = {0, 0, 0}, frameInvExtent = {1, 1, 1};  // position encoding frame (scene bounds)
+};
+
 struct rmd_renderer {
     rmd_scene *scene = nullptr;
     uint32_t width = 0, height = 0, capacity = 0;
@@ -134,16 +147,7 @@ struct rmd_renderer {
     cudaEvent_t ev[4] = {};
     std::vector<cudaEvent_t> stageEvents;  // recorded between the stage kernels
     std::vector<int> stageOf;              // stage of the interval that ends at each event
-    // learned path guiding
-    struct Guide {
-        rmd_guide_settings settings{};
-        rmd_guide_stats stats{};
-        rmdhost::GuideNet net;
-        DevBuf mixtures, features, rec, finRec, shRec, records;
-        uint32_t pathCapacity = 0;    // paths the mixtures / pending-record buffers hold
-        uint32_t recordCapacity = 0;  // nonzero-target records the replay ring holds
-        bool initialised = false;
-    } guide;
+    GuideState guide;  // learned path guiding
     ~rmd_renderer() {
         if (hostCounters) cudaFreeHost(hostCounters);
         for (auto &e : ev)
@@ -182,6 +186,8 @@ struct rmd_batch {
     cudaKernel_t shade = nullptr;
     int shadeBlocks = 0, shadeMinBlocks = 1, defaultMinBlocks = 1, traceBlocksPerSm = 12;
     bool useGraph = true;
+    GuideState guide;  // learned path guiding (all views of one scene)
+    int guideScene = -1;
     uint64_t samples = 0;
     rmd_stats stats{};
     cudaEvent_t ev[2] = {};
@@ -661,22 +667,27 @@ static rmd_status allocatePool(rmd_renderer *r) {
     return ensureGuideBuffers(r);
 }
 
-static PathPool poolView(rmd_renderer *r) {
-    PathPool pool = carvePathPool(r->pool.ptr, r->capacity);
-    const auto &g = r->guide;
-    if (g.settings.training && g.pathCapacity >= r->capacity) {
+// points a pool of `capacity` paths at the guide's buffers
+static void applyGuide(const GuideState &g, uint32_t capacity, PathPool &pool) {
+    if (g.settings.training && g.pathCapacity >= capacity) {
         pool.s[0].rec = g.rec.as<float4>();
-        pool.s[1].rec = g.rec.as<float4>() + 4 * (size_t)r->capacity;
+        pool.s[1].rec = g.rec.as<float4>() + 4 * (size_t)capacity;
         pool.finRec = g.finRec.as<float4>();
         pool.shRec = g.settings.skip_light_records ? nullptr : g.shRec.as<float4>();
         pool.records = g.records.as<GuideRecord>();
         pool.recordCapacity = g.recordCapacity;
     }
-    if (g.settings.sampling && g.pathCapacity >= r->capacity) {
+    if (g.settings.sampling && g.pathCapacity >= capacity) {
         pool.guide = g.mixtures.as<GuideMixture>();
         pool.guideFeat = g.features.as<uint4>();
-        guideFrame(r->scene, pool.guideMin, pool.guideInvExtent);
+        pool.guideMin = g.frameMin;
+        pool.guideInvExtent = g.frameInvExtent;
     }
+}
+
+static PathPool poolView(rmd_renderer *r) {
+    PathPool pool = carvePathPool(r->pool.ptr, r->capacity);
+    applyGuide(r->guide, r->capacity, pool);
     return pool;
 }
 
@@ -692,11 +703,10 @@ static void guideFrame(const rmd_scene *s, float3 &lo, float3 &invExtent) {
     invExtent = make_float3(inv[0], inv[1], inv[2]);
 }
 
-// (re)allocates the guide's buffers for the renderer's pool size
-static rmd_status ensureGuideBuffers(rmd_renderer *r) {
-    auto &g = r->guide;
+// (re)allocates the guide's buffers for a pool of `capacity` paths
+static rmd_status guideBuffers(GuideState &g, uint32_t capacity, Counters *counters) {
     if (!g.settings.sampling && !g.settings.training) return RMD_OK;
-    if (g.pathCapacity < r->capacity) {
+    if (g.pathCapacity < capacity) {
         g.pathCapacity = 0;
         g.mixtures.release();
         g.features.release();
@@ -705,21 +715,99 @@ static rmd_status ensureGuideBuffers(rmd_renderer *r) {
         g.shRec.release();
     }
     if (g.settings.sampling && !g.mixtures.ptr) {
-        RMD_CUDA(g.mixtures.alloc((size_t)r->capacity * sizeof(GuideMixture)));
-        RMD_CUDA(g.features.alloc((size_t)r->capacity * sizeof(uint4)));
+        RMD_CUDA(g.mixtures.alloc((size_t)capacity * sizeof(GuideMixture)));
+        RMD_CUDA(g.features.alloc((size_t)capacity * sizeof(uint4)));
     }
     if (g.settings.training && !g.rec.ptr) {
-        RMD_CUDA(g.rec.alloc((size_t)r->capacity * 2 * 4 * sizeof(float4)));
-        RMD_CUDA(g.finRec.alloc((size_t)r->capacity * 4 * sizeof(float4)));
-        RMD_CUDA(g.shRec.alloc((size_t)r->capacity * 2 * sizeof(float4)));
+        RMD_CUDA(g.rec.alloc((size_t)capacity * 2 * 4 * sizeof(float4)));
+        RMD_CUDA(g.finRec.alloc((size_t)capacity * 4 * sizeof(float4)));
+        RMD_CUDA(g.shRec.alloc((size_t)capacity * 2 * sizeof(float4)));
     }
-    g.pathCapacity = r->capacity;
+    g.pathCapacity = capacity;
     const uint32_t want = g.settings.replay_records;
     if (g.settings.training && g.recordCapacity != want) {
         g.recordCapacity = 0;
         RMD_CUDA(g.records.alloc((size_t)want * sizeof(GuideRecord)));
         g.recordCapacity = want;
-        RMD_CUDA(cudaMemset(&r->counters.as<Counters>()->numRecords, 0, 2 * sizeof(uint32_t)));
+        RMD_CUDA(cudaMemset(&counters->numRecords, 0, 2 * sizeof(uint32_t)));
+    }
+    return RMD_OK;
+}
+
+static rmd_status ensureGuideBuffers(rmd_renderer *r) {
+    return guideBuffers(r->guide, r->capacity, r->counters.as<Counters>());
+}
+
+// Adam steps due after a counter check: one per `batch_size` samples (times
+// steps_per_batch), each on records drawn from the replay ring.
+static rmd_status guideTrainStep(GuideState &guide, const Counters &h, Counters *cnt, const GuideNetView &net,
+                                 int trainBlocks, cudaStream_t st, uint64_t &trainSteps) {
+    if (!guide.settings.training || h.numSamples < guide.settings.batch_size) return RMD_OK;
+    const uint32_t stored = std::min(h.numRecords, guide.recordCapacity);
+    const uint32_t steps = h.numSamples / guide.settings.batch_size * guide.settings.steps_per_batch;
+    for (uint32_t k = 0; k < steps && stored > 0; k++) {
+        RMD_CUDA(rmdLaunchGuideTrain(guide.records.as<GuideRecord>(), stored, guide.settings.step_records,
+                                     (uint32_t)guide.net.steps + 1u, net, guide.net.scratch, trainBlocks,
+                                     guide.settings.learning_rate, guide.net.steps + 1, st));
+        guide.net.steps++;
+        trainSteps++;
+        guide.stats.steps++;
+    }
+    RMD_CUDA(cudaMemsetAsync(&cnt->numSamples, 0, sizeof(uint32_t), st));
+    guide.stats.samples += h.numSamples;
+    guide.stats.records = h.numRecords;
+    return RMD_OK;
+}
+
+static rmd_status guideReadLoss(GuideState &guide) {
+    float loss = 0;
+    RMD_CUDA(cudaMemcpy(&loss, guide.net.scratch + 1, sizeof(float), cudaMemcpyDeviceToHost));
+    guide.stats.last_loss = loss;
+    return RMD_OK;
+}
+
+// rmd_renderer_set_guide / rmd_batch_set_guide
+static rmd_status setGuide(GuideState &g, const rmd_guide_settings *settings, cudaStream_t stream, Counters *counters) {
+    const uint32_t ring = settings->replay_records;
+    if (settings->sampling > 1 || settings->training > 1 || settings->reset > 1 || settings->learning_rate < 0.0f ||
+        !std::isfinite(settings->learning_rate) || settings->batch_size > (1u << 26) ||
+        (settings->batch_size != 0 && settings->batch_size < 16) || settings->step_records > (1u << 24) ||
+        settings->steps_per_batch > 1024 || settings->skip_light_records > 1 || settings->guided_depth > 65535 ||
+        (ring != 0 && (ring < 1024 || ring > (1u << 26) || (ring & (ring - 1)) != 0)))
+        return fail(RMD_ERROR_INVALID_ARGUMENT, "invalid guide settings");
+    rmd_guide_settings next = *settings;
+    if (next.batch_size == 0) next.batch_size = 1u << 20;
+    if (next.learning_rate == 0.0f) next.learning_rate = 1e-3f;
+    if (next.step_records == 0) next.step_records = 1u << 14;
+    if (next.replay_records == 0) next.replay_records = 1u << 18;
+    if (next.steps_per_batch == 0) next.steps_per_batch = 1;
+    if (next.guided_depth == 0) next.guided_depth = 65535;
+    if (!g.net.allocated()) RMD_CUDA(g.net.allocate());
+    if (!g.initialised || next.reset) {
+        std::vector<float> params(GUIDE_PARAMS);
+        rmdhost::GuideNet::initParams(params.data(), next.seed);
+        RMD_CUDA(g.net.setParams(params.data(), stream));
+        g.initialised = true;
+        g.stats = rmd_guide_stats{};
+        // records gathered by an earlier network are dropped with it
+        RMD_CUDA(cudaMemset(&counters->numRecords, 0, 2 * sizeof(uint32_t)));
+    }
+    next.reset = 0;
+    g.settings = next;
+    return RMD_OK;
+}
+
+static rmd_status guideParams(GuideState &g, float *params, int32_t write, cudaStream_t stream) {
+    if (!g.net.allocated()) RMD_CUDA(g.net.allocate());
+    if (write) {
+        for (int i = 0; i < GUIDE_PARAMS; i++)
+            if (!std::isfinite(params[i])) return fail(RMD_ERROR_INVALID_ARGUMENT, "non-finite guide parameter");
+        RMD_CUDA(g.net.setParams(params, stream));
+        g.initialised = true;
+        g.stats = rmd_guide_stats{};
+    } else {
+        if (!g.initialised) return fail(RMD_ERROR_INVALID_ARGUMENT, "the guide has not been set up");
+        RMD_CUDA(g.net.getParams(params, stream));
     }
     return RMD_OK;
 }
@@ -832,8 +920,8 @@ rmd_status rmd_render(rmd_renderer *r, const rmd_render_settings *s) {
     if (guideSampling || guideTraining) {
         rmd_status gs = ensureGuideBuffers(r);
         if (gs != RMD_OK) return gs;
-        float3 lo, inv;
-        guideFrame(scene, lo, inv);
+        guideFrame(scene, guide.frameMin, guide.frameInvExtent);
+        const float3 lo = guide.frameMin, inv = guide.frameInvExtent;
         net = guide.net.view(lo, inv);
         fp.guideDepth = guideSampling ? guide.settings.guided_depth : 0u;
         fp.guideSceneMin = lo;
@@ -883,21 +971,8 @@ rmd_status rmd_render(rmd_renderer *r, const rmd_render_settings *s) {
             return fail(RMD_ERROR_QUEUE_OVERFLOW, "device error flags " + std::to_string(h.errors));
         }
         if (guideTraining && h.numSamples >= batch) {
-            // one Adam step per `batch` samples gathered since the last check,
-            // each on records drawn from the replay ring
-            const uint32_t stored = std::min(h.numRecords, guide.recordCapacity);
-            const uint32_t steps = h.numSamples / batch * guide.settings.steps_per_batch;
-            for (uint32_t k = 0; k < steps && stored > 0; k++) {
-                RMD_CUDA(rmdLaunchGuideTrain(guide.records.as<GuideRecord>(), stored, guide.settings.step_records,
-                                             (uint32_t)guide.net.steps + 1u, net, guide.net.scratch, trainBlocks,
-                                             guide.settings.learning_rate, guide.net.steps + 1, st));
-                guide.net.steps++;
-                trainSteps++;
-                guide.stats.steps++;
-            }
-            RMD_CUDA(cudaMemsetAsync(&cnt->numSamples, 0, sizeof(uint32_t), st));
-            guide.stats.samples += h.numSamples;
-            guide.stats.records = h.numRecords;
+            rmd_status gs = guideTrainStep(guide, h, cnt, net, trainBlocks, st, trainSteps);
+            if (gs != RMD_OK) return gs;
             RMD_CUDA(r->stageEvent(evi++, STAGE_TRAIN, st));
         }
         if (h.pathsDone >= numPaths) done = true;
@@ -914,9 +989,8 @@ rmd_status rmd_render(rmd_renderer *r, const rmd_render_settings *s) {
         stage[r->stageOf[i]] += t;
     }
     if (trainSteps) {
-        float loss = 0;
-        RMD_CUDA(cudaMemcpy(&loss, guide.net.scratch + 1, sizeof(float), cudaMemcpyDeviceToHost));
-        guide.stats.last_loss = loss;
+        rmd_status gs = guideReadLoss(guide);
+        if (gs != RMD_OK) return gs;
     }
     const Counters &h = *r->hostCounters;
     r->stats.paths = h.pathsDone;
@@ -1110,34 +1184,9 @@ rmd_status rmd_renderer_set_tuning(rmd_renderer *r, const rmd_tune_result *t) {
 // --------------------------------------------------------------------- guiding
 rmd_status rmd_renderer_set_guide(rmd_renderer *r, const rmd_guide_settings *settings) {
     if (!r || !settings) return fail(RMD_ERROR_INVALID_ARGUMENT, "NULL argument");
-    const uint32_t ring = settings->replay_records;
-    if (settings->sampling > 1 || settings->training > 1 || settings->reset > 1 || settings->learning_rate < 0.0f ||
-        !std::isfinite(settings->learning_rate) || settings->batch_size > (1u << 26) ||
-        (settings->batch_size != 0 && settings->batch_size < 16) || settings->step_records > (1u << 24) ||
-        settings->steps_per_batch > 1024 || settings->skip_light_records > 1 || settings->guided_depth > 65535 ||
-        (ring != 0 && (ring < 1024 || ring > (1u << 26) || (ring & (ring - 1)) != 0)))
-        return fail(RMD_ERROR_INVALID_ARGUMENT, "invalid guide settings");
     RMD_CUDA(cudaSetDevice(r->scene->ctx->device));
-    auto &g = r->guide;
-    rmd_guide_settings next = *settings;
-    if (next.batch_size == 0) next.batch_size = 1u << 20;
-    if (next.learning_rate == 0.0f) next.learning_rate = 1e-3f;
-    if (next.step_records == 0) next.step_records = 1u << 14;
-    if (next.replay_records == 0) next.replay_records = 1u << 18;
-    if (next.steps_per_batch == 0) next.steps_per_batch = 1;
-    if (next.guided_depth == 0) next.guided_depth = 65535;
-    if (!g.net.allocated()) RMD_CUDA(g.net.allocate());
-    if (!g.initialised || next.reset) {
-        std::vector<float> params(GUIDE_PARAMS);
-        rmdhost::GuideNet::initParams(params.data(), next.seed);
-        RMD_CUDA(g.net.setParams(params.data(), r->scene->ctx->stream));
-        g.initialised = true;
-        g.stats = rmd_guide_stats{};
-        // records gathered by an earlier network are dropped with it
-        RMD_CUDA(cudaMemset(&r->counters.as<Counters>()->numRecords, 0, 2 * sizeof(uint32_t)));
-    }
-    next.reset = 0;
-    g.settings = next;
+    rmd_status st = setGuide(r->guide, settings, r->scene->ctx->stream, r->counters.as<Counters>());
+    if (st != RMD_OK) return st;
     return ensureGuideBuffers(r);
 }
 
@@ -1150,19 +1199,7 @@ rmd_status rmd_renderer_guide_stats(const rmd_renderer *r, rmd_guide_stats *out)
 rmd_status rmd_renderer_guide_params(rmd_renderer *r, float *params, int32_t write) {
     if (!r || !params || write < 0 || write > 1) return fail(RMD_ERROR_INVALID_ARGUMENT, "invalid argument");
     RMD_CUDA(cudaSetDevice(r->scene->ctx->device));
-    auto &g = r->guide;
-    if (!g.net.allocated()) RMD_CUDA(g.net.allocate());
-    if (write) {
-        for (int i = 0; i < GUIDE_PARAMS; i++)
-            if (!std::isfinite(params[i])) return fail(RMD_ERROR_INVALID_ARGUMENT, "non-finite guide parameter");
-        RMD_CUDA(g.net.setParams(params, r->scene->ctx->stream));
-        g.initialised = true;
-        g.stats = rmd_guide_stats{};
-    } else {
-        if (!g.initialised) return fail(RMD_ERROR_INVALID_ARGUMENT, "the guide has not been set up");
-        RMD_CUDA(g.net.getParams(params, r->scene->ctx->stream));
-    }
-    return RMD_OK;
+    return guideParams(r->guide, params, write, r->scene->ctx->stream);
 }
 
 // --------------------------------------------------------------------- test hooks
@@ -1278,13 +1315,14 @@ static rmd_status batchAllocatePool(rmd_batch *b) {
     RMD_CUDA(b->pool.alloc(pathPoolBytes(b->capacity)));
     RMD_CUDA(b->counters.alloc(sizeof(Counters)));
     RMD_CUDA(cudaMemset(b->counters.ptr, 0, sizeof(Counters)));
-    return RMD_OK;
+    return guideBuffers(b->guide, b->capacity, b->counters.as<Counters>());
 }
 
 static PathPool batchPoolView(const rmd_batch *b) {
     PathPool pool = carvePathPool(b->pool.ptr, b->capacity);
     pool.views = b->viewTable.as<BatchView>();
     pool.numViews = (uint32_t)b->views.size();
+    applyGuide(b->guide, b->capacity, pool);
     return pool;
 }
 
@@ -1396,6 +1434,7 @@ rmd_status rmd_batch_create(rmd_context *ctx, const rmd_scene_desc *descs, int32
     RMD_CUDA(cudaMemset(b->film.ptr, 0, b->film.bytes));
     RMD_CUDA(b->resolve.alloc((size_t)offset * 3 * sizeof(float)));
     b->capacity = poolSize ? poolSize : (1u << 21);
+    if (b->capacity > BATCH_MAX_CAPACITY) return fail(RMD_ERROR_INVALID_ARGUMENT, "batch pools hold at most 2^22 paths");
     rmd_status r = batchAllocatePool(b.get());
     if (r != RMD_OK) return r;
     RMD_CUDA(cudaMallocHost((void **)&b->hostCounters, sizeof(Counters)));
@@ -1421,7 +1460,7 @@ rmd_status rmd_batch_reset(rmd_batch *b) {
 // every 4 iterations) or, with `handle`, as the body of a graph while loop
 // (2 iterations and the condition kernel).
 static rmd_status batchEnqueueIterations(rmd_batch *b, const PathPool &pool, const FrameParams &fp, ShadeParams &sp,
-                                         int iterations, cudaStream_t st) {
+                                         const GuideNetView &net, int iterations, cudaStream_t st) {
     Counters *cnt = b->counters.as<Counters>();
     const int tb = b->ctx->smCount * b->traceBlocksPerSm;
     const int rb = std::min<int>((b->capacity + 255) / 256, b->ctx->smCount * 8);
@@ -1430,6 +1469,9 @@ static rmd_status batchEnqueueIterations(rmd_batch *b, const PathPool &pool, con
         const uint32_t cur = (uint32_t)k & 1u;
         RMD_CUDA(rmdLaunchFilmRegen(b->scenes[0]->dctx, pool, fp, cnt, cur, rb, st));
         RMD_CUDA(rmdLaunchTraceClosest(nullptr, nullptr, pool, cnt, cur, tb, st));
+        if (pool.guide)
+            RMD_CUDA(rmdLaunchGuideInfer(b->scenes[0]->dctx, pool, cnt, cur, fp.guideDepth, net, pool.guide,
+                                         b->ctx->smCount * 2, st));
         sp.cur = cur;
         RMD_CUDA(cudaLaunchKernel((const void *)b->shade, dim3(b->shadeBlocks), dim3(128), shadeArgs, 0, st));
         RMD_CUDA(rmdLaunchTraceShadow(nullptr, nullptr, pool, cnt, cur, tb, st));
@@ -1466,6 +1508,17 @@ rmd_status rmd_batch_render(rmd_batch *b, const rmd_render_settings *s) {
     fp.filmFp64 = s->film_fp64 ? 1 : 0;
     fp.film = b->film.as<float4>();
     fp.film64 = b->film64.as<double>();
+    // guiding (all views of one scene)
+    GuideState &guide = b->guide;
+    GuideNetView net{};
+    if (guide.settings.sampling || guide.settings.training) {
+        rmd_status gs = guideBuffers(guide, b->capacity, b->counters.as<Counters>());
+        if (gs != RMD_OK) return gs;
+        net = guide.net.view(guide.frameMin, guide.frameInvExtent);
+        fp.guideDepth = guide.settings.sampling ? guide.settings.guided_depth : 0u;
+        fp.guideSceneMin = guide.frameMin;
+        fp.guideSceneInvExtent = guide.frameInvExtent;
+    }
     const PathPool pool = batchPoolView(b);
     Counters *cnt = b->counters.as<Counters>();
     ShadeParams sp;
@@ -1479,12 +1532,13 @@ rmd_status rmd_batch_render(rmd_batch *b, const rmd_render_settings *s) {
 
     RMD_CUDA(cudaEventRecord(b->ev[0], st));
     RMD_CUDA(rmdLaunchFrameInit(pool, cnt, firstPath, firstPath + numPaths, st));
-    uint64_t iterations = 0;
-    if (b->useGraph) {
+    uint64_t iterations = 0, trainSteps = 0;
+    // training steps run between counter checks, so a training batch uses the host-driven loop
+    if (b->useGraph && !guide.settings.training) {
         // the graph depends on everything but the sample range (frame init sets that)
         const std::vector<uint64_t> key = {s->max_depth, s->sampling_mode, s->rng, s->seed, (uint64_t)fp.filmFp64,
                                            maxIters, (uint64_t)b->capacity, (uint64_t)b->shadeMinBlocks,
-                                           (uint64_t)b->traceBlocksPerSm};
+                                           (uint64_t)b->traceBlocksPerSm, (uint64_t)fp.guideDepth};
         if (!b->graphExec || b->graphKey != key) {
             if (b->graphExec) cudaGraphExecDestroy(b->graphExec);
             if (b->graph) cudaGraphDestroy(b->graph);
@@ -1503,7 +1557,7 @@ rmd_status rmd_batch_render(rmd_batch *b, const rmd_render_settings *s) {
             cudaGraph_t body = cp.conditional.phGraph_out[0];
             // the body: two iterations (both parities) and the condition kernel
             RMD_CUDA(cudaStreamBeginCaptureToGraph(st, body, nullptr, nullptr, 0, cudaStreamCaptureModeThreadLocal));
-            rmd_status e = batchEnqueueIterations(b, pool, fp, sp, 2, st);
+            rmd_status e = batchEnqueueIterations(b, pool, fp, sp, net, 2, st);
             cudaError_t ce = e == RMD_OK ? rmdLaunchLoopCondition(cnt, handle, 2, (uint32_t)maxIters, st) : cudaSuccess;
             cudaGraph_t captured = nullptr;
             cudaError_t endErr = cudaStreamEndCapture(st, &captured);
@@ -1526,7 +1580,7 @@ rmd_status rmd_batch_render(rmd_batch *b, const rmd_render_settings *s) {
     } else {
         bool done = false;
         while (!done) {
-            rmd_status e = batchEnqueueIterations(b, pool, fp, sp, 4, st);
+            rmd_status e = batchEnqueueIterations(b, pool, fp, sp, net, 4, st);
             if (e != RMD_OK) return e;
             iterations += 4;
             RMD_CUDA(cudaMemcpyAsync(b->hostCounters, cnt, sizeof(Counters), cudaMemcpyDeviceToHost, st));
@@ -1536,6 +1590,7 @@ rmd_status rmd_batch_render(rmd_batch *b, const rmd_render_settings *s) {
                 b->stats.errors = h.errors;
                 return fail(RMD_ERROR_QUEUE_OVERFLOW, "device error flags " + std::to_string(h.errors));
             }
+            if ((e = guideTrainStep(guide, h, cnt, net, b->ctx->smCount, st, trainSteps)) != RMD_OK) return e;
             if (h.pathsDone >= numPaths) done = true;
             else if (iterations > maxIters) return fail(RMD_ERROR_WATCHDOG, "render did not drain in the iteration bound");
         }
@@ -1552,6 +1607,32 @@ rmd_status rmd_batch_render(rmd_batch *b, const rmd_render_settings *s) {
     b->stats.iterations = iterations;
     b->stats.ms_total = ms;
     b->samples = std::max<uint64_t>(b->samples, firstSample + s->spp);
+    if (trainSteps) return guideReadLoss(guide);
+    return RMD_OK;
+}
+
+rmd_status rmd_batch_set_guide(rmd_batch *b, const rmd_guide_settings *settings) {
+    if (!b || !settings) return fail(RMD_ERROR_INVALID_ARGUMENT, "NULL argument");
+    const int scene = b->views[0].scene;
+    for (const auto &v : b->views)
+        if (v.scene != scene)
+            return fail(RMD_ERROR_INVALID_ARGUMENT, "guiding needs every view of the batch on one scene");
+    RMD_CUDA(cudaSetDevice(b->ctx->device));
+    rmd_status st = setGuide(b->guide, settings, b->ctx->stream, b->counters.as<Counters>());
+    if (st != RMD_OK) return st;
+    b->guideScene = scene;
+    guideFrame(b->scenes[scene].get(), b->guide.frameMin, b->guide.frameInvExtent);
+    if (b->graphExec) {  // the graph gains or loses the inference launches
+        cudaGraphExecDestroy(b->graphExec);
+        b->graphExec = nullptr;
+    }
+    b->graphKey.clear();
+    return guideBuffers(b->guide, b->capacity, b->counters.as<Counters>());
+}
+
+rmd_status rmd_batch_guide_stats(const rmd_batch *b, rmd_guide_stats *out) {
+    if (!b || !out) return fail(RMD_ERROR_INVALID_ARGUMENT, "NULL argument");
+    *out = b->guide.stats;
     return RMD_OK;
 }
 
@@ -1642,7 +1723,7 @@ rmd_status rmd_batch_autotune(rmd_batch *b, const rmd_render_settings *settings,
     const uint32_t cap0 = b->capacity;
     uint32_t bestCap = cap0;
     for (uint32_t cap : {cap0 / 2, cap0 * 2}) {
-        if (cap < (1u << 16)) continue;
+        if (cap < (1u << 16) || cap > BATCH_MAX_CAPACITY) continue;
         size_t freeB = 0, totalB = 0;
         if (cudaMemGetInfo(&freeB, &totalB) != cudaSuccess || pathPoolBytes(cap) > freeB / 2) continue;
         b->capacity = cap;

@@ -75,3 +75,28 @@ def test_batch_rejects_bad_views(gpu_ctx, batch_setup):
         api.Batch(gpu_ctx, descs, [{"scene": 2, "width": 8, "height": 8}])
     with pytest.raises(api.RmdError):
         api.Batch(gpu_ctx, descs, [{"scene": 0, "width": 0, "height": 8}])
+
+
+def test_batch_guiding(gpu_ctx, batch_setup):
+    """Guiding in a batch whose views show one scene: training runs (host
+    loop), sampling-only renders run in the graph, and both converge to the
+    plain tracer's images; a batch over two scenes refuses the guide."""
+    descs, views = batch_setup
+    with pytest.raises(api.RmdError):
+        api.Batch(gpu_ctx, descs, views).set_guide()
+    one = [v for v in views if v["scene"] == 0]
+    b = api.Batch(gpu_ctx, descs[:1], one)
+    b.set_guide(sampling=True, training=True, batch_size=1 << 14, steps_per_batch=4, seed=3)
+    b.render(spp=1024, max_depth=8, seed=2, film_fp64=True)
+    st = b.guide_stats()
+    assert st["steps"] > 10 and np.isfinite(st["last_loss"])
+    b.set_guide(sampling=True, training=False, batch_size=1 << 14)
+    b.render(spp=1024, max_depth=8, seed=3, film_fp64=True)  # graph launch with inference inside
+    for i, v in enumerate(one):
+        plain = api.Renderer(api.Scene(gpu_ctx, descs[0]), v["width"], v["height"])
+        if "camera" in v:
+            plain.set_camera(v["camera"])
+        plain.render(spp=2048, max_depth=8, seed=1, film_fp64=True)
+        a = plain.film64() / 2048
+        g = b.film64(i) / 2048
+        assert abs(g.mean() / a.mean() - 1) < 0.02, (i, a.mean(), g.mean())
