@@ -28,6 +28,12 @@ weak scaling, no collective on the data path.
            squared) traced as one batch (one wavefront, one CUDA-graph
            launch per step), 32 spp, depth 10, autotuned; value = aggregate
            Mpaths/s, with each instance's paths and resolution in `instances`.
+--workload config5: 16 glossy rooms tiled 4 x 4 (3.95 M triangles, metallic
+           Bernoulli(0.5), 64 small emitters of radiance 500), 8 views in one
+           batch, depth 20: plain batch at 1,024 spp against the guided batch
+           (online training), relMSE per view against an FP64 oracle of
+           --oracle-spp spp; at --c5-size per view (3840x2160 is the full
+           size; the default is reduced to keep the oracle tractable).
 --impl reference times the reference's own CPU implementation of the path
 (its device code built for the host, oracle/_ref, all host cores; the oracle
 restatement when that build is absent) on a bounded sample of the workload.
@@ -274,6 +280,80 @@ def run_batch(args, ctx=None, steps=None, warmup=None) -> dict:
     return line
 
 
+def run_config5(args) -> dict:
+    """Config 5: guided + batched, 8 views of the 4 x 4 glossy rooms."""
+    from raymond_b200 import api, scenes
+    from raymond_b200._abi import SceneDesc
+    from raymond_b200.metrics import relmse
+
+    W, H = (int(x) for x in args.c5_size.split("x"))
+    depth, chunk = 20, 32
+    t0 = time.perf_counter()
+    desc = SceneDesc(scenes.glossy_rooms_grid(seed=1))
+    cams = scenes.grid_views(8)
+    views = [{"scene": 0, "width": W, "height": H, "camera": c} for c in cams]
+    ctx = api.Context(0)
+
+    def batch():
+        return api.Batch(ctx, [desc], views)
+    oracle = batch()
+    build_s = time.perf_counter() - t0
+    per_call = max(1, min(args.oracle_spp, (1 << 27) // (W * H * 8)))
+    done, oracle_ms = 0, 0.0
+    while done < args.oracle_spp:
+        n = min(per_call, args.oracle_spp - done)
+        oracle.render(spp=n, max_depth=depth, film_fp64=True, seed=77)
+        oracle_ms += oracle.stats()["ms_total"]
+        done += n
+    refs = [oracle.film64(v) / args.oracle_spp for v in range(8)]
+    oracle.close()
+
+    def errors(b):
+        return [relmse(b.film(v, normalize=True), refs[v]) for v in range(8)]
+    plain = batch()
+    plain_ms = 0.0
+    for _ in range(GUIDED_PLAIN_SPP // chunk):
+        plain.render(spp=chunk, max_depth=depth, seed=1)
+        plain_ms += plain.stats()["ms_total"]
+    e_plain = errors(plain)
+    plain.close()
+    g = batch()
+    settings = {"batch_size": 1 << 20, "learning_rate": 1e-3}
+    g.set_guide(sampling=True, training=True, seed=1, **settings)
+    ms, spp, parity, curve = 0.0, 0, None, []
+    target = float(np.mean(e_plain))
+    while ms < 3 * plain_ms:
+        g.render(spp=chunk, max_depth=depth, seed=2)
+        ms += g.stats()["ms_total"]
+        spp += chunk
+        e = errors(g)
+        curve.append((spp, ms, float(np.mean(e))))
+        if parity is None and np.mean(e) <= target:
+            parity = (spp, ms)
+            break
+    e_guided = errors(g)
+    st = g.guide_stats()
+    g.close()
+    return {
+        "metric": "time to the plain tracer's 1024-spp relMSE, guided batch (config 5)",
+        "value": parity[1] / plain_ms if parity else None, "unit": "fraction of the plain batch's time",
+        "higher_is_better": False, "n_gpus": 1,
+        "config": {"workload": f"glossy_rooms_grid_4x4_8views_{W}x{H}_depth{depth}",
+                   "triangles": desc_triangles(desc), "views": 8, "oracle_spp": args.oracle_spp,
+                   "full_size": "3840x2160 per view", "reduced": (W, H) != (3840, 2160)},
+        "oracle_device_s": oracle_ms / 1e3, "scene_build_s": build_s,
+        "plain": {"spp": GUIDED_PLAIN_SPP, "ms": plain_ms, "relmse_per_view": e_plain, "relmse_mean": target},
+        "guided": {"spp": spp, "ms": ms, "relmse_per_view": e_guided, "relmse_mean": float(np.mean(e_guided)),
+                   "parity": {"spp": parity[0], "ms": parity[1]} if parity else None, "adam_steps": st["steps"],
+                   "settings": settings,
+                   "curve": [{"spp": a, "ms": round(b_, 1), "relmse": c} for a, b_, c in curve[::4]]},
+    }
+
+
+def desc_triangles(desc) -> int:
+    return int(sum(len(s["indices"]) for s in desc.scene["shapes"]))
+
+
 def guided_leg(api, ctx, oracle_spp: int, size=(GUIDED_W, GUIDED_H)) -> dict:
     """Equal-time relMSE of the guided tracer against the plain one (config 4)."""
     from raymond_b200 import scenes
@@ -352,7 +432,8 @@ def main():
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-guided", action="store_true")
     ap.add_argument("--no-batch", action="store_true")
-    ap.add_argument("--workload", default="plain", choices=["plain", "batch", "guided", "guided-render"])
+    ap.add_argument("--workload", default="plain", choices=["plain", "batch", "guided", "guided-render", "config5"])
+    ap.add_argument("--c5-size", default="480x270", help="config 5: per-view resolution (full size 3840x2160)")
     ap.add_argument("--guided-size", default=f"{GUIDED_W}x{GUIDED_H}", help="guided leg resolution (profiling runs)")
     ap.add_argument("--oracle-spp", type=int, default=GUIDED_ORACLE_SPP, help="guided leg: oracle samples")
     ap.add_argument("--no-autotune", action="store_true")
@@ -364,6 +445,11 @@ def main():
         return run_reference(args)
     if args.workload == "batch":
         print(json.dumps(run_batch(args)), flush=True)
+        return
+    if args.workload == "config5":
+        if args.oracle_spp == GUIDED_ORACLE_SPP:
+            args.oracle_spp = 8192
+        print(json.dumps(run_config5(args)), flush=True)
         return
     guided_size = tuple(int(x) for x in args.guided_size.split("x"))
     if args.workload == "guided-render":  # the guided tracer alone, --steps chunks of 32 spp (profiling runs)

@@ -412,3 +412,84 @@ def glossy_room(seed: int = 1, num_boxes: int = 136, tess: int = 11, num_materia
         "world_shader": 0,
         "envmap_exponent": envmap_exponent,
     }
+
+
+def glossy_rooms_grid(seed: int = 1, grid: int = 4, boxes_per_room: int = 170, tess: int = 11,
+                      num_materials: int = 64, emitters: int = 64, envmap_exponent: int = 8) -> dict[str, Any]:
+    """grid x grid glossy rooms (each 10 x 10 x 4, a 0.5 x 0.5 window in its
+    z-far wall onto an environment of radiance 5) side by side, furnished with
+    seeded tessellated boxes (170 boxes of 1,452 triangles per room: about 4 M
+    triangles for 4 x 4), surfaces Principled with roughness U[0.01, 0.5] and
+    metallic Bernoulli(0.5), and `emitters` small emissive ceiling quads
+    (0.05 x 0.05, radiance 500) spread over the rooms.  The scene's camera
+    looks into the first room; `grid_views` gives cameras for the others."""
+    rng = np.random.default_rng(seed)
+    mats = []
+    for i in range(num_materials + 6):
+        mats.append((f"mat{i}", M.principled(base_color=tuple(rng.uniform(0.2, 0.9, 3)),
+                                             roughness=float(rng.uniform(0.01, 0.5)),
+                                             metallic=float(rng.uniform() < 0.5))))
+    emit = len(mats)
+    mats.append(("emitter", M.emission((1.0, 1.0, 1.0, 1.0), 500.0)))
+    W, D, Hh = 10.0, 10.0, 4.0
+    shapes = []
+    for gx in range(grid):
+        for gz in range(grid):
+            ox, oz = gx * W, gz * D
+            walls = [
+                quad_mesh([[ox, 0, oz], [ox + W, 0, oz], [ox + W, 0, oz + D], [ox, 0, oz + D]], [0, 1, 0], num_materials),
+                quad_mesh([[ox, Hh, oz], [ox + W, Hh, oz], [ox + W, Hh, oz + D], [ox, Hh, oz + D]], [0, -1, 0],
+                          num_materials + 1),
+                quad_mesh([[ox, 0, oz], [ox + W, 0, oz], [ox + W, Hh, oz], [ox, Hh, oz]], [0, 0, 1], num_materials + 2),
+                quad_mesh([[ox, 0, oz], [ox, Hh, oz], [ox, Hh, oz + D], [ox, 0, oz + D]], [1, 0, 0], num_materials + 3),
+                quad_mesh([[ox + W, 0, oz], [ox + W, Hh, oz], [ox + W, Hh, oz + D], [ox + W, 0, oz + D]], [-1, 0, 0],
+                          num_materials + 4),
+            ]
+            wx0, wx1, wy0, wy1, zD = ox + 4.75, ox + 5.25, 2.25, 2.75, oz + D
+            for (x0, x1, y0, y1) in [(ox, ox + W, 0, wy0), (ox, ox + W, wy1, Hh), (ox, wx0, wy0, wy1),
+                                     (wx1, ox + W, wy0, wy1)]:
+                walls.append(quad_mesh([[x0, y0, zD], [x1, y0, zD], [x1, y1, zD], [x0, y1, zD]], [0, 0, -1],
+                                       num_materials + 5))
+            n = boxes_per_room
+            size = np.stack([rng.uniform(0.3, 1.2, n), rng.uniform(0.2, 1.5, n), rng.uniform(0.3, 1.2, n)],
+                            1).astype(np.float32)
+            pos = np.stack([rng.uniform(0.1, W - 1.3, n), np.zeros(n), rng.uniform(0.1, D - 1.3, n)], 1).astype(np.float32)
+            floating = rng.uniform(0, 1, n) < 0.3
+            pos[floating, 1] = rng.uniform(0.5, Hh - 1.6, floating.sum())
+            near_cam = (np.abs(pos[:, 0] + 0.5 * size[:, 0] - 2.0) < 1.5) & (np.abs(pos[:, 2] + 0.5 * size[:, 2] - 1.5) < 1.5)
+            pos[near_cam, 0] += 3.0
+            hi = np.minimum(pos + size, [W - 0.05, Hh - 0.05, D - 0.05]).astype(np.float32)
+            pos += np.array([ox, 0, oz], np.float32)
+            hi += np.array([ox, 0, oz], np.float32)
+            shapes.append(merge_meshes(walls + [_boxes_mesh(pos, hi, rng.integers(0, num_materials, n), tess)]))
+    # small emitters on the ceilings, facing down
+    quads = []
+    for e in range(emitters):
+        cx, cz = rng.uniform(0.5, grid * W - 0.5), rng.uniform(0.5, grid * D - 0.5)
+        y, h = Hh - 0.01, 0.025
+        quads.append(quad_mesh([[cx - h, y, cz - h], [cx + h, y, cz - h], [cx + h, y, cz + h], [cx - h, y, cz + h]],
+                               [0, -1, 0], emit))
+    shapes.append(merge_meshes(quads))
+    ident = _identity()
+    return {
+        "name": "glossy_rooms_grid",
+        "materials": mats,
+        "light_materials": [("world", M.world((1.0, 1.0, 1.0, 1.0), 5.0))],
+        "shapes": shapes,
+        "entities": [{"shape": i, "matrix": ident, "visibility": VISIBLE_ALL} for i in range(len(shapes))],
+        "camera": grid_views(1, grid)[0],
+        "world_shader": 0,
+        "envmap_exponent": envmap_exponent,
+    }
+
+
+def grid_views(n: int, grid: int = 4) -> list[dict[str, Any]]:
+    """n cameras of glossy_rooms_grid, each inside a different room looking
+    across it towards its window."""
+    out = []
+    for k in range(n):
+        gx, gz = k % grid, (k // grid) % grid
+        ox, oz = gx * 10.0, gz * 10.0
+        out.append({"transform": look_at((ox + 2.0, 1.6, oz + 1.5), (ox + 6.0, 1.4, oz + 9.0)), "near_clip": 1e-3,
+                    "far_clip": 100.0, "focal_length": 1.2})
+    return out
