@@ -379,6 +379,15 @@ def render_noalloc(scene: Scene, camera: dict[str, Any], width: int, height: int
                                    pool_size))
 
 
+def load_scene(ctx: "Context", path) -> tuple["Scene", tuple[int, int] | None]:
+    """A scene from the reference's on-disk format (exporter JSON + PLY meshes,
+    raymond_b200.loader) and the file's render resolution."""
+    from . import loader
+
+    sc, size = loader.load_scene(path)
+    return Scene(ctx, sc), size
+
+
 def guide_param_count() -> int:
     return int(lib().rmd_guide_param_count())
 
