@@ -79,9 +79,7 @@ GUIDED_W, GUIDED_H, GUIDED_DEPTH, GUIDED_ORACLE_SPP, GUIDED_PLAIN_SPP, GUIDED_CH
 CPU_BASELINE_SPP = 16  # CPU sample: 16 one-spp frames of the full image (about 10-20 s on 16 cores)
 
 
-def rank_info():
-    return int(os.environ.get("RANK", "0")), int(os.environ.get("WORLD_SIZE", "1")), \
-        int(os.environ.get("LOCAL_RANK", "0"))
+from raymond_b200.multi import rank_info, sample_range, shard_views, max_over_ranks, sum_over_ranks  # noqa: E402
 
 
 class ClockSampler:
@@ -228,15 +226,19 @@ def run_batch(args, ctx=None, steps=None, warmup=None) -> dict:
     from raymond_b200 import api, scenes
     from raymond_b200._abi import SceneDesc
 
+    rank, world, local = rank_info()
+    mine = set(shard_views(BATCH_INSTANCES, rank, world))  # instances of this rank (no exchange)
     rng = np.random.default_rng(3)
     t0 = time.perf_counter()
     descs, views, targets = [], [], []
     for i in range(BATCH_INSTANCES):
-        sc, res, target = batch_instance(i, rng)
+        sc, res, target = batch_instance(i, rng)  # every rank draws all, so instance i is the same everywhere
+        if i not in mine:
+            continue
         descs.append(SceneDesc(sc))
-        views.append({"scene": i, "width": res, "height": res})
+        views.append({"scene": len(descs) - 1, "width": res, "height": res})
         targets.append(target)
-    ctx = ctx or api.Context(0)
+    ctx = ctx or api.Context(local)
     steps = args.steps if steps is None else steps
     warmup = args.warmup if warmup is None else warmup
     b = api.Batch(ctx, descs, views)
@@ -260,12 +262,15 @@ def run_batch(args, ctx=None, steps=None, warmup=None) -> dict:
     clocks = sampler.stop()
     tris = [int(sum(len(s["indices"]) for s in d.scene["shapes"])) for d in descs]
     pixels = [v["width"] * v["height"] for v in views]
+    tot_ms, = max_over_ranks([tot_ms])
+    paths, segments = (int(x) for x in sum_over_ranks([float(paths), float(segments)]))
     value = paths / (tot_ms / 1e3) / 1e6
     line = {
-        "metric": "Mpaths/s (batched, config 3)", "value": value, "unit": "Mpaths/s", "n_gpus": 1,
+        "metric": "Mpaths/s (batched, config 3)", "value": value, "unit": "Mpaths/s", "n_gpus": world,
         "steps": steps, "warmup": warmup, "ms_per_step": tot_ms / steps, "higher_is_better": True,
-        "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic (seeded procedural scenes)",
+        "scaling": "strong", "vs_baseline": None, "dtype": "f32", "data": "synthetic (seeded procedural scenes)",
         "config": {"workload": f"batch_{BATCH_INSTANCES}_instances_{BATCH_SPP}spp_depth{BATCH_DEPTH}",
+                   "parallelism": f"{world} ranks x round-robin instances",
                    "instances": BATCH_INSTANCES, "total_pixels": sum(pixels), "total_triangles": sum(tris),
                    "launch": "one wavefront, one CUDA-graph launch per step (device-driven while loop)",
                    "l2": "inputs larger than L2 (path pool + BVHs + films)"},
@@ -444,7 +449,16 @@ def main():
     if args.impl == "reference":
         return run_reference(args)
     if args.workload == "batch":
-        print(json.dumps(run_batch(args)), flush=True)
+        rank, world, _ = rank_info()
+        if world > 1:
+            import datetime
+            import torch.distributed as dist
+            dist.init_process_group("gloo", timeout=datetime.timedelta(seconds=600))
+        line = run_batch(args)
+        if rank == 0:
+            print(json.dumps(line), flush=True)
+        if world > 1:
+            dist.destroy_process_group()
         return
     if args.workload == "config5":
         if args.oracle_spp == GUIDED_ORACLE_SPP:
@@ -495,7 +509,7 @@ def main():
     film_host = np.zeros((H, W, 3), np.float32)
 
     def step(k, e2e=False):
-        first = (rank + world * k) * SPP
+        first, _ = sample_range(rank, world, k, SPP)
         if e2e:
             r.set_camera(cam)  # host -> device: camera
         else:
@@ -525,11 +539,7 @@ def main():
         step(k, e2e=True)
     e2e_s = max(time.perf_counter() - t0, 1e-9)
     if dist:
-        import torch
-
-        t = torch.tensor([tot_ms, e2e_s], dtype=torch.float64)
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        tot_ms, e2e_s = float(t[0]), float(t[1])
+        tot_ms, e2e_s = max_over_ranks([tot_ms, e2e_s])
         dist.barrier()
     if rank != 0:
         if dist:
