@@ -24,6 +24,7 @@ constexpr float SHADOW_EPS = 0.001f;  // device/constants.hpp:3
 constexpr uint32_t ERR_QUEUE_OVERFLOW = 1u;
 constexpr uint32_t ERR_STACK_OVERFLOW = 2u;
 constexpr uint32_t ERR_LOOP_BOUND = 4u;  // a device-driven render loop reached its iteration bound
+constexpr uint32_t ERR_GUIDE_TIMEOUT = 8u;  // a guide inference CTA's tensor-core wait expired
 
 // target of a shadow ray: position of its path in S[p ^ 1], or in the finish
 // list when this bit is set

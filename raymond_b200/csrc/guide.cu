@@ -3,11 +3,12 @@
 // (forward, loss gradient, backward, Adam) on the records the tracer
 // produces.  No counterpart in the reference.
 //
-// Each warp processes 16 samples at a time with mma.sync m16n8k16 (BF16
-// inputs, FP32 accumulation): activations live in per-warp shared memory as
-// BF16 rows, weights are read as BF16 [out][in] rows through the read-only
-// cache.  Training accumulates the weight gradient of a block in shared
-// memory (FP32) and adds it to the global gradient once per block.
+// Inference runs on the 5th-generation tensor cores (tcgen05.mma, TMEM
+// accumulators, one thread per sample; see the tcgen05 inference core).
+// Training: each warp processes 16 samples at a time with mma.sync m16n8k16
+// (BF16 inputs, FP32 accumulation), activations in per-warp shared memory as
+// BF16 rows; the block's weight gradient accumulates in shared memory (FP32)
+// and is added to the global gradient once per block.
 #include <cuda_runtime.h>
 
 #include <algorithm>
@@ -262,48 +263,6 @@ struct RecordBatch {
     }
 };
 
-// ------------------------------------------------------- inference core
-// Inference keeps activations in registers: the FP32 accumulator fragment of
-// an m16n8k16 product (rows g, g + 8; columns 2t, 2t + 1 of an n8 tile) is,
-// rounded to BF16 and paired, exactly the A fragment of the next layer for
-// the k16 block made of two adjacent n8 tiles.  A warp runs 32 samples (two
-// m16 tiles) so every weight fragment, read from shared memory, feeds two
-// products, and all 32 lanes decode one sample each at the end.
-constexpr int kInferWarps = 8;  // 8 warps share one copy of the weights; 2 blocks per SM (registers)
-constexpr int kLdW1 = GUIDE_INPUTS + 8, kLdW = GUIDE_HIDDEN + 8;  // padded weight rows (conflict-free fragments)
-constexpr int kLdOut = GUIDE_OUTPUTS + 1;                          // odd stride: conflict-free per-sample reads
-
-struct InferSmem {
-    uint16_t w1[GUIDE_HIDDEN * kLdW1];
-    uint16_t w2[GUIDE_HIDDEN * kLdW];
-    uint16_t w3[GUIDE_HIDDEN * kLdW];
-    uint16_t w4[GUIDE_OUTPUTS * kLdW];
-    float b[3 * GUIDE_HIDDEN + GUIDE_OUTPUTS];
-    float out[kInferWarps][32 * kLdOut];
-};
-
-// copies the bf16 weights (padded rows) and the biases into shared memory
-__device__ void loadInferWeights(InferSmem &sm, const GuideNetView &net) {
-    auto copy = [&](uint16_t *dst, const uint16_t *src, int rows, int cols, int ld) {
-        const int vecs = cols / 8;  // 16-byte vectors per row
-        for (int i = threadIdx.x; i < rows * vecs; i += blockDim.x) {
-            const int r = i / vecs, c = i - r * vecs;
-            *reinterpret_cast<uint4 *>(&dst[r * ld + 8 * c]) = __ldg(reinterpret_cast<const uint4 *>(&src[r * cols + 8 * c]));
-        }
-    };
-    copy(sm.w1, net.w[0], GUIDE_HIDDEN, GUIDE_INPUTS, kLdW1);
-    copy(sm.w2, net.w[1], GUIDE_HIDDEN, GUIDE_HIDDEN, kLdW);
-    copy(sm.w3, net.w[2], GUIDE_HIDDEN, GUIDE_HIDDEN, kLdW);
-    copy(sm.w4, net.w[3], GUIDE_OUTPUTS, GUIDE_HIDDEN, kLdW);
-    for (int i = threadIdx.x; i < 3 * GUIDE_HIDDEN + GUIDE_OUTPUTS; i += blockDim.x) {
-        const int l = min(i / GUIDE_HIDDEN, 3);
-        sm.b[i] = __ldg(&net.b[l][i - l * GUIDE_HIDDEN]);
-    }
-    __syncthreads();
-}
-
-__device__ __forceinline__ uint32_t packBf16(float lo, float hi) { return bf16Bits(lo) | (bf16Bits(hi) << 16); }
-
 // one-blob value of bin `bin` of a feature with `bins` bins
 __device__ __forceinline__ float oneBlob(float v, int bins, int bin) {
     const float d = v * (float)bins - ((float)bin + 0.5f);
@@ -311,100 +270,274 @@ __device__ __forceinline__ float oneBlob(float v, int bins, int bin) {
     return x * x;
 }
 
-// B fragment of W (row-major [n][k], padded stride ld) for n tile n0, k block k0
-__device__ __forceinline__ void loadBs(uint32_t b[2], const uint16_t *w, int ld, int n0, int k0, int g, int t) {
-    b[0] = *reinterpret_cast<const uint32_t *>(&w[(n0 + g) * ld + k0 + 2 * t]);
-    b[1] = *reinterpret_cast<const uint32_t *>(&w[(n0 + g) * ld + k0 + 8 + 2 * t]);
+// ------------------------------------------------ tcgen05 inference core
+// Inference on the 5th-generation tensor cores.  A CTA runs kTcPipes
+// independent pipelines of 128 threads; each pipeline takes 128 samples at a
+// time (M = 128), one thread per sample, and the pipelines share one copy of
+// the weights in shared memory.  Each layer is tcgen05.mma (kind::f16, BF16
+// operands from shared memory, FP32 accumulator in the pipeline's 64 columns
+// of tensor memory) issued by the pipeline's first thread; its completion is
+// committed to the pipeline's mbarrier; every thread then reads its own
+// sample's row of the accumulator (tcgen05.ld, TMEM lane = sample), applies
+// bias and ReLU and writes the BF16 row back to shared memory as the next
+// layer's A operand.  The output layer's row stays in the thread's
+// registers, so each thread decodes and packs its own sample's mixture.
+// While one pipeline runs its epilogue, the tensor core serves the others.
+//
+// Operand layout (the canonical K-major, no-swizzle layout of the UMMA
+// shared-memory descriptor): 8 x 16-byte "core matrices" (8 rows, 8 BF16
+// along K); element (r, k) of a [rows][K] operand sits at byte
+// (r / 8) * SBO + (k / 8) * 128 + (r % 8) * 16 + (k % 8) * 2, SBO = K / 8 * 128.
+constexpr int kTcPipes = 4;
+constexpr int kTcPipeThreads = 128;
+constexpr int kTcThreads = kTcPipes * kTcPipeThreads;
+constexpr uint32_t kTmemCols = 64 * kTcPipes;
+constexpr int kTcSpinLimit = 1 << 22;  // bounded waits: on expiry the pipeline flags an error and stops
+
+struct TcSmem {
+    uint16_t w1[GUIDE_HIDDEN * GUIDE_INPUTS];
+    uint16_t w2[GUIDE_HIDDEN * GUIDE_HIDDEN];
+    uint16_t w3[GUIDE_HIDDEN * GUIDE_HIDDEN];
+    uint16_t w4[GUIDE_OUTPUTS * GUIDE_HIDDEN];
+    uint16_t a[kTcPipes][kTcPipeThreads * GUIDE_INPUTS];  // each pipeline's A operand (inputs, then hidden)
+    float b[3 * GUIDE_HIDDEN + GUIDE_OUTPUTS];
+    unsigned long long mbar[kTcPipes];
+    uint32_t tmemBase;
+    int failed[kTcPipes];
+};
+
+__device__ __forceinline__ uint32_t smemU32(const void *p) { return (uint32_t)__cvta_generic_to_shared(p); }
+
+// two floats to packed BF16 (round to nearest even), hi in the upper half
+__device__ __forceinline__ uint32_t cvtBf16x2(float lo, float hi) {
+    uint32_t r;
+    asm("cvt.rn.bf16x2.f32 %0, %1, %2;\n" : "=r"(r) : "f"(hi), "f"(lo));
+    return r;
 }
 
-// accumulators (2 m tiles x 8 n tiles) -> bias, ReLU, bf16 A fragments (2 m tiles x 4 k blocks)
-__device__ __forceinline__ void hiddenToA(const float acc[2][8][4], const float *bias, uint32_t h[2][4][4], int t) {
-#pragma unroll
-    for (int mt = 0; mt < 2; mt++)
-#pragma unroll
-        for (int nt = 0; nt < 8; nt++) {
-            const float b0 = bias[nt * 8 + 2 * t], b1 = bias[nt * 8 + 2 * t + 1];
-            const uint32_t lo = packBf16(fmaxf(acc[mt][nt][0] + b0, 0.0f), fmaxf(acc[mt][nt][1] + b1, 0.0f));
-            const uint32_t hi = packBf16(fmaxf(acc[mt][nt][2] + b0, 0.0f), fmaxf(acc[mt][nt][3] + b1, 0.0f));
-            h[mt][nt >> 1][(nt & 1) * 2 + 0] = lo;  // a0 / a2: row g
-            h[mt][nt >> 1][(nt & 1) * 2 + 1] = hi;  // a1 / a3: row g + 8
-        }
+// byte offset of element (r, k) in a K-major canonical operand of width K
+__device__ __forceinline__ uint32_t canonOffset(int r, int k, int K) {
+    return (uint32_t)((r >> 3) * (K / 8) * 128 + (k >> 3) * 128 + (r & 7) * 16 + (k & 7) * 2);
 }
 
-// hidden 64 -> 64 layer on register fragments
-__device__ __forceinline__ void hiddenLayer(const uint32_t in[2][4][4], const uint16_t *w, const float *bias,
-                                            uint32_t out[2][4][4], int g, int t) {
-    float acc[2][8][4] = {};
-#pragma unroll
-    for (int kb = 0; kb < 4; kb++)
-#pragma unroll
-        for (int nt = 0; nt < 8; nt++) {
-            uint32_t b[2];
-            loadBs(b, w, kLdW, nt * 8, kb * 16, g, t);
-            mma16816(acc[0][nt], in[0][kb], b);
-            mma16816(acc[1][nt], in[1][kb], b);
-        }
-    hiddenToA(acc, bias, out, t);
+// UMMA shared-memory descriptor: K-major, no swizzle, LBO = 128 B between the
+// two 8-element K chunks of an instruction, SBO between 8-row groups
+__device__ __forceinline__ uint64_t ummaDesc(uint32_t addr, uint32_t sbo) {
+    uint64_t d = 0;
+    d |= (uint64_t)((addr >> 4) & 0x3fffu);
+    d |= (uint64_t)((128u >> 4) & 0x3fffu) << 16;  // leading byte offset
+    d |= (uint64_t)((sbo >> 4) & 0x3fffu) << 32;   // stride byte offset
+    d |= (uint64_t)1 << 46;                        // descriptor version (sm_100)
+    return d;                                      // base offset 0, layout type 0 (no swizzle)
 }
 
-// Forward pass of the 32 samples of a warp (lane l holds the features of
-// sample l); raw outputs (with bias) land in `out` rows of kLdOut floats.
-__device__ void inferWarp(const InferSmem &sm, const GuideFeatures &f, float *out, int lane) {
-    const int g = lane >> 2, t = lane & 3;
-    // layer 1: the one-blob inputs are built in the A fragment registers; k
-    // block kb covers 16 bins of one feature
-    float acc[2][8][4] = {};
+// instruction descriptor, kind::f16: BF16 A and B (K-major), FP32 D, M x N
+__device__ __forceinline__ uint32_t ummaInstr(int M, int N) {
+    return (1u << 4)                       // D format: F32
+           | (1u << 7) | (1u << 10)        // A, B format: BF16
+           | ((uint32_t)(N >> 3) << 17)    // N / 8
+           | ((uint32_t)(M >> 4) << 24);   // M / 16
+}
+
+__device__ __forceinline__ void umma(uint32_t tmem, uint64_t a, uint64_t b, uint32_t idesc, uint32_t accumulate) {
+    asm volatile(
+        "{\n.reg .pred p;\nsetp.ne.b32 p, %4, 0;\n"
+        "tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, p;\n}\n" ::"r"(tmem),
+        "l"(a), "l"(b), "r"(idesc), "r"(accumulate));
+}
+
+__device__ __forceinline__ void ummaCommit(uint32_t mbar) {
+    asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];\n" ::"r"(mbar)
+                 : "memory");
+}
+
+// waits for the mbarrier phase; false after kTcSpinLimit polls
+__device__ __forceinline__ bool mbarWait(uint32_t mbar, uint32_t phase) {
+    for (int i = 0; i < kTcSpinLimit; i++) {
+        uint32_t done;
+        asm volatile(
+            "{\n.reg .pred p;\nmbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\nselp.u32 %0, 1, 0, p;\n}\n"
+            : "=r"(done)
+            : "r"(mbar), "r"(phase)
+            : "memory");
+        if (done) return true;
+    }
+    return false;
+}
+
+// barrier of one pipeline's 128 threads (named barrier 1 + pipe)
+__device__ __forceinline__ void pipeSync(int pipe) {
+    asm volatile("bar.sync %0, %1;\n" ::"r"(1 + pipe), "r"(kTcPipeThreads) : "memory");
+}
+// pipeline barrier that also tells whether any of its threads passed true
+__device__ __forceinline__ bool pipeAny(int pipe, bool v) {
+    uint32_t r;
+    asm volatile(
+        "{\n.reg .pred p, q;\nsetp.ne.b32 p, %1, 0;\nbar.red.or.pred q, %2, %3, p;\nselp.u32 %0, 1, 0, q;\n}\n"
+        : "=r"(r)
+        : "r"((uint32_t)v), "r"(1 + pipe), "r"(kTcPipeThreads)
+        : "memory");
+    return r != 0;
+}
+
+__device__ __forceinline__ void tmemLd32(uint32_t taddr, float *v) {
+    uint32_t r[32];
+    asm volatile(
+        "tcgen05.ld.sync.aligned.32x32b.x32.b32 {%0,%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,%12,%13,%14,%15,"
+        "%16,%17,%18,%19,%20,%21,%22,%23,%24,%25,%26,%27,%28,%29,%30,%31}, [%32];\n"
+        : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]), "=r"(r[7]),
+          "=r"(r[8]), "=r"(r[9]), "=r"(r[10]), "=r"(r[11]), "=r"(r[12]), "=r"(r[13]), "=r"(r[14]), "=r"(r[15]),
+          "=r"(r[16]), "=r"(r[17]), "=r"(r[18]), "=r"(r[19]), "=r"(r[20]), "=r"(r[21]), "=r"(r[22]), "=r"(r[23]),
+          "=r"(r[24]), "=r"(r[25]), "=r"(r[26]), "=r"(r[27]), "=r"(r[28]), "=r"(r[29]), "=r"(r[30]), "=r"(r[31])
+        : "r"(taddr));
 #pragma unroll
-    for (int kb = 0; kb < GUIDE_INPUTS / 16; kb++) {
-        const int feature = kb < 6 ? kb >> 1 : kb - 3;
-        const int bins = kb < 6 ? 32 : 16;
-        const int bin0 = kb < 6 ? (kb & 1) * 16 : 0;
-        uint32_t a[2][4];
+    for (int i = 0; i < 32; i++) v[i] = __uint_as_float(r[i]);
+}
+__device__ __forceinline__ void tmemLd16(uint32_t taddr, float *v) {
+    uint32_t r[16];
+    asm volatile(
+        "tcgen05.ld.sync.aligned.32x32b.x16.b32 {%0,%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,%12,%13,%14,%15}, [%16];\n"
+        : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]), "=r"(r[7]),
+          "=r"(r[8]), "=r"(r[9]), "=r"(r[10]), "=r"(r[11]), "=r"(r[12]), "=r"(r[13]), "=r"(r[14]), "=r"(r[15])
+        : "r"(taddr));
 #pragma unroll
-        for (int mt = 0; mt < 2; mt++) {
-            const float vg = __shfl_sync(0xffffffffu, f.v[feature], mt * 16 + g);
-            const float vh = __shfl_sync(0xffffffffu, f.v[feature], mt * 16 + g + 8);
-            const int c = bin0 + 2 * t;
-            a[mt][0] = packBf16(oneBlob(vg, bins, c), oneBlob(vg, bins, c + 1));
-            a[mt][1] = packBf16(oneBlob(vh, bins, c), oneBlob(vh, bins, c + 1));
-            a[mt][2] = packBf16(oneBlob(vg, bins, c + 8), oneBlob(vg, bins, c + 9));
-            a[mt][3] = packBf16(oneBlob(vh, bins, c + 8), oneBlob(vh, bins, c + 9));
+    for (int i = 0; i < 16; i++) v[i] = __uint_as_float(r[i]);
+}
+__device__ __forceinline__ void tmemLdWait() { asm volatile("tcgen05.wait::ld.sync.aligned;\n" ::: "memory"); }
+__device__ __forceinline__ void tcFenceBefore() { asm volatile("tcgen05.fence::before_thread_sync;\n" ::: "memory"); }
+__device__ __forceinline__ void tcFenceAfter() { asm volatile("tcgen05.fence::after_thread_sync;\n" ::: "memory"); }
+__device__ __forceinline__ void asyncProxyFence() { asm volatile("fence.proxy.async.shared::cta;\n" ::: "memory"); }
+
+// copies a row-major [rows][K] bf16 weight matrix into the canonical layout
+__device__ void loadCanonical(uint16_t *dst, const uint16_t *src, int rows, int K) {
+    const int chunks = K / 8;
+    for (int i = threadIdx.x; i < rows * chunks; i += blockDim.x) {
+        const int r = i / chunks, c = i - r * chunks;
+        *reinterpret_cast<uint4 *>(reinterpret_cast<unsigned char *>(dst) + canonOffset(r, 8 * c, K)) =
+            __ldg(reinterpret_cast<const uint4 *>(&src[r * K + 8 * c]));
+    }
+}
+
+// The CTA's set-up: weights and biases into shared memory, the pipelines'
+// mbarriers, and kTmemCols columns of tensor memory (warp 0 allocates).
+__device__ void tcSetup(TcSmem &sm, const GuideNetView &net) {
+    loadCanonical(sm.w1, net.w[0], GUIDE_HIDDEN, GUIDE_INPUTS);
+    loadCanonical(sm.w2, net.w[1], GUIDE_HIDDEN, GUIDE_HIDDEN);
+    loadCanonical(sm.w3, net.w[2], GUIDE_HIDDEN, GUIDE_HIDDEN);
+    loadCanonical(sm.w4, net.w[3], GUIDE_OUTPUTS, GUIDE_HIDDEN);
+    for (int i = threadIdx.x; i < 3 * GUIDE_HIDDEN + GUIDE_OUTPUTS; i += blockDim.x) {
+        const int l = min(i / GUIDE_HIDDEN, 3);
+        sm.b[i] = __ldg(&net.b[l][i - l * GUIDE_HIDDEN]);
+    }
+    if (threadIdx.x == 0) {
+        for (int p = 0; p < kTcPipes; p++) {
+            sm.failed[p] = 0;
+            asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;\n" ::"r"(smemU32(&sm.mbar[p])), "r"(1) : "memory");
         }
+        asm volatile("fence.mbarrier_init.release.cluster;\n" ::: "memory");
+    }
+    if ((threadIdx.x >> 5) == 0) {
+        asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;\n" ::"r"(smemU32(&sm.tmemBase)),
+                     "r"(kTmemCols)
+                     : "memory");
+        asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;\n" ::: "memory");
+    }
+    asyncProxyFence();
+    tcFenceBefore();
+    __syncthreads();
+    tcFenceAfter();
+}
+
+__device__ void tcTeardown(TcSmem &sm, int pipe, uint32_t phase) {
+    if (sm.failed[pipe]) mbarWait(smemU32(&sm.mbar[pipe]), phase);  // a last bounded wait for work in flight
+    tcFenceBefore();
+    __syncthreads();
+    tcFenceAfter();
+    if ((threadIdx.x >> 5) == 0)
+        asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;\n" ::"r"(sm.tmemBase), "r"(kTmemCols)
+                     : "memory");
+}
+
+// One layer of a pipeline: D (its TMEM columns) = A (its sm.a, [128][K]) x
+// W^T (W [N][K]); the pipeline's first thread issues, all its threads wait.
+// False if the wait expired (the pipeline then stops).
+__device__ bool tcLayer(TcSmem &sm, int pipe, const uint16_t *w, int K, int N, uint32_t &phase) {
+    asyncProxyFence();  // the A rows written by the pipeline's threads, visible to the tensor core
+    tcFenceBefore();
+    pipeSync(pipe);
+    tcFenceAfter();
+    const uint32_t mbar = smemU32(&sm.mbar[pipe]);
+    if ((threadIdx.x & (kTcPipeThreads - 1)) == 0) {
+        const uint32_t idesc = ummaInstr(kTcPipeThreads, N);
+        const uint32_t aBase = smemU32(sm.a[pipe]), bBase = smemU32(w);
+        const uint32_t sbo = (uint32_t)(K / 8) * 128u;
+        const uint32_t tmem = sm.tmemBase + 64u * pipe;
+        for (int kb = 0; kb < K / 16; kb++)
+            umma(tmem, ummaDesc(aBase + kb * 256u, sbo), ummaDesc(bBase + kb * 256u, sbo), idesc, kb > 0);
+        ummaCommit(mbar);
+    }
+    const bool ok = mbarWait(mbar, phase);
+    phase ^= 1u;
+    tcFenceAfter();
+    if (!ok) atomicExch(&sm.failed[pipe], 1);
+    pipeSync(pipe);
+    return sm.failed[pipe] == 0;
+}
+
+// bias + ReLU of a 64-wide hidden row from TMEM, written as the next A row
+__device__ void tcHiddenEpilogue(uint16_t *a, uint32_t taddr, const float *bias, int row) {
+    float v[32];
 #pragma unroll
-        for (int nt = 0; nt < 8; nt++) {
-            uint32_t b[2];
-            loadBs(b, sm.w1, kLdW1, nt * 8, kb * 16, g, t);
-            mma16816(acc[0][nt], a[0], b);
-            mma16816(acc[1][nt], a[1], b);
+    for (int half = 0; half < 2; half++) {
+        tmemLd32(taddr + 32u * half, v);
+        tmemLdWait();
+#pragma unroll
+        for (int c = 0; c < 32; c += 8) {
+            uint32_t q[4];
+#pragma unroll
+            for (int k = 0; k < 4; k++)
+                q[k] = cvtBf16x2(fmaxf(v[c + 2 * k] + bias[32 * half + c + 2 * k], 0.0f),
+                                 fmaxf(v[c + 2 * k + 1] + bias[32 * half + c + 2 * k + 1], 0.0f));
+            *reinterpret_cast<uint4 *>(reinterpret_cast<unsigned char *>(a) +
+                                       canonOffset(row, 32 * half + c, GUIDE_HIDDEN)) = make_uint4(q[0], q[1], q[2], q[3]);
         }
     }
-    uint32_t h1[2][4][4], h2[2][4][4];
-    hiddenToA(acc, sm.b, h1, t);
-    hiddenLayer(h1, sm.w2, sm.b + GUIDE_HIDDEN, h2, g, t);
-    hiddenLayer(h2, sm.w3, sm.b + 2 * GUIDE_HIDDEN, h1, g, t);
-    // output layer: 48 columns (6 n tiles)
-    float o[2][6][4] = {};
+}
+
+// Forward pass of a pipeline's 128 samples (its thread r: sample r, features
+// f); writes the 48 raw outputs to `o`.  False if a wait expired.
+__device__ bool tcForward(TcSmem &sm, int pipe, const GuideFeatures &f, float *o, uint32_t &phase) {
+    const int row = threadIdx.x & (kTcPipeThreads - 1);
+    uint16_t *a = sm.a[pipe];
+    // one-blob input row: 20 chunks of 8 bins
 #pragma unroll
-    for (int kb = 0; kb < 4; kb++)
+    for (int c = 0; c < GUIDE_INPUTS / 8; c++) {
+        const int feature = c < 12 ? c >> 2 : 3 + ((c - 12) >> 1);
+        const int bins = c < 12 ? 32 : 16;
+        const int bin0 = c < 12 ? (c & 3) * 8 : ((c - 12) & 1) * 8;
+        const float v = f.v[feature];
+        uint32_t q[4];
 #pragma unroll
-        for (int nt = 0; nt < 6; nt++) {
-            uint32_t b[2];
-            loadBs(b, sm.w4, kLdW, nt * 8, kb * 16, g, t);
-            mma16816(o[0][nt], h1[0][kb], b);
-            mma16816(o[1][nt], h1[1][kb], b);
-        }
+        for (int k = 0; k < 4; k++) q[k] = cvtBf16x2(oneBlob(v, bins, bin0 + 2 * k), oneBlob(v, bins, bin0 + 2 * k + 1));
+        *reinterpret_cast<uint4 *>(reinterpret_cast<unsigned char *>(a) + canonOffset(row, 8 * c, GUIDE_INPUTS)) =
+            make_uint4(q[0], q[1], q[2], q[3]);
+    }
+    // this warp's 32 lanes (its quarter of the pipeline's rows) in the pipeline's 64 columns
+    const uint32_t taddr = sm.tmemBase + 64u * pipe + ((uint32_t)(row & ~31) << 16);
+    if (!tcLayer(sm, pipe, sm.w1, GUIDE_INPUTS, GUIDE_HIDDEN, phase)) return false;
+    tcHiddenEpilogue(a, taddr, sm.b, row);
+    if (!tcLayer(sm, pipe, sm.w2, GUIDE_HIDDEN, GUIDE_HIDDEN, phase)) return false;
+    tcHiddenEpilogue(a, taddr, sm.b + GUIDE_HIDDEN, row);
+    if (!tcLayer(sm, pipe, sm.w3, GUIDE_HIDDEN, GUIDE_HIDDEN, phase)) return false;
+    tcHiddenEpilogue(a, taddr, sm.b + 2 * GUIDE_HIDDEN, row);
+    if (!tcLayer(sm, pipe, sm.w4, GUIDE_HIDDEN, GUIDE_OUTPUTS, phase)) return false;
+    tmemLd32(taddr, o);
+    tmemLd16(taddr + 32u, o + 32);
+    tmemLdWait();
     const float *b4 = sm.b + 3 * GUIDE_HIDDEN;
 #pragma unroll
-    for (int mt = 0; mt < 2; mt++)
-#pragma unroll
-        for (int nt = 0; nt < 6; nt++) {
-            const int col = nt * 8 + 2 * t, r0 = mt * 16 + g, r1 = r0 + 8;
-            out[r0 * kLdOut + col] = o[mt][nt][0] + b4[col];
-            out[r0 * kLdOut + col + 1] = o[mt][nt][1] + b4[col + 1];
-            out[r1 * kLdOut + col] = o[mt][nt][2] + b4[col];
-            out[r1 * kLdOut + col + 1] = o[mt][nt][3] + b4[col + 1];
-        }
-    __syncwarp();
+    for (int c = 0; c < GUIDE_OUTPUTS; c++) o[c] += b4[c];
+    return true;
 }
 
 // ------------------------------------------------------------------ kernels
@@ -441,28 +574,32 @@ __global__ void __launch_bounds__(256) k_guide_features(Context ctx, PathPool po
 // Guide mixtures of the shading points of this iteration's hits on paths
 // shallower than guideDepth, by shading-order position (the shading kernel's
 // thread for hit q reads mixture q), from the features k_guide_features
-// stored.
-__global__ void __launch_bounds__(32 * kInferWarps) k_guide_infer(Counters *cnt, const uint4 *features,
-                                                               uint32_t guideDepth, GuideNetView net,
-                                                               GuideMixture *out) {
+// stored; tcgen05 tiles of 128 samples.  On an expired wait the CTA sets
+// ERR_GUIDE_TIMEOUT in the counters and stops.
+__global__ void __launch_bounds__(kTcThreads) k_guide_infer(Counters *cnt, const uint4 *features, uint32_t guideDepth,
+                                                         GuideNetView net, GuideMixture *out) {
     extern __shared__ __align__(16) unsigned char smem[];
-    InferSmem &sm = *reinterpret_cast<InferSmem *>(smem);
-    loadInferWeights(sm, net);
-    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    TcSmem &sm = *reinterpret_cast<TcSmem *>(smem);
+    tcSetup(sm, net);
+    const int pipe = threadIdx.x / kTcPipeThreads, row = threadIdx.x & (kTcPipeThreads - 1);
     const uint32_t nHit = cnt->nHit;
-    const uint32_t tiles = (nHit + 31) / 32;
-    for (uint32_t tile = blockIdx.x * kInferWarps + warp; tile < tiles; tile += gridDim.x * kInferWarps) {
-        const uint32_t q = tile * 32 + lane;
+    const uint32_t tiles = (nHit + kTcPipeThreads - 1) / kTcPipeThreads;
+    uint32_t phase = 0;
+    for (uint32_t tile = blockIdx.x * kTcPipes + pipe; tile < tiles; tile += gridDim.x * kTcPipes) {
+        const uint32_t q = tile * kTcPipeThreads + row;
         uint4 packed = make_uint4(0u, 0u, 0u, 0xffff0000u);
         if (q < nHit) packed = __ldcs(&features[q]);
         const bool valid = q < nHit && (packed.w >> 16) < guideDepth;
-        if (!__any_sync(0xffffffffu, valid)) continue;  // no guided vertex in this tile
+        if (!pipeAny(pipe, valid)) continue;  // no guided vertex in this tile
         const GuideFeatures f = unpackFeatures(packed);
-        float *o = sm.out[warp];
-        inferWarp(sm, f, o, lane);
-        if (valid) out[q] = pack(decode(&o[lane * kLdOut]));
-        __syncwarp();
+        float o[GUIDE_OUTPUTS];
+        if (!tcForward(sm, pipe, f, o, phase)) {
+            if (row == 0) atomicOr(&cnt->errors, ERR_GUIDE_TIMEOUT);
+            break;
+        }
+        if (valid) out[q] = pack(decode(o));
     }
+    tcTeardown(sm, pipe, phase);
 }
 
 // Gradient of the mean loss over a batch of records, accumulated into net.grad.
@@ -594,25 +731,29 @@ __global__ void k_guide_mean_y(RecordBatch batch, float *sum) {
 }
 
 // Test hook: forward pass of explicit feature vectors through the inference
-// core, raw outputs.
-__global__ void __launch_bounds__(32 * kInferWarps) k_guide_forward_test(const float *features, uint32_t n,
-                                                                      GuideNetView net, float *out) {
+// core (tcgen05), raw outputs; status[0] = 1 if a wait expired.
+__global__ void __launch_bounds__(kTcThreads) k_guide_forward_test(const float *features, uint32_t n, GuideNetView net,
+                                                                float *out, int *status) {
     extern __shared__ __align__(16) unsigned char smem[];
-    InferSmem &sm = *reinterpret_cast<InferSmem *>(smem);
-    loadInferWeights(sm, net);
-    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-    const uint32_t tiles = (n + 31) / 32;
-    for (uint32_t tile = blockIdx.x * kInferWarps + warp; tile < tiles; tile += gridDim.x * kInferWarps) {
-        const uint32_t q = tile * 32 + lane;
+    TcSmem &sm = *reinterpret_cast<TcSmem *>(smem);
+    tcSetup(sm, net);
+    const int pipe = threadIdx.x / kTcPipeThreads, row = threadIdx.x & (kTcPipeThreads - 1);
+    const uint32_t tiles = (n + kTcPipeThreads - 1) / kTcPipeThreads;
+    uint32_t phase = 0;
+    for (uint32_t tile = blockIdx.x * kTcPipes + pipe; tile < tiles; tile += gridDim.x * kTcPipes) {
+        const uint32_t q = tile * kTcPipeThreads + row;
         GuideFeatures f = {};
         if (q < n)
             for (int k = 0; k < 7; k++) f.v[k] = features[7 * q + k];
-        float *o = sm.out[warp];
-        inferWarp(sm, f, o, lane);
+        float o[GUIDE_OUTPUTS];
+        if (!tcForward(sm, pipe, f, o, phase)) {
+            if (row == 0) atomicExch(status, 1);
+            break;
+        }
         if (q < n)
-            for (int c = 0; c < GUIDE_OUTPUTS; c++) out[GUIDE_OUTPUTS * q + c] = o[lane * kLdOut + c];
-        __syncwarp();
+            for (int c = 0; c < GUIDE_OUTPUTS; c++) out[GUIDE_OUTPUTS * q + c] = o[c];
     }
+    tcTeardown(sm, pipe, phase);
 }
 
 // Uploaded parameters: clear Adam and the gradient, refresh the bf16 copies.
@@ -648,7 +789,7 @@ __global__ void k_guide_mixture_test(const float *outputs, const float *u, int n
 using namespace rmd;
 
 size_t rmdGuideSharedBytes(bool training) {
-    return training ? kWarps * sizeof(WarpScratch) + GUIDE_PARAMS * sizeof(float) : sizeof(InferSmem);
+    return training ? kWarps * sizeof(WarpScratch) + GUIDE_PARAMS * sizeof(float) : sizeof(TcSmem);
 }
 
 cudaError_t rmdGuideConfigure() {
@@ -669,8 +810,7 @@ cudaError_t rmdLaunchGuideInfer(const Context &ctx, const PathPool &pool, Counte
                                                                                               guideDepth);
     cudaError_t e = cudaGetLastError();
     if (e != cudaSuccess) return e;
-    k_guide_infer<<<blocks, 32 * kInferWarps, rmdGuideSharedBytes(false), s>>>(cnt, pool.guideFeat, guideDepth, net,
-                                                                              out);
+    k_guide_infer<<<blocks, kTcThreads, rmdGuideSharedBytes(false), s>>>(cnt, pool.guideFeat, guideDepth, net, out);
     return cudaGetLastError();
 }
 
@@ -691,10 +831,10 @@ cudaError_t rmdLaunchGuideTrain(const GuideRecord *rec, uint32_t total, uint32_t
 }
 
 cudaError_t rmdLaunchGuideForwardTest(const float *features, uint32_t n, const GuideNetView &net, float *out,
-                                      cudaStream_t s) {
-    const int blocks = (int)std::min<uint32_t>(1024, (n + 32 * kInferWarps - 1) / (32 * kInferWarps));
-    k_guide_forward_test<<<std::max(1, blocks), 32 * kInferWarps, rmdGuideSharedBytes(false), s>>>(features, n, net,
-                                                                                                   out);
+                                      int *status, cudaStream_t s) {
+    const int blocks = (int)std::min<uint32_t>(148, (n + kTcThreads - 1) / kTcThreads);
+    k_guide_forward_test<<<std::max(1, blocks), kTcThreads, rmdGuideSharedBytes(false), s>>>(features, n, net, out,
+                                                                                             status);
     return cudaGetLastError();
 }
 
@@ -853,15 +993,20 @@ extern "C" rmd_status rmd_test_guide_forward(const float *params, const float *f
     cudaError_t e;
     if ((e = net.allocate()) != cudaSuccess) return guideFail(e, "guide allocate");
     if ((e = net.setParams(params, 0)) != cudaSuccess) return guideFail(e, "guide params");
-    DeviceArray f, o;
+    DeviceArray f, o, st;
+    const int zero = 0;
     if ((e = f.upload(features, (size_t)n * 7 * sizeof(float))) != cudaSuccess ||
-        (e = o.alloc((size_t)n * GUIDE_OUTPUTS * sizeof(float))) != cudaSuccess)
+        (e = o.alloc((size_t)n * GUIDE_OUTPUTS * sizeof(float))) != cudaSuccess ||
+        (e = st.upload(&zero, sizeof(int))) != cudaSuccess)
         return guideFail(e, "guide buffers");
+    int status = 0;
     if ((e = rmdLaunchGuideForwardTest((const float *)f.p, (uint32_t)n,
-                                       net.view(make_float3(0, 0, 0), make_float3(1, 1, 1)), (float *)o.p, 0)) !=
-            cudaSuccess ||
-        (e = cudaMemcpy(out, o.p, (size_t)n * GUIDE_OUTPUTS * sizeof(float), cudaMemcpyDeviceToHost)) != cudaSuccess)
+                                       net.view(make_float3(0, 0, 0), make_float3(1, 1, 1)), (float *)o.p, (int *)st.p,
+                                       0)) != cudaSuccess ||
+        (e = cudaMemcpy(out, o.p, (size_t)n * GUIDE_OUTPUTS * sizeof(float), cudaMemcpyDeviceToHost)) != cudaSuccess ||
+        (e = cudaMemcpy(&status, st.p, sizeof(int), cudaMemcpyDeviceToHost)) != cudaSuccess)
         return guideFail(e, "guide forward");
+    if (status) return rmdhost::setLastError(RMD_ERROR_WATCHDOG, "guide inference: a tensor-core wait expired");
     return RMD_OK;
 }
 

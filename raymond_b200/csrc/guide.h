@@ -41,8 +41,9 @@ cudaError_t rmdLaunchGuideInfer(const rmd::Context &ctx, const rmd::PathPool &po
 cudaError_t rmdLaunchGuideTrain(const rmd::GuideRecord *rec, uint32_t total, uint32_t n, uint32_t seed,
                                 const rmd::GuideNetView &net, float *scratch, int blocks, float lr, int step,
                                 cudaStream_t s);
+// status[0] = 1 if a tensor-core wait expired
 cudaError_t rmdLaunchGuideForwardTest(const float *features, uint32_t n, const rmd::GuideNetView &net, float *out,
-                                      cudaStream_t s);
+                                      int *status, cudaStream_t s);
 // gradient only (no Adam step): net.grad += d(mean loss); scratch[1] = mean loss
 cudaError_t rmdLaunchGuideGradientTest(const rmd::GuideRecord *rec, uint32_t n, const rmd::GuideNetView &net,
                                        float *scratch, cudaStream_t s);

@@ -930,7 +930,7 @@ rmd_status rmd_render(rmd_renderer *r, const rmd_render_settings *s) {
     const PathPool pool = poolView(r);
     sp.pool = pool;
     sp.fp = fp;
-    const int guideBlocks = ctx->smCount * 2;  // resident blocks of the inference kernel (registers)
+    const int guideBlocks = ctx->smCount;  // the inference kernel: one CTA of 4 pipelines per SM (shared memory)
     const int trainBlocks = ctx->smCount;
     const uint32_t batch = guide.settings.batch_size;
     uint64_t trainSteps = 0;
@@ -968,6 +968,9 @@ rmd_status rmd_render(rmd_renderer *r, const rmd_render_settings *s) {
         const Counters &h = *r->hostCounters;
         if (h.errors) {
             r->stats.errors = h.errors;
+            if (h.errors & ERR_GUIDE_TIMEOUT)
+                return fail(RMD_ERROR_WATCHDOG, "guide inference: a tensor-core wait expired (device error flags " +
+                                                    std::to_string(h.errors) + ")");
             return fail(RMD_ERROR_QUEUE_OVERFLOW, "device error flags " + std::to_string(h.errors));
         }
         if (guideTraining && h.numSamples >= batch) {
@@ -1471,7 +1474,7 @@ static rmd_status batchEnqueueIterations(rmd_batch *b, const PathPool &pool, con
         RMD_CUDA(rmdLaunchTraceClosest(nullptr, nullptr, pool, cnt, cur, tb, st));
         if (pool.guide)
             RMD_CUDA(rmdLaunchGuideInfer(b->scenes[0]->dctx, pool, cnt, cur, fp.guideDepth, net, pool.guide,
-                                         b->ctx->smCount * 2, st));
+                                         b->ctx->smCount, st));
         sp.cur = cur;
         RMD_CUDA(cudaLaunchKernel((const void *)b->shade, dim3(b->shadeBlocks), dim3(128), shadeArgs, 0, st));
         RMD_CUDA(rmdLaunchTraceShadow(nullptr, nullptr, pool, cnt, cur, tb, st));
