@@ -135,11 +135,11 @@ __device__ void encodeInputs(WarpScratch &s, const GuideFeatures &f, int lane) {
     __syncwarp();
 }
 
-__device__ __forceinline__ float sigmoid(float x) { return 1.0f / (1.0f + __expf(-x)); }
+__device__ __forceinline__ float sigmoid(float x) { return __fdividef(1.0f, 1.0f + __expf(-x)); }
 
 // decoded network output of one sample
 struct Decoded {
-    float theta[GUIDE_LOBES], phi[GUIDE_LOBES], st[GUIDE_LOBES], sp[GUIDE_LOBES];  // sigmoids of the raw values
+    float st[GUIDE_LOBES], sp[GUIDE_LOBES];  // sigmoids of the raw values (theta / pi, phi / 2 pi)
     float logKappa[GUIDE_LOBES];
     bool kappaClamped[GUIDE_LOBES];
     float lambda[GUIDE_LOBES];
@@ -154,25 +154,31 @@ __device__ Decoded decode(const float *o) {
     for (int j = 0; j < GUIDE_LOBES; j++) {
         d.st[j] = sigmoid(o[4 * j + 0]);
         d.sp[j] = sigmoid(o[4 * j + 1]);
-        d.theta[j] = M_PI_F * d.st[j];
-        d.phi[j] = 2.0f * M_PI_F * d.sp[j];
         const float lk = o[4 * j + 2];
         d.kappaClamped[j] = lk < GUIDE_LOG_KAPPA_MIN || lk > GUIDE_LOG_KAPPA_MAX;
         d.logKappa[j] = fminf(GUIDE_LOG_KAPPA_MAX, fmaxf(GUIDE_LOG_KAPPA_MIN, lk));
         d.lambda[j] = __expf(o[4 * j + 3] - maxLogit);
         sum += d.lambda[j];
     }
-    for (int j = 0; j < GUIDE_LOBES; j++) d.lambda[j] /= sum;
+    const float invSum = 1.0f / sum;
+    for (int j = 0; j < GUIDE_LOBES; j++) d.lambda[j] *= invSum;
     d.alphaSig = sigmoid(o[4 * GUIDE_LOBES]);
     d.alpha = GUIDE_ALPHA_MIN + (GUIDE_ALPHA_MAX - GUIDE_ALPHA_MIN) * d.alphaSig;
     return d;
 }
 
-__device__ float3 lobeMean(float theta, float phi) {
+// mean direction of lobe j: theta = pi st, phi = 2 pi sp
+__device__ float3 lobeMean(const Decoded &d, int j) {
     float st, ct, sp, cp;
-    sincosf(theta, &st, &ct);
-    sincosf(phi, &sp, &cp);
+    sincospif(d.st[j], &st, &ct);
+    sincospif(2.0f * d.sp[j], &sp, &cp);
     return make_float3(st * cp, st * sp, ct);
+}
+
+// vMF normalisation k / (2 pi (1 - e^{-2k})) for k in [e^-3, e^5], where
+// 1 - e^{-2k} >= 0.09 and needs no expm1
+__device__ __forceinline__ float vmfNormPacked(float k) {
+    return __fdividef(k * (0.5f / M_PI_F), 1.0f - __expf(-2.0f * k));
 }
 
 __device__ GuideMixture pack(const Decoded &d) {
@@ -180,7 +186,7 @@ __device__ GuideMixture pack(const Decoded &d) {
     uint32_t w[4];
     float total = 0.0f, kappa[GUIDE_LOBES];
     for (int j = 0; j < GUIDE_LOBES; j++) {
-        const float3 mu = lobeMean(d.theta[j], d.phi[j]);
+        const float3 mu = lobeMean(d, j);
         const uint32_t kb = bf16Bits(__expf(d.logKappa[j]));
         kappa[j] = bf16Lo(kb);
         total += bf16Lo(bf16Bits(d.lambda[j]));
@@ -189,7 +195,7 @@ __device__ GuideMixture pack(const Decoded &d) {
         else w[j >> 1] = bf16Bits(d.lambda[j]);
     }
     const float inv = 1.0f / total;
-    for (int j = 0; j < GUIDE_LOBES; j++) m.coef[j] = bf16Lo(bf16Bits(d.lambda[j])) * inv * vmfNorm(kappa[j]);
+    for (int j = 0; j < GUIDE_LOBES; j++) m.coef[j] = bf16Lo(bf16Bits(d.lambda[j])) * inv * vmfNormPacked(kappa[j]);
     m.weights = make_uint4(w[0], w[1], w[2], w[3]);
     m.alpha = d.alpha;
     m.invTotal = inv;
@@ -209,7 +215,7 @@ __device__ float lossGradient(const float *o, float3 w, float pb, float y, float
     float3 mu[GUIDE_LOBES];
     float kappa[GUIDE_LOBES], cosw[GUIDE_LOBES];
     for (int j = 0; j < GUIDE_LOBES; j++) {
-        mu[j] = lobeMean(d.theta[j], d.phi[j]);
+        mu[j] = lobeMean(d, j);
         kappa[j] = __expf(d.logKappa[j]);
         cosw[j] = dot(mu[j], w);
         v[j] = vmfNorm(kappa[j]) * __expf(kappa[j] * (cosw[j] - 1.0f));
@@ -236,8 +242,8 @@ __device__ float lossGradient(const float *o, float3 w, float pb, float y, float
         // mean direction: dv/dmu = v k w; mu(theta, phi)
         const float gmu = gv * v[j] * kappa[j];
         float st, ct, sp, cp;
-        sincosf(d.theta[j], &st, &ct);
-        sincosf(d.phi[j], &sp, &cp);
+        sincospif(d.st[j], &st, &ct);
+        sincospif(2.0f * d.sp[j], &sp, &cp);
         const float3 dmu_dtheta = make_float3(ct * cp, ct * sp, -st);
         const float3 dmu_dphi = make_float3(-st * sp, st * cp, 0.0f);
         grad[4 * j + 0] = gmu * dot(w, dmu_dtheta) * M_PI_F * d.st[j] * (1.0f - d.st[j]);
@@ -308,11 +314,31 @@ struct TcSmem {
 
 __device__ __forceinline__ uint32_t smemU32(const void *p) { return (uint32_t)__cvta_generic_to_shared(p); }
 
-// two floats to packed BF16 (round to nearest even), hi in the upper half
-__device__ __forceinline__ uint32_t cvtBf16x2(float lo, float hi) {
+// (lo + blo, hi + bhi) with ReLU as packed BF16 (round to nearest even), hi
+// in the upper half: one paired FP32 add and one converting ReLU
+__device__ __forceinline__ uint32_t biasReluBf16x2(float lo, float hi, float2 bias) {
     uint32_t r;
-    asm("cvt.rn.bf16x2.f32 %0, %1, %2;\n" : "=r"(r) : "f"(hi), "f"(lo));
+    asm("{\n.reg .b64 x, y;\n.reg .f32 l, h;\n"
+        "mov.b64 x, {%1, %2};\nmov.b64 y, {%3, %4};\nadd.rn.f32x2 x, x, y;\nmov.b64 {l, h}, x;\n"
+        "cvt.rn.relu.bf16x2.f32 %0, h, l;\n}\n"
+        : "=r"(r)
+        : "f"(lo), "f"(hi), "f"(bias.x), "f"(bias.y));
     return r;
+}
+
+// BF16 of a float, round to nearest even
+__device__ __forceinline__ uint16_t cvtBf16(float x) {
+    uint16_t r;
+    asm("cvt.rn.bf16.f32 %0, %1;\n" : "=h"(r) : "f"(x));
+    return r;
+}
+
+// paired FP32 add of two bias values
+__device__ __forceinline__ void addBias2(float &lo, float &hi, float2 bias) {
+    asm("{\n.reg .b64 x, y;\nmov.b64 x, {%0, %1};\nmov.b64 y, {%2, %3};\nadd.rn.f32x2 x, x, y;\n"
+        "mov.b64 {%0, %1}, x;\n}\n"
+        : "+f"(lo), "+f"(hi)
+        : "f"(bias.x), "f"(bias.y));
 }
 
 // byte offset of element (r, k) in a K-major canonical operand of width K
@@ -496,8 +522,8 @@ __device__ void tcHiddenEpilogue(uint16_t *a, uint32_t taddr, const float *bias,
             uint32_t q[4];
 #pragma unroll
             for (int k = 0; k < 4; k++)
-                q[k] = cvtBf16x2(fmaxf(v[c + 2 * k] + bias[32 * half + c + 2 * k], 0.0f),
-                                 fmaxf(v[c + 2 * k + 1] + bias[32 * half + c + 2 * k + 1], 0.0f));
+                q[k] = biasReluBf16x2(v[c + 2 * k], v[c + 2 * k + 1],
+                                      *reinterpret_cast<const float2 *>(&bias[32 * half + c + 2 * k]));
             *reinterpret_cast<uint4 *>(reinterpret_cast<unsigned char *>(a) +
                                        canonOffset(row, 32 * half + c, GUIDE_HIDDEN)) = make_uint4(q[0], q[1], q[2], q[3]);
         }
@@ -509,18 +535,26 @@ __device__ void tcHiddenEpilogue(uint16_t *a, uint32_t taddr, const float *bias,
 __device__ bool tcForward(TcSmem &sm, int pipe, const GuideFeatures &f, float *o, uint32_t &phase) {
     const int row = threadIdx.x & (kTcPipeThreads - 1);
     uint16_t *a = sm.a[pipe];
-    // one-blob input row: 20 chunks of 8 bins
+    // one-blob input row.  A feature v with b bins is non-zero only in bins
+    // floor(v b - 1/2) and the one after (|v b - (bin + 1/2)| < 1), so the
+    // row is cleared and those two bins of each of the 7 features written.
+    unsigned char *aRow = reinterpret_cast<unsigned char *>(a);
 #pragma unroll
-    for (int c = 0; c < GUIDE_INPUTS / 8; c++) {
-        const int feature = c < 12 ? c >> 2 : 3 + ((c - 12) >> 1);
-        const int bins = c < 12 ? 32 : 16;
-        const int bin0 = c < 12 ? (c & 3) * 8 : ((c - 12) & 1) * 8;
+    for (int c = 0; c < GUIDE_INPUTS / 8; c++)
+        *reinterpret_cast<uint4 *>(aRow + canonOffset(row, 8 * c, GUIDE_INPUTS)) = make_uint4(0u, 0u, 0u, 0u);
+#pragma unroll
+    for (int feature = 0; feature < 7; feature++) {
+        const int bins = feature < 3 ? 32 : 16;
+        const int first = feature < 3 ? 32 * feature : 96 + 16 * (feature - 3);
         const float v = f.v[feature];
-        uint32_t q[4];
+        const int b = (int)floorf(v * (float)bins - 0.5f);
 #pragma unroll
-        for (int k = 0; k < 4; k++) q[k] = cvtBf16x2(oneBlob(v, bins, bin0 + 2 * k), oneBlob(v, bins, bin0 + 2 * k + 1));
-        *reinterpret_cast<uint4 *>(reinterpret_cast<unsigned char *>(a) + canonOffset(row, 8 * c, GUIDE_INPUTS)) =
-            make_uint4(q[0], q[1], q[2], q[3]);
+        for (int k = 0; k < 2; k++) {
+            const int bin = b + k;
+            if (bin >= 0 && bin < bins)
+                *reinterpret_cast<uint16_t *>(aRow + canonOffset(row, first + bin, GUIDE_INPUTS)) =
+                    cvtBf16(oneBlob(v, bins, bin));
+        }
     }
     // this warp's 32 lanes (its quarter of the pipeline's rows) in the pipeline's 64 columns
     const uint32_t taddr = sm.tmemBase + 64u * pipe + ((uint32_t)(row & ~31) << 16);
@@ -534,9 +568,9 @@ __device__ bool tcForward(TcSmem &sm, int pipe, const GuideFeatures &f, float *o
     tmemLd32(taddr, o);
     tmemLd16(taddr + 32u, o + 32);
     tmemLdWait();
-    const float *b4 = sm.b + 3 * GUIDE_HIDDEN;
+    const float2 *b4 = reinterpret_cast<const float2 *>(sm.b + 3 * GUIDE_HIDDEN);
 #pragma unroll
-    for (int c = 0; c < GUIDE_OUTPUTS; c++) o[c] += b4[c];
+    for (int c = 0; c < GUIDE_OUTPUTS / 2; c++) addBias2(o[2 * c], o[2 * c + 1], b4[c]);
     return true;
 }
 
