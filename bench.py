@@ -442,6 +442,7 @@ def main():
     ap.add_argument("--guided-size", default=f"{GUIDED_W}x{GUIDED_H}", help="guided leg resolution (profiling runs)")
     ap.add_argument("--oracle-spp", type=int, default=GUIDED_ORACLE_SPP, help="guided leg: oracle samples")
     ap.add_argument("--no-autotune", action="store_true")
+    ap.add_argument("--bvh", default="host", choices=["host", "gpu"], help="BVH builder of the plain workload's scene")
     ap.add_argument("--tuning", default="", help="shade_min_blocks,trace_blocks_per_sm,pool_size: apply "
                     "these launch choices instead of autotuning (profiling runs)")
     args = ap.parse_args()
@@ -492,10 +493,11 @@ def main():
     from raymond_b200._abi import SceneDesc, make_camera
 
     desc = SceneDesc(make_scene())
-    ctx = api.Context(local)
+    ctx = api.Context(local, bvh_builder=args.bvh)
     t0 = time.perf_counter()
     scene = api.Scene(ctx, desc)
     build_s = time.perf_counter() - t0
+    bvh = scene.bvh_stats()
     r = api.Renderer(scene, W, H, pool_size=args.pool)
     t0 = time.perf_counter()
     if args.tuning:
@@ -582,7 +584,7 @@ def main():
                                          "d2h_bytes_per_step": W * H * 3 * 4},
         "gpu_launches": int(tot["iterations"] * 4 + args.steps),
         "clocks": clocks,
-        "scene_build_s": build_s,
+        "scene_build_s": build_s, "bvh": bvh,
         "autotune": dict(tune, seconds=tune_s) if tune else None,
     }
     if not args.no_guided and world == 1:

@@ -267,6 +267,23 @@ typedef struct rmd_stats {
     double   ms_guide_train;   /* of which training (gradient and Adam steps) */
 } rmd_stats;
 
+/* ------------------------------------------------ acceleration structures */
+
+#define RMD_BVH_HOST 0u /* binned SAH on the host (OpenMP), the default */
+#define RMD_BVH_GPU 1u  /* on the device: Morton order, locally-ordered clustering, 8-wide collapse */
+
+typedef struct rmd_bvh_stats {
+    uint32_t builder;  /* RMD_BVH_* that built the scene's BVH */
+    uint32_t levels;   /* levels of the 8-wide tree */
+    uint64_t nodes;    /* 8-wide nodes */
+    double build_ms;   /* host wall-clock time of the build, uploads included */
+    double sah_cost;   /* surface-area cost relative to the root: per node the area of its box
+                          (its parent's quantised slot; 1 for the root), plus per leaf the area of
+                          its slot times its triangles */
+    uint32_t cluster_iterations; /* RMD_BVH_GPU: clustering passes until one cluster was left */
+    uint32_t reserved;
+} rmd_bvh_stats;
+
 typedef struct rmd_context rmd_context;
 typedef struct rmd_scene rmd_scene;
 typedef struct rmd_renderer rmd_renderer;
@@ -282,6 +299,16 @@ void rmd_context_destroy(rmd_context *ctx);
  * MaterialBuilder / ShapeBuilder / EntityBuilder / LightBuilder stages. */
 rmd_status rmd_scene_create(rmd_context *ctx, const rmd_scene_desc *desc, rmd_scene **out);
 void rmd_scene_destroy(rmd_scene *scene);
+/* Builder of the acceleration structure of the scenes this context creates
+ * from now on (RMD_BVH_HOST or RMD_BVH_GPU).  Replaces the choice of Metal's
+ * acceleration-structure builder in ShapeBuilder.swift:7-94,302-319 and
+ * EntityBuilder.swift:148-165 (the reference has one builder, Apple's).  Both
+ * produce the same 8-wide node format, so rendering is unchanged. */
+rmd_status rmd_context_set_bvh_builder(rmd_context *ctx, uint32_t builder);
+/* Builder, build time, size and surface-area cost of a scene's BVH (the cost
+ * is computed on the host on the first call).  No counterpart in the
+ * reference, whose acceleration structures are opaque. */
+rmd_status rmd_scene_bvh_stats(rmd_scene *scene, rmd_bvh_stats *out);
 /* Number of triangles after instancing, and BVH nodes. */
 rmd_status rmd_scene_info(const rmd_scene *scene, uint64_t *triangles, uint64_t *bvh_nodes,
                           int32_t *num_lights_total);

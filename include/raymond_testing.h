@@ -26,6 +26,13 @@ rmd_status rmd_test_prng(uint32_t mode, uint64_t a, uint64_t b, int32_t n, float
 rmd_status rmd_test_trace(const rmd_scene *scene, const float *rays, int32_t n, int32_t any, float *out,
                           uint32_t *instances);
 
+/* The scene's BVH as the traversal kernels read it: max_nodes x 80-byte
+ * nodes (the layout of device/traverse.cuh) and max_triangles x 12 floats
+ * (v0, instance bits, v1, primitive bits, v2, 0) in leaf order.  Either
+ * output may be NULL. */
+rmd_status rmd_test_bvh_read(const rmd_scene *scene, void *nodes, uint64_t max_nodes, float *tris,
+                             uint64_t max_triangles);
+
 /* Shade n records with surface material `material` and evaluate / sample its
  * BSDF as handleIntersections does.  Record: position, normal, trueNormal,
  * generated, uv, wo, wi, rnd (float3 each), rayFlags, 3 pad (28 floats).

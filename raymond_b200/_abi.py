@@ -141,6 +141,16 @@ class GuideStats(C.Structure):
                 ("reserved", C.c_float)]
 
 
+BVH_HOST = 0
+BVH_GPU = 1
+BVH_BUILDERS = {"host": BVH_HOST, "gpu": BVH_GPU}
+
+
+class BvhStats(C.Structure):
+    _fields_ = [("builder", C.c_uint32), ("levels", C.c_uint32), ("nodes", C.c_uint64), ("build_ms", C.c_double),
+                ("sah_cost", C.c_double), ("cluster_iterations", C.c_uint32), ("reserved", C.c_uint32)]
+
+
 def _fptr(a: np.ndarray, ctype=C.c_float):
     return a.ctypes.data_as(C.POINTER(ctype))
 

@@ -31,9 +31,9 @@ EXPORTS = [
     "rmd_renderer_set_tuning", "rmd_renderer_set_guide", "rmd_renderer_guide_stats", "rmd_guide_param_count",
     "rmd_renderer_guide_params", "rmd_batch_create", "rmd_batch_destroy", "rmd_batch_reset", "rmd_batch_render",
     "rmd_batch_film_read", "rmd_batch_film_read_f64", "rmd_batch_stats", "rmd_batch_autotune",
-    "rmd_batch_set_guide", "rmd_batch_guide_stats",
+    "rmd_batch_set_guide", "rmd_batch_guide_stats", "rmd_context_set_bvh_builder", "rmd_scene_bvh_stats",
     "rmd_test_prng", "rmd_test_trace", "rmd_test_material_eval", "rmd_test_generate_source", "rmd_test_jit_compile",
-    "rmd_test_guide_forward", "rmd_test_guide_gradient", "rmd_test_guide_mixture",
+    "rmd_test_guide_forward", "rmd_test_guide_gradient", "rmd_test_guide_mixture", "rmd_test_bvh_read",
 ]
 
 
@@ -60,6 +60,9 @@ def lib() -> C.CDLL:
         "rmd_last_error": ([], C.c_char_p),
         "rmd_version": ([], C.c_char_p),
         "rmd_context_create": ([C.c_int32, P(vp)], C.c_int32),
+        "rmd_context_set_bvh_builder": ([vp, C.c_uint32], C.c_int32),
+        "rmd_scene_bvh_stats": ([vp, P(_abi.BvhStats)], C.c_int32),
+        "rmd_test_bvh_read": ([vp, vp, C.c_uint64, P(C.c_float), C.c_uint64], C.c_int32),
         "rmd_context_destroy": ([vp], None),
         "rmd_scene_create": ([vp, P(_abi.SceneDescC), P(vp)], C.c_int32),
         "rmd_scene_destroy": ([vp], None),
@@ -121,11 +124,19 @@ def _f32p(a: np.ndarray):
 
 
 class Context:
-    """A CUDA device and stream (rmd_context)."""
+    """A CUDA device and stream (rmd_context).  `bvh_builder`: "host" (binned
+    SAH on the host) or "gpu" (built on the device) for the scenes created
+    in this context."""
 
-    def __init__(self, device: int = 0):
+    def __init__(self, device: int = 0, bvh_builder: str = "host"):
         self.h = C.c_void_p()
         check(lib().rmd_context_create(device, C.byref(self.h)))
+        self.set_bvh_builder(bvh_builder)
+
+    def set_bvh_builder(self, builder: str) -> None:
+        if builder not in _abi.BVH_BUILDERS:
+            raise ValueError(f"bvh_builder must be one of {sorted(_abi.BVH_BUILDERS)}, not {builder!r}")
+        check(lib().rmd_context_set_bvh_builder(self.h, _abi.BVH_BUILDERS[builder]))
 
     def close(self):
         if self.h.value:
@@ -153,6 +164,24 @@ class Scene:
         lights = C.c_int32()
         check(lib().rmd_scene_info(self.h, C.byref(t), C.byref(n), C.byref(lights)))
         return {"triangles": t.value, "bvh_nodes": n.value, "lights": lights.value}
+
+    def bvh_stats(self) -> dict[str, float]:
+        """Builder, levels, nodes, build time (ms) and surface-area cost of the BVH."""
+        st = _abi.BvhStats()
+        check(lib().rmd_scene_bvh_stats(self.h, C.byref(st)))
+        names = {v: k for k, v in _abi.BVH_BUILDERS.items()}
+        return {"builder": names.get(st.builder, st.builder), "levels": st.levels, "nodes": st.nodes,
+                "build_ms": st.build_ms, "sah_cost": st.sah_cost, "cluster_iterations": st.cluster_iterations}
+
+    def bvh_arrays(self) -> tuple[np.ndarray, np.ndarray]:
+        """The BVH as the traversal kernels read it (test hook): 80-byte nodes
+        as a (nodes, 80) uint8 array and the leaf-ordered triangles (n, 12) float32."""
+        info = self.info()
+        nodes = np.zeros((max(1, info["bvh_nodes"]), 80), np.uint8)
+        tris = np.zeros((max(1, info["triangles"]), 12), np.float32)
+        check(lib().rmd_test_bvh_read(self.h, nodes.ctypes.data_as(C.c_void_p), nodes.shape[0], _f32p(tris),
+                                      tris.shape[0]))
+        return nodes[:info["bvh_nodes"]], tris[:info["triangles"]]
 
     def trace(self, rays: np.ndarray, any_hit: bool = False):
         rays = np.ascontiguousarray(rays, np.float32)

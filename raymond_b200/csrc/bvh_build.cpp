@@ -369,4 +369,56 @@ void buildWideBvh(const std::vector<float> &v0, const std::vector<float> &v1, co
     }
 }
 
+double wideBvhSahCost(const GpuWideNode *nodes, size_t count, uint32_t &levels) {
+    levels = 0;
+    if (count == 0) return 0.0;
+    auto slotBox = [](const GpuWideNode &w, int c, double lo[3], double hi[3]) {
+        for (int k = 0; k < 3; k++) {
+            const double scale = std::ldexp(1.0, (int)w.exponent[k] - 127);
+            lo[k] = (double)w.origin[k] + w.qlo[k][c] * scale;
+            hi[k] = (double)w.origin[k] + w.qhi[k][c] * scale;
+        }
+    };
+    auto area = [](const double lo[3], const double hi[3]) {
+        const double e0 = std::max(0.0, hi[0] - lo[0]), e1 = std::max(0.0, hi[1] - lo[1]),
+                     e2 = std::max(0.0, hi[2] - lo[2]);
+        return 2.0 * (e0 * e1 + e1 * e2 + e2 * e0);
+    };
+    // the root's area: the union of its slots
+    double rlo[3] = {DBL_MAX, DBL_MAX, DBL_MAX}, rhi[3] = {-DBL_MAX, -DBL_MAX, -DBL_MAX};
+    for (int c = 0; c < 8; c++) {
+        const bool used = (nodes[0].imask >> c & 1) || nodes[0].meta[c];
+        if (!used) continue;
+        double lo[3], hi[3];
+        slotBox(nodes[0], c, lo, hi);
+        for (int k = 0; k < 3; k++) {
+            rlo[k] = std::min(rlo[k], lo[k]);
+            rhi[k] = std::max(rhi[k], hi[k]);
+        }
+    }
+    const double rootArea = std::max(area(rlo, rhi), 1e-30);
+    double cost = 0.0;
+    std::vector<std::pair<uint32_t, std::pair<double, uint32_t>>> stack{{0u, {rootArea, 1u}}};
+    while (!stack.empty()) {
+        const auto [idx, rest] = stack.back();
+        const auto [nodeArea, depth] = rest;
+        stack.pop_back();
+        if (idx >= count) continue;
+        levels = std::max(levels, depth);
+        cost += nodeArea / rootArea;
+        const GpuWideNode &w = nodes[idx];
+        uint32_t inner = 0;
+        for (int c = 0; c < 8; c++) {
+            double lo[3], hi[3];
+            slotBox(w, c, lo, hi);
+            if (w.imask >> c & 1) {
+                stack.push_back({w.childBase + inner++, {area(lo, hi), depth + 1}});
+            } else if (w.meta[c]) {
+                cost += area(lo, hi) / rootArea * (double)__builtin_popcount((unsigned)(w.meta[c] >> 5));
+            }
+        }
+    }
+    return cost;
+}
+
 }  // namespace rmdhost

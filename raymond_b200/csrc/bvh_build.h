@@ -30,4 +30,9 @@ struct GpuWideBvh {
 void buildWideBvh(const std::vector<float> &v0, const std::vector<float> &v1, const std::vector<float> &v2,
                   const std::vector<uint32_t> &instance, const std::vector<uint32_t> &prim, GpuWideBvh &out);
 
+// Surface-area cost of a wide BVH relative to its root: per node the area of
+// its box (the parent's decoded slot box; 1 for the root), plus per leaf slot
+// the slot's area times its triangles.  levels = the tree's depth.
+double wideBvhSahCost(const GpuWideNode *nodes, size_t count, uint32_t &levels);
+
 }  // namespace rmdhost

@@ -16,6 +16,7 @@
 #include "../../include/raymond.h"
 #include "../../include/raymond_testing.h"
 #include "bvh_build.h"
+#include "bvh_gpu.h"
 #include "codegen.h"
 #include "device/wavefront.cuh"
 #include "guide.h"
@@ -70,6 +71,11 @@ struct DevBuf {
         if (n == 0) return cudaSuccess;
         return cudaMalloc(&ptr, n);
     }
+    void adopt(void *p, size_t n) {  // takes ownership of a cudaMalloc'd block
+        release();
+        ptr = p;
+        bytes = n;
+    }
     cudaError_t upload(const void *src, size_t n, cudaStream_t s) {
         cudaError_t e = alloc(n);
         if (e != cudaSuccess || n == 0) return e;
@@ -93,6 +99,7 @@ struct rmd_context {
     int device = 0;
     int smCount = 148;
     cudaStream_t stream = nullptr;
+    uint32_t bvhBuilder = RMD_BVH_HOST;  // builder of the scenes created next
 };
 
 struct rmd_scene {
@@ -106,6 +113,8 @@ struct rmd_scene {
     std::string moduleSource;
     std::map<int, std::unique_ptr<rmdhost::JitModule>> variants;  // shade kernels by minimum blocks per SM
     uint64_t triangles = 0, bvhNodeCount = 0;
+    rmd_bvh_stats bvhStats{};  // builder, build time and levels; SAH cost computed when first asked
+    bool bvhSahKnown = false;
     float boundsMin[3] = {0, 0, 0}, boundsMax[3] = {1, 1, 1};  // world-space triangle bounds
     int numSurface = 0, numLight = 0;
     int shadeBlocks = 0, traceBlocks = 0, regenBlocks = 0;
@@ -488,9 +497,37 @@ static rmd_status buildSceneData(rmd_context *ctx, const rmd_scene_desc *d, rmd_
                 s->boundsMax[i % 3] = std::max(s->boundsMax[i % 3], (*t)[i]);
             }
     }
+    // ShapeBuilder / EntityBuilder acceleration structures: one BVH over the
+    // flattened world-space triangles, built on the host or on the device
     rmdhost::GpuWideBvh bvh;
-    rmdhost::buildWideBvh(t0, t1, t2, triInst, triPrim, bvh);
-    s->bvhNodeCount = bvh.nodes.size();
+    const auto buildStart = std::chrono::steady_clock::now();
+    s->bvhStats.builder = ctx->bvhBuilder;
+    if (ctx->bvhBuilder == RMD_BVH_GPU) {
+        DevBuf d0, d1, d2, dInst, dPrim;
+        RMD_CUDA(d0.upload(t0.data(), t0.size() * sizeof(float), st));
+        RMD_CUDA(d1.upload(t1.data(), t1.size() * sizeof(float), st));
+        RMD_CUDA(d2.upload(t2.data(), t2.size() * sizeof(float), st));
+        RMD_CUDA(dInst.upload(triInst.data(), triInst.size() * sizeof(uint32_t), st));
+        RMD_CUDA(dPrim.upload(triPrim.data(), triPrim.size() * sizeof(uint32_t), st));
+        rmdhost::GpuBvhResult g;
+        const cudaError_t e = rmdhost::buildWideBvhGpu(d0.as<float>(), d1.as<float>(), d2.as<float>(),
+                                                       dInst.as<uint32_t>(), dPrim.as<uint32_t>(),
+                                                       (uint32_t)std::min<size_t>(triInst.size(), 0xffffffffu), st, g);
+        s->bvhNodes.adopt(g.nodes, g.nodeCount * sizeof(rmdhost::GpuWideNode));
+        s->bvhTris.adopt(g.tris, triInst.size() * 12 * sizeof(float));
+        if (e != cudaSuccess) {
+            if (!g.error.empty()) return fail(RMD_ERROR_INVALID_ARGUMENT, "device BVH build: " + g.error);
+            RMD_CUDA(e);
+        }
+        s->bvhNodeCount = g.nodeCount;
+        s->bvhStats.levels = g.levels;
+        s->bvhStats.cluster_iterations = g.clusterIterations;
+    } else {
+        rmdhost::buildWideBvh(t0, t1, t2, triInst, triPrim, bvh);
+        s->bvhNodeCount = bvh.nodes.size();
+    }
+    s->bvhStats.build_ms =
+        std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - buildStart).count();
 
     // LightBuilder.build (LightBuilder.swift:179-281)
     std::vector<float> lightFaces(std::max<uint32_t>(1, lightFaceOffset), 0.0f);
@@ -584,8 +621,10 @@ static rmd_status buildSceneData(rmd_context *ctx, const rmd_scene_desc *d, rmd_
     RMD_CUDA(s->surfaceTable.upload(stab.data(), stab.size() * sizeof(uint2), st));
     RMD_CUDA(s->lightTable.upload(ltab.data(), ltab.size() * sizeof(uint2), st));
     RMD_CUDA(s->materialParams.upload(params.data(), params.size() * sizeof(float), st));
-    RMD_CUDA(s->bvhNodes.upload(bvh.nodes.data(), bvh.nodes.size() * sizeof(rmdhost::GpuWideNode), st));
-    RMD_CUDA(s->bvhTris.upload(bvh.tris.data(), bvh.tris.size() * sizeof(float), st));
+    if (ctx->bvhBuilder != RMD_BVH_GPU) {
+        RMD_CUDA(s->bvhNodes.upload(bvh.nodes.data(), bvh.nodes.size() * sizeof(rmdhost::GpuWideNode), st));
+        RMD_CUDA(s->bvhTris.upload(bvh.tris.data(), bvh.tris.size() * sizeof(float), st));
+    }
 
     Context &c = s->dctx;
     c.vertices = s->vertices.as<float4>();
@@ -648,6 +687,32 @@ rmd_status rmd_scene_create(rmd_context *ctx, const rmd_scene_desc *d, rmd_scene
 }
 
 void rmd_scene_destroy(rmd_scene *s) { delete s; }
+
+rmd_status rmd_context_set_bvh_builder(rmd_context *ctx, uint32_t builder) {
+    if (!ctx) return fail(RMD_ERROR_INVALID_ARGUMENT, "NULL context");
+    if (builder != RMD_BVH_HOST && builder != RMD_BVH_GPU) return fail(RMD_ERROR_INVALID_ARGUMENT, "unknown BVH builder");
+    ctx->bvhBuilder = builder;
+    return RMD_OK;
+}
+
+rmd_status rmd_scene_bvh_stats(rmd_scene *s, rmd_bvh_stats *out) {
+    if (!s || !out) return fail(RMD_ERROR_INVALID_ARGUMENT, "NULL argument");
+    if (!s->bvhSahKnown) {
+        std::vector<rmdhost::GpuWideNode> nodes(s->bvhNodeCount);
+        if (!nodes.empty()) {
+            RMD_CUDA(cudaSetDevice(s->ctx->device));
+            RMD_CUDA(cudaMemcpy(nodes.data(), s->bvhNodes.ptr, nodes.size() * sizeof(rmdhost::GpuWideNode),
+                                cudaMemcpyDeviceToHost));
+        }
+        uint32_t levels = 0;
+        s->bvhStats.sah_cost = rmdhost::wideBvhSahCost(nodes.data(), nodes.size(), levels);
+        s->bvhStats.levels = levels;
+        s->bvhSahKnown = true;
+    }
+    *out = s->bvhStats;
+    out->nodes = s->bvhNodeCount;
+    return RMD_OK;
+}
 
 rmd_status rmd_scene_info(const rmd_scene *s, uint64_t *triangles, uint64_t *bvh_nodes, int32_t *num_lights_total) {
     if (!s) return fail(RMD_ERROR_INVALID_ARGUMENT, "NULL scene");
@@ -1232,6 +1297,19 @@ rmd_status rmd_test_trace(const rmd_scene *s, const float *rays, int32_t n, int3
     RMD_CUDA(cudaStreamSynchronize(s->ctx->stream));
     RMD_CUDA(cudaMemcpy(out, dout.ptr, (size_t)n * 4 * sizeof(float), cudaMemcpyDeviceToHost));
     RMD_CUDA(cudaMemcpy(instances, dinst.ptr, (size_t)n * sizeof(uint32_t), cudaMemcpyDeviceToHost));
+    return RMD_OK;
+}
+
+rmd_status rmd_test_bvh_read(const rmd_scene *s, void *nodes, uint64_t max_nodes, float *tris, uint64_t max_triangles) {
+    if (!s) return fail(RMD_ERROR_INVALID_ARGUMENT, "NULL scene");
+    if ((nodes && max_nodes < s->bvhNodeCount) || (tris && max_triangles < s->triangles))
+        return fail(RMD_ERROR_INVALID_ARGUMENT, "output buffers too small");
+    RMD_CUDA(cudaSetDevice(s->ctx->device));
+    if (nodes && s->bvhNodeCount)
+        RMD_CUDA(cudaMemcpy(nodes, s->bvhNodes.ptr, s->bvhNodeCount * sizeof(rmdhost::GpuWideNode),
+                            cudaMemcpyDeviceToHost));
+    if (tris && s->triangles)
+        RMD_CUDA(cudaMemcpy(tris, s->bvhTris.ptr, s->triangles * 12 * sizeof(float), cudaMemcpyDeviceToHost));
     return RMD_OK;
 }
 
