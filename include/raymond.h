@@ -335,6 +335,16 @@ rmd_status rmd_render(rmd_renderer *r, const rmd_render_settings *settings);
  * (exposure * L / samples, then the tonemap; normalizeImage.metal:39-59). */
 rmd_status rmd_film_read(rmd_renderer *r, float *rgb, int32_t normalize, uint32_t tonemapping,
                          float exposure);
+#define RMD_EXR_AUTO 0u /* ZIP, or none when width and height are both below 16 (the reference's choice) */
+#define RMD_EXR_NONE 1u
+#define RMD_EXR_ZIP 2u
+/* MTLTexture.saveEXR(at:normalizedBy:) (utils/Metal.swift:75-126, called by
+ * Renderer.saveFrame, Renderer.swift:804-807): writes the film to an OpenEXR
+ * file of four 32-bit float channels stored A, B, G, R (alpha 1), each colour
+ * the accumulated film times normalized_by (<= 0: 1 / samples, the mean).
+ * The reference wrote it with tinyexr's SaveEXR; this writer is the
+ * library's own (zlib for ZIP). */
+rmd_status rmd_film_save_exr(rmd_renderer *r, const char *path, float normalized_by, uint32_t compression);
 /* The double-precision film (settings.film_fp64), raw sums. */
 rmd_status rmd_film_read_f64(rmd_renderer *r, double *rgb);
 /* Samples accumulated in the film (frameIndex of Renderer.swift:288). */
@@ -438,6 +448,9 @@ rmd_status rmd_batch_render(rmd_batch *batch, const rmd_render_settings *setting
 rmd_status rmd_batch_film_read(rmd_batch *batch, int32_t view, float *rgb, int32_t normalize, uint32_t tonemapping,
                                float exposure);
 rmd_status rmd_batch_film_read_f64(rmd_batch *batch, int32_t view, double *rgb);
+/* rmd_film_save_exr for one view of a batch */
+rmd_status rmd_batch_film_save_exr(rmd_batch *batch, int32_t view, const char *path, float normalized_by,
+                                   uint32_t compression);
 /* aggregate over the views (per-stage times are not taken inside the graph) */
 rmd_status rmd_batch_stats(const rmd_batch *batch, rmd_stats *out);
 rmd_status rmd_batch_autotune(rmd_batch *batch, const rmd_render_settings *settings, rmd_tune_result *out);

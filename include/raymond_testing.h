@@ -26,6 +26,11 @@ rmd_status rmd_test_prng(uint32_t mode, uint64_t a, uint64_t b, int32_t n, float
 rmd_status rmd_test_trace(const rmd_scene *scene, const float *rays, int32_t n, int32_t any, float *out,
                           uint32_t *instances);
 
+/* The EXR writer of rmd_film_save_exr applied to a host image (width x
+ * height x 3 floats) as if it were a film of one sample; needs no GPU. */
+rmd_status rmd_test_exr_write(const char *path, const float *rgb, int32_t width, int32_t height, float normalized_by,
+                              uint32_t compression);
+
 /* The scene's BVH as the traversal kernels read it: max_nodes x 80-byte
  * nodes (the layout of device/traverse.cuh) and max_triangles x 12 floats
  * (v0, instance bits, v1, primitive bits, v2, 0) in leaf order.  Either

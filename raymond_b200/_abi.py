@@ -141,6 +141,9 @@ class GuideStats(C.Structure):
                 ("reserved", C.c_float)]
 
 
+EXR_AUTO = 0
+EXR_NONE = 1
+EXR_ZIP = 2
 BVH_HOST = 0
 BVH_GPU = 1
 BVH_BUILDERS = {"host": BVH_HOST, "gpu": BVH_GPU}

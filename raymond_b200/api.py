@@ -32,8 +32,10 @@ EXPORTS = [
     "rmd_renderer_guide_params", "rmd_batch_create", "rmd_batch_destroy", "rmd_batch_reset", "rmd_batch_render",
     "rmd_batch_film_read", "rmd_batch_film_read_f64", "rmd_batch_stats", "rmd_batch_autotune",
     "rmd_batch_set_guide", "rmd_batch_guide_stats", "rmd_context_set_bvh_builder", "rmd_scene_bvh_stats",
+    "rmd_film_save_exr", "rmd_batch_film_save_exr",
     "rmd_test_prng", "rmd_test_trace", "rmd_test_material_eval", "rmd_test_generate_source", "rmd_test_jit_compile",
     "rmd_test_guide_forward", "rmd_test_guide_gradient", "rmd_test_guide_mixture", "rmd_test_bvh_read",
+    "rmd_test_exr_write",
 ]
 
 
@@ -63,6 +65,9 @@ def lib() -> C.CDLL:
         "rmd_context_set_bvh_builder": ([vp, C.c_uint32], C.c_int32),
         "rmd_scene_bvh_stats": ([vp, P(_abi.BvhStats)], C.c_int32),
         "rmd_test_bvh_read": ([vp, vp, C.c_uint64, P(C.c_float), C.c_uint64], C.c_int32),
+        "rmd_film_save_exr": ([vp, C.c_char_p, C.c_float, C.c_uint32], C.c_int32),
+        "rmd_batch_film_save_exr": ([vp, C.c_int32, C.c_char_p, C.c_float, C.c_uint32], C.c_int32),
+        "rmd_test_exr_write": ([C.c_char_p, P(C.c_float), C.c_int32, C.c_int32, C.c_float, C.c_uint32], C.c_int32),
         "rmd_context_destroy": ([vp], None),
         "rmd_scene_create": ([vp, P(_abi.SceneDescC), P(vp)], C.c_int32),
         "rmd_scene_destroy": ([vp], None),
@@ -234,6 +239,11 @@ class Renderer:
         check(lib().rmd_film_read_f64(self.h, out.ctypes.data_as(C.POINTER(C.c_double))))
         return out
 
+    def save_exr(self, path, normalized_by: float = 0.0, compression: str = "auto") -> None:
+        """The film as an OpenEXR file (rmd_film_save_exr): RGBA float32, colours
+        times `normalized_by` (0: divided by the samples)."""
+        check(lib().rmd_film_save_exr(self.h, str(path).encode(), normalized_by, _exr_compression(compression)))
+
     def samples(self) -> int:
         v = C.c_uint64()
         check(lib().rmd_film_samples(self.h, C.byref(v)))
@@ -355,6 +365,10 @@ class Batch:
         check(lib().rmd_batch_film_read_f64(self.h, view, out.ctypes.data_as(C.POINTER(C.c_double))))
         return out
 
+    def save_exr(self, view: int, path, normalized_by: float = 0.0, compression: str = "auto") -> None:
+        check(lib().rmd_batch_film_save_exr(self.h, view, str(path).encode(), normalized_by,
+                                            _exr_compression(compression)))
+
     def reset(self) -> None:
         check(lib().rmd_batch_reset(self.h))
 
@@ -471,6 +485,20 @@ def jit_compile(scene: dict[str, Any] | SceneDesc, hoist: bool = True) -> tuple[
     nbytes = C.c_int64()
     check(lib().rmd_test_jit_compile(C.byref(desc.c), int(hoist), log, 1 << 16, C.byref(nbytes)))
     return nbytes.value, log.value.decode(errors="replace")
+
+
+def _exr_compression(name: str) -> int:
+    table = {"auto": _abi.EXR_AUTO, "none": _abi.EXR_NONE, "zip": _abi.EXR_ZIP}
+    if name not in table:
+        raise ValueError(f"compression must be one of {sorted(table)}, not {name!r}")
+    return table[name]
+
+
+def test_exr_write(path, rgb: np.ndarray, normalized_by: float = 1.0, compression: str = "auto") -> None:
+    """Test hook: the film EXR writer applied to a host image (h, w, 3)."""
+    a = np.ascontiguousarray(rgb, np.float32)
+    check(lib().rmd_test_exr_write(str(path).encode(), _f32p(a), a.shape[1], a.shape[0], normalized_by,
+                                   _exr_compression(compression)))
 
 
 def test_prng(mode: int, a: int, b: int, n: int) -> np.ndarray:

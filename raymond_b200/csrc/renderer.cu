@@ -18,6 +18,7 @@
 #include "bvh_build.h"
 #include "bvh_gpu.h"
 #include "codegen.h"
+#include "exr.h"
 #include "device/wavefront.cuh"
 #include "guide.h"
 #include "jit.h"
@@ -1094,6 +1095,32 @@ rmd_status rmd_film_read(rmd_renderer *r, float *rgb, int32_t normalize, uint32_
     return RMD_OK;
 }
 
+static rmd_status saveExr(const char *path, const std::vector<float> &rgb, uint32_t w, uint32_t h, float norm,
+                          uint64_t samples, uint32_t compression) {
+    if (!path) return fail(RMD_ERROR_INVALID_ARGUMENT, "NULL path");
+    if (compression > RMD_EXR_ZIP) return fail(RMD_ERROR_INVALID_ARGUMENT, "unknown EXR compression");
+    if (!(norm > 0.0f)) norm = 1.0f / (float)std::max<uint64_t>(1, samples);
+    const std::string err =
+        rmdhost::writeExrFilm(path, rgb.data(), w, h, norm, (rmdhost::ExrCompression)compression);
+    if (!err.empty()) return fail(RMD_ERROR_INVALID_ARGUMENT, "EXR: " + err);
+    return RMD_OK;
+}
+
+rmd_status rmd_film_save_exr(rmd_renderer *r, const char *path, float normalized_by, uint32_t compression) {
+    if (!r) return fail(RMD_ERROR_INVALID_ARGUMENT, "NULL renderer");
+    std::vector<float> rgb((size_t)r->width * r->height * 3);
+    const rmd_status st = rmd_film_read(r, rgb.data(), 0, 0, 1.0f);
+    if (st != RMD_OK) return st;
+    return saveExr(path, rgb, r->width, r->height, normalized_by, r->samples, compression);
+}
+
+rmd_status rmd_test_exr_write(const char *path, const float *rgb, int32_t width, int32_t height, float normalized_by,
+                              uint32_t compression) {
+    if (!rgb || width <= 0 || height <= 0) return fail(RMD_ERROR_INVALID_ARGUMENT, "invalid image");
+    const std::vector<float> v(rgb, rgb + (size_t)width * height * 3);
+    return saveExr(path, v, (uint32_t)width, (uint32_t)height, normalized_by, 1, compression);
+}
+
 rmd_status rmd_film_read_f64(rmd_renderer *r, double *rgb) {
     if (!r || !rgb) return fail(RMD_ERROR_INVALID_ARGUMENT, "NULL argument");
     if (!r->film64.ptr) return fail(RMD_ERROR_INVALID_ARGUMENT, "no double-precision film (render with film_fp64)");
@@ -1734,6 +1761,16 @@ rmd_status rmd_batch_film_read(rmd_batch *b, int32_t view, float *rgb, int32_t n
     RMD_CUDA(cudaMemcpyAsync(rgb, b->resolve.ptr, (size_t)n * 3 * sizeof(float), cudaMemcpyDeviceToHost, st));
     RMD_CUDA(cudaStreamSynchronize(st));
     return RMD_OK;
+}
+
+rmd_status rmd_batch_film_save_exr(rmd_batch *b, int32_t view, const char *path, float normalized_by,
+                                   uint32_t compression) {
+    if (!b || view < 0 || view >= (int32_t)b->views.size()) return fail(RMD_ERROR_INVALID_ARGUMENT, "invalid argument");
+    const uint32_t w = b->views[view].width, h = b->views[view].height;
+    std::vector<float> rgb((size_t)w * h * 3);
+    const rmd_status st = rmd_batch_film_read(b, view, rgb.data(), 0, 0, 1.0f);
+    if (st != RMD_OK) return st;
+    return saveExr(path, rgb, w, h, normalized_by, b->samples, compression);
 }
 
 rmd_status rmd_batch_film_read_f64(rmd_batch *b, int32_t view, double *rgb) {
