@@ -6,7 +6,9 @@ other nodes the oracle restates: every Principled lobe (diffuse, metallic
 specular, transmission, clearcoat, sheen, anisotropy, alpha, emission), the
 Diffuse / Glossy / Glass / Transparent BSDFs, Mix and Add shaders, Math,
 Vector Math, Checker, Texture Coordinate, MixRGB, Fresnel, Layer Weight,
-Invert, Gamma, RGB to BW, Separate/Combine XYZ and Map Range.
+Invert, Gamma, RGB to BW, Separate/Combine XYZ and Map Range, and the next
+node set: Mapping, Normal Map (tangent and world space), Hue/Saturation,
+Bright/Contrast and Blackbody.
 """
 from __future__ import annotations
 
@@ -60,6 +62,13 @@ _DEFAULTS = {
     "INVERT": {"Fac": ("VALUE", 1.0), "Color": ("RGBA", [0, 0, 0, 1])},
     "MIX_RGB": {"Fac": ("VALUE", 0.5), "Color1": ("RGBA", [0.5, 0.5, 0.5, 1]), "Color2": ("RGBA", [0.5, 0.5, 0.5, 1])},
     "RGBTOBW": {"Color": ("RGBA", [0.5, 0.5, 0.5, 1])},
+    "MAPPING": {"Vector": ("VECTOR", [0, 0, 0]), "Location": ("VECTOR", [0, 0, 0]), "Rotation": ("VECTOR", [0, 0, 0]),
+                "Scale": ("VECTOR", [1, 1, 1])},
+    "NORMAL_MAP": {"Strength": ("VALUE", 1.0), "Color": ("RGBA", [0.5, 0.5, 1, 1])},
+    "HUE_SAT": {"Hue": ("VALUE", 0.5), "Saturation": ("VALUE", 1.0), "Value": ("VALUE", 1.0), "Fac": ("VALUE", 1.0),
+                "Color": ("RGBA", [0.8, 0.8, 0.8, 1])},
+    "BRIGHTCONTRAST": {"Color": ("RGBA", [1, 1, 1, 1]), "Bright": ("VALUE", 0.0), "Contrast": ("VALUE", 0.0)},
+    "BLACKBODY": {"Temperature": ("VALUE", 1500.0)},
 }
 
 
@@ -150,6 +159,46 @@ def materials() -> list[tuple[str, dict]]:
         "Material Output": _out(("Principled BSDF", "BSDF")),
     }))
     mats.append(("emission_only", M.emission((1.0, 0.8, 0.6, 1.0), 4.0)))
+    # the "next" node set: Mapping, Hue/Saturation, Bright/Contrast, Normal Map (tangent and world), Blackbody
+    mats.append(("mapping_hue_normal_map", {
+        "Texture Coordinate": _bsdf("TEX_COORD"),
+        "Mapping": _bsdf("MAPPING", {"type": "MAPPING"}, Vector=_v("VECTOR", link=("Texture Coordinate", "Object")),
+                         Location=_v("VECTOR", [0.1, -0.2, 0.3]), Rotation=_v("VECTOR", [0.3, -0.4, 1.1]),
+                         Scale=_v("VECTOR", [2.0, 1.5, 0.7])),
+        "Checker": _bsdf("TEX_CHECKER", Vector=_v("VECTOR", link=("Mapping", "Vector")),
+                         Color1=_v("RGBA", [0.9, 0.4, 0.1, 1]), Color2=_v("RGBA", [0.1, 0.5, 0.8, 1]),
+                         Scale=_v("VALUE", 3.0)),
+        "Hue Saturation": _bsdf("HUE_SAT", Hue=_v("VALUE", 0.3), Saturation=_v("VALUE", 1.4), Value=_v("VALUE", 0.9),
+                                Fac=_v("VALUE", 0.8), Color=_v("RGBA", link=("Checker", "Color"))),
+        "Bright Contrast": _bsdf("BRIGHTCONTRAST", Color=_v("RGBA", link=("Hue Saturation", "Color")),
+                                 Bright=_v("VALUE", 0.05), Contrast=_v("VALUE", 0.3)),
+        "Normal Map": _bsdf("NORMAL_MAP", {"space": "TANGENT", "uv_map": ""}, Strength=_v("VALUE", 0.7),
+                            Color=_v("RGBA", link=("Checker", "Color"))),
+        "Principled BSDF": {"type": "BSDF_PRINCIPLED",
+                            "inputs": dict(M.principled_inputs(roughness=0.35),
+                                           **{"Base Color": _v("RGBA", link=("Bright Contrast", "Color")),
+                                              "Normal": _v("VECTOR", link=("Normal Map", "Normal"))}),
+                            "parameters": {"distribution": "GGX", "subsurface_method": "RANDOM_WALK"}},
+        "Material Output": _out(("Principled BSDF", "BSDF")),
+    }))
+    mats.append(("blackbody_world_normal", {
+        "Texture Coordinate": _bsdf("TEX_COORD"),
+        "Separate XYZ": _bsdf("SEPXYZ", Vector=_v("VECTOR", link=("Texture Coordinate", "Generated"))),
+        "Map Range": _bsdf("MAP_RANGE", {"data_type": "FLOAT", "interpolation_type": "LINEAR", "clamp": False},
+                           Value=_v("VALUE", link=("Separate XYZ", "X")),
+                           **{"From Min": _v("VALUE", 0.0), "From Max": _v("VALUE", 1.0),
+                              "To Min": _v("VALUE", 500.0), "To Max": _v("VALUE", 13000.0)}),
+        "Blackbody": _bsdf("BLACKBODY", Temperature=_v("VALUE", link=("Map Range", "Result"))),
+        "Normal Map": _bsdf("NORMAL_MAP", {"space": "WORLD", "uv_map": ""}, Strength=_v("VALUE", 0.9),
+                            Color=_v("RGBA", link=("Texture Coordinate", "Generated"))),
+        "Principled BSDF": {"type": "BSDF_PRINCIPLED",
+                            "inputs": dict(M.principled_inputs(roughness=0.5, emission_strength=0.2),
+                                           **{"Base Color": _v("RGBA", link=("Blackbody", "Color")),
+                                              "Emission": _v("RGBA", link=("Blackbody", "Color")),
+                                              "Normal": _v("VECTOR", link=("Normal Map", "Normal"))}),
+                            "parameters": {"distribution": "GGX", "subsurface_method": "RANDOM_WALK"}},
+        "Material Output": _out(("Principled BSDF", "BSDF")),
+    }))
     return mats
 
 

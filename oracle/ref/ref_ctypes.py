@@ -77,6 +77,8 @@ def shading_records(n: int, seed: int) -> np.ndarray:
     rec[:, 18:21] = unit(n)
     rec[:, 21:24] = rng.uniform(0, 1, (n, 3))
     rec[:, 24] = 1  # camera ray
+    t = np.cross(nrm, unit(n))  # a tangent; the bitangent is normal x tangent
+    rec[:, 25:28] = t / np.linalg.norm(t, axis=1, keepdims=True)
     return rec
 
 

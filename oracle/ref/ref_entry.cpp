@@ -163,7 +163,7 @@ int ref_num_materials() { return findTable("pin")->numSurface; }
 // One material of pin_materials.py on shading records, evaluated and sampled
 // the way handleIntersections does (intersection.metal:100-104,135-144,149-185).
 // Record (28 floats): position, normal, trueNormal, generated, uv, wo, wi, rnd
-// (float3 each), rayFlags, 3 unused.  Output (16 floats): emission, evaluate
+// (float3 each), rayFlags, tangent tu (bitangent normal x tu).  Output (16 floats): emission, evaluate
 // value, evaluate pdf, sampled wi, sampled weight, sampled pdf, sampled flags,
 // alpha.
 int ref_material_eval(int material, const float *records, int n, float *out) {
@@ -185,7 +185,8 @@ int ref_material_eval(int material, const float *records, int n, float *out) {
         sh.rnd = v3(7);
         sh.rayFlags = RayFlags((uint8_t)r[24]);
         sh.object = sh.generated;
-        sh.tu = sh.tv = float3(0);
+        sh.tu = float3(r[25], r[26], r[27]);  // the tangent frame: tu given, tv = normal x tu
+        sh.tv = cross(sh.normal, sh.tu);
         sh.distance = 0;
         shadeSurface((MaterialIndex)material, ctx, sh);
         float3 shNormal;

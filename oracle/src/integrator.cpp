@@ -596,7 +596,7 @@ extern "C" void oracle_fractal_noise3(const float *p, int32_t n, float detail, f
         out[i] = noise::fractal_noise(float3(p[3 * i], p[3 * i + 1], p[3 * i + 2]), detail, roughness);
 }
 
-// record: position, normal, trueNormal, generated, uv, wo, wi, rnd (8 x float3), rayFlags, 3 pad = 28 floats
+// record: position, normal, trueNormal, generated, uv, wo, wi, rnd (8 x float3), rayFlags, tangent tu (3) = 28 floats
 // out: emission(3), eval(3), evalPdf, sample wi(3), sample weight(3), sample pdf, sample flags, alpha = 16 floats
 extern "C" int oracle_material_eval(const oracle_scene *s, int32_t material, const float *records, int32_t n,
                                     float *out) {
@@ -615,6 +615,8 @@ extern "C" int oracle_material_eval(const oracle_scene *s, int32_t material, con
         sh.rnd = v3(7);
         sh.rayFlags = (uint8_t)r[24];
         sh.object = sh.generated;
+        sh.tu = float3(r[25], r[26], r[27]);  // the tangent frame: tu given, tv = normal x tu
+        sh.tv = cross(sh.normal, sh.tu);
         shadeSurface((uint16_t)material, s->data, sh);
         float3 shNormal;
         if (all_zero(sh.material.normal)) {

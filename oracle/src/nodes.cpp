@@ -415,6 +415,115 @@ struct ColorInvert {  // nodes.hpp:1387-1394
     }
     static void describe(FieldList &fl) { using T = ColorInvert; FLD(T, color, K_F4); FLD(T, fac, K_F1); }
 };
+struct Mapping {  // nodes.hpp:346-364 with euler2mat of math.hpp:46-68 (one Type: MAPPING)
+    float3 scale, rotation, location, vector;
+    void compute(const SceneData &, ShadingContext &) {
+        const float sx = std::sin(rotation.x), cx = std::cos(rotation.x);
+        const float sy = std::sin(rotation.y), cy = std::cos(rotation.y);
+        const float sz = std::sin(rotation.z), cz = std::cos(rotation.z);
+        float3x3 m;
+        m.c[0] = float3(cy * cz, cy * sz, -sy);
+        m.c[1] = float3(sy * sx * cz - cx * sz, sy * sx * sz + cx * cz, cy * sx);
+        m.c[2] = float3(sy * cx * cz + sx * sz, sy * cx * sz - sx * cz, cy * cx);
+        vector = m * (vector * scale) + location;
+    }
+    static void describe(FieldList &fl) {
+        using T = Mapping;
+        FLD(T, scale, K_F3); FLD(T, rotation, K_F3); FLD(T, location, K_F3); FLD(T, vector, K_F3);
+    }
+};
+struct NormalMap {  // nodes.hpp:1060-1097
+    float4 color;
+    float strength;
+    float3 normal;
+    int space = 0;  // 0 tangent, 1 world
+    void compute(const SceneData &, ShadingContext &sh) {
+        const float s = std::max(strength, 0.0f);
+        float3 n = normalize(2 * color.xyz() - float3(1.0f));
+        n = normalize(s * n + (1 - s) * float3(0, 0, 1));
+        if (space == 0) {
+            float3x3 onb;
+            onb.c[0] = sh.tu;
+            onb.c[1] = sh.tv;
+            onb.c[2] = sh.normal;
+            n = onb * n;
+        }
+        normal = n;
+    }
+    static void describe(FieldList &fl) {
+        using T = NormalMap;
+        FLD(T, color, K_F4); FLD(T, strength, K_F1); FLD(T, normal, K_F3);
+    }
+};
+struct HueSaturation {  // nodes.hpp:1261-1277
+    float4 color;
+    float fac, hue, saturation, value;
+    void compute(const SceneData &, ShadingContext &) {
+        float3 hsv = rgb2hsv(color.xyz());
+        hsv.x = std::fmod(hsv.x + hue + 0.5f, 1.0f);
+        hsv.y = saturate(hsv.y * saturation);
+        hsv.z *= value;
+        float3 r = hsv2rgb(hsv);
+        r = float3(std::max(r.x, 0.0f), std::max(r.y, 0.0f), std::max(r.z, 0.0f));
+        color = float4(lerp(color.xyz(), r, fac), color.w);
+    }
+    static void describe(FieldList &fl) {
+        using T = HueSaturation;
+        FLD(T, color, K_F4); FLD(T, fac, K_F1); FLD(T, hue, K_F1); FLD(T, saturation, K_F1); FLD(T, value, K_F1);
+    }
+};
+struct BrightnessContrast {  // nodes.hpp:1279-1290
+    float bright, contrast;
+    float4 color;
+    void compute(const SceneData &, ShadingContext &) {
+        const float a = 1 + contrast, b = bright - contrast / 2;
+        for (int d = 0; d < 4; d++) color[d] = std::max(a * color[d] + b, 0.0f);
+    }
+    static void describe(FieldList &fl) {
+        using T = BrightnessContrast;
+        FLD(T, bright, K_F1); FLD(T, contrast, K_F1); FLD(T, color, K_F4);
+    }
+};
+// Cycles' blackbody fit (the coefficient table of nodes.hpp:1421-1449)
+static const float kBlackbodyR[7][3] = {
+    {1.61919106e+03f, -2.05010916e-03f, 5.02995757e+00f}, {2.48845471e+03f, -1.11330907e-03f, 3.22621544e+00f},
+    {3.34143193e+03f, -4.86551192e-04f, 1.76486769e+00f}, {4.09461742e+03f, -1.27446582e-04f, 7.25731635e-01f},
+    {4.67028036e+03f, 2.91258199e-05f, 1.26703442e-01f},  {4.59509185e+03f, 2.87495649e-05f, 1.50345020e-01f},
+    {3.78717450e+03f, 9.35907826e-06f, 3.99075871e-01f}};
+static const float kBlackbodyG[7][3] = {
+    {-4.88999748e+02f, 6.04330754e-04f, -7.55807526e-02f}, {-7.55994277e+02f, 3.16730098e-04f, 4.78306139e-01f},
+    {-1.02363977e+03f, 1.20223470e-04f, 9.36662319e-01f},  {-1.26571316e+03f, 4.87340896e-06f, 1.27054498e+00f},
+    {-1.42529332e+03f, -4.01150431e-05f, 1.43972784e+00f}, {-1.17554822e+03f, -2.16378048e-05f, 1.30408023e+00f},
+    {-5.00799571e+02f, -4.59832026e-06f, 1.09098763e+00f}};
+static const float kBlackbodyB[7][4] = {
+    {5.96945309e-11f, -4.85742887e-08f, -9.70622247e-05f, -4.07936148e-03f},
+    {2.40430366e-11f, 5.55021075e-08f, -1.98503712e-04f, 2.89312858e-02f},
+    {-1.40949732e-11f, 1.89878968e-07f, -3.56632824e-04f, 9.10767778e-02f},
+    {-3.61460868e-11f, 2.84822009e-07f, -4.93211319e-04f, 1.56723440e-01f},
+    {-1.97075738e-11f, 1.75359352e-07f, -2.50542825e-04f, -2.22783266e-02f},
+    {-1.61997957e-13f, -1.64216008e-08f, 3.86216271e-04f, -7.38077418e-01f},
+    {6.72650283e-13f, -2.73078809e-08f, 4.24098264e-04f, -7.52335691e-01f}};
+struct Blackbody {  // nodes.hpp:1451-1495
+    float temperature;
+    float4 color;
+    void compute(const SceneData &, ShadingContext &) {
+        const float t = temperature;
+        float3 c;
+        if (t >= 12000.0f) {
+            c = float3(0.8262954810464208f, 0.9945080501520986f, 1.566307710274283f);
+        } else if (t < 800.0f) {
+            c = float3(5.413294490189271f, -0.20319390035873933f, -0.0822535242887164f);
+        } else {
+            const int i = t >= 6365.0f ? 6 : t >= 3315.0f ? 5 : t >= 1902.0f ? 4 : t >= 1449.0f ? 3
+                        : t >= 1167.0f ? 2 : t >= 965.0f ? 1 : 0;
+            const float *r = kBlackbodyR[i], *g = kBlackbodyG[i], *b = kBlackbodyB[i];
+            const float inv = 1.0f / t;
+            c = float3(r[0] * inv + r[1] * t + r[2], g[0] * inv + g[1] * t + g[2], ((b[0] * t + b[1]) * t + b[2]) * t + b[3]);
+        }
+        color = float4(c / luminance(c), 1.0f);
+    }
+    static void describe(FieldList &fl) { using T = Blackbody; FLD(T, temperature, K_F1); FLD(T, color, K_F4); }
+};
 struct Gamma {  // nodes.hpp:1292-1302
     float4 color;
     float gamma;
@@ -848,6 +957,19 @@ static std::unique_ptr<NodeImpl> makeKernel(const rmd_node &n) {
     if (t == "RGBTOBW") return std::make_unique<Box<RGBToBW>>();
     if (t == "INVERT") return std::make_unique<Box<ColorInvert>>();
     if (t == "GAMMA") return std::make_unique<Box<Gamma>>();
+    if (t == "MAPPING") {
+        if (enumIndex(paramString(n, "type", "MAPPING"), {"MAPPING"}) < 0) return unsupported();
+        return std::make_unique<Box<Mapping>>();
+    }
+    if (t == "NORMAL_MAP") {
+        auto b = std::make_unique<Box<NormalMap>>();
+        b->v.space = enumIndex(paramString(n, "space", "TANGENT"), {"TANGENT", "WORLD"});
+        if (b->v.space < 0) return unsupported();
+        return b;
+    }
+    if (t == "HUE_SAT") return std::make_unique<Box<HueSaturation>>();
+    if (t == "BRIGHTCONTRAST") return std::make_unique<Box<BrightnessContrast>>();
+    if (t == "BLACKBODY") return std::make_unique<Box<Blackbody>>();
     if (t == "FRESNEL") return std::make_unique<Box<Fresnel>>();
     if (t == "LAYER_WEIGHT") return std::make_unique<Box<LayerWeight>>();
     if (t == "EMISSION") return std::make_unique<Box<Emission>>();

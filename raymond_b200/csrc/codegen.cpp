@@ -98,6 +98,11 @@ const std::map<std::string, KernelDesc> &kernelTable() {
         add("RGBToBW", {{"color", F4}, {"val", F1}});
         add("ColorInvert", {{"color", F4}, {"fac", F1}});
         add("Gamma", {{"color", F4}, {"gamma", F1}});
+        add("Mapping", {{"scale", F3}, {"rotation", F3}, {"location", F3}, {"vector", F3}});
+        add("NormalMap", {{"color", F4}, {"strength", F1}, {"normal", F3}});
+        add("HueSaturation", {{"color", F4}, {"fac", F1}, {"hue", F1}, {"saturation", F1}, {"value", F1}});
+        add("BrightnessContrast", {{"bright", F1}, {"contrast", F1}, {"color", F4}});
+        add("Blackbody", {{"temperature", F1}, {"color", F4}});
         add("Fresnel", {{"ior", F1}, {"normal", F3}, {"fac", F1}});
         add("LayerWeight", {{"blend", F1}, {"normal", F3}, {"fresnel", F1}, {"facing", F1}});
         add("Emission", {{"color", F4}, {"strength", F1}, {"weight", F1}, {"emission", SH}});
@@ -284,6 +289,16 @@ Invocation makeInvocation(const rmd_node &n, Emitter &em) {
     } else if (t == "RGBTOBW") plain("RGBToBW");
     else if (t == "INVERT") plain("ColorInvert");
     else if (t == "GAMMA") plain("Gamma");
+    else if (t == "MAPPING") {  // :507-510
+        inv.kernel = "Mapping";
+        inv.type = "Mapping<" + enumValue("Mapping", "TYPE", paramString(n, "type", "MAPPING"), {"MAPPING"}) + ">";
+    } else if (t == "NORMAL_MAP") {  // :517-523 (UV maps are ignored there too)
+        inv.kernel = "NormalMap";
+        inv.type = "NormalMap<" + enumValue("NormalMap", "SPACE", paramString(n, "space", "TANGENT"), {"TANGENT", "WORLD"}) +
+                   ">";
+    } else if (t == "HUE_SAT") plain("HueSaturation");
+    else if (t == "BRIGHTCONTRAST") plain("BrightnessContrast");
+    else if (t == "BLACKBODY") plain("Blackbody");
     else if (t == "FRESNEL") plain("Fresnel");
     else if (t == "LAYER_WEIGHT") plain("LayerWeight");
     else if (t == "EMISSION") plain("Emission");

@@ -312,7 +312,7 @@ extern "C" __global__ void rmd_envmap_build(const __grid_constant__ rmd::Context
 // Test hook: shade records with one material and evaluate / sample its BSDF the
 // way handleIntersections does (intersection.metal:93-185).  Record layout:
 // position, normal, trueNormal, generated, uv, wo, wi, rnd (float3 each),
-// rayFlags, 3 pad; output: emission, eval value, eval pdf, sampled wi,
+// rayFlags, tangent tu (bitangent normal x tu); output: emission, eval value, eval pdf, sampled wi,
 // sampled weight, sampled pdf, sampled flags, alpha.
 extern "C" __global__ void rmd_material_eval(const __grid_constant__ rmd::Context ctx, unsigned material,
                                              const float *records, float *out, int n) {
@@ -331,7 +331,8 @@ extern "C" __global__ void rmd_material_eval(const __grid_constant__ rmd::Contex
     sh.rnd = make_float3(r[21], r[22], r[23]);
     sh.rayFlags = (unsigned)r[24];
     sh.object = sh.generated;
-    sh.tu = sh.tv = f3(0.0f);
+    sh.tu = make_float3(r[25], r[26], r[27]);  // the tangent frame: tu given, tv = normal x tu
+    sh.tv = cross(sh.normal, sh.tu);
     sh.distance = 0.0f;
     shadeSurface(material, ctx, sh);
     float3 shNormal;

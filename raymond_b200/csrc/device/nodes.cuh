@@ -400,6 +400,123 @@ struct ColorInvert {  // nodes.hpp:1387-1394
         color = f4(c, color.w);
     }
 };
+struct kMapping {
+    enum Type { TYPE_MAPPING };  // the exporter writes the node's type, MAPPING, for every vector type
+};
+// nodes.hpp:346-364: vector = R(rotation) (vector * scale) + location, R the
+// XYZ Euler rotation of math.hpp:46-68 (Cycles' node_mapping.osl)
+template <kMapping::Type Type>
+struct Mapping {
+    float3 scale, rotation, location, vector;
+    RMD_HD void compute(const Context &, const ShadingContext &) {
+        float sx, cx, sy, cy, sz, cz;
+        sincosf(rotation.x, &sx, &cx);
+        sincosf(rotation.y, &sy, &cy);
+        sincosf(rotation.z, &sz, &cz);
+        float3x3 r;
+        r.c[0] = make_float3(cy * cz, cy * sz, -sy);
+        r.c[1] = make_float3(sy * sx * cz - cx * sz, sy * sx * sz + cx * cz, cy * sx);
+        r.c[2] = make_float3(sy * cx * cz + sx * sz, sy * cx * sz - sx * cz, cy * cx);
+        vector = r * (vector * scale) + location;
+    }
+};
+
+struct kNormalMap {
+    enum Space { SPACE_TANGENT, SPACE_WORLD };
+};
+// nodes.hpp:1060-1097: the colour as a normal, blended towards +z by
+// strength, in the shading point's (tu, tv, normal) frame (tangent space) or
+// as it is (world space)
+template <kNormalMap::Space Space>
+struct NormalMap {
+    float4 color;
+    float strength;
+    float3 normal;
+    RMD_HD void compute(const Context &, const ShadingContext &sh) {
+        const float s = fmaxf(strength, 0.0f);
+        float3 n = normalize(2.0f * xyz(color) - f3(1.0f));
+        n = normalize(s * n + (1.0f - s) * make_float3(0.0f, 0.0f, 1.0f));
+        if (Space == kNormalMap::SPACE_TANGENT) n = sh.tu * n.x + sh.tv * n.y + sh.normal * n.z;
+        normal = n;
+    }
+};
+
+struct HueSaturation {  // nodes.hpp:1261-1277
+    float4 color;
+    float fac, hue, saturation, value;
+    RMD_HD void compute(const Context &, const ShadingContext &) {
+        float3 hsv = rgb2hsv(xyz(color));
+        hsv.x = fmodf(hsv.x + hue + 0.5f, 1.0f);
+        hsv.y = saturate(hsv.y * saturation);
+        hsv.z *= value;
+        const float3 rgb = hsv2rgb(hsv);
+        const float3 result = make_float3(fmaxf(rgb.x, 0.0f), fmaxf(rgb.y, 0.0f), fmaxf(rgb.z, 0.0f));
+        color = f4(lerp(xyz(color), result, fac), color.w);
+    }
+};
+
+struct BrightnessContrast {  // nodes.hpp:1279-1290 (alpha included, as there)
+    float bright, contrast;
+    float4 color;
+    RMD_HD void compute(const Context &, const ShadingContext &) {
+        const float a = 1.0f + contrast, b = bright - contrast / 2.0f;
+        color = make_float4(fmaxf(a * color.x + b, 0.0f), fmaxf(a * color.y + b, 0.0f), fmaxf(a * color.z + b, 0.0f),
+                            fmaxf(a * color.w + b, 0.0f));
+    }
+};
+
+// Blackbody colour: Cycles' piecewise fit over 800..12000 K, a / t + b t + c
+// for red and green and a cubic in t for blue, one coefficient row per
+// temperature band (the table of nodes.hpp:1421-1449, which must be the same
+// numbers for the colours to match).
+struct BlackbodyFit {
+    float r[7][3], g[7][3], b[7][4];
+};
+__constant__ const BlackbodyFit kBlackbodyFit = {
+    {{1.61919106e+03f, -2.05010916e-03f, 5.02995757e+00f},
+     {2.48845471e+03f, -1.11330907e-03f, 3.22621544e+00f},
+     {3.34143193e+03f, -4.86551192e-04f, 1.76486769e+00f},
+     {4.09461742e+03f, -1.27446582e-04f, 7.25731635e-01f},
+     {4.67028036e+03f, 2.91258199e-05f, 1.26703442e-01f},
+     {4.59509185e+03f, 2.87495649e-05f, 1.50345020e-01f},
+     {3.78717450e+03f, 9.35907826e-06f, 3.99075871e-01f}},
+    {{-4.88999748e+02f, 6.04330754e-04f, -7.55807526e-02f},
+     {-7.55994277e+02f, 3.16730098e-04f, 4.78306139e-01f},
+     {-1.02363977e+03f, 1.20223470e-04f, 9.36662319e-01f},
+     {-1.26571316e+03f, 4.87340896e-06f, 1.27054498e+00f},
+     {-1.42529332e+03f, -4.01150431e-05f, 1.43972784e+00f},
+     {-1.17554822e+03f, -2.16378048e-05f, 1.30408023e+00f},
+     {-5.00799571e+02f, -4.59832026e-06f, 1.09098763e+00f}},
+    {{5.96945309e-11f, -4.85742887e-08f, -9.70622247e-05f, -4.07936148e-03f},
+     {2.40430366e-11f, 5.55021075e-08f, -1.98503712e-04f, 2.89312858e-02f},
+     {-1.40949732e-11f, 1.89878968e-07f, -3.56632824e-04f, 9.10767778e-02f},
+     {-3.61460868e-11f, 2.84822009e-07f, -4.93211319e-04f, 1.56723440e-01f},
+     {-1.97075738e-11f, 1.75359352e-07f, -2.50542825e-04f, -2.22783266e-02f},
+     {-1.61997957e-13f, -1.64216008e-08f, 3.86216271e-04f, -7.38077418e-01f},
+     {6.72650283e-13f, -2.73078809e-08f, 4.24098264e-04f, -7.52335691e-01f}}};
+
+struct Blackbody {  // nodes.hpp:1451-1495: the fit's colour divided by its luminance
+    float temperature;
+    float4 color;
+    RMD_HD void compute(const Context &, const ShadingContext &) {
+        float3 c;
+        const float t = temperature;
+        if (t >= 12000.0f) {
+            c = make_float3(0.8262954810464208f, 0.9945080501520986f, 1.566307710274283f);
+        } else if (t < 800.0f) {
+            c = make_float3(5.413294490189271f, -0.20319390035873933f, -0.0822535242887164f);
+        } else {
+            const int i = t >= 6365.0f ? 6 : t >= 3315.0f ? 5 : t >= 1902.0f ? 4 : t >= 1449.0f ? 3 :
+                          t >= 1167.0f ? 2 : t >= 965.0f ? 1 : 0;
+            const float *r = kBlackbodyFit.r[i], *g = kBlackbodyFit.g[i], *b = kBlackbodyFit.b[i];
+            const float inv = 1.0f / t;
+            c = make_float3(r[0] * inv + r[1] * t + r[2], g[0] * inv + g[1] * t + g[2],
+                            ((b[0] * t + b[1]) * t + b[2]) * t + b[3]);
+        }
+        color = f4(c / luminance(c), 1.0f);
+    }
+};
+
 struct Gamma {  // nodes.hpp:1292-1302
     float4 color;
     float gamma;

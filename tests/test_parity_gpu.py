@@ -149,6 +149,53 @@ def test_material_eval_parity(spheres):
         assert close.all(axis=1).mean() > 0.999, m
 
 
+def _pin_modules():
+    import sys
+    from pathlib import Path
+
+    sys.path.insert(0, str(Path(__file__).resolve().parents[1] / "oracle" / "ref"))
+    import pin_materials
+    import ref_ctypes
+
+    return pin_materials, ref_ctypes
+
+
+def test_pin_materials_parity(gpu_ctx):
+    """Every pinning material (the node set checked against the reference's own
+    node library on the CPU, Mapping, Normal Map, Hue/Saturation,
+    Bright/Contrast and Blackbody included) evaluated and sampled on the GPU
+    against the oracle, with a tangent frame in the records."""
+    pin, R = _pin_modules()
+    desc = SceneDesc(pin.scene())
+    scene = api.Scene(gpu_ctx, desc)
+    orc = O.OracleScene(desc)
+    rec = R.shading_records(4096, seed=123)
+    for m, (name, _) in enumerate(pin.materials()):
+        g = scene.material_eval(m, rec)
+        c = orc.material_eval(m, rec)
+        close = np.isclose(g, c, rtol=1e-3, atol=1e-5) | (np.isnan(g) & np.isnan(c))
+        assert close.all(axis=1).mean() > 0.999, name
+
+
+def test_next_node_set_render(gpu_ctx):
+    """The Cornell box with its walls in the Mapping / Hue / Bright-Contrast /
+    tangent Normal Map material and its boxes in the Blackbody / world Normal
+    Map one: per-sample parity with the oracle (tangents from the UVs)."""
+    pin, _ = _pin_modules()
+    sc = scenes.cornell(seed=1, envmap_exponent=7)
+    mats = dict(pin.materials())
+    base = len(sc["materials"])
+    sc["materials"] = sc["materials"] + [("nodes_a", mats["mapping_hue_normal_map"]),
+                                         ("nodes_b", mats["blackbody_world_normal"])]
+    for i, sh in enumerate(sc["shapes"][:-1]):  # all but the light
+        sh["materials"] = np.full_like(sh["materials"], base + (0 if i < 5 else 1))
+    desc = SceneDesc(sc)
+    scene = api.Scene(gpu_ctx, desc)
+    orc = O.OracleScene(desc)
+    fr = per_sample(desc, scene, orc, 96, 96, range(4), 8)
+    assert min(fr) >= MIN_MATCH, fr
+
+
 def _all_lights_scene():
     return scenes.cornell_all_lights(seed=4, envmap_exponent=7)
 
