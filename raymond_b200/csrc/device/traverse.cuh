@@ -132,6 +132,13 @@ RMD_HD uint32_t intersectChildren(const WideNode &n, const float3 idir, const fl
     const float bx = (n.originScale.x - org.x) * idir.x;
     const float by = (n.originScale.y - org.y) * idir.y;
     const float bz = (n.originScale.z - org.z) * idir.z;
+    // origin - org and its product with the rounded 1/d each round once, an
+    // absolute error of at most 2^-23 |b| in every plane distance, which a
+    // relative widening cannot cover when the hit lies close to the origin
+    // next to a far node origin: near planes move down and far planes up by
+    // 3e-7 |b| (per axis, so an axis the ray runs parallel to stays decided)
+    const float ex = 3.0e-7f * fabsf(bx), ey = 3.0e-7f * fabsf(by), ez = 3.0e-7f * fabsf(bz);
+    const float bxN = bx - ex, bxF = bx + ex, byN = by - ey, byF = by + ey, bzN = bz - ez, bzF = bz + ez;
     // per axis the near plane is the lower bound for a positive direction
     const uint2 loX = make_uint2(n.qloXY.x, n.qloXY.y), hiX = make_uint2(n.qloZqhiX.z, n.qloZqhiX.w);
     const uint2 loY = make_uint2(n.qloXY.z, n.qloXY.w), hiY = make_uint2(n.qhiYZ.x, n.qhiYZ.y);
@@ -150,9 +157,9 @@ RMD_HD uint32_t intersectChildren(const WideNode &n, const float3 idir, const fl
 #pragma unroll
         for (uint32_t i = 0; i < 4; i++) {
             const uint32_t slot = 4 * half + i;
-            const float t0x = fmaf(byteToFloat(nxw, i), ax, bx), t1x = fmaf(byteToFloat(fxw, i), ax, bx);
-            const float t0y = fmaf(byteToFloat(nyw, i), ay, by), t1y = fmaf(byteToFloat(fyw, i), ay, by);
-            const float t0z = fmaf(byteToFloat(nzw, i), az, bz), t1z = fmaf(byteToFloat(fzw, i), az, bz);
+            const float t0x = fmaf(byteToFloat(nxw, i), ax, bxN), t1x = fmaf(byteToFloat(fxw, i), ax, bxF);
+            const float t0y = fmaf(byteToFloat(nyw, i), ay, byN), t1y = fmaf(byteToFloat(fyw, i), ay, byF);
+            const float t0z = fmaf(byteToFloat(nzw, i), az, bzN), t1z = fmaf(byteToFloat(fzw, i), az, bzF);
             const float enter = fmaxf(fmaxf(t0x, t0y), fmaxf(t0z, tmin));
             const float leave = fminf(fminf(t1x, t1y), fminf(t1z, tmax));
             // widen the far bound by a few ulps (Ize 2013) so FMA rounding never culls a hit
