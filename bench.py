@@ -385,7 +385,7 @@ def guided_leg(api, ctx, oracle_spp: int, size=(GUIDED_W, GUIDED_H)) -> dict:
         plain_ms += plain.stats()["ms_total"]
     e_plain = relmse(plain.film(normalize=True), reference)
     plain.close()
-    settings = {"batch_size": 1 << 20, "learning_rate": 1e-3}
+    settings = {"batch_size": 1 << 20, "learning_rate": 1e-3, "steps_per_batch": 8, "step_records": 1 << 13}
     g = api.Renderer(scene, W, H)
     g.set_guide(sampling=True, training=True, seed=1, **settings)
     ms, spp, curve, parity = 0.0, 0, [], None

@@ -396,9 +396,9 @@ typedef struct rmd_guide_settings {
     float learning_rate;     /* 0 = 1e-3 */
     uint32_t reset;          /* 1: re-initialise the network from `seed` */
     uint32_t seed;
-    uint32_t step_records;   /* records each step trains on, drawn from the replay ring; 0 = 1 << 14 */
+    uint32_t step_records;   /* records each step trains on, drawn from the replay ring; 0 = 1 << 13 */
     uint32_t replay_records; /* ring of the latest nonzero-target records; power of two, 0 = 1 << 18 */
-    uint32_t steps_per_batch; /* Adam steps per `batch_size` samples; 0 = 1 */
+    uint32_t steps_per_batch; /* Adam steps per `batch_size` samples; 0 = 8 */
     uint32_t skip_light_records; /* 1: train on the paths' samples only, not on the light samples */
     uint32_t guided_depth;   /* guide the vertices of path depth below this; 0 = all */
 } rmd_guide_settings;

@@ -40,7 +40,8 @@ rmd_status rmd_test_bvh_read(const rmd_scene *scene, void *nodes, uint64_t max_n
 
 /* Shade n records with surface material `material` and evaluate / sample its
  * BSDF as handleIntersections does.  Record: position, normal, trueNormal,
- * generated, uv, wo, wi, rnd (float3 each), rayFlags, 3 pad (28 floats).
+ * generated, uv, wo, wi, rnd (float3 each), rayFlags, tangent tu (3; the bitangent
+ * is normal x tu) = 28 floats.
  * Output: emission(3), eval(3), eval pdf, sampled wi(3), sampled weight(3),
  * sampled pdf, sampled flags, alpha (16 floats). */
 rmd_status rmd_test_material_eval(const rmd_scene *scene, int32_t material, const float *records, int32_t n,

@@ -286,8 +286,8 @@ class Renderer:
         the guide mixture by one-sample MIS and/or train the network online
         during render().  One Adam step per `batch_size` tracer samples (0 =
         2^20), learning rate 0 = 1e-3, each step on `step_records` records
-        (0 = 2^14) drawn from a ring of the latest `replay_records` (0 = 2^18);
-        `steps_per_batch` (0 = 1) Adam steps per batch; `light_records`: the
+        (0 = 2^13) drawn from a ring of the latest `replay_records` (0 = 2^18);
+        `steps_per_batch` (0 = 8) Adam steps per batch; `light_records`: the
         light samples of every vertex are training samples too; vertices of
         path depth below `guided_depth` (0 = all) sample from the guide.  The
         network is initialised from `seed` on first use or when `reset` is set."""

@@ -24,7 +24,7 @@
 namespace rmd {
 namespace {
 
-constexpr int kWarps = 4;  // warps per block; each owns 16 samples at a time
+constexpr int kWarps = 4;  // warps per block (the shared memory of one block per SM); each owns 16 samples at a time
 constexpr int kLd0 = GUIDE_INPUTS + 8, kLdH = GUIDE_HIDDEN + 8, kLdO = GUIDE_OUTPUTS + 4;  // padded rows
 
 // per-warp shared scratch (bf16 activations as uint16_t)
@@ -62,27 +62,21 @@ __device__ __forceinline__ void loadAT(uint32_t a[4], const uint16_t *m, int ld,
     a[2] = pack2(m[(2 * t + 8) * ld + m0 + g], m[(2 * t + 9) * ld + m0 + g]);
     a[3] = pack2(m[(2 * t + 8) * ld + m0 + g + 8], m[(2 * t + 9) * ld + m0 + g + 8]);
 }
-// B(k, n) = W[n][k] for a row-major [n][k] matrix (forward weights)
+// B(k, n) = W[n][k] for a row-major [n][k] matrix (forward weights, in shared memory)
 __device__ __forceinline__ void loadBnk(uint32_t b[2], const uint16_t *w, int ld, int n0, int k0, int g, int t) {
-    b[0] = __ldg(reinterpret_cast<const uint32_t *>(&w[(n0 + g) * ld + k0 + 2 * t]));
-    b[1] = __ldg(reinterpret_cast<const uint32_t *>(&w[(n0 + g) * ld + k0 + 8 + 2 * t]));
+    b[0] = *reinterpret_cast<const uint32_t *>(&w[(n0 + g) * ld + k0 + 2 * t]);
+    b[1] = *reinterpret_cast<const uint32_t *>(&w[(n0 + g) * ld + k0 + 8 + 2 * t]);
 }
 // B(k, n) = M[k][n] for a row-major [k][n] matrix
-template <bool GLOBAL>
 __device__ __forceinline__ void loadBkn(uint32_t b[2], const uint16_t *m, int ld, int n0, int k0, int g, int t) {
-    if (GLOBAL) {
-        b[0] = pack2(__ldg(&m[(k0 + 2 * t) * ld + n0 + g]), __ldg(&m[(k0 + 2 * t + 1) * ld + n0 + g]));
-        b[1] = pack2(__ldg(&m[(k0 + 2 * t + 8) * ld + n0 + g]), __ldg(&m[(k0 + 2 * t + 9) * ld + n0 + g]));
-    } else {
-        b[0] = pack2(m[(k0 + 2 * t) * ld + n0 + g], m[(k0 + 2 * t + 1) * ld + n0 + g]);
-        b[1] = pack2(m[(k0 + 2 * t + 8) * ld + n0 + g], m[(k0 + 2 * t + 9) * ld + n0 + g]);
-    }
+    b[0] = pack2(m[(k0 + 2 * t) * ld + n0 + g], m[(k0 + 2 * t + 1) * ld + n0 + g]);
+    b[1] = pack2(m[(k0 + 2 * t + 8) * ld + n0 + g], m[(k0 + 2 * t + 9) * ld + n0 + g]);
 }
 
-// out[16][N] = act(in[16][K] . W^T + b): W row-major [N][K] (bf16), b fp32
+// out[16][N] = act(in[16][K] . W^T + b): W row-major [N][K] (bf16, rows ldW apart), b fp32
 template <int K, int N, bool RELU>
-__device__ __forceinline__ void denseForward(const uint16_t *in, int ldIn, const uint16_t *w, const float *bias,
-                                             uint16_t *outBf, float *outF, int ldOut, int g, int t) {
+__device__ __forceinline__ void denseForward(const uint16_t *in, int ldIn, const uint16_t *w, int ldW,
+                                             const float *bias, uint16_t *outBf, float *outF, int ldOut, int g, int t) {
 #pragma unroll 1
     for (int n0 = 0; n0 < N; n0 += 8) {
         float c[4] = {0.0f, 0.0f, 0.0f, 0.0f};
@@ -90,10 +84,10 @@ __device__ __forceinline__ void denseForward(const uint16_t *in, int ldIn, const
         for (int k0 = 0; k0 < K; k0 += 16) {
             uint32_t a[4], b[2];
             loadA(a, in, ldIn, k0, g, t);
-            loadBnk(b, w, K, n0, k0, g, t);
+            loadBnk(b, w, ldW, n0, k0, g, t);
             mma16816(c, a, b);
         }
-        const float b0 = __ldg(&bias[n0 + 2 * t]), b1 = __ldg(&bias[n0 + 2 * t + 1]);
+        const float b0 = bias[n0 + 2 * t], b1 = bias[n0 + 2 * t + 1];
         float v[4] = {c[0] + b0, c[1] + b1, c[2] + b0, c[3] + b1};
         if (RELU)
 #pragma unroll
@@ -113,15 +107,49 @@ __device__ __forceinline__ void denseForward(const uint16_t *in, int ldIn, const
     }
 }
 
+// The training block's copy of the BF16 weights in shared memory, rows padded
+// (168 and 72 elements) so that the mma fragment loads are free of bank conflicts.
+constexpr int kLdW0 = GUIDE_INPUTS + 8, kLdWH = GUIDE_HIDDEN + 8;
+struct TrainWeights {
+    uint16_t w0[GUIDE_HIDDEN * kLdW0];
+    uint16_t w1[GUIDE_HIDDEN * kLdWH];
+    uint16_t w2[GUIDE_HIDDEN * kLdWH];
+    uint16_t w3[GUIDE_OUTPUTS * kLdWH];
+    float b[3 * GUIDE_HIDDEN + GUIDE_OUTPUTS];
+    __device__ const uint16_t *w(int l) const { return l == 0 ? w0 : l == 1 ? w1 : l == 2 ? w2 : w3; }
+    __device__ static int ld(int l) { return l == 0 ? kLdW0 : kLdWH; }
+};
+
+__device__ void loadTrainWeights(TrainWeights &tw, const GuideNetView &net) {
+    const int rows[4] = {GUIDE_HIDDEN, GUIDE_HIDDEN, GUIDE_HIDDEN, GUIDE_OUTPUTS};
+    const int cols[4] = {GUIDE_INPUTS, GUIDE_HIDDEN, GUIDE_HIDDEN, GUIDE_HIDDEN};
+    for (int l = 0; l < 4; l++) {
+        uint32_t *dst = reinterpret_cast<uint32_t *>(const_cast<uint16_t *>(tw.w(l)));
+        const uint32_t *src = reinterpret_cast<const uint32_t *>(net.w[l]);
+        const int half = cols[l] / 2, ldHalf = TrainWeights::ld(l) / 2;
+        for (int i = threadIdx.x; i < rows[l] * half; i += blockDim.x) {
+            const int r = i / half, c = i - r * half;
+            dst[r * ldHalf + c] = __ldg(&src[r * half + c]);
+        }
+    }
+    for (int i = threadIdx.x; i < 3 * GUIDE_HIDDEN + GUIDE_OUTPUTS; i += blockDim.x) {
+        const int l = min(i / GUIDE_HIDDEN, 3);
+        tw.b[i] = __ldg(&net.b[l][i - l * GUIDE_HIDDEN]);
+    }
+}
+
 // the whole forward pass for the 16 samples whose inputs are in s.x
-__device__ void forward(WarpScratch &s, const GuideNetView &net, int g, int t) {
-    denseForward<GUIDE_INPUTS, GUIDE_HIDDEN, true>(s.x, kLd0, net.w[0], net.b[0], s.h[0], nullptr, kLdH, g, t);
+__device__ void forward(WarpScratch &s, const TrainWeights &tw, int g, int t) {
+    denseForward<GUIDE_INPUTS, GUIDE_HIDDEN, true>(s.x, kLd0, tw.w0, kLdW0, tw.b, s.h[0], nullptr, kLdH, g, t);
     __syncwarp();
-    denseForward<GUIDE_HIDDEN, GUIDE_HIDDEN, true>(s.h[0], kLdH, net.w[1], net.b[1], s.h[1], nullptr, kLdH, g, t);
+    denseForward<GUIDE_HIDDEN, GUIDE_HIDDEN, true>(s.h[0], kLdH, tw.w1, kLdWH, tw.b + GUIDE_HIDDEN, s.h[1], nullptr,
+                                                   kLdH, g, t);
     __syncwarp();
-    denseForward<GUIDE_HIDDEN, GUIDE_HIDDEN, true>(s.h[1], kLdH, net.w[2], net.b[2], s.h[2], nullptr, kLdH, g, t);
+    denseForward<GUIDE_HIDDEN, GUIDE_HIDDEN, true>(s.h[1], kLdH, tw.w2, kLdWH, tw.b + 2 * GUIDE_HIDDEN, s.h[2],
+                                                   nullptr, kLdH, g, t);
     __syncwarp();
-    denseForward<GUIDE_HIDDEN, GUIDE_OUTPUTS, false>(s.h[2], kLdH, net.w[3], net.b[3], nullptr, s.o, kLdO, g, t);
+    denseForward<GUIDE_HIDDEN, GUIDE_OUTPUTS, false>(s.h[2], kLdH, tw.w3, kLdWH, tw.b + 3 * GUIDE_HIDDEN, nullptr,
+                                                     s.o, kLdO, g, t);
     __syncwarp();
 }
 
@@ -643,7 +671,9 @@ __global__ void __launch_bounds__(32 * kWarps) k_guide_train(RecordBatch batch, 
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31, g = lane >> 2, t = lane & 3;
     WarpScratch &s = reinterpret_cast<WarpScratch *>(smem)[warp];
     float *acc = reinterpret_cast<float *>(smem + kWarps * sizeof(WarpScratch));  // block gradient, GUIDE_PARAMS
+    TrainWeights &tw = *reinterpret_cast<TrainWeights *>(acc + GUIDE_PARAMS);
     for (int i = threadIdx.x; i < GUIDE_PARAMS; i += blockDim.x) acc[i] = 0.0f;
+    loadTrainWeights(tw, net);
     __syncthreads();
     const uint32_t n = batch.n;
     const float scale = 1.0f / (float)n;
@@ -657,7 +687,7 @@ __global__ void __launch_bounds__(32 * kWarps) k_guide_train(RecordBatch batch, 
         GuideFeatures f;
         for (int k = 0; k < 7; k++) f.v[k] = rc.features[k];
         encodeInputs(s, f, lane);
-        forward(s, net, g, t);
+        forward(s, tw, g, t);
         // output deltas: lanes 0..15, one sample each (zero for padding rows)
         if (lane < 16) {
             float grad[GUIDE_OUTPUTS];
@@ -690,7 +720,7 @@ __global__ void __launch_bounds__(32 * kWarps) k_guide_train(RecordBatch batch, 
                 loadAT(a, delta, kLdH, m0, g, t);
                 for (int n0 = 0; n0 < nIn; n0 += 8) {
                     uint32_t b[2];
-                    loadBkn<false>(b, in, ldIn, n0, 0, g, t);
+                    loadBkn(b, in, ldIn, n0, 0, g, t);
                     float c[4] = {0.0f, 0.0f, 0.0f, 0.0f};
                     mma16816(c, a, b);
                     atomicAdd(&gW[(m0 + g) * nIn + n0 + 2 * t], c[0]);
@@ -713,7 +743,7 @@ __global__ void __launch_bounds__(32 * kWarps) k_guide_train(RecordBatch batch, 
                 for (int k0 = 0; k0 < nOut; k0 += 16) {
                     uint32_t a[4], b[2];
                     loadA(a, delta, kLdH, k0, g, t);
-                    loadBkn<true>(b, net.w[l], nIn, n0, k0, g, t);
+                    loadBkn(b, tw.w(l), TrainWeights::ld(l), n0, k0, g, t);
                     mma16816(c, a, b);
                 }
                 const int col = n0 + 2 * t;
@@ -734,17 +764,28 @@ __global__ void __launch_bounds__(32 * kWarps) k_guide_train(RecordBatch batch, 
     for (int off = 16; off > 0; off >>= 1) lossSum += __shfl_xor_sync(0xffffffffu, lossSum, off);
     if (lane == 0 && lossOut) atomicAdd(lossOut, lossSum * scale);
     __syncthreads();
-    for (int i = threadIdx.x; i < GUIDE_PARAMS; i += blockDim.x)
-        if (acc[i] != 0.0f) atomicAdd(&net.grad[i], acc[i]);
+    // the block's gradient, summed over the blocks by the Adam step (no atomics)
+    float *part = net.partials + (size_t)blockIdx.x * GUIDE_PARAMS;
+    for (int i = threadIdx.x; i < GUIDE_PARAMS; i += blockDim.x) part[i] = acc[i];
+}
+
+// net.grad += the sum of the training blocks' gradients
+__global__ void k_guide_reduce(GuideNetView net, int blocks) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= GUIDE_PARAMS) return;
+    float g = 0.0f;
+    for (int b = 0; b < blocks; b++) g += net.partials[(size_t)b * GUIDE_PARAMS + i];
+    net.grad[i] += g;
 }
 
 // Adam step on every parameter; refreshes the bf16 weight copies and clears
 // the gradient.
-__global__ void k_guide_adam(GuideNetView net, float lr, float beta1, float beta2, float eps, float corr1,
+__global__ void k_guide_adam(GuideNetView net, int blocks, float lr, float beta1, float beta2, float eps, float corr1,
                              float corr2) {
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= GUIDE_PARAMS) return;
-    const float gr = net.grad[i];
+    float gr = net.grad[i];
+    for (int b = 0; b < blocks; b++) gr += net.partials[(size_t)b * GUIDE_PARAMS + i];
     const float m = beta1 * net.adamM[i] + (1.0f - beta1) * gr;
     const float v = beta2 * net.adamV[i] + (1.0f - beta2) * gr * gr;
     net.adamM[i] = m;
@@ -823,7 +864,8 @@ __global__ void k_guide_mixture_test(const float *outputs, const float *u, int n
 using namespace rmd;
 
 size_t rmdGuideSharedBytes(bool training) {
-    return training ? kWarps * sizeof(WarpScratch) + GUIDE_PARAMS * sizeof(float) : sizeof(TcSmem);
+    return training ? kWarps * sizeof(WarpScratch) + GUIDE_PARAMS * sizeof(float) + sizeof(TrainWeights)
+                    : sizeof(TcSmem);
 }
 
 cudaError_t rmdGuideConfigure() {
@@ -856,11 +898,12 @@ cudaError_t rmdLaunchGuideTrain(const GuideRecord *rec, uint32_t total, uint32_t
     RecordBatch batch{rec, total, std::min(n, total), seed};
     k_guide_mean_y<<<256, 256, 0, s>>>(batch, scratch);
     if ((e = cudaGetLastError()) != cudaSuccess) return e;
+    blocks = std::max(1, std::min(blocks, GUIDE_TRAIN_MAX_BLOCKS));
     k_guide_train<<<blocks, 32 * kWarps, rmdGuideSharedBytes(true), s>>>(batch, scratch, net, scratch + 1);
     if ((e = cudaGetLastError()) != cudaSuccess) return e;
     const float beta1 = 0.9f, beta2 = 0.999f;
     const float corr1 = 1.0f / (1.0f - powf(beta1, (float)step)), corr2 = 1.0f / (1.0f - powf(beta2, (float)step));
-    k_guide_adam<<<(GUIDE_PARAMS + 255) / 256, 256, 0, s>>>(net, lr, beta1, beta2, 1e-8f, corr1, corr2);
+    k_guide_adam<<<(GUIDE_PARAMS + 255) / 256, 256, 0, s>>>(net, blocks, lr, beta1, beta2, 1e-8f, corr1, corr2);
     return cudaGetLastError();
 }
 
@@ -880,6 +923,8 @@ cudaError_t rmdLaunchGuideGradientTest(const GuideRecord *rec, uint32_t n, const
     k_guide_mean_y<<<256, 256, 0, s>>>(batch, scratch);
     if ((e = cudaGetLastError()) != cudaSuccess) return e;
     k_guide_train<<<64, 32 * kWarps, rmdGuideSharedBytes(true), s>>>(batch, scratch, net, scratch + 1);
+    if ((e = cudaGetLastError()) != cudaSuccess) return e;
+    k_guide_reduce<<<(GUIDE_PARAMS + 255) / 256, 256, 0, s>>>(net, 64);
     return cudaGetLastError();
 }
 
@@ -902,9 +947,9 @@ void GuideNet::layout(int wOffset[4], int bOffset[4], int bf16Offset[4]) {
 
 void GuideNet::release() {
     for (void *ptr : {(void *)master, (void *)adamM, (void *)adamV, (void *)grad, (void *)scratch,
-                      (void *)weightsBf16, (void *)bf16Index})
+                      (void *)partials, (void *)weightsBf16, (void *)bf16Index})
         if (ptr) cudaFree(ptr);
-    master = adamM = adamV = grad = scratch = nullptr;
+    master = adamM = adamV = grad = scratch = partials = nullptr;
     weightsBf16 = nullptr;
     bf16Index = nullptr;
 }
@@ -916,6 +961,7 @@ cudaError_t GuideNet::allocate() {
     if ((e = cudaMalloc(&master, pb)) != cudaSuccess || (e = cudaMalloc(&adamM, pb)) != cudaSuccess ||
         (e = cudaMalloc(&adamV, pb)) != cudaSuccess || (e = cudaMalloc(&grad, pb)) != cudaSuccess ||
         (e = cudaMalloc(&scratch, 64 * sizeof(float))) != cudaSuccess ||
+        (e = cudaMalloc(&partials, (size_t)GUIDE_TRAIN_MAX_BLOCKS * pb)) != cudaSuccess ||
         (e = cudaMalloc(&weightsBf16, GUIDE_WEIGHTS * sizeof(uint16_t))) != cudaSuccess ||
         (e = cudaMalloc(&bf16Index, GUIDE_PARAMS * sizeof(int))) != cudaSuccess)
         return e;
@@ -956,6 +1002,7 @@ GuideNetView GuideNet::view(float3 sceneMin, float3 sceneInvExtent) const {
     v.adamM = adamM;
     v.adamV = adamV;
     v.grad = grad;
+    v.partials = partials;
     v.weightsBf16 = weightsBf16;
     v.bf16Index = bf16Index;
     v.sceneMin = sceneMin;

@@ -12,6 +12,7 @@ namespace rmd {
 // 160 -> 64 -> 64 -> 64 -> 48: weights and biases of the four layers
 constexpr int GUIDE_PARAMS = GUIDE_HIDDEN * GUIDE_INPUTS + GUIDE_HIDDEN + 2 * (GUIDE_HIDDEN * GUIDE_HIDDEN + GUIDE_HIDDEN) +
                              GUIDE_OUTPUTS * GUIDE_HIDDEN + GUIDE_OUTPUTS;
+constexpr int GUIDE_TRAIN_MAX_BLOCKS = 256;  // blocks of one training launch (each writes its gradient)
 constexpr int GUIDE_WEIGHTS = GUIDE_HIDDEN * GUIDE_INPUTS + 2 * GUIDE_HIDDEN * GUIDE_HIDDEN + GUIDE_OUTPUTS * GUIDE_HIDDEN;
 
 // Device view of the network: FP32 master parameters (row-major [out][in]
@@ -21,6 +22,7 @@ struct GuideNetView {
     const uint16_t *w[4];  // bf16 weights per layer, row-major [out][in]
     const float *b[4];     // fp32 biases (inside `master`)
     float *master, *adamM, *adamV, *grad;  // GUIDE_PARAMS each
+    float *partials;                        // per training block: its gradient (GUIDE_TRAIN_MAX_BLOCKS x GUIDE_PARAMS)
     uint16_t *weightsBf16;                  // GUIDE_WEIGHTS
     const int *bf16Index;                   // per parameter: index into weightsBf16, or -1 (bias)
     int wOffset[4], bOffset[4];             // parameter offsets of each layer's weights / biases
@@ -54,6 +56,7 @@ namespace rmdhost {
 // moments, gradient, BF16 weight copy).
 struct GuideNet {
     float *master = nullptr, *adamM = nullptr, *adamV = nullptr, *grad = nullptr, *scratch = nullptr;
+    float *partials = nullptr;
     uint16_t *weightsBf16 = nullptr;
     int *bf16Index = nullptr;
     int steps = 0;

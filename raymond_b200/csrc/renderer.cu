@@ -844,9 +844,9 @@ static rmd_status setGuide(GuideState &g, const rmd_guide_settings *settings, cu
     rmd_guide_settings next = *settings;
     if (next.batch_size == 0) next.batch_size = 1u << 20;
     if (next.learning_rate == 0.0f) next.learning_rate = 1e-3f;
-    if (next.step_records == 0) next.step_records = 1u << 14;
+    if (next.step_records == 0) next.step_records = 1u << 13;
     if (next.replay_records == 0) next.replay_records = 1u << 18;
-    if (next.steps_per_batch == 0) next.steps_per_batch = 1;
+    if (next.steps_per_batch == 0) next.steps_per_batch = 8;
     if (next.guided_depth == 0) next.guided_depth = 65535;
     if (!g.net.allocated()) RMD_CUDA(g.net.allocate());
     if (!g.initialised || next.reset) {
