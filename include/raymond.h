@@ -209,6 +209,23 @@ typedef struct rmd_camera {                 /* bridge/Camera.hpp:5-11 */
 
 /* ----------------------------------------------------------------- scene */
 
+#define RMD_TEXTURE_U8 0u  /* unsigned bytes, value / 255 */
+#define RMD_TEXTURE_U16 1u /* unsigned shorts, value / 65535 */
+#define RMD_TEXTURE_F32 2u /* floats */
+
+/* The image of an image or environment texture node, found by the node's
+ * `filepath` parameter (MaterialBuilder.registerTexture,
+ * MaterialBuilder.swift:719-735, where MTKTextureLoader reads the file).
+ * Rows from the top of the image, channels interleaved: 1 (a single-channel
+ * texture, sampled as (r, 0, 0, 1)), 3 (RGB, alpha 1) or 4 (RGBA).  A node
+ * whose file is not among the textures reads a 1 x 1 zero texture, as the
+ * reference does when a file fails to load (:224-234). */
+typedef struct rmd_texture {
+    const char *name;
+    uint32_t width, height, channels, format;
+    const void *data;
+} rmd_texture;
+
 typedef struct rmd_scene_desc {
     int32_t num_surface_materials;          /* shadeSurface table */
     const rmd_material *surface_materials;
@@ -233,6 +250,9 @@ typedef struct rmd_scene_desc {
     const rmd_spot_light *spot_lights;
 
     rmd_camera camera;
+
+    int32_t num_textures;
+    const rmd_texture *textures;
 } rmd_scene_desc;
 
 /* -------------------------------------------------------------- renderer */

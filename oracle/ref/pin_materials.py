@@ -69,6 +69,8 @@ _DEFAULTS = {
                 "Color": ("RGBA", [0.8, 0.8, 0.8, 1])},
     "BRIGHTCONTRAST": {"Color": ("RGBA", [1, 1, 1, 1]), "Bright": ("VALUE", 0.0), "Contrast": ("VALUE", 0.0)},
     "BLACKBODY": {"Temperature": ("VALUE", 1500.0)},
+    "TEX_IMAGE": {"Vector": ("VECTOR", [0, 0, 0])},
+    "TEX_ENVIRONMENT": {"Vector": ("VECTOR", [0, 0, 0])},
 }
 
 
@@ -199,7 +201,48 @@ def materials() -> list[tuple[str, dict]]:
                             "parameters": {"distribution": "GGX", "subsurface_method": "RANDOM_WALK"}},
         "Material Output": _out(("Principled BSDF", "BSDF")),
     }))
+    # image textures: flat projection of a mapped UV in sRGB, a single-channel
+    # linear image, an equirectangular environment in XYZ, and a missing file
+    mats.append(("image_textures", {
+        "Texture Coordinate": _bsdf("TEX_COORD"),
+        "Mapping": _bsdf("MAPPING", {"type": "MAPPING"}, Vector=_v("VECTOR", link=("Texture Coordinate", "Generated")),
+                         Location=_v("VECTOR", [0.3, -0.1, 0.0]), Rotation=_v("VECTOR", [0.0, 0.0, 0.4]),
+                         Scale=_v("VECTOR", [2.5, 1.7, 1.0])),
+        "Albedo": _bsdf("TEX_IMAGE", _image_params("textures/albedo.png", "sRGB"),
+                        Vector=_v("VECTOR", link=("Mapping", "Vector"))),
+        "Rough": _bsdf("TEX_IMAGE", _image_params("textures/rough.png", "Non-Color")),
+        "Sky": _bsdf("TEX_ENVIRONMENT", _image_params("textures/sky.exr", "XYZ", "EQUIRECTANGULAR"),
+                     Vector=_v("VECTOR", link=("Texture Coordinate", "Normal"))),
+        "Missing": _bsdf("TEX_IMAGE", _image_params("textures/not_exported.jpg", "sRGB")),
+        "Mix": _bsdf("MIX_RGB", {"blend_type": "ADD", "use_clamp": False}, Fac=_v("VALUE", link=("Albedo", "Alpha")),
+                     Color1=_v("RGBA", link=("Albedo", "Color")), Color2=_v("RGBA", link=("Missing", "Color"))),
+        "Principled BSDF": {"type": "BSDF_PRINCIPLED",
+                            "inputs": dict(M.principled_inputs(emission_strength=0.05),
+                                           **{"Base Color": _v("RGBA", link=("Mix", "Color")),
+                                              "Roughness": _v("VALUE", link=("Rough", "Color")),
+                                              "Emission": _v("RGBA", link=("Sky", "Color"))}),
+                            "parameters": {"distribution": "GGX", "subsurface_method": "RANDOM_WALK"}},
+        "Material Output": _out(("Principled BSDF", "BSDF")),
+    }))
     return mats
+
+
+def _image_params(path, colorspace, projection="FLAT"):
+    return {"filepath": path, "interpolation": "Linear", "projection": projection, "extension": "REPEAT",
+            "source": "FILE", "colorspace": colorspace, "alpha": "STRAIGHT"}
+
+
+def textures() -> dict:
+    """The pinning textures, by file name: an sRGB RGBA byte image, a
+    single-channel 16-bit image and a float RGB environment."""
+    import numpy as np
+
+    rng = np.random.default_rng(31)
+    return {
+        "textures/albedo.png": rng.integers(0, 256, (13, 17, 4), dtype=np.uint8),
+        "textures/rough.png": rng.integers(0, 65536, (9, 6), dtype=np.uint16),
+        "textures/sky.exr": rng.exponential(1.0, (8, 16, 3)).astype(np.float32),
+    }
 
 
 def scene() -> dict:
@@ -210,6 +253,7 @@ def scene() -> dict:
 
     sc = scenes.cornell(seed=1, envmap_exponent=2)
     sc["materials"] = materials()
+    sc["textures"] = textures()
     for sh in sc["shapes"]:
         sh["materials"] = np.zeros_like(sh["materials"])
     return sc

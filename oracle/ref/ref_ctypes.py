@@ -25,6 +25,8 @@ def lib():
         L.ref_num_materials.restype = C.c_int
         L.ref_material_eval.argtypes = [C.c_int, _fp, C.c_int, _fp]
         L.ref_material_eval.restype = C.c_int
+        L.ref_set_texture.argtypes = [C.c_int, _fp, C.c_int, C.c_int]
+        L.ref_set_texture.restype = C.c_int
         L.ref_scene_create.argtypes = [C.c_void_p, C.c_char_p, C.POINTER(C.c_uint8)]
         L.ref_scene_create.restype = C.c_void_p
         L.ref_scene_destroy.argtypes = [C.c_void_p]
@@ -32,6 +34,31 @@ def lib():
         L.ref_render.restype = C.c_int
         _lib = L
     return _lib
+
+
+def texels(img: np.ndarray) -> np.ndarray:
+    """An image (h, w[, 1|3|4]) of uint8, uint16 or float32 as the RGBA floats a
+    texture holds: integers normalised, one channel as (r, 0, 0, 1), RGB with alpha 1."""
+    a = np.asarray(img)
+    if a.ndim == 2:
+        a = a[:, :, None]
+    if a.dtype == np.uint8:
+        f = a.astype(np.float32) / np.float32(255)
+    elif a.dtype == np.uint16:
+        f = a.astype(np.float32) / np.float32(65535)
+    else:
+        f = a.astype(np.float32)
+    out = np.zeros(a.shape[:2] + (4,), np.float32)
+    out[..., 3] = 1
+    out[..., :a.shape[2]] = f
+    return out
+
+
+def set_textures(textures: dict) -> None:
+    """Install the pinning scene's textures (in order) as the reference build's Context.textures."""
+    for slot, img in enumerate(textures.values()):
+        t = np.ascontiguousarray(texels(img))
+        assert lib().ref_set_texture(slot, t.ctypes.data_as(_fp), t.shape[1], t.shape[0]) == 0
 
 
 def prng_tea(a: int, b: int, n: int) -> np.ndarray:

@@ -11,6 +11,8 @@
 // lens library): the host scheduling of Renderer.execute, the scene set-up of
 // ShapeBuilder / EntityBuilder / LightBuilder, the pinhole camera of
 // generateRays, and the intersector itself (the oracle's BVH, ref_bvh.cpp).
+#include <vector>
+
 #include <metal_stdlib>
 using namespace metal;
 
@@ -166,11 +168,26 @@ int ref_num_materials() { return findTable("pin")->numSurface; }
 // (float3 each), rayFlags, tangent tu (bitangent normal x tu).  Output (16 floats): emission, evaluate
 // value, evaluate pdf, sampled wi, sampled weight, sampled pdf, sampled flags,
 // alpha.
+// The pinning materials' textures: slot `slot` becomes a w x h RGBA float
+// image (copied), as the reference's Context.textures holds them.
+static std::vector<float4> g_textureData[NUMBER_OF_TEXTURES];
+static Context g_materialCtx;
+int ref_set_texture(int slot, const float *rgba, int w, int h) {
+    if (slot < 0 || slot >= NUMBER_OF_TEXTURES || w <= 0 || h <= 0) return 1;
+    g_textureData[slot].resize((size_t)w * h);
+    for (size_t i = 0; i < g_textureData[slot].size(); i++)
+        g_textureData[slot][i] = float4(rgba[4 * i], rgba[4 * i + 1], rgba[4 * i + 2], rgba[4 * i + 3]);
+    g_materialCtx.textures[slot].data = g_textureData[slot].data();
+    g_materialCtx.textures[slot].width = (uint)w;
+    g_materialCtx.textures[slot].height = (uint)h;
+    return 0;
+}
+
 int ref_material_eval(int material, const float *records, int n, float *out) {
     const RefMaterialTable *table = findTable("pin");
     if (material < 0 || material >= table->numSurface) return 1;
     g_table = table;
-    static Context ctx;  // the pinned nodes read nothing from it
+    Context &ctx = g_materialCtx;  // the pinned nodes read only its textures
     for (int i = 0; i < n; i++) {
         const float *r = records + 28 * (size_t)i;
         auto v3 = [&](int k) { return float3(r[3 * k], r[3 * k + 1], r[3 * k + 2]); };

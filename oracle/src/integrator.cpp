@@ -319,12 +319,37 @@ extern "C" int oracle_scene_create(const rmd_scene_desc *d, oracle_scene **out, 
     if (!d || !out) return RMD_ERROR_INVALID_ARGUMENT;
     auto s = std::make_unique<oracle_scene>();
     SceneData &ctx = s->data;
+    // the textures (RGBA floats, integers normalised), then the 1 x 1 zero texture
+    std::vector<std::string> texNames;
+    std::vector<int> texChannels;
+    for (int i = 0; i < d->num_textures; i++) {
+        const rmd_texture &t = d->textures[i];
+        Texture tex;
+        tex.width = (int)t.width;
+        tex.height = (int)t.height;
+        tex.channels = (int)t.channels;
+        tex.texels.assign((size_t)t.width * t.height, float4(0, 0, 0, 1));
+        for (size_t p = 0; p < tex.texels.size(); p++)
+            for (uint32_t c = 0; c < t.channels; c++) {
+                const size_t k = p * t.channels + c;
+                float v;
+                if (t.format == RMD_TEXTURE_U8) v = (float)static_cast<const uint8_t *>(t.data)[k] / 255.0f;
+                else if (t.format == RMD_TEXTURE_U16) v = (float)static_cast<const uint16_t *>(t.data)[k] / 65535.0f;
+                else v = static_cast<const float *>(t.data)[k];
+                tex.texels[p][c] = v;
+            }
+        ctx.textures.push_back(std::move(tex));
+        texNames.push_back(t.name ? t.name : "");
+        texChannels.push_back((int)t.channels);
+    }
+    ctx.textures.push_back(Texture());
     try {
         // MaterialBuilder: shadeSurface / shadeLight tables
         for (int i = 0; i < d->num_surface_materials; i++)
-            ctx.surfaceShaders.push_back(std::make_unique<MaterialProgram>(d->surface_materials[i]));
+            ctx.surfaceShaders.push_back(
+                std::make_unique<MaterialProgram>(d->surface_materials[i], texNames, texChannels));
         for (int i = 0; i < d->num_light_materials; i++)
-            ctx.lightShaders.push_back(std::make_unique<MaterialProgram>(d->light_materials[i]));
+            ctx.lightShaders.push_back(std::make_unique<MaterialProgram>(d->light_materials[i], texNames, texChannels));
     } catch (const CodegenError &e) {
         fail(err, errlen, e.message);
         return e.status;

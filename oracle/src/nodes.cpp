@@ -415,6 +415,55 @@ struct ColorInvert {  // nodes.hpp:1387-1394
     }
     static void describe(FieldList &fl) { using T = ColorInvert; FLD(T, color, K_F4); FLD(T, fac, K_F1); }
 };
+// Metal's linear sampler with address::repeat over normalized coordinates
+// (nodes.hpp:517): texel centres at (i + 1/2) / size, bilinear, wrapped.
+static int wrapTexel(float i, int n) {
+    const float m = i - std::floor(i / (float)n) * (float)n;
+    const int k = (int)m;
+    return k < 0 ? 0 : (k >= n ? n - 1 : k);
+}
+static float4 sampleLinearRepeat(const Texture &t, float2 uv) {
+    const float x = uv.x * (float)t.width - 0.5f, y = uv.y * (float)t.height - 0.5f;
+    const float x0f = std::floor(x), y0f = std::floor(y);
+    const float ax = x - x0f, ay = y - y0f;
+    const int x0 = wrapTexel(x0f, t.width), y0 = wrapTexel(y0f, t.height);
+    const int x1 = x0 + 1 == t.width ? 0 : x0 + 1, y1 = y0 + 1 == t.height ? 0 : y0 + 1;
+    const float4 *r0 = t.texels.data() + (size_t)y0 * t.width, *r1 = t.texels.data() + (size_t)y1 * t.width;
+    return lerp(lerp(r0[x0], r0[x1], ax), lerp(r1[x0], r1[x1], ax), ay);
+}
+struct TexImage {  // nodes.hpp:486-564 (image and environment textures)
+    float3 vector;
+    float4 color;
+    float alpha;
+    int slot = 0, projection = 0, colorSpace = 1;  // projection: FLAT, BOX, EQUIRECTANGULAR, MIRROR_BALL
+    bool singleChannel = true;
+    static float srgbToLinear(float c) {
+        if (c < 0.04045f) return c < 0 ? 0.0f : c * (1.0f / 12.92f);
+        return std::pow((c + 0.055f) * (1.0f / 1.055f), 2.4f);
+    }
+    void compute(const SceneData &d, ShadingContext &) {
+        float2 p(0, 0);
+        if (projection == 0) p = float2(vector.x, 1 - vector.y);
+        else if (projection == 2)  // warp.hpp:5-10
+            p = float2((std::atan2(vector.x, vector.y) + (float)M_PI / 2) / (2 * (float)M_PI),
+                       std::acos(vector.z / length(vector)) / (float)M_PI);
+        color = sampleLinearRepeat(d.textures[slot], p);
+        alpha = color.w;
+        if (singleChannel) color = float4(color.x, color.x, color.x, 1);
+        if (colorSpace == 1) {
+            color = float4(srgbToLinear(color.x), srgbToLinear(color.y), srgbToLinear(color.z), color.w);
+        } else if (colorSpace == 4) {  // color.hpp:74-78
+            const float3 c = color.xyz();
+            color = float4(3.240479f * c.x + -1.537150f * c.y + -0.498535f * c.z,
+                           -0.969256f * c.x + 1.875991f * c.y + 0.041556f * c.z,
+                           0.055648f * c.x + -0.204043f * c.y + 1.057311f * c.z, color.w);
+        }
+    }
+    static void describe(FieldList &fl) {
+        using T = TexImage;
+        FLD(T, vector, K_F3); FLD(T, color, K_F4); FLD(T, alpha, K_F1);
+    }
+};
 struct Mapping {  // nodes.hpp:346-364 with euler2mat of math.hpp:46-68 (one Type: MAPPING)
     float3 scale, rotation, location, vector;
     void compute(const SceneData &, ShadingContext &) {
@@ -866,7 +915,8 @@ static int enumIndex(const std::string &v, std::initializer_list<const char *> n
 }
 
 // MaterialBuilder.swift:327-661 (the kernels this oracle implements)
-static std::unique_ptr<NodeImpl> makeKernel(const rmd_node &n) {
+static std::unique_ptr<NodeImpl> makeKernel(const rmd_node &n, const std::vector<std::string> &texNames,
+                                            const std::vector<int> &texChannels) {
     std::string t = n.type ? n.type : "";
     auto unsupported = [&]() -> std::unique_ptr<NodeImpl> {
         throw CodegenError{RMD_ERROR_CODEGEN_UNSUPPORTED, "unsupported node type '" + t + "'"};
@@ -967,6 +1017,25 @@ static std::unique_ptr<NodeImpl> makeKernel(const rmd_node &n) {
         if (b->v.space < 0) return unsupported();
         return b;
     }
+    if (t == "TEX_IMAGE" || t == "TEX_ENVIRONMENT") {  // MaterialBuilder.swift:387-433
+        auto b = std::make_unique<Box<TexImage>>();
+        const std::string file = paramString(n, "filepath", "");
+        int slot = (int)texNames.size();
+        for (size_t i = 0; i < texNames.size(); i++)
+            if (texNames[i] == file) {
+                slot = (int)i;
+                break;
+            }
+        b->v.slot = slot;
+        b->v.singleChannel = slot >= (int)texChannels.size() || texChannels[slot] == 1;
+        if (enumIndex(paramString(n, "interpolation", "Linear"), {"LINEAR"}) < 0) return unsupported();
+        b->v.projection = enumIndex(paramString(n, "projection", t == "TEX_IMAGE" ? "FLAT" : "EQUIRECTANGULAR"),
+                                    {"FLAT", "BOX", "EQUIRECTANGULAR", "MIRROR_BALL"});
+        b->v.colorSpace = enumIndex(paramString(n, "colorspace", "sRGB"),
+                                    {"LINEAR", "SRGB", "NON_COLOR", "RAW", "XYZ", "FILMIC_LOG"});
+        if (b->v.projection < 0 || b->v.colorSpace < 0) return unsupported();
+        return b;
+    }
     if (t == "HUE_SAT") return std::make_unique<Box<HueSaturation>>();
     if (t == "BRIGHTCONTRAST") return std::make_unique<Box<BrightnessContrast>>();
     if (t == "BLACKBODY") return std::make_unique<Box<Blackbody>>();
@@ -1059,7 +1128,8 @@ static void coerce(const std::string &type, Kind k, const void *src, Kind dstKin
     }
 }
 
-MaterialProgram::MaterialProgram(const rmd_material &m) {
+MaterialProgram::MaterialProgram(const rmd_material &m, const std::vector<std::string> &textureNames,
+                                 const std::vector<int> &textureChannels) {
     static std::atomic<uint64_t> nextSerial{1};
     serial_ = nextSerial.fetch_add(1);
     name_ = m.name ? m.name : "";
@@ -1080,7 +1150,7 @@ MaterialProgram::MaterialProgram(const rmd_material &m) {
         state[key] = 1;
         const rmd_node &node = *it->second;
         Step step;
-        step.proto = makeKernel(node);
+        step.proto = makeKernel(node, textureNames, textureChannels);
         void *base = step.proto->base();
 
         // provideDefaults, MaterialBuilder.swift:762-791

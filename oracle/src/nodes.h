@@ -52,7 +52,10 @@ struct CodegenError {
 class MaterialProgram {
 public:
     // throws CodegenError
-    MaterialProgram(const rmd_material &m);
+    // textures: the scene's texture names and channel counts (an image node's
+    // file selects the slot; an unknown file the slot after the last)
+    MaterialProgram(const rmd_material &m, const std::vector<std::string> &textureNames = {},
+                    const std::vector<int> &textureChannels = {});
     // Runs the node chain (s_<material> of MaterialBuilder.swift:696-707).
     void run(const SceneData &ctx, ShadingContext &shading) const;
     bool hasSurfaceEmission() const { return hasEmission_; }

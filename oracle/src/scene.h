@@ -108,6 +108,13 @@ struct Intersection {  // bridge/Ray.hpp:41-46
 class MaterialProgram;  // nodes.h
 class Bvh;              // bvh.h
 
+// A texture as the oracle samples it: RGBA floats from the top row (a
+// single-channel image as (r, 0, 0, 1), RGB with alpha 1).
+struct Texture {
+    int width = 1, height = 1, channels = 1;
+    std::vector<float4> texels{float4(0, 0, 0, 1)};
+};
+
 struct SceneData {
     // Context.hpp:15-26
     std::vector<float3> vertices;
@@ -135,6 +142,8 @@ struct SceneData {
     std::vector<std::unique_ptr<MaterialProgram>> surfaceShaders;
     std::vector<std::unique_ptr<MaterialProgram>> lightShaders;
     std::unique_ptr<Bvh> bvh;
+    // Context.hpp:25 (textures): the scene's, then a 1 x 1 zero texture for missing files
+    std::vector<Texture> textures;
 };
 
 // ShadingContext.metal:4-47

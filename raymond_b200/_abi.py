@@ -97,6 +97,14 @@ class BatchView(C.Structure):
 BATCH_NO_GRAPH = 1
 
 
+TEXTURE_U8, TEXTURE_U16, TEXTURE_F32 = 0, 1, 2
+
+
+class Texture(C.Structure):
+    _fields_ = [("name", C.c_char_p), ("width", C.c_uint32), ("height", C.c_uint32), ("channels", C.c_uint32),
+                ("format", C.c_uint32), ("data", C.c_void_p)]
+
+
 class SceneDescC(C.Structure):
     _fields_ = [("num_surface_materials", C.c_int32), ("surface_materials", C.POINTER(Material)),
                 ("num_light_materials", C.c_int32), ("light_materials", C.POINTER(Material)),
@@ -107,7 +115,7 @@ class SceneDescC(C.Structure):
                 ("num_point_lights", C.c_int32), ("point_lights", C.POINTER(PointLight)),
                 ("num_sun_lights", C.c_int32), ("sun_lights", C.POINTER(SunLight)),
                 ("num_spot_lights", C.c_int32), ("spot_lights", C.POINTER(SpotLight)),
-                ("camera", Camera)]
+                ("camera", Camera), ("num_textures", C.c_int32), ("textures", C.POINTER(Texture))]
 
 
 class RenderSettings(C.Structure):
@@ -168,6 +176,8 @@ class SceneDesc:
                        texcoords (V,2), indices (F,3) u32, materials (F,) u16
       entities:        list of dicts {shape, matrix (4,4) row-major world matrix, visibility}
       world_shader, envmap_exponent, area/point/sun/spot light lists, camera dict
+      textures:        optional {file path: (height, width[, 1|3|4]) uint8, uint16 or
+                       float32 image, top row first} for image / environment texture nodes
     """
 
     def __init__(self, scene: dict[str, Any]):
@@ -254,6 +264,19 @@ class SceneDesc:
         d.num_sun_lights, d.sun_lights = len(suns), self._array(SunLight, suns)
         d.num_spot_lights, d.spot_lights = len(spots), self._array(SpotLight, spots)
         d.camera = make_camera(scene["camera"])
+        texs = []
+        for name, img in scene.get("textures", {}).items():
+            a = np.ascontiguousarray(img)
+            if a.ndim == 2:
+                a = a[:, :, None]
+            if a.ndim != 3 or a.shape[2] not in (1, 3, 4):
+                raise ValueError(f"texture {name!r}: expected (height, width, 1|3|4), got {a.shape}")
+            fmt = {np.dtype(np.uint8): TEXTURE_U8, np.dtype(np.uint16): TEXTURE_U16}.get(a.dtype, TEXTURE_F32)
+            if fmt == TEXTURE_F32:
+                a = np.ascontiguousarray(a, np.float32)
+            self._keep.append(a)
+            texs.append(Texture(self._str(name), a.shape[1], a.shape[0], a.shape[2], fmt, a.ctypes.data))
+        d.num_textures, d.textures = len(texs), self._array(Texture, texs)
         self.c = d
 
     def _array(self, T, items):

@@ -98,6 +98,7 @@ const std::map<std::string, KernelDesc> &kernelTable() {
         add("RGBToBW", {{"color", F4}, {"val", F1}});
         add("ColorInvert", {{"color", F4}, {"fac", F1}});
         add("Gamma", {{"color", F4}, {"gamma", F1}});
+        add("TexImage", {{"vector", F3}, {"color", F4}, {"alpha", F1}});
         add("Mapping", {{"scale", F3}, {"rotation", F3}, {"location", F3}, {"vector", F3}});
         add("NormalMap", {{"color", F4}, {"strength", F1}, {"normal", F3}});
         add("HueSaturation", {{"color", F4}, {"fac", F1}, {"hue", F1}, {"saturation", F1}, {"value", F1}});
@@ -212,7 +213,7 @@ std::string assignment(const std::string &var, const std::string &field, Kind fi
 }
 
 // makeKernelInvocation (MaterialBuilder.swift:327-661) for the kernels of device/nodes.cuh
-Invocation makeInvocation(const rmd_node &n, Emitter &em) {
+Invocation makeInvocation(const rmd_node &n, Emitter &em, const TextureTable &textures) {
     const std::string t = n.type ? n.type : "";
     Invocation inv;
     auto plain = [&](const char *k) {
@@ -296,6 +297,18 @@ Invocation makeInvocation(const rmd_node &n, Emitter &em) {
         inv.kernel = "NormalMap";
         inv.type = "NormalMap<" + enumValue("NormalMap", "SPACE", paramString(n, "space", "TANGENT"), {"TANGENT", "WORLD"}) +
                    ">";
+    } else if (t == "TEX_IMAGE" || t == "TEX_ENVIRONMENT") {  // :387-433
+        const uint32_t slot = textures.slot(paramString(n, "filepath", ""));
+        inv.kernel = "TexImage";
+        inv.type = "TexImage<" + std::to_string(slot) + ", " +
+                   enumValue("TexImage", "INTERPOLATION", paramString(n, "interpolation", "Linear"), {"LINEAR"}) + ", " +
+                   enumValue("TexImage", "PROJECTION",
+                             paramString(n, "projection", t == "TEX_IMAGE" ? "FLAT" : "EQUIRECTANGULAR"),
+                             {"FLAT", "BOX", "EQUIRECTANGULAR", "MIRROR_BALL"}) +
+                   ", kTexImage::EXTENSION_REPEAT, kTexImage::ALPHA_STRAIGHT, " +
+                   enumValue("TexImage", "COLOR_SPACE", paramString(n, "colorspace", "sRGB"),
+                             {"LINEAR", "SRGB", "NON_COLOR", "RAW", "XYZ", "FILMIC_LOG"}) +
+                   ", kTexImage::PIXEL_FORMAT_" + (textures.channelsOf(slot) == 1 ? "R" : "RGBA") + ">";
     } else if (t == "HUE_SAT") plain("HueSaturation");
     else if (t == "BRIGHTCONTRAST") plain("BrightnessContrast");
     else if (t == "BLACKBODY") plain("Blackbody");
@@ -338,7 +351,7 @@ struct MaterialCode {
 };
 
 // Codegen.add(material:named:), MaterialBuilder.swift:676-711 + emitNode :793-825
-MaterialCode emitMaterial(const rmd_material &m, bool hoist) {
+MaterialCode emitMaterial(const rmd_material &m, bool hoist, const TextureTable &textures) {
     std::map<std::string, const rmd_node *> nodes;
     for (int i = 0; i < m.num_nodes; i++) nodes[m.nodes[i].name ? m.nodes[i].name : ""] = &m.nodes[i];
     std::map<std::string, int> state;  // 1 pending, 2 emitted
@@ -358,7 +371,7 @@ MaterialCode emitMaterial(const rmd_material &m, bool hoist) {
         if (it == nodes.end()) throw CodegenError{RMD_ERROR_INVALID_ARGUMENT, "link to unknown node '" + key + "'"};
         state[key] = 1;
         const rmd_node &node = *it->second;
-        Invocation inv = makeInvocation(node, em);
+        Invocation inv = makeInvocation(node, em, textures);
         const std::string var = "n" + std::to_string(counter++);
         const KernelDesc &desc = kernelTable().at(inv.kernel);
         const std::string t = node.type;
@@ -472,14 +485,15 @@ MaterialCode emitMaterial(const rmd_material &m, bool hoist) {
 }
 
 void emitTable(const rmd_material *mats, int n, bool hoist, const std::string &prefix, GeneratedModule &mod,
-               MaterialTable &table, std::string &functions, int &groups, std::vector<bool> *emissive) {
+               MaterialTable &table, std::string &functions, int &groups, std::vector<bool> *emissive,
+               const TextureTable &textures) {
     std::map<std::string, int> groupOf;
     std::vector<std::string> groupBodies;
     std::vector<std::vector<std::string>> groupNames;
     std::vector<std::vector<int>> groupMembers;
     std::vector<MaterialCode> codes;
     for (int i = 0; i < n; i++) {
-        codes.push_back(emitMaterial(mats[i], hoist));
+        codes.push_back(emitMaterial(mats[i], hoist, textures));
         const MaterialCode &mc = codes.back();
         if (emissive) emissive->push_back(mc.emissive);
         int g;
@@ -544,12 +558,28 @@ void emitTable(const rmd_material *mats, int n, bool hoist, const std::string &p
 
 }  // namespace
 
+TextureTable TextureTable::of(const rmd_texture *textures, int count) {
+    TextureTable t;
+    for (int i = 0; i < count; i++) {
+        t.names.push_back(textures[i].name ? textures[i].name : "");
+        t.channels.push_back(textures[i].channels);
+    }
+    return t;
+}
+
+uint32_t TextureTable::slot(const std::string &name) const {
+    for (size_t i = 0; i < names.size(); i++)
+        if (names[i] == name) return (uint32_t)i;
+    return (uint32_t)names.size();
+}
+
 GeneratedModule generateModule(const rmd_material *surface, int numSurface, const rmd_material *light, int numLight,
-                               bool hoist) {
+                               bool hoist, const TextureTable &textures) {
     GeneratedModule mod;
     std::string fns;
-    emitTable(surface, numSurface, hoist, "s_", mod, mod.surface, fns, mod.surfaceGroups, &mod.surfaceEmissive);
-    emitTable(light, numLight, hoist, "l_", mod, mod.light, fns, mod.lightGroups, nullptr);
+    emitTable(surface, numSurface, hoist, "s_", mod, mod.surface, fns, mod.surfaceGroups, &mod.surfaceEmissive,
+              textures);
+    emitTable(light, numLight, hoist, "l_", mod, mod.light, fns, mod.lightGroups, nullptr, textures);
 
     std::string src;
     src += "// generated by raymond_b200 codegen (shader graphs -> CUDA)\n";

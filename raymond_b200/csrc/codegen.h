@@ -29,10 +29,23 @@ struct GeneratedModule {
     int surfaceGroups = 0, lightGroups = 0;
 };
 
+// The scene's textures as the codegen sees them: image-texture nodes name a
+// file, which becomes the slot of the texture of that name (channels decide
+// the pixel format); an unknown file reads slot names.size(), a 1 x 1 zero
+// texture (MaterialBuilder.swift:224-234, where a file that fails to load
+// becomes a 1 x 1 single-channel texture).
+struct TextureTable {
+    std::vector<std::string> names;
+    std::vector<uint32_t> channels;
+    static TextureTable of(const rmd_texture *textures, int count);
+    uint32_t slot(const std::string &name) const;
+    uint32_t channelsOf(uint32_t slot) const { return slot < channels.size() ? channels[slot] : 1u; }
+};
+
 // Emits one function per distinct graph structure; literal inputs become
 // loads from a per-material parameter block when `hoist` is set, or inline
 // constants (the reference's code shape) otherwise.  Throws CodegenError.
 GeneratedModule generateModule(const rmd_material *surface, int numSurface, const rmd_material *light, int numLight,
-                               bool hoist);
+                               bool hoist, const TextureTable &textures = TextureTable());
 
 }  // namespace rmdhost

@@ -400,6 +400,76 @@ struct ColorInvert {  // nodes.hpp:1387-1394
         color = f4(c, color.w);
     }
 };
+// Metal's linear sampler with address::repeat over normalized coordinates
+// (the sampler of nodes.hpp:517): texel centres at (i + 1/2) / size, the four
+// nearest texels wrapped around the image and blended bilinearly, in FP32.
+RMD_HD int wrapTexel(float i, int n) {
+    const float m = i - floorf(i / (float)n) * (float)n;  // in [0, n] up to rounding
+    const int k = (int)m;
+    return k < 0 ? 0 : (k >= n ? n - 1 : k);
+}
+RMD_HD float4 sampleLinearRepeat(const TextureView &t, float2 uv) {
+    const float x = uv.x * (float)t.width - 0.5f, y = uv.y * (float)t.height - 0.5f;
+    const float x0f = floorf(x), y0f = floorf(y);
+    const float ax = x - x0f, ay = y - y0f;
+    const int x0 = wrapTexel(x0f, t.width), y0 = wrapTexel(y0f, t.height);
+    const int x1 = x0 + 1 == t.width ? 0 : x0 + 1, y1 = y0 + 1 == t.height ? 0 : y0 + 1;
+    const float4 *row0 = t.texels + (size_t)y0 * t.width, *row1 = t.texels + (size_t)y1 * t.width;
+    const float4 top = lerp(row0[x0], row0[x1], ax), bottom = lerp(row1[x0], row1[x1], ax);
+    return lerp(top, bottom, ay);
+}
+
+// color.hpp:74-78
+RMD_HD float3 xyz_to_rgb(float3 c) {
+    return make_float3(3.240479f * c.x + -1.537150f * c.y + -0.498535f * c.z,
+                       -0.969256f * c.x + 1.875991f * c.y + 0.041556f * c.z,
+                       0.055648f * c.x + -0.204043f * c.y + 1.057311f * c.z);
+}
+
+struct kTexImage {
+    enum Interpolation { INTERPOLATION_LINEAR };
+    enum Projection { PROJECTION_FLAT, PROJECTION_BOX, PROJECTION_EQUIRECTANGULAR, PROJECTION_MIRROR_BALL };
+    enum Extension { EXTENSION_REPEAT };
+    enum Alpha { ALPHA_STRAIGHT };
+    enum ColorSpace {
+        COLOR_SPACE_LINEAR,
+        COLOR_SPACE_SRGB,
+        COLOR_SPACE_NON_COLOR,
+        COLOR_SPACE_RAW,
+        COLOR_SPACE_XYZ,
+        COLOR_SPACE_FILMIC_LOG
+    };
+    enum PixelFormat { PIXEL_FORMAT_R, PIXEL_FORMAT_RGBA };
+};
+// nodes.hpp:486-564 (the image and environment texture nodes): project the
+// vector (flat: (x, 1 - y); equirectangular: the sphere to the unit square;
+// box and mirror ball are not implemented there and read (0, 0)), sample with
+// repeat, a single-channel image as grey, then decode the colour space.
+template <int TextureIndex, kTexImage::Interpolation Interp, kTexImage::Projection Projection,
+          kTexImage::Extension Extension, kTexImage::Alpha Alpha, kTexImage::ColorSpace ColorSpace,
+          kTexImage::PixelFormat PixelFormat>
+struct TexImage {
+    float3 vector;
+    float4 color;
+    float alpha;
+    RMD_HD static float srgbToLinear(float c) {  // nodes.hpp:556-562
+        if (c < 0.04045f) return c < 0.0f ? 0.0f : c * (1.0f / 12.92f);
+        return powf((c + 0.055f) * (1.0f / 1.055f), 2.4f);
+    }
+    RMD_HD void compute(const Context &ctx, const ShadingContext &) {
+        float2 projected = make_float2(0.0f, 0.0f);
+        if (Projection == kTexImage::PROJECTION_FLAT) projected = make_float2(vector.x, 1.0f - vector.y);
+        else if (Projection == kTexImage::PROJECTION_EQUIRECTANGULAR) projected = warp::equirectSphereToSquare(vector);
+        color = sampleLinearRepeat(ctx.textures[TextureIndex], projected);
+        alpha = color.w;
+        if (PixelFormat == kTexImage::PIXEL_FORMAT_R) color = make_float4(color.x, color.x, color.x, 1.0f);
+        if (ColorSpace == kTexImage::COLOR_SPACE_SRGB)
+            color = make_float4(srgbToLinear(color.x), srgbToLinear(color.y), srgbToLinear(color.z), color.w);
+        else if (ColorSpace == kTexImage::COLOR_SPACE_XYZ)
+            color = f4(xyz_to_rgb(xyz(color)), color.w);
+    }
+};
+
 struct kMapping {
     enum Type { TYPE_MAPPING };  // the exporter writes the node's type, MAPPING, for every vector type
 };

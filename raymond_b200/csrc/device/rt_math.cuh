@@ -193,6 +193,10 @@ RMD_HD float2 uniformSphereToSquare(float3 v) {
     return make_float2(x < 0.0f ? x + 1.0f : x, y);
 }
 RMD_HD float uniformSquareToSpherePdf() { return 1.0f / (4.0f * M_PI_F); }
+// warp.hpp:5-10: longitude from atan2(x, y) shifted by a quarter turn, latitude from z
+RMD_HD float2 equirectSphereToSquare(float3 v) {
+    return make_float2((atan2f(v.x, v.y) + M_PI_F / 2.0f) / (2.0f * M_PI_F), acosf(v.z / length(v)) / M_PI_F);
+}
 RMD_HD float2 uniformSquareToDisk(float2 uv) {
     float s, c;
     sincosf(2.0f * M_PI_F * uv.x, &s, &c);

@@ -49,6 +49,13 @@ struct ShapeLight {  // bridge/lights/ShapeLight.hpp
     float emissiveArea;
 };
 
+// One texture of the scene, RGBA floats row by row from the top of the image
+// (single-channel images as (r, 0, 0, 1), RGB with alpha 1).
+struct TextureView {
+    const float4 *texels;
+    int width, height, channels, pad;
+};
+
 struct Context {
     const float4 *vertices;  // object space, xyz
     const float4 *normals;   // xyz
@@ -73,6 +80,8 @@ struct Context {
     float4 cameraTransform[4];
     float nearClip, farClip, focalLength, pad;
     float2 shift;
+    const TextureView *textures;  // the scene's textures, then a 1 x 1 zero texture for missing files
+    int numTextures, pad2;
 };
 
 struct LightSample {  // lights/LightSample.hpp:6-34

@@ -110,6 +110,7 @@ struct rmd_scene {
     DevBuf areaLights, pointLights, sunLights, spotLights, shapeLights;
     DevBuf surfaceTable, lightTable, materialParams;
     DevBuf bvhNodes, bvhTris;
+    DevBuf textureTexels, textureViews;  // RGBA float texels of all textures; one TextureView each
     rmdhost::JitModule jit;   // default variant (envmap build, test hooks, default shade kernel)
     std::string moduleSource;
     std::map<int, std::unique_ptr<rmdhost::JitModule>> variants;  // shade kernels by minimum blocks per SM
@@ -366,6 +367,50 @@ static rmd_status validateSceneDesc(const rmd_scene_desc *d) {
     if (d->world_shader >= d->num_light_materials) return fail(RMD_ERROR_INVALID_ARGUMENT, "world_shader out of range");
     if (d->envmap_exponent < 0 || d->envmap_exponent > 12)
         return fail(RMD_ERROR_INVALID_ARGUMENT, "envmap_exponent out of range (0..12)");
+    if (d->num_textures < 0 || (d->num_textures > 0 && !d->textures))
+        return fail(RMD_ERROR_INVALID_ARGUMENT, "invalid texture list");
+    for (int i = 0; i < d->num_textures; i++) {
+        const rmd_texture &t = d->textures[i];
+        if (!t.name || !t.data || t.width == 0 || t.height == 0 || t.width > 65536 || t.height > 65536 ||
+            (t.channels != 1 && t.channels != 3 && t.channels != 4) || t.format > RMD_TEXTURE_F32)
+            return fail(RMD_ERROR_INVALID_ARGUMENT, "invalid texture " + std::to_string(i));
+    }
+    return RMD_OK;
+}
+
+// The textures as the device reads them: RGBA floats (a single-channel
+// image as (r, 0, 0, 1), RGB with alpha 1, integers normalised), then a
+// 1 x 1 zero single-channel texture, the slot of files that are missing.
+static rmd_status uploadTextures(const rmd_texture *textures, int count, rmd_scene *s, cudaStream_t st) {
+    std::vector<float4> texels;
+    std::vector<TextureView> views;
+    std::vector<size_t> offsets;
+    for (int i = 0; i < count; i++) {
+        const rmd_texture &t = textures[i];
+        offsets.push_back(texels.size());
+        const size_t n = (size_t)t.width * t.height;
+        texels.resize(texels.size() + n);
+        float4 *out = texels.data() + offsets.back();
+        for (size_t p = 0; p < n; p++) {
+            float v[4] = {0.0f, 0.0f, 0.0f, 1.0f};
+            for (uint32_t c = 0; c < t.channels; c++) {
+                const size_t k = p * t.channels + c;
+                if (t.format == RMD_TEXTURE_U8) v[c] = (float)static_cast<const uint8_t *>(t.data)[k] / 255.0f;
+                else if (t.format == RMD_TEXTURE_U16) v[c] = (float)static_cast<const uint16_t *>(t.data)[k] / 65535.0f;
+                else v[c] = static_cast<const float *>(t.data)[k];
+            }
+            out[p] = make_float4(v[0], v[1], v[2], v[3]);
+        }
+        views.push_back(TextureView{nullptr, (int)t.width, (int)t.height, (int)t.channels, 0});
+    }
+    offsets.push_back(texels.size());
+    texels.push_back(make_float4(0.0f, 0.0f, 0.0f, 1.0f));
+    views.push_back(TextureView{nullptr, 1, 1, 1, 0});
+    RMD_CUDA(s->textureTexels.upload(texels.data(), texels.size() * sizeof(float4), st));
+    for (size_t i = 0; i < views.size(); i++) views[i].texels = s->textureTexels.as<float4>() + offsets[i];
+    RMD_CUDA(s->textureViews.upload(views.data(), views.size() * sizeof(TextureView), st));
+    s->dctx.textures = s->textureViews.as<TextureView>();
+    s->dctx.numTextures = (int)views.size();
     return RMD_OK;
 }
 
@@ -375,7 +420,8 @@ static rmd_status validateSceneDesc(const rmd_scene_desc *d) {
 // (0 for a scene of its own; the scene's slice of a module shared by the
 // scenes of a batch).
 static rmd_status buildSceneData(rmd_context *ctx, const rmd_scene_desc *d, rmd_scene *s,
-                                 const rmdhost::GeneratedModule &mod, int surfaceBase, int lightBase) {
+                                 const rmdhost::GeneratedModule &mod, int surfaceBase, int lightBase,
+                                 const rmd_texture *textures, int numTextures) {
     cudaStream_t st = ctx->stream;
     s->ctx = ctx;
     s->numSurface = d->num_surface_materials;
@@ -656,6 +702,8 @@ static rmd_status buildSceneData(rmd_context *ctx, const rmd_scene_desc *d, rmd_
     c.farClip = d->camera.far_clip;
     c.focalLength = d->camera.focal_length;
     c.shift = make_float2(d->camera.shift[0], d->camera.shift[1]);
+    rmd_status tr = uploadTextures(textures, numTextures, s, st);
+    if (tr != RMD_OK) return tr;
 
     s->defaultMinBlocks = defaultShadeMinBlocks();
     return RMD_OK;
@@ -672,11 +720,12 @@ rmd_status rmd_scene_create(rmd_context *ctx, const rmd_scene_desc *d, rmd_scene
     try {
         const bool hoist = std::getenv("RMD_NO_HOIST") == nullptr;
         mod = rmdhost::generateModule(d->surface_materials, d->num_surface_materials, d->light_materials,
-                                      d->num_light_materials, hoist);
+                                      d->num_light_materials, hoist,
+                                      rmdhost::TextureTable::of(d->textures, d->num_textures));
     } catch (const rmdhost::CodegenError &e) {
         return fail(e.status, e.message);
     }
-    if ((r = buildSceneData(ctx, d, s.get(), mod, 0, 0)) != RMD_OK) return r;
+    if ((r = buildSceneData(ctx, d, s.get(), mod, 0, 0, d->textures, d->num_textures)) != RMD_OK) return r;
     const std::string err = rmdhost::compileModule(
         mod.source, s->jit, {"-DRMD_SHADE_MIN_BLOCKS=" + std::to_string(s->defaultMinBlocks)});
     if (!err.empty()) return fail(RMD_ERROR_NVRTC, err);
@@ -1364,8 +1413,10 @@ rmd_status rmd_test_generate_source(const rmd_scene_desc *d, int32_t hoist, char
                                     int64_t *needed) {
     if (!d) return fail(RMD_ERROR_INVALID_ARGUMENT, "NULL desc");
     try {
-        rmdhost::GeneratedModule mod = rmdhost::generateModule(d->surface_materials, d->num_surface_materials,
-                                                               d->light_materials, d->num_light_materials, hoist != 0);
+        rmdhost::GeneratedModule mod =
+            rmdhost::generateModule(d->surface_materials, d->num_surface_materials, d->light_materials,
+                                    d->num_light_materials, hoist != 0,
+                                    rmdhost::TextureTable::of(d->textures, d->num_textures));
         if (needed) *needed = (int64_t)mod.source.size() + 1;
         if (buf && buflen > 0) {
             const size_t n = std::min<size_t>((size_t)buflen - 1, mod.source.size());
@@ -1383,8 +1434,10 @@ rmd_status rmd_test_jit_compile(const rmd_scene_desc *d, int32_t hoist, char *lo
     if (!d) return fail(RMD_ERROR_INVALID_ARGUMENT, "NULL desc");
     std::string msg;
     try {
-        rmdhost::GeneratedModule mod = rmdhost::generateModule(d->surface_materials, d->num_surface_materials,
-                                                               d->light_materials, d->num_light_materials, hoist != 0);
+        rmdhost::GeneratedModule mod =
+            rmdhost::generateModule(d->surface_materials, d->num_surface_materials, d->light_materials,
+                                    d->num_light_materials, hoist != 0,
+                                    rmdhost::TextureTable::of(d->textures, d->num_textures));
         std::vector<char> cubin;
         bool cached = false;
         std::string err = rmdhost::compileCubin(mod.source, cubin, msg, cached,
@@ -1491,9 +1544,26 @@ rmd_status rmd_batch_create(rmd_context *ctx, const rmd_scene_desc *descs, int32
         surf.insert(surf.end(), descs[i].surface_materials, descs[i].surface_materials + descs[i].num_surface_materials);
         light.insert(light.end(), descs[i].light_materials, descs[i].light_materials + descs[i].num_light_materials);
     }
+    // the scenes' textures in one table (slots are baked into the shared
+    // module); a name used by two scenes must name the same image
+    std::vector<rmd_texture> texUnion;
+    for (int i = 0; i < numScenes; i++)
+        for (int k = 0; k < descs[i].num_textures; k++) {
+            const rmd_texture &t = descs[i].textures[k];
+            auto same = std::find_if(texUnion.begin(), texUnion.end(),
+                                     [&](const rmd_texture &u) { return std::strcmp(u.name, t.name) == 0; });
+            if (same == texUnion.end()) {
+                texUnion.push_back(t);
+            } else if (same->data != t.data || same->width != t.width || same->height != t.height ||
+                       same->channels != t.channels || same->format != t.format) {
+                return fail(RMD_ERROR_INVALID_ARGUMENT,
+                            std::string("texture '") + t.name + "' names different images in two scenes of the batch");
+            }
+        }
     rmdhost::GeneratedModule mod;
     try {
-        mod = rmdhost::generateModule(surf.data(), (int)surf.size(), light.data(), (int)light.size(), true);
+        mod = rmdhost::generateModule(surf.data(), (int)surf.size(), light.data(), (int)light.size(), true,
+                                      rmdhost::TextureTable::of(texUnion.data(), (int)texUnion.size()));
     } catch (const rmdhost::CodegenError &e) {
         return fail(e.status, e.message);
     }
@@ -1504,7 +1574,8 @@ rmd_status rmd_batch_create(rmd_context *ctx, const rmd_scene_desc *descs, int32
     b->moduleSource = mod.source;
     for (int i = 0; i < numScenes; i++) {
         auto sc = std::make_unique<rmd_scene>();
-        rmd_status r = buildSceneData(ctx, &descs[i], sc.get(), mod, surfBase[i], lightBase[i]);
+        rmd_status r = buildSceneData(ctx, &descs[i], sc.get(), mod, surfBase[i], lightBase[i], texUnion.data(),
+                                      (int)texUnion.size());
         if (r != RMD_OK) return r;
         sc->jit = b->jit;  // the batch's module builds the scene's environment map
         sc->ownsModule = false;

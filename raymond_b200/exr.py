@@ -120,3 +120,35 @@ def read_rgba(path: str | Path) -> np.ndarray:
     if a is None:
         a = np.ones_like(ch["R"])
     return np.stack([ch["R"], ch["G"], ch["B"], a], axis=-1)
+
+
+def write_exr(path: str | Path, img: np.ndarray) -> None:
+    """A float image (height, width[, channels]) as an uncompressed FLOAT EXR:
+    1 channel as Y, 3 as R, G, B, 4 as R, G, B, A (stored in name order)."""
+    a = np.asarray(img, np.float32)
+    if a.ndim == 2:
+        a = a[:, :, None]
+    h, w, n = a.shape
+    names = {1: ["Y"], 3: ["R", "G", "B"], 4: ["R", "G", "B", "A"]}[n]
+    order = sorted(range(n), key=lambda k: names[k])
+
+    def attr(name, typ, value):
+        return name.encode() + b"\0" + typ.encode() + b"\0" + struct.pack("<i", len(value)) + value
+
+    chl = b"".join(names[k].encode() + b"\0" + struct.pack("<iB3xii", 2, 0, 1, 1) for k in order) + b"\0"
+    box = struct.pack("<4i", 0, 0, w - 1, h - 1)
+    head = struct.pack("<II", 20000630, 2) + attr("channels", "chlist", chl) + \
+        attr("compression", "compression", b"\0") + attr("dataWindow", "box2i", box) + \
+        attr("displayWindow", "box2i", box) + attr("lineOrder", "lineOrder", b"\0") + \
+        attr("pixelAspectRatio", "float", struct.pack("<f", 1.0)) + \
+        attr("screenWindowCenter", "v2f", struct.pack("<2f", 0, 0)) + \
+        attr("screenWindowWidth", "float", struct.pack("<f", 1.0)) + b"\0"
+    at = len(head) + 8 * h
+    table, blocks = [], []
+    for y in range(h):
+        data = b"".join(a[y, :, k].astype("<f4").tobytes() for k in order)
+        table.append(struct.pack("<Q", at))
+        blocks.append(struct.pack("<ii", y, len(data)) + data)
+        at += 8 + len(data)
+    Path(path).write_bytes(head + b"".join(table) + b"".join(blocks))
+

@@ -22,11 +22,18 @@ Reading rules kept from the reference:
   of its half angle and blend scaled by (1 - that cosine), sun angle as the
   cosine of its half angle, directions normalised.
 * Visibility flags from the exporter's booleans (EntityBuilder.swift:55-64).
+* Image and environment texture nodes name their image file (relative to the
+  scene file); PNG and OpenEXR files, the formats the exporter writes
+  (materials.py:194-209), are read into `scene["textures"]`.  A file that is
+  absent or in another format is left out with a warning, and the node then
+  reads the 1 x 1 zero texture, as the reference does when MTKTextureLoader
+  fails (MaterialBuilder.swift:224-234).
 """
 from __future__ import annotations
 
 import json
 import os
+import warnings
 from pathlib import Path
 from typing import Any
 
@@ -210,9 +217,46 @@ def load_scene(path: str | os.PathLike) -> tuple[dict[str, Any], tuple[int, int]
     else:  # SceneLoader.makeDefaultCamera (SceneLoader.swift:30-41)
         scene["camera"] = {"transform": np.eye(4, dtype=np.float32), "near_clip": 0.1, "far_clip": 100.0,
                            "focal_length": 2.5, "shift": (0.0, 0.0)}
+    scene["textures"] = _read_textures(path.parent, list(materials.values()))
     res = doc.get("render", {}).get("resolution")
     size = (int(res["width"]), int(res["height"])) if res else None
     return scene, size
+
+
+def read_image(path: str | os.PathLike) -> np.ndarray:
+    """A PNG (uint8 / uint16) or OpenEXR (float32) image as (height, width, channels)."""
+    from . import exr, png
+
+    p = Path(path)
+    head = p.read_bytes()[:8]
+    if head.startswith(b"\x89PNG"):
+        return png.read_png(p)
+    if head[:4] == bytes([0x76, 0x2F, 0x31, 0x01]):
+        ch, _ = exr.read_exr(p)
+        if set("RGB") <= set(ch):
+            names = ["R", "G", "B"] + (["A"] if "A" in ch else [])
+        elif "Y" in ch:
+            names = ["Y"]
+        else:
+            names = sorted(ch)[:4]
+        return np.stack([ch[n] for n in names], axis=-1).astype(np.float32)
+    raise SceneFormatError(f"{p.name}: not a PNG or OpenEXR image")
+
+
+def _read_textures(base: Path, graphs: list) -> dict[str, np.ndarray]:
+    out: dict[str, np.ndarray] = {}
+    for graph in graphs:
+        for node in graph.values():
+            if node.get("type") not in ("TEX_IMAGE", "TEX_ENVIRONMENT"):
+                continue
+            file = node.get("parameters", {}).get("filepath")
+            if not file or file in out:
+                continue
+            try:
+                out[file] = read_image(base / file)
+            except (OSError, ValueError) as e:
+                warnings.warn(f"texture {file!r} not loaded ({e}); the node reads a 1 x 1 zero texture")
+    return out
 
 
 def save_scene(scene: dict[str, Any], path: str | os.PathLike, resolution: tuple[int, int] | None = None) -> None:
@@ -269,4 +313,16 @@ def save_scene(scene: dict[str, Any], path: str | os.PathLike, resolution: tuple
                       "focal_length": cam.get("focal_length", 2.5) * 18.0}}
     if resolution:
         doc["render"] = {"resolution": {"width": resolution[0], "height": resolution[1]}}
+    from . import exr, png
+
+    for name, img in scene.get("textures", {}).items():  # beside the scene file, where the nodes name them
+        out = path.parent / name
+        out.parent.mkdir(parents=True, exist_ok=True)
+        a = np.asarray(img)
+        if a.dtype in (np.uint8, np.uint16) and out.suffix.lower() == ".png":
+            png.write_png(out, a, filters=(0, 1, 2, 3, 4))
+        elif out.suffix.lower() == ".exr":
+            exr.write_exr(out, a)
+        else:
+            raise SceneFormatError(f"texture {name!r}: PNG needs uint8 / uint16 data, other images an .exr name")
     path.write_text(json.dumps(doc, indent=2, default=lambda o: o.tolist() if hasattr(o, "tolist") else o))

@@ -47,6 +47,7 @@ def main() -> None:
     out["noise_points"] = pts
     out["noise_cases"] = np.array(NOISE_CASES, np.float32)
     out["noise"] = np.stack([R.fractal_noise3(pts, d, r) for d, r in NOISE_CASES])
+    R.set_textures(pin_materials.textures())
     rec = R.shading_records(RECORDS, RECORD_SEED)
     names = [n for n, _ in pin_materials.materials()]
     out["records"] = rec

@@ -196,6 +196,26 @@ def test_next_node_set_render(gpu_ctx):
     assert min(fr) >= MIN_MATCH, fr
 
 
+def test_image_textures_render(gpu_ctx):
+    """The Cornell box with its walls and boxes in the image-texture material
+    (an sRGB byte image through a Mapping, a 16-bit single-channel image, a
+    float environment image and a missing file) and the textures in the scene:
+    per-sample parity with the oracle."""
+    pin, _ = _pin_modules()
+    sc = scenes.cornell(seed=1, envmap_exponent=7)
+    mats = dict(pin.materials())
+    base = len(sc["materials"])
+    sc["materials"] = sc["materials"] + [("textured", mats["image_textures"])]
+    sc["textures"] = pin.textures()
+    for sh in sc["shapes"][:-1]:
+        sh["materials"] = np.full_like(sh["materials"], base)
+    desc = SceneDesc(sc)
+    scene = api.Scene(gpu_ctx, desc)
+    orc = O.OracleScene(desc)
+    fr = per_sample(desc, scene, orc, 96, 96, range(4), 8)
+    assert min(fr) >= MIN_MATCH, fr
+
+
 def _all_lights_scene():
     return scenes.cornell_all_lights(seed=4, envmap_exponent=7)
 

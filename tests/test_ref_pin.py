@@ -69,6 +69,7 @@ def test_oracle_matches_reference_live(oracle_pin_scene):
     pts = np.random.default_rng(9).uniform(-1e3, 1e3, (4096, 3)).astype(np.float32)
     for d, r in [(1.0, 0.3), (6.25, 0.55)]:
         assert np.array_equal(R.fractal_noise3(pts, d, r).view(np.uint32), O.fractal_noise3(pts, d, r).view(np.uint32))
+    R.set_textures(pin_materials.textures())
     rec = R.shading_records(2048, seed=77)
     names = [n for n, _ in pin_materials.materials()]
     ref_out = np.stack([R.material_eval(m, rec) for m in range(len(names))])
