@@ -105,7 +105,20 @@ __device__ __forceinline__ bool shadePath(const ShadeParams &p, uint32_t i, uint
         // then alpha q + (1 - alpha) p_bsdf in every MIS weight that uses it.
         const bool guided = depth < fp.guideDepth;
         const GuideMixture *gm = &pool.guide[orderPos];  // hits are shaded in order: mixture by that position
-        const float alpha = guided ? gm->alpha : 0.0f;
+        float alpha = guided ? gm->alpha : 0.0f;
+        if (guided) {
+            // A warp whose lanes are all guided uses one selection probability,
+            // the mean of their alphas: the technique choice below is then the
+            // same on every lane and the warp does not run both techniques.  A
+            // probability that does not depend on this path's own sample keeps
+            // the one-sample MIS estimator unbiased.
+            if (__activemask() == 0xffffffffu) {
+                float sum = alpha;
+#pragma unroll
+                for (int off = 16; off > 0; off >>= 1) sum += __shfl_xor_sync(0xffffffffu, sum, off);
+                alpha = sum * (1.0f / 32.0f);
+            }
+        }
         GuideFeatures gf;  // training: the guide's input features of this vertex
         const float meanThroughput = mean(rayWeight);
         if (training)
