@@ -177,8 +177,10 @@ struct Decoded {
 __device__ Decoded decode(const float *o) {
     Decoded d;
     float maxLogit = -1e30f;
+#pragma unroll
     for (int j = 0; j < GUIDE_LOBES; j++) maxLogit = fmaxf(maxLogit, o[4 * j + 3]);
     float sum = 0.0f;
+#pragma unroll
     for (int j = 0; j < GUIDE_LOBES; j++) {
         d.st[j] = sigmoid(o[4 * j + 0]);
         d.sp[j] = sigmoid(o[4 * j + 1]);
@@ -237,11 +239,15 @@ __device__ GuideMixture pack(const Decoded &d) {
 // alone, -y log q(w); the selection probability a learns the MIS combination,
 // -y log(a q(w) + (1 - a) pb), with q held fixed.  The returned loss is the
 // second (the cross entropy of the distribution that is sampled).
-__device__ float lossGradient(const float *o, float3 w, float pb, float y, float scale, float *grad) {
+// The gradient is written as BF16 to out[0..GUIDE_OUTPUTS) (the unused
+// outputs and clamped concentrations zero), one lobe at a time, so nothing of
+// it is held in an indexed local array.
+__device__ float lossGradient(const float *o, float3 w, float pb, float y, float scale, uint16_t *out) {
     const Decoded d = decode(o);
     float v[GUIDE_LOBES], q = 0.0f;
     float3 mu[GUIDE_LOBES];
     float kappa[GUIDE_LOBES], cosw[GUIDE_LOBES];
+#pragma unroll
     for (int j = 0; j < GUIDE_LOBES; j++) {
         mu[j] = lobeMean(d, j);
         kappa[j] = __expf(d.logKappa[j]);
@@ -252,21 +258,24 @@ __device__ float lossGradient(const float *o, float3 w, float pb, float y, float
     const float a = d.alpha;
     const float pmix = fmaxf(a * q + (1.0f - a) * pb, 1e-20f);
     const float loss = -y * logf(pmix);
-    for (int c = 0; c < GUIDE_OUTPUTS; c++) grad[c] = 0.0f;
+    for (int c = 4 * GUIDE_LOBES + 1; c < GUIDE_OUTPUTS; c++) out[c] = 0;
     // selection probability: a = amin + (amax - amin) sigmoid(z)
-    grad[4 * GUIDE_LOBES] = -y / pmix * scale * (q - pb) * (GUIDE_ALPHA_MAX - GUIDE_ALPHA_MIN) * d.alphaSig *
-                            (1.0f - d.alphaSig);
+    out[4 * GUIDE_LOBES] = toBf16(-y / pmix * scale * (q - pb) * (GUIDE_ALPHA_MAX - GUIDE_ALPHA_MIN) * d.alphaSig *
+                                  (1.0f - d.alphaSig));
     const float gq = -y / fmaxf(q, 1e-20f) * scale;  // dL/dq of -y log q
+#pragma unroll
     for (int j = 0; j < GUIDE_LOBES; j++) {
         // softmax weights
-        grad[4 * j + 3] = gq * d.lambda[j] * (v[j] - q);
+        out[4 * j + 3] = toBf16(gq * d.lambda[j] * (v[j] - q));
         const float gv = gq * d.lambda[j];  // dL/dv_j
         // concentration: dv/dk = v (1/k - 2 / (e^{2k} - 1) + cos - 1), dk/dlogk = k
+        float gk = 0.0f;
         if (!d.kappaClamped[j]) {
             const float k = kappa[j];
             const float dlogC = 1.0f / k - 2.0f / expm1f(2.0f * k);
-            grad[4 * j + 2] = gv * v[j] * (dlogC + cosw[j] - 1.0f) * k;
+            gk = gv * v[j] * (dlogC + cosw[j] - 1.0f) * k;
         }
+        out[4 * j + 2] = toBf16(gk);
         // mean direction: dv/dmu = v k w; mu(theta, phi)
         const float gmu = gv * v[j] * kappa[j];
         float st, ct, sp, cp;
@@ -274,8 +283,8 @@ __device__ float lossGradient(const float *o, float3 w, float pb, float y, float
         sincospif(2.0f * d.sp[j], &sp, &cp);
         const float3 dmu_dtheta = make_float3(ct * cp, ct * sp, -st);
         const float3 dmu_dphi = make_float3(-st * sp, st * cp, 0.0f);
-        grad[4 * j + 0] = gmu * dot(w, dmu_dtheta) * M_PI_F * d.st[j] * (1.0f - d.st[j]);
-        grad[4 * j + 1] = gmu * dot(w, dmu_dphi) * 2.0f * M_PI_F * d.sp[j] * (1.0f - d.sp[j]);
+        out[4 * j + 0] = toBf16(gmu * dot(w, dmu_dtheta) * M_PI_F * d.st[j] * (1.0f - d.st[j]));
+        out[4 * j + 1] = toBf16(gmu * dot(w, dmu_dphi) * 2.0f * M_PI_F * d.sp[j] * (1.0f - d.sp[j]));
     }
     return loss;
 }
@@ -665,7 +674,7 @@ __global__ void __launch_bounds__(kTcThreads) k_guide_infer(Counters *cnt, const
 }
 
 // Gradient of the mean loss over a batch of records, accumulated into net.grad.
-__global__ void __launch_bounds__(32 * kWarps) k_guide_train(RecordBatch batch, const float *sumY, GuideNetView net,
+__global__ void __launch_bounds__(32 * kWarps, 1) k_guide_train(RecordBatch batch, const float *sumY, GuideNetView net,
                                                           float *lossOut) {
     extern __shared__ __align__(16) unsigned char smem[];
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31, g = lane >> 2, t = lane & 3;
@@ -690,28 +699,25 @@ __global__ void __launch_bounds__(32 * kWarps) k_guide_train(RecordBatch batch, 
         forward(s, tw, g, t);
         // output deltas: lanes 0..15, one sample each (zero for padding rows)
         if (lane < 16) {
-            float grad[GUIDE_OUTPUTS];
+            uint16_t *deltaRow = &s.d[0][lane * kLdH];
             if (r < n) {
                 const float y = fminf(rc.y * invMeanY, 100.0f);
                 lossSum += lossGradient(&s.o[lane * kLdO], make_float3(rc.dir[0], rc.dir[1], rc.dir[2]), rc.pdfBsdf,
-                                        y, scale, grad);
+                                        y, scale, deltaRow);
             } else {
-                for (int c = 0; c < GUIDE_OUTPUTS; c++) grad[c] = 0.0f;
+                for (int c = 0; c < GUIDE_OUTPUTS; c++) deltaRow[c] = 0;
             }
-            for (int c = 0; c < GUIDE_OUTPUTS; c++) s.d[0][lane * kLdH + c] = toBf16(grad[c]);
         }
         __syncwarp();
         // backward through the four layers: layer l maps h[l-1] (x for l = 0) to h[l]
-        const uint16_t *acts[4] = {s.x, s.h[0], s.h[1], s.h[2]};
-        const int ldActs[4] = {kLd0, kLdH, kLdH, kLdH};
         int cur = 0;  // delta of layer l's output in s.d[cur]
 #pragma unroll 1
         for (int l = 3; l >= 0; l--) {
             const int nOut = l == 3 ? GUIDE_OUTPUTS : GUIDE_HIDDEN;
             const int nIn = l == 0 ? GUIDE_INPUTS : GUIDE_HIDDEN;
             const uint16_t *delta = s.d[cur];
-            const uint16_t *in = acts[l];
-            const int ldIn = ldActs[l];
+            const uint16_t *in = l == 0 ? s.x : s.h[l - 1];
+            const int ldIn = l == 0 ? kLd0 : kLdH;
             float *gW = acc + net.wOffset[l];
             float *gB = acc + net.bOffset[l];
             // dW[nOut][nIn] += delta^T . in
