@@ -298,7 +298,8 @@ Invocation makeInvocation(const rmd_node &n, Emitter &em, const TextureTable &te
         inv.type = "NormalMap<" + enumValue("NormalMap", "SPACE", paramString(n, "space", "TANGENT"), {"TANGENT", "WORLD"}) +
                    ">";
     } else if (t == "TEX_IMAGE" || t == "TEX_ENVIRONMENT") {  // :387-433
-        const uint32_t slot = textures.slot(paramString(n, "filepath", ""));
+        uint32_t slot, channels;
+        textures.lookup(paramString(n, "filepath", ""), slot, channels);
         inv.kernel = "TexImage";
         inv.type = "TexImage<" + std::to_string(slot) + ", " +
                    enumValue("TexImage", "INTERPOLATION", paramString(n, "interpolation", "Linear"), {"LINEAR"}) + ", " +
@@ -308,7 +309,7 @@ Invocation makeInvocation(const rmd_node &n, Emitter &em, const TextureTable &te
                    ", kTexImage::EXTENSION_REPEAT, kTexImage::ALPHA_STRAIGHT, " +
                    enumValue("TexImage", "COLOR_SPACE", paramString(n, "colorspace", "sRGB"),
                              {"LINEAR", "SRGB", "NON_COLOR", "RAW", "XYZ", "FILMIC_LOG"}) +
-                   ", kTexImage::PIXEL_FORMAT_" + (textures.channelsOf(slot) == 1 ? "R" : "RGBA") + ">";
+                   ", kTexImage::PIXEL_FORMAT_" + (channels == 1 ? "R" : "RGBA") + ">";
     } else if (t == "HUE_SAT") plain("HueSaturation");
     else if (t == "BRIGHTCONTRAST") plain("BrightnessContrast");
     else if (t == "BLACKBODY") plain("Blackbody");
@@ -486,14 +487,14 @@ MaterialCode emitMaterial(const rmd_material &m, bool hoist, const TextureTable 
 
 void emitTable(const rmd_material *mats, int n, bool hoist, const std::string &prefix, GeneratedModule &mod,
                MaterialTable &table, std::string &functions, int &groups, std::vector<bool> *emissive,
-               const TextureTable &textures) {
+               const TextureTable &textures, const std::vector<const TextureTable *> &perMaterial) {
     std::map<std::string, int> groupOf;
     std::vector<std::string> groupBodies;
     std::vector<std::vector<std::string>> groupNames;
     std::vector<std::vector<int>> groupMembers;
     std::vector<MaterialCode> codes;
     for (int i = 0; i < n; i++) {
-        codes.push_back(emitMaterial(mats[i], hoist, textures));
+        codes.push_back(emitMaterial(mats[i], hoist, i < (int)perMaterial.size() ? *perMaterial[i] : textures));
         const MaterialCode &mc = codes.back();
         if (emissive) emissive->push_back(mc.emissive);
         int g;
@@ -567,19 +568,26 @@ TextureTable TextureTable::of(const rmd_texture *textures, int count) {
     return t;
 }
 
-uint32_t TextureTable::slot(const std::string &name) const {
+void TextureTable::lookup(const std::string &name, uint32_t &slot, uint32_t &numChannels) const {
     for (size_t i = 0; i < names.size(); i++)
-        if (names[i] == name) return (uint32_t)i;
-    return (uint32_t)names.size();
+        if (names[i] == name) {
+            slot = slots.empty() ? (uint32_t)i : slots[i];
+            numChannels = channels[i];
+            return;
+        }
+    slot = slots.empty() ? (uint32_t)names.size() : missingSlot;
+    numChannels = 1;
 }
 
 GeneratedModule generateModule(const rmd_material *surface, int numSurface, const rmd_material *light, int numLight,
-                               bool hoist, const TextureTable &textures) {
+                               bool hoist, const TextureTable &textures,
+                               const std::vector<const TextureTable *> &surfaceTables,
+                               const std::vector<const TextureTable *> &lightTables) {
     GeneratedModule mod;
     std::string fns;
     emitTable(surface, numSurface, hoist, "s_", mod, mod.surface, fns, mod.surfaceGroups, &mod.surfaceEmissive,
-              textures);
-    emitTable(light, numLight, hoist, "l_", mod, mod.light, fns, mod.lightGroups, nullptr, textures);
+              textures, surfaceTables);
+    emitTable(light, numLight, hoist, "l_", mod, mod.light, fns, mod.lightGroups, nullptr, textures, lightTables);
 
     std::string src;
     src += "// generated by raymond_b200 codegen (shader graphs -> CUDA)\n";

@@ -37,15 +37,21 @@ struct GeneratedModule {
 struct TextureTable {
     std::vector<std::string> names;
     std::vector<uint32_t> channels;
+    std::vector<uint32_t> slots;  // slot of each name (empty: the name's index)
+    uint32_t missingSlot = 0;     // slot of unknown names (names.size() when slots is empty)
     static TextureTable of(const rmd_texture *textures, int count);
-    uint32_t slot(const std::string &name) const;
-    uint32_t channelsOf(uint32_t slot) const { return slot < channels.size() ? channels[slot] : 1u; }
+    // the slot a file name reads and that texture's channel count (1 for the zero texture)
+    void lookup(const std::string &name, uint32_t &slot, uint32_t &numChannels) const;
 };
 
 // Emits one function per distinct graph structure; literal inputs become
 // loads from a per-material parameter block when `hoist` is set, or inline
 // constants (the reference's code shape) otherwise.  Throws CodegenError.
+// `surfaceTables` / `lightTables`, when given, hold one texture table per
+// material (the scenes of a batch share a module but not their textures).
 GeneratedModule generateModule(const rmd_material *surface, int numSurface, const rmd_material *light, int numLight,
-                               bool hoist, const TextureTable &textures = TextureTable());
+                               bool hoist, const TextureTable &textures = TextureTable(),
+                               const std::vector<const TextureTable *> &surfaceTables = {},
+                               const std::vector<const TextureTable *> &lightTables = {});
 
 }  // namespace rmdhost

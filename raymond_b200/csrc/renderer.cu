@@ -1544,26 +1544,35 @@ rmd_status rmd_batch_create(rmd_context *ctx, const rmd_scene_desc *descs, int32
         surf.insert(surf.end(), descs[i].surface_materials, descs[i].surface_materials + descs[i].num_surface_materials);
         light.insert(light.end(), descs[i].light_materials, descs[i].light_materials + descs[i].num_light_materials);
     }
-    // the scenes' textures in one table (slots are baked into the shared
-    // module); a name used by two scenes must name the same image
+    // The scenes' textures in one table (slots are baked into the shared
+    // module; an image two scenes pass under the same name is stored once).
+    // Each scene's materials resolve file names against its own textures.
     std::vector<rmd_texture> texUnion;
-    for (int i = 0; i < numScenes; i++)
+    std::vector<rmdhost::TextureTable> sceneTables(numScenes);
+    for (int i = 0; i < numScenes; i++) {
+        rmdhost::TextureTable &t = sceneTables[i];
         for (int k = 0; k < descs[i].num_textures; k++) {
-            const rmd_texture &t = descs[i].textures[k];
-            auto same = std::find_if(texUnion.begin(), texUnion.end(),
-                                     [&](const rmd_texture &u) { return std::strcmp(u.name, t.name) == 0; });
-            if (same == texUnion.end()) {
-                texUnion.push_back(t);
-            } else if (same->data != t.data || same->width != t.width || same->height != t.height ||
-                       same->channels != t.channels || same->format != t.format) {
-                return fail(RMD_ERROR_INVALID_ARGUMENT,
-                            std::string("texture '") + t.name + "' names different images in two scenes of the batch");
-            }
+            const rmd_texture &x = descs[i].textures[k];
+            auto same = std::find_if(texUnion.begin(), texUnion.end(), [&](const rmd_texture &u) {
+                return std::strcmp(u.name, x.name) == 0 && u.data == x.data && u.width == x.width &&
+                       u.height == x.height && u.channels == x.channels && u.format == x.format;
+            });
+            t.names.push_back(x.name);
+            t.channels.push_back(x.channels);
+            t.slots.push_back((uint32_t)(same - texUnion.begin()));
+            if (same == texUnion.end()) texUnion.push_back(x);
         }
+    }
+    std::vector<const rmdhost::TextureTable *> surfTables, lightTables;
+    for (int i = 0; i < numScenes; i++) {
+        sceneTables[i].missingSlot = (uint32_t)texUnion.size();  // the zero texture after the union
+        surfTables.insert(surfTables.end(), descs[i].num_surface_materials, &sceneTables[i]);
+        lightTables.insert(lightTables.end(), descs[i].num_light_materials, &sceneTables[i]);
+    }
     rmdhost::GeneratedModule mod;
     try {
         mod = rmdhost::generateModule(surf.data(), (int)surf.size(), light.data(), (int)light.size(), true,
-                                      rmdhost::TextureTable::of(texUnion.data(), (int)texUnion.size()));
+                                      rmdhost::TextureTable(), surfTables, lightTables);
     } catch (const rmdhost::CodegenError &e) {
         return fail(e.status, e.message);
     }

@@ -69,6 +69,48 @@ def test_batch_graph_equals_host_loop_and_accumulates(gpu_ctx, batch_setup):
     assert g.stats()["iterations"] >= 2 and g.stats()["errors"] == 0
 
 
+def _textured_cornell(seed, textures):
+    import sys
+    from pathlib import Path
+
+    sys.path.insert(0, str(Path(__file__).resolve().parents[1] / "oracle" / "ref"))
+    import pin_materials
+
+    sc = scenes.cornell(seed=seed, envmap_exponent=6)
+    base = len(sc["materials"])
+    sc["materials"] = sc["materials"] + [("textured", dict(pin_materials.materials())["image_textures"])]
+    sc["textures"] = textures
+    for sh in sc["shapes"][:-1]:
+        sh["materials"] = np.full_like(sh["materials"], base)
+    return sc
+
+
+def test_batch_with_textures(gpu_ctx):
+    """Textured scenes in one batch: every scene's image nodes read its own
+    textures (a file another scene has but this one lacks reads the zero
+    texture; one name may mean different images in two scenes), and each view
+    renders as it does alone."""
+    import sys
+    from pathlib import Path
+
+    sys.path.insert(0, str(Path(__file__).resolve().parents[1] / "oracle" / "ref"))
+    import pin_materials
+
+    tex = pin_materials.textures()
+    lacking = {k: v for k, v in tex.items() if k != "textures/sky.exr"}
+    other = dict(tex)
+    other["textures/albedo.png"] = tex["textures/albedo.png"][::-1].copy()  # same name, another image
+    descs = [SceneDesc(_textured_cornell(1, tex)), SceneDesc(_textured_cornell(2, lacking)),
+             SceneDesc(_textured_cornell(3, other))]
+    views = [{"scene": 0, "width": 64, "height": 48}, {"scene": 1, "width": 40, "height": 40},
+             {"scene": 2, "width": 48, "height": 32}]
+    b = api.Batch(gpu_ctx, descs, views)
+    b.render(spp=1, max_depth=8, first_sample=3)
+    for i, v in enumerate(views):
+        single = _single(gpu_ctx, descs[v["scene"]], v, 1, 3, max_depth=8)
+        assert _match(b.film(i), single) >= 0.999, i
+
+
 def test_batch_rejects_bad_views(gpu_ctx, batch_setup):
     descs, views = batch_setup
     with pytest.raises(api.RmdError):
