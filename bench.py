@@ -323,7 +323,7 @@ def run_config5(args) -> dict:
     e_plain = errors(plain)
     plain.close()
     g = batch()
-    settings = {"batch_size": 1 << 20, "learning_rate": 1e-3}
+    settings = {"batch_size": 1 << 20, "learning_rate": 1e-3, "steps_per_batch": 8, "step_records": 1 << 13}
     g.set_guide(sampling=True, training=True, seed=1, **settings)
     ms, spp, parity, curve = 0.0, 0, None, []
     target = float(np.mean(e_plain))
