@@ -72,8 +72,8 @@ BYTES_SHADE_PER_SEGMENT = 84 + 136 + 80 + 48
 BYTES_SHADOW_PER_RAY = 48 + 32
 BYTES_FILM_PER_PATH = 16 + 32 + 80
 # DRAM bytes per unit measured by ncu (dram__bytes_read.sum + dram__bytes_write.sum
-# of one steady-state launch divided by the units it processed; small case, see
-# profiles/ncu_full_spheres_terrain_480x270.md); only the closest-hit kernel's is used
+# of one steady-state launch of the 480x270 case divided by the rays it
+# processed); only the closest-hit kernel's is used
 TRAFFIC_PER_UNIT = {"trace": 78.5}
 GUIDED_W, GUIDED_H, GUIDED_DEPTH, GUIDED_ORACLE_SPP, GUIDED_PLAIN_SPP, GUIDED_CHUNK = 1280, 720, 16, 65536, 1024, 32
 CPU_BASELINE_SPP = 16  # CPU sample: 16 one-spp frames of the full image (about 10-20 s on 16 cores)
