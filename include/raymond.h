@@ -285,6 +285,8 @@ typedef struct rmd_stats {
     uint64_t rays;             /* closest-hit rays traced (segments + misses) */
     double   ms_guide;         /* guide inference and training (0 without guiding) */
     double   ms_guide_train;   /* of which training (gradient and Adam steps) */
+    uint64_t invalid_samples;  /* light and BSDF samples dropped for a non-finite weight (the
+                                  reference drops them without a count) */
 } rmd_stats;
 
 /* ------------------------------------------------ acceleration structures */

@@ -134,7 +134,7 @@ class Stats(C.Structure):
                 ("iterations", C.c_uint64), ("ms_total", C.c_double), ("ms_trace", C.c_double),
                 ("ms_shade", C.c_double), ("ms_shadow", C.c_double), ("ms_film", C.c_double),
                 ("pool_size", C.c_uint32), ("errors", C.c_uint32), ("rays", C.c_uint64),
-                ("ms_guide", C.c_double), ("ms_guide_train", C.c_double)]
+                ("ms_guide", C.c_double), ("ms_guide_train", C.c_double), ("invalid_samples", C.c_uint64)]
 
 
 class GuideSettings(C.Structure):

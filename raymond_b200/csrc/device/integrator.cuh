@@ -136,6 +136,9 @@ __device__ __forceinline__ bool shadePath(const ShadeParams &p, uint32_t i, uint
                 const float misWeight =
                     fp.samplingMode == 1u || !nee.canBeHit ? 1.0f : computeMisWeight(nee.pdf, bsdfPdf);
                 const float3 neeWeight = misWeight * contribution;
+                // a non-finite light sample is dropped, as the reference's
+                // device code drops it, and counted
+                if (!isfinite3(neeWeight)) atomicAdd(&cnt->invalid, 1ull);
                 // shadow rays of the last shade pass are never traced (Renderer.swift:623-625)
                 if (isfinite3(neeWeight) && any_nonzero(neeWeight) && !lastDepth) {
                     const uint32_t k = warpAppend(&cnt->nShadow);
@@ -196,6 +199,7 @@ __device__ __forceinline__ bool shadePath(const ShadeParams &p, uint32_t i, uint
         }
         const float3 weight = rayWeight * bs.weight;
         const float meanWeight = mean(weight);
+        if (!is_finite(meanWeight)) atomicAdd(&cnt->invalid, 1ull);  // the path ends, as in the reference
         if (is_finite(meanWeight)) {
             // Guided, roulette keeps the path with the probability BSDF sampling
             // would give its direction, so directions the guide favours (high

@@ -72,6 +72,7 @@ struct Counters {
     unsigned long long segments;    // closest-hit rays shaded
     unsigned long long shadowRays;  // shadow rays traced
     unsigned long long rays;        // closest-hit rays traced (hits and misses)
+    unsigned long long invalid;     // light and BSDF samples dropped for a non-finite weight
 };
 
 

@@ -27,6 +27,7 @@ __global__ void k_frame_init(Counters *cnt, uint32_t capacity, uint64_t firstPat
     cnt->segments = 0;
     cnt->shadowRays = 0;
     cnt->rays = 0;
+    cnt->invalid = 0;
 }
 
 // ------------------------------------------------------------- film + regeneration

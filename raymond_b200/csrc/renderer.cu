@@ -1115,6 +1115,7 @@ rmd_status rmd_render(rmd_renderer *r, const rmd_render_settings *s) {
     r->stats.segments = h.segments;
     r->stats.rays = h.rays;
     r->stats.shadow_rays = h.shadowRays;
+    r->stats.invalid_samples = h.invalid;
     r->stats.iterations = it;
     r->stats.ms_total = ms;
     r->stats.ms_film = stage[STAGE_FILM];
@@ -1792,6 +1793,7 @@ rmd_status rmd_batch_render(rmd_batch *b, const rmd_render_settings *s) {
     b->stats.segments = h.segments;
     b->stats.rays = h.rays;
     b->stats.shadow_rays = h.shadowRays;
+    b->stats.invalid_samples = h.invalid;
     b->stats.iterations = iterations;
     b->stats.ms_total = ms;
     b->samples = std::max<uint64_t>(b->samples, firstSample + s->spp);

@@ -216,6 +216,34 @@ def test_image_textures_render(gpu_ctx):
     assert min(fr) >= MIN_MATCH, fr
 
 
+def test_non_finite_samples_dropped_and_counted(gpu_ctx):
+    """A material whose base colour is NaN (a Math node's power of -1 to 0.5):
+    its light and BSDF samples are dropped, as the reference drops them, the
+    film stays finite and the renderer counts them."""
+    pin, _ = _pin_modules()
+    sc = scenes.cornell(seed=1, envmap_exponent=4)
+    nan_mat = {
+        "Math": {"type": "MATH", "parameters": {"operation": "POWER", "use_clamp": False},
+                 "inputs": {"Value": {"type": "VALUE", "value": -1.0}, "Value_001": {"type": "VALUE", "value": 0.5},
+                            "Value_002": {"type": "VALUE", "value": 0.0}}},
+        "Principled BSDF": {"type": "BSDF_PRINCIPLED",
+                            "inputs": dict(pin.M.principled_inputs(),
+                                           **{"Base Color": {"type": "RGBA", "links": [["Math", "Value"]]}}),
+                            "parameters": {"distribution": "GGX", "subsurface_method": "RANDOM_WALK"}},
+        "Material Output": {"type": "OUTPUT_MATERIAL", "parameters": {},
+                            "inputs": {"Surface": {"type": "SHADER", "links": [["Principled BSDF", "BSDF"]]}}},
+    }
+    sc["materials"] = sc["materials"] + [("nan", nan_mat)]
+    sc["shapes"][0]["materials"] = np.full_like(sc["shapes"][0]["materials"], len(sc["materials"]) - 1)  # floor
+    r = api.Renderer(api.Scene(gpu_ctx, SceneDesc(sc)), 64, 64)
+    r.render(spp=4, max_depth=8)
+    assert np.all(np.isfinite(r.film()))
+    assert r.stats()["invalid_samples"] > 0
+    plain = api.Renderer(api.Scene(gpu_ctx, SceneDesc(scenes.cornell(seed=1, envmap_exponent=4))), 64, 64)
+    plain.render(spp=4, max_depth=8)
+    assert plain.stats()["invalid_samples"] == 0
+
+
 def _all_lights_scene():
     return scenes.cornell_all_lights(seed=4, envmap_exponent=7)
 
