@@ -401,8 +401,8 @@ def guided_leg(api, ctx, oracle_spp: int, size=(GUIDED_W, GUIDED_H)) -> dict:
         curve.append((spp, ms, e))
         if parity is None and e <= e_plain:
             parity = (spp, ms)
-            if ms >= plain_ms:
-                break
+        if parity is not None and ms >= plain_ms:  # both the parity time and the equal-time error are known
+            break
     # relMSE at the plain tracer's time (interpolated between chunks)
     e_eq = None
     for (s0, t0, e0), (s1, t1, e1) in zip(curve, curve[1:]):
