@@ -490,20 +490,24 @@ rmd_status rmd_batch_guide_stats(const rmd_batch *batch, rmd_guide_stats *out);
  * allocation, a real-time loop that must not pay allocation latency, a
  * process held to a fixed memory budget): renders like rmd_render but keeps
  * its path pool, queues and counters in one fixed device array compiled into
- * the library (RMD_NOALLOC_MAX_PATHS paths, about 8.1 MB, reserved on every
- * GPU that loads the library until it is unloaded) and never calls
- * cudaMalloc, cudaFree or any other allocating routine.
+ * the library (RMD_NOALLOC_MAX_PATHS paths, about 8.1 MB) and never calls
+ * cudaMalloc, cudaFree or any other allocating routine.  The array is
+ * reserved on a GPU when the first rmd_context for that GPU is created
+ * (rmd_context_create looks up its device address, which loads the module
+ * holding it) and stays reserved until the library is unloaded.
  *
  * film: caller-owned DEVICE memory of width * height float4 (RGB radiance
  * sums and a path count per pixel, row-major from the top-left pixel); the
  * call adds to it, so clear it first for a fresh image.  settings->first_sample
  * must be >= 0 and film_fp64 must be 0.  pool_size: paths in flight, 0 for
  * RMD_NOALLOC_MAX_PATHS; larger values are rejected with
- * RMD_ERROR_INVALID_ARGUMENT.  The first call on a device looks up the
- * array's device address; make that first call before any stream capture.
- * All calls share the array: calls whose GPU work overlaps (several streams or
- * threads) race and corrupt each other, so serialise them.  Runs on the
- * scene's stream and returns when the frame is finished.
+ * RMD_ERROR_INVALID_ARGUMENT.  All calls share the array, which keeps what
+ * the last call left in it (each call clears its counters and queues before
+ * use): calls whose GPU work overlaps (several streams or threads) race and
+ * corrupt each other, so serialise them.  The call is synchronous: it runs on
+ * the scene's stream and returns when the frame is finished.  A device reset
+ * invalidates every scene; a context created after it refreshes the array's
+ * address.
  */
 #define RMD_NOALLOC_MAX_PATHS 32768
 rmd_status rmd_render_noalloc(rmd_scene *scene, const rmd_camera *camera, uint32_t width, uint32_t height,

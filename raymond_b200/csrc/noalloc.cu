@@ -9,12 +9,16 @@
 // fixed size instead of memory owned by an rmd_renderer; the caller passes
 // the scene (created earlier) and its own device film.
 //
-// The array is defined in this file and reserved on every GPU that loads the
-// library, for as long as the library stays loaded.  Host code cannot use the
-// array's name as a device address: its address is fetched once per device
-// with cudaGetSymbolAddress and handed to the kernels.  All calls share the
-// array, so two calls whose work overlaps on the GPU (different streams,
-// other threads) corrupt each other.
+// The array is defined in this file.  Host code cannot use the array's name
+// as a device address: rmd_context_create looks the address up for its device
+// with cudaGetSymbolAddress (noallocSetup below) and this entry point hands it
+// to the kernels.  The lookup is what makes the CUDA runtime load this file's
+// module, and with it reserve the array on that GPU, so with lazy module
+// loading (the default since CUDA 12.2) the reservation happens when the
+// context is created, not in the middle of a render.  Every context created
+// refreshes the address, so contexts made after a device reset hand out the
+// array's new address.  All calls share the array, so two calls whose work
+// overlaps on the GPU (different streams, other threads) corrupt each other.
 #include <cuda_runtime.h>
 
 #include <cstring>
@@ -38,7 +42,7 @@ constexpr size_t kScratchBytes = kCountersBytes + pathPoolBytes(kMaxPaths);
 static __device__ __align__(256) unsigned char g_noallocScratch[kScratchBytes];
 
 std::mutex g_mutex;
-void *g_scratch[64] = {};  // device address of g_noallocScratch per device
+void *g_scratch[64] = {};  // device address of g_noallocScratch per device, set by noallocSetup
 
 rmd_status cudaFail(cudaError_t e, const char *what) {
     std::string msg = std::string("rmd_render_noalloc: ") + what + ": " + cudaGetErrorString(e);
@@ -46,6 +50,21 @@ rmd_status cudaFail(cudaError_t e, const char *what) {
 }
 
 }  // namespace
+
+namespace rmdhost {
+
+// Called by rmd_context_create with `device` current.
+rmd_status noallocSetup(int device) {
+    if (device < 0 || device >= 64) return RMD_OK;  // rmd_render_noalloc rejects such devices
+    void *ptr = nullptr;
+    const cudaError_t e = cudaGetSymbolAddress(&ptr, g_noallocScratch);
+    if (e != cudaSuccess) return cudaFail(e, "cudaGetSymbolAddress");
+    std::lock_guard<std::mutex> lock(g_mutex);
+    g_scratch[device] = ptr;
+    return RMD_OK;
+}
+
+}  // namespace rmdhost
 
 extern "C" rmd_status rmd_render_noalloc(rmd_scene *scene, const rmd_camera *camera, uint32_t width, uint32_t height,
                                          const rmd_render_settings *s, float *film, uint32_t pool_size) {
@@ -70,14 +89,9 @@ extern "C" rmd_status rmd_render_noalloc(rmd_scene *scene, const rmd_camera *cam
     void *base;
     {
         std::lock_guard<std::mutex> lock(g_mutex);
-        if (!g_scratch[v.device]) {  // first call on this device: resolve the array's device address
-            void *ptr = nullptr;
-            e = cudaGetSymbolAddress(&ptr, g_noallocScratch);
-            if (e != cudaSuccess) return cudaFail(e, "cudaGetSymbolAddress");
-            g_scratch[v.device] = ptr;
-        }
-        base = g_scratch[v.device];
+        base = g_scratch[v.device];  // set when the scene's context was created
     }
+    if (!base) return rmdhost::setLastError(RMD_ERROR_CUDA, "rmd_render_noalloc: scratch array not set up");
     const uint32_t P = pool_size ? pool_size : kMaxPaths;
     Counters *cnt = static_cast<Counters *>(base);
     const PathPool pool = carvePathPool(static_cast<unsigned char *>(base) + kCountersBytes, P);

@@ -351,6 +351,11 @@ rmd_status rmd_context_create(int32_t device, rmd_context **out) {
     RMD_CUDA(cudaSetDevice(device));
     RMD_CUDA(cudaDeviceGetAttribute(&c->smCount, cudaDevAttrMultiProcessorCount, device));
     RMD_CUDA(cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking));
+    const rmd_status ns = rmdhost::noallocSetup(device);
+    if (ns != RMD_OK) {
+        cudaStreamDestroy(c->stream);
+        return ns;
+    }
     *out = c.release();
     return RMD_OK;
 }

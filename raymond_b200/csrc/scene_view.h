@@ -23,5 +23,7 @@ struct SceneView {
 bool sceneView(const rmd_scene *scene, SceneView &out);
 // records `msg` as the calling thread's rmd_last_error and returns `status`
 rmd_status setLastError(rmd_status status, const char *msg);
+// looks up the device address of rmd_render_noalloc's scratch array on `device` (current)
+rmd_status noallocSetup(int device);
 
 }  // namespace rmdhost

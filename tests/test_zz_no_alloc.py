@@ -43,6 +43,36 @@ def test_noalloc_matches_regular_render(gpu_ctx):
         assert np.abs(got).sum() > 0
 
 
+def test_noalloc_small_pool_allocates_nothing(gpu_ctx):
+    """A pool of 1,024 paths carved from the array drains 32,768 paths in many
+    regeneration rounds and matches rmd_render; after a first call, a second
+    call leaves the device's free memory unchanged."""
+    import torch
+
+    W = H = 128
+    desc = SceneDesc(scenes.cornell(seed=1, envmap_exponent=6))
+    scene = api.Scene(gpu_ctx, desc)
+    regular = api.Renderer(scene, W, H)
+    regular.render(spp=2, max_depth=8, first_sample=0)
+    ref = regular.film().astype(np.float64)
+    films = [torch.zeros((H, W, 4), dtype=torch.float32, device="cuda") for _ in range(2)]
+    torch.cuda.synchronize()
+    api.render_noalloc(scene, desc.scene["camera"], W, H, films[0].data_ptr(), spp=2, first_sample=0,
+                       max_depth=8, pool_size=1024)
+    torch.cuda.synchronize()
+    free_before = torch.cuda.mem_get_info()[0]
+    api.render_noalloc(scene, desc.scene["camera"], W, H, films[1].data_ptr(), spp=2, first_sample=0,
+                       max_depth=8, pool_size=1024)
+    torch.cuda.synchronize()
+    assert torch.cuda.mem_get_info()[0] == free_before
+    for film in films:
+        f = film.cpu().numpy()
+        got = f[..., :3].astype(np.float64)
+        ok = np.abs(got - ref) <= REL * np.abs(ref) + ABS
+        assert ok.all(axis=-1).mean() >= MIN_MATCH
+        assert np.all(f[..., 3] == 2)  # every pixel received both of its paths
+
+
 def test_noalloc_rejects_oversized_pool(gpu_ctx):
     import torch
 
