@@ -32,6 +32,17 @@
 extern "C" {
 #endif
 
+/* Alignment of a struct member.  The host-facing records below keep the
+ * memory layout of the reference's DEVICE_STRUCTs (raymond/bridge/ *.hpp) as
+ * Swift and Metal see them: simd float3 takes 16 bytes with 16-byte
+ * alignment (its 4th float is padding), float2 8 with 8, float4x4 64 and
+ * float3x3 / float3x4 48 with 16, bool one byte. */
+#if defined(__cplusplus)
+#define RMD_ALIGN(n) alignas(n)
+#else
+#define RMD_ALIGN(n) _Alignas(n)
+#endif
+
 /* ------------------------------------------------------------------ status */
 
 typedef int32_t rmd_status;
@@ -155,57 +166,110 @@ typedef struct rmd_entity {
 } rmd_entity;
 
 /* --------------------------------------------------------------- lights */
-/* Field-for-field the device records of raymond/bridge/lights/ *.hpp, as
- * LightBuilder.build fills them (LightBuilder.swift:187-223): colours
- * already multiplied by power, spot angles already as cosines. */
+/* The device records of raymond/bridge/lights/ *.hpp, with their layout
+ * (sizes and field offsets as in Swift / Metal; checked by static_assert in
+ * the library and by a C test program), as LightBuilder.build fills them
+ * (LightBuilder.swift:187-223): colours already multiplied by power, spot
+ * angles already as cosines.  A float3 field is float[4]; its [3] is
+ * padding and ignored. */
 
-typedef struct rmd_light_info {             /* bridge/lights/LightInfo.hpp:5-9 */
+typedef struct rmd_light_info {             /* bridge/lights/LightInfo.hpp:5-9, 4 bytes */
     uint16_t shader_index;                  /* index into light_materials */
-    uint8_t casts_shadows;
-    uint8_t uses_mis;                       /* the reference forces 0 (LightBuilder.swift:45) */
+    uint8_t casts_shadows;                  /* bool */
+    uint8_t uses_mis;                       /* bool; the reference forces 0 (LightBuilder.swift:45) */
 } rmd_light_info;
 
-typedef struct rmd_area_light {             /* bridge/lights/AreaLight.hpp:6-16 */
-    rmd_light_info info;
-    float transform[12];                    /* float3x4: three float4 columns =
+typedef struct rmd_area_light {             /* bridge/lights/AreaLight.hpp:6-16, 96 bytes */
+    rmd_light_info info;                    /* offset 0 */
+    RMD_ALIGN(16) float transform[12];      /* offset 16: float3x4, three float4 columns =
                                                the first three rows of the world matrix */
-    float color[3];
-    uint32_t is_circular;
+    RMD_ALIGN(16) float color[4];           /* offset 64: float3 */
+    uint8_t is_circular;                    /* offset 80: bool */
 } rmd_area_light;
 
-typedef struct rmd_point_light {            /* bridge/lights/PointLight.hpp:6-16 */
-    rmd_light_info info;
-    float location[3];
-    float radius;
-    float color[3];
+typedef struct rmd_point_light {            /* bridge/lights/PointLight.hpp:6-16, 64 bytes */
+    rmd_light_info info;                    /* offset 0 */
+    RMD_ALIGN(16) float location[4];        /* offset 16: float3 */
+    float radius;                           /* offset 32 */
+    RMD_ALIGN(16) float color[4];           /* offset 48: float3 */
 } rmd_point_light;
 
-typedef struct rmd_sun_light {              /* bridge/lights/SunLight.hpp:6-16 */
-    rmd_light_info info;
-    float direction[3];
-    float cos_angle;
-    float color[3];
+typedef struct rmd_sun_light {              /* bridge/lights/SunLight.hpp:6-16, 64 bytes */
+    rmd_light_info info;                    /* offset 0 */
+    RMD_ALIGN(16) float direction[4];       /* offset 16: float3 */
+    float cos_angle;                        /* offset 32 */
+    RMD_ALIGN(16) float color[4];           /* offset 48: float3 */
 } rmd_sun_light;
 
-typedef struct rmd_spot_light {             /* bridge/lights/SpotLight.hpp:6-19 */
-    rmd_light_info info;
-    float location[3];
-    float direction[3];
-    float radius;
-    float color[3];
-    float spot_size;                        /* cos(size / 2) */
-    float spot_blend;                       /* (1 - spot_size) * blend */
+typedef struct rmd_spot_light {             /* bridge/lights/SpotLight.hpp:6-19, 96 bytes */
+    rmd_light_info info;                    /* offset 0 */
+    RMD_ALIGN(16) float location[4];        /* offset 16: float3 */
+    RMD_ALIGN(16) float direction[4];       /* offset 32: float3 */
+    float radius;                           /* offset 48 */
+    RMD_ALIGN(16) float color[4];           /* offset 64: float3 */
+    float spot_size;                        /* offset 80: cos(size / 2) */
+    float spot_blend;                       /* offset 84: (1 - spot_size) * blend */
 } rmd_spot_light;
 
 /* ---------------------------------------------------------------- camera */
 
-typedef struct rmd_camera {                 /* bridge/Camera.hpp:5-11 */
-    float transform[16];                    /* column-major camera-to-world */
-    float near_clip;
-    float far_clip;
-    float focal_length;                     /* lens_mm / (sensor_width / 2), SceneLoader.swift:135-136 */
-    float shift[2];
+typedef struct rmd_camera {                 /* bridge/Camera.hpp:5-11, 96 bytes */
+    RMD_ALIGN(16) float transform[16];      /* offset 0: float4x4, column-major camera-to-world */
+    float near_clip;                        /* offset 64 */
+    float far_clip;                         /* offset 68 */
+    float focal_length;                     /* offset 72: lens_mm / (sensor_width / 2), SceneLoader.swift:135-136 */
+    RMD_ALIGN(8) float shift[2];            /* offset 80: float2 */
 } rmd_camera;
+
+/* ------------------------------------------------------ instance records */
+
+/* bridge/PerInstanceData.hpp:6-20 (192 bytes): what EntityBuilder computes
+ * per entity (EntityBuilder.swift:66-146) and the device reads in
+ * ShadingContext::build.  rmd_scene_instance_data returns the library's
+ * records in this layout. */
+typedef struct rmd_per_instance_data {
+    uint32_t vertex_offset;                 /* offset 0: first vertex of the shape in the scene's vertex array */
+    uint32_t face_offset;                   /* offset 4: first face of the shape */
+    uint32_t light_face_offset;             /* offset 8: the shape light's face CDF (shape lights only) */
+    uint32_t light_face_count;              /* offset 12 */
+    uint32_t light_index;                   /* offset 16: its shape light among the scene's shape
+                                               lights (LightBuilder.swift:169-177), or 0xffffffff */
+    RMD_ALIGN(16) float bounds_min[4];      /* offset 32: float3, object space */
+    RMD_ALIGN(16) float bounds_size[4];     /* offset 48: float3 */
+    RMD_ALIGN(16) float point_transform[16]; /* offset 64: float4x4, column-major */
+    RMD_ALIGN(16) float normal_transform[12]; /* offset 128: float3x3, three float3 columns */
+    uint8_t visibility;                     /* offset 176: RayFlags (RMD_RAY_*) */
+} rmd_per_instance_data;
+
+/* --------------------------------------------------------------- uniforms */
+
+/* OutputChannel and RussianRoulette, raymond/bridge/Uniforms.hpp:17-26 */
+#define RMD_OUTPUT_IMAGE 0
+#define RMD_RR_NONE 0
+#define RMD_RR_THROUGHPUT 1
+
+/* bridge/Uniforms.hpp:29-47 (64 bytes): the per-frame settings the
+ * reference's host writes and its kernels read (Renderer.swift:331-349,
+ * 438-443).  rmd_render_frame and rmd_film_normalize take them. */
+typedef struct rmd_uniforms {
+    uint32_t num_lens_surfaces;             /* offset 0: must be 0 (pinhole camera) */
+    uint32_t frame_index;                   /* offset 4: frames accumulated before this one */
+    uint32_t random_seed;                   /* offset 8: PrngState seed of the frame (>= 1) */
+    uint8_t accumulate;                     /* offset 12: bool; 0 clears the film first */
+    uint8_t lens_spectral;                  /* offset 13: bool, lens only (ignored) */
+    float sensor_scale;                     /* offset 16: lens only (ignored) */
+    float camera_scale;                     /* offset 20: lens only (ignored) */
+    float focus;                            /* offset 24: lens only (ignored) */
+    float exposure;                         /* offset 28 */
+    int32_t stop_index;                     /* offset 32: lens only (ignored) */
+    float relative_stop;                    /* offset 36: lens only (ignored) */
+    int32_t num_aperture_blades;            /* offset 40: lens only (ignored) */
+    uint32_t sampling_mode;                 /* offset 44: RMD_SAMPLING_* */
+    uint32_t tonemapping;                   /* offset 48: RMD_TONEMAP_* */
+    uint32_t rr;                            /* offset 52: RMD_RR_* (the device code reads neither rr */
+    int32_t rr_depth;                       /* offset 56:  nor rr_depth; ignored) */
+    uint32_t output_channel;                /* offset 60: RMD_OUTPUT_IMAGE */
+} rmd_uniforms;
 
 /* ----------------------------------------------------------------- scene */
 
@@ -331,6 +395,12 @@ rmd_status rmd_context_set_bvh_builder(rmd_context *ctx, uint32_t builder);
  * is computed on the host on the first call).  No counterpart in the
  * reference, whose acceleration structures are opaque. */
 rmd_status rmd_scene_bvh_stats(rmd_scene *scene, rmd_bvh_stats *out);
+/* The per-instance records the library computed (EntityBuilder.build,
+ * EntityBuilder.swift:79-127), one per entity in entity order, in the
+ * bridge layout.  Writes min(capacity, entities) records; *count receives the
+ * number of entities. */
+rmd_status rmd_scene_instance_data(const rmd_scene *scene, rmd_per_instance_data *out, int32_t capacity,
+                                   int32_t *count);
 /* Number of triangles after instancing, and BVH nodes. */
 rmd_status rmd_scene_info(const rmd_scene *scene, uint64_t *triangles, uint64_t *bvh_nodes,
                           int32_t *num_lights_total);
@@ -351,6 +421,21 @@ rmd_status rmd_renderer_set_camera(rmd_renderer *r, const rmd_camera *camera);
  * Runs on the renderer's stream; returns when the work is enqueued and
  * finished (blocking), with device error flags checked. */
 rmd_status rmd_render(rmd_renderer *r, const rmd_render_settings *settings);
+
+/* One frame of Renderer.execute(in:) (Renderer.swift:480-696) driven by the
+ * reference's Uniforms: the reference's TEA generator seeded with
+ * uniforms->random_seed per ray (generate.metal:88-94), sampling mode
+ * uniforms->sampling_mode, `max_depth` shade passes (the reference hard-codes
+ * 8, Renderer.swift:290), and, when uniforms->accumulate is 0, the film
+ * cleared first (generate.metal:103-106).  The host advances frame_index and
+ * random_seed between frames as updateState does (Renderer.swift:438-443).
+ * Lens cameras (num_lens_surfaces > 0) are rejected. */
+rmd_status rmd_render_frame(rmd_renderer *r, const rmd_uniforms *uniforms, uint32_t max_depth);
+/* normalizeImage (kernels/utils/normalizeImage.metal:39-59) with the
+ * reference's Uniforms: per pixel exposure * film, divided by frame_index + 1
+ * when accumulate is set, then the Hable or ACES tonemap; W*H*4 floats
+ * (RGB and alpha 1), row-major from the top-left pixel. */
+rmd_status rmd_film_normalize(rmd_renderer *r, const rmd_uniforms *uniforms, float *rgba);
 
 /* Copy the film to host memory: W*H*3 floats, row-major from the top-left
  * pixel.  With normalize != 0 the normalizeImage kernel math is applied

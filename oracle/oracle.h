@@ -37,6 +37,11 @@ typedef struct oracle_settings {
     int64_t first_sample;   /* sample index of the first frame */
     int32_t threads;        /* 0 = all */
     int32_t film_fp64;      /* accumulate in double */
+    /* NULL: every pixel.  Otherwise trace only these pixels (y * width + x,
+     * each at most once); their paths keep the full image's PRNG streams and
+     * ray indices, and the other pixels of the film stay zero. */
+    const uint32_t *pixels;
+    uint64_t num_pixels;
 } oracle_settings;
 
 /* returns 0 or an RMD_ERROR_* code; err receives a message */
@@ -44,11 +49,19 @@ int oracle_scene_create(const rmd_scene_desc *desc, oracle_scene **out, char *er
 void oracle_scene_destroy(oracle_scene *s);
 /* per surface material: 1 if it emits; returns the number of materials */
 int oracle_surface_emissive(const oracle_scene *s, uint8_t *out);
+/* replace the scene's camera (the reference's Renderer.updateProjection) */
+int oracle_scene_set_camera(oracle_scene *s, const rmd_camera *camera);
 int oracle_scene_info(const oracle_scene *s, uint64_t *triangles, int32_t *num_lights_total, int32_t *num_shape_lights);
 
 /* Film sums (W*H*3, row-major from the top-left pixel) of `spp` frames;
  * stats[0..2] = paths, segments (closest-hit rays shaded), shadow rays. */
 int oracle_render(oracle_scene *s, const oracle_settings *st, double *film_rgb, uint64_t *stats);
+
+/* normalizeImage (kernels/utils/normalizeImage.metal:11-59): per pixel of a
+ * W*H float4 film, exposure * rgb, divided by frame_index + 1 when
+ * accumulating, then the Hable or ACES tonemap; out W*H float4 with alpha 1. */
+void oracle_normalize_image(const float *film, uint32_t width, uint32_t height, float exposure, int32_t accumulate,
+                            uint32_t frame_index, uint32_t tonemapping, float *out);
 
 /* Unit hooks. */
 /* n values of PrngState.sample() for the stream (a, b): TEA(a, b) or PCG32(seed=a, seq=b). */

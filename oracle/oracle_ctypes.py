@@ -19,7 +19,8 @@ LIB = HERE / "_build" / "liboracle.so"
 class OracleSettings(C.Structure):
     _fields_ = [("width", C.c_uint32), ("height", C.c_uint32), ("spp", C.c_uint32), ("max_depth", C.c_uint32),
                 ("sampling_mode", C.c_uint32), ("rng", C.c_uint32), ("seed", C.c_uint64),
-                ("first_sample", C.c_int64), ("threads", C.c_int32), ("film_fp64", C.c_int32)]
+                ("first_sample", C.c_int64), ("threads", C.c_int32), ("film_fp64", C.c_int32),
+                ("pixels", C.POINTER(C.c_uint32)), ("num_pixels", C.c_uint64)]
 
 
 def build() -> Path:
@@ -51,6 +52,9 @@ def lib():
                                             C.POINTER(C.c_float)]
         L.oracle_material_eval.argtypes = [C.c_void_p, C.c_int32, C.POINTER(C.c_float), C.c_int32,
                                            C.POINTER(C.c_float)]
+        L.oracle_scene_set_camera.argtypes = [C.c_void_p, C.c_void_p]
+        L.oracle_normalize_image.argtypes = [C.POINTER(C.c_float), C.c_uint32, C.c_uint32, C.c_float, C.c_int32,
+                                             C.c_uint32, C.c_uint32, C.POINTER(C.c_float)]
         _lib = L
     return _lib
 
@@ -80,6 +84,14 @@ class OracleScene:
         lib().oracle_surface_emissive(self.h, out.ctypes.data_as(C.POINTER(C.c_uint8)))
         return out
 
+    def set_camera(self, camera: dict) -> None:
+        """Replace the camera (a camera dict as in the scene descriptions)."""
+        from raymond_b200._abi import make_camera
+
+        cam = make_camera(camera)
+        if lib().oracle_scene_set_camera(self.h, C.byref(cam)) != 0:
+            raise RuntimeError("oracle_scene_set_camera failed")
+
     def info(self):
         t = C.c_uint64()
         n = C.c_int32()
@@ -88,10 +100,16 @@ class OracleScene:
         return {"triangles": t.value, "lights": n.value, "shape_lights": s.value}
 
     def render(self, width, height, spp, max_depth, sampling_mode=2, rng=0, seed=1, first_sample=0, threads=0,
-               film_fp64=False):
-        """Film sums (H, W, 3) float64 and stats (paths, segments, shadow rays)."""
+               film_fp64=False, pixels=None):
+        """Film sums (H, W, 3) float64 and stats (paths, segments, shadow rays).
+        `pixels`: trace only these linear pixel indices (y * width + x), with
+        the full image's PRNG streams; the rest of the film stays zero."""
         st = OracleSettings(width, height, spp, max_depth, sampling_mode, rng, seed, first_sample, threads,
                             int(film_fp64))
+        if pixels is not None:
+            pixels = np.ascontiguousarray(pixels, np.uint32)
+            st.pixels = pixels.ctypes.data_as(C.POINTER(C.c_uint32))
+            st.num_pixels = len(pixels)
         film = np.zeros((height, width, 3), np.float64)
         stats = (C.c_uint64 * 3)()
         r = lib().oracle_render(self.h, C.byref(st), film.ctypes.data_as(C.POINTER(C.c_double)), stats)
@@ -117,6 +135,19 @@ class OracleScene:
         if r != 0:
             raise RuntimeError(f"oracle_material_eval failed ({r})")
         return out
+
+
+def normalize_image(film: np.ndarray, exposure: float, accumulate: bool, frame_index: int,
+                    tonemapping: int) -> np.ndarray:
+    """normalizeImage restated: (h, w, 3 or 4) film sums -> (h, w, 4) float32."""
+    film = np.asarray(film, np.float32)
+    h, w = film.shape[:2]
+    rgba = np.zeros((h, w, 4), np.float32)
+    rgba[..., :3] = film[..., :3]
+    out = np.zeros((h, w, 4), np.float32)
+    lib().oracle_normalize_image(rgba.ctypes.data_as(C.POINTER(C.c_float)), w, h, exposure, int(accumulate),
+                                 frame_index, tonemapping, out.ctypes.data_as(C.POINTER(C.c_float)))
+    return out
 
 
 def prng(mode: int, a: int, b: int, n: int) -> np.ndarray:

@@ -32,6 +32,8 @@ def lib():
         L.ref_scene_destroy.argtypes = [C.c_void_p]
         L.ref_render.argtypes = [C.c_void_p] + [C.c_uint32] * 6 + [_fp]
         L.ref_render.restype = C.c_int
+        L.ref_normalize_image.argtypes = [_fp, C.c_uint32, C.c_uint32, C.c_float] + [C.c_uint32] * 3 + [_fp]
+        L.ref_normalize_image.restype = C.c_int
         _lib = L
     return _lib
 
@@ -133,3 +135,14 @@ class RefScene:
         film = np.zeros((height, width, 4), np.float32)
         lib().ref_render(self.h, width, height, frames, max_depth, sampling_mode, first_frame, film.ctypes.data_as(_fp))
         return film
+
+
+def normalize_image(film: np.ndarray, exposure: float, accumulate: bool, frame_index: int,
+                    tonemapping: int) -> np.ndarray:
+    """The reference's normalizeImage kernel over a (h, w, 4) float32 film: (h, w, 4)."""
+    film = np.ascontiguousarray(film, np.float32)
+    h, w = film.shape[:2]
+    out = np.zeros((h, w, 4), np.float32)
+    lib().ref_normalize_image(film.ctypes.data_as(_fp), w, h, exposure, int(accumulate), frame_index, tonemapping,
+                              out.ctypes.data_as(_fp))
+    return out

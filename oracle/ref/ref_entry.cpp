@@ -34,6 +34,7 @@ using namespace metal;
 #include <device/kernels/envmap/build.metal>
 #include <device/kernels/envmap/reduce.metal>
 #include <device/kernels/envmap/normalize.metal>
+#include <device/kernels/utils/normalizeImage.metal>
 
 #include <memory>
 #include <string>
@@ -511,6 +512,28 @@ int ref_render(void *scene, uint32_t W, uint32_t H, uint32_t frames, uint32_t ma
             std::swap(cur, next);
         }
     }
+    return 0;
+}
+
+// normalizeImage (kernels/utils/normalizeImage.metal:39-59) over a W*H float4
+// film with the given Uniforms fields; out: W*H float4.
+int ref_normalize_image(const float *film, uint32_t W, uint32_t H, float exposure, uint32_t accumulate,
+                        uint32_t frameIndex, uint32_t tonemapping, float *out) {
+    texture2d<float, access::read> input;
+    input.data = reinterpret_cast<float4 *>(const_cast<float *>(film));
+    input.width = W;
+    input.height = H;
+    texture2d<float, access::write> output;
+    output.data = reinterpret_cast<float4 *>(out);
+    output.width = W;
+    output.height = H;
+    Uniforms uniforms{};
+    uniforms.exposure = exposure;
+    uniforms.accumulate = accumulate != 0;
+    uniforms.frameIndex = frameIndex;
+    uniforms.tonemapping = Tonemapping(tonemapping);
+    for (uint32_t y = 0; y < H; y++)
+        for (uint32_t x = 0; x < W; x++) normalizeImage(uniforms, input, output, uint2(x, y));
     return 0;
 }
 

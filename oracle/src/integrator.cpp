@@ -131,7 +131,7 @@ struct Frame {
     std::atomic<uint64_t> segments{0}, shadows{0};
 
     Frame(const SceneData &c, const oracle_settings &s, Film<FilmT> &f) : ctx(c), st(s), film(f) {
-        size_t n = (size_t)s.width * s.height;
+        size_t n = s.pixels ? (size_t)s.num_pixels : (size_t)s.width * s.height;
         rays[0].resize(n);
         rays[1].resize(n);
         shadowRays.resize(n);
@@ -151,7 +151,8 @@ struct Frame {
     }
 
     // generate.metal:72-121 (pinhole branch) + :165-191 (fused trace)
-    void generate(uint32_t x, uint32_t y, uint64_t sampleIndex) {
+    // `slot`: position in the ray arrays (the ray index when every pixel is traced)
+    void generate(uint32_t x, uint32_t y, uint64_t sampleIndex, uint32_t slot) {
         const uint32_t W = st.width, H = st.height;
         const uint32_t rayIndex = blockLinearIndex(x, y, W, H);
         Ray ray;
@@ -170,8 +171,8 @@ struct Frame {
         ray.origin = (ctx.cameraTransform * float4(0, 0, 0, 1.f)).xyz();
         ray.direction = normalize((ctx.cameraTransform * float4(uv.x, uv.y * aspect, -ctx.focalLength, 0)).xyz());
         ray.weight = float3(1.0f);
-        rays[0][rayIndex] = ray;
-        trace(ray, intersections[rayIndex]);
+        rays[0][slot] = ray;
+        trace(ray, intersections[slot]);
     }
 
     // intersection.metal:22-211
@@ -279,10 +280,19 @@ struct Frame {
     // Renderer.swift:480-696, one frame
     void run(uint64_t sampleIndex) {
         const uint32_t W = st.width, H = st.height;
+        uint32_t count;
+        if (st.pixels) {
+#pragma omp parallel for schedule(dynamic, 256)
+            for (int64_t i = 0; i < (int64_t)st.num_pixels; i++)
+                generate(st.pixels[i] % W, st.pixels[i] / W, sampleIndex, (uint32_t)i);
+            count = (uint32_t)st.num_pixels;
+        } else {
 #pragma omp parallel for schedule(dynamic, 4)
-        for (int y = 0; y < (int)H; y++)
-            for (uint32_t x = 0; x < W; x++) generate(x, (uint32_t)y, sampleIndex);
-        uint32_t count = W * H;
+            for (int y = 0; y < (int)H; y++)
+                for (uint32_t x = 0; x < W; x++)
+                    generate(x, (uint32_t)y, sampleIndex, blockLinearIndex(x, (uint32_t)y, W, H));
+            count = W * H;
+        }
         int cur = 0;
         for (uint32_t depth = 0; depth < st.max_depth; depth++) {
             const bool isMaxDepth = depth + 1 == st.max_depth;
@@ -539,6 +549,17 @@ extern "C" int oracle_surface_emissive(const oracle_scene *s, uint8_t *out) {
     return (int)s->data.surfaceShaders.size();
 }
 
+// Renderer.updateProjection / scene.camera (Renderer.swift:749-755)
+extern "C" int oracle_scene_set_camera(oracle_scene *s, const rmd_camera *c) {
+    if (!s || !c) return RMD_ERROR_INVALID_ARGUMENT;
+    s->data.cameraTransform = toMatrix(c->transform);
+    s->data.nearClip = c->near_clip;
+    s->data.farClip = c->far_clip;
+    s->data.focalLength = c->focal_length;
+    s->data.shift = float2(c->shift[0], c->shift[1]);
+    return 0;
+}
+
 extern "C" int oracle_scene_info(const oracle_scene *s, uint64_t *triangles, int32_t *num_lights_total,
                                  int32_t *num_shape_lights) {
     if (triangles) *triangles = s->triangles;
@@ -563,7 +584,7 @@ static void renderFrames(oracle_scene *s, const oracle_settings *st, double *fil
     for (size_t p = 0; p < (size_t)st->width * st->height; p++)
         for (int c = 0; c < 3; c++) film_rgb[3 * p + c] = (double)film.rgba[4 * p + c];
     if (stats) {
-        stats[0] = (uint64_t)st->spp * st->width * st->height;
+        stats[0] = (uint64_t)st->spp * (st->pixels ? st->num_pixels : (uint64_t)st->width * st->height);
         stats[1] = segs;
         stats[2] = shadows;
     }
@@ -573,12 +594,53 @@ extern "C" int oracle_render(oracle_scene *s, const oracle_settings *st, double 
     if (!s || !st || !film_rgb || st->width == 0 || st->height == 0 || st->width > 65535 || st->height > 65535 ||
         st->max_depth == 0)
         return RMD_ERROR_INVALID_ARGUMENT;
+    if (st->pixels) {  // each pixel once, inside the image
+        std::vector<uint8_t> seen((size_t)st->width * st->height, 0);
+        for (uint64_t i = 0; i < st->num_pixels; i++) {
+            const uint32_t p = st->pixels[i];
+            if (p >= seen.size() || seen[p]) return RMD_ERROR_INVALID_ARGUMENT;
+            seen[p] = 1;
+        }
+    }
 #ifdef _OPENMP
     if (st->threads > 0) omp_set_num_threads(st->threads);
 #endif
     if (st->film_fp64) renderFrames<double>(s, st, film_rgb, stats);
     else renderFrames<float>(s, st, film_rgb, stats);
     return 0;
+}
+
+// ------------------------------------------------------------- film read-out
+// normalizeImage.metal:11-19, the Hable filmic curve with its six constants
+static float3 tonemapHablePartial(float3 x) {
+    const float hA = 0.15f, hB = 0.50f, hC = 0.10f, hD = 0.20f, hE = 0.02f, hF = 0.30f;
+    return ((x * (hA * x + float3(hC * hB)) + float3(hD * hE)) / (x * (hA * x + float3(hB)) + float3(hD * hF))) -
+           float3(hE / hF);
+}
+
+extern "C" void oracle_normalize_image(const float *film, uint32_t width, uint32_t height, float exposure,
+                                       int32_t accumulate, uint32_t frame_index, uint32_t tonemapping, float *out) {
+    const size_t n = (size_t)width * height;
+    for (size_t i = 0; i < n; i++) {
+        // normalizeImage.metal:45-46
+        float3 c = exposure * float3(film[4 * i], film[4 * i + 1], film[4 * i + 2]);
+        if (accumulate) c = c / float3((float)(frame_index + 1));
+        if (tonemapping == RMD_TONEMAP_HABLE) {  // :21-28, exposure bias 2 and white point 11.2
+            const float3 curr = tonemapHablePartial(c * 2.0f);
+            const float3 whiteScale = float3(1.0f) / tonemapHablePartial(float3(11.2f));
+            c = curr * whiteScale;
+        } else if (tonemapping == RMD_TONEMAP_ACES) {  // :30-37, Narkowicz's fit
+            const float tA = 2.51f, tB = 0.03f, tC = 2.43f, tD = 0.59f, tE = 0.14f;
+            c = (c * (tA * c + float3(tB))) / (c * (tC * c + float3(tD)) + float3(tE));
+            // saturate: fmax/fmin semantics, so an overflow's NaN becomes 0
+            c = float3(std::fmin(std::fmax(c.x, 0.0f), 1.0f), std::fmin(std::fmax(c.y, 0.0f), 1.0f),
+                       std::fmin(std::fmax(c.z, 0.0f), 1.0f));
+        }
+        out[4 * i] = c.x;
+        out[4 * i + 1] = c.y;
+        out[4 * i + 2] = c.z;
+        out[4 * i + 3] = 1.0f;
+    }
 }
 
 // ---------------------------------------------------------------- unit hooks

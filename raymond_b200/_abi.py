@@ -30,6 +30,28 @@ RNG_PCG32, RNG_TEA = 0, 1
 PARAM_STRING, PARAM_NUMBER, PARAM_BOOL, PARAM_NUMBERS = 0, 1, 2, 3
 
 
+def _layout(fields):
+    """ctypes fields laid out as C lays out the header's structs, including
+    members declared RMD_ALIGN(n): entries are (name, type) or (name, type,
+    alignment).  Padding fields (_padN) are inserted where C pads, so nested
+    records and arrays of them have the C offsets and sizes.  Returns the
+    fields and the struct's alignment."""
+    out, off, align, npad = [], 0, 1, 0
+    for f in fields:
+        name, typ = f[0], f[1]
+        a = max(f[2] if len(f) > 2 else 1, getattr(typ, "_rmd_align_", C.alignment(typ)))
+        if off % a:
+            out.append((f"_pad{npad}", C.c_uint8 * (a - off % a)))
+            npad += 1
+            off += a - off % a
+        out.append((name, typ))
+        off += C.sizeof(typ)
+        align = max(align, a)
+    if off % align:
+        out.append((f"_pad{npad}", C.c_uint8 * (align - off % align)))
+    return out, align
+
+
 class NodeParam(C.Structure):
     _fields_ = [("key", C.c_char_p), ("kind", C.c_int32), ("string_value", C.c_char_p),
                 ("number_value", C.c_double), ("numbers", C.POINTER(C.c_float)), ("num_numbers", C.c_int32)]
@@ -65,33 +87,70 @@ class LightInfo(C.Structure):
     _fields_ = [("shader_index", C.c_uint16), ("casts_shadows", C.c_uint8), ("uses_mis", C.c_uint8)]
 
 
-class AreaLight(C.Structure):
-    _fields_ = [("info", LightInfo), ("transform", C.c_float * 12), ("color", C.c_float * 3),
-                ("is_circular", C.c_uint32)]
+class AreaLight(C.Structure):  # bridge/lights/AreaLight.hpp, 96 bytes
+    _fields_, _rmd_align_ = _layout([("info", LightInfo), ("transform", C.c_float * 12, 16),
+                                     ("color", C.c_float * 4, 16), ("is_circular", C.c_uint8)])
 
 
-class PointLight(C.Structure):
-    _fields_ = [("info", LightInfo), ("location", C.c_float * 3), ("radius", C.c_float), ("color", C.c_float * 3)]
+class PointLight(C.Structure):  # bridge/lights/PointLight.hpp, 64 bytes
+    _fields_, _rmd_align_ = _layout([("info", LightInfo), ("location", C.c_float * 4, 16), ("radius", C.c_float),
+                                     ("color", C.c_float * 4, 16)])
 
 
-class SunLight(C.Structure):
-    _fields_ = [("info", LightInfo), ("direction", C.c_float * 3), ("cos_angle", C.c_float),
-                ("color", C.c_float * 3)]
+class SunLight(C.Structure):  # bridge/lights/SunLight.hpp, 64 bytes
+    _fields_, _rmd_align_ = _layout([("info", LightInfo), ("direction", C.c_float * 4, 16),
+                                     ("cos_angle", C.c_float), ("color", C.c_float * 4, 16)])
 
 
-class SpotLight(C.Structure):
-    _fields_ = [("info", LightInfo), ("location", C.c_float * 3), ("direction", C.c_float * 3),
-                ("radius", C.c_float), ("color", C.c_float * 3), ("spot_size", C.c_float),
-                ("spot_blend", C.c_float)]
+class SpotLight(C.Structure):  # bridge/lights/SpotLight.hpp, 96 bytes
+    _fields_, _rmd_align_ = _layout([("info", LightInfo), ("location", C.c_float * 4, 16),
+                                     ("direction", C.c_float * 4, 16), ("radius", C.c_float),
+                                     ("color", C.c_float * 4, 16), ("spot_size", C.c_float),
+                                     ("spot_blend", C.c_float)])
 
 
-class Camera(C.Structure):
-    _fields_ = [("transform", C.c_float * 16), ("near_clip", C.c_float), ("far_clip", C.c_float),
-                ("focal_length", C.c_float), ("shift", C.c_float * 2)]
+class Camera(C.Structure):  # bridge/Camera.hpp, 96 bytes
+    _fields_, _rmd_align_ = _layout([("transform", C.c_float * 16, 16), ("near_clip", C.c_float),
+                                     ("far_clip", C.c_float), ("focal_length", C.c_float),
+                                     ("shift", C.c_float * 2, 8)])
+
+
+class PerInstanceData(C.Structure):  # bridge/PerInstanceData.hpp, 192 bytes
+    _fields_, _rmd_align_ = _layout([("vertex_offset", C.c_uint32), ("face_offset", C.c_uint32),
+                                     ("light_face_offset", C.c_uint32), ("light_face_count", C.c_uint32),
+                                     ("light_index", C.c_uint32), ("bounds_min", C.c_float * 4, 16),
+                                     ("bounds_size", C.c_float * 4, 16), ("point_transform", C.c_float * 16, 16),
+                                     ("normal_transform", C.c_float * 12, 16), ("visibility", C.c_uint8)])
+
+
+OUTPUT_IMAGE, RR_NONE, RR_THROUGHPUT = 0, 0, 1
+
+
+class Uniforms(C.Structure):  # bridge/Uniforms.hpp, 64 bytes
+    _fields_, _rmd_align_ = _layout([("num_lens_surfaces", C.c_uint32), ("frame_index", C.c_uint32),
+                                     ("random_seed", C.c_uint32), ("accumulate", C.c_uint8),
+                                     ("lens_spectral", C.c_uint8), ("sensor_scale", C.c_float),
+                                     ("camera_scale", C.c_float), ("focus", C.c_float), ("exposure", C.c_float),
+                                     ("stop_index", C.c_int32), ("relative_stop", C.c_float),
+                                     ("num_aperture_blades", C.c_int32), ("sampling_mode", C.c_uint32),
+                                     ("tonemapping", C.c_uint32), ("rr", C.c_uint32), ("rr_depth", C.c_int32),
+                                     ("output_channel", C.c_uint32)])
+
+
+def default_uniforms(**kw) -> Uniforms:
+    """The reference's initial Uniforms (Renderer.swift:331-349), with `kw` overrides."""
+    u = Uniforms(num_lens_surfaces=0, frame_index=0, random_seed=1, accumulate=1, lens_spectral=1,
+                 sensor_scale=1.0, camera_scale=0.001, focus=0.0, exposure=1.0, stop_index=0, relative_stop=1.0,
+                 num_aperture_blades=7, sampling_mode=SAMPLING_MIS, tonemapping=TONEMAP_LINEAR, rr=RR_THROUGHPUT,
+                 rr_depth=0, output_channel=OUTPUT_IMAGE)
+    for k, v in kw.items():
+        setattr(u, k, v)
+    return u
 
 
 class BatchView(C.Structure):
-    _fields_ = [("scene", C.c_int32), ("width", C.c_uint32), ("height", C.c_uint32), ("camera", Camera)]
+    _fields_, _rmd_align_ = _layout([("scene", C.c_int32), ("width", C.c_uint32), ("height", C.c_uint32),
+                                     ("camera", Camera)])
 
 
 BATCH_NO_GRAPH = 1
@@ -106,16 +165,17 @@ class Texture(C.Structure):
 
 
 class SceneDescC(C.Structure):
-    _fields_ = [("num_surface_materials", C.c_int32), ("surface_materials", C.POINTER(Material)),
-                ("num_light_materials", C.c_int32), ("light_materials", C.POINTER(Material)),
-                ("num_shapes", C.c_int32), ("shapes", C.POINTER(Shape)),
-                ("num_entities", C.c_int32), ("entities", C.POINTER(Entity)),
-                ("world_shader", C.c_uint16), ("envmap_exponent", C.c_int32),
-                ("num_area_lights", C.c_int32), ("area_lights", C.POINTER(AreaLight)),
-                ("num_point_lights", C.c_int32), ("point_lights", C.POINTER(PointLight)),
-                ("num_sun_lights", C.c_int32), ("sun_lights", C.POINTER(SunLight)),
-                ("num_spot_lights", C.c_int32), ("spot_lights", C.POINTER(SpotLight)),
-                ("camera", Camera), ("num_textures", C.c_int32), ("textures", C.POINTER(Texture))]
+    _fields_, _rmd_align_ = _layout([
+        ("num_surface_materials", C.c_int32), ("surface_materials", C.POINTER(Material)),
+        ("num_light_materials", C.c_int32), ("light_materials", C.POINTER(Material)),
+        ("num_shapes", C.c_int32), ("shapes", C.POINTER(Shape)),
+        ("num_entities", C.c_int32), ("entities", C.POINTER(Entity)),
+        ("world_shader", C.c_uint16), ("envmap_exponent", C.c_int32),
+        ("num_area_lights", C.c_int32), ("area_lights", C.POINTER(AreaLight)),
+        ("num_point_lights", C.c_int32), ("point_lights", C.POINTER(PointLight)),
+        ("num_sun_lights", C.c_int32), ("sun_lights", C.POINTER(SunLight)),
+        ("num_spot_lights", C.c_int32), ("spot_lights", C.POINTER(SpotLight)),
+        ("camera", Camera), ("num_textures", C.c_int32), ("textures", C.POINTER(Texture))])
 
 
 class RenderSettings(C.Structure):
@@ -226,35 +286,35 @@ class SceneDesc:
             a = AreaLight()
             a.info = info(l)
             a.transform[:] = np.asarray(l["transform"], np.float32).reshape(3, 4).reshape(-1).tolist()
-            a.color[:] = list(l["color"])
+            a.color[:3] = list(l["color"])
             a.is_circular = int(l.get("is_circular", False))
             areas.append(a)
         points = []
         for l in scene.get("point_lights", []):
             p = PointLight()
             p.info = info(l)
-            p.location[:] = list(l["location"])
+            p.location[:3] = list(l["location"])
             p.radius = l.get("radius", 0.0)
-            p.color[:] = list(l["color"])
+            p.color[:3] = list(l["color"])
             points.append(p)
         suns = []
         for l in scene.get("sun_lights", []):
             s = SunLight()
             s.info = info(l)
             dvec = np.asarray(l["direction"], np.float64)
-            s.direction[:] = (dvec / np.linalg.norm(dvec)).tolist()
+            s.direction[:3] = (dvec / np.linalg.norm(dvec)).tolist()
             s.cos_angle = float(np.cos(l.get("angle", 0.0) / 2))
-            s.color[:] = list(l["color"])
+            s.color[:3] = list(l["color"])
             suns.append(s)
         spots = []
         for l in scene.get("spot_lights", []):
             s = SpotLight()
             s.info = info(l)
-            s.location[:] = list(l["location"])
+            s.location[:3] = list(l["location"])
             dvec = np.asarray(l["direction"], np.float64)
-            s.direction[:] = (dvec / np.linalg.norm(dvec)).tolist()
+            s.direction[:3] = (dvec / np.linalg.norm(dvec)).tolist()
             s.radius = l.get("radius", 0.0)
-            s.color[:] = list(l["color"])
+            s.color[:3] = list(l["color"])
             ang = float(np.cos(l["spot_size"] / 2))
             s.spot_size = ang
             s.spot_blend = (1 - ang) * l.get("spot_blend", 0.0)

@@ -32,7 +32,8 @@ EXPORTS = [
     "rmd_renderer_guide_params", "rmd_batch_create", "rmd_batch_destroy", "rmd_batch_reset", "rmd_batch_render",
     "rmd_batch_film_read", "rmd_batch_film_read_f64", "rmd_batch_stats", "rmd_batch_autotune",
     "rmd_batch_set_guide", "rmd_batch_guide_stats", "rmd_context_set_bvh_builder", "rmd_scene_bvh_stats",
-    "rmd_film_save_exr", "rmd_batch_film_save_exr",
+    "rmd_film_save_exr", "rmd_batch_film_save_exr", "rmd_scene_instance_data", "rmd_render_frame",
+    "rmd_film_normalize",
     "rmd_test_prng", "rmd_test_trace", "rmd_test_material_eval", "rmd_test_generate_source", "rmd_test_jit_compile",
     "rmd_test_guide_forward", "rmd_test_guide_gradient", "rmd_test_guide_mixture", "rmd_test_bvh_read",
     "rmd_test_exr_write",
@@ -72,6 +73,9 @@ def lib() -> C.CDLL:
         "rmd_scene_create": ([vp, P(_abi.SceneDescC), P(vp)], C.c_int32),
         "rmd_scene_destroy": ([vp], None),
         "rmd_scene_info": ([vp, P(C.c_uint64), P(C.c_uint64), P(C.c_int32)], C.c_int32),
+        "rmd_scene_instance_data": ([vp, P(_abi.PerInstanceData), C.c_int32, P(C.c_int32)], C.c_int32),
+        "rmd_render_frame": ([vp, P(_abi.Uniforms), C.c_uint32], C.c_int32),
+        "rmd_film_normalize": ([vp, P(_abi.Uniforms), P(C.c_float)], C.c_int32),
         "rmd_renderer_create": ([vp, C.c_uint32, C.c_uint32, C.c_uint32, P(vp)], C.c_int32),
         "rmd_renderer_destroy": ([vp], None),
         "rmd_renderer_set_size": ([vp, C.c_uint32, C.c_uint32], C.c_int32),
@@ -188,6 +192,14 @@ class Scene:
                                       tris.shape[0]))
         return nodes[:info["bvh_nodes"]], tris[:info["triangles"]]
 
+    def instance_data(self) -> list[_abi.PerInstanceData]:
+        """The per-instance records (bridge/PerInstanceData.hpp layout), one per entity."""
+        n = C.c_int32()
+        check(lib().rmd_scene_instance_data(self.h, None, 0, C.byref(n)))
+        arr = (_abi.PerInstanceData * max(1, n.value))()
+        check(lib().rmd_scene_instance_data(self.h, arr, n.value, C.byref(n)))
+        return list(arr)[:n.value]
+
     def trace(self, rays: np.ndarray, any_hit: bool = False):
         rays = np.ascontiguousarray(rays, np.float32)
         n = len(rays)
@@ -232,6 +244,16 @@ class Renderer:
     def film(self, normalize: bool = False, tonemapping: int = _abi.TONEMAP_LINEAR, exposure: float = 1.0) -> np.ndarray:
         out = np.zeros((self.height, self.width, 3), np.float32)
         check(lib().rmd_film_read(self.h, _f32p(out), int(normalize), tonemapping, exposure))
+        return out
+
+    def render_frame(self, uniforms: _abi.Uniforms, max_depth: int = 8) -> None:
+        """One frame of the reference's Renderer.execute driven by its Uniforms (rmd_render_frame)."""
+        check(lib().rmd_render_frame(self.h, C.byref(uniforms), max_depth))
+
+    def film_normalize(self, uniforms: _abi.Uniforms) -> np.ndarray:
+        """normalizeImage with the reference's Uniforms (rmd_film_normalize): (H, W, 4) float32."""
+        out = np.zeros((self.height, self.width, 4), np.float32)
+        check(lib().rmd_film_normalize(self.h, C.byref(uniforms), out.ctypes.data_as(C.POINTER(C.c_float))))
         return out
 
     def film64(self) -> np.ndarray:

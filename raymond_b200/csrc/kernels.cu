@@ -307,14 +307,18 @@ __device__ float3 tonemapHablePartial(float3 x) {
     const float hA = 0.15f, hB = 0.50f, hC = 0.10f, hD = 0.20f, hE = 0.02f, hF = 0.30f;
     return ((x * (hA * x + hC * hB) + hD * hE) / (x * (hA * x + hB) + hD * hF)) - hE / hF;
 }
+// color = exposure * film; color /= divisor (the frame count, 1 when not
+// accumulating), then the tonemap, in the reference's order of operations;
+// `channels` 3 (RGB) or 4 (RGB and alpha 1, as normalizeImage writes).
 __global__ void k_film_resolve(const float4 *film, const double *film64, int fp64, float *out, uint32_t numPixels,
-                               float scale, uint32_t tonemapping) {
+                               float exposure, float divisor, uint32_t tonemapping, uint32_t channels) {
     const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= numPixels) return;
     float3 c;
     if (fp64) c = make_float3((float)film64[3 * (size_t)i], (float)film64[3 * (size_t)i + 1], (float)film64[3 * (size_t)i + 2]);
     else c = xyz(film[i]);
-    c = c * scale;
+    c = exposure * c;
+    if (divisor != 1.0f) c = make_float3(__fdiv_rn(c.x, divisor), __fdiv_rn(c.y, divisor), __fdiv_rn(c.z, divisor));
     if (tonemapping == 1u) {
         const float3 curr = tonemapHablePartial(c * 2.0f);
         const float3 whiteScale = 1.0f / tonemapHablePartial(f3(11.2f));
@@ -323,9 +327,11 @@ __global__ void k_film_resolve(const float4 *film, const double *film64, int fp6
         const float tA = 2.51f, tB = 0.03f, tC = 2.43f, tD = 0.59f, tE = 0.14f;
         c = saturate((c * (tA * c + tB)) / (c * (tC * c + tD) + tE));
     }
-    out[3 * (size_t)i + 0] = c.x;
-    out[3 * (size_t)i + 1] = c.y;
-    out[3 * (size_t)i + 2] = c.z;
+    float *o = out + (size_t)channels * i;
+    o[0] = c.x;
+    o[1] = c.y;
+    o[2] = c.z;
+    if (channels == 4) o[3] = 1.0f;
 }
 
 // ------------------------------------------------------------- test hooks
@@ -398,8 +404,9 @@ cudaError_t rmdLaunchEnvmapNormalize(const float *sum, float *pdfs, uint32_t gri
     return cudaGetLastError();
 }
 cudaError_t rmdLaunchFilmResolve(const float4 *film, const double *film64, int fp64, float *out, uint32_t numPixels,
-                                 float scale, uint32_t tonemapping, cudaStream_t s) {
-    k_film_resolve<<<(numPixels + 255) / 256, 256, 0, s>>>(film, film64, fp64, out, numPixels, scale, tonemapping);
+                                 float exposure, float divisor, uint32_t tonemapping, uint32_t channels, cudaStream_t s) {
+    k_film_resolve<<<(numPixels + 255) / 256, 256, 0, s>>>(film, film64, fp64, out, numPixels, exposure, divisor,
+                                                            tonemapping, channels);
     return cudaGetLastError();
 }
 cudaError_t rmdLaunchDebugPrng(uint32_t mode, uint64_t a, uint64_t b, int n, float *out, cudaStream_t s) {

@@ -20,7 +20,8 @@ cudaError_t rmdLaunchTraceShadow(const rmd::WideNode *nodes, const float4 *tris,
 cudaError_t rmdLaunchEnvmapReduce(float *mip, int cur, cudaStream_t s);
 cudaError_t rmdLaunchEnvmapNormalize(const float *sum, float *pdfs, uint32_t gridSize, cudaStream_t s);
 cudaError_t rmdLaunchFilmResolve(const float4 *film, const double *film64, int fp64, float *out, uint32_t numPixels,
-                                 float scale, uint32_t tonemapping, cudaStream_t s);
+                                 float exposure, float divisor, uint32_t tonemapping, uint32_t channels,
+                                 cudaStream_t s);
 cudaError_t rmdLaunchDebugPrng(uint32_t mode, uint64_t a, uint64_t b, int n, float *out, cudaStream_t s);
 cudaError_t rmdLaunchDebugTrace(const rmd::WideNode *nodes, const float4 *tris, const float *rays, int n, int any,
                                 float *out, uint32_t *inst, uint32_t *errors, cudaStream_t s);

@@ -27,6 +27,44 @@
 
 using namespace rmd;
 
+// The host-facing records keep the layout of the reference's DEVICE_STRUCTs
+// (raymond/bridge/Camera.hpp, PerInstanceData.hpp, Uniforms.hpp, lights/ *.hpp)
+// as Swift and Metal lay them out: float3 16 bytes aligned to 16, float2 8
+// aligned to 8, bool one byte.
+static_assert(sizeof(rmd_camera) == 96 && alignof(rmd_camera) == 16, "Camera.hpp layout");
+static_assert(offsetof(rmd_camera, near_clip) == 64 && offsetof(rmd_camera, far_clip) == 68 &&
+                  offsetof(rmd_camera, focal_length) == 72 && offsetof(rmd_camera, shift) == 80,
+              "Camera.hpp layout");
+static_assert(sizeof(rmd_light_info) == 4 && offsetof(rmd_light_info, casts_shadows) == 2 &&
+                  offsetof(rmd_light_info, uses_mis) == 3,
+              "LightInfo.hpp layout");
+static_assert(sizeof(rmd_area_light) == 96 && offsetof(rmd_area_light, transform) == 16 &&
+                  offsetof(rmd_area_light, color) == 64 && offsetof(rmd_area_light, is_circular) == 80,
+              "AreaLight.hpp layout");
+static_assert(sizeof(rmd_point_light) == 64 && offsetof(rmd_point_light, location) == 16 &&
+                  offsetof(rmd_point_light, radius) == 32 && offsetof(rmd_point_light, color) == 48,
+              "PointLight.hpp layout");
+static_assert(sizeof(rmd_sun_light) == 64 && offsetof(rmd_sun_light, direction) == 16 &&
+                  offsetof(rmd_sun_light, cos_angle) == 32 && offsetof(rmd_sun_light, color) == 48,
+              "SunLight.hpp layout");
+static_assert(sizeof(rmd_spot_light) == 96 && offsetof(rmd_spot_light, location) == 16 &&
+                  offsetof(rmd_spot_light, direction) == 32 && offsetof(rmd_spot_light, radius) == 48 &&
+                  offsetof(rmd_spot_light, color) == 64 && offsetof(rmd_spot_light, spot_size) == 80 &&
+                  offsetof(rmd_spot_light, spot_blend) == 84,
+              "SpotLight.hpp layout");
+static_assert(sizeof(rmd_per_instance_data) == 192 && offsetof(rmd_per_instance_data, light_index) == 16 &&
+                  offsetof(rmd_per_instance_data, bounds_min) == 32 &&
+                  offsetof(rmd_per_instance_data, bounds_size) == 48 &&
+                  offsetof(rmd_per_instance_data, point_transform) == 64 &&
+                  offsetof(rmd_per_instance_data, normal_transform) == 128 &&
+                  offsetof(rmd_per_instance_data, visibility) == 176,
+              "PerInstanceData.hpp layout");
+static_assert(sizeof(rmd_uniforms) == 64 && offsetof(rmd_uniforms, accumulate) == 12 &&
+                  offsetof(rmd_uniforms, lens_spectral) == 13 && offsetof(rmd_uniforms, sensor_scale) == 16 &&
+                  offsetof(rmd_uniforms, exposure) == 28 && offsetof(rmd_uniforms, sampling_mode) == 44 &&
+                  offsetof(rmd_uniforms, tonemapping) == 48 && offsetof(rmd_uniforms, output_channel) == 60,
+              "Uniforms.hpp layout");
+
 namespace {
 
 thread_local std::string g_lastError;
@@ -115,6 +153,7 @@ struct rmd_scene {
     std::string moduleSource;
     std::map<int, std::unique_ptr<rmdhost::JitModule>> variants;  // shade kernels by minimum blocks per SM
     uint64_t triangles = 0, bvhNodeCount = 0;
+    std::vector<rmd_per_instance_data> instanceRecords;  // EntityBuilder's records, bridge layout
     rmd_bvh_stats bvhStats{};  // builder, build time and levels; SAH cost computed when first asked
     bool bvhSahKnown = false;
     float boundsMin[3] = {0, 0, 0}, boundsMax[3] = {1, 1, 1};  // world-space triangle bounds
@@ -664,6 +703,21 @@ static rmd_status buildSceneData(rmd_context *ctx, const rmd_scene_desc *d, rmd_
     RMD_CUDA(s->texcoords.upload(uvs.data(), uvs.size() * sizeof(float2), st));
     RMD_CUDA(s->faces.upload(faces.data(), faces.size() * sizeof(uint4), st));
     RMD_CUDA(s->instances.upload(insts.data(), insts.size() * sizeof(PerInstanceData), st));
+    s->instanceRecords.assign(insts.size(), rmd_per_instance_data{});
+    for (size_t i = 0; i < insts.size(); i++) {
+        const PerInstanceData &p = insts[i];
+        rmd_per_instance_data &o = s->instanceRecords[i];
+        o.vertex_offset = p.vertexOffset;
+        o.face_offset = p.faceOffset;
+        o.light_face_offset = p.lightFaceOffset;
+        o.light_face_count = p.lightFaceCount;
+        o.light_index = p.lightIndex;
+        std::memcpy(o.bounds_min, &p.boundsMin, 3 * sizeof(float));
+        std::memcpy(o.bounds_size, &p.boundsSize, 3 * sizeof(float));
+        std::memcpy(o.point_transform, p.pointTransform, 16 * sizeof(float));
+        for (int c = 0; c < 3; c++) std::memcpy(o.normal_transform + 4 * c, &p.normalTransform[c], 3 * sizeof(float));
+        o.visibility = (uint8_t)p.visibility;
+    }
     RMD_CUDA(s->lightFaces.upload(lightFaces.data(), lightFaces.size() * sizeof(float), st));
     RMD_CUDA(s->areaLights.upload(areas.data(), areas.size() * sizeof(AreaLight), st));
     RMD_CUDA(s->pointLights.upload(points.data(), points.size() * sizeof(PointLight), st));
@@ -774,6 +828,14 @@ rmd_status rmd_scene_info(const rmd_scene *s, uint64_t *triangles, uint64_t *bvh
     if (triangles) *triangles = s->triangles;
     if (bvh_nodes) *bvh_nodes = s->bvhNodeCount;
     if (num_lights_total) *num_lights_total = s->dctx.numLightsTotal;
+    return RMD_OK;
+}
+
+rmd_status rmd_scene_instance_data(const rmd_scene *s, rmd_per_instance_data *out, int32_t capacity, int32_t *count) {
+    if (!s || (capacity > 0 && !out) || capacity < 0) return fail(RMD_ERROR_INVALID_ARGUMENT, "invalid argument");
+    const size_t n = std::min<size_t>((size_t)capacity, s->instanceRecords.size());
+    if (n) std::memcpy(out, s->instanceRecords.data(), n * sizeof(rmd_per_instance_data));
+    if (count) *count = (int32_t)s->instanceRecords.size();
     return RMD_OK;
 }
 
@@ -940,7 +1002,7 @@ rmd_status rmd_renderer_set_size(rmd_renderer *r, uint32_t width, uint32_t heigh
     r->height = height;
     RMD_CUDA(r->film.alloc((size_t)width * height * sizeof(float4)));
     r->film64.release();
-    RMD_CUDA(r->resolve.alloc((size_t)width * height * 3 * sizeof(float)));
+    RMD_CUDA(r->resolve.alloc((size_t)width * height * 4 * sizeof(float)));  // RGB or RGBA (rmd_film_normalize)
     return rmd_renderer_reset(r);
 }
 
@@ -988,6 +1050,38 @@ rmd_status rmd_renderer_set_camera(rmd_renderer *r, const rmd_camera *cam) {
     c.focalLength = cam->focal_length;
     c.shift = make_float2(cam->shift[0], cam->shift[1]);
     return rmd_renderer_reset(r);
+}
+
+rmd_status rmd_render_frame(rmd_renderer *r, const rmd_uniforms *u, uint32_t max_depth) {
+    if (!r || !u) return fail(RMD_ERROR_INVALID_ARGUMENT, "NULL argument");
+    if (u->num_lens_surfaces != 0) return fail(RMD_ERROR_INVALID_ARGUMENT, "lens cameras are not supported");
+    if (u->random_seed == 0) return fail(RMD_ERROR_INVALID_ARGUMENT, "random_seed must be >= 1");
+    if (u->sampling_mode > 2 || u->output_channel != RMD_OUTPUT_IMAGE)
+        return fail(RMD_ERROR_INVALID_ARGUMENT, "invalid uniforms");
+    if (!u->accumulate) {  // generate.metal:103-106 clears each pixel before the frame adds to it
+        const rmd_status st = rmd_renderer_reset(r);
+        if (st != RMD_OK) return st;
+    }
+    rmd_render_settings s{};
+    s.spp = 1;
+    s.max_depth = max_depth;
+    s.sampling_mode = u->sampling_mode;
+    s.rng = RMD_RNG_TEA;
+    s.first_sample = (int64_t)u->random_seed - 1;  // TEA seeds sample k with k + 1
+    return rmd_render(r, &s);
+}
+
+rmd_status rmd_film_normalize(rmd_renderer *r, const rmd_uniforms *u, float *rgba) {
+    if (!r || !u || !rgba) return fail(RMD_ERROR_INVALID_ARGUMENT, "NULL argument");
+    if (u->tonemapping > 2) return fail(RMD_ERROR_INVALID_ARGUMENT, "tonemapping out of range");
+    cudaStream_t st = r->scene->ctx->stream;
+    const uint32_t n = r->width * r->height;
+    const float div = u->accumulate ? (float)u->frame_index + 1.0f : 1.0f;
+    RMD_CUDA(rmdLaunchFilmResolve(r->film.as<float4>(), r->film64.as<double>(), 0, r->resolve.as<float>(), n,
+                                  u->exposure, div, u->tonemapping, 4, st));
+    RMD_CUDA(cudaMemcpyAsync(rgba, r->resolve.ptr, (size_t)n * 4 * sizeof(float), cudaMemcpyDeviceToHost, st));
+    RMD_CUDA(cudaStreamSynchronize(st));
+    return RMD_OK;
 }
 
 rmd_status rmd_render(rmd_renderer *r, const rmd_render_settings *s) {
@@ -1138,13 +1232,15 @@ rmd_status rmd_film_read(rmd_renderer *r, float *rgb, int32_t normalize, uint32_
     if (tonemapping > 2) return fail(RMD_ERROR_INVALID_ARGUMENT, "tonemapping out of range");
     cudaStream_t st = r->scene->ctx->stream;
     const uint32_t n = r->width * r->height;
-    float scale = 1.0f;
+    float ex = 1.0f, div = 1.0f;
     uint32_t tm = 0;
     if (normalize) {
-        scale = exposure / (float)std::max<uint64_t>(1, r->samples);
+        ex = exposure;
+        div = (float)std::max<uint64_t>(1, r->samples);
         tm = tonemapping;
     }
-    RMD_CUDA(rmdLaunchFilmResolve(r->film.as<float4>(), r->film64.as<double>(), 0, r->resolve.as<float>(), n, scale, tm, st));
+    RMD_CUDA(rmdLaunchFilmResolve(r->film.as<float4>(), r->film64.as<double>(), 0, r->resolve.as<float>(), n, ex, div,
+                                  tm, 3, st));
     RMD_CUDA(cudaMemcpyAsync(rgb, r->resolve.ptr, (size_t)n * 3 * sizeof(float), cudaMemcpyDeviceToHost, st));
     RMD_CUDA(cudaStreamSynchronize(st));
     return RMD_OK;
@@ -1837,14 +1933,15 @@ rmd_status rmd_batch_film_read(rmd_batch *b, int32_t view, float *rgb, int32_t n
     if (tonemapping > 2) return fail(RMD_ERROR_INVALID_ARGUMENT, "tonemapping out of range");
     cudaStream_t st = b->ctx->stream;
     const uint32_t n = b->views[view].width * b->views[view].height, off = b->offsets[view];
-    float scale = 1.0f;
+    float ex = 1.0f, div = 1.0f;
     uint32_t tm = 0;
     if (normalize) {
-        scale = exposure / (float)std::max<uint64_t>(1, b->samples);
+        ex = exposure;
+        div = (float)std::max<uint64_t>(1, b->samples);
         tm = tonemapping;
     }
     RMD_CUDA(rmdLaunchFilmResolve(b->film.as<float4>() + off, b->film64.ptr ? b->film64.as<double>() + 3 * (size_t)off : nullptr,
-                                  0, b->resolve.as<float>(), n, scale, tm, st));
+                                  0, b->resolve.as<float>(), n, ex, div, tm, 3, st));
     RMD_CUDA(cudaMemcpyAsync(rgb, b->resolve.ptr, (size_t)n * 3 * sizeof(float), cudaMemcpyDeviceToHost, st));
     RMD_CUDA(cudaStreamSynchronize(st));
     return RMD_OK;

@@ -2,9 +2,10 @@
 own device code (oracle/_ref/libref.so, built by oracle/ref/Makefile from the
 mounted reference).  Run from the repository root:
 
-    make -C oracle/ref && python tests/golden/make_ref_golden.py
+    make -C oracle/ref && python tests/golden/make_ref_golden.py [--only pin|render|tonemap]
 
-Contents: TEA PRNG streams, fractal noise values and the evaluate/sample
+Contents: the reference's normalizeImage (exposure, accumulation, Hable and
+ACES tonemaps) on a random film (ref_tonemap.npz); TEA PRNG streams, fractal noise values and the evaluate/sample
 results of every material in oracle/ref/pin_materials.py on seeded shading
 records, all computed by the reference's code (ref_pin.npz); and one-sample
 images of the reference-render scenes rendered by the reference's own kernels
@@ -13,6 +14,7 @@ the environment map) in all three sampling modes (ref_render.npz).
 """
 from __future__ import annotations
 
+import argparse
 import sys
 from pathlib import Path
 
@@ -38,7 +40,29 @@ RENDER_CASES = [("cornell", 48, 40, 8, [0, 5]), ("cornell_all_lights", 48, 40, 6
 SAMPLING_MODES = [0, 1, 2]  # BSDF, NEE, MIS
 
 
+# normalizeImage cases: exposure, accumulate, frame index, tonemapping (linear, Hable, ACES)
+TONEMAP_CASES = [(e, a, f, t) for t in (0, 1, 2) for e, a, f in ((1.0, 0, 0), (1.7, 1, 0), (0.6, 1, 6))]
+
+
+def tonemap_golden() -> None:
+    """ref_tonemap.npz: the reference's normalizeImage kernel on a heavy-tailed
+    random film (zeros, tiny and very large values included)."""
+    rng = np.random.default_rng(11)
+    film = (np.abs(rng.standard_cauchy((41, 29, 4))) * 3).astype(np.float32)
+    film[0, :4] = [0, 1e-30, 1e20, 3e38]
+    out = {"film": film, "cases": np.array(TONEMAP_CASES, np.float32),
+           "images": np.stack([R.normalize_image(film, e, bool(a), int(f), int(t)) for e, a, f, t in TONEMAP_CASES])}
+    np.savez_compressed(ROOT / "tests" / "golden" / "ref_tonemap.npz", **out)
+
+
 def main() -> None:
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--only", choices=["pin", "render", "tonemap"], help="regenerate one file")
+    args = ap.parse_args()
+    if args.only in (None, "tonemap"):
+        tonemap_golden()
+    if args.only == "tonemap":
+        return
     out = {}
     out["prng_cases"] = np.array(PRNG_CASES, np.uint64)
     out["prng"] = np.stack([R.prng_tea(a, b, 256) for a, b in PRNG_CASES])

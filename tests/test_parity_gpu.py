@@ -9,7 +9,8 @@ import pytest
 
 import oracle_ctypes as O
 from raymond_b200 import api, scenes
-from raymond_b200._abi import RNG_PCG32, RNG_TEA, SAMPLING_BSDF, SAMPLING_MIS, SAMPLING_NEE, SceneDesc
+from raymond_b200._abi import (RNG_PCG32, RNG_TEA, SAMPLING_BSDF, SAMPLING_MIS, SAMPLING_NEE, TONEMAP_ACES,
+                               TONEMAP_HABLE, TONEMAP_LINEAR, SceneDesc, default_uniforms)
 
 pytestmark = pytest.mark.gpu
 
@@ -292,3 +293,42 @@ def test_set_tuning_keeps_parity(cornell):
     assert match_fraction(r.film(), cpu) >= MIN_MATCH
     with pytest.raises(api.RmdError):
         r.set_tuning({"shade_min_blocks": 0, "trace_blocks_per_sm": 4, "pool_size": 0})
+
+
+@pytest.mark.parametrize("tonemapping", [TONEMAP_LINEAR, TONEMAP_HABLE, TONEMAP_ACES])
+def test_film_tonemap(cornell, tonemapping):
+    """normalizeImage on the GPU (rmd_film_read and rmd_film_normalize with the
+    reference's Uniforms) against the oracle's restatement, which is pinned bit
+    for bit to the reference's kernel; the GPU may fuse multiply-adds, so the
+    bar is 1e-5 relative + 1e-6 absolute (the Hable curve subtracts nearly
+    equal terms near black)."""
+    desc, scene, orc = cornell
+    r = api.Renderer(scene, 64, 64)
+    r.render(spp=4, max_depth=8)
+    raw = r.film()
+    got = r.film(normalize=True, tonemapping=tonemapping, exposure=1.7)
+    ref = O.normalize_image(raw, 1.7, True, 3, tonemapping)
+    np.testing.assert_allclose(got, ref[..., :3], rtol=1e-5, atol=1e-6)
+    for accumulate in (1, 0):
+        u = default_uniforms(exposure=0.8, tonemapping=tonemapping, frame_index=3, accumulate=accumulate)
+        got4 = r.film_normalize(u)
+        ref4 = O.normalize_image(raw, 0.8, bool(accumulate), 3, tonemapping)
+        np.testing.assert_allclose(got4, ref4, rtol=1e-5, atol=1e-6)
+
+
+def test_render_frame_uniforms(cornell):
+    """rmd_render_frame: frames driven by the reference's Uniforms equal the
+    oracle's TEA frames (random seed k = sample k - 1); accumulate = 0 clears
+    the film first."""
+    desc, scene, orc = cornell
+    W = H = 80
+    r = api.Renderer(scene, W, H)
+    for frame in range(3):
+        r.render_frame(default_uniforms(frame_index=frame, random_seed=frame + 1, accumulate=1), max_depth=8)
+    cpu, _ = orc.render(W, H, 3, 8, rng=RNG_TEA, first_sample=0)
+    assert match_fraction(r.film(), cpu) >= MIN_MATCH
+    r.render_frame(default_uniforms(random_seed=5, accumulate=0, sampling_mode=SAMPLING_NEE), max_depth=8)
+    cpu, _ = orc.render(W, H, 1, 8, rng=RNG_TEA, first_sample=4, sampling_mode=SAMPLING_NEE)
+    assert match_fraction(r.film(), cpu) >= MIN_MATCH
+    with pytest.raises(api.RmdError):
+        r.render_frame(default_uniforms(num_lens_surfaces=3))

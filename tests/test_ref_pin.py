@@ -123,3 +123,26 @@ def test_oracle_images_match_reference_live(ref_scene_descs, name):
             rf = ref.render(40, 30, 1, 10, sampling_mode=mode, first_frame=frame)
             cpu, _ = orc.render(40, 30, 1, 10, sampling_mode=mode, rng=RNG_TEA, first_sample=frame)
             assert _match(rf, cpu) >= MIN_MATCH, (mode, frame)
+
+
+# ------------------------------------------------------------------ tonemapping
+# normalizeImage (normalizeImage.metal:11-59): the oracle's restatement against
+# the reference's own kernel, bit for bit.
+TONEMAP_GOLDEN = Path(__file__).resolve().parent / "golden" / "ref_tonemap.npz"
+
+
+def test_oracle_tonemap_matches_reference_golden():
+    g = np.load(TONEMAP_GOLDEN)
+    for (e, a, f, t), ref in zip(g["cases"], g["images"]):
+        got = O.normalize_image(g["film"], float(e), bool(a), int(f), int(t))
+        assert np.array_equal(got.view(np.uint32), ref.view(np.uint32)), (e, a, f, t)
+
+
+@pytest.mark.skipif(not R.available(), reason="host build of the reference (oracle/_ref/libref.so) not present")
+def test_oracle_tonemap_matches_reference_live():
+    film = np.random.default_rng(4).gamma(0.5, 4.0, (23, 31, 4)).astype(np.float32)
+    for t in (0, 1, 2):
+        for e, a, f in ((2.5, 1, 3), (1.0, 0, 9)):
+            ref = R.normalize_image(film, e, bool(a), f, t)
+            got = O.normalize_image(film, e, bool(a), f, t)
+            assert np.array_equal(got.view(np.uint32), ref.view(np.uint32)), (t, e, a, f)
