@@ -7,7 +7,10 @@ terrain, 851,968 triangles, noise->ramp->mix Principled material per object,
 1 sun + 16 point lights, 1920x1080, 64 spp, max depth 12, PCG32 seed 1.
 A step renders one full 64-spp frame (132.7 M paths).  With N ranks every
 rank renders its own 64 samples of the same image (sample ranges disjoint):
-weak scaling, no collective on the data path.
+weak scaling, no collective inside the timed steps.  Afterwards the ranks'
+films of their last step are summed into rank 0's renderer (one NCCL reduce
+of the W x H float4 film on the devices, `frame` in the line), so rank 0
+holds one image of all ranks' samples.
 
 `value`  : paths of all ranks / max-over-ranks device time (CUDA events of
            the library's stream, reported by rmd_renderer_stats), scene and
@@ -79,7 +82,8 @@ GUIDED_W, GUIDED_H, GUIDED_DEPTH, GUIDED_ORACLE_SPP, GUIDED_PLAIN_SPP, GUIDED_CH
 CPU_BASELINE_SPP = 16  # CPU sample: 16 one-spp frames of the full image (about 10-20 s on 16 cores)
 
 
-from raymond_b200.multi import rank_info, sample_range, shard_views, max_over_ranks, sum_over_ranks  # noqa: E402
+from raymond_b200.multi import (combine_films, max_over_ranks, rank_info, sample_range, shard_views,  # noqa: E402
+                                sum_over_ranks)
 
 
 class ClockSampler:
@@ -485,9 +489,17 @@ def main():
     rank, world, local = rank_info()
     dist = None
     if world > 1:
+        import datetime
+
+        import torch
         import torch.distributed as dist  # noqa: F811
 
-        dist.init_process_group("gloo", timeout=__import__("datetime").timedelta(seconds=600))
+        if torch.cuda.is_available():  # one rank per GPU: NCCL for the timing reductions and the film reduce
+            torch.cuda.set_device(local)
+            dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300),
+                                    device_id=torch.device(f"cuda:{local}"))
+        else:
+            dist.init_process_group("gloo", timeout=datetime.timedelta(seconds=300))
 
     from raymond_b200 import api
     from raymond_b200._abi import SceneDesc, make_camera
@@ -540,8 +552,13 @@ def main():
     for k in range(0 if args.no_e2e else args.steps):
         step(k, e2e=True)
     e2e_s = max(time.perf_counter() - t0, 1e-9)
+    # the frame of all ranks: each rank's last step holds its own SPP samples of the image; the films
+    # are summed into rank 0's renderer on the devices (NCCL reduce of W*H float4)
+    t0 = time.perf_counter()
+    frame_samples = combine_films(r)
+    reduce_s = time.perf_counter() - t0
     if dist:
-        tot_ms, e2e_s = max_over_ranks([tot_ms, e2e_s])
+        tot_ms, e2e_s, reduce_s = max_over_ranks([tot_ms, e2e_s, reduce_s])
         dist.barrier()
     if rank != 0:
         if dist:
@@ -583,6 +600,9 @@ def main():
         "e2e": None if args.no_e2e else {"value": e2e_value, "unit": "Mpaths/s", "h2d_bytes_per_step": 64 + 40,
                                          "d2h_bytes_per_step": W * H * 3 * 4},
         "gpu_launches": int(tot["iterations"] * 4 + args.steps),
+        "frame": {"samples": frame_samples, "ranks": world, "reduce_ms": reduce_s * 1e3,
+                  "reduce_bytes": W * H * 16 if world > 1 else 0,
+                  "mean_radiance": float(r.film(normalize=True).mean())},
         "clocks": clocks,
         "scene_build_s": build_s, "bvh": bvh,
         "autotune": dict(tune, seconds=tune_s) if tune else None,

@@ -456,6 +456,18 @@ rmd_status rmd_film_save_exr(rmd_renderer *r, const char *path, float normalized
 rmd_status rmd_film_read_f64(rmd_renderer *r, double *rgb);
 /* Samples accumulated in the film (frameIndex of Renderer.swift:288). */
 rmd_status rmd_film_samples(const rmd_renderer *r, uint64_t *samples);
+/* Device address of the renderer's film: width * height float4 (RGB radiance
+ * sums and a path count per pixel), row-major from the top-left pixel, on the
+ * renderer's device; valid until the renderer is resized or destroyed.  For
+ * collectives that sum the films of renderers on several GPUs (one image's
+ * samples split over ranks) without a round trip through host memory.  The
+ * film is complete when rmd_render returns; a writer on another stream must
+ * finish before the next call on this renderer.  No counterpart in the
+ * reference (one GPU, Renderer.swift:285). */
+rmd_status rmd_film_device(rmd_renderer *r, float **film, uint64_t *num_pixels);
+/* Set the sample count of the film (what rmd_film_read divides by) after
+ * other renderers' films were summed into it. */
+rmd_status rmd_film_set_samples(rmd_renderer *r, uint64_t samples);
 
 /* Launch choices picked by rmd_renderer_autotune. */
 typedef struct rmd_tune_result {

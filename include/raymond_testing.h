@@ -69,6 +69,12 @@ rmd_status rmd_test_guide_forward(const float *params, const float *features, in
 rmd_status rmd_test_guide_gradient(const float *params, const float *records, int32_t n, float *grad, float *loss);
 /* Packed mixture of one output vector (48): a direction and its pdf per row
  * of u (n x 3, into dirs_pdf n x 4), and the pdf at m query directions. */
+/* One Adam step (beta 0.9 / 0.999, eps 1e-8, bias-corrected for `step` >= 1)
+ * of the guide's parameters on a given gradient and moments: the new FP32
+ * parameters and moments, and the BF16 weight copy the tensor cores read
+ * (rmd_guide_param_count() floats each; weights only in bf16_out). */
+rmd_status rmd_test_guide_adam(const float *params, const float *grad, const float *m, const float *v, int32_t step,
+                               float lr, float *params_out, float *m_out, float *v_out, uint16_t *bf16_out);
 rmd_status rmd_test_guide_mixture(const float *outputs, const float *u, int32_t n, float *dirs_pdf,
                                   const float *queries, int32_t m, float *pdfs);
 

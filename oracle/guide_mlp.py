@@ -213,3 +213,19 @@ def init_params(seed: int = 0) -> np.ndarray:
             b[32] = np.log(s / (1 - s))
         parts += [rng.uniform(-a, a, i * o), b]
     return np.concatenate(parts).astype(np.float32)
+
+
+def adam_step(params, grad, m, v, step: int, lr: float, beta1=0.9, beta2=0.999, eps=1e-8):
+    """One Adam step (Kingma and Ba 2015, bias-corrected moments), float64:
+    returns the new parameters and moments."""
+    g = np.asarray(grad, np.float64)
+    m = beta1 * np.asarray(m, np.float64) + (1 - beta1) * g
+    v = beta2 * np.asarray(v, np.float64) + (1 - beta2) * g * g
+    mh = m / (1 - beta1 ** step)
+    vh = v / (1 - beta2 ** step)
+    return np.asarray(params, np.float64) - lr * mh / (np.sqrt(vh) + eps), m, v
+
+
+def weight_mask() -> np.ndarray:
+    """True at the flat parameters that are weights (False at biases)."""
+    return np.concatenate([np.concatenate([np.ones(i * o, bool), np.zeros(o, bool)]) for i, o in LAYERS])

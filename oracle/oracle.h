@@ -63,6 +63,13 @@ int oracle_render(oracle_scene *s, const oracle_settings *st, double *film_rgb, 
 void oracle_normalize_image(const float *film, uint32_t width, uint32_t height, float exposure, int32_t accumulate,
                             uint32_t frame_index, uint32_t tonemapping, float *out);
 
+/* The Nishita sky restated (host/sky/sky_nishita.cpp): the width x height
+ * RGBA float texture (XYZ in rgb) and the TEX_SKY node's ten data values. */
+void oracle_sky_texture(int32_t width, int32_t height, float sun_elevation, float altitude, float air, float dust,
+                        float ozone, float *rgba);
+void oracle_sky_data(float sun_elevation, float sun_rotation, int32_t sun_disc, float sun_size, float sun_intensity,
+                     float altitude, float air, float dust, float *data10);
+
 /* Unit hooks. */
 /* n values of PrngState.sample() for the stream (a, b): TEA(a, b) or PCG32(seed=a, seq=b). */
 void oracle_prng(int32_t mode, uint64_t a, uint64_t b, int32_t n, float *out);

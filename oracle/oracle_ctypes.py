@@ -53,6 +53,8 @@ def lib():
         L.oracle_material_eval.argtypes = [C.c_void_p, C.c_int32, C.POINTER(C.c_float), C.c_int32,
                                            C.POINTER(C.c_float)]
         L.oracle_scene_set_camera.argtypes = [C.c_void_p, C.c_void_p]
+        L.oracle_sky_texture.argtypes = [C.c_int32, C.c_int32] + [C.c_float] * 5 + [C.POINTER(C.c_float)]
+        L.oracle_sky_data.argtypes = [C.c_float, C.c_float, C.c_int32] + [C.c_float] * 5 + [C.POINTER(C.c_float)]
         L.oracle_normalize_image.argtypes = [C.POINTER(C.c_float), C.c_uint32, C.c_uint32, C.c_float, C.c_int32,
                                              C.c_uint32, C.c_uint32, C.POINTER(C.c_float)]
         _lib = L
@@ -147,6 +149,23 @@ def normalize_image(film: np.ndarray, exposure: float, accumulate: bool, frame_i
     out = np.zeros((h, w, 4), np.float32)
     lib().oracle_normalize_image(rgba.ctypes.data_as(C.POINTER(C.c_float)), w, h, exposure, int(accumulate),
                                  frame_index, tonemapping, out.ctypes.data_as(C.POINTER(C.c_float)))
+    return out
+
+
+def sky_texture(width: int, height: int, sun_elevation: float, altitude: float, air: float, dust: float,
+                ozone: float) -> np.ndarray:
+    """The Nishita sky texture restated: (height, width, 4) float32, XYZ in rgb."""
+    out = np.zeros((height, width, 4), np.float32)
+    lib().oracle_sky_texture(width, height, sun_elevation, altitude, air, dust, ozone,
+                             out.ctypes.data_as(C.POINTER(C.c_float)))
+    return out
+
+
+def sky_data(sun_elevation, sun_rotation, sun_disc, sun_size, sun_intensity, altitude, air, dust) -> np.ndarray:
+    """The TEX_SKY node's ten data values (sun disc colours, elevation, rotation, size or -1, intensity)."""
+    out = np.zeros(10, np.float32)
+    lib().oracle_sky_data(sun_elevation, sun_rotation, int(sun_disc), sun_size, sun_intensity, altitude, air, dust,
+                          out.ctypes.data_as(C.POINTER(C.c_float)))
     return out
 
 

@@ -224,7 +224,34 @@ def materials() -> list[tuple[str, dict]]:
                             "parameters": {"distribution": "GGX", "subsurface_method": "RANDOM_WALK"}},
         "Material Output": _out(("Principled BSDF", "BSDF")),
     }))
+    # the Nishita sky as an emissive colour (its node reads the shading point's wo); a large sun disc so that
+    # some records look into it
+    mats.append(("sky_emission", {
+        "Sky Texture": _bsdf("TEX_SKY", dict(SKY, sky_type="NISHITA"), Vector=_v("VECTOR", [0.0, 0.0, 0.0])),
+        "Emission": _bsdf("EMISSION", Color=_v("RGBA", link=("Sky Texture", "Color")),
+                          Strength=_v("VALUE", 1e-3)),
+        "Material Output": _out(("Emission", "Emission")),
+    }))
     return mats
+
+
+# parameters of the pinning sky (Blender's TEX_SKY node as the exporter writes them)
+SKY = {"sun_elevation": 0.35, "sun_rotation": 0.7, "sun_disc": True, "sun_size": 0.6, "sun_intensity": 1.5,
+       "altitude": 200.0, "air_density": 1.2, "dust_density": 0.8, "ozone_density": 1.1}
+
+
+def install_ref_textures(R) -> None:
+    """The reference build's Context.textures for the pinning materials: the
+    image textures in order, then the sky texture of the sky material made by
+    the reference's own sky model (its texture follows the scene's images)."""
+    tex = textures()
+    R.set_textures(tex)
+    xyz = R.sky_texture(512, 512, SKY["sun_elevation"], SKY["altitude"], SKY["air_density"], SKY["dust_density"],
+                        SKY["ozone_density"])
+    import numpy as np
+
+    rgba = np.concatenate([xyz, np.ones(xyz.shape[:2] + (1,), np.float32)], axis=-1)
+    R.set_texture(len(tex), rgba)
 
 
 def _image_params(path, colorspace, projection="FLAT"):

@@ -63,6 +63,12 @@ def set_textures(textures: dict) -> None:
         assert lib().ref_set_texture(slot, t.ctypes.data_as(_fp), t.shape[1], t.shape[0]) == 0
 
 
+def set_texture(slot: int, rgba: np.ndarray) -> None:
+    """Install one (h, w, 4) float texture at `slot` of the reference build's Context.textures."""
+    t = np.ascontiguousarray(rgba, np.float32)
+    assert lib().ref_set_texture(slot, t.ctypes.data_as(_fp), t.shape[1], t.shape[0]) == 0
+
+
 def prng_tea(a: int, b: int, n: int) -> np.ndarray:
     out = np.zeros(n, np.float32)
     lib().ref_prng_tea(a, b, n, out.ctypes.data_as(_fp))
@@ -145,4 +151,33 @@ def normalize_image(film: np.ndarray, exposure: float, accumulate: bool, frame_i
     out = np.zeros((h, w, 4), np.float32)
     lib().ref_normalize_image(film.ctypes.data_as(_fp), w, h, exposure, int(accumulate), frame_index, tonemapping,
                               out.ctypes.data_as(_fp))
+    return out
+
+
+SKY_LIB = Path(__file__).resolve().parents[1] / "_ref" / "libsky.so"
+
+
+def sky_available() -> bool:
+    return SKY_LIB.exists()
+
+
+def sky_texture(width: int, height: int, sun_elevation: float, altitude: float, air: float, dust: float,
+                ozone: float) -> np.ndarray:
+    """The reference's SKY_nishita_skymodel_precompute_texture: (height, width, 3) XYZ (the stride-4
+    buffer's fourth channel is never written by it)."""
+    L = C.CDLL(str(SKY_LIB))
+    L.SKY_nishita_skymodel_precompute_texture.argtypes = [_fp] + [C.c_int] * 5 + [C.c_float] * 5
+    px = np.zeros((height, width, 4), np.float32)
+    L.SKY_nishita_skymodel_precompute_texture(px.ctypes.data_as(_fp), 4, 0, height, width, height, sun_elevation,
+                                              altitude, air, dust, ozone)
+    return px[..., :3]
+
+
+def sky_sun(sun_elevation: float, angular_diameter: float, altitude: float, air: float, dust: float) -> np.ndarray:
+    """The reference's SKY_nishita_skymodel_precompute_sun: bottom and top XYZ (6 floats)."""
+    L = C.CDLL(str(SKY_LIB))
+    L.SKY_nishita_skymodel_precompute_sun.argtypes = [C.c_float] * 5 + [_fp, _fp]
+    out = np.zeros(6, np.float32)
+    L.SKY_nishita_skymodel_precompute_sun(sun_elevation, angular_diameter, altitude, air, dust,
+                                          out[:3].ctypes.data_as(_fp), out[3:].ctypes.data_as(_fp))
     return out

@@ -10,6 +10,8 @@
 #include <vector>
 #ifdef _OPENMP
 #include <omp.h>
+
+#include "sky.h"
 #endif
 
 #include "../oracle.h"
@@ -352,6 +354,32 @@ extern "C" int oracle_scene_create(const rmd_scene_desc *d, oracle_scene **out, 
         texNames.push_back(t.name ? t.name : "");
         texChannels.push_back((int)t.channels);
     }
+    // the sky textures of the TEX_SKY nodes (SkyLoader.generate, MaterialBuilder.swift:350-372), one per
+    // distinct set of parameters, after the scene's images
+    try {
+        auto addSkies = [&](const rmd_material *mats, int count) {
+            for (int m = 0; m < count; m++)
+                for (int k = 0; k < mats[m].num_nodes; k++) {
+                    const rmd_node &n = mats[m].nodes[k];
+                    if (!n.type || std::string(n.type) != "TEX_SKY") continue;
+                    const SkyParams p = skyParams(n);
+                    const std::string key = skyTextureKey(p);
+                    if (std::find(texNames.begin(), texNames.end(), key) != texNames.end()) continue;
+                    Texture tex;
+                    tex.width = tex.height = 512;
+                    tex.channels = 4;
+                    tex.texels = oracle_sky::skyTexture(512, 512, p.elevation, p.altitude, p.air, p.dust, p.ozone);
+                    ctx.textures.push_back(std::move(tex));
+                    texNames.push_back(key);
+                    texChannels.push_back(4);
+                }
+        };
+        addSkies(d->surface_materials, d->num_surface_materials);
+        addSkies(d->light_materials, d->num_light_materials);
+    } catch (const CodegenError &e) {
+        fail(err, errlen, e.message);
+        return e.status;
+    }
     ctx.textures.push_back(Texture());
     try {
         // MaterialBuilder: shadeSurface / shadeLight tables
@@ -641,6 +669,19 @@ extern "C" void oracle_normalize_image(const float *film, uint32_t width, uint32
         out[4 * i + 2] = c.z;
         out[4 * i + 3] = 1.0f;
     }
+}
+
+// ---------------------------------------------------------------- sky hooks
+extern "C" void oracle_sky_texture(int32_t width, int32_t height, float sun_elevation, float altitude, float air,
+                                   float dust, float ozone, float *rgba) {
+    const std::vector<float4> t = oracle_sky::skyTexture(width, height, sun_elevation, altitude, air, dust, ozone);
+    std::memcpy(rgba, t.data(), t.size() * sizeof(float4));
+}
+
+extern "C" void oracle_sky_data(float sun_elevation, float sun_rotation, int32_t sun_disc, float sun_size,
+                                float sun_intensity, float altitude, float air, float dust, float *data10) {
+    oracle_sky::skyData(sun_elevation, sun_rotation, sun_disc != 0, sun_size, sun_intensity, altitude, air, dust,
+                        data10);
 }
 
 // ---------------------------------------------------------------- unit hooks

@@ -5,11 +5,13 @@
 #include <algorithm>
 #include <atomic>
 #include <cctype>
+#include <cstdio>
 #include <functional>
 #include <map>
 #include <set>
 
 #include "noise.h"
+#include "sky.h"
 
 namespace orc {
 
@@ -464,6 +466,58 @@ struct TexImage {  // nodes.hpp:486-564 (image and environment textures)
         FLD(T, vector, K_F3); FLD(T, color, K_F4); FLD(T, alpha, K_F1);
     }
 };
+struct TexNishita {  // nodes.hpp:774-870 (sky_radiance_nishita, TexNishita)
+    float scale = 1;
+    float3 vector;
+    float4 color;
+    float data[10] = {};
+    int slot = 0;
+    void compute(const SceneData &d, ShadingContext &sh) {
+        const float3 dir = sh.wo * float3(1, -1, -1);
+        const float elev = data[6], rot = data[7], diameter = data[8], intensity = data[9];
+        float3 xyz(0, 0, 0);
+        const float theta = std::acos(dir.z), phi = std::atan2(dir.x, dir.y);
+        const float pi = (float)M_PI, halfPi = (float)M_PI / 2;
+        if (dir.z >= 0.0f) {
+            const float3 sun = oracle_sky::direction(elev, rot + halfPi);
+            const float angle = 2.f * std::atan2(length(dir - sun), length(dir + sun));
+            const float half = diameter / 2.0f;
+            const float dirElev = halfPi - theta;
+            if (angle < half && diameter > 0) {
+                const float3 bottom(data[0], data[1], data[2]), top(data[3], data[4], data[5]);
+                if (elev - half > 0.0f) {
+                    if (elev + half > 0.0f) {
+                        const float y = ((dirElev - elev) / diameter) + 0.5f;
+                        xyz = (bottom + (top - bottom) * y) * intensity;
+                    }
+                } else if (elev + half > 0.0f) {
+                    const float y = dirElev / (elev + half);
+                    xyz = (bottom + (top - bottom) * y) * intensity;
+                }
+                const float f = angle / half;
+                xyz = xyz * (1.0f - 0.6f * (1.0f - std::sqrt(1.0f - f * f)));
+            } else {
+                float x = (phi + pi + rot) / (2 * pi);
+                const float y = std::sqrt(dirElev / halfPi);
+                if (x > 1.0f) x = x - 1.0f;
+                xyz = sampleLinearRepeat(d.textures[slot], float2(x, y)).xyz();
+            }
+        } else if (dir.z >= -0.4f) {
+            const float mul = std::pow(1.0f + dir.z * 2.5f, 3.0f);
+            float x = (phi + pi + rot) / (2 * pi);
+            if (x > 1.0f) x = x - 1.0f;
+            xyz = sampleLinearRepeat(d.textures[slot], float2(x, 1e-3f)).xyz() * mul;
+        }
+        const float3 rgb(3.240479f * xyz.x + -1.537150f * xyz.y + -0.498535f * xyz.z,  // color.hpp:74-78
+                         -0.969256f * xyz.x + 1.875991f * xyz.y + 0.041556f * xyz.z,
+                         0.055648f * xyz.x + -0.204043f * xyz.y + 1.057311f * xyz.z);
+        color = float4(scale * rgb.x, scale * rgb.y, scale * rgb.z, 1);
+    }
+    static void describe(FieldList &fl) {
+        using T = TexNishita;
+        FLD(T, vector, K_F3); FLD(T, color, K_F4);
+    }
+};
 struct Mapping {  // nodes.hpp:346-364 with euler2mat of math.hpp:46-68 (one Type: MAPPING)
     float3 scale, rotation, location, vector;
     void compute(const SceneData &, ShadingContext &) {
@@ -902,6 +956,50 @@ static bool paramBool(const rmd_node &n, const char *key, bool fb) {
     auto p = findParam(n, key);
     return p ? p->number_value != 0 : fb;
 }
+static float paramNumber(const rmd_node &n, const char *key, float fb) {
+    auto p = findParam(n, key);
+    return (p && (p->kind == RMD_PARAM_NUMBER || p->kind == RMD_PARAM_BOOL)) ? (float)p->number_value : fb;
+}
+
+SkyParams skyParams(const rmd_node &n) {
+    const float deg = (float)M_PI / 180.0f;
+    SkyParams p;
+    std::string type = paramString(n, "sky_type", "NISHITA");
+    p.elevation = paramNumber(n, "sun_elevation", 15.0f * deg);
+    p.rotation = paramNumber(n, "sun_rotation", 0.0f);
+    p.disc = paramBool(n, "sun_disc", true);
+    p.size = paramNumber(n, "sun_size", 0.545f * deg);
+    p.intensity = paramNumber(n, "sun_intensity", 1.0f);
+    p.altitude = paramNumber(n, "altitude", 0.0f);
+    p.air = paramNumber(n, "air_density", 1.0f);
+    p.dust = paramNumber(n, "dust_density", 1.0f);
+    p.ozone = paramNumber(n, "ozone_density", 1.0f);
+    p.scale = 1.0f;
+    if (type == "HOSEK_WILKIE") {  // MaterialBuilder.swift:333-348
+        float d[3] = {0, 0, 1};
+        auto q = findParam(n, "sun_direction");
+        if (q && q->num_numbers >= 3)
+            for (int i = 0; i < 3; i++) d[i] = q->numbers[i];
+        p.rotation = std::atan2(d[0], d[1]);
+        p.elevation = std::max(std::asin(d[2]), 5 * deg);
+        p.disc = false;
+        p.air = 2;
+        p.dust = 0.5f;
+        p.ozone = 1;
+        p.scale = 0.08f;
+        type = "NISHITA";
+    }
+    if (type != "NISHITA") throw CodegenError{RMD_ERROR_CODEGEN_UNSUPPORTED, "TexSky: unsupported sky type " + type};
+    return p;
+}
+
+std::string skyTextureKey(const SkyParams &p) {
+    char buf[200];
+    std::snprintf(buf, sizeof(buf), "sky %a %a %a %a %a", (double)p.elevation, (double)p.altitude, (double)p.air,
+                  (double)p.dust, (double)p.ozone);
+    return buf;
+}
+
 static int enumIndex(const std::string &v, std::initializer_list<const char *> names, int fb = -1) {
     // MaterialBuilder.swift:147-149: value with non-word characters replaced by '_', uppercased
     std::string e;
@@ -1034,6 +1132,18 @@ static std::unique_ptr<NodeImpl> makeKernel(const rmd_node &n, const std::vector
         b->v.colorSpace = enumIndex(paramString(n, "colorspace", "sRGB"),
                                     {"LINEAR", "SRGB", "NON_COLOR", "RAW", "XYZ", "FILMIC_LOG"});
         if (b->v.projection < 0 || b->v.colorSpace < 0) return unsupported();
+        return b;
+    }
+    if (t == "TEX_SKY") {  // MaterialBuilder.swift:329-388
+        const SkyParams p = skyParams(n);
+        auto b = std::make_unique<Box<TexNishita>>();
+        const std::string key = skyTextureKey(p);
+        b->v.slot = (int)texNames.size();
+        for (size_t i = 0; i < texNames.size(); i++)
+            if (texNames[i] == key) b->v.slot = (int)i;
+        oracle_sky::skyData(p.elevation, p.rotation, p.disc, p.size, p.intensity, p.altitude, p.air, p.dust,
+                            b->v.data);
+        b->v.scale = p.scale;
         return b;
     }
     if (t == "HUE_SAT") return std::make_unique<Box<HueSaturation>>();

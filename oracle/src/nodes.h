@@ -82,4 +82,17 @@ private:
     uint64_t serial_ = 0;  // unique per program ever built: keys the per-thread node scratch
 };
 
+// TEX_SKY as MaterialBuilder.swift:329-349 resolves it: a Hosek-Wilkie sky
+// becomes a Nishita sky of its sun direction (no disc, air 2, dust 0.5,
+// ozone 1, sun at least 5 degrees up, scale 0.08); other types are
+// unsupported (throws CodegenError).  Missing parameters: Blender's defaults.
+struct SkyParams {
+    float elevation, rotation, size, intensity, altitude, air, dust, ozone, scale;
+    bool disc;
+};
+SkyParams skyParams(const rmd_node &n);
+// the name under which the scene's texture table holds the sky texture of
+// these parameters (the texture depends on elevation, altitude and densities)
+std::string skyTextureKey(const SkyParams &p);
+
 }  // namespace orc

@@ -33,10 +33,10 @@ EXPORTS = [
     "rmd_batch_film_read", "rmd_batch_film_read_f64", "rmd_batch_stats", "rmd_batch_autotune",
     "rmd_batch_set_guide", "rmd_batch_guide_stats", "rmd_context_set_bvh_builder", "rmd_scene_bvh_stats",
     "rmd_film_save_exr", "rmd_batch_film_save_exr", "rmd_scene_instance_data", "rmd_render_frame",
-    "rmd_film_normalize",
+    "rmd_film_normalize", "rmd_film_device", "rmd_film_set_samples",
     "rmd_test_prng", "rmd_test_trace", "rmd_test_material_eval", "rmd_test_generate_source", "rmd_test_jit_compile",
     "rmd_test_guide_forward", "rmd_test_guide_gradient", "rmd_test_guide_mixture", "rmd_test_bvh_read",
-    "rmd_test_exr_write",
+    "rmd_test_exr_write", "rmd_test_guide_adam",
 ]
 
 
@@ -85,6 +85,8 @@ def lib() -> C.CDLL:
         "rmd_film_read": ([vp, P(C.c_float), C.c_int32, C.c_uint32, C.c_float], C.c_int32),
         "rmd_film_read_f64": ([vp, P(C.c_double)], C.c_int32),
         "rmd_film_samples": ([vp, P(C.c_uint64)], C.c_int32),
+        "rmd_film_device": ([vp, P(vp), P(C.c_uint64)], C.c_int32),
+        "rmd_film_set_samples": ([vp, C.c_uint64], C.c_int32),
         "rmd_renderer_stats": ([vp, P(Stats)], C.c_int32),
         "rmd_renderer_autotune": ([vp, P(RenderSettings), P(_abi.TuneResult)], C.c_int32),
         "rmd_renderer_set_tuning": ([vp, P(_abi.TuneResult)], C.c_int32),
@@ -109,6 +111,8 @@ def lib() -> C.CDLL:
         "rmd_batch_guide_stats": ([vp, P(_abi.GuideStats)], C.c_int32),
         "rmd_render_noalloc": ([vp, P(_abi.Camera), C.c_uint32, C.c_uint32, P(RenderSettings), C.c_void_p,
                                 C.c_uint32], C.c_int32),
+        "rmd_test_guide_adam": ([P(C.c_float)] * 4 + [C.c_int32, C.c_float] + [P(C.c_float)] * 3 + [P(C.c_uint16)],
+                                C.c_int32),
         "rmd_test_prng": ([C.c_uint32, C.c_uint64, C.c_uint64, C.c_int32, P(C.c_float)], C.c_int32),
         "rmd_test_trace": ([vp, P(C.c_float), C.c_int32, C.c_int32, P(C.c_float), P(C.c_uint32)], C.c_int32),
         "rmd_test_material_eval": ([vp, C.c_int32, P(C.c_float), C.c_int32, P(C.c_float)], C.c_int32),
@@ -138,6 +142,7 @@ class Context:
     in this context."""
 
     def __init__(self, device: int = 0, bvh_builder: str = "host"):
+        self.device = device
         self.h = C.c_void_p()
         check(lib().rmd_context_create(device, C.byref(self.h)))
         self.set_bvh_builder(bvh_builder)
@@ -227,6 +232,14 @@ class Scene:
             pass
 
 
+class DeviceFilm:
+    """A renderer's device film seen through the CUDA array interface (no copy)."""
+
+    def __init__(self, ptr: int, shape: tuple[int, int, int]):
+        self.__cuda_array_interface__ = {"shape": shape, "typestr": "<f4", "data": (ptr, False), "version": 3,
+                                         "strides": None, "stream": None}
+
+
 class Renderer:
     """Wavefront renderer for one film (rmd_renderer)."""
 
@@ -245,6 +258,25 @@ class Renderer:
         out = np.zeros((self.height, self.width, 3), np.float32)
         check(lib().rmd_film_read(self.h, _f32p(out), int(normalize), tonemapping, exposure))
         return out
+
+    def film_device(self) -> "DeviceFilm":
+        """The film in device memory, zero-copy (rmd_film_device): an object with
+        __cuda_array_interface__ of shape (H, W, 4) float32 (RGB sums, path count),
+        e.g. for torch.as_tensor(..., device="cuda") and a collective."""
+        ptr = C.c_void_p()
+        n = C.c_uint64()
+        check(lib().rmd_film_device(self.h, C.byref(ptr), C.byref(n)))
+        return DeviceFilm(ptr.value, (self.height, self.width, 4))
+
+    def film_tensor(self):
+        """The device film as a torch CUDA tensor (H, W, 4) aliasing the library's buffer."""
+        import torch
+
+        return torch.as_tensor(self.film_device(), device=f"cuda:{self.scene.ctx.device}")
+
+    def set_samples(self, samples: int) -> None:
+        """The film's sample count after other renderers' films were summed into it."""
+        check(lib().rmd_film_set_samples(self.h, samples))
 
     def render_frame(self, uniforms: _abi.Uniforms, max_depth: int = 8) -> None:
         """One frame of the reference's Renderer.execute driven by its Uniforms (rmd_render_frame)."""
@@ -362,7 +394,7 @@ class Batch:
         for i, v in enumerate(views):
             known = 0 <= v["scene"] < len(self.descs)  # an unknown index is the library's to reject
             cam = v.get("camera") or self.descs[v["scene"] if known else 0].scene["camera"]
-            vs[i] = _abi.BatchView(v["scene"], v["width"], v["height"], _abi.make_camera(cam))
+            vs[i] = _abi.BatchView(scene=v["scene"], width=v["width"], height=v["height"], camera=_abi.make_camera(cam))
             self.sizes.append((v["height"], v["width"]))
         self.h = C.c_void_p()
         flags = 0 if graph else _abi.BATCH_NO_GRAPH
@@ -475,6 +507,16 @@ def guide_gradient(params: np.ndarray, records: np.ndarray) -> tuple[np.ndarray,
     loss = C.c_float()
     check(lib().rmd_test_guide_gradient(_f32p(p), _f32p(r), r.shape[0], _f32p(grad), C.byref(loss)))
     return grad, loss.value
+
+
+def guide_adam(params: np.ndarray, grad: np.ndarray, m: np.ndarray, v: np.ndarray, step: int, lr: float):
+    """Test hook: one Adam step on the device: (params, m, v, bf16 weight bits)."""
+    f = [np.ascontiguousarray(a, np.float32) for a in (params, grad, m, v)]
+    outs = [np.zeros_like(f[0]) for _ in range(3)]
+    bits = np.zeros(guide_param_count(), np.uint16)  # the first (weights) entries are written
+    check(lib().rmd_test_guide_adam(*[_f32p(a) for a in f], step, lr, *[_f32p(a) for a in outs],
+                                    bits.ctypes.data_as(C.POINTER(C.c_uint16))))
+    return outs[0], outs[1], outs[2], bits
 
 
 def guide_mixture(outputs: np.ndarray, u: np.ndarray, queries: np.ndarray) -> tuple[np.ndarray, np.ndarray]:

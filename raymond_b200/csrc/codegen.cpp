@@ -18,10 +18,13 @@
 // function (one code path for a warp that shades several of them).
 #include "codegen.h"
 
+#include "sky.h"
+
 #include <algorithm>
 #include <cctype>
 #include <cmath>
 #include <cstdio>
+#include <cstdlib>
 #include <functional>
 #include <map>
 #include <set>
@@ -99,6 +102,7 @@ const std::map<std::string, KernelDesc> &kernelTable() {
         add("ColorInvert", {{"color", F4}, {"fac", F1}});
         add("Gamma", {{"color", F4}, {"gamma", F1}});
         add("TexImage", {{"vector", F3}, {"color", F4}, {"alpha", F1}});
+        add("TexNishita", {{"vector", F3}, {"color", F4}});
         add("Mapping", {{"scale", F3}, {"rotation", F3}, {"location", F3}, {"vector", F3}});
         add("NormalMap", {{"color", F4}, {"strength", F1}, {"normal", F3}});
         add("HueSaturation", {{"color", F4}, {"fac", F1}, {"hue", F1}, {"saturation", F1}, {"value", F1}});
@@ -142,6 +146,49 @@ bool paramBool(const rmd_node &n, const char *key, bool fb) {
     auto p = findParam(n, key);
     return p ? p->number_value != 0 : fb;
 }
+float paramNumber(const rmd_node &n, const char *key, float fb) {
+    auto p = findParam(n, key);
+    return (p && (p->kind == RMD_PARAM_NUMBER || p->kind == RMD_PARAM_BOOL)) ? (float)p->number_value : fb;
+}
+
+// The sky of a TEX_SKY node as MaterialBuilder.swift:329-349 resolves it: a
+// Hosek-Wilkie sky becomes a Nishita sky of the same sun direction (no disc,
+// air 2, dust 0.5, ozone 1, the sun at least 5 degrees up, radiance scaled by
+// 0.08); other types than Nishita are unsupported.  Missing parameters take
+// Blender's defaults.
+rmdsky::SkyOptions skyOptionsOf(const rmd_node &n) {
+    rmdsky::SkyOptions o;
+    std::string type = paramString(n, "sky_type", "NISHITA");
+    o.sunElevation = paramNumber(n, "sun_elevation", 15.0f * (float)M_PI / 180.0f);
+    o.sunRotation = paramNumber(n, "sun_rotation", 0.0f);
+    o.sunDisc = paramBool(n, "sun_disc", true);
+    o.sunSize = paramNumber(n, "sun_size", 0.545f * (float)M_PI / 180.0f);
+    o.sunIntensity = paramNumber(n, "sun_intensity", 1.0f);
+    o.altitude = paramNumber(n, "altitude", 0.0f);
+    o.airDensity = paramNumber(n, "air_density", 1.0f);
+    o.dustDensity = paramNumber(n, "dust_density", 1.0f);
+    o.ozoneDensity = paramNumber(n, "ozone_density", 1.0f);
+    o.scale = 1.0f;
+    if (type == "HOSEK_WILKIE") {
+        float dir[3] = {0.0f, 0.0f, 1.0f};
+        auto p = findParam(n, "sun_direction");
+        if (p && p->num_numbers >= 3)
+            for (int i = 0; i < 3; i++) dir[i] = p->numbers[i];
+        const float rotation = std::atan2(dir[0], dir[1]);
+        const float elevation = std::asin(dir[2]);
+        type = "NISHITA";
+        o.sunDisc = false;
+        o.airDensity = 2.0f;
+        o.dustDensity = 0.5f;
+        o.ozoneDensity = 1.0f;
+        o.sunElevation = std::max(elevation, 5.0f * (float)M_PI / 180.0f);
+        o.sunRotation = rotation;
+        o.scale = 0.08f;
+    }
+    if (type != "NISHITA") throw CodegenError{RMD_ERROR_CODEGEN_UNSUPPORTED, "TexSky: unsupported sky type '" + type + "'"};
+    return o;
+}
+
 // MaterialBuilder.swift:147-149
 std::string enumValue(const std::string &kernel, const std::string &ns, const std::string &v,
                       const std::vector<std::string> &known) {
@@ -310,6 +357,17 @@ Invocation makeInvocation(const rmd_node &n, Emitter &em, const TextureTable &te
                    enumValue("TexImage", "COLOR_SPACE", paramString(n, "colorspace", "sRGB"),
                              {"LINEAR", "SRGB", "NON_COLOR", "RAW", "XYZ", "FILMIC_LOG"}) +
                    ", kTexImage::PIXEL_FORMAT_" + (channels == 1 ? "R" : "RGBA") + ">";
+    } else if (t == "TEX_SKY") {  // MaterialBuilder.swift:329-388
+        const rmdsky::SkyOptions o = skyOptionsOf(n);
+        uint32_t slot, channels;
+        textures.lookup(skyTextureName(o.sunElevation, o.altitude, o.airDensity, o.dustDensity, o.ozoneDensity), slot,
+                        channels);
+        float data[10];
+        rmdsky::skyNodeData(o, data);
+        inv.kernel = "TexNishita";
+        inv.type = "TexNishita<" + std::to_string(slot) + ">";
+        for (int i = 0; i < 10; i++) inv.lines.push_back("@.data[" + std::to_string(i) + "] = " + em.lit(data[i]) + ";");
+        inv.lines.push_back("@.scale = " + em.lit(o.scale) + ";");
     } else if (t == "HUE_SAT") plain("HueSaturation");
     else if (t == "BRIGHTCONTRAST") plain("BrightnessContrast");
     else if (t == "BLACKBODY") plain("Blackbody");
@@ -558,6 +616,58 @@ void emitTable(const rmd_material *mats, int n, bool hoist, const std::string &p
 }
 
 }  // namespace
+
+std::string skyTextureName(float sunElevation, float altitude, float air, float dust, float ozone) {
+    char buf[256];
+    std::snprintf(buf, sizeof(buf), "@nishita:%a,%a,%a,%a,%a", (double)sunElevation, (double)altitude, (double)air,
+                  (double)dust, (double)ozone);
+    return buf;
+}
+
+bool parseSkyTextureName(const std::string &name, float v[5]) {
+    if (name.rfind("@nishita:", 0) != 0) return false;
+    const char *p = name.c_str() + 9;
+    for (int i = 0; i < 5; i++) {
+        char *end = nullptr;
+        v[i] = std::strtof(p, &end);
+        if (end == p) return false;
+        p = end;
+        if (i < 4) {
+            if (*p != ',') return false;
+            p++;
+        }
+    }
+    return *p == 0;
+}
+
+SceneTextures sceneTextures(const rmd_scene_desc *d) {
+    SceneTextures out;
+    for (int i = 0; i < d->num_textures; i++) out.list.push_back(d->textures[i]);
+    auto scan = [&](const rmd_material *mats, int count) {
+        for (int m = 0; m < count; m++)
+            for (int k = 0; k < mats[m].num_nodes; k++) {
+                const rmd_node &n = mats[m].nodes[k];
+                if (!n.type || std::string(n.type) != "TEX_SKY") continue;
+                const rmdsky::SkyOptions o = skyOptionsOf(n);
+                const std::string name =
+                    skyTextureName(o.sunElevation, o.altitude, o.airDensity, o.dustDensity, o.ozoneDensity);
+                if (std::find(out.generatedNames.begin(), out.generatedNames.end(), name) == out.generatedNames.end())
+                    out.generatedNames.push_back(name);
+            }
+    };
+    scan(d->surface_materials, d->num_surface_materials);
+    scan(d->light_materials, d->num_light_materials);
+    for (const std::string &name : out.generatedNames) {
+        rmd_texture t{};
+        t.name = name.c_str();
+        t.width = t.height = rmdsky::kSkyTextureSize;
+        t.channels = 4;
+        t.format = RMD_TEXTURE_F32;
+        t.data = nullptr;
+        out.list.push_back(t);
+    }
+    return out;
+}
 
 TextureTable TextureTable::of(const rmd_texture *textures, int count) {
     TextureTable t;

@@ -44,6 +44,23 @@ struct TextureTable {
     void lookup(const std::string &name, uint32_t &slot, uint32_t &numChannels) const;
 };
 
+// The textures a scene's materials read: the scene's own images, then one
+// generated 512 x 512 sky texture per distinct Nishita sky of its TEX_SKY
+// nodes (MaterialBuilder.swift:350-372, where SkyLoader fills the texture on
+// the host).  A generated entry has data == NULL and a name that encodes the
+// five parameters the texture depends on (skyTextureName); the library fills
+// its texels on the device.  Throws CodegenError for an unsupported sky type.
+struct SceneTextures {
+    std::vector<rmd_texture> list;
+    std::vector<std::string> generatedNames;
+};
+SceneTextures sceneTextures(const rmd_scene_desc *d);
+// "@nishita:" and the sun elevation, altitude, air, dust and ozone densities
+// as hexadecimal floats
+std::string skyTextureName(float sunElevation, float altitude, float air, float dust, float ozone);
+// parses a name made by skyTextureName; false for any other name
+bool parseSkyTextureName(const std::string &name, float v[5]);
+
 // Emits one function per distinct graph structure; literal inputs become
 // loads from a per-material parameter block when `hoist` is set, or inline
 // constants (the reference's code shape) otherwise.  Throws CodegenError.

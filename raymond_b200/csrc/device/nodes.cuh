@@ -470,6 +470,67 @@ struct TexImage {
     }
 };
 
+// The Nishita sky (nodes.hpp:774-870): radiance of direction `dir` from the
+// sky texture the scene generated for this node (rows: elevation, from the
+// horizon up with sqrt spacing; columns: azimuth), the sun disc between its
+// bottom and top colours with limb darkening, and below the horizon the
+// horizon row fading to black by -0.4; XYZ converted to linear RGB.
+// data: sun bottom and top XYZ, sun elevation, rotation, angular diameter
+// (-1 without a disc), intensity.
+RMD_HD float3 skyRadianceNishita(float3 dir, const float *data, const TextureView &texture) {
+    const float sunElevation = data[6], sunRotation = data[7], angularDiameter = data[8], sunIntensity = data[9];
+    const bool sunDisc = angularDiameter > 0.0f;
+    float3 xyzc = f3(0.0f);
+    const float theta = acosf(dir.z), phi = atan2f(dir.x, dir.y);  // sky_spherical_coordinates
+    if (dir.z >= 0.0f) {
+        const float lat = sunElevation, lon = sunRotation + 0.5f * M_PI_F;
+        const float3 sunDir = make_float3(cosf(lat) * cosf(lon), cosf(lat) * sinf(lon), sinf(lat));
+        const float sunAngle = 2.0f * atan2f(length(dir - sunDir), length(dir + sunDir));  // precise_angle
+        const float halfAngular = angularDiameter / 2.0f;
+        const float dirElevation = 0.5f * M_PI_F - theta;
+        if (sunAngle < halfAngular && sunDisc) {
+            const float3 bottom = make_float3(data[0], data[1], data[2]), top = make_float3(data[3], data[4], data[5]);
+            if (sunElevation - halfAngular > 0.0f) {
+                if (sunElevation + halfAngular > 0.0f) {
+                    const float y = ((dirElevation - sunElevation) / angularDiameter) + 0.5f;
+                    xyzc = (bottom + (top - bottom) * y) * sunIntensity;  // Metal mix
+                }
+            } else if (sunElevation + halfAngular > 0.0f) {
+                const float y = dirElevation / (sunElevation + halfAngular);
+                xyzc = (bottom + (top - bottom) * y) * sunIntensity;  // Metal mix
+            }
+            const float fraction = sunAngle / halfAngular;
+            xyzc = xyzc * (1.0f - 0.6f * (1.0f - sqrtf(1.0f - fraction * fraction)));  // limb darkening
+        } else {
+            float x = (phi + M_PI_F + sunRotation) / (2.0f * M_PI_F);
+            const float y = sqrtf(dirElevation / (0.5f * M_PI_F));
+            if (x > 1.0f) x = x - 1.0f;
+            xyzc = xyz(sampleLinearRepeat(texture, make_float2(x, y)));
+        }
+    } else if (dir.z >= -0.4f) {
+        const float mul = powf(1.0f + dir.z * 2.5f, 3.0f);  // black ground fade
+        float x = (phi + M_PI_F + sunRotation) / (2.0f * M_PI_F);
+        if (x > 1.0f) x = x - 1.0f;
+        xyzc = xyz(sampleLinearRepeat(texture, make_float2(x, 1e-3f))) * mul;
+    }
+    return xyz_to_rgb(xyzc);
+}
+
+// TexNishita (nodes.hpp:857-870); the texture slot holds the sky texture the
+// scene generated from the node's parameters (MaterialBuilder.swift:350-388)
+template <int TextureIndex>
+struct TexNishita {
+    float scale;
+    float3 vector;
+    float4 color;
+    float data[10];
+    RMD_HD void compute(const Context &ctx, const ShadingContext &shading) {
+        color = f4(scale * skyRadianceNishita(shading.wo * make_float3(1.0f, -1.0f, -1.0f), data,
+                                              ctx.textures[TextureIndex]),
+                   1.0f);
+    }
+};
+
 struct kMapping {
     enum Type { TYPE_MAPPING };  // the exporter writes the node's type, MAPPING, for every vector type
 };

@@ -12,7 +12,9 @@
 #include <cuda_runtime.h>
 
 #include <algorithm>
+#include <cstddef>
 #include <cmath>
+#include <cstring>
 #include <string>
 #include <vector>
 
@@ -620,6 +622,388 @@ __device__ bool tcForward(TcSmem &sm, int pipe, const GuideFeatures &f, float *o
     return true;
 }
 
+// ------------------------------------------------- tcgen05 training core
+// Training on the 5th-generation tensor cores.  A CTA of 128 threads takes
+// tiles of 128 records, one thread per record (M = 128).  Per tile:
+//
+//   forward   4 layers as in inference (A = the previous layer's rows, B = W);
+//             every thread keeps its record's ReLU masks, and the activations
+//             are also written transposed, [feature][record], for the weight
+//             gradients
+//   loss      each thread the gradient of its record's loss with respect to
+//             the 48 raw outputs (CUDA cores), as rows and transposed
+//   backward  per layer l = 3..0: dW_l += delta_l^T . a_(l-1) (A = delta
+//             transposed, B = the activations transposed, K = the 128
+//             records), accumulated in tensor memory over the CTA's tiles;
+//             and delta_(l-1) = (delta_l . W_l) masked by ReLU' (A = delta
+//             rows, B = W_l transposed), both issued together
+//
+// All operands are in shared memory in the canonical K-major layout.  The
+// weight gradients' M is the layer's output width (64, or 48) padded to 128:
+// rows past the width read whatever follows the delta buffer, and their
+// products land in tensor-memory lanes that are never read.  Tensor memory:
+// columns 0..63 the layer accumulator, then dW0 (160), dW1, dW2, dW3 (64
+// each).  Bias gradients (column sums of the deltas) are reduced across each
+// warp with shuffles into shared memory.  At the end warps 0 and 1 (lanes
+// 0..63, the output features) read the CTA's weight gradient out of tensor
+// memory into the CTA's slot of net.partials.
+constexpr int kTrThreads = 128;
+constexpr uint32_t kTrTmemCols = 512;
+// tensor-memory column of dW_l: dW0 at 64 (160 wide), dW1 224, dW2 288, dW3 352
+__device__ __forceinline__ uint32_t trColDw(int l) { return l == 0 ? 64u : 224u + 64u * (uint32_t)(l - 1); }
+
+struct TrainSmem {
+    uint16_t w0[GUIDE_HIDDEN * GUIDE_INPUTS];  // [out][in], canonical K-major (K = in)
+    uint16_t w1[GUIDE_HIDDEN * GUIDE_HIDDEN];
+    uint16_t w2[GUIDE_HIDDEN * GUIDE_HIDDEN];
+    uint16_t w3[GUIDE_OUTPUTS * GUIDE_HIDDEN];
+    uint16_t w1t[GUIDE_HIDDEN * GUIDE_HIDDEN];  // [in][out], canonical (K = out)
+    uint16_t w2t[GUIDE_HIDDEN * GUIDE_HIDDEN];
+    uint16_t w3t[GUIDE_HIDDEN * GUIDE_OUTPUTS];
+    uint16_t dT[GUIDE_HIDDEN * kTrThreads];     // delta transposed [out][record]; must precede xT (see above)
+    uint16_t xT[GUIDE_INPUTS * kTrThreads];     // inputs transposed [in][record]
+    uint16_t hT[3][GUIDE_HIDDEN * kTrThreads];  // hidden activations transposed
+    uint16_t rowA[kTrThreads * GUIDE_INPUTS];   // input rows, then layer-2 inputs; deltas in the backward pass
+    uint16_t rowB[kTrThreads * GUIDE_HIDDEN];   // layer-1 inputs, then layer-3 inputs; deltas
+    float b[3 * GUIDE_HIDDEN + GUIDE_OUTPUTS];
+    float db[3 * GUIDE_HIDDEN + GUIDE_OUTPUTS];  // the CTA's bias gradient
+    unsigned long long mbar;
+    uint32_t tmemBase;
+    int failed;
+};
+static_assert(sizeof(TrainSmem) <= 232448, "training shared memory exceeds the per-CTA limit");
+static_assert(offsetof(TrainSmem, xT) == offsetof(TrainSmem, dT) + sizeof(uint16_t) * GUIDE_HIDDEN * kTrThreads,
+              "the padded delta rows of a weight gradient (128 rows from dT) must read inside shared memory");
+
+// copies a row-major [rows][cols] bf16 matrix transposed into the canonical
+// layout of a [cols][rows] operand (K = rows)
+__device__ void loadCanonicalT(uint16_t *dst, const uint16_t *src, int rows, int cols) {
+    unsigned char *d = reinterpret_cast<unsigned char *>(dst);
+    for (int i = threadIdx.x; i < rows * cols; i += blockDim.x) {
+        const int r = i / cols, c = i - r * cols;
+        *reinterpret_cast<uint16_t *>(d + canonOffset(c, r, rows)) = __ldg(&src[i]);
+    }
+}
+
+// element (row, k) of a canonical operand with K = 128 records: row = feature, k = record
+__device__ __forceinline__ uint16_t *tElem(uint16_t *base, int feature, int record) {
+    return reinterpret_cast<uint16_t *>(reinterpret_cast<unsigned char *>(base) + canonOffset(feature, record, kTrThreads));
+}
+
+// Sum over the warp's 32 lanes of each of v[0..31]: afterwards lane l holds
+// the sum of column l in v[0] (a butterfly that halves the columns a lane
+// keeps at every step: 31 shuffles for 32 columns).
+__device__ __forceinline__ float warpColumnSums(float v[32], int lane) {
+#pragma unroll
+    for (int s = 16, n = 32; s >= 1; s >>= 1, n >>= 1) {
+        const bool upper = (lane & s) != 0;
+#pragma unroll
+        for (int k = 0; k < n / 2; k++) {
+            const float send = upper ? v[k] : v[k + n / 2];
+            const float keep = upper ? v[k + n / 2] : v[k];
+            v[k] = keep + __shfl_xor_sync(0xffffffffu, send, s);
+        }
+    }
+    return v[0];
+}
+
+// adds the column sums of 32 delta values per thread to db[c0..c0+32)
+__device__ __forceinline__ void addBiasGrad(float *db, int c0, float v[32], int lane) {
+    const float sum = warpColumnSums(v, lane);
+    atomicAdd(&db[c0 + lane], sum);
+}
+
+// issues D = A . B^T over K (canonical operands, sbo = K / 8 * 128), committed later
+__device__ __forceinline__ void trMma(uint32_t tmem, const void *a, const void *b, int K, int N, bool accumulate) {
+    const uint32_t idesc = ummaInstr(kTrThreads, N);
+    const uint32_t aBase = smemU32(a), bBase = smemU32(b), sbo = (uint32_t)(K / 8) * 128u;
+    for (int kb = 0; kb < K / 16; kb++)
+        umma(tmem, ummaDesc(aBase + kb * 256u, sbo), ummaDesc(bBase + kb * 256u, sbo), idesc,
+             (accumulate || kb > 0) ? 1u : 0u);
+}
+
+// makes the threads' shared-memory writes visible to the tensor core and syncs the CTA
+__device__ __forceinline__ void trPublish() {
+    asyncProxyFence();
+    tcFenceBefore();
+    __syncthreads();
+    tcFenceAfter();
+}
+
+// thread 0 commits the issued MMAs; everyone waits.  False if the wait expired.
+__device__ bool trCommitWait(TrainSmem &sm, uint32_t &phase) {
+    const uint32_t mbar = smemU32(&sm.mbar);
+    if (threadIdx.x == 0) ummaCommit(mbar);
+    const bool ok = mbarWait(mbar, phase);
+    phase ^= 1u;
+    tcFenceAfter();
+    if (!ok) atomicExch(&sm.failed, 1);
+    __syncthreads();
+    return sm.failed == 0;
+}
+
+// Epilogue of a forward hidden layer: bias + ReLU of the thread's row of the
+// accumulator, written as the next layer's A row and transposed (hT); returns
+// the ReLU mask (bit c: column c positive).
+__device__ uint64_t trHiddenEpilogue(TrainSmem &sm, uint32_t taddr, const float *bias, uint16_t *rowOut,
+                                     uint16_t *tOut, int row) {
+    uint64_t mask = 0;
+    float v[32];
+#pragma unroll
+    for (int half = 0; half < 2; half++) {
+        tmemLd32(taddr + 32u * half, v);
+        tmemLdWait();
+#pragma unroll
+        for (int c = 0; c < 32; c += 8) {
+            uint32_t q[4];
+#pragma unroll
+            for (int k = 0; k < 4; k++)
+                q[k] = biasReluBf16x2(v[c + 2 * k], v[c + 2 * k + 1],
+                                      *reinterpret_cast<const float2 *>(&bias[32 * half + c + 2 * k]));
+            *reinterpret_cast<uint4 *>(reinterpret_cast<unsigned char *>(rowOut) +
+                                       canonOffset(row, 32 * half + c, GUIDE_HIDDEN)) = make_uint4(q[0], q[1], q[2], q[3]);
+#pragma unroll
+            for (int k = 0; k < 4; k++) {
+                const int col = 32 * half + c + 2 * k;
+                const uint16_t lo = (uint16_t)(q[k] & 0xffffu), hi = (uint16_t)(q[k] >> 16);
+                *tElem(tOut, col, row) = lo;
+                *tElem(tOut, col + 1, row) = hi;
+                mask |= (uint64_t)(lo != 0) << col;
+                mask |= (uint64_t)(hi != 0) << (col + 1);
+            }
+        }
+    }
+    return mask;
+}
+
+// Epilogue of a backward layer: the thread's row of delta . W masked by the
+// ReLU mask, as BF16 delta rows (when rowOut) and transposed; bias gradient
+// into db[0..64).
+__device__ void trDeltaEpilogue(TrainSmem &sm, uint32_t taddr, uint64_t mask, uint16_t *rowOut, float *db, int row,
+                                int lane) {
+    float v[32];
+#pragma unroll
+    for (int half = 0; half < 2; half++) {
+        tmemLd32(taddr + 32u * half, v);
+        tmemLdWait();
+#pragma unroll
+        for (int c = 0; c < 32; c += 2) {
+            const int col = 32 * half + c;
+            const float a = ((mask >> col) & 1u) ? v[c] : 0.0f;
+            const float b = ((mask >> (col + 1)) & 1u) ? v[c + 1] : 0.0f;
+            const uint16_t lo = cvtBf16(a), hi = cvtBf16(b);
+            if (rowOut)
+                *reinterpret_cast<uint32_t *>(reinterpret_cast<unsigned char *>(rowOut) +
+                                              canonOffset(row, col, GUIDE_HIDDEN)) = (uint32_t)lo | ((uint32_t)hi << 16);
+            *tElem(sm.dT, col, row) = lo;
+            *tElem(sm.dT, col + 1, row) = hi;
+            v[c] = fromBf16(lo);  // the bias gradient sums the rounded deltas the MMAs use
+            v[c + 1] = fromBf16(hi);
+        }
+        addBiasGrad(db, 32 * half, v, lane);
+    }
+}
+
+// The gradient of the mean loss over a batch of records on the tensor cores:
+// each CTA writes its gradient (weights and biases) to its slot of
+// net.partials.  On an expired wait the CTA sets ERR_GUIDE_TIMEOUT in
+// *errors and writes a zero gradient.
+__global__ void __launch_bounds__(kTrThreads, 1) k_guide_train_tc(RecordBatch batch, const float *sumY, GuideNetView net,
+                                                                float *lossOut, uint32_t *errors) {
+    extern __shared__ __align__(16) unsigned char smem[];
+    TrainSmem &sm = *reinterpret_cast<TrainSmem *>(smem);
+    const int row = threadIdx.x, warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    // set-up: weights (forward and transposed), biases, mbarrier, tensor memory
+    loadCanonical(sm.w0, net.w[0], GUIDE_HIDDEN, GUIDE_INPUTS);
+    loadCanonical(sm.w1, net.w[1], GUIDE_HIDDEN, GUIDE_HIDDEN);
+    loadCanonical(sm.w2, net.w[2], GUIDE_HIDDEN, GUIDE_HIDDEN);
+    loadCanonical(sm.w3, net.w[3], GUIDE_OUTPUTS, GUIDE_HIDDEN);
+    loadCanonicalT(sm.w1t, net.w[1], GUIDE_HIDDEN, GUIDE_HIDDEN);
+    loadCanonicalT(sm.w2t, net.w[2], GUIDE_HIDDEN, GUIDE_HIDDEN);
+    loadCanonicalT(sm.w3t, net.w[3], GUIDE_OUTPUTS, GUIDE_HIDDEN);
+    for (int i = threadIdx.x; i < 3 * GUIDE_HIDDEN + GUIDE_OUTPUTS; i += blockDim.x) {
+        const int l = min(i / GUIDE_HIDDEN, 3);
+        sm.b[i] = __ldg(&net.b[l][i - l * GUIDE_HIDDEN]);
+        sm.db[i] = 0.0f;
+    }
+    if (threadIdx.x == 0) {
+        sm.failed = 0;
+        asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;\n" ::"r"(smemU32(&sm.mbar)), "r"(1) : "memory");
+        asm volatile("fence.mbarrier_init.release.cluster;\n" ::: "memory");
+    }
+    if (warp == 0) {
+        asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;\n" ::"r"(smemU32(&sm.tmemBase)),
+                     "r"(kTrTmemCols)
+                     : "memory");
+        asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;\n" ::: "memory");
+    }
+    trPublish();
+    const uint32_t tmem = sm.tmemBase;
+    const uint32_t taddr = tmem + ((uint32_t)(row & ~31) << 16);  // this warp's lanes, work columns
+    const uint32_t n = batch.n;
+    const float scale = 1.0f / (float)n;
+    const float invMeanY = sumY[0] > 0.0f ? (float)n / sumY[0] : 0.0f;
+    const uint32_t tiles = (n + kTrThreads - 1) / kTrThreads;
+    float lossSum = 0.0f;
+    uint32_t phase = 0;
+    bool first = true, ok = true;
+    for (uint32_t tile = blockIdx.x; tile < tiles && ok; tile += gridDim.x) {
+        const uint32_t r = tile * kTrThreads + row;
+        GuideRecord rc = {};
+        const bool valid = r < n;
+        if (valid) rc = batch.pick(r);
+        // inputs: one-blob rows (two non-zero bins per feature) and their transpose
+        unsigned char *aRow = reinterpret_cast<unsigned char *>(sm.rowA);
+#pragma unroll
+        for (int c = 0; c < GUIDE_INPUTS / 8; c++)
+            *reinterpret_cast<uint4 *>(aRow + canonOffset(row, 8 * c, GUIDE_INPUTS)) = make_uint4(0u, 0u, 0u, 0u);
+        for (int i = threadIdx.x; i < GUIDE_INPUTS * kTrThreads / 8; i += blockDim.x)
+            reinterpret_cast<uint4 *>(sm.xT)[i] = make_uint4(0u, 0u, 0u, 0u);
+        __syncthreads();
+        if (valid) {
+#pragma unroll
+            for (int feature = 0; feature < 7; feature++) {
+                const int bins = feature < 3 ? 32 : 16;
+                const int firstCol = feature < 3 ? 32 * feature : 96 + 16 * (feature - 3);
+                const float v = rc.features[feature];
+                const int b = (int)floorf(v * (float)bins - 0.5f);
+#pragma unroll
+                for (int k = 0; k < 2; k++) {
+                    const int bin = b + k;
+                    if (bin >= 0 && bin < bins) {
+                        const uint16_t x = cvtBf16(oneBlob(v, bins, bin));
+                        *reinterpret_cast<uint16_t *>(aRow + canonOffset(row, firstCol + bin, GUIDE_INPUTS)) = x;
+                        *tElem(sm.xT, firstCol + bin, row) = x;
+                    }
+                }
+            }
+        }
+        // forward
+        trPublish();
+        if (threadIdx.x == 0) trMma(tmem, sm.rowA, sm.w0, GUIDE_INPUTS, GUIDE_HIDDEN, false);
+        if (!(ok = trCommitWait(sm, phase))) break;
+        const uint64_t m0 = trHiddenEpilogue(sm, taddr, sm.b, sm.rowB, sm.hT[0], row);
+        trPublish();
+        if (threadIdx.x == 0) trMma(tmem, sm.rowB, sm.w1, GUIDE_HIDDEN, GUIDE_HIDDEN, false);
+        if (!(ok = trCommitWait(sm, phase))) break;
+        const uint64_t m1 = trHiddenEpilogue(sm, taddr, sm.b + GUIDE_HIDDEN, sm.rowA, sm.hT[1], row);
+        trPublish();
+        if (threadIdx.x == 0) trMma(tmem, sm.rowA, sm.w2, GUIDE_HIDDEN, GUIDE_HIDDEN, false);
+        if (!(ok = trCommitWait(sm, phase))) break;
+        const uint64_t m2 = trHiddenEpilogue(sm, taddr, sm.b + 2 * GUIDE_HIDDEN, sm.rowB, sm.hT[2], row);
+        trPublish();
+        if (threadIdx.x == 0) trMma(tmem, sm.rowB, sm.w3, GUIDE_HIDDEN, GUIDE_OUTPUTS, false);
+        if (!(ok = trCommitWait(sm, phase))) break;
+        float o[GUIDE_OUTPUTS];
+        tmemLd32(taddr, o);
+        tmemLd16(taddr + 32u, o + 32);
+        tmemLdWait();
+        const float2 *b4 = reinterpret_cast<const float2 *>(sm.b + 3 * GUIDE_HIDDEN);
+#pragma unroll
+        for (int c = 0; c < GUIDE_OUTPUTS / 2; c++) addBias2(o[2 * c], o[2 * c + 1], b4[c]);
+        // loss gradient of the record (zero for the padding rows of the last tile)
+        uint16_t d3[GUIDE_OUTPUTS];
+        if (valid) {
+            const float y = fminf(rc.y * invMeanY, 100.0f);
+            lossSum += lossGradient(o, make_float3(rc.dir[0], rc.dir[1], rc.dir[2]), rc.pdfBsdf, y, scale, d3);
+        } else {
+#pragma unroll
+            for (int c = 0; c < GUIDE_OUTPUTS; c++) d3[c] = 0;
+        }
+        {
+            unsigned char *dRow = reinterpret_cast<unsigned char *>(sm.rowA);
+#pragma unroll
+            for (int c = 0; c < GUIDE_OUTPUTS; c += 8)
+                *reinterpret_cast<uint4 *>(dRow + canonOffset(row, c, GUIDE_OUTPUTS)) =
+                    make_uint4(pack2(d3[c], d3[c + 1]), pack2(d3[c + 2], d3[c + 3]), pack2(d3[c + 4], d3[c + 5]),
+                               pack2(d3[c + 6], d3[c + 7]));
+            float v[32];
+#pragma unroll
+            for (int c = 0; c < 32; c++) {
+                *tElem(sm.dT, c, row) = d3[c];
+                v[c] = fromBf16(d3[c]);
+            }
+            addBiasGrad(sm.db + 3 * GUIDE_HIDDEN, 0, v, lane);
+#pragma unroll
+            for (int c = 0; c < 32; c++) v[c] = 0.0f;
+#pragma unroll
+            for (int c = 32; c < GUIDE_OUTPUTS; c++) {
+                *tElem(sm.dT, c, row) = d3[c];
+                v[c - 32] = fromBf16(d3[c]);
+            }
+            const float sum = warpColumnSums(v, lane);
+            if (lane < GUIDE_OUTPUTS - 32) atomicAdd(&sm.db[3 * GUIDE_HIDDEN + 32 + lane], sum);
+        }
+        // backward: layer 3 (dW3, delta2), 2 (dW2, delta1), 1 (dW1, delta0), 0 (dW0)
+        trPublish();
+        if (threadIdx.x == 0) {
+            trMma(tmem + trColDw(3), sm.dT, sm.hT[2], kTrThreads, GUIDE_HIDDEN, !first);
+            trMma(tmem, sm.rowA, sm.w3t, GUIDE_OUTPUTS, GUIDE_HIDDEN, false);
+        }
+        if (!(ok = trCommitWait(sm, phase))) break;
+        trDeltaEpilogue(sm, taddr, m2, sm.rowB, sm.db + 2 * GUIDE_HIDDEN, row, lane);
+        trPublish();
+        if (threadIdx.x == 0) {
+            trMma(tmem + trColDw(2), sm.dT, sm.hT[1], kTrThreads, GUIDE_HIDDEN, !first);
+            trMma(tmem, sm.rowB, sm.w2t, GUIDE_HIDDEN, GUIDE_HIDDEN, false);
+        }
+        if (!(ok = trCommitWait(sm, phase))) break;
+        trDeltaEpilogue(sm, taddr, m1, sm.rowA, sm.db + GUIDE_HIDDEN, row, lane);
+        trPublish();
+        if (threadIdx.x == 0) {
+            trMma(tmem + trColDw(1), sm.dT, sm.hT[0], kTrThreads, GUIDE_HIDDEN, !first);
+            trMma(tmem, sm.rowA, sm.w1t, GUIDE_HIDDEN, GUIDE_HIDDEN, false);
+        }
+        if (!(ok = trCommitWait(sm, phase))) break;
+        trDeltaEpilogue(sm, taddr, m0, nullptr, sm.db, row, lane);
+        trPublish();
+        if (threadIdx.x == 0) trMma(tmem + trColDw(0), sm.dT, sm.xT, kTrThreads, GUIDE_INPUTS, !first);
+        if (!(ok = trCommitWait(sm, phase))) break;
+        first = false;
+    }
+    // the CTA's gradient: weights from tensor memory (lanes = output features), biases from shared memory
+    float *part = net.partials + (size_t)blockIdx.x * GUIDE_PARAMS;
+    const bool have = ok && !first;
+    if (warp < 2) {
+        const int o = row;  // output feature = tensor-memory lane
+        const uint32_t lanes = (uint32_t)(warp * 32) << 16;
+        const int width[4] = {GUIDE_INPUTS, GUIDE_HIDDEN, GUIDE_HIDDEN, GUIDE_HIDDEN};
+        const int outs[4] = {GUIDE_HIDDEN, GUIDE_HIDDEN, GUIDE_HIDDEN, GUIDE_OUTPUTS};
+#pragma unroll 1
+        for (int l = 0; l < 4; l++) {
+#pragma unroll 1
+            for (int c0 = 0; c0 < width[l]; c0 += 32) {
+                float v[32];
+                if (have) {
+                    tmemLd32(tmem + lanes + trColDw(l) + (uint32_t)c0, v);
+                    tmemLdWait();
+                } else {
+#pragma unroll
+                    for (int c = 0; c < 32; c++) v[c] = 0.0f;
+                }
+                if (o < outs[l])
+#pragma unroll
+                    for (int c = 0; c < 32; c++) part[net.wOffset[l] + o * width[l] + c0 + c] = v[c];
+            }
+        }
+    }
+    __syncthreads();
+    for (int i = threadIdx.x; i < 3 * GUIDE_HIDDEN + GUIDE_OUTPUTS; i += blockDim.x) {
+        const int l = min(i / GUIDE_HIDDEN, 3);
+        part[net.bOffset[l] + i - l * GUIDE_HIDDEN] = have ? sm.db[i] : 0.0f;
+    }
+    for (int off = 16; off > 0; off >>= 1) lossSum += __shfl_xor_sync(0xffffffffu, lossSum, off);
+    if (lane == 0 && lossOut && ok) atomicAdd(lossOut, lossSum * scale);
+    if (!ok && threadIdx.x == 0 && errors) atomicOr(errors, ERR_GUIDE_TIMEOUT);
+    // teardown: a last bounded wait for work in flight after an expired wait, then free tensor memory
+    if (!ok) mbarWait(smemU32(&sm.mbar), phase);
+    tcFenceBefore();
+    __syncthreads();
+    tcFenceAfter();
+    if (warp == 0)
+        asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;\n" ::"r"(tmem), "r"(kTrTmemCols) : "memory");
+}
+
 // ------------------------------------------------------------------ kernels
 // The guide's input features of this iteration's hits (shading order
 // 0..nHit-1): position on the ray, the triangle's geometric normal, the
@@ -878,13 +1262,10 @@ __global__ void k_guide_mixture_test(const float *outputs, const float *u, int n
 
 using namespace rmd;
 
-size_t rmdGuideSharedBytes(bool training) {
-    return training ? kWarps * sizeof(WarpScratch) + GUIDE_PARAMS * sizeof(float) + sizeof(TrainWeights)
-                    : sizeof(TcSmem);
-}
+size_t rmdGuideSharedBytes(bool training) { return training ? sizeof(TrainSmem) : sizeof(TcSmem); }
 
 cudaError_t rmdGuideConfigure() {
-    cudaError_t e = cudaFuncSetAttribute(k_guide_train, cudaFuncAttributeMaxDynamicSharedMemorySize,
+    cudaError_t e = cudaFuncSetAttribute(k_guide_train_tc, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                          (int)rmdGuideSharedBytes(true));
     if (e != cudaSuccess) return e;
     e = cudaFuncSetAttribute(k_guide_infer, cudaFuncAttributeMaxDynamicSharedMemorySize,
@@ -906,16 +1287,23 @@ cudaError_t rmdLaunchGuideInfer(const Context &ctx, const PathPool &pool, Counte
 }
 
 cudaError_t rmdLaunchGuideTrain(const GuideRecord *rec, uint32_t total, uint32_t n, uint32_t seed,
-                                const GuideNetView &net, float *scratch, int blocks, float lr, int step, cudaStream_t s) {
+                                const GuideNetView &net, float *scratch, int blocks, float lr, int step,
+                                uint32_t *errors, cudaStream_t s) {
     // scratch[0]: sum of the target weights, scratch[1]: mean loss
     cudaError_t e = cudaMemsetAsync(scratch, 0, 2 * sizeof(float), s);
     if (e != cudaSuccess || total == 0) return e;
     RecordBatch batch{rec, total, std::min(n, total), seed};
     k_guide_mean_y<<<256, 256, 0, s>>>(batch, scratch);
     if ((e = cudaGetLastError()) != cudaSuccess) return e;
-    blocks = std::max(1, std::min(blocks, GUIDE_TRAIN_MAX_BLOCKS));
-    k_guide_train<<<blocks, 32 * kWarps, rmdGuideSharedBytes(true), s>>>(batch, scratch, net, scratch + 1);
+    // one CTA per tile of 128 records, at most `blocks` (each CTA then takes several tiles)
+    const int tiles = (int)((batch.n + kTrThreads - 1) / kTrThreads);
+    blocks = std::max(1, std::min(std::min(blocks, tiles), GUIDE_TRAIN_MAX_BLOCKS));
+    k_guide_train_tc<<<blocks, kTrThreads, rmdGuideSharedBytes(true), s>>>(batch, scratch, net, scratch + 1, errors);
     if ((e = cudaGetLastError()) != cudaSuccess) return e;
+    return rmdLaunchGuideAdam(net, blocks, lr, step, s);
+}
+
+cudaError_t rmdLaunchGuideAdam(const GuideNetView &net, int blocks, float lr, int step, cudaStream_t s) {
     const float beta1 = 0.9f, beta2 = 0.999f;
     const float corr1 = 1.0f / (1.0f - powf(beta1, (float)step)), corr2 = 1.0f / (1.0f - powf(beta2, (float)step));
     k_guide_adam<<<(GUIDE_PARAMS + 255) / 256, 256, 0, s>>>(net, blocks, lr, beta1, beta2, 1e-8f, corr1, corr2);
@@ -931,15 +1319,19 @@ cudaError_t rmdLaunchGuideForwardTest(const float *features, uint32_t n, const G
 }
 
 cudaError_t rmdLaunchGuideGradientTest(const GuideRecord *rec, uint32_t n, const GuideNetView &net, float *scratch,
-                                       cudaStream_t s) {
-    cudaError_t e = cudaMemsetAsync(scratch, 0, 2 * sizeof(float), s);
+                                       int blocks, cudaStream_t s) {
+    // scratch[0]: sum of the targets, [1]: mean loss, [2]: error flags
+    cudaError_t e = cudaMemsetAsync(scratch, 0, 3 * sizeof(float), s);
     if (e != cudaSuccess || n == 0) return e;
     RecordBatch batch{rec, n, n, 0};
     k_guide_mean_y<<<256, 256, 0, s>>>(batch, scratch);
     if ((e = cudaGetLastError()) != cudaSuccess) return e;
-    k_guide_train<<<64, 32 * kWarps, rmdGuideSharedBytes(true), s>>>(batch, scratch, net, scratch + 1);
+    const int tiles = (int)((n + kTrThreads - 1) / kTrThreads);
+    blocks = std::max(1, std::min(std::min(blocks, tiles), GUIDE_TRAIN_MAX_BLOCKS));
+    k_guide_train_tc<<<blocks, kTrThreads, rmdGuideSharedBytes(true), s>>>(batch, scratch, net, scratch + 1,
+                                                                           reinterpret_cast<uint32_t *>(scratch + 2));
     if ((e = cudaGetLastError()) != cudaSuccess) return e;
-    k_guide_reduce<<<(GUIDE_PARAMS + 255) / 256, 256, 0, s>>>(net, 64);
+    k_guide_reduce<<<(GUIDE_PARAMS + 255) / 256, 256, 0, s>>>(net, blocks);
     return cudaGetLastError();
 }
 
@@ -1117,15 +1509,44 @@ extern "C" rmd_status rmd_test_guide_gradient(const float *params, const float *
     if ((e = net.setParams(params, 0)) != cudaSuccess) return guideFail(e, "guide params");
     DeviceArray r;
     if ((e = r.upload(records, (size_t)n * sizeof(GuideRecord))) != cudaSuccess) return guideFail(e, "guide records");
+    int sms = 148;
+    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, 0);
     if ((e = rmdLaunchGuideGradientTest((const GuideRecord *)r.p, (uint32_t)n,
-                                        net.view(make_float3(0, 0, 0), make_float3(1, 1, 1)), net.scratch, 0)) !=
+                                        net.view(make_float3(0, 0, 0), make_float3(1, 1, 1)), net.scratch, sms, 0)) !=
             cudaSuccess ||
         (e = cudaMemcpy(grad, net.grad, GUIDE_PARAMS * sizeof(float), cudaMemcpyDeviceToHost)) != cudaSuccess)
         return guideFail(e, "guide gradient");
-    float s[2];
+    float s[3];
     if ((e = cudaMemcpy(s, net.scratch, sizeof(s), cudaMemcpyDeviceToHost)) != cudaSuccess)
         return guideFail(e, "guide loss");
+    uint32_t flags;
+    std::memcpy(&flags, &s[2], sizeof(flags));
+    if (flags) return rmdhost::setLastError(RMD_ERROR_WATCHDOG, "guide training: a tensor-core wait expired");
     if (loss) *loss = s[1];
+    return RMD_OK;
+}
+
+extern "C" rmd_status rmd_test_guide_adam(const float *params, const float *grad, const float *m, const float *v,
+                                          int32_t step, float lr, float *params_out, float *m_out, float *v_out,
+                                          uint16_t *bf16_out) {
+    if (!params || !grad || !m || !v || step < 1 || !params_out || !m_out || !v_out || !bf16_out)
+        return rmdhost::setLastError(RMD_ERROR_INVALID_ARGUMENT, "rmd_test_guide_adam: invalid arguments");
+    rmdhost::GuideNet net;
+    cudaError_t e;
+    const size_t pb = GUIDE_PARAMS * sizeof(float);
+    if ((e = net.allocate()) != cudaSuccess) return guideFail(e, "guide allocate");
+    if ((e = net.setParams(params, 0)) != cudaSuccess) return guideFail(e, "guide params");
+    if ((e = cudaMemcpy(net.grad, grad, pb, cudaMemcpyHostToDevice)) != cudaSuccess ||
+        (e = cudaMemcpy(net.adamM, m, pb, cudaMemcpyHostToDevice)) != cudaSuccess ||
+        (e = cudaMemcpy(net.adamV, v, pb, cudaMemcpyHostToDevice)) != cudaSuccess ||
+        (e = rmdLaunchGuideAdam(net.view(make_float3(0, 0, 0), make_float3(1, 1, 1)), 0, lr, step, 0)) !=
+            cudaSuccess ||
+        (e = cudaMemcpy(params_out, net.master, pb, cudaMemcpyDeviceToHost)) != cudaSuccess ||
+        (e = cudaMemcpy(m_out, net.adamM, pb, cudaMemcpyDeviceToHost)) != cudaSuccess ||
+        (e = cudaMemcpy(v_out, net.adamV, pb, cudaMemcpyDeviceToHost)) != cudaSuccess ||
+        (e = cudaMemcpy(bf16_out, net.weightsBf16, GUIDE_WEIGHTS * sizeof(uint16_t), cudaMemcpyDeviceToHost)) !=
+            cudaSuccess)
+        return guideFail(e, "guide adam");
     return RMD_OK;
 }
 

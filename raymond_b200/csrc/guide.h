@@ -40,15 +40,20 @@ cudaError_t rmdLaunchGuideInfer(const rmd::Context &ctx, const rmd::PathPool &po
 // One Adam step (`step` counts from 1) on the mean loss over a batch of n
 // records drawn from the `total` stored ones (all of them when n >= total;
 // `seed` varies the draw)
+// (tensor cores: one CTA per 128 records, at most `blocks`); an expired
+// tensor-core wait sets ERR_GUIDE_TIMEOUT in *errors
 cudaError_t rmdLaunchGuideTrain(const rmd::GuideRecord *rec, uint32_t total, uint32_t n, uint32_t seed,
                                 const rmd::GuideNetView &net, float *scratch, int blocks, float lr, int step,
-                                cudaStream_t s);
+                                uint32_t *errors, cudaStream_t s);
+// Adam (beta 0.9 / 0.999, eps 1e-8, `step` from 1) on net.grad plus the first
+// `blocks` per-CTA gradients; refreshes the BF16 weights and clears net.grad
+cudaError_t rmdLaunchGuideAdam(const rmd::GuideNetView &net, int blocks, float lr, int step, cudaStream_t s);
 // status[0] = 1 if a tensor-core wait expired
 cudaError_t rmdLaunchGuideForwardTest(const float *features, uint32_t n, const rmd::GuideNetView &net, float *out,
                                       int *status, cudaStream_t s);
-// gradient only (no Adam step): net.grad += d(mean loss); scratch[1] = mean loss
+// gradient only (no Adam step): net.grad += d(mean loss); scratch[1] = mean loss, scratch[2] error flags
 cudaError_t rmdLaunchGuideGradientTest(const rmd::GuideRecord *rec, uint32_t n, const rmd::GuideNetView &net,
-                                       float *scratch, cudaStream_t s);
+                                       float *scratch, int blocks, cudaStream_t s);
 
 namespace rmdhost {
 

@@ -7,6 +7,7 @@
 #include "device/traverse.cuh"
 #include "device/wavefront.cuh"
 #include "kernels.h"
+#include "sky.h"
 
 namespace rmd {
 
@@ -334,6 +335,21 @@ __global__ void k_film_resolve(const float4 *film, const double *film64, int fp6
     if (channels == 4) o[3] = 1.0f;
 }
 
+// ------------------------------------------------------------- sky texture
+// SKY_nishita_skymodel_precompute_texture (host/sky/sky_nishita.cpp:295-341)
+// on the device: texel (x, y) of the left half and its mirror image.
+__global__ void k_sky_texture(float4 *texels, int width, int height, float sunElevation, float altitude, float air,
+                              float dust, float ozone) {
+    const int half = width / 2;
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= half * height) return;
+    const int y = i / half, x = i - y * half;
+    const rmdsky::V3 c = rmdsky::skyTexel(x, y, width, height, sunElevation, altitude, air, dust, ozone);
+    const float4 v = make_float4(c.x, c.y, c.z, 1.0f);
+    texels[(size_t)y * width + x] = v;
+    texels[(size_t)y * width + (width - x - 1)] = v;
+}
+
 // ------------------------------------------------------------- test hooks
 __global__ void k_debug_prng(uint32_t mode, uint64_t a, uint64_t b, int n, float *out) {
     if (blockIdx.x != 0 || threadIdx.x != 0) return;
@@ -416,5 +432,13 @@ cudaError_t rmdLaunchDebugPrng(uint32_t mode, uint64_t a, uint64_t b, int n, flo
 cudaError_t rmdLaunchDebugTrace(const WideNode *nodes, const float4 *tris, const float *rays, int n, int any, float *out,
                                 uint32_t *inst, uint32_t *errors, cudaStream_t s) {
     k_debug_trace<<<(n + 127) / 128, 128, 0, s>>>(nodes, tris, rays, n, any, out, inst, errors);
+    return cudaGetLastError();
+}
+cudaError_t rmdLaunchSkyTexture(float4 *texels, uint32_t width, uint32_t height, float sunElevation, float altitude,
+                                float air, float dust, float ozone, cudaStream_t s) {
+    const uint32_t n = width / 2 * height;
+    if (n == 0) return cudaSuccess;
+    k_sky_texture<<<(n + 127) / 128, 128, 0, s>>>(texels, (int)width, (int)height, sunElevation, altitude, air, dust,
+                                                  ozone);
     return cudaGetLastError();
 }

@@ -25,3 +25,7 @@ cudaError_t rmdLaunchFilmResolve(const float4 *film, const double *film64, int f
 cudaError_t rmdLaunchDebugPrng(uint32_t mode, uint64_t a, uint64_t b, int n, float *out, cudaStream_t s);
 cudaError_t rmdLaunchDebugTrace(const rmd::WideNode *nodes, const float4 *tris, const float *rays, int n, int any,
                                 float *out, uint32_t *inst, uint32_t *errors, cudaStream_t s);
+// The Nishita sky texture of a TEX_SKY node (width x height RGBA float, CIE
+// XYZ in rgb): one thread per texel of the left half, mirrored to the right
+cudaError_t rmdLaunchSkyTexture(float4 *texels, uint32_t width, uint32_t height, float sunElevation, float altitude,
+                                float air, float dust, float ozone, cudaStream_t s);

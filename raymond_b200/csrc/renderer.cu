@@ -429,12 +429,18 @@ static rmd_status uploadTextures(const rmd_texture *textures, int count, rmd_sce
     std::vector<float4> texels;
     std::vector<TextureView> views;
     std::vector<size_t> offsets;
+    std::vector<std::pair<size_t, int>> skies;  // (texel offset, texture index) of generated sky textures
     for (int i = 0; i < count; i++) {
         const rmd_texture &t = textures[i];
         offsets.push_back(texels.size());
         const size_t n = (size_t)t.width * t.height;
         texels.resize(texels.size() + n);
         float4 *out = texels.data() + offsets.back();
+        if (!t.data) {  // a sky texture, filled on the device below
+            skies.push_back({offsets.back(), i});
+            views.push_back(TextureView{nullptr, (int)t.width, (int)t.height, (int)t.channels, 0});
+            continue;
+        }
         for (size_t p = 0; p < n; p++) {
             float v[4] = {0.0f, 0.0f, 0.0f, 1.0f};
             for (uint32_t c = 0; c < t.channels; c++) {
@@ -451,6 +457,13 @@ static rmd_status uploadTextures(const rmd_texture *textures, int count, rmd_sce
     texels.push_back(make_float4(0.0f, 0.0f, 0.0f, 1.0f));
     views.push_back(TextureView{nullptr, 1, 1, 1, 0});
     RMD_CUDA(s->textureTexels.upload(texels.data(), texels.size() * sizeof(float4), st));
+    for (const auto &sky : skies) {  // the Nishita sky textures of the scene's TEX_SKY nodes
+        float v[5];
+        if (!rmdhost::parseSkyTextureName(textures[sky.second].name, v))
+            return fail(RMD_ERROR_INVALID_ARGUMENT, "texture " + std::to_string(sky.second) + " has no data");
+        RMD_CUDA(rmdLaunchSkyTexture(s->textureTexels.as<float4>() + sky.first, textures[sky.second].width,
+                                     textures[sky.second].height, v[0], v[1], v[2], v[3], v[4], st));
+    }
     for (size_t i = 0; i < views.size(); i++) views[i].texels = s->textureTexels.as<float4>() + offsets[i];
     RMD_CUDA(s->textureViews.upload(views.data(), views.size() * sizeof(TextureView), st));
     s->dctx.textures = s->textureViews.as<TextureView>();
@@ -776,15 +789,17 @@ rmd_status rmd_scene_create(rmd_context *ctx, const rmd_scene_desc *d, rmd_scene
     auto s = std::make_unique<rmd_scene>();
     // MaterialBuilder.build: generate and JIT-compile the material module
     rmdhost::GeneratedModule mod;
+    rmdhost::SceneTextures tex;
     try {
         const bool hoist = std::getenv("RMD_NO_HOIST") == nullptr;
+        tex = rmdhost::sceneTextures(d);
         mod = rmdhost::generateModule(d->surface_materials, d->num_surface_materials, d->light_materials,
                                       d->num_light_materials, hoist,
-                                      rmdhost::TextureTable::of(d->textures, d->num_textures));
+                                      rmdhost::TextureTable::of(tex.list.data(), (int)tex.list.size()));
     } catch (const rmdhost::CodegenError &e) {
         return fail(e.status, e.message);
     }
-    if ((r = buildSceneData(ctx, d, s.get(), mod, 0, 0, d->textures, d->num_textures)) != RMD_OK) return r;
+    if ((r = buildSceneData(ctx, d, s.get(), mod, 0, 0, tex.list.data(), (int)tex.list.size())) != RMD_OK) return r;
     const std::string err = rmdhost::compileModule(
         mod.source, s->jit, {"-DRMD_SHADE_MIN_BLOCKS=" + std::to_string(s->defaultMinBlocks)});
     if (!err.empty()) return fail(RMD_ERROR_NVRTC, err);
@@ -930,7 +945,7 @@ static rmd_status guideTrainStep(GuideState &guide, const Counters &h, Counters 
     for (uint32_t k = 0; k < steps && stored > 0; k++) {
         RMD_CUDA(rmdLaunchGuideTrain(guide.records.as<GuideRecord>(), stored, guide.settings.step_records,
                                      (uint32_t)guide.net.steps + 1u, net, guide.net.scratch, trainBlocks,
-                                     guide.settings.learning_rate, guide.net.steps + 1, st));
+                                     guide.settings.learning_rate, guide.net.steps + 1, &cnt->errors, st));
         guide.net.steps++;
         trainSteps++;
         guide.stats.steps++;
@@ -1287,6 +1302,19 @@ rmd_status rmd_film_samples(const rmd_renderer *r, uint64_t *samples) {
     return RMD_OK;
 }
 
+rmd_status rmd_film_device(rmd_renderer *r, float **film, uint64_t *num_pixels) {
+    if (!r || !film) return fail(RMD_ERROR_INVALID_ARGUMENT, "NULL argument");
+    *film = r->film.as<float>();
+    if (num_pixels) *num_pixels = (uint64_t)r->width * r->height;
+    return RMD_OK;
+}
+
+rmd_status rmd_film_set_samples(rmd_renderer *r, uint64_t samples) {
+    if (!r) return fail(RMD_ERROR_INVALID_ARGUMENT, "NULL renderer");
+    r->samples = samples;
+    return RMD_OK;
+}
+
 rmd_status rmd_renderer_stats(const rmd_renderer *r, rmd_stats *out) {
     if (!r || !out) return fail(RMD_ERROR_INVALID_ARGUMENT, "NULL argument");
     *out = r->stats;
@@ -1515,10 +1543,11 @@ rmd_status rmd_test_generate_source(const rmd_scene_desc *d, int32_t hoist, char
                                     int64_t *needed) {
     if (!d) return fail(RMD_ERROR_INVALID_ARGUMENT, "NULL desc");
     try {
+        const rmdhost::SceneTextures tex = rmdhost::sceneTextures(d);
         rmdhost::GeneratedModule mod =
             rmdhost::generateModule(d->surface_materials, d->num_surface_materials, d->light_materials,
                                     d->num_light_materials, hoist != 0,
-                                    rmdhost::TextureTable::of(d->textures, d->num_textures));
+                                    rmdhost::TextureTable::of(tex.list.data(), (int)tex.list.size()));
         if (needed) *needed = (int64_t)mod.source.size() + 1;
         if (buf && buflen > 0) {
             const size_t n = std::min<size_t>((size_t)buflen - 1, mod.source.size());
@@ -1536,10 +1565,11 @@ rmd_status rmd_test_jit_compile(const rmd_scene_desc *d, int32_t hoist, char *lo
     if (!d) return fail(RMD_ERROR_INVALID_ARGUMENT, "NULL desc");
     std::string msg;
     try {
+        const rmdhost::SceneTextures tex = rmdhost::sceneTextures(d);
         rmdhost::GeneratedModule mod =
             rmdhost::generateModule(d->surface_materials, d->num_surface_materials, d->light_materials,
                                     d->num_light_materials, hoist != 0,
-                                    rmdhost::TextureTable::of(d->textures, d->num_textures));
+                                    rmdhost::TextureTable::of(tex.list.data(), (int)tex.list.size()));
         std::vector<char> cubin;
         bool cached = false;
         std::string err = rmdhost::compileCubin(mod.source, cubin, msg, cached,
@@ -1651,10 +1681,15 @@ rmd_status rmd_batch_create(rmd_context *ctx, const rmd_scene_desc *descs, int32
     // Each scene's materials resolve file names against its own textures.
     std::vector<rmd_texture> texUnion;
     std::vector<rmdhost::TextureTable> sceneTables(numScenes);
+    std::vector<rmdhost::SceneTextures> sceneTex(numScenes);  // images and generated skies (names live here)
+    try {
+        for (int i = 0; i < numScenes; i++) sceneTex[i] = rmdhost::sceneTextures(&descs[i]);
+    } catch (const rmdhost::CodegenError &e) {
+        return fail(e.status, e.message);
+    }
     for (int i = 0; i < numScenes; i++) {
         rmdhost::TextureTable &t = sceneTables[i];
-        for (int k = 0; k < descs[i].num_textures; k++) {
-            const rmd_texture &x = descs[i].textures[k];
+        for (const rmd_texture &x : sceneTex[i].list) {
             auto same = std::find_if(texUnion.begin(), texUnion.end(), [&](const rmd_texture &u) {
                 return std::strcmp(u.name, x.name) == 0 && u.data == x.data && u.width == x.width &&
                        u.height == x.height && u.channels == x.channels && u.format == x.format;

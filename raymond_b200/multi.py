@@ -7,6 +7,9 @@ sharded without any exchange on the data path.
 * `max_over_ranks` / `sum_over_ranks`: the host-side reductions of
   timings and counts (gloo on CPU, NCCL on GPUs).
 * `gather_films`: the views' films brought to rank 0 (host gather).
+* `reduce_film` / `combine_films`: one image whose samples were split over
+  ranks, summed into rank 0's film: an NCCL reduce on the device films in
+  place (gloo on host tensors).
 
 The process group comes from torch.distributed (launched by torchrun, one
 rank per GPU); without one, every helper acts as a world of one.
@@ -84,3 +87,39 @@ def gather_films(films: dict[int, np.ndarray]) -> dict[int, np.ndarray] | None:
     for part in out:
         merged.update(part)
     return merged
+
+
+def reduce_film(film):
+    """Sum a film tensor over ranks into rank 0's, in place.  The other ranks'
+    tensors hold unspecified values afterwards (a reduce may keep partial sums
+    there).  A CUDA tensor under NCCL, a CPU tensor under gloo.  Returns the
+    tensor on rank 0, None elsewhere."""
+    dist = _dist()
+    if dist is None:
+        return film
+    dist.reduce(film, dst=0, op=dist.ReduceOp.SUM)
+    return film if dist.get_rank() == 0 else None
+
+
+def combine_films(renderer) -> int:
+    """The frame of all ranks: every rank's renderer holds its own disjoint
+    samples of one image; their films are summed into rank 0's renderer, whose
+    sample count becomes the total (the other ranks' films are left unspecified).  `renderer.film_tensor()` aliases the
+    film: on GPUs a zero-copy CUDA view of the library's buffer, reduced by
+    NCCL in place.  Returns the total sample count."""
+    total = int(sum_over_ranks([float(renderer.samples())])[0])
+    dist = _dist()
+    if dist is None:
+        return total
+    film = renderer.film_tensor()
+    if film.is_cuda:
+        import torch
+
+        torch.cuda.synchronize()  # the renderer's stream has finished before the collective reads
+        reduce_film(film)
+        torch.cuda.synchronize()  # the sum is in place before the library's stream reads the film again
+    else:
+        reduce_film(film)
+    if dist.get_rank() == 0:
+        renderer.set_samples(total)
+    return total

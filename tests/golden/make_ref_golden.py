@@ -2,10 +2,12 @@
 own device code (oracle/_ref/libref.so, built by oracle/ref/Makefile from the
 mounted reference).  Run from the repository root:
 
-    make -C oracle/ref && python tests/golden/make_ref_golden.py [--only pin|render|tonemap]
+    make -C oracle/ref && python tests/golden/make_ref_golden.py [--only pin|render|tonemap|sky]
 
 Contents: the reference's normalizeImage (exposure, accumulation, Hable and
-ACES tonemaps) on a random film (ref_tonemap.npz); TEA PRNG streams, fractal noise values and the evaluate/sample
+ACES tonemaps) on a random film (ref_tonemap.npz); its Nishita sky model
+(host/sky/sky_nishita.cpp) on small textures and the sun disc (ref_sky.npz);
+TEA PRNG streams, fractal noise values and the evaluate/sample
 results of every material in oracle/ref/pin_materials.py on seeded shading
 records, all computed by the reference's code (ref_pin.npz); and one-sample
 images of the reference-render scenes rendered by the reference's own kernels
@@ -55,14 +57,38 @@ def tonemap_golden() -> None:
     np.savez_compressed(ROOT / "tests" / "golden" / "ref_tonemap.npz", **out)
 
 
+# Nishita sky cases: sun elevation, altitude, air, dust, ozone (the texture) and sun rotation, size, intensity
+SKY_CASES = [(0.2618, 0.0, 1.0, 1.0, 1.0, 0.0, 0.0095, 1.0), (0.05, 1000.0, 2.0, 0.5, 1.0, 1.3, 0.2, 2.0),
+             (-0.1, 0.0, 1.0, 1.0, 1.0, 4.0, 0.05, 1.0), (1.2, 5e4, 0.3, 4.0, 2.0, 0.5, 0.6, 0.5)]
+SKY_SIZE = 64  # texture width and height of the golden (the renderer's is 512)
+
+
+def sky_golden() -> None:
+    """ref_sky.npz: the reference's sky model (host/sky/sky_nishita.cpp) on a
+    64 x 64 texture and the sun disc colours, for each case."""
+    tex, sun = [], []
+    for e, alt, air, dust, oz, _rot, size, _inten in SKY_CASES:
+        tex.append(R.sky_texture(SKY_SIZE, SKY_SIZE, e, alt, air, dust, oz))
+        sun.append(R.sky_sun(e, size, alt, air, dust))
+    np.savez_compressed(ROOT / "tests" / "golden" / "ref_sky.npz", cases=np.array(SKY_CASES, np.float32),
+                        textures=np.stack(tex), sun=np.stack(sun))
+
+
 def main() -> None:
     ap = argparse.ArgumentParser()
-    ap.add_argument("--only", choices=["pin", "render", "tonemap"], help="regenerate one file")
+    ap.add_argument("--only", choices=["pin", "render", "tonemap", "sky"], help="regenerate one file")
     args = ap.parse_args()
     if args.only in (None, "tonemap"):
         tonemap_golden()
-    if args.only == "tonemap":
-        return
+    if args.only in (None, "sky"):
+        sky_golden()
+    if args.only in (None, "pin"):
+        pin_golden()
+    if args.only in (None, "render"):
+        render_golden()
+
+
+def pin_golden() -> None:
     out = {}
     out["prng_cases"] = np.array(PRNG_CASES, np.uint64)
     out["prng"] = np.stack([R.prng_tea(a, b, 256) for a, b in PRNG_CASES])
@@ -71,7 +97,7 @@ def main() -> None:
     out["noise_points"] = pts
     out["noise_cases"] = np.array(NOISE_CASES, np.float32)
     out["noise"] = np.stack([R.fractal_noise3(pts, d, r) for d, r in NOISE_CASES])
-    R.set_textures(pin_materials.textures())
+    pin_materials.install_ref_textures(R)
     rec = R.shading_records(RECORDS, RECORD_SEED)
     names = [n for n, _ in pin_materials.materials()]
     out["records"] = rec
@@ -79,6 +105,8 @@ def main() -> None:
     out["materials"] = np.stack([R.material_eval(m, rec) for m in range(len(names))])
     np.savez_compressed(ROOT / "tests" / "golden" / "ref_pin.npz", **out)
 
+
+def render_golden() -> None:
     scenes = pin_materials.ref_scenes()
     renders = {}
     for name, w, h, depth, frames in RENDER_CASES:

@@ -102,6 +102,30 @@ def test_guide_gradient_matches_oracle(gpu_ctx):
 
 
 @pytest.mark.gpu
+def test_guide_adam_matches_oracle(gpu_ctx):
+    """The device Adam step (k_guide_adam) against the float64 Adam of the
+    oracle, for a first step and a later one with non-zero moments: new
+    parameters within 1e-6 relative (+1e-9), moments within 1e-5 relative,
+    and the BF16 weight copy equal to the new FP32 weights rounded."""
+    rng = np.random.default_rng(21)
+    n = api.guide_param_count()
+    params = G.init_params(4)
+    grad = (rng.normal(0, 1e-2, n) * rng.uniform(0, 1, n) ** 4).astype(np.float32)
+    grad[rng.uniform(0, 1, n) < 0.1] = 0.0  # parameters without gradient (inputs never active)
+    for step, m, v in [(1, np.zeros(n), np.zeros(n)),
+                       (37, rng.normal(0, 1e-3, n), rng.uniform(0, 1e-4, n))]:
+        m32, v32 = m.astype(np.float32), v.astype(np.float32)
+        p_g, m_g, v_g, bits = api.guide_adam(params, grad, m32, v32, step, 1e-3)
+        p_c, m_c, v_c = G.adam_step(params, grad, m32, v32, step, 1e-3)
+        np.testing.assert_allclose(m_g, m_c, rtol=1e-5, atol=1e-12)
+        np.testing.assert_allclose(v_g, v_c, rtol=1e-5, atol=1e-15)
+        np.testing.assert_allclose(p_g, p_c, rtol=1e-6, atol=1e-9)
+        wmask = G.weight_mask()
+        want = (G.bf16(p_g[wmask]).astype(np.float32).view(np.uint32) >> 16).astype(np.uint16)
+        np.testing.assert_array_equal(bits[:wmask.sum()], want)
+
+
+@pytest.mark.gpu
 def test_guide_mixture_sampling_matches_pdf(gpu_ctx):
     rng = np.random.default_rng(4)
     out = rng.normal(0, 1.0, G.OUTPUTS).astype(np.float32)

@@ -69,7 +69,7 @@ def test_oracle_matches_reference_live(oracle_pin_scene):
     pts = np.random.default_rng(9).uniform(-1e3, 1e3, (4096, 3)).astype(np.float32)
     for d, r in [(1.0, 0.3), (6.25, 0.55)]:
         assert np.array_equal(R.fractal_noise3(pts, d, r).view(np.uint32), O.fractal_noise3(pts, d, r).view(np.uint32))
-    R.set_textures(pin_materials.textures())
+    pin_materials.install_ref_textures(R)
     rec = R.shading_records(2048, seed=77)
     names = [n for n, _ in pin_materials.materials()]
     ref_out = np.stack([R.material_eval(m, rec) for m in range(len(names))])
@@ -146,3 +146,28 @@ def test_oracle_tonemap_matches_reference_live():
             ref = R.normalize_image(film, e, bool(a), f, t)
             got = O.normalize_image(film, e, bool(a), f, t)
             assert np.array_equal(got.view(np.uint32), ref.view(np.uint32)), (t, e, a, f)
+
+
+# ------------------------------------------------------------------ Nishita sky
+# The sky texture and sun disc of the TEX_SKY node (host/sky/sky_nishita.cpp):
+# the oracle's restatement against the reference's own model, bit for bit.
+SKY_GOLDEN = Path(__file__).resolve().parent / "golden" / "ref_sky.npz"
+
+
+def test_oracle_sky_matches_reference_golden():
+    g = np.load(SKY_GOLDEN)
+    n = g["textures"].shape[1]
+    for (e, alt, air, dust, oz, rot, size, inten), tex, sun in zip(g["cases"], g["textures"], g["sun"]):
+        got = O.sky_texture(n, n, e, alt, air, dust, oz)[..., :3]
+        assert np.array_equal(got.view(np.uint32), tex.view(np.uint32)), (e, alt)
+        data = O.sky_data(e, rot, True, size, inten, alt, air, dust)
+        assert np.array_equal(data[:6].view(np.uint32), sun.view(np.uint32)), (e, alt)
+        assert list(data[6:]) == [np.float32(e), np.float32(rot), np.float32(size), np.float32(inten)]
+
+
+@pytest.mark.skipif(not R.sky_available(), reason="host build of the reference's sky model not present")
+def test_oracle_sky_matches_reference_live():
+    for args in [(0.7, 300.0, 1.1, 0.9, 1.3), (0.01, 0.0, 1.0, 1.0, 1.0)]:
+        ref = R.sky_texture(96, 80, *args)
+        got = O.sky_texture(96, 80, *args)[..., :3]
+        assert np.array_equal(got.view(np.uint32), ref.view(np.uint32)), args

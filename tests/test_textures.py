@@ -109,8 +109,10 @@ def test_codegen_texture_nodes(built):
     assert "kTexImage::COLOR_SPACE_NON_COLOR, kTexImage::PIXEL_FORMAT_R>" in src
     assert "TexImage<2, kTexImage::INTERPOLATION_LINEAR, kTexImage::PROJECTION_EQUIRECTANGULAR" in src
     assert "kTexImage::COLOR_SPACE_XYZ, kTexImage::PIXEL_FORMAT_RGBA>" in src
-    # the missing file: the zero texture after the scene's three, single channel
-    assert "TexImage<3, kTexImage::INTERPOLATION_LINEAR, kTexImage::PROJECTION_FLAT" in src
+    # the sky material's generated texture follows the scene's three images
+    assert "TexNishita<3>" in src
+    # the missing file: the zero texture after them, single channel
+    assert "TexImage<4, kTexImage::INTERPOLATION_LINEAR, kTexImage::PROJECTION_FLAT" in src
     # the reference's node knows linear interpolation only
     sc = pin_materials.scene()
     graph = dict(sc["materials"])["image_textures"]
