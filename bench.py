@@ -363,8 +363,15 @@ def desc_triangles(desc) -> int:
     return int(sum(len(s["indices"]) for s in desc.scene["shapes"]))
 
 
-def guided_leg(api, ctx, oracle_spp: int, size=(GUIDED_W, GUIDED_H)) -> dict:
-    """Equal-time relMSE of the guided tracer against the plain one (config 4)."""
+GUIDE_DEFAULTS = {"batch_size": 1 << 20, "learning_rate": 1e-3, "steps_per_batch": 8, "step_records": 1 << 13}
+
+
+def guided_leg(api, ctx, oracle_spp: int, size=(GUIDED_W, GUIDED_H), guide: dict | None = None,
+               oracle_cache: str = "") -> dict:
+    """Equal-time relMSE of the guided tracer against the plain one (config 4).
+    `guide` overrides the guide settings (GUIDE_DEFAULTS); `oracle_cache`, a
+    .npy path: reuse the FP64 oracle film stored there by an earlier run of the
+    same size and spp (its device time is then the stored run's)."""
     from raymond_b200 import scenes
     from raymond_b200._abi import SceneDesc
     from raymond_b200.metrics import relmse
@@ -372,16 +379,24 @@ def guided_leg(api, ctx, oracle_spp: int, size=(GUIDED_W, GUIDED_H)) -> dict:
     desc = SceneDesc(scenes.glossy_room(seed=1))
     scene = api.Scene(ctx, desc)
     (W, H), depth = size, GUIDED_DEPTH
-    oracle = api.Renderer(scene, W, H)
-    per_call = max(1, min(oracle_spp, (1 << 27) // (W * H)))
-    done, oracle_ms = 0, 0.0
-    while done < oracle_spp:
-        n = min(per_call, oracle_spp - done)
-        oracle.render(spp=n, max_depth=depth, film_fp64=True, seed=77)
-        oracle_ms += oracle.stats()["ms_total"]
-        done += n
-    reference = oracle.film64() / oracle_spp
-    oracle.close()
+    cache = Path(oracle_cache) if oracle_cache else None
+    if cache and cache.exists():
+        stored = np.load(cache, allow_pickle=True).item()
+        assert stored["size"] == (W, H) and stored["spp"] == oracle_spp
+        reference, oracle_ms = stored["film"], stored["ms"]
+    else:
+        oracle = api.Renderer(scene, W, H)
+        per_call = max(1, min(oracle_spp, (1 << 27) // (W * H)))
+        done, oracle_ms = 0, 0.0
+        while done < oracle_spp:
+            n = min(per_call, oracle_spp - done)
+            oracle.render(spp=n, max_depth=depth, film_fp64=True, seed=77)
+            oracle_ms += oracle.stats()["ms_total"]
+            done += n
+        reference = oracle.film64() / oracle_spp
+        oracle.close()
+        if cache:
+            np.save(cache, {"size": (W, H), "spp": oracle_spp, "film": reference, "ms": oracle_ms})
     plain = api.Renderer(scene, W, H)
     plain_ms = 0.0
     for _ in range(GUIDED_PLAIN_SPP // GUIDED_CHUNK):
@@ -389,7 +404,7 @@ def guided_leg(api, ctx, oracle_spp: int, size=(GUIDED_W, GUIDED_H)) -> dict:
         plain_ms += plain.stats()["ms_total"]
     e_plain = relmse(plain.film(normalize=True), reference)
     plain.close()
-    settings = {"batch_size": 1 << 20, "learning_rate": 1e-3, "steps_per_batch": 8, "step_records": 1 << 13}
+    settings = dict(GUIDE_DEFAULTS, **(guide or {}))
     g = api.Renderer(scene, W, H)
     g.set_guide(sampling=True, training=True, seed=1, **settings)
     ms, spp, curve, parity = 0.0, 0, [], None
@@ -446,6 +461,12 @@ def main():
     ap.add_argument("--guided-size", default=f"{GUIDED_W}x{GUIDED_H}", help="guided leg resolution (profiling runs)")
     ap.add_argument("--oracle-spp", type=int, default=GUIDED_ORACLE_SPP, help="guided leg: oracle samples")
     ap.add_argument("--no-autotune", action="store_true")
+    ap.add_argument("--guide-steps", type=int, default=0, help="--workload guided: Adam steps per batch")
+    ap.add_argument("--guide-records", type=int, default=0, help="--workload guided: records per Adam step")
+    ap.add_argument("--guide-batch", type=int, default=0, help="--workload guided: tracer samples per batch")
+    ap.add_argument("--guide-lr", type=float, default=0.0, help="--workload guided: learning rate")
+    ap.add_argument("--guide-depth", type=int, default=0, help="--workload guided: guided path depths (0: all)")
+    ap.add_argument("--oracle-cache", default="", help="--workload guided: .npy file of the FP64 oracle film")
     ap.add_argument("--bvh", default="host", choices=["host", "gpu"], help="BVH builder of the plain workload's scene")
     ap.add_argument("--tuning", default="", help="shade_min_blocks,trace_blocks_per_sm,pool_size: apply "
                     "these launch choices instead of autotuning (profiling runs)")
@@ -483,7 +504,11 @@ def main():
         return
     if args.workload == "guided":  # the config-4 leg alone
         from raymond_b200 import api as api_
-        print(json.dumps(guided_leg(api_, api_.Context(0), args.oracle_spp, guided_size)), flush=True)
+        guide = {k: v for k, v in (("steps_per_batch", args.guide_steps), ("step_records", args.guide_records),
+                                   ("batch_size", args.guide_batch), ("learning_rate", args.guide_lr),
+                                   ("guided_depth", args.guide_depth)) if v}
+        print(json.dumps(guided_leg(api_, api_.Context(0), args.oracle_spp, guided_size, guide, args.oracle_cache)),
+              flush=True)
         return
 
     rank, world, local = rank_info()

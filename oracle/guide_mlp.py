@@ -216,13 +216,17 @@ def init_params(seed: int = 0) -> np.ndarray:
 
 
 def adam_step(params, grad, m, v, step: int, lr: float, beta1=0.9, beta2=0.999, eps=1e-8):
-    """One Adam step (Kingma and Ba 2015, bias-corrected moments), float64:
-    returns the new parameters and moments."""
+    """One Adam step (Kingma and Ba 2015, bias-corrected moments) in float64
+    with the device's FP32 coefficients (beta and 1 - beta rounded to float:
+    1 - 0.999f is 9.9998713e-4): returns the new parameters and moments."""
+    b1, b2 = np.float32(beta1), np.float32(beta2)
+    c1, c2 = float(np.float32(1) - b1), float(np.float32(1) - b2)
+    b1, b2 = float(b1), float(b2)
     g = np.asarray(grad, np.float64)
-    m = beta1 * np.asarray(m, np.float64) + (1 - beta1) * g
-    v = beta2 * np.asarray(v, np.float64) + (1 - beta2) * g * g
-    mh = m / (1 - beta1 ** step)
-    vh = v / (1 - beta2 ** step)
+    m = b1 * np.asarray(m, np.float64) + c1 * g
+    v = b2 * np.asarray(v, np.float64) + c2 * g * g
+    mh = m / (1 - b1 ** step)
+    vh = v / (1 - b2 ** step)
     return np.asarray(params, np.float64) - lr * mh / (np.sqrt(vh) + eps), m, v
 
 

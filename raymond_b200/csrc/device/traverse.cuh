@@ -213,9 +213,12 @@ RMD_HD void beginTraversal(TraversalState &s, const WideNode *nodes, float3 o, f
 // culls what follows.  ANY: stop at the first hit (raytrace.metal:52-85);
 // otherwise keep the closest (raytrace.metal:11-50).  (Dynamic ray fetch,
 // Aila & Laine, HPG 2009, measured slower with this tree too.)
+// `budget` bounds the node visits of this call: when it runs out the
+// traversal pauses (its group and stack depth kept in `s`) and a later call
+// resumes it.
 template <bool ANY>
 RMD_HD void traverse(TraversalState &s, TraversalStack &stack, const WideNode *__restrict__ nodes,
-                     const float4 *__restrict__ tris, uint32_t *errors) {
+                     const float4 *__restrict__ tris, uint32_t *errors, int budget = 0x7fffffff) {
     if (s.sp < 0) return;
     const float3 idir = s.r.idir, org = s.r.org;
     const uint32_t octant = rayOctant(idir);
@@ -223,6 +226,11 @@ RMD_HD void traverse(TraversalState &s, TraversalStack &stack, const WideNode *_
     int sp = s.sp;
     while (true) {
         if (group.y > 0x00ffffffu) {
+            if (budget-- == 0) {  // pause before the next node
+                s.group = group;
+                s.sp = sp;
+                return;
+            }
             const uint32_t key = __ffs(group.y >> 24) - 1;
             group.y &= ~(1u << (24u + key));
             const uint32_t slot = key ^ octant;

@@ -3,12 +3,11 @@
 // (forward, loss gradient, backward, Adam) on the records the tracer
 // produces.  No counterpart in the reference.
 //
-// Inference runs on the 5th-generation tensor cores (tcgen05.mma, TMEM
-// accumulators, one thread per sample; see the tcgen05 inference core).
-// Training: each warp processes 16 samples at a time with mma.sync m16n8k16
-// (BF16 inputs, FP32 accumulation), activations in per-warp shared memory as
-// BF16 rows; the block's weight gradient accumulates in shared memory (FP32)
-// and is added to the global gradient once per block.
+// Both run on the 5th-generation tensor cores (tcgen05.mma, operands in
+// shared memory, FP32 accumulators in tensor memory): inference one thread per
+// sample in pipelines of 128 (see the tcgen05 inference core), training one
+// CTA per tile of 128 records, the weight gradients accumulated in tensor
+// memory (see the tcgen05 training core).
 #include <cuda_runtime.h>
 
 #include <algorithm>
@@ -26,144 +25,9 @@
 namespace rmd {
 namespace {
 
-constexpr int kWarps = 4;  // warps per block (the shared memory of one block per SM); each owns 16 samples at a time
-constexpr int kLd0 = GUIDE_INPUTS + 8, kLdH = GUIDE_HIDDEN + 8, kLdO = GUIDE_OUTPUTS + 4;  // padded rows
-
-// per-warp shared scratch (bf16 activations as uint16_t)
-struct WarpScratch {
-    uint16_t x[16 * kLd0];
-    uint16_t h[3][16 * kLdH];
-    float o[16 * kLdO];
-    uint16_t d[2][16 * kLdH];  // deltas (ping-pong); the output delta uses the first 48 columns
-};
-
 __device__ __forceinline__ uint16_t toBf16(float x) { return (uint16_t)bf16Bits(x); }
 __device__ __forceinline__ float fromBf16(uint16_t b) { return __uint_as_float((uint32_t)b << 16); }
 __device__ __forceinline__ uint32_t pack2(uint16_t lo, uint16_t hi) { return (uint32_t)lo | ((uint32_t)hi << 16); }
-
-__device__ __forceinline__ void mma16816(float c[4], const uint32_t a[4], const uint32_t b[2]) {
-    asm volatile(
-        "mma.sync.aligned.m16n8k16.row.col.f32.bf16.bf16.f32 {%0, %1, %2, %3}, {%4, %5, %6, %7}, {%8, %9}, "
-        "{%0, %1, %2, %3};\n"
-        : "+f"(c[0]), "+f"(c[1]), "+f"(c[2]), "+f"(c[3])
-        : "r"(a[0]), "r"(a[1]), "r"(a[2]), "r"(a[3]), "r"(b[0]), "r"(b[1]));
-}
-
-// Fragment loads.  g = lane / 4, t = lane % 4.  A(m, k) 16 x 16, B(k, n) 16 x 8.
-// A from a row-major [m][k] matrix
-__device__ __forceinline__ void loadA(uint32_t a[4], const uint16_t *m, int ld, int k0, int g, int t) {
-    a[0] = *reinterpret_cast<const uint32_t *>(&m[g * ld + k0 + 2 * t]);
-    a[1] = *reinterpret_cast<const uint32_t *>(&m[(g + 8) * ld + k0 + 2 * t]);
-    a[2] = *reinterpret_cast<const uint32_t *>(&m[g * ld + k0 + 8 + 2 * t]);
-    a[3] = *reinterpret_cast<const uint32_t *>(&m[(g + 8) * ld + k0 + 8 + 2 * t]);
-}
-// A = M^T for a row-major [k][m] matrix M (rows m0.., columns of the 16 samples)
-__device__ __forceinline__ void loadAT(uint32_t a[4], const uint16_t *m, int ld, int m0, int g, int t) {
-    a[0] = pack2(m[(2 * t) * ld + m0 + g], m[(2 * t + 1) * ld + m0 + g]);
-    a[1] = pack2(m[(2 * t) * ld + m0 + g + 8], m[(2 * t + 1) * ld + m0 + g + 8]);
-    a[2] = pack2(m[(2 * t + 8) * ld + m0 + g], m[(2 * t + 9) * ld + m0 + g]);
-    a[3] = pack2(m[(2 * t + 8) * ld + m0 + g + 8], m[(2 * t + 9) * ld + m0 + g + 8]);
-}
-// B(k, n) = W[n][k] for a row-major [n][k] matrix (forward weights, in shared memory)
-__device__ __forceinline__ void loadBnk(uint32_t b[2], const uint16_t *w, int ld, int n0, int k0, int g, int t) {
-    b[0] = *reinterpret_cast<const uint32_t *>(&w[(n0 + g) * ld + k0 + 2 * t]);
-    b[1] = *reinterpret_cast<const uint32_t *>(&w[(n0 + g) * ld + k0 + 8 + 2 * t]);
-}
-// B(k, n) = M[k][n] for a row-major [k][n] matrix
-__device__ __forceinline__ void loadBkn(uint32_t b[2], const uint16_t *m, int ld, int n0, int k0, int g, int t) {
-    b[0] = pack2(m[(k0 + 2 * t) * ld + n0 + g], m[(k0 + 2 * t + 1) * ld + n0 + g]);
-    b[1] = pack2(m[(k0 + 2 * t + 8) * ld + n0 + g], m[(k0 + 2 * t + 9) * ld + n0 + g]);
-}
-
-// out[16][N] = act(in[16][K] . W^T + b): W row-major [N][K] (bf16, rows ldW apart), b fp32
-template <int K, int N, bool RELU>
-__device__ __forceinline__ void denseForward(const uint16_t *in, int ldIn, const uint16_t *w, int ldW,
-                                             const float *bias, uint16_t *outBf, float *outF, int ldOut, int g, int t) {
-#pragma unroll 1
-    for (int n0 = 0; n0 < N; n0 += 8) {
-        float c[4] = {0.0f, 0.0f, 0.0f, 0.0f};
-#pragma unroll
-        for (int k0 = 0; k0 < K; k0 += 16) {
-            uint32_t a[4], b[2];
-            loadA(a, in, ldIn, k0, g, t);
-            loadBnk(b, w, ldW, n0, k0, g, t);
-            mma16816(c, a, b);
-        }
-        const float b0 = bias[n0 + 2 * t], b1 = bias[n0 + 2 * t + 1];
-        float v[4] = {c[0] + b0, c[1] + b1, c[2] + b0, c[3] + b1};
-        if (RELU)
-#pragma unroll
-            for (int q = 0; q < 4; q++) v[q] = fmaxf(v[q], 0.0f);
-        const int r0 = g, r1 = g + 8, col = n0 + 2 * t;
-        if (outBf) {
-            outBf[r0 * ldOut + col] = toBf16(v[0]);
-            outBf[r0 * ldOut + col + 1] = toBf16(v[1]);
-            outBf[r1 * ldOut + col] = toBf16(v[2]);
-            outBf[r1 * ldOut + col + 1] = toBf16(v[3]);
-        } else {
-            outF[r0 * ldOut + col] = v[0];
-            outF[r0 * ldOut + col + 1] = v[1];
-            outF[r1 * ldOut + col] = v[2];
-            outF[r1 * ldOut + col + 1] = v[3];
-        }
-    }
-}
-
-// The training block's copy of the BF16 weights in shared memory, rows padded
-// (168 and 72 elements) so that the mma fragment loads are free of bank conflicts.
-constexpr int kLdW0 = GUIDE_INPUTS + 8, kLdWH = GUIDE_HIDDEN + 8;
-struct TrainWeights {
-    uint16_t w0[GUIDE_HIDDEN * kLdW0];
-    uint16_t w1[GUIDE_HIDDEN * kLdWH];
-    uint16_t w2[GUIDE_HIDDEN * kLdWH];
-    uint16_t w3[GUIDE_OUTPUTS * kLdWH];
-    float b[3 * GUIDE_HIDDEN + GUIDE_OUTPUTS];
-    __device__ const uint16_t *w(int l) const { return l == 0 ? w0 : l == 1 ? w1 : l == 2 ? w2 : w3; }
-    __device__ static int ld(int l) { return l == 0 ? kLdW0 : kLdWH; }
-};
-
-__device__ void loadTrainWeights(TrainWeights &tw, const GuideNetView &net) {
-    const int rows[4] = {GUIDE_HIDDEN, GUIDE_HIDDEN, GUIDE_HIDDEN, GUIDE_OUTPUTS};
-    const int cols[4] = {GUIDE_INPUTS, GUIDE_HIDDEN, GUIDE_HIDDEN, GUIDE_HIDDEN};
-    for (int l = 0; l < 4; l++) {
-        uint32_t *dst = reinterpret_cast<uint32_t *>(const_cast<uint16_t *>(tw.w(l)));
-        const uint32_t *src = reinterpret_cast<const uint32_t *>(net.w[l]);
-        const int half = cols[l] / 2, ldHalf = TrainWeights::ld(l) / 2;
-        for (int i = threadIdx.x; i < rows[l] * half; i += blockDim.x) {
-            const int r = i / half, c = i - r * half;
-            dst[r * ldHalf + c] = __ldg(&src[r * half + c]);
-        }
-    }
-    for (int i = threadIdx.x; i < 3 * GUIDE_HIDDEN + GUIDE_OUTPUTS; i += blockDim.x) {
-        const int l = min(i / GUIDE_HIDDEN, 3);
-        tw.b[i] = __ldg(&net.b[l][i - l * GUIDE_HIDDEN]);
-    }
-}
-
-// the whole forward pass for the 16 samples whose inputs are in s.x
-__device__ void forward(WarpScratch &s, const TrainWeights &tw, int g, int t) {
-    denseForward<GUIDE_INPUTS, GUIDE_HIDDEN, true>(s.x, kLd0, tw.w0, kLdW0, tw.b, s.h[0], nullptr, kLdH, g, t);
-    __syncwarp();
-    denseForward<GUIDE_HIDDEN, GUIDE_HIDDEN, true>(s.h[0], kLdH, tw.w1, kLdWH, tw.b + GUIDE_HIDDEN, s.h[1], nullptr,
-                                                   kLdH, g, t);
-    __syncwarp();
-    denseForward<GUIDE_HIDDEN, GUIDE_HIDDEN, true>(s.h[1], kLdH, tw.w2, kLdWH, tw.b + 2 * GUIDE_HIDDEN, s.h[2],
-                                                   nullptr, kLdH, g, t);
-    __syncwarp();
-    denseForward<GUIDE_HIDDEN, GUIDE_OUTPUTS, false>(s.h[2], kLdH, tw.w3, kLdWH, tw.b + 3 * GUIDE_HIDDEN, nullptr,
-                                                     s.o, kLdO, g, t);
-    __syncwarp();
-}
-
-// one-blob inputs of 16 samples (features held by lanes 0..15): lane l fills half a row
-__device__ void encodeInputs(WarpScratch &s, const GuideFeatures &f, int lane) {
-    const int row = lane & 15, c0 = (lane >> 4) * (GUIDE_INPUTS / 2);
-    GuideFeatures fr;
-#pragma unroll
-    for (int k = 0; k < 7; k++) fr.v[k] = __shfl_sync(0xffffffffu, f.v[k], row);
-    for (int c = c0; c < c0 + GUIDE_INPUTS / 2; c++) s.x[row * kLd0 + c] = toBf16(guideInput(fr, c));
-    __syncwarp();
-}
 
 __device__ __forceinline__ float sigmoid(float x) { return __fdividef(1.0f, 1.0f + __expf(-x)); }
 
@@ -667,6 +531,7 @@ struct TrainSmem {
     uint16_t rowB[kTrThreads * GUIDE_HIDDEN];   // layer-1 inputs, then layer-3 inputs; deltas
     float b[3 * GUIDE_HIDDEN + GUIDE_OUTPUTS];
     float db[3 * GUIDE_HIDDEN + GUIDE_OUTPUTS];  // the CTA's bias gradient
+    float reduce[8];                             // per warp: target sums, then loss sums
     unsigned long long mbar;
     uint32_t tmemBase;
     int failed;
@@ -806,13 +671,21 @@ __device__ void trDeltaEpilogue(TrainSmem &sm, uint32_t taddr, uint64_t mask, ui
 
 // The gradient of the mean loss over a batch of records on the tensor cores:
 // each CTA writes its gradient (weights and biases) to its slot of
-// net.partials.  On an expired wait the CTA sets ERR_GUIDE_TIMEOUT in
+// net.partials and its share of the loss to partials[GUIDE_PARTIAL_LOSS + CTA];
+// the Adam (or reduce) kernel sums them.  Every CTA sums the batch's targets
+// itself (the loss normalises them by their mean), so a step is this kernel
+// and the Adam step.  On an expired wait the CTA sets ERR_GUIDE_TIMEOUT in
 // *errors and writes a zero gradient.
-__global__ void __launch_bounds__(kTrThreads, 1) k_guide_train_tc(RecordBatch batch, const float *sumY, GuideNetView net,
-                                                                float *lossOut, uint32_t *errors) {
+__global__ void __launch_bounds__(kTrThreads, 1) k_guide_train_tc(RecordBatch batch, GuideNetView net,
+                                                                uint32_t *errors) {
     extern __shared__ __align__(16) unsigned char smem[];
     TrainSmem &sm = *reinterpret_cast<TrainSmem *>(smem);
     const int row = threadIdx.x, warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    // the batch's targets (L2-resident records), summed while the weights load
+    float ySum = 0.0f;
+    for (uint32_t i = threadIdx.x; i < batch.n; i += blockDim.x) ySum += batch.pick(i).y;
+    for (int off = 16; off > 0; off >>= 1) ySum += __shfl_xor_sync(0xffffffffu, ySum, off);
+    if (lane == 0) sm.reduce[warp] = ySum;
     // set-up: weights (forward and transposed), biases, mbarrier, tensor memory
     loadCanonical(sm.w0, net.w[0], GUIDE_HIDDEN, GUIDE_INPUTS);
     loadCanonical(sm.w1, net.w[1], GUIDE_HIDDEN, GUIDE_HIDDEN);
@@ -842,7 +715,8 @@ __global__ void __launch_bounds__(kTrThreads, 1) k_guide_train_tc(RecordBatch ba
     const uint32_t taddr = tmem + ((uint32_t)(row & ~31) << 16);  // this warp's lanes, work columns
     const uint32_t n = batch.n;
     const float scale = 1.0f / (float)n;
-    const float invMeanY = sumY[0] > 0.0f ? (float)n / sumY[0] : 0.0f;
+    const float sumY = sm.reduce[0] + sm.reduce[1] + sm.reduce[2] + sm.reduce[3];  // published by trPublish
+    const float invMeanY = sumY > 0.0f ? (float)n / sumY : 0.0f;
     const uint32_t tiles = (n + kTrThreads - 1) / kTrThreads;
     float lossSum = 0.0f;
     uint32_t phase = 0;
@@ -993,7 +867,11 @@ __global__ void __launch_bounds__(kTrThreads, 1) k_guide_train_tc(RecordBatch ba
         part[net.bOffset[l] + i - l * GUIDE_HIDDEN] = have ? sm.db[i] : 0.0f;
     }
     for (int off = 16; off > 0; off >>= 1) lossSum += __shfl_xor_sync(0xffffffffu, lossSum, off);
-    if (lane == 0 && lossOut && ok) atomicAdd(lossOut, lossSum * scale);
+    if (lane == 0) sm.reduce[4 + warp] = lossSum;
+    __syncthreads();
+    if (threadIdx.x == 0)
+        net.partials[GUIDE_PARTIAL_LOSS + blockIdx.x] =
+            ok ? (sm.reduce[4] + sm.reduce[5] + sm.reduce[6] + sm.reduce[7]) * scale : 0.0f;
     if (!ok && threadIdx.x == 0 && errors) atomicOr(errors, ERR_GUIDE_TIMEOUT);
     // teardown: a last bounded wait for work in flight after an expired wait, then free tensor memory
     if (!ok) mbarWait(smemU32(&sm.mbar), phase);
@@ -1066,110 +944,18 @@ __global__ void __launch_bounds__(kTcThreads) k_guide_infer(Counters *cnt, const
     tcTeardown(sm, pipe, phase);
 }
 
-// Gradient of the mean loss over a batch of records, accumulated into net.grad.
-__global__ void __launch_bounds__(32 * kWarps, 1) k_guide_train(RecordBatch batch, const float *sumY, GuideNetView net,
-                                                          float *lossOut) {
-    extern __shared__ __align__(16) unsigned char smem[];
-    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31, g = lane >> 2, t = lane & 3;
-    WarpScratch &s = reinterpret_cast<WarpScratch *>(smem)[warp];
-    float *acc = reinterpret_cast<float *>(smem + kWarps * sizeof(WarpScratch));  // block gradient, GUIDE_PARAMS
-    TrainWeights &tw = *reinterpret_cast<TrainWeights *>(acc + GUIDE_PARAMS);
-    for (int i = threadIdx.x; i < GUIDE_PARAMS; i += blockDim.x) acc[i] = 0.0f;
-    loadTrainWeights(tw, net);
-    __syncthreads();
-    const uint32_t n = batch.n;
-    const float scale = 1.0f / (float)n;
-    const float invMeanY = sumY[0] > 0.0f ? (float)n / sumY[0] : 0.0f;
-    float lossSum = 0.0f;
-    const uint32_t tiles = (n + 15) / 16;
-    for (uint32_t tile = blockIdx.x * kWarps + warp; tile < tiles; tile += gridDim.x * kWarps) {
-        const uint32_t r = tile * 16 + (lane & 15);
-        GuideRecord rc = {};
-        if (lane < 16 && r < n) rc = batch.pick(r);
-        GuideFeatures f;
-        for (int k = 0; k < 7; k++) f.v[k] = rc.features[k];
-        encodeInputs(s, f, lane);
-        forward(s, tw, g, t);
-        // output deltas: lanes 0..15, one sample each (zero for padding rows)
-        if (lane < 16) {
-            uint16_t *deltaRow = &s.d[0][lane * kLdH];
-            if (r < n) {
-                const float y = fminf(rc.y * invMeanY, 100.0f);
-                lossSum += lossGradient(&s.o[lane * kLdO], make_float3(rc.dir[0], rc.dir[1], rc.dir[2]), rc.pdfBsdf,
-                                        y, scale, deltaRow);
-            } else {
-                for (int c = 0; c < GUIDE_OUTPUTS; c++) deltaRow[c] = 0;
-            }
-        }
-        __syncwarp();
-        // backward through the four layers: layer l maps h[l-1] (x for l = 0) to h[l]
-        int cur = 0;  // delta of layer l's output in s.d[cur]
-#pragma unroll 1
-        for (int l = 3; l >= 0; l--) {
-            const int nOut = l == 3 ? GUIDE_OUTPUTS : GUIDE_HIDDEN;
-            const int nIn = l == 0 ? GUIDE_INPUTS : GUIDE_HIDDEN;
-            const uint16_t *delta = s.d[cur];
-            const uint16_t *in = l == 0 ? s.x : s.h[l - 1];
-            const int ldIn = l == 0 ? kLd0 : kLdH;
-            float *gW = acc + net.wOffset[l];
-            float *gB = acc + net.bOffset[l];
-            // dW[nOut][nIn] += delta^T . in
-            for (int m0 = 0; m0 < nOut; m0 += 16) {
-                uint32_t a[4];
-                loadAT(a, delta, kLdH, m0, g, t);
-                for (int n0 = 0; n0 < nIn; n0 += 8) {
-                    uint32_t b[2];
-                    loadBkn(b, in, ldIn, n0, 0, g, t);
-                    float c[4] = {0.0f, 0.0f, 0.0f, 0.0f};
-                    mma16816(c, a, b);
-                    atomicAdd(&gW[(m0 + g) * nIn + n0 + 2 * t], c[0]);
-                    atomicAdd(&gW[(m0 + g) * nIn + n0 + 2 * t + 1], c[1]);
-                    atomicAdd(&gW[(m0 + g + 8) * nIn + n0 + 2 * t], c[2]);
-                    atomicAdd(&gW[(m0 + g + 8) * nIn + n0 + 2 * t + 1], c[3]);
-                }
-            }
-            // db[nOut] += column sums of delta
-            for (int c = lane; c < nOut; c += 32) {
-                float sum = 0.0f;
-                for (int row = 0; row < 16; row++) sum += fromBf16(delta[row * kLdH + c]);
-                atomicAdd(&gB[c], sum);
-            }
-            if (l == 0) break;
-            // delta of the layer input: (delta . W) masked by ReLU'(in)
-            uint16_t *next = s.d[cur ^ 1];
-            for (int n0 = 0; n0 < nIn; n0 += 8) {
-                float c[4] = {0.0f, 0.0f, 0.0f, 0.0f};
-                for (int k0 = 0; k0 < nOut; k0 += 16) {
-                    uint32_t a[4], b[2];
-                    loadA(a, delta, kLdH, k0, g, t);
-                    loadBkn(b, tw.w(l), TrainWeights::ld(l), n0, k0, g, t);
-                    mma16816(c, a, b);
-                }
-                const int col = n0 + 2 * t;
-                const float m00 = fromBf16(in[g * ldIn + col]) > 0.0f ? 1.0f : 0.0f;
-                const float m01 = fromBf16(in[g * ldIn + col + 1]) > 0.0f ? 1.0f : 0.0f;
-                const float m10 = fromBf16(in[(g + 8) * ldIn + col]) > 0.0f ? 1.0f : 0.0f;
-                const float m11 = fromBf16(in[(g + 8) * ldIn + col + 1]) > 0.0f ? 1.0f : 0.0f;
-                next[g * kLdH + col] = toBf16(c[0] * m00);
-                next[g * kLdH + col + 1] = toBf16(c[1] * m01);
-                next[(g + 8) * kLdH + col] = toBf16(c[2] * m10);
-                next[(g + 8) * kLdH + col + 1] = toBf16(c[3] * m11);
-            }
-            __syncwarp();
-            cur ^= 1;
-        }
-        __syncwarp();
+// the training CTAs' loss shares summed into *lossOut (one thread)
+__device__ __forceinline__ void sumLoss(const GuideNetView &net, int blocks, float *lossOut) {
+    if (blockIdx.x == 0 && threadIdx.x == 0 && lossOut) {
+        float loss = 0.0f;
+        for (int b = 0; b < blocks; b++) loss += net.partials[GUIDE_PARTIAL_LOSS + b];
+        *lossOut = loss;
     }
-    for (int off = 16; off > 0; off >>= 1) lossSum += __shfl_xor_sync(0xffffffffu, lossSum, off);
-    if (lane == 0 && lossOut) atomicAdd(lossOut, lossSum * scale);
-    __syncthreads();
-    // the block's gradient, summed over the blocks by the Adam step (no atomics)
-    float *part = net.partials + (size_t)blockIdx.x * GUIDE_PARAMS;
-    for (int i = threadIdx.x; i < GUIDE_PARAMS; i += blockDim.x) part[i] = acc[i];
 }
 
 // net.grad += the sum of the training blocks' gradients
-__global__ void k_guide_reduce(GuideNetView net, int blocks) {
+__global__ void k_guide_reduce(GuideNetView net, int blocks, float *lossOut) {
+    sumLoss(net, blocks, lossOut);
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= GUIDE_PARAMS) return;
     float g = 0.0f;
@@ -1180,7 +966,8 @@ __global__ void k_guide_reduce(GuideNetView net, int blocks) {
 // Adam step on every parameter; refreshes the bf16 weight copies and clears
 // the gradient.
 __global__ void k_guide_adam(GuideNetView net, int blocks, float lr, float beta1, float beta2, float eps, float corr1,
-                             float corr2) {
+                             float corr2, float *lossOut) {
+    sumLoss(net, blocks, lossOut);
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= GUIDE_PARAMS) return;
     float gr = net.grad[i];
@@ -1193,15 +980,6 @@ __global__ void k_guide_adam(GuideNetView net, int blocks, float lr, float beta1
     net.master[i] = w;
     net.grad[i] = 0.0f;
     if (net.bf16Index[i] >= 0) net.weightsBf16[net.bf16Index[i]] = (uint16_t)bf16Bits(w);
-}
-
-// Sum of the batch's target weights (for the loss normalisation).
-__global__ void k_guide_mean_y(RecordBatch batch, float *sum) {
-    float s = 0.0f;
-    for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < batch.n; i += gridDim.x * blockDim.x)
-        s += batch.pick(i).y;
-    for (int off = 16; off > 0; off >>= 1) s += __shfl_xor_sync(0xffffffffu, s, off);
-    if ((threadIdx.x & 31) == 0 && s != 0.0f) atomicAdd(sum, s);
 }
 
 // Test hook: forward pass of explicit feature vectors through the inference
@@ -1289,24 +1067,24 @@ cudaError_t rmdLaunchGuideInfer(const Context &ctx, const PathPool &pool, Counte
 cudaError_t rmdLaunchGuideTrain(const GuideRecord *rec, uint32_t total, uint32_t n, uint32_t seed,
                                 const GuideNetView &net, float *scratch, int blocks, float lr, int step,
                                 uint32_t *errors, cudaStream_t s) {
-    // scratch[0]: sum of the target weights, scratch[1]: mean loss
-    cudaError_t e = cudaMemsetAsync(scratch, 0, 2 * sizeof(float), s);
-    if (e != cudaSuccess || total == 0) return e;
+    // scratch[1]: the step's mean loss (written by the Adam step)
+    if (total == 0) return cudaSuccess;
     RecordBatch batch{rec, total, std::min(n, total), seed};
-    k_guide_mean_y<<<256, 256, 0, s>>>(batch, scratch);
-    if ((e = cudaGetLastError()) != cudaSuccess) return e;
     // one CTA per tile of 128 records, at most `blocks` (each CTA then takes several tiles)
     const int tiles = (int)((batch.n + kTrThreads - 1) / kTrThreads);
     blocks = std::max(1, std::min(std::min(blocks, tiles), GUIDE_TRAIN_MAX_BLOCKS));
-    k_guide_train_tc<<<blocks, kTrThreads, rmdGuideSharedBytes(true), s>>>(batch, scratch, net, scratch + 1, errors);
-    if ((e = cudaGetLastError()) != cudaSuccess) return e;
-    return rmdLaunchGuideAdam(net, blocks, lr, step, s);
+    k_guide_train_tc<<<blocks, kTrThreads, rmdGuideSharedBytes(true), s>>>(batch, net, errors);
+    cudaError_t e = cudaGetLastError();
+    if (e != cudaSuccess) return e;
+    return rmdLaunchGuideAdam(net, blocks, lr, step, scratch + 1, s);
 }
 
-cudaError_t rmdLaunchGuideAdam(const GuideNetView &net, int blocks, float lr, int step, cudaStream_t s) {
+cudaError_t rmdLaunchGuideAdam(const GuideNetView &net, int blocks, float lr, int step, float *lossOut,
+                               cudaStream_t s) {
     const float beta1 = 0.9f, beta2 = 0.999f;
     const float corr1 = 1.0f / (1.0f - powf(beta1, (float)step)), corr2 = 1.0f / (1.0f - powf(beta2, (float)step));
-    k_guide_adam<<<(GUIDE_PARAMS + 255) / 256, 256, 0, s>>>(net, blocks, lr, beta1, beta2, 1e-8f, corr1, corr2);
+    k_guide_adam<<<(GUIDE_PARAMS + 255) / 256, 256, 0, s>>>(net, blocks, lr, beta1, beta2, 1e-8f, corr1, corr2,
+                                                            lossOut);
     return cudaGetLastError();
 }
 
@@ -1320,18 +1098,16 @@ cudaError_t rmdLaunchGuideForwardTest(const float *features, uint32_t n, const G
 
 cudaError_t rmdLaunchGuideGradientTest(const GuideRecord *rec, uint32_t n, const GuideNetView &net, float *scratch,
                                        int blocks, cudaStream_t s) {
-    // scratch[0]: sum of the targets, [1]: mean loss, [2]: error flags
+    // scratch[1]: mean loss, [2]: error flags
     cudaError_t e = cudaMemsetAsync(scratch, 0, 3 * sizeof(float), s);
     if (e != cudaSuccess || n == 0) return e;
     RecordBatch batch{rec, n, n, 0};
-    k_guide_mean_y<<<256, 256, 0, s>>>(batch, scratch);
-    if ((e = cudaGetLastError()) != cudaSuccess) return e;
     const int tiles = (int)((n + kTrThreads - 1) / kTrThreads);
     blocks = std::max(1, std::min(std::min(blocks, tiles), GUIDE_TRAIN_MAX_BLOCKS));
-    k_guide_train_tc<<<blocks, kTrThreads, rmdGuideSharedBytes(true), s>>>(batch, scratch, net, scratch + 1,
+    k_guide_train_tc<<<blocks, kTrThreads, rmdGuideSharedBytes(true), s>>>(batch, net,
                                                                            reinterpret_cast<uint32_t *>(scratch + 2));
     if ((e = cudaGetLastError()) != cudaSuccess) return e;
-    k_guide_reduce<<<(GUIDE_PARAMS + 255) / 256, 256, 0, s>>>(net, blocks);
+    k_guide_reduce<<<(GUIDE_PARAMS + 255) / 256, 256, 0, s>>>(net, blocks, scratch + 1);
     return cudaGetLastError();
 }
 
@@ -1368,7 +1144,7 @@ cudaError_t GuideNet::allocate() {
     if ((e = cudaMalloc(&master, pb)) != cudaSuccess || (e = cudaMalloc(&adamM, pb)) != cudaSuccess ||
         (e = cudaMalloc(&adamV, pb)) != cudaSuccess || (e = cudaMalloc(&grad, pb)) != cudaSuccess ||
         (e = cudaMalloc(&scratch, 64 * sizeof(float))) != cudaSuccess ||
-        (e = cudaMalloc(&partials, (size_t)GUIDE_TRAIN_MAX_BLOCKS * pb)) != cudaSuccess ||
+        (e = cudaMalloc(&partials, (size_t)GUIDE_TRAIN_MAX_BLOCKS * (pb + sizeof(float)))) != cudaSuccess ||
         (e = cudaMalloc(&weightsBf16, GUIDE_WEIGHTS * sizeof(uint16_t))) != cudaSuccess ||
         (e = cudaMalloc(&bf16Index, GUIDE_PARAMS * sizeof(int))) != cudaSuccess)
         return e;
@@ -1539,7 +1315,7 @@ extern "C" rmd_status rmd_test_guide_adam(const float *params, const float *grad
     if ((e = cudaMemcpy(net.grad, grad, pb, cudaMemcpyHostToDevice)) != cudaSuccess ||
         (e = cudaMemcpy(net.adamM, m, pb, cudaMemcpyHostToDevice)) != cudaSuccess ||
         (e = cudaMemcpy(net.adamV, v, pb, cudaMemcpyHostToDevice)) != cudaSuccess ||
-        (e = rmdLaunchGuideAdam(net.view(make_float3(0, 0, 0), make_float3(1, 1, 1)), 0, lr, step, 0)) !=
+        (e = rmdLaunchGuideAdam(net.view(make_float3(0, 0, 0), make_float3(1, 1, 1)), 0, lr, step, nullptr, 0)) !=
             cudaSuccess ||
         (e = cudaMemcpy(params_out, net.master, pb, cudaMemcpyDeviceToHost)) != cudaSuccess ||
         (e = cudaMemcpy(m_out, net.adamM, pb, cudaMemcpyDeviceToHost)) != cudaSuccess ||

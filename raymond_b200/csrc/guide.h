@@ -13,6 +13,8 @@ namespace rmd {
 constexpr int GUIDE_PARAMS = GUIDE_HIDDEN * GUIDE_INPUTS + GUIDE_HIDDEN + 2 * (GUIDE_HIDDEN * GUIDE_HIDDEN + GUIDE_HIDDEN) +
                              GUIDE_OUTPUTS * GUIDE_HIDDEN + GUIDE_OUTPUTS;
 constexpr int GUIDE_TRAIN_MAX_BLOCKS = 256;  // blocks of one training launch (each writes its gradient)
+// net.partials: GUIDE_TRAIN_MAX_BLOCKS gradient slots, then one loss share per block
+constexpr size_t GUIDE_PARTIAL_LOSS = (size_t)GUIDE_TRAIN_MAX_BLOCKS * GUIDE_PARAMS;
 constexpr int GUIDE_WEIGHTS = GUIDE_HIDDEN * GUIDE_INPUTS + 2 * GUIDE_HIDDEN * GUIDE_HIDDEN + GUIDE_OUTPUTS * GUIDE_HIDDEN;
 
 // Device view of the network: FP32 master parameters (row-major [out][in]
@@ -22,7 +24,7 @@ struct GuideNetView {
     const uint16_t *w[4];  // bf16 weights per layer, row-major [out][in]
     const float *b[4];     // fp32 biases (inside `master`)
     float *master, *adamM, *adamV, *grad;  // GUIDE_PARAMS each
-    float *partials;                        // per training block: its gradient (GUIDE_TRAIN_MAX_BLOCKS x GUIDE_PARAMS)
+    float *partials;                        // per training block: its gradient, then its loss (GUIDE_PARTIAL_LOSS)
     uint16_t *weightsBf16;                  // GUIDE_WEIGHTS
     const int *bf16Index;                   // per parameter: index into weightsBf16, or -1 (bias)
     int wOffset[4], bOffset[4];             // parameter offsets of each layer's weights / biases
@@ -46,8 +48,10 @@ cudaError_t rmdLaunchGuideTrain(const rmd::GuideRecord *rec, uint32_t total, uin
                                 const rmd::GuideNetView &net, float *scratch, int blocks, float lr, int step,
                                 uint32_t *errors, cudaStream_t s);
 // Adam (beta 0.9 / 0.999, eps 1e-8, `step` from 1) on net.grad plus the first
-// `blocks` per-CTA gradients; refreshes the BF16 weights and clears net.grad
-cudaError_t rmdLaunchGuideAdam(const rmd::GuideNetView &net, int blocks, float lr, int step, cudaStream_t s);
+// `blocks` per-CTA gradients; refreshes the BF16 weights, clears net.grad and
+// writes the sum of the blocks' loss shares to *lossOut (when not NULL)
+cudaError_t rmdLaunchGuideAdam(const rmd::GuideNetView &net, int blocks, float lr, int step, float *lossOut,
+                               cudaStream_t s);
 // status[0] = 1 if a tensor-core wait expired
 cudaError_t rmdLaunchGuideForwardTest(const float *features, uint32_t n, const rmd::GuideNetView &net, float *out,
                                       int *status, cudaStream_t s);

@@ -50,9 +50,17 @@ void mkdirs(const std::string &path) {
     }
 }
 
+// RMD_JIT_FMAD=0 compiles the shading module without multiply-add
+// contraction (NVRTC contracts by default), the evaluation order of the
+// oracle's host build.
 const std::vector<const char *> &options() {
-    static std::vector<const char *> o = {"--gpu-architecture=sm_100a", "-std=c++17", "-lineinfo", "-DRMD_JIT=1",
-                                          "--device-as-default-execution-space"};
+    static std::vector<const char *> o = [] {
+        std::vector<const char *> v = {"--gpu-architecture=sm_100a", "-std=c++17", "-lineinfo", "-DRMD_JIT=1",
+                                       "--device-as-default-execution-space"};
+        const char *f = std::getenv("RMD_JIT_FMAD");
+        if (f && std::string(f) == "0") v.push_back("--fmad=false");
+        return v;
+    }();
     return o;
 }
 

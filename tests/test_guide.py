@@ -104,9 +104,11 @@ def test_guide_gradient_matches_oracle(gpu_ctx):
 @pytest.mark.gpu
 def test_guide_adam_matches_oracle(gpu_ctx):
     """The device Adam step (k_guide_adam) against the float64 Adam of the
-    oracle, for a first step and a later one with non-zero moments: new
-    parameters within 1e-6 relative (+1e-9), moments within 1e-5 relative,
-    and the BF16 weight copy equal to the new FP32 weights rounded."""
+    oracle (with the device's FP32 coefficients), for a first step and a
+    later one with non-zero moments: new parameters within 1e-6 relative
+    (+1e-9), moments within 1e-5 relative (+1e-9 for the first moment, whose
+    two terms can cancel), and the BF16 weight copy equal to the new FP32
+    weights rounded."""
     rng = np.random.default_rng(21)
     n = api.guide_param_count()
     params = G.init_params(4)
@@ -117,7 +119,7 @@ def test_guide_adam_matches_oracle(gpu_ctx):
         m32, v32 = m.astype(np.float32), v.astype(np.float32)
         p_g, m_g, v_g, bits = api.guide_adam(params, grad, m32, v32, step, 1e-3)
         p_c, m_c, v_c = G.adam_step(params, grad, m32, v32, step, 1e-3)
-        np.testing.assert_allclose(m_g, m_c, rtol=1e-5, atol=1e-12)
+        np.testing.assert_allclose(m_g, m_c, rtol=1e-5, atol=1e-9)
         np.testing.assert_allclose(v_g, v_c, rtol=1e-5, atol=1e-15)
         np.testing.assert_allclose(p_g, p_c, rtol=1e-6, atol=1e-9)
         wmask = G.weight_mask()
