@@ -216,7 +216,11 @@ bool Bvh::intersect(float3 org, float3 dir, float tmin, float tmax, HitRecord &h
             for (int i = 0; i < n.count; i++) {
                 const Tri &tr = tris_[n.first + i];
                 float t, b0, b1;
-                if (intersectTriangle(wr, tr.v0, tr.v1, tr.v2, tmin, best, t, b0, b1)) {
+                // equal distances go to the lower (instance, primitive), so the
+                // result does not depend on the tree's visiting order
+                if (intersectTriangle(wr, tr.v0, tr.v1, tr.v2, tmin, best, t, b0, b1) &&
+                    (t < best || !found || tr.instance < hit.instance ||
+                     (tr.instance == hit.instance && tr.prim < hit.prim))) {
                     best = t;
                     found = true;
                     hit.t = t;

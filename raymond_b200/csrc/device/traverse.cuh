@@ -182,6 +182,7 @@ struct TraversalState {
     TraceRay r;
     float tmin, tmax;  // tmax shrinks to the closest hit found so far
     int hitTri;        // closest (any-hit: first) triangle hit, -1 if none
+    uint32_t hitInst, hitPrim;  // its instance and primitive (the tie-break key)
     float b0, b1;
     uint2 group;       // node group being visited
     int sp;            // stack depth, -1 when finished
@@ -199,6 +200,7 @@ RMD_HD void beginTraversal(TraversalState &s, const WideNode *nodes, float3 o, f
     s.tmin = tmin;
     s.tmax = tmax;
     s.hitTri = -1;
+    s.hitInst = s.hitPrim = 0xffffffffu;
     s.b0 = s.b1 = 0.0f;
     // a virtual parent whose only inner child, in slot 0, is the root
     s.group = make_uint2(0u, (1u << (24u + rayOctant(s.r.idir))) | 1u);
@@ -213,12 +215,9 @@ RMD_HD void beginTraversal(TraversalState &s, const WideNode *nodes, float3 o, f
 // culls what follows.  ANY: stop at the first hit (raytrace.metal:52-85);
 // otherwise keep the closest (raytrace.metal:11-50).  (Dynamic ray fetch,
 // Aila & Laine, HPG 2009, measured slower with this tree too.)
-// `budget` bounds the node visits of this call: when it runs out the
-// traversal pauses (its group and stack depth kept in `s`) and a later call
-// resumes it.
 template <bool ANY>
 RMD_HD void traverse(TraversalState &s, TraversalStack &stack, const WideNode *__restrict__ nodes,
-                     const float4 *__restrict__ tris, uint32_t *errors, int budget = 0x7fffffff) {
+                     const float4 *__restrict__ tris, uint32_t *errors) {
     if (s.sp < 0) return;
     const float3 idir = s.r.idir, org = s.r.org;
     const uint32_t octant = rayOctant(idir);
@@ -226,11 +225,6 @@ RMD_HD void traverse(TraversalState &s, TraversalStack &stack, const WideNode *_
     int sp = s.sp;
     while (true) {
         if (group.y > 0x00ffffffu) {
-            if (budget-- == 0) {  // pause before the next node
-                s.group = group;
-                s.sp = sp;
-                return;
-            }
             const uint32_t key = __ffs(group.y >> 24) - 1;
             group.y &= ~(1u << (24u + key));
             const uint32_t slot = key ^ octant;
@@ -253,14 +247,23 @@ RMD_HD void traverse(TraversalState &s, TraversalStack &stack, const WideNode *_
                 const float4 c = __ldg(&tris[3 * ti + 2]);
                 float t, b0, b1;
                 if (intersectTriangle(s.r.wr, xyz(a), xyz(b), xyz(c), s.tmin, s.tmax, t, b0, b1)) {
-                    s.hitTri = ti;
                     if (ANY) {
+                        s.hitTri = ti;
                         s.sp = -1;
                         return;
                     }
-                    s.tmax = t;
-                    s.b0 = b0;
-                    s.b1 = b1;
+                    // Equal distances (coplanar overlapping faces) go to the lower
+                    // (instance, primitive), whatever order the tree is visited in,
+                    // so every BVH of the scene reports the same closest hit.
+                    const uint32_t inst = __float_as_uint(a.w), prim = __float_as_uint(b.w);
+                    if (t < s.tmax || s.hitTri < 0 || inst < s.hitInst || (inst == s.hitInst && prim < s.hitPrim)) {
+                        s.hitTri = ti;
+                        s.hitInst = inst;
+                        s.hitPrim = prim;
+                        s.tmax = t;
+                        s.b0 = b0;
+                        s.b1 = b1;
+                    }
                 }
             }
         }

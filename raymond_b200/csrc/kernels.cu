@@ -148,48 +148,10 @@ __global__ void __launch_bounds__(256) k_film_regen(Context ctx, PathPool pool, 
 template <bool ANY, class Begin, class Finish>
 __device__ __forceinline__ void persistentTrace(const WideNode *__restrict__ sceneNodes,
                                                 const float4 *__restrict__ sceneTris, uint32_t *work, uint32_t n,
-                                                uint32_t *errors, Begin begin, Finish finish, int refill) {
+                                                uint32_t *errors, Begin begin, Finish finish) {
     TraversalState s;
     TraversalStack stack;
     const int lane = threadIdx.x & 31;
-    if (refill > 0) {
-        // Lanes whose ray finished take the next rays every `refill` node
-        // visits (one warp vote and one atomic per round), so a warp does not
-        // idle behind its longest traversal.
-        const WideNode *nodes = sceneNodes;
-        const float4 *tris = sceneTris;
-        uint32_t idx = 0;
-        bool have = false, exhausted = false;
-        while (true) {
-            const unsigned need = __ballot_sync(0xffffffffu, !have);
-            if (need && !exhausted) {
-                const int leader = __ffs(need) - 1;
-                uint32_t base = 0;
-                if (lane == leader) base = atomicAdd(work, (uint32_t)__popc(need));
-                base = __shfl_sync(0xffffffffu, base, leader);
-                if (base + __popc(need) >= n) exhausted = true;  // warp-uniform
-                if (!have) {
-                    const uint32_t mine = base + __popc(need & ((1u << lane) - 1u));
-                    if (mine < n) {
-                        idx = mine;
-                        have = true;
-                        nodes = sceneNodes;
-                        tris = sceneTris;
-                        begin(idx, s, stack, nodes, tris);
-                    }
-                }
-            }
-            if (__ballot_sync(0xffffffffu, have) == 0u) break;
-            if (have) {
-                traverse<ANY>(s, stack, nodes, tris, errors, refill);
-                if (s.sp < 0) {
-                    finish(idx, s, tris);
-                    have = false;
-                }
-            }
-        }
-        return;
-    }
     while (true) {
         uint32_t base = 0;
         if (lane == 0) base = atomicAdd(work, 32u);
@@ -209,7 +171,7 @@ __device__ __forceinline__ void persistentTrace(const WideNode *__restrict__ sce
 template <bool BATCH>
 __global__ void __launch_bounds__(128) k_trace_closest(const WideNode *__restrict__ sceneNodes,
                                                        const float4 *__restrict__ sceneTris, PathPool pool,
-                                                       Counters *cnt, uint32_t p, int refill) {
+                                                       Counters *cnt, uint32_t p) {
     const uint32_t n = activeCount(cnt, p);
     const PathState S = pool.s[p];
     persistentTrace<false>(
@@ -233,8 +195,7 @@ __global__ void __launch_bounds__(128) k_trace_closest(const WideNode *__restric
 
             if (found) pool.order[warpAppend(&cnt->nHit)] = idx;
             else pool.order[pool.capacity - 1u - warpAppend(&cnt->nMiss)] = idx;
-        },
-        refill);
+        });
 }
 
 // raytraceAny fused with handleShadowRays (shadow.metal:6-29): an unoccluded
@@ -245,7 +206,7 @@ __global__ void __launch_bounds__(128) k_trace_closest(const WideNode *__restric
 template <bool BATCH>
 __global__ void __launch_bounds__(128) k_trace_shadow(const WideNode *__restrict__ sceneNodes,
                                                       const float4 *__restrict__ sceneTris, PathPool pool,
-                                                      Counters *cnt, uint32_t p, int refill) {
+                                                      Counters *cnt, uint32_t p) {
     const uint32_t n = cnt->nShadow;
     if (blockIdx.x == 0 && threadIdx.x == 0) cnt->nextPath += newPaths(cnt, p);
     float4 *nextL = pool.s[p ^ 1u].L;
@@ -303,8 +264,7 @@ __global__ void __launch_bounds__(128) k_trace_shadow(const WideNode *__restrict
                     pool.records[k] = g;
                 }
             }
-        },
-        refill);
+        });
     blockAdd64(&cnt->shadowRays, traced);
 }
 
@@ -441,25 +401,16 @@ cudaError_t rmdLaunchFilmRegen(const Context &ctx, const PathPool &pool, const F
     else k_film_regen<false><<<blocks, 256, 0, s>>>(ctx, pool, fp, cnt, cur);
     return cudaGetLastError();
 }
-// Node visits between lane refills in the persistent traversal loops (0: a
-// warp takes 32 rays and traces them all to the end before the next 32).
-static int traceRefill() {
-    static const int r = [] {
-        const char *e = std::getenv("RMD_TRACE_REFILL");
-        return e ? std::max(0, std::atoi(e)) : 0;
-    }();
-    return r;
-}
 cudaError_t rmdLaunchTraceClosest(const WideNode *nodes, const float4 *tris, const PathPool &pool, Counters *cnt,
                                   uint32_t cur, int blocks, cudaStream_t s) {
-    if (pool.views) k_trace_closest<true><<<blocks, 128, 0, s>>>(nodes, tris, pool, cnt, cur, traceRefill());
-    else k_trace_closest<false><<<blocks, 128, 0, s>>>(nodes, tris, pool, cnt, cur, traceRefill());
+    if (pool.views) k_trace_closest<true><<<blocks, 128, 0, s>>>(nodes, tris, pool, cnt, cur);
+    else k_trace_closest<false><<<blocks, 128, 0, s>>>(nodes, tris, pool, cnt, cur);
     return cudaGetLastError();
 }
 cudaError_t rmdLaunchTraceShadow(const WideNode *nodes, const float4 *tris, const PathPool &pool, Counters *cnt,
                                  uint32_t cur, int blocks, cudaStream_t s) {
-    if (pool.views) k_trace_shadow<true><<<blocks, 128, 0, s>>>(nodes, tris, pool, cnt, cur, traceRefill());
-    else k_trace_shadow<false><<<blocks, 128, 0, s>>>(nodes, tris, pool, cnt, cur, traceRefill());
+    if (pool.views) k_trace_shadow<true><<<blocks, 128, 0, s>>>(nodes, tris, pool, cnt, cur);
+    else k_trace_shadow<false><<<blocks, 128, 0, s>>>(nodes, tris, pool, cnt, cur);
     return cudaGetLastError();
 }
 cudaError_t rmdLaunchEnvmapReduce(float *mip, int cur, cudaStream_t s) {
