@@ -79,6 +79,8 @@ BYTES_FILM_PER_PATH = 16 + 32 + 80
 # processed); only the closest-hit kernel's is used
 TRAFFIC_PER_UNIT = {"trace": 78.5}
 GUIDED_W, GUIDED_H, GUIDED_DEPTH, GUIDED_ORACLE_SPP, GUIDED_PLAIN_SPP, GUIDED_CHUNK = 1280, 720, 16, 65536, 1024, 32
+# guide settings of the guided legs (configs 4 and 5): Adam steps per 2^20 tracer samples, records per step
+GUIDE_DEFAULTS = {"batch_size": 1 << 20, "learning_rate": 1e-3, "steps_per_batch": 8, "step_records": 1 << 13}
 CPU_BASELINE_SPP = 16  # CPU sample: 16 one-spp frames of the full image (about 10-20 s on 16 cores)
 
 
@@ -327,7 +329,7 @@ def run_config5(args) -> dict:
     e_plain = errors(plain)
     plain.close()
     g = batch()
-    settings = {"batch_size": 1 << 20, "learning_rate": 1e-3, "steps_per_batch": 8, "step_records": 1 << 13}
+    settings = dict(GUIDE_DEFAULTS)
     g.set_guide(sampling=True, training=True, seed=1, **settings)
     ms, spp, parity, curve = 0.0, 0, None, []
     target = float(np.mean(e_plain))
@@ -361,9 +363,6 @@ def run_config5(args) -> dict:
 
 def desc_triangles(desc) -> int:
     return int(sum(len(s["indices"]) for s in desc.scene["shapes"]))
-
-
-GUIDE_DEFAULTS = {"batch_size": 1 << 20, "learning_rate": 1e-3, "steps_per_batch": 8, "step_records": 1 << 13}
 
 
 def guided_leg(api, ctx, oracle_spp: int, size=(GUIDED_W, GUIDED_H), guide: dict | None = None,

@@ -328,8 +328,9 @@ typedef struct rmd_render_settings {
     uint32_t sampling_mode;    /* RMD_SAMPLING_* (Uniforms.samplingMode) */
     uint32_t rng;              /* RMD_RNG_* */
     uint64_t seed;             /* PCG32 initstate */
-    int64_t first_sample;      /* <0: continue after the samples already in
-                                  the film; >=0: start at this sample index */
+    int64_t first_sample;      /* <0: continue after the highest sample index
+                                  rendered since the last reset; >=0: start at
+                                  this sample index */
     uint32_t film_fp64;        /* accumulate the film in double precision */
     uint32_t reserved;
 } rmd_render_settings;
@@ -454,7 +455,8 @@ rmd_status rmd_film_read(rmd_renderer *r, float *rgb, int32_t normalize, uint32_
 rmd_status rmd_film_save_exr(rmd_renderer *r, const char *path, float normalized_by, uint32_t compression);
 /* The double-precision film (settings.film_fp64), raw sums. */
 rmd_status rmd_film_read_f64(rmd_renderer *r, double *rgb);
-/* Samples accumulated in the film (frameIndex of Renderer.swift:288). */
+/* Samples accumulated in the film since the last reset, whatever their
+ * indices (frameIndex of Renderer.swift:288); what normalisation divides by. */
 rmd_status rmd_film_samples(const rmd_renderer *r, uint64_t *samples);
 /* Device address of the renderer's film: width * height float4 (RGB radiance
  * sums and a path count per pixel), row-major from the top-left pixel, on the

@@ -192,7 +192,8 @@ struct rmd_renderer {
     DevBuf counters, film, film64, resolve;
     Counters *hostCounters = nullptr;  // pinned
     Context dctx{};
-    uint64_t samples = 0;
+    uint64_t samples = 0;     // samples accumulated in the film (what normalisation divides by)
+    uint64_t nextSample = 0;  // sample index a render continues at (first_sample < 0)
     rmd_stats stats{};
     cudaEvent_t ev[4] = {};
     std::vector<cudaEvent_t> stageEvents;  // recorded between the stage kernels
@@ -238,7 +239,8 @@ struct rmd_batch {
     bool useGraph = true;
     GuideState guide;  // learned path guiding (all views of one scene)
     int guideScene = -1;
-    uint64_t samples = 0;
+    uint64_t samples = 0;     // samples of every view accumulated in the films
+    uint64_t nextSample = 0;  // sample index a render continues at (first_sample < 0)
     rmd_stats stats{};
     cudaEvent_t ev[2] = {};
     // the instantiated render graph and the settings it was captured for
@@ -1051,6 +1053,7 @@ rmd_status rmd_renderer_reset(rmd_renderer *r) {
     if (r->film64.ptr) RMD_CUDA(cudaMemsetAsync(r->film64.ptr, 0, r->film64.bytes, st));
     RMD_CUDA(cudaStreamSynchronize(st));
     r->samples = 0;
+    r->nextSample = 0;
     return RMD_OK;
 }
 
@@ -1108,7 +1111,7 @@ rmd_status rmd_render(rmd_renderer *r, const rmd_render_settings *s) {
     RMD_CUDA(cudaSetDevice(ctx->device));
     cudaStream_t st = ctx->stream;
     const uint64_t numPixels = (uint64_t)r->width * r->height;
-    const uint64_t firstSample = s->first_sample >= 0 ? (uint64_t)s->first_sample : r->samples;
+    const uint64_t firstSample = s->first_sample >= 0 ? (uint64_t)s->first_sample : r->nextSample;
     const uint64_t numPaths = (uint64_t)s->spp * numPixels;
     if (firstSample + s->spp > 0xffffffffull) return fail(RMD_ERROR_INVALID_ARGUMENT, "sample index overflow");
     if (s->film_fp64 && !r->film64.ptr) {
@@ -1238,7 +1241,8 @@ rmd_status rmd_render(rmd_renderer *r, const rmd_render_settings *s) {
     r->stats.ms_shadow = stage[STAGE_SHADOW];
     r->stats.ms_guide = stage[STAGE_GUIDE] + stage[STAGE_TRAIN];
     r->stats.ms_guide_train = stage[STAGE_TRAIN];
-    r->samples = std::max<uint64_t>(r->samples, firstSample + s->spp);
+    r->samples += s->spp;
+    r->nextSample = std::max<uint64_t>(r->nextSample, firstSample + s->spp);
     return RMD_OK;
 }
 
@@ -1778,6 +1782,7 @@ rmd_status rmd_batch_reset(rmd_batch *b) {
     if (b->film64.ptr) RMD_CUDA(cudaMemsetAsync(b->film64.ptr, 0, b->film64.bytes, st));
     RMD_CUDA(cudaStreamSynchronize(st));
     b->samples = 0;
+    b->nextSample = 0;
     return RMD_OK;
 }
 
@@ -1811,7 +1816,7 @@ rmd_status rmd_batch_render(rmd_batch *b, const rmd_render_settings *s) {
     rmd_context *ctx = b->ctx;
     RMD_CUDA(cudaSetDevice(ctx->device));
     cudaStream_t st = ctx->stream;
-    const uint64_t firstSample = s->first_sample >= 0 ? (uint64_t)s->first_sample : b->samples;
+    const uint64_t firstSample = s->first_sample >= 0 ? (uint64_t)s->first_sample : b->nextSample;
     if (firstSample + s->spp > BATCH_SAMPLE_MASK)
         return fail(RMD_ERROR_INVALID_ARGUMENT, "batch sample index beyond 2^24");
     const uint64_t numPaths = (uint64_t)s->spp * b->totalPixels;
@@ -1932,7 +1937,8 @@ rmd_status rmd_batch_render(rmd_batch *b, const rmd_render_settings *s) {
     b->stats.invalid_samples = h.invalid;
     b->stats.iterations = iterations;
     b->stats.ms_total = ms;
-    b->samples = std::max<uint64_t>(b->samples, firstSample + s->spp);
+    b->samples += s->spp;
+    b->nextSample = std::max<uint64_t>(b->nextSample, firstSample + s->spp);
     if (trainSteps) return guideReadLoss(guide);
     return RMD_OK;
 }

@@ -367,3 +367,29 @@ def test_sky_world_per_sample(gpu_ctx, sky_type):
     r = api.Renderer(scene, 96, 96)
     r.render(spp=1, max_depth=8, first_sample=0)
     assert np.isfinite(r.film()).all() and r.film().sum() > 0
+
+
+def test_film_device_view_and_sample_count(cornell):
+    """rmd_film_device: a zero-copy torch view of the renderer's film equals the
+    read-back film; a film summed into it (as the ranks' films are by the NCCL
+    reduce) is what rmd_film_read returns, normalised by the sample count set
+    with rmd_film_set_samples."""
+    import torch
+
+    desc, scene, orc = cornell
+    a = api.Renderer(scene, 64, 48)
+    b = api.Renderer(scene, 64, 48)
+    a.render(spp=2, max_depth=8, first_sample=0)
+    b.render(spp=2, max_depth=8, first_sample=2)
+    ta, tb = a.film_tensor(), b.film_tensor()
+    assert ta.shape == (48, 64, 4) and ta.is_cuda
+    torch.cuda.synchronize()
+    np.testing.assert_array_equal(ta[..., :3].cpu().numpy(), a.film())
+    assert torch.all(ta[..., 3] == 2)  # two paths per pixel
+    ta += tb  # the sum a reduce over two ranks leaves in rank 0's film
+    torch.cuda.synchronize()
+    a.set_samples(4)
+    assert a.samples() == 4
+    cpu, _ = orc.render(64, 48, 4, 8, first_sample=0)
+    assert match_fraction(a.film(), cpu) >= MIN_MATCH
+    np.testing.assert_allclose(a.film(normalize=True), a.film() / 4, rtol=1e-6)
