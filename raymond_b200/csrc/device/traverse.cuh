@@ -117,28 +117,6 @@ RMD_HD float byteToFloat(uint32_t w, uint32_t i) {
     return __uint_as_float(__byte_perm(w, 0x4B000000u, 0x7540u | i)) - 8388608.0f;
 }
 
-// Paired FP32 operations (one instruction for two lanes' worth of work on
-// sm_100): each half is rounded exactly as the scalar fmaf / add.
-RMD_HD float2 ffma2(float2 a, float2 b, float2 c) {
-    float2 d;
-    asm("{\n.reg .b64 ra, rb, rc, rd;\nmov.b64 ra, {%2, %3};\nmov.b64 rb, {%4, %5};\nmov.b64 rc, {%6, %7};\n"
-        "fma.rn.f32x2 rd, ra, rb, rc;\nmov.b64 {%0, %1}, rd;\n}\n"
-        : "=f"(d.x), "=f"(d.y)
-        : "f"(a.x), "f"(a.y), "f"(b.x), "f"(b.y), "f"(c.x), "f"(c.y));
-    return d;
-}
-// bytes i of w0 and of w1 as floats (the byteToFloat trick with one paired subtract)
-RMD_HD float2 bytesToFloat2(uint32_t w0, uint32_t w1, uint32_t i) {
-    const float a = __uint_as_float(__byte_perm(w0, 0x4B000000u, 0x7540u | i));
-    const float b = __uint_as_float(__byte_perm(w1, 0x4B000000u, 0x7540u | i));
-    float2 d;
-    asm("{\n.reg .b64 ra, rb, rd;\nmov.b64 ra, {%2, %3};\nmov.b64 rb, {%4, %4};\nadd.rn.f32x2 rd, ra, rb;\n"
-        "mov.b64 {%0, %1}, rd;\n}\n"
-        : "=f"(d.x), "=f"(d.y)
-        : "f"(a), "f"(b), "f"(-8388608.0f));
-    return d;
-}
-
 // Ray/box tests of a node's 8 children.  Returns the children the ray enters
 // within [tmin, tmax]: inner children as bits 24 + (slot ^ octant) (so the
 // lowest bit is the nearest child in the node's octant order), leaf
@@ -170,7 +148,6 @@ RMD_HD uint32_t intersectChildren(const WideNode &n, const float3 idir, const fl
     const uint2 nearY = ny ? hiY : loY, farY = ny ? loY : hiY;
     const uint2 nearZ = nz ? hiZ : loZ, farZ = nz ? loZ : hiZ;
     uint32_t hits = 0;
-#ifdef RMD_TRAVERSE_SCALAR_BOX
 #pragma unroll
     for (int half = 0; half < 2; half++) {
         const uint32_t nxw = half ? nearX.y : nearX.x, fxw = half ? farX.y : farX.x;
@@ -185,43 +162,12 @@ RMD_HD uint32_t intersectChildren(const WideNode &n, const float3 idir, const fl
             const float t0z = fmaf(byteToFloat(nzw, i), az, bzN), t1z = fmaf(byteToFloat(fzw, i), az, bzF);
             const float enter = fmaxf(fmaxf(t0x, t0y), fmaxf(t0z, tmin));
             const float leave = fminf(fminf(t1x, t1y), fminf(t1z, tmax));
-            if (enter <= leave * 1.0000004f) {
-                if ((imask >> slot) & 1u) {
-                    hits |= 1u << (24u + (slot ^ octant));
-                } else {
-                    const uint32_t meta = (metaw >> (8 * i)) & 0xffu;
-                    hits |= (meta >> 5) << (meta & 31u);
-                }
-            }
-        }
-    }
-    return hits;
-#endif
-    const float2 ax2 = make_float2(ax, ax), ay2 = make_float2(ay, ay), az2 = make_float2(az, az);
-    const float2 bxN2 = make_float2(bxN, bxN), bxF2 = make_float2(bxF, bxF), byN2 = make_float2(byN, byN);
-    const float2 byF2 = make_float2(byF, byF), bzN2 = make_float2(bzN, bzN), bzF2 = make_float2(bzF, bzF);
-    // slots i and i + 4 in the two halves of each paired operation
-#pragma unroll
-    for (uint32_t i = 0; i < 4; i++) {
-        const float2 t0x = ffma2(bytesToFloat2(nearX.x, nearX.y, i), ax2, bxN2);
-        const float2 t1x = ffma2(bytesToFloat2(farX.x, farX.y, i), ax2, bxF2);
-        const float2 t0y = ffma2(bytesToFloat2(nearY.x, nearY.y, i), ay2, byN2);
-        const float2 t1y = ffma2(bytesToFloat2(farY.x, farY.y, i), ay2, byF2);
-        const float2 t0z = ffma2(bytesToFloat2(nearZ.x, nearZ.y, i), az2, bzN2);
-        const float2 t1z = ffma2(bytesToFloat2(farZ.x, farZ.y, i), az2, bzF2);
-#pragma unroll
-        for (int half = 0; half < 2; half++) {
-            const uint32_t slot = 4 * half + i;
-            const float enter = fmaxf(fmaxf(half ? t0x.y : t0x.x, half ? t0y.y : t0y.x),
-                                      fmaxf(half ? t0z.y : t0z.x, tmin));
-            const float leave = fminf(fminf(half ? t1x.y : t1x.x, half ? t1y.y : t1y.x),
-                                      fminf(half ? t1z.y : t1z.x, tmax));
             // widen the far bound by a few ulps (Ize 2013) so FMA rounding never culls a hit
             if (enter <= leave * 1.0000004f) {
                 if ((imask >> slot) & 1u) {
                     hits |= 1u << (24u + (slot ^ octant));
                 } else {
-                    const uint32_t meta = ((half ? n.bases.w : n.bases.z) >> (8 * i)) & 0xffu;
+                    const uint32_t meta = (metaw >> (8 * i)) & 0xffu;
                     hits |= (meta >> 5) << (meta & 31u);
                 }
             }

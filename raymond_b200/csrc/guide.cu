@@ -531,7 +531,7 @@ struct TrainSmem {
     uint16_t rowB[kTrThreads * GUIDE_HIDDEN];   // layer-1 inputs, then layer-3 inputs; deltas
     float b[3 * GUIDE_HIDDEN + GUIDE_OUTPUTS];
     float db[3 * GUIDE_HIDDEN + GUIDE_OUTPUTS];  // the CTA's bias gradient
-    float reduce[8];                             // per warp: target sums, then loss sums
+    float reduce[8];                             // per warp: loss sums
     unsigned long long mbar;
     uint32_t tmemBase;
     int failed;
@@ -669,23 +669,34 @@ __device__ void trDeltaEpilogue(TrainSmem &sm, uint32_t taddr, uint64_t mask, ui
     }
 }
 
+// The sum of the batch's targets (the loss normalises them by their mean),
+// written to *sum by one block: no atomics, so nothing to clear first.
+constexpr int kSumThreads = 1024;
+__global__ void __launch_bounds__(kSumThreads) k_guide_sum_y(RecordBatch batch, float *sum) {
+    __shared__ float part[kSumThreads / 32];
+    float s = 0.0f;
+#pragma unroll 8
+    for (uint32_t i = threadIdx.x; i < batch.n; i += kSumThreads) s += batch.pick(i).y;
+    for (int off = 16; off > 0; off >>= 1) s += __shfl_xor_sync(0xffffffffu, s, off);
+    if ((threadIdx.x & 31) == 0) part[threadIdx.x >> 5] = s;
+    __syncthreads();
+    if (threadIdx.x < 32) {
+        s = part[threadIdx.x];
+        for (int off = 16; off > 0; off >>= 1) s += __shfl_xor_sync(0xffffffffu, s, off);
+        if (threadIdx.x == 0) *sum = s;
+    }
+}
+
 // The gradient of the mean loss over a batch of records on the tensor cores:
 // each CTA writes its gradient (weights and biases) to its slot of
 // net.partials and its share of the loss to partials[GUIDE_PARTIAL_LOSS + CTA];
-// the Adam (or reduce) kernel sums them.  Every CTA sums the batch's targets
-// itself (the loss normalises them by their mean), so a step is this kernel
-// and the Adam step.  On an expired wait the CTA sets ERR_GUIDE_TIMEOUT in
-// *errors and writes a zero gradient.
-__global__ void __launch_bounds__(kTrThreads, 1) k_guide_train_tc(RecordBatch batch, GuideNetView net,
-                                                                uint32_t *errors) {
+// the Adam (or reduce) kernel sums them.  On an expired wait the CTA sets
+// ERR_GUIDE_TIMEOUT in *errors and writes a zero gradient.
+__global__ void __launch_bounds__(kTrThreads, 1) k_guide_train_tc(RecordBatch batch, const float *sumY,
+                                                                GuideNetView net, uint32_t *errors) {
     extern __shared__ __align__(16) unsigned char smem[];
     TrainSmem &sm = *reinterpret_cast<TrainSmem *>(smem);
     const int row = threadIdx.x, warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-    // the batch's targets (L2-resident records), summed while the weights load
-    float ySum = 0.0f;
-    for (uint32_t i = threadIdx.x; i < batch.n; i += blockDim.x) ySum += batch.pick(i).y;
-    for (int off = 16; off > 0; off >>= 1) ySum += __shfl_xor_sync(0xffffffffu, ySum, off);
-    if (lane == 0) sm.reduce[warp] = ySum;
     // set-up: weights (forward and transposed), biases, mbarrier, tensor memory
     loadCanonical(sm.w0, net.w[0], GUIDE_HIDDEN, GUIDE_INPUTS);
     loadCanonical(sm.w1, net.w[1], GUIDE_HIDDEN, GUIDE_HIDDEN);
@@ -715,8 +726,7 @@ __global__ void __launch_bounds__(kTrThreads, 1) k_guide_train_tc(RecordBatch ba
     const uint32_t taddr = tmem + ((uint32_t)(row & ~31) << 16);  // this warp's lanes, work columns
     const uint32_t n = batch.n;
     const float scale = 1.0f / (float)n;
-    const float sumY = sm.reduce[0] + sm.reduce[1] + sm.reduce[2] + sm.reduce[3];  // published by trPublish
-    const float invMeanY = sumY > 0.0f ? (float)n / sumY : 0.0f;
+    const float invMeanY = sumY[0] > 0.0f ? (float)n / sumY[0] : 0.0f;
     const uint32_t tiles = (n + kTrThreads - 1) / kTrThreads;
     float lossSum = 0.0f;
     uint32_t phase = 0;
@@ -867,11 +877,11 @@ __global__ void __launch_bounds__(kTrThreads, 1) k_guide_train_tc(RecordBatch ba
         part[net.bOffset[l] + i - l * GUIDE_HIDDEN] = have ? sm.db[i] : 0.0f;
     }
     for (int off = 16; off > 0; off >>= 1) lossSum += __shfl_xor_sync(0xffffffffu, lossSum, off);
-    if (lane == 0) sm.reduce[4 + warp] = lossSum;
+    if (lane == 0) sm.reduce[warp] = lossSum;
     __syncthreads();
     if (threadIdx.x == 0)
         net.partials[GUIDE_PARTIAL_LOSS + blockIdx.x] =
-            ok ? (sm.reduce[4] + sm.reduce[5] + sm.reduce[6] + sm.reduce[7]) * scale : 0.0f;
+            ok ? (sm.reduce[0] + sm.reduce[1] + sm.reduce[2] + sm.reduce[3]) * scale : 0.0f;
     if (!ok && threadIdx.x == 0 && errors) atomicOr(errors, ERR_GUIDE_TIMEOUT);
     // teardown: a last bounded wait for work in flight after an expired wait, then free tensor memory
     if (!ok) mbarWait(smemU32(&sm.mbar), phase);
@@ -1067,15 +1077,17 @@ cudaError_t rmdLaunchGuideInfer(const Context &ctx, const PathPool &pool, Counte
 cudaError_t rmdLaunchGuideTrain(const GuideRecord *rec, uint32_t total, uint32_t n, uint32_t seed,
                                 const GuideNetView &net, float *scratch, int blocks, float lr, int step,
                                 uint32_t *errors, cudaStream_t s) {
-    // scratch[1]: the step's mean loss (written by the Adam step)
+    // scratch[0]: the batch's target sum, scratch[1]: the step's mean loss (written by the Adam step)
     if (total == 0) return cudaSuccess;
     RecordBatch batch{rec, total, std::min(n, total), seed};
+    k_guide_sum_y<<<1, kSumThreads, 0, s>>>(batch, scratch);
+    cudaError_t e = cudaGetLastError();
+    if (e != cudaSuccess) return e;
     // one CTA per tile of 128 records, at most `blocks` (each CTA then takes several tiles)
     const int tiles = (int)((batch.n + kTrThreads - 1) / kTrThreads);
     blocks = std::max(1, std::min(std::min(blocks, tiles), GUIDE_TRAIN_MAX_BLOCKS));
-    k_guide_train_tc<<<blocks, kTrThreads, rmdGuideSharedBytes(true), s>>>(batch, net, errors);
-    cudaError_t e = cudaGetLastError();
-    if (e != cudaSuccess) return e;
+    k_guide_train_tc<<<blocks, kTrThreads, rmdGuideSharedBytes(true), s>>>(batch, scratch, net, errors);
+    if ((e = cudaGetLastError()) != cudaSuccess) return e;
     return rmdLaunchGuideAdam(net, blocks, lr, step, scratch + 1, s);
 }
 
@@ -1098,13 +1110,15 @@ cudaError_t rmdLaunchGuideForwardTest(const float *features, uint32_t n, const G
 
 cudaError_t rmdLaunchGuideGradientTest(const GuideRecord *rec, uint32_t n, const GuideNetView &net, float *scratch,
                                        int blocks, cudaStream_t s) {
-    // scratch[1]: mean loss, [2]: error flags
+    // scratch[0]: target sum, [1]: mean loss, [2]: error flags
     cudaError_t e = cudaMemsetAsync(scratch, 0, 3 * sizeof(float), s);
     if (e != cudaSuccess || n == 0) return e;
     RecordBatch batch{rec, n, n, 0};
+    k_guide_sum_y<<<1, kSumThreads, 0, s>>>(batch, scratch);
+    if ((e = cudaGetLastError()) != cudaSuccess) return e;
     const int tiles = (int)((n + kTrThreads - 1) / kTrThreads);
     blocks = std::max(1, std::min(std::min(blocks, tiles), GUIDE_TRAIN_MAX_BLOCKS));
-    k_guide_train_tc<<<blocks, kTrThreads, rmdGuideSharedBytes(true), s>>>(batch, net,
+    k_guide_train_tc<<<blocks, kTrThreads, rmdGuideSharedBytes(true), s>>>(batch, scratch, net,
                                                                            reinterpret_cast<uint32_t *>(scratch + 2));
     if ((e = cudaGetLastError()) != cudaSuccess) return e;
     k_guide_reduce<<<(GUIDE_PARAMS + 255) / 256, 256, 0, s>>>(net, blocks, scratch + 1);
