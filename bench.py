@@ -321,6 +321,8 @@ def run_config5(args) -> dict:
 
     def errors(b):
         return [relmse(b.film(v, normalize=True), refs[v]) for v in range(8)]
+    sampler = ClockSampler(0)
+    sampler.start()
     plain = batch()
     plain_ms = 0.0
     for _ in range(GUIDED_PLAIN_SPP // chunk):
@@ -345,8 +347,10 @@ def run_config5(args) -> dict:
     e_guided = errors(g)
     st = g.guide_stats()
     g.close()
+    clocks = sampler.stop()
     return {
         "metric": "time to the plain tracer's 1024-spp relMSE, guided batch (config 5)",
+        "clocks": clocks,
         "value": parity[1] / plain_ms if parity else None, "unit": "fraction of the plain batch's time",
         "higher_is_better": False, "n_gpus": 1,
         "config": {"workload": f"glossy_rooms_grid_4x4_8views_{W}x{H}_depth{depth}",
