@@ -548,7 +548,13 @@ def main():
         tune = None if args.no_autotune else r.autotune(spp=SPP, max_depth=DEPTH, seed=SEED)
     tune_s = time.perf_counter() - t0
     cam = desc.scene["camera"]
-    film_host = np.zeros((H, W, 3), np.float32)
+    # the frame's host buffer in pinned memory (the device -> host read of every e2e step)
+    try:
+        import torch
+
+        film_host = torch.empty((H, W, 3), dtype=torch.float32, pin_memory=True).numpy()
+    except (ImportError, RuntimeError):
+        film_host = np.zeros((H, W, 3), np.float32)
 
     def step(k, e2e=False):
         first, _ = sample_range(rank, world, k, SPP)
@@ -558,7 +564,7 @@ def main():
             r.reset()
         r.render(spp=SPP, max_depth=DEPTH, seed=SEED, first_sample=first)
         if e2e:
-            film_host[:] = r.film()  # device -> host: the frame
+            r.film(out=film_host)  # device -> host: the frame
         return r.stats()
 
     for k in range(args.warmup):

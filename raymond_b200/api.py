@@ -254,8 +254,14 @@ class Renderer:
         s = RenderSettings(spp, max_depth, sampling_mode, rng, seed, first_sample, int(film_fp64), 0)
         check(lib().rmd_render(self.h, C.byref(s)))
 
-    def film(self, normalize: bool = False, tonemapping: int = _abi.TONEMAP_LINEAR, exposure: float = 1.0) -> np.ndarray:
-        out = np.zeros((self.height, self.width, 3), np.float32)
+    def film(self, normalize: bool = False, tonemapping: int = _abi.TONEMAP_LINEAR, exposure: float = 1.0,
+             out: np.ndarray | None = None) -> np.ndarray:
+        """The film (H, W, 3) float32 (rmd_film_read); `out`: a C-contiguous float32
+        array of that shape to read into (e.g. in pinned host memory)."""
+        if out is None:
+            out = np.zeros((self.height, self.width, 3), np.float32)
+        elif out.shape != (self.height, self.width, 3) or out.dtype != np.float32 or not out.flags.c_contiguous:
+            raise ValueError("out must be a C-contiguous float32 array of shape (height, width, 3)")
         check(lib().rmd_film_read(self.h, _f32p(out), int(normalize), tonemapping, exposure))
         return out
 
