@@ -74,7 +74,8 @@ void oracle_sky_data(float sun_elevation, float sun_rotation, int32_t sun_disc, 
 /* n values of PrngState.sample() for the stream (a, b): TEA(a, b) or PCG32(seed=a, seq=b). */
 void oracle_prng(int32_t mode, uint64_t a, uint64_t b, int32_t n, float *out);
 /* rays: n x 8 floats (origin, tmin, direction, tmax); out: n x 4 (t, b0, b1, as-float prim)
- * plus n instance ids; any != 0 runs the occlusion query (t = 1 occluded, -1 not). */
+ * plus n instance ids; any = 1 runs the occlusion query (t = 1 occluded, -1 not); any = 2 the
+ * closest-hit query without culling against the best hit so far (every box the ray enters). */
 int oracle_trace(const oracle_scene *s, const float *rays, int32_t n, int32_t any, float *out, uint32_t *instances);
 /* Perlin/fractal noise of utils/noise.hpp at n points (x,y,z): out[i] = fractal_noise(p, detail, roughness). */
 void oracle_fractal_noise3(const float *p, int32_t n, float detail, float roughness, float *out);

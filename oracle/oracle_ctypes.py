@@ -14,6 +14,11 @@ import numpy as np
 
 HERE = Path(__file__).resolve().parent
 LIB = HERE / "_build" / "liboracle.so"
+# The same sources built with fused multiply-adds contracted (-ffp-contract=fast
+# -mfma): every result may move by an ulp or so.  Rendering a scene with both
+# measures how far the scene's own arithmetic amplifies rounding, the noise
+# floor against which another implementation's per-sample match is judged.
+LIB_FMA = HERE / "_build" / "liboracle_fma.so"
 
 
 class OracleSettings(C.Structure):
@@ -29,15 +34,24 @@ def build() -> Path:
     return LIB
 
 
-_lib = None
+_libs = {}
 
 
-def lib():
-    global _lib
-    if _lib is None:
-        if not LIB.exists():
+def fma_available() -> bool:
+    """The contracted build needs a host CPU with FMA instructions."""
+    try:
+        return any(line.startswith("flags") and " fma " in line + " " for line in open("/proc/cpuinfo"))
+    except OSError:
+        return False
+
+
+def lib(variant: str = ""):
+    """The oracle library; variant "fma" is the contracted build (LIB_FMA)."""
+    if variant not in _libs:
+        path = {"": LIB, "fma": LIB_FMA}[variant]
+        if not path.exists():
             build()
-        L = C.CDLL(str(LIB))
+        L = C.CDLL(str(path))
         L.oracle_scene_create.argtypes = [C.c_void_p, C.POINTER(C.c_void_p), C.c_char_p, C.c_int]
         L.oracle_scene_destroy.argtypes = [C.c_void_p]
         L.oracle_surface_emissive.argtypes = [C.c_void_p, C.POINTER(C.c_uint8)]
@@ -57,8 +71,8 @@ def lib():
         L.oracle_sky_data.argtypes = [C.c_float, C.c_float, C.c_int32] + [C.c_float] * 5 + [C.POINTER(C.c_float)]
         L.oracle_normalize_image.argtypes = [C.POINTER(C.c_float), C.c_uint32, C.c_uint32, C.c_float, C.c_int32,
                                              C.c_uint32, C.c_uint32, C.POINTER(C.c_float)]
-        _lib = L
-    return _lib
+        _libs[variant] = L
+    return _libs[variant]
 
 
 def _f32(a):
@@ -66,24 +80,25 @@ def _f32(a):
 
 
 class OracleScene:
-    def __init__(self, desc):
-        """desc: raymond_b200._abi.SceneDesc"""
+    def __init__(self, desc, variant: str = ""):
+        """desc: raymond_b200._abi.SceneDesc; variant: "" or "fma" (see LIB_FMA)."""
         self.desc = desc
+        self.L = lib(variant)
         self.h = C.c_void_p()
         err = C.create_string_buffer(512)
-        st = lib().oracle_scene_create(C.byref(desc.c), C.byref(self.h), err, 512)
+        st = self.L.oracle_scene_create(C.byref(desc.c), C.byref(self.h), err, 512)
         if st != 0:
             raise RuntimeError(f"oracle_scene_create failed ({st}): {err.value.decode()}")
 
     def __del__(self):
         if getattr(self, "h", None) and self.h.value:
-            lib().oracle_scene_destroy(self.h)
+            self.L.oracle_scene_destroy(self.h)
             self.h = C.c_void_p()
 
     def surface_emissive(self) -> np.ndarray:
         """Per surface material: 1 if it emits (a shape carrying it is a shape light)."""
         out = np.zeros(len(self.desc.scene["materials"]), np.uint8)
-        lib().oracle_surface_emissive(self.h, out.ctypes.data_as(C.POINTER(C.c_uint8)))
+        self.L.oracle_surface_emissive(self.h, out.ctypes.data_as(C.POINTER(C.c_uint8)))
         return out
 
     def set_camera(self, camera: dict) -> None:
@@ -91,14 +106,14 @@ class OracleScene:
         from raymond_b200._abi import make_camera
 
         cam = make_camera(camera)
-        if lib().oracle_scene_set_camera(self.h, C.byref(cam)) != 0:
+        if self.L.oracle_scene_set_camera(self.h, C.byref(cam)) != 0:
             raise RuntimeError("oracle_scene_set_camera failed")
 
     def info(self):
         t = C.c_uint64()
         n = C.c_int32()
         s = C.c_int32()
-        lib().oracle_scene_info(self.h, C.byref(t), C.byref(n), C.byref(s))
+        self.L.oracle_scene_info(self.h, C.byref(t), C.byref(n), C.byref(s))
         return {"triangles": t.value, "lights": n.value, "shape_lights": s.value}
 
     def render(self, width, height, spp, max_depth, sampling_mode=2, rng=0, seed=1, first_sample=0, threads=0,
@@ -114,17 +129,20 @@ class OracleScene:
             st.num_pixels = len(pixels)
         film = np.zeros((height, width, 3), np.float64)
         stats = (C.c_uint64 * 3)()
-        r = lib().oracle_render(self.h, C.byref(st), film.ctypes.data_as(C.POINTER(C.c_double)), stats)
+        r = self.L.oracle_render(self.h, C.byref(st), film.ctypes.data_as(C.POINTER(C.c_double)), stats)
         if r != 0:
             raise RuntimeError(f"oracle_render failed ({r})")
         return film, {"paths": stats[0], "segments": stats[1], "shadow_rays": stats[2]}
 
-    def trace(self, rays: np.ndarray, any_hit=False):
+    def trace(self, rays: np.ndarray, any_hit=False, exhaustive=False):
+        """Closest hits (or occlusion with any_hit); `exhaustive` visits every
+        box the ray enters instead of culling against the best hit so far."""
         rays = _f32(rays)
         n = len(rays)
         out = np.zeros((n, 4), np.float32)
         inst = np.zeros(n, np.uint32)
-        lib().oracle_trace(self.h, rays.ctypes.data_as(C.POINTER(C.c_float)), n, int(any_hit),
+        mode = 1 if any_hit else 2 if exhaustive else 0
+        self.L.oracle_trace(self.h, rays.ctypes.data_as(C.POINTER(C.c_float)), n, mode,
                            out.ctypes.data_as(C.POINTER(C.c_float)), inst.ctypes.data_as(C.POINTER(C.c_uint32)))
         return out, inst
 
@@ -132,7 +150,7 @@ class OracleScene:
         records = _f32(records)
         n = len(records)
         out = np.zeros((n, 16), np.float32)
-        r = lib().oracle_material_eval(self.h, material, records.ctypes.data_as(C.POINTER(C.c_float)), n,
+        r = self.L.oracle_material_eval(self.h, material, records.ctypes.data_as(C.POINTER(C.c_float)), n,
                                        out.ctypes.data_as(C.POINTER(C.c_float)))
         if r != 0:
             raise RuntimeError(f"oracle_material_eval failed ({r})")

@@ -183,9 +183,21 @@ void Bvh::build(std::vector<Tri> tris) {
     for (size_t i = 0; i < n; i++) tris_[i] = tris[prims[i].idx];
 }
 
+// The closest-hit search culls boxes against the best distance found so far.
+// A box's rounded near plane can lie beyond the rounded distance of a
+// triangle on that plane: by a few ulps of the distance, and, for a triangle
+// whose vertices lie far from the ray origin compared with the hit, by a few
+// ulps of those vertex offsets.  A box holding a hit closer than the best one
+// (a face coplanar with another, a box standing on the floor traced from the
+// floor) would then be culled and the result would depend on the visiting
+// order.  The bound is therefore widened by 2e-6 of the distance plus 1e-5
+// of the box's largest offset from the origin, which leaves the closest hit
+// that of an exhaustive search over every box the ray enters.
 static inline bool slab(const float *bmin, const float *bmax, float3 org, float3 inv, float tmin, float tmax,
                         float &tnear) {
-    float t0 = tmin, t1 = tmax;
+    float reach = 0.0f;
+    for (int k = 0; k < 3; k++) reach = std::max(reach, std::max(std::fabs(bmin[k] - org[k]), std::fabs(bmax[k] - org[k])));
+    float t0 = tmin, t1 = tmax * 1.000002f + 1e-5f * reach;
     for (int k = 0; k < 3; k++) {
         float a = (bmin[k] - org[k]) * inv[k];
         float b = (bmax[k] - org[k]) * inv[k];
@@ -199,7 +211,7 @@ static inline bool slab(const float *bmin, const float *bmax, float3 org, float3
     return t0 <= t1;
 }
 
-bool Bvh::intersect(float3 org, float3 dir, float tmin, float tmax, HitRecord &hit) const {
+bool Bvh::intersect(float3 org, float3 dir, float tmin, float tmax, HitRecord &hit, bool exhaustive) const {
     if (nodes_.empty() || tris_.empty()) return false;
     WatertightRay wr(org, dir);
     float3 inv(1.0f / dir.x, 1.0f / dir.y, 1.0f / dir.z);
@@ -211,7 +223,7 @@ bool Bvh::intersect(float3 org, float3 dir, float tmin, float tmax, HitRecord &h
     while (sp) {
         const Node &n = nodes_[stack[--sp]];
         float tn;
-        if (!slab(n.bmin, n.bmax, org, inv, tmin, best, tn)) continue;
+        if (!slab(n.bmin, n.bmax, org, inv, tmin, exhaustive ? INFINITY : best, tn)) continue;
         if (n.count > 0) {
             for (int i = 0; i < n.count; i++) {
                 const Tri &tr = tris_[n.first + i];
@@ -233,8 +245,9 @@ bool Bvh::intersect(float3 org, float3 dir, float tmin, float tmax, HitRecord &h
         } else {
             const Node &l = nodes_[n.first], &r = nodes_[n.first + 1];
             float tl, tr;
-            bool hl = slab(l.bmin, l.bmax, org, inv, tmin, best, tl);
-            bool hr = slab(r.bmin, r.bmax, org, inv, tmin, best, tr);
+            const float bound = exhaustive ? INFINITY : best;
+            bool hl = slab(l.bmin, l.bmax, org, inv, tmin, bound, tl);
+            bool hr = slab(r.bmin, r.bmax, org, inv, tmin, bound, tr);
             if (hl && hr) {
                 if (tl <= tr) {
                     stack[sp++] = n.first + 1;

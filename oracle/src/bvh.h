@@ -29,8 +29,10 @@ public:
         uint32_t instance, prim;
     };
     void build(std::vector<Tri> tris);
-    // closest hit with t in [tmin, tmax]
-    bool intersect(float3 org, float3 dir, float tmin, float tmax, HitRecord &hit) const;
+    // closest hit with t in [tmin, tmax]; `exhaustive` visits every box the
+    // ray enters instead of culling against the best hit so far (a check of
+    // the culling bound)
+    bool intersect(float3 org, float3 dir, float tmin, float tmax, HitRecord &hit, bool exhaustive = false) const;
     // any hit with t in [tmin, tmax]
     bool occluded(float3 org, float3 dir, float tmin, float tmax) const;
     size_t numNodes() const { return nodes_.size(); }

@@ -697,13 +697,13 @@ extern "C" int oracle_trace(const oracle_scene *s, const float *rays, int32_t n,
         const float *r = rays + 8 * (size_t)i;
         float3 o(r[0], r[1], r[2]), d(r[4], r[5], r[6]);
         float *w = out + 4 * (size_t)i;
-        if (any) {
+        if (any == 1) {
             w[0] = s->data.bvh->occluded(o, d, r[3], r[7]) ? 1.0f : -1.0f;
             w[1] = w[2] = w[3] = 0;
             if (instances) instances[i] = 0;
         } else {
             HitRecord h;
-            if (s->data.bvh->intersect(o, d, r[3], r[7], h)) {
+            if (s->data.bvh->intersect(o, d, r[3], r[7], h, any == 2)) {
                 w[0] = h.t;
                 w[1] = h.b0;
                 w[2] = h.b1;

@@ -181,6 +181,7 @@ RMD_HD uint32_t intersectChildren(const WideNode &n, const float3 idir, const fl
 struct TraversalState {
     TraceRay r;
     float tmin, tmax;  // tmax shrinks to the closest hit found so far
+    float slack;       // absolute widening of tmax when boxes are culled against it
     int hitTri;        // closest (any-hit: first) triangle hit, -1 if none
     uint32_t hitInst, hitPrim;  // its instance and primitive (the tie-break key)
     float b0, b1;
@@ -202,6 +203,27 @@ RMD_HD void beginTraversal(TraversalState &s, const WideNode *nodes, float3 o, f
     s.hitTri = -1;
     s.hitInst = s.hitPrim = 0xffffffffu;
     s.b0 = s.b1 = 0.0f;
+    // A box's rounded near plane can lie beyond the rounded distance of a
+    // triangle on that plane: by a few ulps of the distance, and, for a
+    // triangle whose vertices lie far from the origin compared with the hit,
+    // by a few ulps of those offsets.  Boxes are therefore culled against
+    // tmax widened by 2e-6 of it plus 1e-5 of the scene's largest offset from
+    // the origin (the root's quantisation frame), so a box holding a hit
+    // closer than the best so far (a face coplanar with another, a box on the
+    // floor traced from the floor) is never culled, and the closest hit is
+    // that of an exhaustive search, whatever the tree.
+    s.slack = 0.0f;
+    if (nodes != nullptr) {
+        const float4 os = __ldg(&nodes[0].originScale);
+        const uint32_t ew = __float_as_uint(os.w);
+        const float ex = 255.0f * __uint_as_float((ew & 0xffu) << 23);
+        const float ey = 255.0f * __uint_as_float(((ew >> 8) & 0xffu) << 23);
+        const float ez = 255.0f * __uint_as_float(((ew >> 16) & 0xffu) << 23);
+        const float ox = os.x - o.x, oy = os.y - o.y, oz = os.z - o.z;
+        const float reach = fmaxf(fmaxf(fmaxf(fabsf(ox), fabsf(ox + ex)), fmaxf(fabsf(oy), fabsf(oy + ey))),
+                                  fmaxf(fabsf(oz), fabsf(oz + ez)));
+        s.slack = 1e-5f * reach;
+    }
     // a virtual parent whose only inner child, in slot 0, is the root
     s.group = make_uint2(0u, (1u << (24u + rayOctant(s.r.idir))) | 1u);
     s.sp = nodes != nullptr ? 0 : -1;  // a scene without triangles misses everything
@@ -236,7 +258,7 @@ RMD_HD void traverse(TraversalState &s, TraversalStack &stack, const WideNode *_
             const WideNode *np = &nodes[index];
             const WideNode n = {__ldg(&np->originScale), __ldg(&np->bases), __ldg(&np->qloXY),
                                 __ldg(&np->qloZqhiX), __ldg(&np->qhiYZ)};
-            const uint32_t hits = intersectChildren(n, idir, org, octant, s.tmin, s.tmax);
+            const uint32_t hits = intersectChildren(n, idir, org, octant, s.tmin, fmaf(s.tmax, 1.000002f, s.slack));
             group = make_uint2(n.bases.x, (hits & 0xff000000u) | (__float_as_uint(n.originScale.w) >> 24));
             uint32_t triHits = hits & 0x00ffffffu;
             while (triHits) {

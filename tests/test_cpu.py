@@ -141,6 +141,41 @@ def test_oracle_energy_white_furnace():
     assert 1.5 < mean < 2.1, mean
 
 
+@pytest.mark.parametrize("name", ["glossy_room", "glossy_rooms_grid"])
+def test_oracle_bvh_culling_keeps_the_closest_hit(name):
+    """The oracle's BVH culls boxes against the best hit so far with a widened
+    bound; its closest hits equal those of the exhaustive search (every box
+    the ray enters) bit for bit, on random rays and on rays leaving surfaces,
+    in scenes with coplanar shared walls and boxes standing on floors.  (With
+    an unwidened bound 6e-4 of the random and 1e-3 of the secondary rays in
+    the glossy room returned a farther face.)"""
+    d = getattr(scenes, name)(seed=1)
+    orc = O.OracleScene(SceneDesc(d))
+    v = np.concatenate([np.asarray(d["shapes"][e["shape"]]["vertices"], np.float64).reshape(-1, 3)
+                        @ np.asarray(e["matrix"], np.float64)[:3, :3].T + np.asarray(e["matrix"], np.float64)[:3, 3]
+                        for e in d["entities"]])
+    rng = np.random.default_rng(11)
+    n = 100000
+    o = rng.uniform(v.min(0), v.max(0), (n, 3))
+    dirs = rng.normal(size=(n, 3))
+    dirs /= np.linalg.norm(dirs, axis=1, keepdims=True)
+    rays = np.zeros((n, 8), np.float32)
+    rays[:, 0:3], rays[:, 4:7], rays[:, 7] = o, dirs, 1e30
+    h, _ = orc.trace(rays)
+    hit = h[:, 0] > 0
+    second = np.zeros((int(hit.sum()), 8), np.float32)
+    second[:, 0:3] = o[hit] + dirs[hit] * h[hit, 0:1]
+    d2 = rng.normal(size=(len(second), 3))
+    second[:, 4:7] = d2 / np.linalg.norm(d2, axis=1, keepdims=True)
+    second[:, 3], second[:, 7] = 1e-4, 1e30
+    for r in (rays, second):
+        a, ia = orc.trace(r)
+        b, ib = orc.trace(r, exhaustive=True)
+        assert (a[:, 0] > 0).mean() > 0.5
+        np.testing.assert_array_equal(a.view(np.uint32), b.view(np.uint32))
+        np.testing.assert_array_equal(ia, ib)
+
+
 def test_oracle_scenes_are_independent():
     """A scene built after others were destroyed renders exactly as a fresh one
     (the oracle's per-thread node scratch must not outlive its program)."""

@@ -108,16 +108,14 @@ def test_trace_parity(spheres):
     rays = np.concatenate([o, np.full((n, 1), 1e-3), d, np.full((n, 1), 1e30)], 1).astype(np.float32)
     g, gi = scene.trace(rays)
     c, ci = orc.trace(rays)
-    hit_c = c[:, 0] > 0
-    assert np.mean((g[:, 0] > 0) == hit_c) > 0.9999
-    same = (g[:, 3].view(np.uint32) == c[:, 3].view(np.uint32)) & (gi == ci)
-    assert np.mean(same[hit_c]) > 0.9999
-    both = hit_c & same
-    np.testing.assert_allclose(g[both, 0], c[both, 0], rtol=1e-5)
-    np.testing.assert_allclose(g[both, 1:3], c[both, 1:3], atol=1e-5)
+    # both return the closest hit of an exhaustive search with the same
+    # triangle test and tie-break, so every record is identical bit for bit
+    assert (c[:, 0] > 0).mean() > 0.5
+    np.testing.assert_array_equal(g.view(np.uint32), c.view(np.uint32))
+    np.testing.assert_array_equal(gi, ci)
     ga, _ = scene.trace(rays, any_hit=True)
     ca, _ = orc.trace(rays, any_hit=True)
-    assert np.mean(ga[:, 0] == ca[:, 0]) > 0.9999
+    np.testing.assert_array_equal(ga[:, 0], ca[:, 0])
 
 
 def test_material_eval_parity(spheres):
