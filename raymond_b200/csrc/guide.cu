@@ -610,11 +610,15 @@ __device__ bool trCommitWait(TrainSmem &sm, uint32_t &phase) {
 // Epilogue of a forward hidden layer: bias + ReLU of the thread's row of the
 // accumulator, written as the next layer's A row and transposed (hT); returns
 // the ReLU mask (bit c: column c positive).
-__device__ uint64_t trHiddenEpilogue(TrainSmem &sm, uint32_t taddr, const float *bias, uint16_t *rowOut,
-                                     uint16_t *tOut, int row) {
+// The epilogues run three times per tile, and a CTA traces its code once per
+// Adam step: kept out of line and not unrolled over the two column halves, so
+// the second and later calls find their instructions cached (instruction
+// fetch, not the tensor cores, bounds a step).
+__device__ __noinline__ uint64_t trHiddenEpilogue(TrainSmem &sm, uint32_t taddr, const float *bias,
+                                                  uint16_t *rowOut, uint16_t *tOut, int row) {
     uint64_t mask = 0;
     float v[32];
-#pragma unroll
+#pragma unroll 1
     for (int half = 0; half < 2; half++) {
         tmemLd32(taddr + 32u * half, v);
         tmemLdWait();
@@ -644,10 +648,10 @@ __device__ uint64_t trHiddenEpilogue(TrainSmem &sm, uint32_t taddr, const float 
 // Epilogue of a backward layer: the thread's row of delta . W masked by the
 // ReLU mask, as BF16 delta rows (when rowOut) and transposed; bias gradient
 // into db[0..64).
-__device__ void trDeltaEpilogue(TrainSmem &sm, uint32_t taddr, uint64_t mask, uint16_t *rowOut, float *db, int row,
-                                int lane) {
+__device__ __noinline__ void trDeltaEpilogue(TrainSmem &sm, uint32_t taddr, uint64_t mask, uint16_t *rowOut,
+                                             float *db, int row, int lane) {
     float v[32];
-#pragma unroll
+#pragma unroll 1
     for (int half = 0; half < 2; half++) {
         tmemLd32(taddr + 32u * half, v);
         tmemLdWait();

@@ -110,7 +110,7 @@ def test_trace_parity(spheres):
     c, ci = orc.trace(rays)
     # both return the closest hit of an exhaustive search with the same
     # triangle test and tie-break, so every record is identical bit for bit
-    assert (c[:, 0] > 0).mean() > 0.5
+    assert (c[:, 0] > 0).mean() > 0.25
     np.testing.assert_array_equal(g.view(np.uint32), c.view(np.uint32))
     np.testing.assert_array_equal(gi, ci)
     ga, _ = scene.trace(rays, any_hit=True)
