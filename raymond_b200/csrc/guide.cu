@@ -254,20 +254,23 @@ __device__ __forceinline__ void addBias2(float &lo, float &hi, float2 bias) {
 }
 
 // byte offset of element (r, k) in a K-major canonical operand of width K
-__device__ __forceinline__ uint32_t canonOffset(int r, int k, int K) {
+__host__ __device__ __forceinline__ uint32_t canonOffset(int r, int k, int K) {
     return (uint32_t)((r >> 3) * (K / 8) * 128 + (k >> 3) * 128 + (r & 7) * 16 + (k & 7) * 2);
 }
 
-// UMMA shared-memory descriptor: K-major, no swizzle, LBO = 128 B between the
-// two 8-element K chunks of an instruction, SBO between 8-row groups
-__device__ __forceinline__ uint64_t ummaDesc(uint32_t addr, uint32_t sbo) {
+// UMMA shared-memory descriptor, no swizzle: leading and stride byte offsets
+// (K-major: LBO between the 8-element K chunks, SBO between 8-row groups;
+// MN-major: LBO between 8-deep K groups, SBO between 8-element MN chunks)
+__device__ __forceinline__ uint64_t ummaDesc(uint32_t addr, uint32_t lbo, uint32_t sbo) {
     uint64_t d = 0;
     d |= (uint64_t)((addr >> 4) & 0x3fffu);
-    d |= (uint64_t)((128u >> 4) & 0x3fffu) << 16;  // leading byte offset
-    d |= (uint64_t)((sbo >> 4) & 0x3fffu) << 32;   // stride byte offset
-    d |= (uint64_t)1 << 46;                        // descriptor version (sm_100)
-    return d;                                      // base offset 0, layout type 0 (no swizzle)
+    d |= (uint64_t)((lbo >> 4) & 0x3fffu) << 16;  // leading byte offset
+    d |= (uint64_t)((sbo >> 4) & 0x3fffu) << 32;  // stride byte offset
+    d |= (uint64_t)1 << 46;                       // descriptor version (sm_100)
+    return d;                                     // base offset 0, layout type 0 (no swizzle)
 }
+// K-major with the two K chunks of an instruction 128 B apart
+__device__ __forceinline__ uint64_t ummaDesc(uint32_t addr, uint32_t sbo) { return ummaDesc(addr, 128u, sbo); }
 
 // instruction descriptor, kind::f16: BF16 A and B (K-major), FP32 D, M x N
 __device__ __forceinline__ uint32_t ummaInstr(int M, int N) {
@@ -414,8 +417,10 @@ __device__ bool tcLayer(TcSmem &sm, int pipe, const uint16_t *w, int K, int N, u
             umma(tmem, ummaDesc(aBase + kb * 256u, sbo), ummaDesc(bBase + kb * 256u, sbo), idesc, kb > 0);
         ummaCommit(mbar);
     }
+    // on expiry `phase` stays that of the commit in flight, which the
+    // teardown's last bounded wait then waits for
     const bool ok = mbarWait(mbar, phase);
-    phase ^= 1u;
+    if (ok) phase ^= 1u;
     tcFenceAfter();
     if (!ok) atomicExch(&sm.failed[pipe], 1);
     pipeSync(pipe);
@@ -491,44 +496,44 @@ __device__ bool tcForward(TcSmem &sm, int pipe, const GuideFeatures &f, float *o
 // tiles of 128 records, one thread per record (M = 128).  Per tile:
 //
 //   forward   4 layers as in inference (A = the previous layer's rows, B = W);
-//             every thread keeps its record's ReLU masks, and the activations
-//             are also written transposed, [feature][record], for the weight
-//             gradients
+//             every layer's input rows stay in shared memory for the
+//             backward pass, and every thread keeps its record's ReLU masks
 //   loss      each thread the gradient of its record's loss with respect to
-//             the 48 raw outputs (CUDA cores), as rows and transposed
-//   backward  per layer l = 3..0: dW_l += delta_l^T . a_(l-1) (A = delta
-//             transposed, B = the activations transposed, K = the 128
-//             records), accumulated in tensor memory over the CTA's tiles;
-//             and delta_(l-1) = (delta_l . W_l) masked by ReLU' (A = delta
-//             rows, B = W_l transposed), both issued together
+//             the 48 raw outputs (CUDA cores), as delta rows
+//   backward  per layer l = 3..0: dW_l += delta_l^T . a_(l-1), contracting
+//             the 128 records, accumulated in tensor memory over the CTA's
+//             tiles; and delta_(l-1) = (delta_l . W_l) masked by ReLU',
+//             both issued together
 //
-// All operands are in shared memory in the canonical K-major layout.  The
-// weight gradients' M is the layer's output width (64, or 48) padded to 128:
-// rows past the width read whatever follows the delta buffer, and their
-// products land in tensor-memory lanes that are never read.  Tensor memory:
-// columns 0..63 the layer accumulator, then dW0 (160), dW1, dW2, dW3 (64
-// each).  Bias gradients (column sums of the deltas) are reduced across each
-// warp with shuffles into shared memory.  At the end warps 0 and 1 (lanes
-// 0..63, the output features) read the CTA's weight gradient out of tensor
-// memory into the CTA's slot of net.partials.
+// Every operand is a [rows][features] buffer in the canonical no-swizzle
+// layout with K along the features (8 x 16-byte core matrices).  Read
+// K-major it is an operand whose M or N is the rows; read MN-major (UMMA
+// descriptor bits 15/16, leading offset = the 8-row groups, stride offset =
+// the 8-feature chunks) the same bytes are the operand whose K is the rows.
+// So the record-contracted weight gradients read the delta and activation
+// rows as they are (A and B MN-major, K = records), and delta . W_l reads
+// the forward weights as W_l^T (B MN-major): nothing is stored transposed.
+// The weight gradients' M is the layer's output width (64, or 48) padded to
+// 128: the extra rows read the bytes after the delta buffer (the other delta
+// buffer, then the input rows) and land in tensor-memory lanes that are
+// never read.  Tensor memory: columns 0..63 the layer accumulator, then dW0
+// (160), dW1, dW2, dW3 (64 each).  Bias gradients (column sums of the
+// deltas) are reduced across each warp with shuffles into shared memory.  At
+// the end warps 0 and 1 (lanes 0..63, the output features) read the CTA's
+// weight gradient out of tensor memory into the CTA's slot of net.partials.
 constexpr int kTrThreads = 128;
 constexpr uint32_t kTrTmemCols = 512;
 // tensor-memory column of dW_l: dW0 at 64 (160 wide), dW1 224, dW2 288, dW3 352
 __device__ __forceinline__ uint32_t trColDw(int l) { return l == 0 ? 64u : 224u + 64u * (uint32_t)(l - 1); }
 
 struct TrainSmem {
-    uint16_t w0[GUIDE_HIDDEN * GUIDE_INPUTS];  // [out][in], canonical K-major (K = in)
+    uint16_t w0[GUIDE_HIDDEN * GUIDE_INPUTS];  // [out][in], canonical (K = in): the weight image
     uint16_t w1[GUIDE_HIDDEN * GUIDE_HIDDEN];
     uint16_t w2[GUIDE_HIDDEN * GUIDE_HIDDEN];
     uint16_t w3[GUIDE_OUTPUTS * GUIDE_HIDDEN];
-    uint16_t w1t[GUIDE_HIDDEN * GUIDE_HIDDEN];  // [in][out], canonical (K = out)
-    uint16_t w2t[GUIDE_HIDDEN * GUIDE_HIDDEN];
-    uint16_t w3t[GUIDE_HIDDEN * GUIDE_OUTPUTS];
-    uint16_t dT[GUIDE_HIDDEN * kTrThreads];     // delta transposed [out][record]; must precede xT (see above)
-    uint16_t xT[GUIDE_INPUTS * kTrThreads];     // inputs transposed [in][record]
-    uint16_t hT[3][GUIDE_HIDDEN * kTrThreads];  // hidden activations transposed
-    uint16_t rowA[kTrThreads * GUIDE_INPUTS];   // input rows, then layer-2 inputs; deltas in the backward pass
-    uint16_t rowB[kTrThreads * GUIDE_HIDDEN];   // layer-1 inputs, then layer-3 inputs; deltas
+    uint16_t d[2][kTrThreads * GUIDE_HIDDEN];  // delta rows [record][feature], ping-pong (delta_3 is 48 wide)
+    uint16_t x[kTrThreads * GUIDE_INPUTS];     // one-blob input rows; follows the deltas (see above)
+    uint16_t h[3][kTrThreads * GUIDE_HIDDEN];  // hidden activation rows, the inputs of layers 1..3
     float b[3 * GUIDE_HIDDEN + GUIDE_OUTPUTS];
     float db[3 * GUIDE_HIDDEN + GUIDE_OUTPUTS];  // the CTA's bias gradient
     float reduce[8];                             // per warp: loss sums
@@ -537,23 +542,20 @@ struct TrainSmem {
     int failed;
 };
 static_assert(sizeof(TrainSmem) <= 232448, "training shared memory exceeds the per-CTA limit");
-static_assert(offsetof(TrainSmem, xT) == offsetof(TrainSmem, dT) + sizeof(uint16_t) * GUIDE_HIDDEN * kTrThreads,
-              "the padded delta rows of a weight gradient (128 rows from dT) must read inside shared memory");
-
-// copies a row-major [rows][cols] bf16 matrix transposed into the canonical
-// layout of a [cols][rows] operand (K = rows)
-__device__ void loadCanonicalT(uint16_t *dst, const uint16_t *src, int rows, int cols) {
-    unsigned char *d = reinterpret_cast<unsigned char *>(dst);
-    for (int i = threadIdx.x; i < rows * cols; i += blockDim.x) {
-        const int r = i / cols, c = i - r * cols;
-        *reinterpret_cast<uint16_t *>(d + canonOffset(c, r, rows)) = __ldg(&src[i]);
-    }
-}
-
-// element (row, k) of a canonical operand with K = 128 records: row = feature, k = record
-__device__ __forceinline__ uint16_t *tElem(uint16_t *base, int feature, int record) {
-    return reinterpret_cast<uint16_t *>(reinterpret_cast<unsigned char *>(base) + canonOffset(feature, record, kTrThreads));
-}
+static_assert(GUIDE_PARAMS % 4 == 0 && (GUIDE_HIDDEN * GUIDE_INPUTS + GUIDE_HIDDEN) % 4 == 0 &&
+                  (GUIDE_HIDDEN * GUIDE_HIDDEN + GUIDE_HIDDEN) % 4 == 0,
+              "a CTA's gradient slot and its layers start on 16-byte boundaries");
+// the weight image (GuideNetView::image) is TrainSmem's leading weight region
+constexpr uint32_t kImageBytes = (uint32_t)offsetof(TrainSmem, d);
+static_assert(offsetof(TrainSmem, w0) == 0 && kImageBytes % 16 == 0 &&
+                  kImageBytes == sizeof(uint16_t) * GUIDE_WEIGHTS,
+              "the weight image must be the contiguous weight region of the training CTA's shared memory");
+// An MN-major A of M = 128 over a delta buffer of width F reads up to byte
+// 15 * 16F + 2047 from its start (16 record groups of 16F bytes, 16 chunks of
+// 128 bytes): at most 2 KB past the buffer, which must stay inside TrainSmem.
+static_assert(offsetof(TrainSmem, x) == offsetof(TrainSmem, d) + sizeof(uint16_t) * 2 * kTrThreads * GUIDE_HIDDEN &&
+                  sizeof(uint16_t) * kTrThreads * GUIDE_INPUTS >= 2048,
+              "the padded delta rows of a weight gradient must read inside shared memory");
 
 // Sum over the warp's 32 lanes of each of v[0..31]: afterwards lane l holds
 // the sum of column l in v[0] (a butterfly that halves the columns a lane
@@ -578,13 +580,25 @@ __device__ __forceinline__ void addBiasGrad(float *db, int c0, float v[32], int 
     atomicAdd(&db[c0 + lane], sum);
 }
 
-// issues D = A . B^T over K (canonical operands, sbo = K / 8 * 128), committed later
-__device__ __forceinline__ void trMma(uint32_t tmem, const void *a, const void *b, int K, int N, bool accumulate) {
-    const uint32_t idesc = ummaInstr(kTrThreads, N);
-    const uint32_t aBase = smemU32(a), bBase = smemU32(b), sbo = (uint32_t)(K / 8) * 128u;
+// One operand of a training MMA: a [rows][F] canonical buffer read K-major
+// (M or N = the rows, K = the F features) or MN-major (M or N = the F
+// features, K = the rows); kStep: bytes per 16-deep K step.
+struct TrOperand {
+    uint32_t addr, lbo, sbo, kStep, mnMajor;
+};
+__device__ __forceinline__ TrOperand kMajor(const void *rows, int F) {
+    return {smemU32(rows), 128u, (uint32_t)F * 16u, 256u, 0u};
+}
+__device__ __forceinline__ TrOperand mnMajor(const void *rows, int F) {
+    return {smemU32(rows), (uint32_t)F * 16u, 128u, (uint32_t)F * 32u, 1u};
+}
+
+// issues D (tmem) = A . B^T over K, N columns (accumulating if asked); committed later
+__device__ __forceinline__ void trMma(uint32_t tmem, TrOperand a, TrOperand b, int K, int N, bool accumulate) {
+    const uint32_t idesc = ummaInstr(kTrThreads, N) | (a.mnMajor << 15) | (b.mnMajor << 16);
     for (int kb = 0; kb < K / 16; kb++)
-        umma(tmem, ummaDesc(aBase + kb * 256u, sbo), ummaDesc(bBase + kb * 256u, sbo), idesc,
-             (accumulate || kb > 0) ? 1u : 0u);
+        umma(tmem, ummaDesc(a.addr + kb * a.kStep, a.lbo, a.sbo), ummaDesc(b.addr + kb * b.kStep, b.lbo, b.sbo),
+             idesc, (accumulate || kb > 0) ? 1u : 0u);
 }
 
 // makes the threads' shared-memory writes visible to the tensor core and syncs the CTA
@@ -600,7 +614,7 @@ __device__ bool trCommitWait(TrainSmem &sm, uint32_t &phase) {
     const uint32_t mbar = smemU32(&sm.mbar);
     if (threadIdx.x == 0) ummaCommit(mbar);
     const bool ok = mbarWait(mbar, phase);
-    phase ^= 1u;
+    if (ok) phase ^= 1u;  // else the teardown waits for the commit in flight
     tcFenceAfter();
     if (!ok) atomicExch(&sm.failed, 1);
     __syncthreads();
@@ -608,14 +622,13 @@ __device__ bool trCommitWait(TrainSmem &sm, uint32_t &phase) {
 }
 
 // Epilogue of a forward hidden layer: bias + ReLU of the thread's row of the
-// accumulator, written as the next layer's A row and transposed (hT); returns
-// the ReLU mask (bit c: column c positive).
+// accumulator, written as the next layer's A row (kept for the backward
+// pass); returns the ReLU mask (bit c: column c positive).
 // The epilogues run three times per tile, and a CTA traces its code once per
 // Adam step: kept out of line and not unrolled over the two column halves, so
 // the second and later calls find their instructions cached (instruction
 // fetch, not the tensor cores, bounds a step).
-__device__ __noinline__ uint64_t trHiddenEpilogue(TrainSmem &sm, uint32_t taddr, const float *bias,
-                                                  uint16_t *rowOut, uint16_t *tOut, int row) {
+__device__ __noinline__ uint64_t trHiddenEpilogue(uint32_t taddr, const float *bias, uint16_t *rowOut, int row) {
     uint64_t mask = 0;
     float v[32];
 #pragma unroll 1
@@ -634,11 +647,8 @@ __device__ __noinline__ uint64_t trHiddenEpilogue(TrainSmem &sm, uint32_t taddr,
 #pragma unroll
             for (int k = 0; k < 4; k++) {
                 const int col = 32 * half + c + 2 * k;
-                const uint16_t lo = (uint16_t)(q[k] & 0xffffu), hi = (uint16_t)(q[k] >> 16);
-                *tElem(tOut, col, row) = lo;
-                *tElem(tOut, col + 1, row) = hi;
-                mask |= (uint64_t)(lo != 0) << col;
-                mask |= (uint64_t)(hi != 0) << (col + 1);
+                mask |= (uint64_t)((q[k] & 0xffffu) != 0u) << col;
+                mask |= (uint64_t)((q[k] >> 16) != 0u) << (col + 1);
             }
         }
     }
@@ -646,10 +656,9 @@ __device__ __noinline__ uint64_t trHiddenEpilogue(TrainSmem &sm, uint32_t taddr,
 }
 
 // Epilogue of a backward layer: the thread's row of delta . W masked by the
-// ReLU mask, as BF16 delta rows (when rowOut) and transposed; bias gradient
-// into db[0..64).
-__device__ __noinline__ void trDeltaEpilogue(TrainSmem &sm, uint32_t taddr, uint64_t mask, uint16_t *rowOut,
-                                             float *db, int row, int lane) {
+// ReLU mask, as BF16 delta rows; bias gradient into db[0..64).
+__device__ __noinline__ void trDeltaEpilogue(uint32_t taddr, uint64_t mask, uint16_t *rowOut, float *db, int row,
+                                             int lane) {
     float v[32];
 #pragma unroll 1
     for (int half = 0; half < 2; half++) {
@@ -661,11 +670,8 @@ __device__ __noinline__ void trDeltaEpilogue(TrainSmem &sm, uint32_t taddr, uint
             const float a = ((mask >> col) & 1u) ? v[c] : 0.0f;
             const float b = ((mask >> (col + 1)) & 1u) ? v[c + 1] : 0.0f;
             const uint16_t lo = cvtBf16(a), hi = cvtBf16(b);
-            if (rowOut)
-                *reinterpret_cast<uint32_t *>(reinterpret_cast<unsigned char *>(rowOut) +
-                                              canonOffset(row, col, GUIDE_HIDDEN)) = (uint32_t)lo | ((uint32_t)hi << 16);
-            *tElem(sm.dT, col, row) = lo;
-            *tElem(sm.dT, col + 1, row) = hi;
+            *reinterpret_cast<uint32_t *>(reinterpret_cast<unsigned char *>(rowOut) +
+                                          canonOffset(row, col, GUIDE_HIDDEN)) = (uint32_t)lo | ((uint32_t)hi << 16);
             v[c] = fromBf16(lo);  // the bias gradient sums the rounded deltas the MMAs use
             v[c + 1] = fromBf16(hi);
         }
@@ -673,11 +679,13 @@ __device__ __noinline__ void trDeltaEpilogue(TrainSmem &sm, uint32_t taddr, uint
     }
 }
 
-// The sum of the batch's targets (the loss normalises them by their mean),
-// written to *sum by one block: no atomics, so nothing to clear first.
+// The sum of a batch's targets (the loss normalises them by their mean),
+// one block per Adam step of a burst: block b sums the batch drawn with seed
+// batch.seed + b into sums[b].  No atomics, so nothing to clear first.
 constexpr int kSumThreads = 1024;
-__global__ void __launch_bounds__(kSumThreads) k_guide_sum_y(RecordBatch batch, float *sum) {
+__global__ void __launch_bounds__(kSumThreads) k_guide_sum_y(RecordBatch batch, float *sums) {
     __shared__ float part[kSumThreads / 32];
+    batch.seed += blockIdx.x;
     float s = 0.0f;
 #pragma unroll 8
     for (uint32_t i = threadIdx.x; i < batch.n; i += kSumThreads) s += batch.pick(i).y;
@@ -687,7 +695,7 @@ __global__ void __launch_bounds__(kSumThreads) k_guide_sum_y(RecordBatch batch, 
     if (threadIdx.x < 32) {
         s = part[threadIdx.x];
         for (int off = 16; off > 0; off >>= 1) s += __shfl_xor_sync(0xffffffffu, s, off);
-        if (threadIdx.x == 0) *sum = s;
+        if (threadIdx.x == 0) sums[blockIdx.x] = s;
     }
 }
 
@@ -701,23 +709,25 @@ __global__ void __launch_bounds__(kTrThreads, 1) k_guide_train_tc(RecordBatch ba
     extern __shared__ __align__(16) unsigned char smem[];
     TrainSmem &sm = *reinterpret_cast<TrainSmem *>(smem);
     const int row = threadIdx.x, warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-    // set-up: weights (forward and transposed), biases, mbarrier, tensor memory
-    loadCanonical(sm.w0, net.w[0], GUIDE_HIDDEN, GUIDE_INPUTS);
-    loadCanonical(sm.w1, net.w[1], GUIDE_HIDDEN, GUIDE_HIDDEN);
-    loadCanonical(sm.w2, net.w[2], GUIDE_HIDDEN, GUIDE_HIDDEN);
-    loadCanonical(sm.w3, net.w[3], GUIDE_OUTPUTS, GUIDE_HIDDEN);
-    loadCanonicalT(sm.w1t, net.w[1], GUIDE_HIDDEN, GUIDE_HIDDEN);
-    loadCanonicalT(sm.w2t, net.w[2], GUIDE_HIDDEN, GUIDE_HIDDEN);
-    loadCanonicalT(sm.w3t, net.w[3], GUIDE_OUTPUTS, GUIDE_HIDDEN);
+    // set-up: the weights (forward and transposed, already in their shared-
+    // memory layout) arrive by one bulk copy on the mbarrier's phase 0 while
+    // the biases load, the tensor memory is allocated and the inputs encode
+    if (threadIdx.x == 0) {
+        sm.failed = 0;
+        const uint32_t mbar = smemU32(&sm.mbar);
+        asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;\n" ::"r"(mbar), "r"(1) : "memory");
+        asm volatile("fence.mbarrier_init.release.cluster;\n" ::: "memory");
+        asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;\n" ::"r"(mbar), "r"(kImageBytes)
+                     : "memory");
+        asm volatile("cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];\n" ::"r"(
+                         smemU32(sm.w0)),
+                     "l"(net.image), "r"(kImageBytes), "r"(mbar)
+                     : "memory");
+    }
     for (int i = threadIdx.x; i < 3 * GUIDE_HIDDEN + GUIDE_OUTPUTS; i += blockDim.x) {
         const int l = min(i / GUIDE_HIDDEN, 3);
         sm.b[i] = __ldg(&net.b[l][i - l * GUIDE_HIDDEN]);
         sm.db[i] = 0.0f;
-    }
-    if (threadIdx.x == 0) {
-        sm.failed = 0;
-        asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;\n" ::"r"(smemU32(&sm.mbar)), "r"(1) : "memory");
-        asm volatile("fence.mbarrier_init.release.cluster;\n" ::: "memory");
     }
     if (warp == 0) {
         asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;\n" ::"r"(smemU32(&sm.tmemBase)),
@@ -735,19 +745,23 @@ __global__ void __launch_bounds__(kTrThreads, 1) k_guide_train_tc(RecordBatch ba
     float lossSum = 0.0f;
     uint32_t phase = 0;
     bool first = true, ok = true;
+    {  // the weight image (phase 0); the MMA commits follow on phase 1, 0, ...
+        const bool arrived = mbarWait(smemU32(&sm.mbar), phase);
+        if (arrived) phase ^= 1u;  // else the teardown waits for the copy in flight
+        else atomicExch(&sm.failed, 1);
+        __syncthreads();
+        ok = sm.failed == 0;
+    }
     for (uint32_t tile = blockIdx.x; tile < tiles && ok; tile += gridDim.x) {
         const uint32_t r = tile * kTrThreads + row;
         GuideRecord rc = {};
         const bool valid = r < n;
         if (valid) rc = batch.pick(r);
-        // inputs: one-blob rows (two non-zero bins per feature) and their transpose
-        unsigned char *aRow = reinterpret_cast<unsigned char *>(sm.rowA);
+        // inputs: one-blob rows (two non-zero bins per feature)
+        unsigned char *xRow = reinterpret_cast<unsigned char *>(sm.x);
 #pragma unroll
         for (int c = 0; c < GUIDE_INPUTS / 8; c++)
-            *reinterpret_cast<uint4 *>(aRow + canonOffset(row, 8 * c, GUIDE_INPUTS)) = make_uint4(0u, 0u, 0u, 0u);
-        for (int i = threadIdx.x; i < GUIDE_INPUTS * kTrThreads / 8; i += blockDim.x)
-            reinterpret_cast<uint4 *>(sm.xT)[i] = make_uint4(0u, 0u, 0u, 0u);
-        __syncthreads();
+            *reinterpret_cast<uint4 *>(xRow + canonOffset(row, 8 * c, GUIDE_INPUTS)) = make_uint4(0u, 0u, 0u, 0u);
         if (valid) {
 #pragma unroll
             for (int feature = 0; feature < 7; feature++) {
@@ -758,29 +772,31 @@ __global__ void __launch_bounds__(kTrThreads, 1) k_guide_train_tc(RecordBatch ba
 #pragma unroll
                 for (int k = 0; k < 2; k++) {
                     const int bin = b + k;
-                    if (bin >= 0 && bin < bins) {
-                        const uint16_t x = cvtBf16(oneBlob(v, bins, bin));
-                        *reinterpret_cast<uint16_t *>(aRow + canonOffset(row, firstCol + bin, GUIDE_INPUTS)) = x;
-                        *tElem(sm.xT, firstCol + bin, row) = x;
-                    }
+                    if (bin >= 0 && bin < bins)
+                        *reinterpret_cast<uint16_t *>(xRow + canonOffset(row, firstCol + bin, GUIDE_INPUTS)) =
+                            cvtBf16(oneBlob(v, bins, bin));
                 }
             }
         }
-        // forward
+        // forward: every layer's input rows stay for the backward pass
         trPublish();
-        if (threadIdx.x == 0) trMma(tmem, sm.rowA, sm.w0, GUIDE_INPUTS, GUIDE_HIDDEN, false);
+        if (threadIdx.x == 0)
+            trMma(tmem, kMajor(sm.x, GUIDE_INPUTS), kMajor(sm.w0, GUIDE_INPUTS), GUIDE_INPUTS, GUIDE_HIDDEN, false);
         if (!(ok = trCommitWait(sm, phase))) break;
-        const uint64_t m0 = trHiddenEpilogue(sm, taddr, sm.b, sm.rowB, sm.hT[0], row);
+        const uint64_t m0 = trHiddenEpilogue(taddr, sm.b, sm.h[0], row);
         trPublish();
-        if (threadIdx.x == 0) trMma(tmem, sm.rowB, sm.w1, GUIDE_HIDDEN, GUIDE_HIDDEN, false);
+        if (threadIdx.x == 0)
+            trMma(tmem, kMajor(sm.h[0], GUIDE_HIDDEN), kMajor(sm.w1, GUIDE_HIDDEN), GUIDE_HIDDEN, GUIDE_HIDDEN, false);
         if (!(ok = trCommitWait(sm, phase))) break;
-        const uint64_t m1 = trHiddenEpilogue(sm, taddr, sm.b + GUIDE_HIDDEN, sm.rowA, sm.hT[1], row);
+        const uint64_t m1 = trHiddenEpilogue(taddr, sm.b + GUIDE_HIDDEN, sm.h[1], row);
         trPublish();
-        if (threadIdx.x == 0) trMma(tmem, sm.rowA, sm.w2, GUIDE_HIDDEN, GUIDE_HIDDEN, false);
+        if (threadIdx.x == 0)
+            trMma(tmem, kMajor(sm.h[1], GUIDE_HIDDEN), kMajor(sm.w2, GUIDE_HIDDEN), GUIDE_HIDDEN, GUIDE_HIDDEN, false);
         if (!(ok = trCommitWait(sm, phase))) break;
-        const uint64_t m2 = trHiddenEpilogue(sm, taddr, sm.b + 2 * GUIDE_HIDDEN, sm.rowB, sm.hT[2], row);
+        const uint64_t m2 = trHiddenEpilogue(taddr, sm.b + 2 * GUIDE_HIDDEN, sm.h[2], row);
         trPublish();
-        if (threadIdx.x == 0) trMma(tmem, sm.rowB, sm.w3, GUIDE_HIDDEN, GUIDE_OUTPUTS, false);
+        if (threadIdx.x == 0)
+            trMma(tmem, kMajor(sm.h[2], GUIDE_HIDDEN), kMajor(sm.w3, GUIDE_HIDDEN), GUIDE_HIDDEN, GUIDE_OUTPUTS, false);
         if (!(ok = trCommitWait(sm, phase))) break;
         float o[GUIDE_OUTPUTS];
         tmemLd32(taddr, o);
@@ -798,8 +814,8 @@ __global__ void __launch_bounds__(kTrThreads, 1) k_guide_train_tc(RecordBatch ba
 #pragma unroll
             for (int c = 0; c < GUIDE_OUTPUTS; c++) d3[c] = 0;
         }
-        {
-            unsigned char *dRow = reinterpret_cast<unsigned char *>(sm.rowA);
+        {  // delta_3 rows (48 wide) into d[0], and its bias gradient
+            unsigned char *dRow = reinterpret_cast<unsigned char *>(sm.d[0]);
 #pragma unroll
             for (int c = 0; c < GUIDE_OUTPUTS; c += 8)
                 *reinterpret_cast<uint4 *>(dRow + canonOffset(row, c, GUIDE_OUTPUTS)) =
@@ -807,45 +823,47 @@ __global__ void __launch_bounds__(kTrThreads, 1) k_guide_train_tc(RecordBatch ba
                                pack2(d3[c + 6], d3[c + 7]));
             float v[32];
 #pragma unroll
-            for (int c = 0; c < 32; c++) {
-                *tElem(sm.dT, c, row) = d3[c];
-                v[c] = fromBf16(d3[c]);
-            }
+            for (int c = 0; c < 32; c++) v[c] = fromBf16(d3[c]);
             addBiasGrad(sm.db + 3 * GUIDE_HIDDEN, 0, v, lane);
 #pragma unroll
-            for (int c = 0; c < 32; c++) v[c] = 0.0f;
-#pragma unroll
-            for (int c = 32; c < GUIDE_OUTPUTS; c++) {
-                *tElem(sm.dT, c, row) = d3[c];
-                v[c - 32] = fromBf16(d3[c]);
-            }
+            for (int c = 0; c < 32; c++) v[c] = c < GUIDE_OUTPUTS - 32 ? fromBf16(d3[32 + c]) : 0.0f;
             const float sum = warpColumnSums(v, lane);
             if (lane < GUIDE_OUTPUTS - 32) atomicAdd(&sm.db[3 * GUIDE_HIDDEN + 32 + lane], sum);
         }
-        // backward: layer 3 (dW3, delta2), 2 (dW2, delta1), 1 (dW1, delta0), 0 (dW0)
+        // backward: layer 3 (dW3, delta2), 2 (dW2, delta1), 1 (dW1, delta0), 0 (dW0); the weight
+        // gradients read delta and activation rows MN-major (K = the records), delta . W_l reads
+        // the forward W_l MN-major (as W_l^T)
         trPublish();
         if (threadIdx.x == 0) {
-            trMma(tmem + trColDw(3), sm.dT, sm.hT[2], kTrThreads, GUIDE_HIDDEN, !first);
-            trMma(tmem, sm.rowA, sm.w3t, GUIDE_OUTPUTS, GUIDE_HIDDEN, false);
+            trMma(tmem + trColDw(3), mnMajor(sm.d[0], GUIDE_OUTPUTS), mnMajor(sm.h[2], GUIDE_HIDDEN), kTrThreads,
+                  GUIDE_HIDDEN, !first);
+            trMma(tmem, kMajor(sm.d[0], GUIDE_OUTPUTS), mnMajor(sm.w3, GUIDE_HIDDEN), GUIDE_OUTPUTS, GUIDE_HIDDEN,
+                  false);
         }
         if (!(ok = trCommitWait(sm, phase))) break;
-        trDeltaEpilogue(sm, taddr, m2, sm.rowB, sm.db + 2 * GUIDE_HIDDEN, row, lane);
+        trDeltaEpilogue(taddr, m2, sm.d[1], sm.db + 2 * GUIDE_HIDDEN, row, lane);
         trPublish();
         if (threadIdx.x == 0) {
-            trMma(tmem + trColDw(2), sm.dT, sm.hT[1], kTrThreads, GUIDE_HIDDEN, !first);
-            trMma(tmem, sm.rowB, sm.w2t, GUIDE_HIDDEN, GUIDE_HIDDEN, false);
+            trMma(tmem + trColDw(2), mnMajor(sm.d[1], GUIDE_HIDDEN), mnMajor(sm.h[1], GUIDE_HIDDEN), kTrThreads,
+                  GUIDE_HIDDEN, !first);
+            trMma(tmem, kMajor(sm.d[1], GUIDE_HIDDEN), mnMajor(sm.w2, GUIDE_HIDDEN), GUIDE_HIDDEN, GUIDE_HIDDEN,
+                  false);
         }
         if (!(ok = trCommitWait(sm, phase))) break;
-        trDeltaEpilogue(sm, taddr, m1, sm.rowA, sm.db + GUIDE_HIDDEN, row, lane);
+        trDeltaEpilogue(taddr, m1, sm.d[0], sm.db + GUIDE_HIDDEN, row, lane);
         trPublish();
         if (threadIdx.x == 0) {
-            trMma(tmem + trColDw(1), sm.dT, sm.hT[0], kTrThreads, GUIDE_HIDDEN, !first);
-            trMma(tmem, sm.rowA, sm.w1t, GUIDE_HIDDEN, GUIDE_HIDDEN, false);
+            trMma(tmem + trColDw(1), mnMajor(sm.d[0], GUIDE_HIDDEN), mnMajor(sm.h[0], GUIDE_HIDDEN), kTrThreads,
+                  GUIDE_HIDDEN, !first);
+            trMma(tmem, kMajor(sm.d[0], GUIDE_HIDDEN), mnMajor(sm.w1, GUIDE_HIDDEN), GUIDE_HIDDEN, GUIDE_HIDDEN,
+                  false);
         }
         if (!(ok = trCommitWait(sm, phase))) break;
-        trDeltaEpilogue(sm, taddr, m0, nullptr, sm.db, row, lane);
+        trDeltaEpilogue(taddr, m0, sm.d[1], sm.db, row, lane);
         trPublish();
-        if (threadIdx.x == 0) trMma(tmem + trColDw(0), sm.dT, sm.xT, kTrThreads, GUIDE_INPUTS, !first);
+        if (threadIdx.x == 0)
+            trMma(tmem + trColDw(0), mnMajor(sm.d[1], GUIDE_HIDDEN), mnMajor(sm.x, GUIDE_INPUTS), kTrThreads,
+                  GUIDE_INPUTS, !first);
         if (!(ok = trCommitWait(sm, phase))) break;
         first = false;
     }
@@ -869,9 +887,12 @@ __global__ void __launch_bounds__(kTrThreads, 1) k_guide_train_tc(RecordBatch ba
 #pragma unroll
                     for (int c = 0; c < 32; c++) v[c] = 0.0f;
                 }
-                if (o < outs[l])
+                if (o < outs[l]) {
+                    // 16-byte stores: every layer offset, row width and column block is a multiple of 4 floats
+                    float4 *dst = reinterpret_cast<float4 *>(part + net.wOffset[l] + o * width[l] + c0);
 #pragma unroll
-                    for (int c = 0; c < 32; c++) part[net.wOffset[l] + o * width[l] + c0 + c] = v[c];
+                    for (int c = 0; c < 32; c += 4) dst[c / 4] = make_float4(v[c], v[c + 1], v[c + 2], v[c + 3]);
+                }
             }
         }
     }
@@ -977,6 +998,14 @@ __global__ void k_guide_reduce(GuideNetView net, int blocks, float *lossOut) {
     net.grad[i] += g;
 }
 
+// Parameter i's BF16 copies: row-major and in the weight image (a bias has none).
+__device__ __forceinline__ void storeBf16Weight(const GuideNetView &net, int i, float w) {
+    if (net.bf16Index[i] < 0) return;
+    const uint16_t q = (uint16_t)bf16Bits(w);
+    net.weightsBf16[net.bf16Index[i]] = q;
+    net.image[net.imageIndex[i]] = q;
+}
+
 // Adam step on every parameter; refreshes the bf16 weight copies and clears
 // the gradient.
 __global__ void k_guide_adam(GuideNetView net, int blocks, float lr, float beta1, float beta2, float eps, float corr1,
@@ -993,7 +1022,7 @@ __global__ void k_guide_adam(GuideNetView net, int blocks, float lr, float beta1
     const float w = net.master[i] - lr * (m * corr1) / (sqrtf(v * corr2) + eps);
     net.master[i] = w;
     net.grad[i] = 0.0f;
-    if (net.bf16Index[i] >= 0) net.weightsBf16[net.bf16Index[i]] = (uint16_t)bf16Bits(w);
+    storeBf16Weight(net, i, w);
 }
 
 // Test hook: forward pass of explicit feature vectors through the inference
@@ -1029,7 +1058,7 @@ __global__ void k_guide_refresh(GuideNetView net) {
     net.adamM[i] = 0.0f;
     net.adamV[i] = 0.0f;
     net.grad[i] = 0.0f;
-    if (net.bf16Index[i] >= 0) net.weightsBf16[net.bf16Index[i]] = (uint16_t)bf16Bits(net.master[i]);
+    storeBf16Weight(net, i, net.master[i]);
 }
 
 // Test hook: the packed mixture of one output vector, n samples with their
@@ -1078,21 +1107,33 @@ cudaError_t rmdLaunchGuideInfer(const Context &ctx, const PathPool &pool, Counte
     return cudaGetLastError();
 }
 
-cudaError_t rmdLaunchGuideTrain(const GuideRecord *rec, uint32_t total, uint32_t n, uint32_t seed,
+cudaError_t rmdLaunchGuideTrain(const GuideRecord *rec, uint32_t total, uint32_t n, uint32_t seed, uint32_t steps,
                                 const GuideNetView &net, float *scratch, int blocks, float lr, int step,
                                 uint32_t *errors, cudaStream_t s) {
-    // scratch[0]: the batch's target sum, scratch[1]: the step's mean loss (written by the Adam step)
+    // scratch[1]: the last step's mean loss (written by the Adam step);
+    // scratch[kSumSlots .. 2 kSumSlots): the target sums of up to kSumSlots steps
+    constexpr uint32_t kSumSlots = 32;
     if (total == 0) return cudaSuccess;
     RecordBatch batch{rec, total, std::min(n, total), seed};
-    k_guide_sum_y<<<1, kSumThreads, 0, s>>>(batch, scratch);
-    cudaError_t e = cudaGetLastError();
-    if (e != cudaSuccess) return e;
     // one CTA per tile of 128 records, at most `blocks` (each CTA then takes several tiles)
     const int tiles = (int)((batch.n + kTrThreads - 1) / kTrThreads);
     blocks = std::max(1, std::min(std::min(blocks, tiles), GUIDE_TRAIN_MAX_BLOCKS));
-    k_guide_train_tc<<<blocks, kTrThreads, rmdGuideSharedBytes(true), s>>>(batch, scratch, net, errors);
-    if ((e = cudaGetLastError()) != cudaSuccess) return e;
-    return rmdLaunchGuideAdam(net, blocks, lr, step, scratch + 1, s);
+    cudaError_t e = cudaSuccess;
+    for (uint32_t k = 0; k < steps; k++) {
+        float *sums = scratch + kSumSlots;
+        if (k % kSumSlots == 0) {  // the batches of the next kSumSlots steps (the ring does not change meanwhile)
+            RecordBatch first = batch;
+            first.seed = seed + k;
+            k_guide_sum_y<<<std::min(kSumSlots, steps - k), kSumThreads, 0, s>>>(first, sums);
+            if ((e = cudaGetLastError()) != cudaSuccess) return e;
+        }
+        batch.seed = seed + k;
+        k_guide_train_tc<<<blocks, kTrThreads, rmdGuideSharedBytes(true), s>>>(batch, sums + k % kSumSlots, net,
+                                                                               errors);
+        if ((e = cudaGetLastError()) != cudaSuccess) return e;
+        if ((e = rmdLaunchGuideAdam(net, blocks, lr, step + (int)k, scratch + 1, s)) != cudaSuccess) return e;
+    }
+    return e;
 }
 
 cudaError_t rmdLaunchGuideAdam(const GuideNetView &net, int blocks, float lr, int step, float *lossOut,
@@ -1148,11 +1189,13 @@ void GuideNet::layout(int wOffset[4], int bOffset[4], int bf16Offset[4]) {
 
 void GuideNet::release() {
     for (void *ptr : {(void *)master, (void *)adamM, (void *)adamV, (void *)grad, (void *)scratch,
-                      (void *)partials, (void *)weightsBf16, (void *)bf16Index})
+                      (void *)partials, (void *)weightsBf16, (void *)bf16Index, (void *)image, (void *)imageIndex})
         if (ptr) cudaFree(ptr);
     master = adamM = adamV = grad = scratch = partials = nullptr;
     weightsBf16 = nullptr;
     bf16Index = nullptr;
+    image = nullptr;
+    imageIndex = nullptr;
 }
 
 cudaError_t GuideNet::allocate() {
@@ -1164,14 +1207,26 @@ cudaError_t GuideNet::allocate() {
         (e = cudaMalloc(&scratch, 64 * sizeof(float))) != cudaSuccess ||
         (e = cudaMalloc(&partials, (size_t)GUIDE_TRAIN_MAX_BLOCKS * (pb + sizeof(float)))) != cudaSuccess ||
         (e = cudaMalloc(&weightsBf16, GUIDE_WEIGHTS * sizeof(uint16_t))) != cudaSuccess ||
-        (e = cudaMalloc(&bf16Index, GUIDE_PARAMS * sizeof(int))) != cudaSuccess)
+        (e = cudaMalloc(&bf16Index, GUIDE_PARAMS * sizeof(int))) != cudaSuccess ||
+        (e = cudaMalloc(&image, kImageBytes)) != cudaSuccess ||
+        (e = cudaMalloc(&imageIndex, GUIDE_PARAMS * sizeof(int))) != cudaSuccess)
         return e;
-    std::vector<int> idx(GUIDE_PARAMS, -1);
+    std::vector<int> idx(GUIDE_PARAMS, -1), img(GUIDE_PARAMS, -1);
     int wOff[4], bOff[4], qOff[4];
     layout(wOff, bOff, qOff);
+    const int in[4] = {GUIDE_INPUTS, GUIDE_HIDDEN, GUIDE_HIDDEN, GUIDE_HIDDEN};
+    const int out[4] = {GUIDE_HIDDEN, GUIDE_HIDDEN, GUIDE_HIDDEN, GUIDE_OUTPUTS};
+    const size_t fwd[4] = {offsetof(TrainSmem, w0), offsetof(TrainSmem, w1), offsetof(TrainSmem, w2),
+                           offsetof(TrainSmem, w3)};
     for (int l = 0; l < 4; l++)
-        for (int k = 0; k < bOff[l] - wOff[l]; k++) idx[wOff[l] + k] = qOff[l] + k;
-    if ((e = cudaMemcpy(bf16Index, idx.data(), idx.size() * sizeof(int), cudaMemcpyHostToDevice)) != cudaSuccess)
+        for (int o = 0; o < out[l]; o++)
+            for (int k = 0; k < in[l]; k++) {
+                const int p = wOff[l] + o * in[l] + k;
+                idx[p] = qOff[l] + o * in[l] + k;
+                img[p] = (int)((fwd[l] + canonOffset(o, k, in[l])) / sizeof(uint16_t));  // row o, K = inputs
+            }
+    if ((e = cudaMemcpy(bf16Index, idx.data(), idx.size() * sizeof(int), cudaMemcpyHostToDevice)) != cudaSuccess ||
+        (e = cudaMemcpy(imageIndex, img.data(), img.size() * sizeof(int), cudaMemcpyHostToDevice)) != cudaSuccess)
         return e;
     return rmdGuideConfigure();
 }
@@ -1206,6 +1261,8 @@ GuideNetView GuideNet::view(float3 sceneMin, float3 sceneInvExtent) const {
     v.partials = partials;
     v.weightsBf16 = weightsBf16;
     v.bf16Index = bf16Index;
+    v.image = image;
+    v.imageIndex = imageIndex;
     v.sceneMin = sceneMin;
     v.sceneInvExtent = sceneInvExtent;
     return v;

@@ -27,6 +27,11 @@ struct GuideNetView {
     float *partials;                        // per training block: its gradient, then its loss (GUIDE_PARTIAL_LOSS)
     uint16_t *weightsBf16;                  // GUIDE_WEIGHTS
     const int *bf16Index;                   // per parameter: index into weightsBf16, or -1 (bias)
+    // the BF16 weights in the training kernel's shared-memory layout (every
+    // layer canonical, K = its inputs), copied into each training CTA with
+    // one bulk copy; imageIndex: per parameter, its element (-1: a bias)
+    uint16_t *image;
+    const int *imageIndex;
     int wOffset[4], bOffset[4];             // parameter offsets of each layer's weights / biases
     float3 sceneMin, sceneInvExtent;        // position encoding frame
 };
@@ -39,12 +44,12 @@ cudaError_t rmdGuideConfigure();
 cudaError_t rmdLaunchGuideInfer(const rmd::Context &ctx, const rmd::PathPool &pool, rmd::Counters *cnt, uint32_t cur,
                                 uint32_t guideDepth, const rmd::GuideNetView &net, rmd::GuideMixture *out, int blocks,
                                 cudaStream_t s);
-// One Adam step (`step` counts from 1) on the mean loss over a batch of n
-// records drawn from the `total` stored ones (all of them when n >= total;
-// `seed` varies the draw)
+// `steps` Adam steps (the first is `step`, counting from 1), each on the mean
+// loss over a batch of n records drawn from the `total` stored ones (all of
+// them when n >= total; step k draws with seed `seed` + k)
 // (tensor cores: one CTA per 128 records, at most `blocks`); an expired
 // tensor-core wait sets ERR_GUIDE_TIMEOUT in *errors
-cudaError_t rmdLaunchGuideTrain(const rmd::GuideRecord *rec, uint32_t total, uint32_t n, uint32_t seed,
+cudaError_t rmdLaunchGuideTrain(const rmd::GuideRecord *rec, uint32_t total, uint32_t n, uint32_t seed, uint32_t steps,
                                 const rmd::GuideNetView &net, float *scratch, int blocks, float lr, int step,
                                 uint32_t *errors, cudaStream_t s);
 // Adam (beta 0.9 / 0.999, eps 1e-8, `step` from 1) on net.grad plus the first
@@ -68,6 +73,8 @@ struct GuideNet {
     float *partials = nullptr;
     uint16_t *weightsBf16 = nullptr;
     int *bf16Index = nullptr;
+    uint16_t *image = nullptr;
+    int *imageIndex = nullptr;
     int steps = 0;
     GuideNet() = default;
     GuideNet(const GuideNet &) = delete;

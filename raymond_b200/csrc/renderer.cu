@@ -944,13 +944,13 @@ static rmd_status guideTrainStep(GuideState &guide, const Counters &h, Counters 
     if (!guide.settings.training || h.numSamples < guide.settings.batch_size) return RMD_OK;
     const uint32_t stored = std::min(h.numRecords, guide.recordCapacity);
     const uint32_t steps = h.numSamples / guide.settings.batch_size * guide.settings.steps_per_batch;
-    for (uint32_t k = 0; k < steps && stored > 0; k++) {
+    if (steps > 0 && stored > 0) {
         RMD_CUDA(rmdLaunchGuideTrain(guide.records.as<GuideRecord>(), stored, guide.settings.step_records,
-                                     (uint32_t)guide.net.steps + 1u, net, guide.net.scratch, trainBlocks,
+                                     (uint32_t)guide.net.steps + 1u, steps, net, guide.net.scratch, trainBlocks,
                                      guide.settings.learning_rate, guide.net.steps + 1, &cnt->errors, st));
-        guide.net.steps++;
-        trainSteps++;
-        guide.stats.steps++;
+        guide.net.steps += (int)steps;
+        trainSteps += steps;
+        guide.stats.steps += steps;
     }
     RMD_CUDA(cudaMemsetAsync(&cnt->numSamples, 0, sizeof(uint32_t), st));
     guide.stats.samples += h.numSamples;
