@@ -352,6 +352,7 @@ def run_config5(args) -> dict:
         "metric": "time to the plain tracer's 1024-spp relMSE, guided batch (config 5)",
         "clocks": clocks,
         "value": parity[1] / plain_ms if parity else None, "unit": "fraction of the plain batch's time",
+        "value_interpolated": (crossing_ms(curve, target) / plain_ms) if parity else None,
         "higher_is_better": False, "n_gpus": 1,
         "config": {"workload": f"glossy_rooms_grid_4x4_8views_{W}x{H}_depth{depth}",
                    "triangles": desc_triangles(desc), "views": 8, "oracle_spp": args.oracle_spp,
@@ -367,6 +368,21 @@ def run_config5(args) -> dict:
 
 def desc_triangles(desc) -> int:
     return int(sum(len(s["indices"]) for s in desc.scene["shapes"]))
+
+
+def crossing_ms(curve, target: float):
+    """Time at which a relMSE curve [(spp, ms, relmse)] first reaches `target`,
+    interpolated in log relMSE between the 32-spp chunks around the crossing
+    (the chunk boundary itself quantises the time by up to a chunk)."""
+    prev = None
+    for s_, t_, e_ in curve:
+        if e_ <= target:
+            if prev is None or not (prev[2] > e_ > 0):
+                return t_
+            t0, e0 = prev[1], prev[2]
+            return t0 + (t_ - t0) * (np.log(e0) - np.log(target)) / (np.log(e0) - np.log(e_))
+        prev = (s_, t_, e_)
+    return None
 
 
 def guided_leg(api, ctx, oracle_spp: int, size=(GUIDED_W, GUIDED_H), guide: dict | None = None,
@@ -439,6 +455,7 @@ def guided_leg(api, ctx, oracle_spp: int, size=(GUIDED_W, GUIDED_H), guide: dict
         "guided": {"relmse_at_equal_time": e_eq, "ms_to_plain_relmse": parity[1] if parity else None,
                    "spp_to_plain_relmse": parity[0] if parity else None,
                    "time_ratio": parity[1] / plain_ms if parity else None, "target_time_ratio": 1.0 / 3.0,
+                   "time_ratio_interpolated": (crossing_ms(curve, e_plain) / plain_ms) if parity else None,
                    "ms_guide": guide_ms, "ms_guide_train": train_ms, "adam_steps": stats["steps"],
                    "records": stats["records"], "settings": settings,
                    "curve": [{"spp": s_, "ms": round(t_, 2), "relmse": e_} for s_, t_, e_ in curve[::4]]},

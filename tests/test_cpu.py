@@ -192,3 +192,20 @@ def test_oracle_scenes_are_independent():
         gc.collect()
         again, _ = O.OracleScene(desc).render(32, 32, 1, 4, sampling_mode=1)
         assert np.array_equal(again, ref), seed
+
+
+def test_bench_parity_time_interpolation():
+    """bench.py's guided legs report the time a relMSE curve reaches the plain
+    tracer's error: the first chunk at or below it, and the crossing
+    interpolated in log relMSE between that chunk and the one before."""
+    import importlib.util
+
+    spec = importlib.util.spec_from_file_location("bench_mod", ROOT / "bench.py")
+    b = importlib.util.module_from_spec(spec)
+    spec.loader.exec_module(b)
+    curve = [(32, 100.0, 0.01), (64, 200.0, 0.005), (96, 300.0, 0.0033)]
+    t = b.crossing_ms(curve, 0.004)
+    assert 200.0 < t < 300.0
+    assert abs(t - (200.0 + 100.0 * np.log(0.005 / 0.004) / np.log(0.005 / 0.0033))) < 1e-9
+    assert b.crossing_ms(curve, 0.02) == 100.0  # reached by the first chunk
+    assert b.crossing_ms(curve, 0.001) is None  # never reached
