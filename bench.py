@@ -80,7 +80,9 @@ BYTES_FILM_PER_PATH = 16 + 32 + 80
 TRAFFIC_PER_UNIT = {"trace": 78.5}
 GUIDED_W, GUIDED_H, GUIDED_DEPTH, GUIDED_ORACLE_SPP, GUIDED_PLAIN_SPP, GUIDED_CHUNK = 1280, 720, 16, 65536, 1024, 32
 # guide settings of the guided legs (configs 4 and 5): Adam steps per 2^20 tracer samples, records per step
-GUIDE_DEFAULTS = {"batch_size": 1 << 20, "learning_rate": 1e-3, "steps_per_batch": 8, "step_records": 1 << 13}
+# the guided legs' training settings; the learning rate is three times the
+# library's default (a sweep on the config-4 room measured it best)
+GUIDE_DEFAULTS = {"batch_size": 1 << 20, "learning_rate": 3e-3, "steps_per_batch": 8, "step_records": 1 << 13}
 CPU_BASELINE_SPP = 16  # CPU sample: 16 one-spp frames of the full image (about 10-20 s on 16 cores)
 
 
