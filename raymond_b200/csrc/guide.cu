@@ -974,7 +974,27 @@ __global__ void __launch_bounds__(kTcThreads) k_guide_infer(Counters *cnt, const
             if (row == 0) atomicOr(&cnt->errors, ERR_GUIDE_TIMEOUT);
             break;
         }
-        if (valid) out[q] = pack(decode(o));
+        // The tile's 128 mixtures are one contiguous block of `out`: staged in
+        // the pipeline's A buffer (free once the last layer's MMA has read it),
+        // each row's eight 16-byte chunks rotated by the row so that 8
+        // consecutive rows store to different banks, then copied out by the
+        // pipeline with coalesced stores.  Rows past the guided depth are
+        // written too; shading reads a mixture only at guided depths.
+        union {
+            GuideMixture m;
+            uint4 c[8];
+        } mix;
+        static_assert(sizeof(GuideMixture) == 8 * sizeof(uint4), "a mixture is eight 16-byte chunks");
+        mix.m = pack(decode(o));
+        uint4 *stage = reinterpret_cast<uint4 *>(sm.a[pipe]);
+#pragma unroll
+        for (int j = 0; j < 8; j++) stage[row * 8 + (j ^ (row & 7))] = mix.c[j];
+        pipeSync(pipe);
+        const uint32_t first = tile * kTcPipeThreads;
+        const uint32_t chunks = min((uint32_t)kTcPipeThreads, nHit - first) * 8u;
+        uint4 *dst = reinterpret_cast<uint4 *>(out + first);
+        for (uint32_t k = row; k < chunks; k += kTcPipeThreads) dst[k] = stage[(k & ~7u) + ((k & 7u) ^ ((k >> 3) & 7u))];
+        pipeSync(pipe);  // the next tile's input rows overwrite the stage
     }
     tcTeardown(sm, pipe, phase);
 }
