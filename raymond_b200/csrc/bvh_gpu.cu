@@ -23,7 +23,7 @@
 //  4. The collapse into 8-wide nodes, level by level: a node opens the
 //     inner child of largest area until it has 8 children (subtrees of at
 //     most 3 triangles are leaves), places the children in octant slots and
-//     quantises their boxes, exactly as the host collapse does; scans of
+//     quantises their boxes, as the host's greedy collapse does; scans of
 //     the children and leaf triangles per node place the next level's nodes
 //     and the triangles.
 //
@@ -416,7 +416,7 @@ struct Tree {
 };
 
 // Children of one 8-wide node by slot (-1: empty) and its (inner children,
-// leaf triangles); the same choices as the host collapse.
+// leaf triangles); the same choices as the host's greedy collapse.
 __global__ void k_collapse_plan(Tree t, const uint2 *entries, uint32_t m, int *slots, uint2 *counts) {
     for (uint32_t e = blockIdx.x * blockDim.x + threadIdx.x; e < m; e += gridDim.x * blockDim.x) {
         const int root = (int)entries[e].x;

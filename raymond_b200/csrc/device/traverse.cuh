@@ -235,67 +235,79 @@ RMD_HD void beginTraversal(TraversalState &s, const WideNode *nodes, float3 o, f
 // group waits on the stack.  The triangles a node's leaf children hit are
 // intersected as soon as the node is visited, so the closest hit found so far
 // culls what follows.  ANY: stop at the first hit (raytrace.metal:52-85);
-// otherwise keep the closest (raytrace.metal:11-50).  (Dynamic ray fetch,
-// Aila & Laine, HPG 2009, measured slower with this tree too.)
+// otherwise keep the closest (raytrace.metal:11-50).
+//
+// One call visits one node (and its triangles) and returns true once the
+// traversal has finished, so a persistent warp can hand a finished lane a new
+// ray between two steps.
 template <bool ANY>
-RMD_HD void traverse(TraversalState &s, TraversalStack &stack, const WideNode *__restrict__ nodes,
-                     const float4 *__restrict__ tris, uint32_t *errors) {
-    if (s.sp < 0) return;
+RMD_HD bool traverseStep(TraversalState &s, TraversalStack &stack, const WideNode *__restrict__ nodes,
+                         const float4 *__restrict__ tris, uint32_t *errors) {
+    if (s.sp < 0) return true;
     const float3 idir = s.r.idir, org = s.r.org;
     const uint32_t octant = rayOctant(idir);
     uint2 group = s.group;
     int sp = s.sp;
-    while (true) {
+    if (group.y > 0x00ffffffu) {
+        const uint32_t key = __ffs(group.y >> 24) - 1;
+        group.y &= ~(1u << (24u + key));
+        const uint32_t slot = key ^ octant;
+        const uint32_t index = group.x + __popc(group.y & ((1u << slot) - 1u) & 0xffu);
         if (group.y > 0x00ffffffu) {
-            const uint32_t key = __ffs(group.y >> 24) - 1;
-            group.y &= ~(1u << (24u + key));
-            const uint32_t slot = key ^ octant;
-            const uint32_t index = group.x + __popc(group.y & ((1u << slot) - 1u) & 0xffu);
-            if (group.y > 0x00ffffffu) {
-                if (sp < TRAVERSAL_STACK) stack[sp++] = group;
-                else atomicOr(errors, 2u);
-            }
-            const WideNode *np = &nodes[index];
-            const WideNode n = {__ldg(&np->originScale), __ldg(&np->bases), __ldg(&np->qloXY),
-                                __ldg(&np->qloZqhiX), __ldg(&np->qhiYZ)};
-            const uint32_t hits = intersectChildren(n, idir, org, octant, s.tmin, fmaf(s.tmax, 1.000002f, s.slack));
-            group = make_uint2(n.bases.x, (hits & 0xff000000u) | (__float_as_uint(n.originScale.w) >> 24));
-            uint32_t triHits = hits & 0x00ffffffu;
-            while (triHits) {
-                const int ti = (int)n.bases.y + __ffs(triHits) - 1;
-                triHits &= triHits - 1u;
-                const float4 a = __ldg(&tris[3 * ti + 0]);
-                const float4 b = __ldg(&tris[3 * ti + 1]);
-                const float4 c = __ldg(&tris[3 * ti + 2]);
-                float t, b0, b1;
-                if (intersectTriangle(s.r.wr, xyz(a), xyz(b), xyz(c), s.tmin, s.tmax, t, b0, b1)) {
-                    if (ANY) {
-                        s.hitTri = ti;
-                        s.sp = -1;
-                        return;
-                    }
-                    // Equal distances (coplanar overlapping faces) go to the lower
-                    // (instance, primitive), whatever order the tree is visited in,
-                    // so every BVH of the scene reports the same closest hit.
-                    const uint32_t inst = __float_as_uint(a.w), prim = __float_as_uint(b.w);
-                    if (t < s.tmax || s.hitTri < 0 || inst < s.hitInst || (inst == s.hitInst && prim < s.hitPrim)) {
-                        s.hitTri = ti;
-                        s.hitInst = inst;
-                        s.hitPrim = prim;
-                        s.tmax = t;
-                        s.b0 = b0;
-                        s.b1 = b1;
-                    }
+            if (sp < TRAVERSAL_STACK) stack[sp++] = group;
+            else atomicOr(errors, 2u);
+        }
+        const WideNode *np = &nodes[index];
+        const WideNode n = {__ldg(&np->originScale), __ldg(&np->bases), __ldg(&np->qloXY),
+                            __ldg(&np->qloZqhiX), __ldg(&np->qhiYZ)};
+        const uint32_t hits = intersectChildren(n, idir, org, octant, s.tmin, fmaf(s.tmax, 1.000002f, s.slack));
+        group = make_uint2(n.bases.x, (hits & 0xff000000u) | (__float_as_uint(n.originScale.w) >> 24));
+        uint32_t triHits = hits & 0x00ffffffu;
+        while (triHits) {
+            const int ti = (int)n.bases.y + __ffs(triHits) - 1;
+            triHits &= triHits - 1u;
+            const float4 a = __ldg(&tris[3 * ti + 0]);
+            const float4 b = __ldg(&tris[3 * ti + 1]);
+            const float4 c = __ldg(&tris[3 * ti + 2]);
+            float t, b0, b1;
+            if (intersectTriangle(s.r.wr, xyz(a), xyz(b), xyz(c), s.tmin, s.tmax, t, b0, b1)) {
+                if (ANY) {
+                    s.hitTri = ti;
+                    s.sp = -1;
+                    return true;
+                }
+                // Equal distances (coplanar overlapping faces) go to the lower
+                // (instance, primitive), whatever order the tree is visited in,
+                // so every BVH of the scene reports the same closest hit.
+                const uint32_t inst = __float_as_uint(a.w), prim = __float_as_uint(b.w);
+                if (t < s.tmax || s.hitTri < 0 || inst < s.hitInst || (inst == s.hitInst && prim < s.hitPrim)) {
+                    s.hitTri = ti;
+                    s.hitInst = inst;
+                    s.hitPrim = prim;
+                    s.tmax = t;
+                    s.b0 = b0;
+                    s.b1 = b1;
                 }
             }
         }
-        if (group.y <= 0x00ffffffu) {
-            if (sp == 0) {
-                s.sp = -1;
-                return;
-            }
-            group = stack[--sp];
+    }
+    if (group.y <= 0x00ffffffu) {
+        if (sp == 0) {
+            s.sp = -1;
+            return true;
         }
+        group = stack[--sp];
+    }
+    s.group = group;
+    s.sp = sp;
+    return false;
+}
+
+// The whole traversal of one ray.
+template <bool ANY>
+RMD_HD void traverse(TraversalState &s, TraversalStack &stack, const WideNode *__restrict__ nodes,
+                     const float4 *__restrict__ tris, uint32_t *errors) {
+    while (!traverseStep<ANY>(s, stack, nodes, tris, errors)) {
     }
 }
 
