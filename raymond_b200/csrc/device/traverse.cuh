@@ -111,10 +111,12 @@ RMD_HD TraceRay makeTraceRay(float3 o, float3 d) {
     return r;
 }
 
-// Byte i of w as a float, exactly: the byte becomes the low mantissa byte of
-// 2^23 (one byte permute) and 2^23 is subtracted.
-RMD_HD float byteToFloat(uint32_t w, uint32_t i) {
-    return __uint_as_float(__byte_perm(w, 0x4B000000u, 0x7540u | i)) - 8388608.0f;
+// Byte q = byte i of w as the float 256 + q / 128, exactly: one byte permute
+// puts q in the mantissa of 256.  A plane at q quanta from the node origin
+// then lies at t = (256 + q / 128) * (128 a) + (b - 32768 a), one multiply-add
+// per plane with no conversion of q.
+RMD_HD float bytePlane(uint32_t w, uint32_t i) {
+    return __uint_as_float(__byte_perm(w, 0x43800000u, 0x7604u | (i << 4)));
 }
 
 // Ray/box tests of a node's 8 children.  Returns the children the ray enters
@@ -128,17 +130,24 @@ RMD_HD uint32_t intersectChildren(const WideNode &n, const float3 idir, const fl
     const float sy = __uint_as_float(((ew >> 8) & 0xffu) << 23);
     const float sz = __uint_as_float(((ew >> 16) & 0xffu) << 23);
     const uint32_t imask = ew >> 24;
-    const float ax = sx * idir.x, ay = sy * idir.y, az = sz * idir.z;  // exact: powers of two
+    const float ax = sx * idir.x, ay = sy * idir.y, az = sz * idir.z;  // one quantum in t: exact, powers of two
     const float bx = (n.originScale.x - org.x) * idir.x;
     const float by = (n.originScale.y - org.y) * idir.y;
     const float bz = (n.originScale.z - org.z) * idir.z;
     // origin - org and its product with the rounded 1/d each round once, an
     // absolute error of at most 2^-23 |b| in every plane distance, which a
     // relative widening cannot cover when the hit lies close to the origin
-    // next to a far node origin: near planes move down and far planes up by
-    // 3e-7 |b| (per axis, so an axis the ray runs parallel to stays decided)
-    const float ex = 3.0e-7f * fabsf(bx), ey = 3.0e-7f * fabsf(by), ez = 3.0e-7f * fabsf(bz);
-    const float bxN = bx - ex, bxF = bx + ex, byN = by - ey, byF = by + ey, bzN = bz - ez, bzF = bz + ez;
+    // next to a far node origin; b +- w and b - 32768 a round once more each
+    // (2^-24 |b| + 2^-9 a).  Near planes therefore move down and far planes
+    // up by w = 4e-7 |b| + a / 128 (per axis, so an axis the ray runs
+    // parallel to stays decided).  (128 a) * (256 + q / 128) is exact.
+    const float wx = fmaf(4.0e-7f, fabsf(bx), 0.0078125f * fabsf(ax));
+    const float wy = fmaf(4.0e-7f, fabsf(by), 0.0078125f * fabsf(ay));
+    const float wz = fmaf(4.0e-7f, fabsf(bz), 0.0078125f * fabsf(az));
+    const float bxN = fmaf(-32768.0f, ax, bx - wx), bxF = fmaf(-32768.0f, ax, bx + wx);
+    const float byN = fmaf(-32768.0f, ay, by - wy), byF = fmaf(-32768.0f, ay, by + wy);
+    const float bzN = fmaf(-32768.0f, az, bz - wz), bzF = fmaf(-32768.0f, az, bz + wz);
+    const float Ax = 128.0f * ax, Ay = 128.0f * ay, Az = 128.0f * az;
     // per axis the near plane is the lower bound for a positive direction
     const uint2 loX = make_uint2(n.qloXY.x, n.qloXY.y), hiX = make_uint2(n.qloZqhiX.z, n.qloZqhiX.w);
     const uint2 loY = make_uint2(n.qloXY.z, n.qloXY.w), hiY = make_uint2(n.qhiYZ.x, n.qhiYZ.y);
@@ -157,9 +166,9 @@ RMD_HD uint32_t intersectChildren(const WideNode &n, const float3 idir, const fl
 #pragma unroll
         for (uint32_t i = 0; i < 4; i++) {
             const uint32_t slot = 4 * half + i;
-            const float t0x = fmaf(byteToFloat(nxw, i), ax, bxN), t1x = fmaf(byteToFloat(fxw, i), ax, bxF);
-            const float t0y = fmaf(byteToFloat(nyw, i), ay, byN), t1y = fmaf(byteToFloat(fyw, i), ay, byF);
-            const float t0z = fmaf(byteToFloat(nzw, i), az, bzN), t1z = fmaf(byteToFloat(fzw, i), az, bzF);
+            const float t0x = fmaf(bytePlane(nxw, i), Ax, bxN), t1x = fmaf(bytePlane(fxw, i), Ax, bxF);
+            const float t0y = fmaf(bytePlane(nyw, i), Ay, byN), t1y = fmaf(bytePlane(fyw, i), Ay, byF);
+            const float t0z = fmaf(bytePlane(nzw, i), Az, bzN), t1z = fmaf(bytePlane(fzw, i), Az, bzF);
             const float enter = fmaxf(fmaxf(t0x, t0y), fmaxf(t0z, tmin));
             const float leave = fminf(fminf(t1x, t1y), fminf(t1z, tmax));
             // widen the far bound by a few ulps (Ize 2013) so FMA rounding never culls a hit
