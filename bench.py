@@ -77,7 +77,7 @@ BYTES_FILM_PER_PATH = 16 + 32 + 80
 # DRAM bytes per unit measured by ncu (dram__bytes_read.sum + dram__bytes_write.sum
 # of one steady-state launch of the 480x270 case divided by the rays it
 # processed); only the closest-hit kernel's is used
-TRAFFIC_PER_UNIT = {"trace": 78.5}
+TRAFFIC_PER_UNIT = {"trace": 76.9}
 GUIDED_W, GUIDED_H, GUIDED_DEPTH, GUIDED_ORACLE_SPP, GUIDED_PLAIN_SPP, GUIDED_CHUNK = 1280, 720, 16, 65536, 1024, 32
 # guide settings of the guided legs (configs 4 and 5): Adam steps per 2^20 tracer samples, records per step
 # the guided legs' training settings; the learning rate is three times the
