@@ -58,7 +58,15 @@ __device__ __forceinline__ bool shadePath(const ShadeParams &p, uint32_t i, uint
     float3 shadowDir = f3(0.0f);
     float4 next[3];                      // rayO, rayD, tp of the continued path
     float L4next = 0.0f;                 // its depth | flags word
-    const bool training = S.rec != nullptr;
+    // RMD_PLAIN_SHADE: the module of a renderer or batch that neither samples
+    // from nor trains the guide, with the guide's code compiled out (a shorter
+    // kernel fetches fewer instructions)
+#ifdef RMD_PLAIN_SHADE
+    constexpr bool kGuideCode = false;
+#else
+    constexpr bool kGuideCode = true;
+#endif
+    const bool training = kGuideCode && S.rec != nullptr;
     float4 record[4] = {f4(0.0f), f4(0.0f), f4(0.0f), f4(0.0f)};  // guide training record
     bool recorded = false;  // this vertex replaced the path's record
 
@@ -103,7 +111,7 @@ __device__ __forceinline__ bool shadePath(const ShadeParams &p, uint32_t i, uint
         // Guiding: directions come from the BSDF or, with probability alpha, from
         // the guide mixture of this point (one-sample MIS); the technique's pdf is
         // then alpha q + (1 - alpha) p_bsdf in every MIS weight that uses it.
-        const bool guided = depth < fp.guideDepth;
+        const bool guided = kGuideCode && depth < fp.guideDepth;
         const GuideMixture *gm = &pool.guide[orderPos];  // hits are shaded in order: mixture by that position
         float alpha = guided ? gm->alpha : 0.0f;
         if (guided) {

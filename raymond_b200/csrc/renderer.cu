@@ -151,7 +151,9 @@ struct rmd_scene {
     DevBuf textureTexels, textureViews;  // RGBA float texels of all textures; one TextureView each
     rmdhost::JitModule jit;   // default variant (envmap build, test hooks, default shade kernel)
     std::string moduleSource;
-    std::map<int, std::unique_ptr<rmdhost::JitModule>> variants;  // shade kernels by minimum blocks per SM
+    // shading kernels by shadeVariantKey(minimum blocks per SM, guide code);
+    // `jit` is the default budget without the guide's code
+    std::map<int, std::unique_ptr<rmdhost::JitModule>> variants;
     uint64_t triangles = 0, bvhNodeCount = 0;
     std::vector<rmd_per_instance_data> instanceRecords;  // EntityBuilder's records, bridge layout
     rmd_bvh_stats bvhStats{};  // builder, build time and levels; SAH cost computed when first asked
@@ -187,6 +189,7 @@ struct rmd_renderer {
     cudaKernel_t shade = nullptr;
     int shadeBlocks = 0;
     int shadeMinBlocks = 1;
+    bool shadeGuided = false;  // the shading kernel carries the guide's sampling and training code
     int traceBlocksPerSm = 12;
     DevBuf pool;  // path state, finish list and shadow rays (carvePathPool)
     DevBuf counters, film, film64, resolve;
@@ -227,7 +230,7 @@ struct rmd_batch {
     std::vector<std::unique_ptr<rmd_scene>> scenes;
     rmdhost::JitModule jit;  // the merged material module of all scenes (batch shading kernel)
     std::string moduleSource;
-    std::map<int, std::unique_ptr<rmdhost::JitModule>> variants;  // shading kernels by minimum blocks per SM
+    std::map<int, std::unique_ptr<rmdhost::JitModule>> variants;  // shading kernels by shadeVariantKey
     std::vector<rmd_batch_view> views;
     std::vector<uint32_t> offsets;  // film pixel offset of each view
     uint32_t totalPixels = 0;
@@ -236,6 +239,7 @@ struct rmd_batch {
     uint32_t capacity = 0;
     cudaKernel_t shade = nullptr;
     int shadeBlocks = 0, shadeMinBlocks = 1, defaultMinBlocks = 1, traceBlocksPerSm = 12;
+    bool shadeGuided = false;
     bool useGraph = true;
     GuideState guide;  // learned path guiding (all views of one scene)
     int guideScene = -1;
@@ -378,6 +382,10 @@ rmd_status setLastError(rmd_status status, const char *msg) { return fail(status
 
 // --------------------------------------------------------------------- C ABI
 extern "C" {
+
+// shading-kernel variants (defined with the autotuner)
+static rmd_status ensureVariants(rmd_scene *s, const std::vector<int> &minBlocks, bool guided);
+static void selectShade(rmd_renderer *r, int mb, bool guided);
 
 const char *rmd_last_error(void) { return g_lastError.c_str(); }
 const char *rmd_version(void) { return "raymond_b200 0.1 (sm_100a)"; }
@@ -803,7 +811,7 @@ rmd_status rmd_scene_create(rmd_context *ctx, const rmd_scene_desc *d, rmd_scene
     }
     if ((r = buildSceneData(ctx, d, s.get(), mod, 0, 0, tex.list.data(), (int)tex.list.size())) != RMD_OK) return r;
     const std::string err = rmdhost::compileModule(
-        mod.source, s->jit, {"-DRMD_SHADE_MIN_BLOCKS=" + std::to_string(s->defaultMinBlocks)});
+        mod.source, s->jit, {"-DRMD_SHADE_MIN_BLOCKS=" + std::to_string(s->defaultMinBlocks), "-DRMD_PLAIN_SHADE"});
     if (!err.empty()) return fail(RMD_ERROR_NVRTC, err);
     s->moduleSource = mod.source;
     if ((r = buildEnvironmentMap(s.get(), d->envmap_exponent)) != RMD_OK) return r;
@@ -1142,12 +1150,17 @@ rmd_status rmd_render(rmd_renderer *r, const rmd_render_settings *s) {
     void *shadeArgs[] = {&sp};
     const int tb = ctx->smCount * r->traceBlocksPerSm;
     const int rb = std::min<int>((r->capacity + 255) / 256, ctx->smCount * 8);
-    const int sb = r->shadeBlocks;
 
     // guiding
     auto &guide = r->guide;
     const bool guideSampling = guide.settings.sampling != 0;
     const bool guideTraining = guide.settings.training != 0;
+    if (r->shadeGuided != (guideSampling || guideTraining)) {  // the shading kernel with or without the guide's code
+        rmd_status vs = ensureVariants(scene, {r->shadeMinBlocks}, guideSampling || guideTraining);
+        if (vs != RMD_OK) return vs;
+        selectShade(r, r->shadeMinBlocks, guideSampling || guideTraining);
+    }
+    const int sb = r->shadeBlocks;
     GuideNetView net{};
     if (guideSampling || guideTraining) {
         rmd_status gs = ensureGuideBuffers(r);
@@ -1326,10 +1339,21 @@ rmd_status rmd_renderer_stats(const rmd_renderer *r, rmd_stats *out) {
 }
 
 // --------------------------------------------------------------------- autotuner
-static rmd_status ensureVariants(rmd_scene *s, const std::vector<int> &minBlocks) {
+// Shading-kernel variants: a register budget (minimum 128-thread blocks per
+// SM) and whether the kernel carries the guide's sampling and training code;
+// renderers and batches that do not guide run the kernel without it.
+static int shadeVariantKey(int minBlocks, bool guided) { return minBlocks | (guided ? 0x100 : 0); }
+static std::vector<std::string> shadeDefines(int minBlocks, bool guided) {
+    std::vector<std::string> d = {"-DRMD_SHADE_MIN_BLOCKS=" + std::to_string(minBlocks)};
+    if (!guided) d.push_back("-DRMD_PLAIN_SHADE");
+    return d;
+}
+
+static rmd_status ensureVariants(rmd_scene *s, const std::vector<int> &minBlocks, bool guided) {
     std::vector<int> missing;
     for (int mb : minBlocks)
-        if (mb != s->defaultMinBlocks && !s->variants.count(mb)) missing.push_back(mb);
+        if ((guided || mb != s->defaultMinBlocks) && !s->variants.count(shadeVariantKey(mb, guided)))
+            missing.push_back(mb);
     // NVRTC is thread-safe: compile the missing variants in parallel, load them serially
     std::vector<std::vector<char>> cubins(missing.size());
     std::vector<std::string> errs(missing.size()), logs(missing.size());
@@ -1338,7 +1362,7 @@ static rmd_status ensureVariants(rmd_scene *s, const std::vector<int> &minBlocks
         th.emplace_back([&, i] {
             bool cached = false;
             errs[i] = rmdhost::compileCubin(s->moduleSource, cubins[i], logs[i], cached,
-                                            {"-DRMD_SHADE_MIN_BLOCKS=" + std::to_string(missing[i])});
+                                            shadeDefines(missing[i], guided));
         });
     }
     for (auto &t : th) t.join();
@@ -1347,24 +1371,29 @@ static rmd_status ensureVariants(rmd_scene *s, const std::vector<int> &minBlocks
         auto m = std::make_unique<rmdhost::JitModule>();
         RMD_CUDA(cudaLibraryLoadData(&m->library, cubins[i].data(), nullptr, nullptr, 0, nullptr, nullptr, 0));
         RMD_CUDA(cudaLibraryGetKernel(&m->shade, m->library, "rmd_shade"));
-        s->variants[missing[i]] = std::move(m);
+        s->variants[shadeVariantKey(missing[i], guided)] = std::move(m);
     }
     return RMD_OK;
 }
 
-static void selectShade(rmd_renderer *r, int mb) {
+// the variant must have been compiled (ensureVariants)
+static void selectShade(rmd_renderer *r, int mb, bool guided) {
     rmd_scene *s = r->scene;
-    cudaKernel_t k = mb == s->defaultMinBlocks ? s->jit.shade : s->variants.at(mb)->shade;
+    cudaKernel_t k = !guided && mb == s->defaultMinBlocks ? s->jit.shade : s->variants.at(shadeVariantKey(mb, guided))->shade;
     r->shade = k;
     r->shadeMinBlocks = mb;
+    r->shadeGuided = guided;
     r->shadeBlocks = occupancyBlocks((const void *)k, 128, s->ctx->smCount);
 }
+
+static bool guideActive(const GuideState &g) { return g.settings.sampling || g.settings.training; }
 
 rmd_status rmd_renderer_autotune(rmd_renderer *r, const rmd_render_settings *settings, rmd_tune_result *out) {
     if (!r || !settings) return fail(RMD_ERROR_INVALID_ARGUMENT, "NULL argument");
     rmd_scene *s = r->scene;
     const std::vector<int> mbs = {1, 3, 4, 5, 6};
-    rmd_status st = ensureVariants(s, mbs);
+    const bool guided = guideActive(r->guide);
+    rmd_status st = ensureVariants(s, mbs, guided);
     if (st != RMD_OK) return st;
     // calibration: enough paths for several pool generations, capped in time
     rmd_render_settings cal = *settings;
@@ -1391,7 +1420,7 @@ rmd_status rmd_renderer_autotune(rmd_renderer *r, const rmd_render_settings *set
     double bestMs = base;
     for (int mb : mbs) {
         if (mb == r->shadeMinBlocks) continue;
-        selectShade(r, mb);
+        selectShade(r, mb, guided);
         double ms;
         if ((st = trial(ms)) != RMD_OK) return st;
         if (ms < bestMs) {
@@ -1399,7 +1428,7 @@ rmd_status rmd_renderer_autotune(rmd_renderer *r, const rmd_render_settings *set
             bestMb = mb;
         }
     }
-    selectShade(r, bestMb);
+    selectShade(r, bestMb, guided);
     // 2) traversal blocks per SM
     int bestTb = r->traceBlocksPerSm;
     for (int tb : {4, 12, 16}) {
@@ -1448,9 +1477,9 @@ rmd_status rmd_renderer_set_tuning(rmd_renderer *r, const rmd_tune_result *t) {
         return fail(RMD_ERROR_INVALID_ARGUMENT, "tuning out of range");
     RMD_CUDA(cudaSetDevice(r->scene->ctx->device));
     const int mb = (int)t->shade_min_blocks;
-    rmd_status st = ensureVariants(r->scene, {mb});
+    rmd_status st = ensureVariants(r->scene, {mb}, r->shadeGuided);
     if (st != RMD_OK) return st;
-    selectShade(r, mb);
+    selectShade(r, mb, r->shadeGuided);
     r->traceBlocksPerSm = (int)t->trace_blocks_per_sm;
     if (t->pool_size != 0 && t->pool_size != r->capacity) {
         r->capacity = t->pool_size;
@@ -1623,10 +1652,12 @@ static PathPool batchPoolView(const rmd_batch *b) {
     return pool;
 }
 
-static void batchSelectShade(rmd_batch *b, int mb) {
-    cudaKernel_t k = mb == b->defaultMinBlocks ? b->jit.shade : b->variants.at(mb)->shade;
+// the variant must have been compiled (batchEnsureVariants)
+static void batchSelectShade(rmd_batch *b, int mb, bool guided) {
+    cudaKernel_t k = !guided && mb == b->defaultMinBlocks ? b->jit.shade : b->variants.at(shadeVariantKey(mb, guided))->shade;
     b->shade = k;
     b->shadeMinBlocks = mb;
+    b->shadeGuided = guided;
     b->shadeBlocks = occupancyBlocks((const void *)k, 128, b->ctx->smCount);
     if (b->graphExec) {
         cudaGraphExecDestroy(b->graphExec);
@@ -1635,14 +1666,16 @@ static void batchSelectShade(rmd_batch *b, int mb) {
     b->graphKey.clear();
 }
 
-static rmd_status batchEnsureVariants(rmd_batch *b, const std::vector<int> &minBlocks) {
+static rmd_status batchEnsureVariants(rmd_batch *b, const std::vector<int> &minBlocks, bool guided) {
     for (int mb : minBlocks) {
-        if (mb == b->defaultMinBlocks || b->variants.count(mb)) continue;
+        const int key = shadeVariantKey(mb, guided);
+        if ((!guided && mb == b->defaultMinBlocks) || b->variants.count(key)) continue;
         auto m = std::make_unique<rmdhost::JitModule>();
-        const std::string err =
-            rmdhost::compileModule(b->moduleSource, *m, {"-DRMD_SHADE_MIN_BLOCKS=" + std::to_string(mb), "-DRMD_BATCH"});
+        std::vector<std::string> defines = shadeDefines(mb, guided);
+        defines.push_back("-DRMD_BATCH");
+        const std::string err = rmdhost::compileModule(b->moduleSource, *m, defines);
         if (!err.empty()) return fail(RMD_ERROR_NVRTC, err);
-        b->variants[mb] = std::move(m);
+        b->variants[key] = std::move(m);
     }
     return RMD_OK;
 }
@@ -1719,7 +1752,7 @@ rmd_status rmd_batch_create(rmd_context *ctx, const rmd_scene_desc *descs, int32
     }
     b->defaultMinBlocks = defaultShadeMinBlocks();
     const std::string err = rmdhost::compileModule(
-        mod.source, b->jit, {"-DRMD_SHADE_MIN_BLOCKS=" + std::to_string(b->defaultMinBlocks), "-DRMD_BATCH"});
+        mod.source, b->jit, {"-DRMD_SHADE_MIN_BLOCKS=" + std::to_string(b->defaultMinBlocks), "-DRMD_PLAIN_SHADE", "-DRMD_BATCH"});
     if (!err.empty()) return fail(RMD_ERROR_NVRTC, err);
     b->moduleSource = mod.source;
     for (int i = 0; i < numScenes; i++) {
@@ -1768,7 +1801,7 @@ rmd_status rmd_batch_create(rmd_context *ctx, const rmd_scene_desc *descs, int32
     if (r != RMD_OK) return r;
     RMD_CUDA(cudaMallocHost((void **)&b->hostCounters, sizeof(Counters)));
     for (auto &e : b->ev) RMD_CUDA(cudaEventCreate(&e));
-    batchSelectShade(b.get(), b->defaultMinBlocks);
+    batchSelectShade(b.get(), b->defaultMinBlocks, false);
     *out = b.release();
     return RMD_OK;
 }
@@ -1840,6 +1873,11 @@ rmd_status rmd_batch_render(rmd_batch *b, const rmd_render_settings *s) {
     fp.film64 = b->film64.as<double>();
     // guiding (all views of one scene)
     GuideState &guide = b->guide;
+    if (b->shadeGuided != guideActive(guide)) {  // the shading kernel with or without the guide's code
+        rmd_status vs = batchEnsureVariants(b, {b->shadeMinBlocks}, guideActive(guide));
+        if (vs != RMD_OK) return vs;
+        batchSelectShade(b, b->shadeMinBlocks, guideActive(guide));
+    }
     GuideNetView net{};
     if (guide.settings.sampling || guide.settings.training) {
         rmd_status gs = guideBuffers(guide, b->capacity, b->counters.as<Counters>());
@@ -2018,7 +2056,8 @@ rmd_status rmd_batch_stats(const rmd_batch *b, rmd_stats *out) {
 rmd_status rmd_batch_autotune(rmd_batch *b, const rmd_render_settings *settings, rmd_tune_result *out) {
     if (!b || !settings) return fail(RMD_ERROR_INVALID_ARGUMENT, "NULL argument");
     const std::vector<int> mbs = {1, 3, 4, 5, 6};
-    rmd_status st = batchEnsureVariants(b, mbs);
+    const bool guided = guideActive(b->guide);
+    rmd_status st = batchEnsureVariants(b, mbs, guided);
     if (st != RMD_OK) return st;
     rmd_render_settings cal = *settings;
     cal.film_fp64 = 0;
@@ -2043,7 +2082,7 @@ rmd_status rmd_batch_autotune(rmd_batch *b, const rmd_render_settings *settings,
     double bestMs = base;
     for (int mb : mbs) {
         if (mb == b->shadeMinBlocks) continue;
-        batchSelectShade(b, mb);
+        batchSelectShade(b, mb, guided);
         double ms;
         if ((st = trial(ms)) != RMD_OK) return st;
         if (ms < bestMs) {
@@ -2051,7 +2090,7 @@ rmd_status rmd_batch_autotune(rmd_batch *b, const rmd_render_settings *settings,
             bestMb = mb;
         }
     }
-    batchSelectShade(b, bestMb);
+    batchSelectShade(b, bestMb, guided);
     int bestTb = b->traceBlocksPerSm;
     for (int tb : {4, 12, 16}) {
         b->traceBlocksPerSm = tb;
