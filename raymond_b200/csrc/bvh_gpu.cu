@@ -20,12 +20,19 @@
 //     regular geometry (grids of equal triangles) still merges in parallel;
 //     an iteration that merges fewer than 1/16 of the clusters is replaced
 //     by merging Morton neighbours pairwise, which bounds the iteration count.
-//  4. The collapse into 8-wide nodes, level by level: a node opens the
-//     inner child of largest area until it has 8 children (subtrees of at
-//     most 3 triangles are leaves), places the children in octant slots and
-//     quantises their boxes, as the host's greedy collapse does; scans of
-//     the children and leaf triangles per node place the next level's nodes
-//     and the triangles.
+//  4. The SAH-optimal collapse into 8-wide nodes, as the host builder makes
+//     it (Ylitie, Karras and Laine 2017, section 3.1): bottom up, one launch
+//     per clustering iteration (a node's children were made in earlier
+//     iterations), every binary node gets the least surface-area cost of its
+//     subtree as at most 1..8 slots of its parent (a leaf of at most 3
+//     triangles, an inner node, or a spread over several slots) and the
+//     choices that reach it.  Then level by level from the root, each node
+//     collects its slots from those choices, places the children in octant
+//     slots and quantises their boxes; scans of the children and leaf
+//     triangles per node place the next level's nodes and the triangles.  A
+//     tree the optimal collapse would make deeper than the traversal stack is
+//     collapsed again greedily (open the inner child of largest area until a
+//     node has 8 children).
 //
 // Every kernel's indexes are bounded by its element count; the host loop
 // reads one 8-byte total per clustering iteration and per tree level.
@@ -401,12 +408,82 @@ __global__ void k_ploc_compact(const uint32_t *cl, const float4 *clLo, const flo
     }
 }
 
+// ------------------------------------------------------- optimal collapse
+// cost[8 i + s - 1]: the least cost of node i's subtree given as at most s
+// slots of its parent (leaf slot: area * triangles; inner node: area + its
+// subtree as 8 slots); choice[8 i]: 1 if i as one slot is a leaf; choice[8 i +
+// s - 1], s > 1: 0 if s - 1 slots do as well, else the left child's slots;
+// split[i]: the left child's slots when i is an inner node.  Ties favour
+// more slots (a shallower tree).  The host builder's recurrence.
+__device__ __forceinline__ float boxArea(float4 l, float4 h) {
+    const float ex = h.x - l.x, ey = h.y - l.y, ez = h.z - l.z;
+    if (ex < 0.0f) return 0.0f;
+    return 2.0f * (ex * ey + ey * ez + ez * ex);
+}
+
+__global__ void k_dp_leaves(const float4 *lo, const float4 *hi, uint32_t n, float *cost, uint8_t *choice) {
+    for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+        const float leaf = boxArea(lo[i], hi[i]);  // one triangle
+        for (int k = 0; k < 8; k++) {
+            cost[8 * (size_t)i + k] = leaf;
+            choice[8 * (size_t)i + k] = k == 0 ? 1 : 0;
+        }
+    }
+}
+
+__global__ void k_dp_nodes(const float4 *lo, const float4 *hi, const int2 *child, uint32_t base, uint32_t count,
+                           float *cost, uint8_t *choice, uint8_t *split) {
+    for (uint32_t j = blockIdx.x * blockDim.x + threadIdx.x; j < count; j += gridDim.x * blockDim.x) {
+        const size_t i = (size_t)base + j;
+        const int2 ch = child[i];
+        const float4 l = lo[i], h = hi[i];
+        const uint32_t tris = __float_as_uint(l.w);
+        const float area = boxArea(l, h);
+        const float leaf = tris <= kLeafTris ? area * (float)tris : FLT_MAX;
+        float cl[8], cr[8];
+        for (int k = 0; k < 8; k++) {
+            cl[k] = cost[8 * (size_t)ch.x + k];
+            cr[k] = cost[8 * (size_t)ch.y + k];
+        }
+        float dist[9];
+        uint8_t distK[9];
+        for (int s = 2; s <= 8; s++) {
+            dist[s] = FLT_MAX;
+            distK[s] = 1;
+            for (int k = 1; k < s; k++) {
+                const float v = cl[k - 1] + cr[s - k - 1];
+                if (v < dist[s]) {
+                    dist[s] = v;
+                    distK[s] = (uint8_t)k;
+                }
+            }
+        }
+        const float inner = area + dist[8];
+        split[i] = distK[8];
+        float c = fminf(leaf, inner);
+        cost[8 * i] = c;
+        choice[8 * i] = tris <= kLeafTris && leaf <= inner ? 1 : 0;
+        for (int s = 2; s <= 8; s++) {
+            if (dist[s] <= c) {
+                c = dist[s];
+                choice[8 * i + s - 1] = distK[s];
+            } else {
+                choice[8 * i + s - 1] = 0;
+            }
+            cost[8 * i + s - 1] = c;
+        }
+    }
+}
+
 // ---------------------------------------------------------------- collapse
 struct Tree {
     const float4 *lo, *hi;
     const int2 *child;
+    const uint8_t *choice, *split;  // the optimal collapse's choices; null: the greedy collapse
     __device__ uint32_t count(int i) const { return __float_as_uint(lo[i].w); }
     __device__ bool leaf(int i) const { return child[i].x < 0 || count(i) <= kLeafTris; }
+    // whether binary node i, as one slot of its parent, is a leaf
+    __device__ bool leafSlot(int i) const { return choice ? choice[8 * (size_t)i] == 1 : leaf(i); }
     __device__ float area(int i) const {
         const float4 l = lo[i], h = hi[i];
         const float ex = h.x - l.x, ey = h.y - l.y, ez = h.z - l.z;
@@ -422,13 +499,33 @@ __global__ void k_collapse_plan(Tree t, const uint2 *entries, uint32_t m, int *s
         const int root = (int)entries[e].x;
         int kids[8];
         int nk = 0;
-        if (t.leaf(root)) {
-            kids[nk++] = root;
+        if (entries[e].y == 0u && t.count(root) <= kLeafTris) {
+            kids[nk++] = root;  // the whole scene is one leaf
+        } else if (t.choice) {
+            // the slots of the optimal collapse: (subtree, slots it may take), left child first
+            int stNode[16], stSlots[16];
+            int top = 0;
+            const int k0 = t.split[root];
+            stNode[top] = t.child[root].y, stSlots[top++] = 8 - k0;
+            stNode[top] = t.child[root].x, stSlots[top++] = k0;
+            while (top > 0 && nk < 8) {
+                const int x = stNode[--top];
+                int sl = stSlots[top];
+                const bool binLeaf = t.child[x].x < 0;
+                while (sl > 1 && !binLeaf && t.choice[8 * (size_t)x + sl - 1] == 0) sl--;
+                if (sl == 1 || binLeaf) {
+                    kids[nk++] = x;
+                } else if (top + 2 <= 16) {
+                    const int k = t.choice[8 * (size_t)x + sl - 1];
+                    stNode[top] = t.child[x].y, stSlots[top++] = sl - k;
+                    stNode[top] = t.child[x].x, stSlots[top++] = k;
+                }
+            }
         } else {
             kids[nk++] = t.child[root].x;
             kids[nk++] = t.child[root].y;
         }
-        while (nk < 8) {
+        while (!t.choice && nk < 8) {
             int best = -1;
             float bestArea = -1.0f;
             for (int i = 0; i < nk; i++)
@@ -486,7 +583,7 @@ __global__ void k_collapse_plan(Tree t, const uint2 *entries, uint32_t m, int *s
             const int node = slotKid[sl] >= 0 ? kids[slotKid[sl]] : -1;
             slots[8 * (size_t)e + sl] = node;
             if (node < 0) continue;
-            if (t.leaf(node)) tris += t.count(node);
+            if (t.leafSlot(node)) tris += t.count(node);
             else inner++;
         }
         counts[e] = make_uint2(inner, tris);
@@ -558,7 +655,7 @@ __global__ void k_collapse_emit(Tree t, const uint2 *entries, uint32_t m, const 
         for (int sl = 0; sl < 8; sl++) {
             if (!used[sl]) continue;
             const int node = kid[sl];
-            if (!t.leaf(node)) {
+            if (!t.leafSlot(node)) {
                 w.imask |= (uint8_t)(1u << sl);
                 next[off.x + innerAt] = make_uint2((uint32_t)node, w.childBase + innerAt);
                 innerAt++;
@@ -701,6 +798,7 @@ cudaError_t buildWideBvhGpu(const float *v0, const float *v1, const float *v2, c
     int radius = kRadius;
     if (const char *env = std::getenv("RMD_BVH_RADIUS")) radius = std::max(1, std::min(kMaxRadius, std::atoi(env)));
     uint32_t clusters = n, nodeBase = n;
+    std::vector<std::pair<uint32_t, uint32_t>> made;  // (first node, count) of each clustering iteration
     int c = 0;
     while (clusters > 1) {
         if (++out.clusterIterations > 4096) {
@@ -722,6 +820,7 @@ cudaError_t buildWideBvhGpu(const float *v0, const float *v1, const float *v2, c
                                                                nodeBase, cl[c ^ 1], clLo[c ^ 1], clHi[c ^ 1], nodeLo,
                                                                nodeHi, nodeChild);
         BVH_TRY(cudaGetLastError());
+        made.emplace_back(nodeBase, total.y);
         nodeBase += total.y;
         clusters = total.x;
         c ^= 1;
@@ -745,13 +844,33 @@ cudaError_t buildWideBvhGpu(const float *v0, const float *v1, const float *v2, c
     BVH_TRY(S.alloc(slots, 8 * (size_t)n));
     BVH_TRY(S.alloc(plan, n));
     BVH_TRY(S.alloc(planPos, n));
+    // the optimal collapse's costs and choices, bottom up
+    float *dpCost;
+    uint8_t *dpChoice, *dpSplit;
+    BVH_TRY(S.alloc(dpCost, 8 * nodes2));
+    BVH_TRY(S.alloc(dpChoice, 8 * nodes2));
+    BVH_TRY(S.alloc(dpSplit, nodes2));
+    k_dp_leaves<<<gridFor(n, 256), 256, 0, s>>>(nodeLo, nodeHi, n, dpCost, dpChoice);
+    for (const auto &r : made)
+        if (r.second > 0)
+            k_dp_nodes<<<gridFor(r.second, 128), 128, 0, s>>>(nodeLo, nodeHi, nodeChild, r.first, r.second, dpCost,
+                                                               dpChoice, dpSplit);
+    BVH_TRY(cudaGetLastError());
     const uint2 first = make_uint2(root, 0u);
-    BVH_TRY(cudaMemcpyAsync(entries[0], &first, sizeof(first), cudaMemcpyHostToDevice, s));
-    const Tree t{nodeLo, nodeHi, nodeChild};
-    uint32_t level = 0, width = 1, wideCount = 1, triCount = 0;
+    Tree t{nodeLo, nodeHi, nodeChild, dpChoice, dpSplit};
+    uint32_t level = 0, width = 0, wideCount = 0, triCount = 0;
     int e = 0;
+    for (bool restart = true; restart;) {  // the optimal collapse, or the greedy one if that is too deep
+        restart = false;
+        BVH_TRY(cudaMemcpyAsync(entries[0], &first, sizeof(first), cudaMemcpyHostToDevice, s));
+        level = 0, width = 1, wideCount = 1, triCount = 0, e = 0;
     while (width > 0) {
         if (++level > kMaxWideLevels) {
+            if (t.choice) {
+                t.choice = t.split = nullptr;
+                restart = true;
+                break;
+            }
             out.error = "device BVH deeper than the traversal stack (32 levels)";
             return cudaErrorInvalidValue;
         }
@@ -770,6 +889,7 @@ cudaError_t buildWideBvhGpu(const float *v0, const float *v1, const float *v2, c
             out.error = "device BVH collapse produced more nodes than triangles";
             return cudaErrorInvalidValue;
         }
+    }
     }
     if (triCount != n) {
         out.error = "device BVH collapse placed " + std::to_string(triCount) + " of " + std::to_string(n) +
