@@ -1391,15 +1391,24 @@ static bool guideActive(const GuideState &g) { return g.settings.sampling || g.s
 rmd_status rmd_renderer_autotune(rmd_renderer *r, const rmd_render_settings *settings, rmd_tune_result *out) {
     if (!r || !settings) return fail(RMD_ERROR_INVALID_ARGUMENT, "NULL argument");
     rmd_scene *s = r->scene;
-    const std::vector<int> mbs = {1, 3, 4, 5, 6};
+    const std::vector<int> mbs = {1, 3, 4, 5, 6, 7, 8};
     const bool guided = guideActive(r->guide);
     rmd_status st = ensureVariants(s, mbs, guided);
     if (st != RMD_OK) return st;
-    // calibration: enough paths for several pool generations, capped in time
+    // pool sizes tried: half, twice and four times the current one
+    const uint32_t cap0 = r->capacity;
+    std::vector<uint32_t> caps;
+    const uint64_t candidates[3] = {(uint64_t)cap0 / 2, 2 * (uint64_t)cap0, 4 * (uint64_t)cap0};
+    for (uint64_t cap : candidates)
+        if (cap >= (1u << 16) && cap <= (1ull << 30)) caps.push_back((uint32_t)cap);
+    // calibration: enough paths for several generations of the largest pool
+    // tried (a pool drained once measures its tail, not its throughput), at
+    // most the caller's samples
     rmd_render_settings cal = *settings;
     cal.film_fp64 = 0;
     const uint64_t pixels = (uint64_t)r->width * r->height;
-    cal.spp = (uint32_t)std::max<uint64_t>(1, std::min<uint64_t>(settings->spp, (4ull * r->capacity + pixels - 1) / pixels));
+    const uint64_t maxCap = std::max<uint64_t>(cap0, caps.empty() ? 0 : *std::max_element(caps.begin(), caps.end()));
+    cal.spp = (uint32_t)std::max<uint64_t>(1, std::min<uint64_t>(settings->spp, (4ull * maxCap + pixels - 1) / pixels));
     cal.first_sample = 1u << 30;  // a sample range the caller does not use
     auto trial = [&](double &ms) -> rmd_status {
         double best = 1e30;
@@ -1442,10 +1451,8 @@ rmd_status rmd_renderer_autotune(rmd_renderer *r, const rmd_render_settings *set
     }
     r->traceBlocksPerSm = bestTb;
     // 3) paths in flight (queue sizes)
-    const uint32_t cap0 = r->capacity;
     uint32_t bestCap = cap0;
-    for (uint32_t cap : {cap0 / 2, cap0 * 2}) {
-        if (cap < (1u << 16)) continue;
+    for (uint32_t cap : caps) {
         size_t freeB = 0, totalB = 0;
         if (cudaMemGetInfo(&freeB, &totalB) != cudaSuccess || pathPoolBytes(cap) > freeB / 2) continue;
         r->capacity = cap;
@@ -2055,14 +2062,20 @@ rmd_status rmd_batch_stats(const rmd_batch *b, rmd_stats *out) {
 
 rmd_status rmd_batch_autotune(rmd_batch *b, const rmd_render_settings *settings, rmd_tune_result *out) {
     if (!b || !settings) return fail(RMD_ERROR_INVALID_ARGUMENT, "NULL argument");
-    const std::vector<int> mbs = {1, 3, 4, 5, 6};
+    const std::vector<int> mbs = {1, 3, 4, 5, 6, 7, 8};
     const bool guided = guideActive(b->guide);
     rmd_status st = batchEnsureVariants(b, mbs, guided);
     if (st != RMD_OK) return st;
-    rmd_render_settings cal = *settings;
+    const uint32_t cap0 = b->capacity;
+    std::vector<uint32_t> caps;  // half, twice and four times the current pool
+    const uint64_t candidates[3] = {(uint64_t)cap0 / 2, 2 * (uint64_t)cap0, 4 * (uint64_t)cap0};
+    for (uint64_t cap : candidates)
+        if (cap >= (1u << 16) && cap <= BATCH_MAX_CAPACITY) caps.push_back((uint32_t)cap);
+    rmd_render_settings cal = *settings;  // several generations of the largest pool tried
     cal.film_fp64 = 0;
+    const uint64_t maxCap = std::max<uint64_t>(cap0, caps.empty() ? 0 : *std::max_element(caps.begin(), caps.end()));
     cal.spp = (uint32_t)std::max<uint64_t>(
-        1, std::min<uint64_t>(settings->spp, (4ull * b->capacity + b->totalPixels - 1) / b->totalPixels));
+        1, std::min<uint64_t>(settings->spp, (4ull * maxCap + b->totalPixels - 1) / b->totalPixels));
     cal.first_sample = BATCH_SAMPLE_MASK - 2 * cal.spp;  // a sample range the caller does not use
     auto trial = [&](double &ms) -> rmd_status {
         double best = 1e30;
@@ -2102,10 +2115,8 @@ rmd_status rmd_batch_autotune(rmd_batch *b, const rmd_render_settings *settings,
         }
     }
     b->traceBlocksPerSm = bestTb;
-    const uint32_t cap0 = b->capacity;
     uint32_t bestCap = cap0;
-    for (uint32_t cap : {cap0 / 2, cap0 * 2}) {
-        if (cap < (1u << 16) || cap > BATCH_MAX_CAPACITY) continue;
+    for (uint32_t cap : caps) {
         size_t freeB = 0, totalB = 0;
         if (cudaMemGetInfo(&freeB, &totalB) != cudaSuccess || pathPoolBytes(cap) > freeB / 2) continue;
         b->capacity = cap;
