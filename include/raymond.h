@@ -485,8 +485,12 @@ typedef struct rmd_tune_result {
  * 64-thread threadgroups (Renderer.swift:471-474, 616-619).  Times short
  * calibration renders of this renderer's scene and size with `settings`
  * (depth, sampling mode, RNG) and keeps the fastest shading-kernel register
- * budget, traversal grid and path-pool size.  Compiles the shading-kernel
- * variants it needs (NVRTC, cached on disk).  Clears the film. */
+ * budget (1 to 8 blocks of 128 per SM), traversal grid and path-pool size
+ * (half, twice or four times the current pool, memory permitting); the
+ * calibration covers several generations of the largest pool tried, at most
+ * settings->spp samples.  Compiles the shading-kernel variants it needs
+ * (NVRTC, cached on disk): with the guide's code when guiding is switched on
+ * for this renderer, without it otherwise.  Clears the film. */
 rmd_status rmd_renderer_autotune(rmd_renderer *r, const rmd_render_settings *settings, rmd_tune_result *out);
 /* Apply launch choices found earlier (by rmd_renderer_autotune, possibly in
  * another process): shade_min_blocks 1..16, trace_blocks_per_sm 1..32,
