@@ -223,3 +223,28 @@ def test_trained_guide_lowers_error(gpu_ctx):
     assert st["steps"] > 100
     assert e_guided < 0.5 * e_plain, (e_plain, e_guided)
     assert e_guided < 0.5 * e_untrained, (e_untrained, e_guided)
+
+
+@pytest.mark.gpu
+def test_guide_switch_selects_the_shading_kernel(gpu_ctx):
+    """A renderer compiles its shading kernel without the guide's code until
+    guiding is switched on, then takes the kernel with it on the next render,
+    and the plain one again once guiding is off: the plain image after the
+    guided render equals the one before it, bit for bit (two samples per
+    pixel, so the film's atomic sums do not depend on their order)."""
+    _, scene = _scene(gpu_ctx, scenes.cornell(seed=1, envmap_exponent=6))
+    W = H = 64
+    r = api.Renderer(scene, W, H)
+    r.render(spp=2, max_depth=8, seed=5, first_sample=0)
+    before = r.film()
+    r.set_guide(sampling=True, training=True, batch_size=1 << 12, steps_per_batch=2, seed=3)
+    r.reset()
+    r.render(spp=2, max_depth=8, seed=5, first_sample=0)
+    guided = r.film()
+    assert np.isfinite(guided).all() and guided.mean() > 0
+    assert r.guide_stats()["steps"] > 0 and r.stats()["ms_guide"] > 0
+    r.set_guide(sampling=False, training=False)
+    r.reset()
+    r.render(spp=2, max_depth=8, seed=5, first_sample=0)
+    assert r.stats()["ms_guide"] == 0
+    assert np.array_equal(r.film(), before)
