@@ -78,6 +78,11 @@ BYTES_FILM_PER_PATH = 16 + 32 + 80
 # of one steady-state launch of the 480x270 case divided by the rays it
 # processed); only the closest-hit kernel's is used
 TRAFFIC_PER_UNIT = {"trace": 76.9}
+# One segment (a closest-hit ray traced and shaded, with its NEE shadow ray) must move at least: ray in 32,
+# hit written and read 20 + 20, path state read and written 32 + 32, next ray 32, hit-triangle attributes
+# 110, shadow ray written 48, read by the shadow trace 32, occlusion flag written and read 8, shadow
+# resolve read 16, film add 24.
+BYTES_PER_SEGMENT = 406
 GUIDED_W, GUIDED_H, GUIDED_DEPTH, GUIDED_ORACLE_SPP, GUIDED_PLAIN_SPP, GUIDED_CHUNK = 1280, 720, 16, 65536, 1024, 32
 # guide settings of the guided legs (configs 4 and 5): Adam steps per 2^20 tracer samples, records per step
 # the guided legs' training settings; the learning rate is three times the
@@ -650,6 +655,11 @@ def main():
                      "frac": achieved / peak, "peak_source": "measured" if peaks else "fallback",
                      "bytes_per_unit": bpu, "traffic": traffic,
                      "units_per_launch": n_units / launches},
+        # the whole path's roofline by the per-segment definition: compulsory structure-of-arrays traffic
+        # of one closest-hit ray traced and shaded with its shadow ray, at the measured segment rate
+        "roofline_segment": {"bound": "hbm", "bytes_per_segment": BYTES_PER_SEGMENT,
+                             "achieved": seg_rate * BYTES_PER_SEGMENT / 1e9, "peak": peak, "unit": "GB/s",
+                             "frac": seg_rate * BYTES_PER_SEGMENT / 1e9 / peak},
         "e2e": None if args.no_e2e else {"value": e2e_value, "unit": "Mpaths/s", "h2d_bytes_per_step": 64 + 40,
                                          "d2h_bytes_per_step": W * H * 3 * 4},
         "gpu_launches": int(tot["iterations"] * 4 + args.steps),
