@@ -237,9 +237,9 @@ def test_guide_switch_selects_the_shading_kernel(gpu_ctx):
     r = api.Renderer(scene, W, H)
     r.render(spp=2, max_depth=8, seed=5, first_sample=0)
     before = r.film()
-    r.set_guide(sampling=True, training=True, batch_size=1 << 12, steps_per_batch=2, seed=3)
+    r.set_guide(sampling=True, training=True, batch_size=1 << 10, steps_per_batch=2, seed=3)
     r.reset()
-    r.render(spp=2, max_depth=8, seed=5, first_sample=0)
+    r.render(spp=8, max_depth=8, seed=5, first_sample=0)
     guided = r.film()
     assert np.isfinite(guided).all() and guided.mean() > 0
     assert r.guide_stats()["steps"] > 0 and r.stats()["ms_guide"] > 0
