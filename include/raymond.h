@@ -536,6 +536,11 @@ typedef struct rmd_guide_stats {
     float reserved;
 } rmd_guide_stats;
 
+/* A renderer that neither samples from nor trains the guide runs a shading
+ * kernel compiled without the guide's code; the first rmd_render after
+ * guiding is switched on takes (and, once per scene and register budget,
+ * compiles with NVRTC, cached on disk) the kernel with it, and the plain one
+ * again after both are switched off. */
 rmd_status rmd_renderer_set_guide(rmd_renderer *r, const rmd_guide_settings *settings);
 rmd_status rmd_renderer_guide_stats(const rmd_renderer *r, rmd_guide_stats *out);
 /* Read (write = 0) or replace (write = 1) the network's FP32 parameters:
