@@ -9,9 +9,12 @@
 // triangle (leaf children's triangles are consecutive, at most 3 per leaf and
 // 24 per node), one meta byte per leaf slot (unary triangle count << 5 |
 // offset), and the child boxes quantised to 8 bits per plane.
-//   Triangles in leaf order, 48 B: world-space v0, v1, v2 (float4 each);
+//   Triangles in leaf order, three copies of each side by side (144 B):
+//   copy k holds v0, v1, v2 (float4 each) with the coordinates rotated so
+//   that axis k comes last, (v[k+1], v[k+2], v[k]); copy 2 is (x, y, z).
 //   v0.w carries the instance index, v1.w the primitive index within the
-//   instance's shape.
+//   instance's shape.  A ray reads the copy of its dominant axis, so the
+//   watertight test needs no per-triangle selection of components.
 //
 // Ray/triangle test: Woop, Benthin, Wald, "Watertight Ray/Triangle
 // Intersection", JCGT 2(1) 2013, evaluated with explicitly rounded products
@@ -33,44 +36,47 @@ struct WideNode {
 
 constexpr int TRAVERSAL_STACK = 32;  // node groups; one per level of the 8-wide tree at most
 
+constexpr int TRI_FLOAT4 = 9;  // float4 per triangle: three rotated copies of its three vertices
+
+// The ray in the frame of the triangle copy it reads: kz is its dominant
+// axis, kx = kz + 1 and ky = kz + 2 (mod 3).  WBW swap kx and ky when d[kz]
+// is negative to keep the winding; that only negates U, V, W, the
+// determinant and T, which leaves t and the barycentrics unchanged bit for
+// bit (rounding is symmetric), so the rotation alone is used.
 struct WatertightRay {
-    int kx, ky, kz;
+    int kz;
     float Sx, Sy, Sz;
-    float3 org;
+    float3 org;  // (o[kx], o[ky], o[kz])
 };
 
 RMD_HD WatertightRay makeWatertight(float3 o, float3 d) {
     WatertightRay r;
     const float ax = fabsf(d.x), ay = fabsf(d.y), az = fabsf(d.z);
     r.kz = (ax > ay) ? (ax > az ? 0 : 2) : (ay > az ? 1 : 2);
-    r.kx = r.kz + 1 == 3 ? 0 : r.kz + 1;
-    r.ky = r.kx + 1 == 3 ? 0 : r.kx + 1;
-    if (comp(d, r.kz) < 0.0f) {
-        const int t = r.kx;
-        r.kx = r.ky;
-        r.ky = t;
-    }
+    const int kx = r.kz + 1 == 3 ? 0 : r.kz + 1;
+    const int ky = kx + 1 == 3 ? 0 : kx + 1;
     const float dz = comp(d, r.kz);
-    r.Sx = __fdiv_rn(comp(d, r.kx), dz);
-    r.Sy = __fdiv_rn(comp(d, r.ky), dz);
+    r.Sx = __fdiv_rn(comp(d, kx), dz);
+    r.Sy = __fdiv_rn(comp(d, ky), dz);
     r.Sz = __frcp_rn(dz);
-    r.org = o;
+    r.org = make_float3(comp(o, kx), comp(o, ky), comp(o, r.kz));
     return r;
 }
 
-// Returns true with t in [tmin, tmax]; b0/b1 the weights of v0/v1.
+// Returns true with t in [tmin, tmax]; b0/b1 the weights of v0/v1.  The
+// vertices are the ray's copy: (v[kx], v[ky], v[kz]).
 RMD_HD bool intersectTriangle(const WatertightRay &r, float3 v0, float3 v1, float3 v2, float tmin, float tmax,
                               float &t, float &b0, float &b1) {
     const float3 A = make_float3(__fsub_rn(v0.x, r.org.x), __fsub_rn(v0.y, r.org.y), __fsub_rn(v0.z, r.org.z));
     const float3 B = make_float3(__fsub_rn(v1.x, r.org.x), __fsub_rn(v1.y, r.org.y), __fsub_rn(v1.z, r.org.z));
     const float3 C = make_float3(__fsub_rn(v2.x, r.org.x), __fsub_rn(v2.y, r.org.y), __fsub_rn(v2.z, r.org.z));
-    const float Akz = comp(A, r.kz), Bkz = comp(B, r.kz), Ckz = comp(C, r.kz);
-    const float Ax = __fsub_rn(comp(A, r.kx), __fmul_rn(r.Sx, Akz));
-    const float Ay = __fsub_rn(comp(A, r.ky), __fmul_rn(r.Sy, Akz));
-    const float Bx = __fsub_rn(comp(B, r.kx), __fmul_rn(r.Sx, Bkz));
-    const float By = __fsub_rn(comp(B, r.ky), __fmul_rn(r.Sy, Bkz));
-    const float Cx = __fsub_rn(comp(C, r.kx), __fmul_rn(r.Sx, Ckz));
-    const float Cy = __fsub_rn(comp(C, r.ky), __fmul_rn(r.Sy, Ckz));
+    const float Akz = A.z, Bkz = B.z, Ckz = C.z;
+    const float Ax = __fsub_rn(A.x, __fmul_rn(r.Sx, Akz));
+    const float Ay = __fsub_rn(A.y, __fmul_rn(r.Sy, Akz));
+    const float Bx = __fsub_rn(B.x, __fmul_rn(r.Sx, Bkz));
+    const float By = __fsub_rn(B.y, __fmul_rn(r.Sy, Bkz));
+    const float Cx = __fsub_rn(C.x, __fmul_rn(r.Sx, Ckz));
+    const float Cy = __fsub_rn(C.y, __fmul_rn(r.Sy, Ckz));
     float U = __fsub_rn(__fmul_rn(Cx, By), __fmul_rn(Cy, Bx));
     float V = __fsub_rn(__fmul_rn(Ax, Cy), __fmul_rn(Ay, Cx));
     float W = __fsub_rn(__fmul_rn(Bx, Ay), __fmul_rn(By, Ax));
@@ -275,9 +281,10 @@ RMD_HD bool traverseStep(TraversalState &s, TraversalStack &stack, const WideNod
         while (triHits) {
             const int ti = (int)n.bases.y + __ffs(triHits) - 1;
             triHits &= triHits - 1u;
-            const float4 a = __ldg(&tris[3 * ti + 0]);
-            const float4 b = __ldg(&tris[3 * ti + 1]);
-            const float4 c = __ldg(&tris[3 * ti + 2]);
+            const float4 *tv = &tris[TRI_FLOAT4 * (size_t)ti + 3 * s.r.wr.kz];  // the ray's copy
+            const float4 a = __ldg(&tv[0]);
+            const float4 b = __ldg(&tv[1]);
+            const float4 c = __ldg(&tv[2]);
             float t, b0, b1;
             if (intersectTriangle(s.r.wr, xyz(a), xyz(b), xyz(c), s.tmin, s.tmax, t, b0, b1)) {
                 if (ANY) {
@@ -328,8 +335,8 @@ RMD_HD bool closestHit(const TraversalState &s, const float4 *__restrict__ tris,
         inst = 0xffffffffu;
         return false;
     }
-    const float4 a = __ldg(&tris[3 * s.hitTri + 0]);
-    const float4 b = __ldg(&tris[3 * s.hitTri + 1]);
+    const float4 a = __ldg(&tris[TRI_FLOAT4 * (size_t)s.hitTri + 6]);  // copy 2: the instance and primitive
+    const float4 b = __ldg(&tris[TRI_FLOAT4 * (size_t)s.hitTri + 7]);
     hit = make_float4(s.tmax, s.b0, s.b1, b.w);
     inst = __float_as_uint(a.w);
     return true;

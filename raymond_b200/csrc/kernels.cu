@@ -379,6 +379,21 @@ __global__ void k_debug_trace(const WideNode *nodes, const float4 *tris, const f
     inst[i] = id;
 }
 
+// The traversal kernels' triangle layout from the builders' (v0, v1, v2 per
+// triangle, float4 each): three copies per triangle, copy k with the
+// coordinates rotated so that axis k comes last (device/traverse.cuh).
+__global__ void k_rotate_triangles(const float4 *__restrict__ in, float4 *__restrict__ out, uint32_t n) {
+    for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+#pragma unroll
+        for (int j = 0; j < 3; j++) {
+            const float4 v = in[3 * (size_t)i + j];
+            out[TRI_FLOAT4 * (size_t)i + 0 + j] = make_float4(v.y, v.z, v.x, v.w);
+            out[TRI_FLOAT4 * (size_t)i + 3 + j] = make_float4(v.z, v.x, v.y, v.w);
+            out[TRI_FLOAT4 * (size_t)i + 6 + j] = v;
+        }
+    }
+}
+
 }  // namespace rmd
 
 // ------------------------------------------------------------- launch wrappers
@@ -430,6 +445,11 @@ cudaError_t rmdLaunchFilmResolve(const float4 *film, const double *film64, int f
 }
 cudaError_t rmdLaunchDebugPrng(uint32_t mode, uint64_t a, uint64_t b, int n, float *out, cudaStream_t s) {
     k_debug_prng<<<1, 1, 0, s>>>(mode, a, b, n, out);
+    return cudaGetLastError();
+}
+cudaError_t rmdLaunchRotateTriangles(const float4 *in, float4 *out, uint32_t n, cudaStream_t s) {
+    if (n == 0) return cudaSuccess;
+    k_rotate_triangles<<<std::min<uint32_t>((n + 255) / 256, 148u * 16u), 256, 0, s>>>(in, out, n);
     return cudaGetLastError();
 }
 cudaError_t rmdLaunchDebugTrace(const WideNode *nodes, const float4 *tris, const float *rays, int n, int any, float *out,

@@ -23,6 +23,8 @@ cudaError_t rmdLaunchFilmResolve(const float4 *film, const double *film64, int f
                                  float exposure, float divisor, uint32_t tonemapping, uint32_t channels,
                                  cudaStream_t s);
 cudaError_t rmdLaunchDebugPrng(uint32_t mode, uint64_t a, uint64_t b, int n, float *out, cudaStream_t s);
+// three rotated copies per triangle (the traversal kernels' layout) from n x (v0, v1, v2)
+cudaError_t rmdLaunchRotateTriangles(const float4 *in, float4 *out, uint32_t n, cudaStream_t s);
 cudaError_t rmdLaunchDebugTrace(const rmd::WideNode *nodes, const float4 *tris, const float *rays, int n, int any,
                                 float *out, uint32_t *inst, uint32_t *errors, cudaStream_t s);
 // The Nishita sky texture of a TEX_SKY node (width x height RGBA float, CIE

@@ -754,6 +754,15 @@ static rmd_status buildSceneData(rmd_context *ctx, const rmd_scene_desc *d, rmd_
         RMD_CUDA(s->bvhNodes.upload(bvh.nodes.data(), bvh.nodes.size() * sizeof(rmdhost::GpuWideNode), st));
         RMD_CUDA(s->bvhTris.upload(bvh.tris.data(), bvh.tris.size() * sizeof(float), st));
     }
+    if (s->triangles) {  // the traversal kernels read three rotated copies of each triangle (device/traverse.cuh)
+        DevBuf rotated;
+        RMD_CUDA(rotated.alloc(s->triangles * TRI_FLOAT4 * sizeof(float4)));
+        RMD_CUDA(rmdLaunchRotateTriangles(s->bvhTris.as<float4>(), rotated.as<float4>(), (uint32_t)s->triangles, st));
+        RMD_CUDA(cudaStreamSynchronize(st));
+        s->bvhTris.adopt(rotated.ptr, rotated.bytes);
+        rotated.ptr = nullptr;
+        rotated.bytes = 0;
+    }
 
     Context &c = s->dctx;
     c.vertices = s->vertices.as<float4>();
@@ -1554,8 +1563,9 @@ rmd_status rmd_test_bvh_read(const rmd_scene *s, void *nodes, uint64_t max_nodes
     if (nodes && s->bvhNodeCount)
         RMD_CUDA(cudaMemcpy(nodes, s->bvhNodes.ptr, s->bvhNodeCount * sizeof(rmdhost::GpuWideNode),
                             cudaMemcpyDeviceToHost));
-    if (tris && s->triangles)
-        RMD_CUDA(cudaMemcpy(tris, s->bvhTris.ptr, s->triangles * 12 * sizeof(float), cudaMemcpyDeviceToHost));
+    if (tris && s->triangles)  // copy 2 of each triangle: the builders' (v0, v1, v2) in world coordinates
+        RMD_CUDA(cudaMemcpy2D(tris, 3 * sizeof(float4), static_cast<const float4 *>(s->bvhTris.ptr) + 6,
+                              TRI_FLOAT4 * sizeof(float4), 3 * sizeof(float4), s->triangles, cudaMemcpyDeviceToHost));
     return RMD_OK;
 }
 
