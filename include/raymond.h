@@ -485,7 +485,7 @@ typedef struct rmd_tune_result {
  * 64-thread threadgroups (Renderer.swift:471-474, 616-619).  Times short
  * calibration renders of this renderer's scene and size with `settings`
  * (depth, sampling mode, RNG) and keeps the fastest shading-kernel register
- * budget (1 to 8 blocks of 128 per SM), traversal grid and path-pool size
+ * budget (1 to 16 blocks of 128 per SM), traversal grid and path-pool size
  * (half, twice or four times the current pool, memory permitting); the
  * calibration covers several generations of the largest pool tried, at most
  * settings->spp samples.  Compiles the shading-kernel variants it needs

@@ -1400,7 +1400,7 @@ static bool guideActive(const GuideState &g) { return g.settings.sampling || g.s
 rmd_status rmd_renderer_autotune(rmd_renderer *r, const rmd_render_settings *settings, rmd_tune_result *out) {
     if (!r || !settings) return fail(RMD_ERROR_INVALID_ARGUMENT, "NULL argument");
     rmd_scene *s = r->scene;
-    const std::vector<int> mbs = {1, 3, 4, 5, 6, 7, 8};
+    const std::vector<int> mbs = {1, 3, 4, 5, 6, 8, 10, 12, 16};
     const bool guided = guideActive(r->guide);
     rmd_status st = ensureVariants(s, mbs, guided);
     if (st != RMD_OK) return st;
@@ -2072,7 +2072,7 @@ rmd_status rmd_batch_stats(const rmd_batch *b, rmd_stats *out) {
 
 rmd_status rmd_batch_autotune(rmd_batch *b, const rmd_render_settings *settings, rmd_tune_result *out) {
     if (!b || !settings) return fail(RMD_ERROR_INVALID_ARGUMENT, "NULL argument");
-    const std::vector<int> mbs = {1, 3, 4, 5, 6, 7, 8};
+    const std::vector<int> mbs = {1, 3, 4, 5, 6, 8, 10, 12, 16};
     const bool guided = guideActive(b->guide);
     rmd_status st = batchEnsureVariants(b, mbs, guided);
     if (st != RMD_OK) return st;
