@@ -77,7 +77,7 @@ BYTES_FILM_PER_PATH = 16 + 32 + 80
 # DRAM bytes per unit measured by ncu (dram__bytes_read.sum + dram__bytes_write.sum
 # of one steady-state launch of the 480x270 case divided by the rays it
 # processed); only the closest-hit kernel's is used
-TRAFFIC_PER_UNIT = {"trace": 76.9}
+TRAFFIC_PER_UNIT = {"trace": 172.3}
 # One segment (a closest-hit ray traced and shaded, with its NEE shadow ray) must move at least: ray in 32,
 # hit written and read 20 + 20, path state read and written 32 + 32, next ray 32, hit-triangle attributes
 # 110, shadow ray written 48, read by the shadow trace 32, occlusion flag written and read 8, shadow
