@@ -1449,7 +1449,7 @@ rmd_status rmd_renderer_autotune(rmd_renderer *r, const rmd_render_settings *set
     selectShade(r, bestMb, guided);
     // 2) traversal blocks per SM
     int bestTb = r->traceBlocksPerSm;
-    for (int tb : {4, 12, 16}) {
+    for (int tb : {4, 8, 12, 16}) {
         r->traceBlocksPerSm = tb;
         double ms;
         if ((st = trial(ms)) != RMD_OK) return st;
@@ -2115,7 +2115,7 @@ rmd_status rmd_batch_autotune(rmd_batch *b, const rmd_render_settings *settings,
     }
     batchSelectShade(b, bestMb, guided);
     int bestTb = b->traceBlocksPerSm;
-    for (int tb : {4, 12, 16}) {
+    for (int tb : {4, 8, 12, 16}) {
         b->traceBlocksPerSm = tb;
         double ms;
         if ((st = trial(ms)) != RMD_OK) return st;
