@@ -63,13 +63,6 @@ __device__ Decoded decode(const float *o) {
     return d;
 }
 
-// mean direction of lobe j: theta = pi st, phi = 2 pi sp
-__device__ float3 lobeMean(const Decoded &d, int j) {
-    float st, ct, sp, cp;
-    sincospif(d.st[j], &st, &ct);
-    sincospif(2.0f * d.sp[j], &sp, &cp);
-    return make_float3(st * cp, st * sp, ct);
-}
 
 // vMF normalisation k / (2 pi (1 - e^{-2k})) for k in [e^-3, e^5], where
 // 1 - e^{-2k} >= 0.09 and needs no expm1
@@ -117,22 +110,24 @@ __device__ GuideMixture pack(const Decoded &d) {
 // The gradient is written as BF16 to out[0..GUIDE_OUTPUTS) (the unused
 // outputs and clamped concentrations zero), one lobe at a time, so nothing of
 // it is held in an indexed local array.
+// The training step's gradient is rounded to BF16, so the fast intrinsics
+// (errors near 1e-6 relative on the concentrations' range [e^-3, e^5] and
+// on angles in [0, 2 pi]) stand in for the precise library functions.
 __device__ float lossGradient(const float *o, float3 w, float pb, float y, float scale, uint16_t *out) {
     const Decoded d = decode(o);
     float v[GUIDE_LOBES], q = 0.0f;
-    float3 mu[GUIDE_LOBES];
     float kappa[GUIDE_LOBES], cosw[GUIDE_LOBES];
 #pragma unroll
     for (int j = 0; j < GUIDE_LOBES; j++) {
-        mu[j] = lobeMean(d, j);
+        const float3 mu = lobeMeanPacked(d, j);
         kappa[j] = __expf(d.logKappa[j]);
-        cosw[j] = dot(mu[j], w);
-        v[j] = vmfNorm(kappa[j]) * __expf(kappa[j] * (cosw[j] - 1.0f));
+        cosw[j] = dot(mu, w);
+        v[j] = vmfNormPacked(kappa[j]) * __expf(kappa[j] * (cosw[j] - 1.0f));
         q += d.lambda[j] * v[j];
     }
     const float a = d.alpha;
     const float pmix = fmaxf(a * q + (1.0f - a) * pb, 1e-20f);
-    const float loss = -y * logf(pmix);
+    const float loss = -y * __logf(pmix);
     for (int c = 4 * GUIDE_LOBES + 1; c < GUIDE_OUTPUTS; c++) out[c] = 0;
     // selection probability: a = amin + (amax - amin) sigmoid(z)
     out[4 * GUIDE_LOBES] = toBf16(-y / pmix * scale * (q - pb) * (GUIDE_ALPHA_MAX - GUIDE_ALPHA_MIN) * d.alphaSig *
@@ -146,16 +141,16 @@ __device__ float lossGradient(const float *o, float3 w, float pb, float y, float
         // concentration: dv/dk = v (1/k - 2 / (e^{2k} - 1) + cos - 1), dk/dlogk = k
         float gk = 0.0f;
         if (!d.kappaClamped[j]) {
-            const float k = kappa[j];
-            const float dlogC = 1.0f / k - 2.0f / expm1f(2.0f * k);
+            const float k = kappa[j];  // e^{2k} - 1 >= 0.105 for k >= e^-3: no cancellation to guard
+            const float dlogC = __fdividef(1.0f, k) - __fdividef(2.0f, __expf(2.0f * k) - 1.0f);
             gk = gv * v[j] * (dlogC + cosw[j] - 1.0f) * k;
         }
         out[4 * j + 2] = toBf16(gk);
         // mean direction: dv/dmu = v k w; mu(theta, phi)
         const float gmu = gv * v[j] * kappa[j];
         float st, ct, sp, cp;
-        sincospif(d.st[j], &st, &ct);
-        sincospif(2.0f * d.sp[j], &sp, &cp);
+        __sincosf(M_PI_F * d.st[j], &st, &ct);
+        __sincosf(2.0f * M_PI_F * d.sp[j], &sp, &cp);
         const float3 dmu_dtheta = make_float3(ct * cp, ct * sp, -st);
         const float3 dmu_dphi = make_float3(-st * sp, st * cp, 0.0f);
         out[4 * j + 0] = toBf16(gmu * dot(w, dmu_dtheta) * M_PI_F * d.st[j] * (1.0f - d.st[j]));
@@ -225,6 +220,15 @@ struct TcSmem {
 };
 
 __device__ __forceinline__ uint32_t smemU32(const void *p) { return (uint32_t)__cvta_generic_to_shared(p); }
+
+// Programmatic dependent launch: a kernel launched with
+// cudaLaunchAttributeProgrammaticStreamSerialization may start while the
+// kernel before it in the stream finishes; it waits here, before reading
+// anything that kernel wrote, until that grid has completed and its writes
+// are visible (no wait for a kernel launched the ordinary way).  The other
+// lets the next such kernel be scheduled before this one ends.
+__device__ __forceinline__ void gridDependencyWait() { asm volatile("griddepcontrol.wait;\n" ::: "memory"); }
+__device__ __forceinline__ void gridDependentsMayLaunch() { asm volatile("griddepcontrol.launch_dependents;\n" ::: "memory"); }
 
 // (lo + blo, hi + bhi) with ReLU as packed BF16 (round to nearest even), hi
 // in the upper half: one paired FP32 add and one converting ReLU
@@ -345,6 +349,13 @@ __device__ __forceinline__ void tmemLd16(uint32_t taddr, float *v) {
     for (int i = 0; i < 16; i++) v[i] = __uint_as_float(r[i]);
 }
 __device__ __forceinline__ void tmemLdWait() { asm volatile("tcgen05.wait::ld.sync.aligned;\n" ::: "memory"); }
+// the wait, with v[0..32) tied to it, so no use of them moves above it
+__device__ __forceinline__ void tmemLdWaitFor(float *v) {
+    asm volatile("tcgen05.wait::ld.sync.aligned;\n"
+                 : "+f"(v[0]), "+f"(v[1]), "+f"(v[2]), "+f"(v[3]), "+f"(v[4]), "+f"(v[5]), "+f"(v[6]), "+f"(v[7]), "+f"(v[8]), "+f"(v[9]), "+f"(v[10]), "+f"(v[11]), "+f"(v[12]), "+f"(v[13]), "+f"(v[14]), "+f"(v[15]), "+f"(v[16]), "+f"(v[17]), "+f"(v[18]), "+f"(v[19]), "+f"(v[20]), "+f"(v[21]), "+f"(v[22]), "+f"(v[23]), "+f"(v[24]), "+f"(v[25]), "+f"(v[26]), "+f"(v[27]), "+f"(v[28]), "+f"(v[29]), "+f"(v[30]), "+f"(v[31])
+                 :
+                 : "memory");
+}
 __device__ __forceinline__ void tcFenceBefore() { asm volatile("tcgen05.fence::before_thread_sync;\n" ::: "memory"); }
 __device__ __forceinline__ void tcFenceAfter() { asm volatile("tcgen05.fence::after_thread_sync;\n" ::: "memory"); }
 __device__ __forceinline__ void asyncProxyFence() { asm volatile("fence.proxy.async.shared::cta;\n" ::: "memory"); }
@@ -709,6 +720,7 @@ __global__ void __launch_bounds__(kTrThreads, 1) k_guide_train_tc(RecordBatch ba
     extern __shared__ __align__(16) unsigned char smem[];
     TrainSmem &sm = *reinterpret_cast<TrainSmem *>(smem);
     const int row = threadIdx.x, warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    gridDependencyWait();  // the previous Adam step's weights (launched overlapped with it)
     // set-up: the weights (forward and transposed, already in their shared-
     // memory layout) arrive by one bulk copy on the mbarrier's phase 0 while
     // the biases load, the tensor memory is allocated and the inputs encode
@@ -867,33 +879,60 @@ __global__ void __launch_bounds__(kTrThreads, 1) k_guide_train_tc(RecordBatch ba
         if (!(ok = trCommitWait(sm, phase))) break;
         first = false;
     }
-    // the CTA's gradient: weights from tensor memory (lanes = output features), biases from shared memory
+    gridDependentsMayLaunch();  // the Adam step's blocks may be scheduled (they wait for this grid's gradient)
+    // the CTA's gradient: weights from tensor memory (lanes = output features), biases from shared memory.
+    // A warp's 32 rows x 32 columns go through shared memory (the input rows, free once the last MMA has
+    // read them; rows padded to 36 floats, so neither side meets a bank conflict) and leave as four
+    // 128-byte row pieces per store instruction instead of 32 scattered 16-byte pieces.
     float *part = net.partials + (size_t)blockIdx.x * GUIDE_PARAMS;
     const bool have = ok && !first;
     if (warp < 2) {
-        const int o = row;  // output feature = tensor-memory lane
         const uint32_t lanes = (uint32_t)(warp * 32) << 16;
-        const int width[4] = {GUIDE_INPUTS, GUIDE_HIDDEN, GUIDE_HIDDEN, GUIDE_HIDDEN};
-        const int outs[4] = {GUIDE_HIDDEN, GUIDE_HIDDEN, GUIDE_HIDDEN, GUIDE_OUTPUTS};
-#pragma unroll 1
-        for (int l = 0; l < 4; l++) {
-#pragma unroll 1
-            for (int c0 = 0; c0 < width[l]; c0 += 32) {
-                float v[32];
-                if (have) {
-                    tmemLd32(tmem + lanes + trColDw(l) + (uint32_t)c0, v);
-                    tmemLdWait();
-                } else {
+        constexpr int kPitch = 36;  // floats per staged row
+        static_assert(2 * 32 * kPitch * sizeof(float) <= sizeof(TrainSmem::x), "gradient staging fits the input rows");
+        float *stage = reinterpret_cast<float *>(sm.x) + warp * 32 * kPitch;
+        // the 11 blocks of 32 columns: layer 0 (160 inputs) five, layers 1-3 two each
+        auto layerOf = [](int q) { return q < 5 ? 0 : 1 + (q - 5) / 2; };
+        auto colOf = [](int q) { return q < 5 ? 32 * q : 32 * ((q - 5) & 1); };
+        auto load = [&](int q, float *v) {
+            if (have) {
+                tmemLd32(tmem + lanes + trColDw(layerOf(q)) + (uint32_t)colOf(q), v);
+            } else {
 #pragma unroll
-                    for (int c = 0; c < 32; c++) v[c] = 0.0f;
-                }
-                if (o < outs[l]) {
-                    // 16-byte stores: every layer offset, row width and column block is a multiple of 4 floats
-                    float4 *dst = reinterpret_cast<float4 *>(part + net.wOffset[l] + o * width[l] + c0);
-#pragma unroll
-                    for (int c = 0; c < 32; c += 4) dst[c / 4] = make_float4(v[c], v[c + 1], v[c + 2], v[c + 3]);
-                }
+                for (int c = 0; c < 32; c++) v[c] = 0.0f;
             }
+        };
+        auto store = [&](int q, const float *v) {
+            const int l = layerOf(q), c0 = colOf(q);
+            const int width = l == 0 ? GUIDE_INPUTS : GUIDE_HIDDEN, outs = l == 3 ? GUIDE_OUTPUTS : GUIDE_HIDDEN;
+            float4 *mine = reinterpret_cast<float4 *>(stage + lane * kPitch);
+#pragma unroll
+            for (int c = 0; c < 32; c += 4) mine[c / 4] = make_float4(v[c], v[c + 1], v[c + 2], v[c + 3]);
+            __syncwarp();
+            // 16-byte pieces: every layer offset, row width and column block is a multiple of 4 floats
+#pragma unroll
+            for (int k = 0; k < 8; k++) {
+                const int r = 4 * k + (lane >> 3), c = 4 * (lane & 7);
+                const int o = warp * 32 + r;  // output feature
+                if (o < outs)
+                    *reinterpret_cast<float4 *>(part + net.wOffset[l] + o * width + c0 + c) =
+                        *reinterpret_cast<const float4 *>(stage + r * kPitch + c);
+            }
+            __syncwarp();
+        };
+        // the next block's tensor-memory load is in flight while this one is stored
+        constexpr int kBlocks = 11;
+        float va[32], vb[32];
+        load(0, va);
+        tmemLdWaitFor(va);
+#pragma unroll 1
+        for (int q = 0; q < kBlocks; q += 2) {
+            if (q + 1 < kBlocks) load(q + 1, vb);
+            store(q, va);
+            tmemLdWaitFor(vb);
+            if (q + 2 < kBlocks) load(q + 2, va);
+            if (q + 1 < kBlocks) store(q + 1, vb);
+            tmemLdWaitFor(va);
         }
     }
     __syncthreads();
@@ -999,13 +1038,13 @@ __global__ void __launch_bounds__(kTcThreads) k_guide_infer(Counters *cnt, const
     tcTeardown(sm, pipe, phase);
 }
 
-// the training CTAs' loss shares summed into *lossOut (one thread)
+// the training CTAs' loss shares summed into *lossOut (the first warp of block 0)
 __device__ __forceinline__ void sumLoss(const GuideNetView &net, int blocks, float *lossOut) {
-    if (blockIdx.x == 0 && threadIdx.x == 0 && lossOut) {
-        float loss = 0.0f;
-        for (int b = 0; b < blocks; b++) loss += net.partials[GUIDE_PARTIAL_LOSS + b];
-        *lossOut = loss;
-    }
+    if (blockIdx.x != 0 || threadIdx.x >= 32 || !lossOut) return;
+    float loss = 0.0f;
+    for (int b = (int)threadIdx.x; b < blocks; b += 32) loss += net.partials[GUIDE_PARTIAL_LOSS + b];
+    for (int off = 16; off > 0; off >>= 1) loss += __shfl_xor_sync(0xffffffffu, loss, off);
+    if (threadIdx.x == 0) *lossOut = loss;
 }
 
 // net.grad += the sum of the training blocks' gradients
@@ -1026,15 +1065,26 @@ __device__ __forceinline__ void storeBf16Weight(const GuideNetView &net, int i, 
     net.image[net.imageIndex[i]] = q;
 }
 
+static_assert(GUIDE_INPUTS == 5 * 32 && GUIDE_HIDDEN == 2 * 32 && GUIDE_OUTPUTS <= GUIDE_HIDDEN,
+              "the gradient write-out walks 5 + 2 + 2 + 2 blocks of 32 columns");
+constexpr int kAdamSplit = 8;  // a power of two, at most 32 (one warp's lanes)
 // Adam step on every parameter; refreshes the bf16 weight copies and clears
-// the gradient.
+// the gradient.  kAdamSplit threads per parameter (neighbouring lanes) each
+// sum every kAdamSplit-th of the blocks' gradient slots, so a thread waits
+// on a fraction of the loads.
 __global__ void k_guide_adam(GuideNetView net, int blocks, float lr, float beta1, float beta2, float eps, float corr1,
                              float corr2, float *lossOut) {
+    gridDependencyWait();  // the training blocks' gradient slots (launched overlapped with them)
+    gridDependentsMayLaunch();
     sumLoss(net, blocks, lossOut);
-    const int i = blockIdx.x * blockDim.x + threadIdx.x;
-    if (i >= GUIDE_PARAMS) return;
-    float gr = net.grad[i];
-    for (int b = 0; b < blocks; b++) gr += net.partials[(size_t)b * GUIDE_PARAMS + i];
+    const int t = blockIdx.x * blockDim.x + threadIdx.x;
+    const int i = t / kAdamSplit, part = t % kAdamSplit;
+    float gr = 0.0f;
+    if (i < GUIDE_PARAMS)
+        for (int b = part; b < blocks; b += kAdamSplit) gr += net.partials[(size_t)b * GUIDE_PARAMS + i];
+    for (int off = 1; off < kAdamSplit; off <<= 1) gr += __shfl_xor_sync(0xffffffffu, gr, off);
+    if (i >= GUIDE_PARAMS || part != 0) return;
+    gr += net.grad[i];
     const float m = beta1 * net.adamM[i] + (1.0f - beta1) * gr;
     const float v = beta2 * net.adamV[i] + (1.0f - beta2) * gr * gr;
     net.adamM[i] = m;
@@ -1127,6 +1177,32 @@ cudaError_t rmdLaunchGuideInfer(const Context &ctx, const PathPool &pool, Counte
     return cudaGetLastError();
 }
 
+constexpr float kAdamBeta1 = 0.9f, kAdamBeta2 = 0.999f;
+// Adam's bias corrections 1 / (1 - beta^step)
+static void adamCorrections(int step, float &corr1, float &corr2) {
+    corr1 = 1.0f / (1.0f - powf(kAdamBeta1, (float)step));
+    corr2 = 1.0f / (1.0f - powf(kAdamBeta2, (float)step));
+}
+
+// Launches `kernel` allowed to start while the kernel before it in the
+// stream finishes (programmatic dependent launch); the kernel waits for that
+// grid before reading its results (gridDependencyWait).
+template <class... Params, class... Args>
+static cudaError_t launchOverlapped(void (*kernel)(Params...), dim3 grid, dim3 block, size_t smem, cudaStream_t s,
+                                   Args... args) {
+    cudaLaunchConfig_t cfg = {};
+    cfg.gridDim = grid;
+    cfg.blockDim = block;
+    cfg.dynamicSmemBytes = smem;
+    cfg.stream = s;
+    cudaLaunchAttribute attr[1];
+    attr[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+    attr[0].val.programmaticStreamSerializationAllowed = 1;
+    cfg.attrs = attr;
+    cfg.numAttrs = 1;
+    return cudaLaunchKernelEx(&cfg, kernel, static_cast<Params>(args)...);
+}
+
 cudaError_t rmdLaunchGuideTrain(const GuideRecord *rec, uint32_t total, uint32_t n, uint32_t seed, uint32_t steps,
                                 const GuideNetView &net, float *scratch, int blocks, float lr, int step,
                                 uint32_t *errors, cudaStream_t s) {
@@ -1148,20 +1224,25 @@ cudaError_t rmdLaunchGuideTrain(const GuideRecord *rec, uint32_t total, uint32_t
             if ((e = cudaGetLastError()) != cudaSuccess) return e;
         }
         batch.seed = seed + k;
-        k_guide_train_tc<<<blocks, kTrThreads, rmdGuideSharedBytes(true), s>>>(batch, sums + k % kSumSlots, net,
-                                                                               errors);
-        if ((e = cudaGetLastError()) != cudaSuccess) return e;
-        if ((e = rmdLaunchGuideAdam(net, blocks, lr, step + (int)k, scratch + 1, s)) != cudaSuccess) return e;
+        // each step's two kernels overlap the tail of the one before (programmatic dependent launch)
+        if ((e = launchOverlapped(k_guide_train_tc, dim3(blocks), dim3(kTrThreads), rmdGuideSharedBytes(true), s, batch,
+                                  (const float *)(sums + k % kSumSlots), net, errors)) != cudaSuccess)
+            return e;
+        float corr1, corr2;
+        adamCorrections(step + (int)k, corr1, corr2);
+        if ((e = launchOverlapped(k_guide_adam, dim3((kAdamSplit * GUIDE_PARAMS + 255) / 256), dim3(256), 0, s, net,
+                                  blocks, lr, kAdamBeta1, kAdamBeta2, 1e-8f, corr1, corr2, scratch + 1)) != cudaSuccess)
+            return e;
     }
     return e;
 }
 
 cudaError_t rmdLaunchGuideAdam(const GuideNetView &net, int blocks, float lr, int step, float *lossOut,
                                cudaStream_t s) {
-    const float beta1 = 0.9f, beta2 = 0.999f;
-    const float corr1 = 1.0f / (1.0f - powf(beta1, (float)step)), corr2 = 1.0f / (1.0f - powf(beta2, (float)step));
-    k_guide_adam<<<(GUIDE_PARAMS + 255) / 256, 256, 0, s>>>(net, blocks, lr, beta1, beta2, 1e-8f, corr1, corr2,
-                                                            lossOut);
+    float corr1, corr2;
+    adamCorrections(step, corr1, corr2);
+    k_guide_adam<<<(kAdamSplit * GUIDE_PARAMS + 255) / 256, 256, 0, s>>>(net, blocks, lr, kAdamBeta1, kAdamBeta2, 1e-8f,
+                                                                         corr1, corr2, lossOut);
     return cudaGetLastError();
 }
 
